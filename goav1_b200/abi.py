@@ -1,0 +1,220 @@
+"""ctypes mirror of include/goav1pf.h (the C ABI of the post-filter chain).
+
+These Structure classes are the Python view of the boundary structs; field
+order and types follow the header exactly.  They carry plain pointers and
+sizes only, so the same layout is what a cgo binding passes from goav1's
+FrameWorkPostFilterContext.
+"""
+
+import ctypes as C
+
+PF_OK = 0
+PF_ERR_INVALID_CDEF = -1
+PF_ERR_INVALID_FILTER = -2
+PF_ERR_INVALID_PLAN = -3
+PF_ERR_UNSUPPORTED = -4
+PF_ERR_SHORT_BUFFER = -5
+PF_ERR_INVALID_FORMAT = -6
+PF_ERR_INVALID_ARG = -7
+PF_ERR_DEVICE = -8
+PF_ERR_TIMEOUT = -9
+PF_ERR_NO_DEVICE = -10
+
+PF_STAGE_LOOP_FILTER = 1 << 0
+PF_STAGE_CDEF = 1 << 1
+PF_STAGE_LOOP_RESTORATION = 1 << 2
+PF_STAGE_FILM_GRAIN = 1 << 3
+PF_STAGE_EXTEND_BORDERS = 1 << 4
+PF_STAGES_ALL = 0x1F
+
+PF_MEM_HOST = 0
+PF_MEM_DEVICE = 1
+
+PF_LR_NONE = 0
+PF_LR_SWITCHABLE = 1
+PF_LR_WIENER = 2
+PF_LR_SGRPROJ = 3
+
+PF_LF_MASK_WORDS = 640
+
+
+class pf_plane(C.Structure):
+    _fields_ = [
+        ("data", C.c_void_p),
+        ("stride", C.c_int64),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("alloc_width", C.c_int32),
+        ("alloc_height", C.c_int32),
+    ]
+
+
+class pf_frame(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("bit_depth", C.c_uint8),
+        ("ss_x", C.c_uint8),
+        ("ss_y", C.c_uint8),
+        ("mono", C.c_uint8),
+        ("memory", C.c_uint8),
+        ("reserved", C.c_uint8 * 3),
+        ("plane", pf_plane * 3),
+    ]
+
+
+class pf_loop_filter(C.Structure):
+    _fields_ = [
+        ("level_y", C.c_uint8 * 2),
+        ("level_u", C.c_uint8),
+        ("level_v", C.c_uint8),
+        ("sharpness", C.c_uint8),
+        ("reserved", C.c_uint8 * 3),
+        ("masks", C.c_void_p),
+        ("sb128_w", C.c_int32),
+        ("sb128_h", C.c_int32),
+        ("level_cache", C.c_void_p),
+        ("mi_cols", C.c_int32),
+        ("mi_rows", C.c_int32),
+    ]
+
+
+class pf_cdef(C.Structure):
+    _fields_ = [
+        ("damping", C.c_uint8),
+        ("bits", C.c_uint8),
+        ("strength_count", C.c_uint8),
+        ("reserved", C.c_uint8),
+        ("y_strength", C.c_uint8 * 8),
+        ("uv_strength", C.c_uint8 * 8),
+        ("index", C.c_void_p),
+        ("read", C.c_void_p),
+        ("index_stride", C.c_int32),
+        ("index_rows", C.c_int32),
+        ("noskip", C.c_void_p),
+    ]
+
+
+class pf_lr_unit(C.Structure):
+    _fields_ = [
+        ("type", C.c_uint8),
+        ("sgr_set", C.c_uint8),
+        ("sgr_xqd", C.c_int8 * 2),
+        ("wiener_v", C.c_int8 * 3),
+        ("wiener_h", C.c_int8 * 3),
+    ]
+
+
+class pf_restoration(C.Structure):
+    _fields_ = [
+        ("type", C.c_uint8 * 3),
+        ("reserved", C.c_uint8),
+        ("unit_size_y", C.c_uint16),
+        ("unit_size_uv", C.c_uint16),
+        ("units", C.c_void_p * 3),
+        ("unit_count", C.c_int32 * 3),
+    ]
+
+
+class pf_film_grain(C.Structure):
+    _fields_ = [
+        ("apply", C.c_uint8),
+        ("chroma_scaling_from_luma", C.c_uint8),
+        ("seed", C.c_uint16),
+        ("num_y_points", C.c_uint8),
+        ("y_points", (C.c_uint8 * 2) * 14),
+        ("num_cb_points", C.c_uint8),
+        ("cb_points", (C.c_uint8 * 2) * 10),
+        ("num_cr_points", C.c_uint8),
+        ("cr_points", (C.c_uint8 * 2) * 10),
+        ("scaling_shift", C.c_uint8),
+        ("ar_coeff_lag", C.c_uint8),
+        ("ar_coeffs_y", C.c_int8 * 24),
+        ("ar_coeffs_cb", C.c_int8 * 25),
+        ("ar_coeffs_cr", C.c_int8 * 25),
+        ("ar_coeff_shift", C.c_uint8),
+        ("grain_scale_shift", C.c_uint8),
+        ("cb_mult", C.c_uint8),
+        ("cb_luma_mult", C.c_uint8),
+        ("cb_offset", C.c_uint16),
+        ("cr_mult", C.c_uint8),
+        ("cr_luma_mult", C.c_uint8),
+        ("cr_offset", C.c_uint16),
+        ("overlap", C.c_uint8),
+        ("clip_to_restricted_range", C.c_uint8),
+        ("matrix_identity", C.c_uint8),
+        ("reserved", C.c_uint8),
+    ]
+
+
+class pf_frame_side(C.Structure):
+    _fields_ = [
+        ("stages", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("lf", pf_loop_filter),
+        ("cdef", pf_cdef),
+        ("lr", pf_restoration),
+        ("fg", pf_film_grain),
+    ]
+
+
+class pf_stats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_uint32),
+        ("cdef_units", C.c_uint32),
+        ("lr_units", C.c_uint32),
+        ("fg_rows", C.c_uint32),
+        ("stage_ms", C.c_float * 5),
+    ]
+
+
+class pf_config(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("timing", C.c_int32),
+        ("max_width", C.c_int64),
+        ("max_height", C.c_int64),
+    ]
+
+
+class pf_batch_item(C.Structure):
+    _fields_ = [
+        ("frame", C.POINTER(pf_frame)),
+        ("side", C.POINTER(pf_frame_side)),
+        ("display", C.POINTER(pf_frame)),
+    ]
+
+
+class pf_cdef_search_params(C.Structure):
+    _fields_ = [
+        ("qindex", C.c_int32),
+        ("damping", C.c_int32),
+        ("max_presets", C.c_int32),
+        ("lam", C.c_double),
+    ]
+
+
+class pf_cdef_search_result(C.Structure):
+    _fields_ = [
+        ("bits", C.c_uint8),
+        ("strength_count", C.c_uint8),
+        ("y_strength", C.c_uint8 * 8),
+        ("uv_strength", C.c_uint8 * 8),
+        ("reserved", C.c_uint8 * 2),
+        ("cost", C.c_double),
+    ]
+
+
+# Every symbol include/goav1pf.h declares (checked by tests/test_abi.py).
+EXPORTED_SYMBOLS = (
+    "pf_abi_version",
+    "pf_status_string",
+    "pf_create",
+    "pf_destroy",
+    "pf_frame_apply",
+    "pf_frame_validate",
+    "pf_sync",
+    "pf_stream",
+    "pf_batch_apply",
+    "pf_cdef_search",
+)

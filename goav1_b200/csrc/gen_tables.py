@@ -1,0 +1,114 @@
+"""Generate pf_tables.h: the normative AV1 data tables the post-filter chain needs.
+
+The tables are AV1 spec data (the 2048-entry film-grain Gaussian sequence and
+the self-guided restoration tables).  They must match goav1 value for value,
+so they are parsed straight out of the reference sources:
+
+  internal/av1/filmgrain/gaussian.go        gaussianSequence
+  internal/av1/restoration/selfguided.go    SGRParameterTable, xByXPlus1, oneByX
+
+Run once where the reference checkout exists; the generated header is
+committed, so builds elsewhere never read the reference.  The film-grain
+table is checked against the checksums goav1's own test pins
+(internal/av1/filmgrain/filmgrain_test.go:2129-2172) before anything is
+written.
+
+Usage: python goav1_b200/csrc/gen_tables.py /path/to/goav1
+"""
+
+import os
+import re
+import sys
+
+
+def _block(text, start_pattern):
+    m = re.search(start_pattern, text)
+    if not m:
+        raise SystemExit("pattern not found: " + start_pattern)
+    depth = 0
+    i = text.index("{", m.end() - 1)
+    for j in range(i, len(text)):
+        if text[j] == "{":
+            depth += 1
+        elif text[j] == "}":
+            depth -= 1
+            if depth == 0:
+                return text[i + 1:j]
+    raise SystemExit("unbalanced block after " + start_pattern)
+
+
+def _ints(body):
+    return [int(v) for v in re.findall(r"-?\d+", re.sub(r"//[^\n]*", "", body))]
+
+
+def parse(ref):
+    fg = open(os.path.join(ref, "internal/av1/filmgrain/gaussian.go")).read()
+    gauss = _ints(_block(fg, r"var gaussianSequence = \[\.\.\.\]int16\{"))
+    sg = open(os.path.join(ref, "internal/av1/restoration/selfguided.go")).read()
+    params_body = _block(sg, r"var SGRParameterTable = \[SGRProjParams\]SGRParams\{")
+    params = []
+    for entry in re.findall(r"Radius: \[2\]uint8\{([^}]*)\}, S: \[2\]int16\{([^}]*)\}", params_body):
+        r = [int(v) for v in entry[0].split(",")]
+        s = [int(v) for v in entry[1].split(",")]
+        params.append((r[0], r[1], s[0], s[1]))
+    xby = _ints(_block(sg, r"var xByXPlus1 = \[256\]uint16\{"))
+    oneby = _ints(_block(sg, r"var oneByX = \[25\]uint16\{"))
+    return gauss, params, xby, oneby
+
+
+def check(gauss, params, xby, oneby):
+    assert len(gauss) == 2048, len(gauss)
+    s = sum(gauss)
+    a = sum(abs(v) for v in gauss)
+    w = sum((i + 1) * v for i, v in enumerate(gauss))
+    if (s, a, w) != (1120, 837192, -8011268):
+        raise SystemExit("gaussian checksum mismatch: %r" % ((s, a, w),))
+    assert len(params) == 16 and len(xby) == 256 and len(oneby) == 25
+
+
+def emit(gauss, params, xby, oneby):
+    out = []
+    out.append("/* Generated by gen_tables.py from goav1's normative AV1 tables")
+    out.append(" * (internal/av1/filmgrain/gaussian.go, internal/av1/restoration/selfguided.go).")
+    out.append(" * Do not edit by hand. */")
+    out.append("#ifndef PF_TABLES_H")
+    out.append("#define PF_TABLES_H")
+    out.append("#include <stdint.h>")
+    out.append("")
+    out.append("#define PF_GAUSSIAN_LEN 2048")
+    out.append("static const int16_t pf_gaussian_sequence[PF_GAUSSIAN_LEN] = {")
+    for i in range(0, len(gauss), 16):
+        out.append("  " + ", ".join(str(v) for v in gauss[i:i + 16]) + ",")
+    out.append("};")
+    out.append("")
+    out.append("/* {r0, r1, s0, s1} per SGR parameter set. */")
+    out.append("static const int16_t pf_sgr_params[16][4] = {")
+    for p in params:
+        out.append("  {%d, %d, %d, %d}," % p)
+    out.append("};")
+    out.append("")
+    out.append("static const uint16_t pf_sgr_x_by_xplus1[256] = {")
+    for i in range(0, 256, 16):
+        out.append("  " + ", ".join(str(v) for v in xby[i:i + 16]) + ",")
+    out.append("};")
+    out.append("")
+    out.append("static const uint16_t pf_sgr_one_by_x[25] = {")
+    out.append("  " + ", ".join(str(v) for v in oneby) + ",")
+    out.append("};")
+    out.append("")
+    out.append("#endif /* PF_TABLES_H */")
+    return "\n".join(out) + "\n"
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    tabs = parse(ref)
+    check(*tabs)
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pf_tables.h")
+    with open(dst, "w") as f:
+        f.write(emit(*tabs))
+    print("wrote", dst)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,466 @@
+"""Seeded synthetic frames and side information for the post-filter workloads.
+
+The reference measures on no public corpus for this path, so every workload
+is generated from a seed: a reconstruction built from 2-D cosine gradients,
+per-8x8 DC offsets and Gaussian noise, plus the decode-time side information
+goav1's decoder would hand its post-filter runner (deblocking edge masks and
+level cache, CDEF index map and noskip words, restoration units, film-grain
+parameters).  Layouts are exactly the reference's (see include/goav1pf.h).
+
+Frames are allocated like goav1's frame.RequiredSize (frame/buffer.go:141-186):
+planes are padded to the 64-pixel superblock grid and reconstruction data
+fills the whole allocation, so the 8-aligned padding that CDEF and the
+deblocking taps may touch holds real samples.
+"""
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+# ---------------------------------------------------------------------------
+# Frame container
+
+
+@dataclass
+class HostFrame:
+    """Planes of one frame in host memory (numpy), with a pf_frame view."""
+
+    width: int
+    height: int
+    bit_depth: int
+    ss_x: int
+    ss_y: int
+    planes: list  # numpy arrays [alloc_h, alloc_w], uint8 or uint16
+    crop: list  # (w, h) per plane
+    mono: int = 0
+
+    @staticmethod
+    def alloc(width, height, bit_depth, ss_x=1, ss_y=1, sb=64):
+        dtype = np.uint8 if bit_depth == 8 else np.uint16
+        aw = (width + sb - 1) // sb * sb
+        ah = (height + sb - 1) // sb * sb
+        planes = [np.zeros((ah, aw), dtype)]
+        crop = [(width, height)]
+        cw, ch = (width + ss_x) >> ss_x, (height + ss_y) >> ss_y
+        planes.append(np.zeros((ah >> ss_y, aw >> ss_x), dtype))
+        planes.append(np.zeros((ah >> ss_y, aw >> ss_x), dtype))
+        crop += [(cw, ch), (cw, ch)]
+        return HostFrame(width, height, bit_depth, ss_x, ss_y, planes, crop)
+
+    def copy(self):
+        return HostFrame(self.width, self.height, self.bit_depth, self.ss_x, self.ss_y,
+                         [p.copy() for p in self.planes], list(self.crop), self.mono)
+
+    def like(self):
+        return HostFrame(self.width, self.height, self.bit_depth, self.ss_x, self.ss_y,
+                         [np.zeros_like(p) for p in self.planes], list(self.crop), self.mono)
+
+    def pf(self, memory=abi.PF_MEM_HOST, ptrs=None):
+        f = abi.pf_frame()
+        f.width, f.height = self.width, self.height
+        f.bit_depth, f.ss_x, f.ss_y, f.mono = self.bit_depth, self.ss_x, self.ss_y, self.mono
+        f.memory = memory
+        for i, p in enumerate(self.planes):
+            f.plane[i].data = ptrs[i] if ptrs is not None else p.ctypes.data
+            f.plane[i].stride = p.strides[0]
+            f.plane[i].width, f.plane[i].height = self.crop[i]
+            f.plane[i].alloc_height, f.plane[i].alloc_width = p.shape
+        return f
+
+    @property
+    def luma_pixels(self):
+        return self.width * self.height
+
+    def nbytes(self):
+        return sum(p.nbytes for p in self.planes)
+
+
+@dataclass
+class SideInfo:
+    """Side information arrays plus the pf_frame_side struct pointing at them."""
+
+    side: abi.pf_frame_side
+    keep: list = field(default_factory=list)  # arrays the struct points into
+    blocks: dict = field(default_factory=dict)  # generator bookkeeping
+
+
+# ---------------------------------------------------------------------------
+# Content
+
+
+def gen_content(rng, frame, noise_sigma, dc_range, mv=(0, 0), params=None):
+    """Cosine-gradient texture + per-8x8 DC offsets + Gaussian noise, clipped.
+
+    params (periods/phases/amplitudes) can be passed so a sequence shares one
+    texture translated by a per-frame motion vector."""
+    maxv = (1 << frame.bit_depth) - 1
+    scale = 1 << (frame.bit_depth - 8)
+    if params is None:
+        params = []
+        for _ in range(3):
+            params.append(dict(
+                px=rng.uniform(8, 64), py=rng.uniform(8, 64),
+                qx=rng.uniform(8, 64), qy=rng.uniform(8, 64),
+                fx=rng.uniform(0, 2 * np.pi), fy=rng.uniform(0, 2 * np.pi),
+                a=rng.uniform(20, 60), b=rng.uniform(10, 40), c=rng.uniform(10, 30)))
+    for i, p in enumerate(frame.planes):
+        h, w = p.shape
+        sx = frame.ss_x if i else 0
+        sy = frame.ss_y if i else 0
+        pr = params[i]
+        ys = (np.arange(h, dtype=np.float64) + (mv[1] >> sy))[:, None]
+        xs = (np.arange(w, dtype=np.float64) + (mv[0] >> sx))[None, :]
+        tex = (128 + pr["a"] * np.cos(2 * np.pi * xs / pr["px"] + pr["fx"])
+               + pr["b"] * np.cos(2 * np.pi * ys / pr["py"] + pr["fy"])
+               + pr["c"] * np.cos(2 * np.pi * xs / pr["qx"]) * np.cos(2 * np.pi * ys / pr["qy"]))
+        tex = tex * scale
+        dc = rng.integers(-dc_range, dc_range + 1, size=((h + 7) // 8, (w + 7) // 8))
+        tex = tex + np.repeat(np.repeat(dc, 8, 0), 8, 1)[:h, :w]
+        if noise_sigma:
+            tex = tex + rng.normal(0.0, noise_sigma, size=(h, w))
+        p[:] = np.clip(np.rint(tex), 0, maxv).astype(p.dtype)
+    return params
+
+
+# ---------------------------------------------------------------------------
+# Block / transform layout
+
+
+def aligned_blocks(rng, mi_cols, mi_rows, sizes=(1, 2, 4, 8)):
+    """Config-0 layout: per aligned 32x32 region one square size from
+    {4,8,16,32} px; transform = block.  Returns a list of (x4, y4, s4)."""
+    blocks = []
+    for y4 in range(0, mi_rows, 8):
+        for x4 in range(0, mi_cols, 8):
+            s4 = int(rng.choice(sizes))
+            for yy in range(y4, min(y4 + 8, mi_rows), s4):
+                for xx in range(x4, min(x4 + 8, mi_cols), s4):
+                    blocks.append((xx, yy, s4, s4))
+    return blocks
+
+
+def quadtree_blocks(rng, mi_cols, mi_rows, split_p=0.55):
+    """Config-1 layout: a random quadtree over 64x64 superblocks down to 4x4.
+    Returns (x4, y4, block s4, tx s4) with tx <= block (and <= 32 px)."""
+    blocks = []
+
+    def rec(x4, y4, s4):
+        if x4 >= mi_cols or y4 >= mi_rows:
+            return
+        if s4 > 1 and rng.random() < split_p:
+            h = s4 // 2
+            for dy in (0, h):
+                for dx in (0, h):
+                    rec(x4 + dx, y4 + dy, h)
+            return
+        tmax = min(s4, 8)
+        choices = [t for t in (1, 2, 4, 8) if t <= tmax]
+        blocks.append((x4, y4, s4, int(rng.choice(choices))))
+
+    for y4 in range(0, mi_rows, 16):
+        for x4 in range(0, mi_cols, 16):
+            rec(x4, y4, 16)
+    return blocks
+
+
+def _class_luma(t4):
+    return np.minimum(np.log2(t4).astype(np.int32), 2)
+
+
+def build_lf_masks(frame, blocks, mi_cols, mi_rows):
+    """Deblocking edge masks in lfmask.FilterMask layout (lfmask/mask.go:25-41).
+
+    An edge sits on every transform boundary (every block is coded intra, so
+    inner transform edges are filtered); its width class is the smaller of
+    the transform classes on its two sides (the rule dav1d's
+    mask_edges_intra/chroma carries through its a[]/l[] context arrays,
+    lfmask/mask.go:334-430)."""
+    sb128_w = (mi_cols + 31) // 32
+    sb128_h = (mi_rows + 31) // 32
+    masks = np.zeros((sb128_h * sb128_w, abi.PF_LF_MASK_WORDS), np.uint16)
+    # Luma transform grid: tx width/height (4-px units) and tx origin per cell.
+    txs = np.zeros((mi_rows, mi_cols), np.int32)
+    tx0x = np.zeros((mi_rows, mi_cols), np.int32)
+    tx0y = np.zeros((mi_rows, mi_cols), np.int32)
+    bsz = np.zeros((mi_rows, mi_cols), np.int32)
+    b0x = np.zeros((mi_rows, mi_cols), np.int32)
+    b0y = np.zeros((mi_rows, mi_cols), np.int32)
+    for (x4, y4, s4, t4) in blocks:
+        ys, xs = slice(y4, min(y4 + s4, mi_rows)), slice(x4, min(x4 + s4, mi_cols))
+        bsz[ys, xs] = s4
+        b0x[ys, xs] = x4
+        b0y[ys, xs] = y4
+        txs[ys, xs] = t4
+        gy, gx = np.mgrid[ys, xs]
+        tx0x[ys, xs] = x4 + ((gx - x4) // t4) * t4
+        tx0y[ys, xs] = y4 + ((gy - y4) // t4) * t4
+
+    def put(region_idx, word_idx, bit):
+        np.bitwise_or.at(masks, (region_idx, word_idx), (1 << bit).astype(np.uint16))
+
+    cls = _class_luma(txs)
+    gy, gx = np.mgrid[0:mi_rows, 0:mi_cols]
+    # vertical edges (dir 0): left side of a tx, x4 > 0
+    sel = (tx0x == gx) & (gx > 0)
+    y, x = gy[sel], gx[sel]
+    k = np.minimum(cls[y, x], cls[y, x - 1])
+    reg = (y // 32) * sb128_w + (x // 32)
+    pos, b = x & 31, y & 31
+    put(reg, ((0 * 32 + pos) * 3 + k) * 2 + (b >> 4), b & 15)
+    sel = (tx0y == gy) & (gy > 0)
+    y, x = gy[sel], gx[sel]
+    k = np.minimum(cls[y, x], cls[y - 1, x])
+    reg = (y // 32) * sb128_w + (x // 32)
+    pos, b = y & 31, x & 31
+    put(reg, ((1 * 32 + pos) * 3 + k) * 2 + (b >> 4), b & 15)
+
+    # Chroma: a block of s4 luma cells owns a chroma transform of
+    # max(1, s4 >> ss) chroma cells (at most 8), aligned to its own size.
+    ssx, ssy = frame.ss_x, frame.ss_y
+    cc, cr = (mi_cols + ssx) >> ssx, (mi_rows + ssy) >> ssy
+    cgy, cgx = np.mgrid[0:cr, 0:cc]
+    ly = np.minimum(cgy << ssy, mi_rows - 1)
+    lx = np.minimum(cgx << ssx, mi_cols - 1)
+    cts = np.clip(np.minimum(bsz[ly, lx] >> ssx, bsz[ly, lx] >> ssy), 1, 8)
+    ct0x = (cgx // cts) * cts
+    ct0y = (cgy // cts) * cts
+    ccls = (cts >= 2).astype(np.int32)
+    rw, rh = 32 >> ssx, 32 >> ssy
+    lane_v, lane_h = 16 >> ssy, 16 >> ssx
+    sel = (ct0x == cgx) & (cgx > 0)
+    y, x = cgy[sel], cgx[sel]
+    k = np.minimum(ccls[y, x], ccls[y, x - 1])
+    reg = (y // rh) * sb128_w + (x // rw)
+    pos, b = x % rw, y % rh
+    put(reg, 384 + ((0 * 32 + pos) * 2 + k) * 2 + b // lane_v, b % lane_v)
+    sel = (ct0y == cgy) & (cgy > 0)
+    y, x = cgy[sel], cgx[sel]
+    k = np.minimum(ccls[y, x], ccls[y - 1, x])
+    reg = (y // rh) * sb128_w + (x // rw)
+    pos, b = y % rh, x % rw
+    put(reg, 384 + ((1 * 32 + pos) * 2 + k) * 2 + b // lane_h, b % lane_h)
+    return masks, sb128_w, sb128_h, (b0x, b0y)
+
+
+def calc_lf_values(level_y, level_u, level_v, seg_deltas):
+    """dav1d_calc_lf_values without delta_lf / mode-ref deltas
+    (lfmask/values.go:59-119): levels[seg] = (YV, YH, U, V)."""
+    out = []
+    for sd in seg_deltas:
+        lv = []
+        for base, d in zip((level_y[0], level_y[1], level_u, level_v), sd):
+            if level_y[0] == 0 and level_y[1] == 0:
+                lv.append(0)
+                continue
+            if base == 0 and len(lv) >= 2:  # chroma with zero base
+                lv.append(0)
+                continue
+            lv.append(int(np.clip(np.clip(base, 0, 63) + d, 0, 63)))
+        out.append(lv)
+    return out
+
+
+def build_level_cache(frame, blocks, mi_cols, mi_rows, seg_of_block, seg_levels):
+    """Level cache: 4 bytes per MI cell [YV, YH, U, V]; chroma cells at chroma
+    coordinates with the luma stride (postfilter_loopfilter_masks.go:135-228)."""
+    lc = np.zeros((mi_rows, mi_cols, 4), np.uint8)
+    ssx, ssy = frame.ss_x, frame.ss_y
+    for bi, (x4, y4, s4, _t4) in enumerate(blocks):
+        lv = seg_levels[seg_of_block[bi]]
+        lc[y4:y4 + s4, x4:x4 + s4, 0] = lv[0]
+        lc[y4:y4 + s4, x4:x4 + s4, 1] = lv[1]
+    cc, cr = (mi_cols + ssx) >> ssx, (mi_rows + ssy) >> ssy
+    owner = np.zeros((mi_rows, mi_cols), np.int32)
+    for bi, (x4, y4, s4, _t4) in enumerate(blocks):
+        owner[y4:y4 + s4, x4:x4 + s4] = bi
+    for cy in range(cr):
+        for cx in range(cc):
+            bi = owner[min(cy << ssy, mi_rows - 1), min(cx << ssx, mi_cols - 1)]
+            lv = seg_levels[seg_of_block[bi]]
+            lc[cy, cx, 2] = lv[2]
+            lc[cy, cx, 3] = lv[3]
+    return lc
+
+
+def build_noskip(blocks, skip, mi_cols, mi_rows):
+    """CDEF noskip words (threading/loop_filter_noskip.go:27-71): 8 bytes per
+    64x64 unit, bit by*8+bx set when the 8x8 block carries residual; bits of
+    blocks outside the frame are preset."""
+    ucols, urows = (mi_cols + 15) >> 4, (mi_rows + 15) >> 4
+    ns = np.zeros((urows, ucols, 8), np.uint8)
+    valid_c, valid_r = mi_cols >> 1, mi_rows >> 1
+    if valid_c & 7:
+        ns[:, ucols - 1, :] |= np.uint8((0xFF << (valid_c & 7)) & 0xFF)
+    if valid_r & 7:
+        ns[urows - 1, :, (valid_r & 7):] = 0xFF
+    for bi, (x4, y4, s4, _t4) in enumerate(blocks):
+        if skip[bi]:
+            continue
+        x0, y0 = x4 >> 1, y4 >> 1
+        x1, y1 = (min(x4 + s4, mi_cols) + 1) >> 1, (min(y4 + s4, mi_rows) + 1) >> 1
+        for y in range(y0, y1):
+            for x in range(x0, x1):
+                ns[y >> 3, x >> 3, y & 7] |= np.uint8(1 << (x & 7))
+    return ns
+
+
+# ---------------------------------------------------------------------------
+# Workload builders
+
+
+def _pack_cdef(pri, sec):
+    code = {0: 0, 1: 1, 2: 2, 4: 3}[sec]
+    return (pri << 2) | code
+
+
+def make_frame(config, seed, frame_index=0, texture=None, width=None, height=None,
+               bit_depth=None, ss=None, stages=abi.PF_STAGES_ALL):
+    """Builds (HostFrame, SideInfo) for a workload configuration.
+
+    config 0: 352x288 8-bit 4:2:0, deblock + CDEF (aligned square blocks).
+    config 1: 1920x1080 8-bit 4:2:0 full chain (quadtree, segments, LR, FG).
+    config 2: 3840x2160 10-bit 4:2:0 full chain.
+    Sizes / depth / subsampling can be overridden (the batched mix)."""
+    rng = np.random.default_rng([seed, frame_index])
+    if config == 0:
+        W, H, bd, (ssx, ssy) = 352, 288, 8, (1, 1)
+    elif config == 1:
+        W, H, bd, (ssx, ssy) = 1920, 1080, 8, (1, 1)
+    elif config == 2:
+        W, H, bd, (ssx, ssy) = 3840, 2160, 10, (1, 1)
+    else:
+        raise ValueError(config)
+    W = width or W
+    H = height or H
+    bd = bit_depth or bd
+    if ss is not None:
+        ssx, ssy = ss
+    fr = HostFrame.alloc(W, H, bd, ssx, ssy)
+    mi_cols, mi_rows = ((W + 7) >> 3) << 1, ((H + 7) >> 3) << 1
+    if config == 0:
+        gen_content(rng, fr, 4.0, 12)
+        blocks = aligned_blocks(rng, mi_cols, mi_rows)
+        nseg = 1
+    else:
+        scale = 1 << (bd - 8)
+        mv = (int(rng.integers(-8, 9)) * (frame_index + 1), int(rng.integers(-8, 9)) * (frame_index + 1))
+        tex_rng = np.random.default_rng([seed, 0xC0DE])
+        params = texture or None
+        if params is None:
+            params = gen_content(tex_rng, fr.like(), 0, 0)
+        gen_content(rng, fr, 4.0 * scale if bd == 8 else 16.0, 12 * scale if bd == 8 else 48, mv=mv, params=params)
+        blocks = quadtree_blocks(rng, mi_cols, mi_rows)
+        nseg = 8
+    nb = len(blocks)
+    skip = rng.random(nb) < 0.3
+    seg_of_block = rng.integers(0, nseg, size=nb)
+
+    side = abi.pf_frame_side()
+    side.stages = stages
+    keep = []
+
+    # Deblocking.
+    lvl = [int(v) for v in rng.integers(0, 64, size=4)]
+    lf = side.lf
+    lf.level_y[0], lf.level_y[1], lf.level_u, lf.level_v = lvl
+    lf.sharpness = 0
+    seg_deltas = [[0, 0, 0, 0]] if nseg == 1 else [list(rng.integers(-15, 16, size=4)) for _ in range(nseg)]
+    seg_levels = calc_lf_values(lvl[0:2], lvl[2], lvl[3], seg_deltas)
+    masks, sw, sh, _ = build_lf_masks(fr, blocks, mi_cols, mi_rows)
+    lc = build_level_cache(fr, blocks, mi_cols, mi_rows, seg_of_block, seg_levels)
+    keep += [masks, lc]
+    lf.masks, lf.sb128_w, lf.sb128_h = masks.ctypes.data, sw, sh
+    lf.level_cache, lf.mi_cols, lf.mi_rows = lc.ctypes.data, mi_cols, mi_rows
+
+    # CDEF.
+    cd = side.cdef
+    ucols, urows = (W + 63) // 64, (H + 63) // 64
+    if config == 0:
+        cd.bits, cd.damping = 2, 3
+    else:
+        cd.bits, cd.damping = 3, int(rng.integers(3, 7))
+    cd.strength_count = 1 << cd.bits
+    for i in range(cd.strength_count):
+        cd.y_strength[i] = _pack_cdef(int(rng.integers(0, 16)), int(rng.choice([0, 1, 2, 4])))
+        cd.uv_strength[i] = _pack_cdef(int(rng.integers(0, 16)), int(rng.choice([0, 1, 2, 4])))
+    noskip = build_noskip(blocks, skip, mi_cols, mi_rows)
+    index = rng.integers(0, cd.strength_count, size=(urows, ucols)).astype(np.uint8)
+    # Read=false for units whose in-frame 8x8 blocks are all skip.
+    read = np.zeros((urows, ucols), np.uint8)
+    for ur in range(urows):
+        for uc in range(ucols):
+            bc = min(8, (mi_cols >> 1) - uc * 8)
+            br = min(8, (mi_rows >> 1) - ur * 8)
+            word = noskip[ur, uc]
+            any_ns = any(int(word[by]) & ((1 << bc) - 1) for by in range(br))
+            read[ur, uc] = 1 if any_ns else 0
+    keep += [noskip, index, read]
+    cd.index, cd.read = index.ctypes.data, read.ctypes.data
+    cd.index_stride, cd.index_rows = ucols, urows
+    cd.noskip = noskip.ctypes.data
+
+    # Loop restoration.
+    lr = side.lr
+    if config == 0:
+        lr.type[0] = lr.type[1] = lr.type[2] = abi.PF_LR_NONE
+        side.stages &= ~abi.PF_STAGE_LOOP_RESTORATION
+    else:
+        lr.unit_size_y = 128 if config == 1 else 256
+        lr.unit_size_uv = 64 if config == 1 else 128
+        for p in range(3):
+            lr.type[p] = abi.PF_LR_SWITCHABLE
+            us = lr.unit_size_y if p == 0 else lr.unit_size_uv
+            pw, ph = fr.crop[p]
+            hz = max(1, (pw + us // 2) // us)
+            vt = max(1, (ph + us // 2) // us)
+            units = (abi.pf_lr_unit * (hz * vt))()
+            for i in range(hz * vt):
+                u = units[i]
+                u.type = [abi.PF_LR_NONE, abi.PF_LR_WIENER, abi.PF_LR_SGRPROJ][int(rng.integers(0, 3))]
+                t0 = 0 if p else int(rng.integers(-5, 11))
+                u.wiener_v[0], u.wiener_v[1], u.wiener_v[2] = t0, int(rng.integers(-23, 9)), int(rng.integers(-17, 47))
+                t0 = 0 if p else int(rng.integers(-5, 11))
+                u.wiener_h[0], u.wiener_h[1], u.wiener_h[2] = t0, int(rng.integers(-23, 9)), int(rng.integers(-17, 47))
+                u.sgr_set = int(rng.integers(0, 16))
+                u.sgr_xqd[0], u.sgr_xqd[1] = int(rng.integers(-96, 32)), int(rng.integers(-32, 96))
+            keep.append(units)
+            lr.units[p] = C.addressof(units)
+            lr.unit_count[p] = hz * vt
+
+    # Film grain.
+    fg = side.fg
+    if config == 0:
+        side.stages &= ~abi.PF_STAGE_FILM_GRAIN
+    else:
+        fg.apply = 1
+        fg.seed = int(rng.integers(0, 65536))
+        fg.num_y_points = 14
+        xs = np.sort(rng.choice(256, size=14, replace=False))
+        for i in range(14):
+            fg.y_points[i][0], fg.y_points[i][1] = int(xs[i]), int(rng.integers(0, 256))
+        fg.chroma_scaling_from_luma = 0
+        for pts, name in ((fg.cb_points, "num_cb_points"), (fg.cr_points, "num_cr_points")):
+            xs = np.sort(rng.choice(256, size=10, replace=False))
+            for i in range(10):
+                pts[i][0], pts[i][1] = int(xs[i]), int(rng.integers(0, 256))
+            setattr(fg, name, 10)
+        fg.scaling_shift = 11 if config == 2 else int(rng.integers(8, 12))
+        fg.ar_coeff_lag = 3
+        for i in range(24):
+            fg.ar_coeffs_y[i] = int(rng.integers(-128, 128))
+        for i in range(25):
+            fg.ar_coeffs_cb[i] = int(rng.integers(-128, 128))
+            fg.ar_coeffs_cr[i] = int(rng.integers(-128, 128))
+        fg.ar_coeff_shift = int(rng.integers(6, 10))
+        fg.grain_scale_shift = 0
+        fg.cb_mult, fg.cb_luma_mult, fg.cb_offset = int(rng.integers(0, 256)), int(rng.integers(0, 256)), int(rng.integers(0, 512))
+        fg.cr_mult, fg.cr_luma_mult, fg.cr_offset = int(rng.integers(0, 256)), int(rng.integers(0, 256)), int(rng.integers(0, 512))
+        fg.overlap = 1
+        fg.clip_to_restricted_range = 0
+        fg.matrix_identity = 0
+
+    si = SideInfo(side=side, keep=keep, blocks=dict(blocks=blocks, skip=skip))
+    return fr, si

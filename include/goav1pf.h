@@ -1,0 +1,295 @@
+/*
+ * goav1pf.h - C ABI of the B200 AV1 post-reconstruction filter chain.
+ *
+ * This is the drop-in boundary for goav1's decoder post-filter runner and its
+ * encoder CDEF strength search.  Every entry point takes plain pointers and
+ * sizes; nothing here names a PyTorch or CUDA-runtime type, so cgo, ctypes or
+ * any C caller can bind it directly.
+ *
+ * Reference interfaces each part replaces (paths inside thesyncim/goav1):
+ *   - pf_frame_apply      internal/av1/decoder/work.go:151-155
+ *                          (FrameWorkPostFilterRunner.Apply) as implemented by
+ *                          decoderFrameWorkReusableSupportedPostFilterRunner,
+ *                          decoder_postfilter_bind.go:398-440; its display
+ *                          output replaces PostFilterOutput()
+ *                          (decoder_postfilter_bind.go:252-256, :434-439).
+ *   - pf_cdef_search      internal/av1/encoder/cdef_search.go:580-634
+ *                          (cdefSearcher.search) + :886-945 (finish).
+ *   - status codes        sentinel errors: cdef.ErrInvalidCDEF
+ *                          (cdef/direction.go:11), loopfilter.ErrInvalidFilter,
+ *                          tile.ErrInvalidPlan, decoder.ErrUnsupportedPostFilter,
+ *                          frame.ErrShortBuffer.
+ *
+ * Side-information layouts are the reference's own decode-time products, so a
+ * Go runner passes its slices through unchanged:
+ *   - loop-filter edge masks: lfmask.FilterMask per 128x128 region
+ *     (lfmask/mask.go:25-41): Y[2][32][3][2] then UV[2][32][2][2] uint16;
+ *   - level cache: 4 bytes per 4x4 MI cell [YV, YH, U, V]
+ *     (threading/loop_filter_masks.go:20-27, lfmask/build.go:25-32);
+ *   - CDEF noskip words: 8 bytes per 64x64 unit, bit by*8+bx
+ *     (threading/loop_filter_noskip.go:5-19);
+ *   - CDEF index map: Index[] / Read[] per unit (threading/cdef_index.go:13-18).
+ */
+#ifndef GOAV1PF_H
+#define GOAV1PF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PF_ABI_VERSION 1
+
+/* ---- status codes (negative = error; the frame is untouched on every error
+ *      reported before any kernel was queued, mirroring the reference's
+ *      validate-before-mutate rule, postfilter.go:596-613) ---- */
+enum {
+  PF_OK = 0,
+  PF_ERR_INVALID_CDEF = -1,      /* cdef.ErrInvalidCDEF */
+  PF_ERR_INVALID_FILTER = -2,    /* loopfilter.ErrInvalidFilter */
+  PF_ERR_INVALID_PLAN = -3,      /* tile.ErrInvalidPlan (loop restoration) */
+  PF_ERR_UNSUPPORTED = -4,       /* decoder.ErrUnsupportedPostFilter */
+  PF_ERR_SHORT_BUFFER = -5,      /* frame.ErrShortBuffer */
+  PF_ERR_INVALID_FORMAT = -6,    /* frame.ErrInvalidFormat (film grain) */
+  PF_ERR_INVALID_ARG = -7,       /* null pointer, bad size or enum */
+  PF_ERR_DEVICE = -8,            /* a CUDA call failed */
+  PF_ERR_TIMEOUT = -9,           /* a bounded device wait ran out */
+  PF_ERR_NO_DEVICE = -10         /* no usable sm_100 device */
+};
+
+/* ---- stage bits (FrameWorkPostFilterStage, postfilter.go:13-21) ---- */
+enum {
+  PF_STAGE_LOOP_FILTER = 1u << 0,
+  PF_STAGE_CDEF = 1u << 1,
+  PF_STAGE_LOOP_RESTORATION = 1u << 2,
+  PF_STAGE_FILM_GRAIN = 1u << 3,
+  /* Edge-replicate the planes into their allocated padding after loop
+   * restoration (frame.Frame.ExtendBordersFrom, applied when the frame
+   * refreshes a reference slot, postfilter.go:769-771). */
+  PF_STAGE_EXTEND_BORDERS = 1u << 4
+};
+
+enum { PF_MEM_HOST = 0, PF_MEM_DEVICE = 1 };
+
+/* Restoration types (parser.RestorationType, parser/restoration.go). */
+enum {
+  PF_LR_NONE = 0,
+  PF_LR_SWITCHABLE = 1,
+  PF_LR_WIENER = 2,
+  PF_LR_SGRPROJ = 3
+};
+
+/* One plane of a frame.  data points at sample (0,0); 10/12-bit samples are
+ * little-endian uint16 (frame/buffer.go, cdef/filter.go:366). */
+typedef struct pf_plane {
+  void* data;
+  int64_t stride;        /* bytes between rows */
+  int32_t width;         /* cropped (visible) width in samples */
+  int32_t height;        /* cropped (visible) height */
+  int32_t alloc_width;   /* allocated width in samples (>= 8-aligned width) */
+  int32_t alloc_height;  /* allocated rows (>= 8-aligned height) */
+} pf_plane;
+
+/* A frame (frame.Frame, frame/buffer.go:128-141).  width/height are the
+ * cropped luma size (FrameSize.CodedWidth x Height; super-res is not
+ * supported).  Chroma planes are ((width+ss_x)>>ss_x) x ((height+ss_y)>>ss_y). */
+typedef struct pf_frame {
+  int32_t width;
+  int32_t height;
+  uint8_t bit_depth;     /* 8, 10 or 12 */
+  uint8_t ss_x;
+  uint8_t ss_y;
+  uint8_t mono;
+  uint8_t memory;        /* PF_MEM_HOST or PF_MEM_DEVICE */
+  uint8_t reserved[3];
+  pf_plane plane[3];
+} pf_frame;
+
+/* lfmask.FilterMask: 384 uint16 of Y masks then 256 of UV masks. */
+#define PF_LF_MASK_WORDS 640
+
+typedef struct pf_loop_filter {
+  uint8_t level_y[2];    /* LoopFilterParams.LevelY (vertical, horizontal) */
+  uint8_t level_u;
+  uint8_t level_v;
+  uint8_t sharpness;
+  uint8_t reserved[3];
+  const uint16_t* masks; /* sb128_w*sb128_h*PF_LF_MASK_WORDS */
+  int32_t sb128_w;
+  int32_t sb128_h;
+  const uint8_t* level_cache; /* 4*mi_cols*mi_rows */
+  int32_t mi_cols;       /* ((width+7)>>3)<<1, the decoder's MI grid */
+  int32_t mi_rows;       /* ((height+7)>>3)<<1 */
+} pf_loop_filter;
+
+typedef struct pf_cdef {
+  uint8_t damping;       /* CDEFParams.Damping (3..6) */
+  uint8_t bits;
+  uint8_t strength_count;
+  uint8_t reserved;
+  uint8_t y_strength[8]; /* packed pri<<2 | sec code */
+  uint8_t uv_strength[8];
+  const uint8_t* index;  /* unit grid, row stride = index_stride */
+  const uint8_t* read;   /* 0/1 per unit */
+  int32_t index_stride;
+  int32_t index_rows;
+  const uint8_t* noskip; /* 8 bytes per unit, unit_cols*unit_rows, or NULL =
+                            every block filtered */
+} pf_cdef;
+
+/* One decoded restoration unit (tile.RestorationUnit). */
+typedef struct pf_lr_unit {
+  uint8_t type;          /* PF_LR_NONE / PF_LR_WIENER / PF_LR_SGRPROJ */
+  uint8_t sgr_set;       /* SGRProjInfo.ParamsIndex */
+  int8_t sgr_xqd[2];     /* SGRProjInfo.XQD */
+  int8_t wiener_v[3];    /* taps 0..2 of the vertical filter */
+  int8_t wiener_h[3];    /* taps 0..2 of the horizontal filter */
+} pf_lr_unit;
+
+typedef struct pf_restoration {
+  uint8_t type[3];       /* frame type per plane (PF_LR_*) */
+  uint8_t reserved;
+  uint16_t unit_size_y;
+  uint16_t unit_size_uv;
+  const pf_lr_unit* units[3]; /* horz*vert units per plane, raster order */
+  int32_t unit_count[3];      /* entries available in units[p] */
+} pf_restoration;
+
+/* parser.FilmGrainParams (parser/film_grain.go:21-56). */
+typedef struct pf_film_grain {
+  uint8_t apply;
+  uint8_t chroma_scaling_from_luma;
+  uint16_t seed;
+  uint8_t num_y_points;
+  uint8_t y_points[14][2];
+  uint8_t num_cb_points;
+  uint8_t cb_points[10][2];
+  uint8_t num_cr_points;
+  uint8_t cr_points[10][2];
+  uint8_t scaling_shift;
+  uint8_t ar_coeff_lag;
+  int8_t ar_coeffs_y[24];
+  int8_t ar_coeffs_cb[25];
+  int8_t ar_coeffs_cr[25];
+  uint8_t ar_coeff_shift;
+  uint8_t grain_scale_shift;
+  uint8_t cb_mult;
+  uint8_t cb_luma_mult;
+  uint16_t cb_offset;
+  uint8_t cr_mult;
+  uint8_t cr_luma_mult;
+  uint16_t cr_offset;
+  uint8_t overlap;
+  uint8_t clip_to_restricted_range;
+  uint8_t matrix_identity; /* ColorConfig.MatrixCoefficients == identity */
+  uint8_t reserved;
+} pf_film_grain;
+
+/* Everything the runner needs for one frame (FrameWorkPostFilterContext,
+ * work.go:85-101, reduced to its post-filter inputs). */
+typedef struct pf_frame_side {
+  uint32_t stages;       /* PF_STAGE_* still to run */
+  uint32_t reserved;
+  pf_loop_filter lf;
+  pf_cdef cdef;
+  pf_restoration lr;
+  pf_film_grain fg;
+} pf_frame_side;
+
+/* Per-call counters (FrameWorkCDEFPostFilterResult & co.). */
+typedef struct pf_stats {
+  uint32_t completed;    /* PF_STAGE_* bits run */
+  uint32_t cdef_units;
+  uint32_t lr_units;
+  uint32_t fg_rows;
+  float stage_ms[5];     /* device time per stage when timing is on */
+} pf_stats;
+
+typedef struct pf_config {
+  int32_t device;        /* CUDA ordinal */
+  int32_t timing;        /* 1 = record per-stage CUDA events */
+  int64_t max_width;     /* largest luma frame the context will see (0 = grow) */
+  int64_t max_height;
+} pf_config;
+
+typedef struct pf_ctx pf_ctx;
+
+/* Library identity. */
+int pf_abi_version(void);
+const char* pf_status_string(int status);
+
+/* Context life cycle.  One context per decoder; calls on one context are
+ * serialised by the caller (the reference calls Apply once per frame on the
+ * decoder goroutine).  pf_create returns NULL and writes *status on error. */
+pf_ctx* pf_create(const pf_config* cfg, int* status);
+void pf_destroy(pf_ctx* ctx);
+
+/* Runs the stages named in side->stages on `frame` in place (deblock, CDEF,
+ * loop restoration, border extension; the result is the publishable
+ * reference frame) and, when PF_STAGE_FILM_GRAIN is set and grain applies,
+ * writes the grained display picture into `display` (which must have the
+ * same geometry).  Host frames are copied to the device and back inside the
+ * call; device frames are filtered where they lie.  Returns when the work is
+ * complete (host frames) or queued on the context's stream (device frames;
+ * pf_sync waits for it). */
+int pf_frame_apply(pf_ctx* ctx, const pf_frame* frame, const pf_frame_side* side,
+                   const pf_frame* display, pf_stats* stats);
+
+/* Validation alone: the status pf_frame_apply would return before touching
+ * anything. */
+int pf_frame_validate(const pf_frame* frame, const pf_frame_side* side,
+                      const pf_frame* display);
+
+int pf_sync(pf_ctx* ctx);
+
+/* The CUDA stream the context queues on (cudaStream_t as void*), so a caller
+ * that owns device frames can order its own work around the chain. */
+void* pf_stream(pf_ctx* ctx);
+
+/* ---- batched persistent queue: many frames, one launch per stage ---- */
+typedef struct pf_batch_item {
+  const pf_frame* frame;
+  const pf_frame_side* side;
+  const pf_frame* display;
+} pf_batch_item;
+
+/* Filters n device-resident frames of any size, bit depth and chroma format.
+ * Work units of all frames share one queue per stage, drained by persistent
+ * CTAs (one per SM).  Equivalent to n pf_frame_apply calls. */
+int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats* stats);
+
+/* ---- encoder CDEF strength search (cdef_search.go) ---- */
+typedef struct pf_cdef_search_params {
+  int32_t qindex;        /* frame base_q_idx */
+  int32_t damping;       /* 0 = derive 3 + (qindex >> 6) */
+  int32_t max_presets;   /* nb_strengths limit: 1, 2, 4 or 8 */
+  double lambda;         /* RD lambda of svtRDCost */
+} pf_cdef_search_params;
+
+typedef struct pf_cdef_search_result {
+  uint8_t bits;
+  uint8_t strength_count;
+  uint8_t y_strength[8];
+  uint8_t uv_strength[8];
+  uint8_t reserved[2];
+  double cost;
+} pf_cdef_search_result;
+
+/* Exhaustive per-64x64 search: for every filter block and every one of the
+ * 64 packed strengths, the SSE against `source` of the CDEF-filtered
+ * `recon` (luma, and U+V summed for chroma) is written to mse_out
+ * (uint64, [2][n_fb][64]); then the greedy preset selection picks the frame
+ * presets and fb_index_out gets each unit's preset.  recon is the deblocked
+ * frame; noskip as in pf_cdef. */
+int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
+                   const uint8_t* noskip, const pf_cdef_search_params* params,
+                   uint64_t* mse_out, uint8_t* fb_index_out,
+                   pf_cdef_search_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GOAV1PF_H */

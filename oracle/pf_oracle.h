@@ -1,0 +1,82 @@
+/*
+ * pf_oracle.h - CPU oracle for the AV1 post-filter chain (test infrastructure).
+ *
+ * A plain, scalar C++ restatement of goav1's canonical Go paths, used only as
+ * the checker in tests/ and as the CPU-baseline leg of bench.py.  Nothing in
+ * the product (goav1_b200/) links or calls it.  Each function cites the
+ * reference file:line it follows (paths inside thesyncim/goav1).
+ *
+ * Parity pinning: the reference is pure Go and no Go toolchain exists here,
+ * so the reference cannot be run.  The oracle is pinned by the literal
+ * known-answer tests of goav1's own test files (LFSR draws, Gaussian table
+ * checksums, scaling-LUT points, CDEF direction patterns, the filter14 row-7
+ * case, SGR tables, Wiener taps) and by the libaom restatements those tests
+ * use as second oracles; see tests/test_oracle_kat.py.
+ */
+#ifndef PF_ORACLE_H
+#define PF_ORACLE_H
+
+#include "goav1pf.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Whole chain on a host frame, in place; display written when FG applies.
+ * Returns a PF_* status. */
+int oracle_frame_apply(const pf_frame* frame, const pf_frame_side* side,
+                       const pf_frame* display);
+
+/* Single-stage entry points (same semantics, one stage). */
+int oracle_loop_filter(const pf_frame* frame, const pf_frame_side* side);
+int oracle_cdef(const pf_frame* frame, const pf_frame_side* side);
+
+/* ---- kernel-level entry points for known-answer tests ---- */
+/* cdef/direction.go:37-79, :432-467.  img: 8x8 uint16, row stride. */
+int oracle_cdef_find_dir(const uint16_t* img, int stride, int coeff_shift, int32_t* variance);
+/* cdef/filter.go:79-169.  in: CDEF input buffer with origin at in_origin and
+ * stride 144; writes w*h samples to dst (stride w). */
+void oracle_cdef_filter_block(uint16_t* dst, const uint16_t* in, int in_origin,
+                              int pri, int sec, int dir, int pri_damping,
+                              int sec_damping, int coeff_shift, int w, int h);
+/* cdef/filter.go:603-612 */
+int oracle_cdef_adjust_strength(int strength, int32_t variance);
+/* loopfilter/sb.go:348-446 on a line of 16 samples (q0 at index 8). */
+void oracle_lpf_line(uint16_t* line16, int bit_depth, int level, int sharpness, int wd);
+/* filmgrain/random.go */
+uint16_t oracle_lfsr_next(uint16_t* reg, int bits);
+uint16_t oracle_stripe_seed(uint16_t seed, int luma_line);
+/* filmgrain/scaling.go:18-48 */
+int oracle_scaling_lut(uint8_t* dst256, const uint8_t* points, int n);
+int oracle_scale_lut(const uint8_t* lut, int index, int bit_depth);
+/* filmgrain/luma.go:24-82, chroma.go:29-91 */
+int oracle_luma_grain(int16_t* dst /*73*82*/, const pf_film_grain* fg, int bit_depth);
+int oracle_chroma_grain(int16_t* dst /*73*82*/, const int16_t* luma, const pf_film_grain* fg,
+                        int plane, int bit_depth, int ss_x, int ss_y);
+int16_t oracle_gaussian(int index);
+/* restoration/selfguided.go:111-127 */
+void oracle_sgr_decode_xq(const int8_t* xqd, int set, int16_t* xq);
+/* restoration/wiener.go:59-80 on a (w+6)x(h+6) window (stride sstride,
+ * origin at the window's (3,3)). */
+void oracle_wiener(const uint16_t* src, int sstride, uint16_t* dst, int dstride,
+                   int w, int h, const int16_t* vfilter7, const int16_t* hfilter7,
+                   int bit_depth);
+/* restoration/selfguided.go:132-210 */
+void oracle_sgr(const uint16_t* src, int sstride, uint16_t* dst, int dstride,
+                int w, int h, int set, const int8_t* xqd, int bit_depth);
+
+/* Encoder CDEF search (encoder/cdef_search.go); see pf_cdef_search. */
+int oracle_cdef_search(const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
+                       const pf_cdef_search_params* params, uint64_t* mse_out,
+                       uint8_t* fb_index_out, pf_cdef_search_result* result);
+
+/* Per-unit SSE for one strength (the search's inner trial). */
+int oracle_cdef_unit_sse(const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
+                         int damping, int plane, int unit_row, int unit_col,
+                         int packed_strength, uint64_t* sse);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
