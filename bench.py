@@ -1,0 +1,349 @@
+"""Benchmark: bit-exact AV1 post-filter throughput (Mpix/s) on B200.
+
+Workload (one step): the full post-filter chain (deblock -> CDEF -> loop
+restoration -> border extension -> film grain) over a batch of 60 seeded
+1920x1080 8-bit 4:2:0 frames with quadtree partitions, 8 segments, 8 CDEF
+presets, switchable Wiener/SGR restoration units and lag-3 film grain.
+Throughput counts luma pixels of output frames.
+
+  value  - frames and side information resident in HBM; each step filters all
+           frames of the batch (per-rank batch; multi-GPU shards frames, weak
+           scaling, no collective on the data path).
+  e2e    - the same work through the public C ABI with host (pinned) frames:
+           every step copies each frame and its side information up, filters,
+           and copies the reference and display frames back.
+  --impl reference - the reference's CPU path: goav1 is pure Go and no Go
+           toolchain exists on the box, so this times the C++ restatement of
+           goav1's Go path (oracle/) on all host threads.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "bit-exact postfilter Mpix/s"
+UNIT = "Mpix/s"
+CONFIG_NAME = "full chain 1920x1080 8-bit 4:2:0, 60 frames (seed 2)"
+N_FRAMES = 60
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=N_FRAMES)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_batch(n, rank, pinned=False):
+    from goav1_b200 import synth
+
+    frames = []
+    tex = None
+    for i in range(n):
+        fr, si = synth.make_frame(1, 2, frame_index=rank * n + i, texture=tex)
+        frames.append((fr, si))
+    if pinned:
+        import torch
+
+        for fr, _ in frames:
+            for k, p in enumerate(fr.planes):
+                t = torch.empty(p.shape, dtype=torch.uint8, pin_memory=True)
+                a = t.numpy()
+                a[:] = p
+                fr.planes[k] = a
+                fr._pin = getattr(fr, "_pin", []) + [t]
+    return frames
+
+
+def side_bytes(si, fr):
+    s = si.side
+    n = s.lf.sb128_w * s.lf.sb128_h * 640 * 2 + 4 * s.lf.mi_cols * s.lf.mi_rows
+    ucols, urows = (fr.width + 63) // 64, (fr.height + 63) // 64
+    n += 2 * s.cdef.index_stride * s.cdef.index_rows + 8 * ucols * urows
+    from goav1_b200 import abi
+
+    n += sum(s.lr.unit_count[p] * C.sizeof(abi.pf_lr_unit) for p in range(3))
+    return n
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(frames, seconds=10.0):
+    """The oracle (C++ restatement of goav1's Go path) on all host threads over a
+    bounded sample of the workload's frames."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_ctypes
+
+    lib = oracle_ctypes.lib()
+    cores = os.cpu_count() or 1
+    lock = threading.Lock()
+    state = {"i": 0, "px": 0, "frames": 0}
+    t_end = time.perf_counter() + seconds
+
+    def work():
+        while time.perf_counter() < t_end:
+            with lock:
+                i = state["i"]
+                state["i"] += 1
+            fr, si = frames[i % len(frames)]
+            out = fr.copy()
+            disp = fr.like()
+            st = lib.oracle_frame_apply(C.byref(out.pf()), C.byref(si.side), C.byref(disp.pf()))
+            assert st == 0
+            with lock:
+                state["px"] += fr.luma_pixels
+                state["frames"] += 1
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=work) for _ in range(cores)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    dt = time.perf_counter() - t0
+    return {"value": state["px"] / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d frames of the 1080p full-chain workload in %.1f s on %d threads "
+                      "(oracle C++ restatement of goav1's Go path; Go toolchain absent)"
+                      % (state["frames"], dt, cores)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    frames = make_batch(min(args.frames, 8), 0)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(frames, seconds=6.0)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = statistics.mean(vals)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * N_FRAMES * 1920 * 1080 / 1e6 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": CONFIG_NAME}, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": r["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from goav1_b200 import abi
+    from goav1_b200.postfilter import DeviceFrame, PostFilterRunner, device_side
+
+    n = args.frames
+    frames = make_batch(n, rank, pinned=not args.no_e2e)
+    runner = PostFilterRunner(device=local)
+    dev = [(DeviceFrame(fr), DeviceFrame(fr.like()), device_side(si, fr)) for fr, si in frames]
+    pristine = [[t.clone() for t in d.tensors] for d, _, _ in dev]
+    pf_frames = [(d.pf(), s.side, dd.pf()) for d, dd, s in dev]
+    stream = torch.cuda.ExternalStream(runner.stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def reset():
+        with torch.cuda.stream(stream):
+            for (d, _, _), src in zip(dev, pristine):
+                for t, s in zip(d.tensors, src):
+                    t.copy_(s, non_blocking=True)
+            flush.fill_(1)
+
+    def step():
+        for f, s, d in pf_frames:
+            runner.apply(f, s, d)
+
+    # Warm-up.
+    for _ in range(max(args.warmup, 3)):
+        reset()
+        step()
+    torch.cuda.synchronize()
+    launches_per_frame = 8
+    clocks = ClockSampler(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        reset()
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms = statistics.mean(step_ms)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    px = sum(fr.luma_pixels for fr, _ in frames)
+    value = world * px / (ms / 1e3) / 1e6
+
+    # Per-stage device times (CUDA events recorded by the library on its stream).
+    trunner = PostFilterRunner(device=local, timing=True)
+    stage = np.zeros(5)
+    for (f, s, d) in pf_frames:
+        st = trunner.apply(f, s, d)
+        stage += np.array(list(st.stage_ms))
+    trunner.close()
+    stage_names = ["deblock", "cdef", "restoration", "extend", "film_grain"]
+    per_frame = stage / n
+    dom = int(np.argmax(per_frame))
+    c = 1.5
+    frame_px = 1920 * 1080
+    # Algorithmic bytes per frame of each stage (read + write of the planes it
+    # rewrites, side information once); see DESIGN.md.
+    algo = {"deblock": 2 * c * frame_px, "cdef": 2 * c * frame_px, "restoration": 2 * c * frame_px,
+            "extend": 0, "film_grain": 2 * c * frame_px}
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo[stage_names[dom]] / (per_frame[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": stage_names[dom],
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "stage_ms_per_frame": dict(zip(stage_names, [round(float(x), 4) for x in per_frame])),
+                "chain_algorithmic_bytes_per_px": 3 * c + 0.33,
+                "chain_frac": (3 * c + 0.33) * px / (ms / 1e3) / 1e9 / peak}
+
+    # End to end through the public API with host (pinned) buffers.
+    e2e = None
+    if not args.no_e2e:
+        hb = [(fr.copy(), fr.like(), si) for fr, si in frames]
+        for fr, _ in frames:
+            pass
+        h2d = sum(fr.nbytes() + side_bytes(si, fr) for fr, si in frames)
+        d2h = sum(2 * fr.nbytes() for fr, _ in frames)
+        ehost = []
+        for _ in range(2):  # warm-up
+            for out, disp, si in hb:
+                runner.apply(out.pf(), si.side, disp.pf())
+        for k in range(max(1, args.steps // 2)):
+            for (out, disp, si), (fr, _) in zip(hb, frames):
+                for a, b in zip(out.planes, fr.planes):
+                    a[:] = b
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for out, disp, si in hb:
+                runner.apply(out.pf(), si.side, disp.pf())
+            torch.cuda.synchronize()
+            ehost.append(time.perf_counter() - t0)
+        es = statistics.mean(ehost)
+        if world > 1:
+            t = torch.tensor([es], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            es = float(t.item())
+        e2e = {"value": world * px / es / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "note": "pinned host frames, one pf_frame_apply call per frame"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(frames[:8], seconds=10.0)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+                "config": {"workload": CONFIG_NAME, "frames_per_rank": n, "parallelism": "frame-shard x%d" % world,
+                           "l2": "inputs (%.0f MB per rank) larger than L2, and a 256 MB L2 flush between steps"
+                                 % (sum(fr.nbytes() for fr, _ in frames) / 1e6)},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "gpu_launches": launches_per_frame * n * args.steps}
+        print(json.dumps(line))
+    runner.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

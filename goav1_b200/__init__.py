@@ -1,0 +1,48 @@
+"""goav1_b200 - the AV1 post-reconstruction filter chain of goav1 on NVIDIA B200.
+
+The product is libgoav1pf.so (hand-written sm_100a CUDA behind the C ABI in
+include/goav1pf.h).  This package loads it and mirrors goav1's post-filter
+runner interface for Python callers (postfilter.PostFilterRunner).  There is
+no CPU fallback: without the built library or a CUDA device every entry point
+raises.
+"""
+
+import ctypes as C
+import os
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgoav1pf.so")
+_lib = None
+
+
+def lib():
+    """The loaded C-ABI library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("goav1_b200: %s is missing; build it with `python -m goav1_b200.build`" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    L.pf_abi_version.restype = C.c_int
+    L.pf_status_string.argtypes = [C.c_int]
+    L.pf_status_string.restype = C.c_char_p
+    L.pf_create.argtypes = [C.POINTER(abi.pf_config), C.POINTER(C.c_int)]
+    L.pf_create.restype = C.c_void_p
+    L.pf_destroy.argtypes = [C.c_void_p]
+    L.pf_destroy.restype = None
+    L.pf_frame_apply.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame_side),
+                                 C.POINTER(abi.pf_frame), C.POINTER(abi.pf_stats)]
+    L.pf_frame_validate.argtypes = [C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame_side), C.POINTER(abi.pf_frame)]
+    L.pf_sync.argtypes = [C.c_void_p]
+    L.pf_stream.argtypes = [C.c_void_p]
+    L.pf_stream.restype = C.c_void_p
+    L.pf_batch_apply.argtypes = [C.c_void_p, C.POINTER(abi.pf_batch_item), C.c_int32, C.POINTER(abi.pf_stats)]
+    L.pf_cdef_search.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame), C.c_void_p,
+                                 C.POINTER(abi.pf_cdef_search_params), C.c_void_p, C.c_void_p,
+                                 C.POINTER(abi.pf_cdef_search_result)]
+    if L.pf_abi_version() != 1:
+        raise RuntimeError("goav1_b200: ABI version mismatch")
+    _lib = L
+    return L

@@ -150,7 +150,7 @@ class pf_film_grain(C.Structure):
 class pf_frame_side(C.Structure):
     _fields_ = [
         ("stages", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("side_memory", C.c_uint32),
         ("lf", pf_loop_filter),
         ("cdef", pf_cdef),
         ("lr", pf_restoration),

@@ -1,0 +1,334 @@
+// pf_cdef.cu - CDEF on the GPU, one CTA per 64x64 filter unit (all planes).
+//
+// Semantics follow goav1's snapshot walk: internal/av1/decoder/
+// postfilter_cdef.go:525-710 (applyCDEFPostFilterRows), :936-1035
+// (unitStrength, applySnapshot), :1041-1047 (luma direction gate),
+// :1101-1249 (VeryLarge halo fill and the row/column replicate quirk of
+// frameWorkCopyCDEFInput), :1390-1412 (MI-aligned plane extent), :1544-1561
+// (block list from the noskip word); and the kernels cdef/direction.go:37-79,
+// :432-501, cdef/filter.go:79-169, :231-241, :396-543, :603-633.
+//
+// The kernel reads the deblocked frame (never written here) and writes every
+// sample of the unit's MI-aligned extent to the output frame, filtered or
+// copied, so the output is a pure function of the pre-CDEF frame exactly as
+// in the reference's immutable-snapshot walk.  It also saves, straight from
+// the pre-CDEF input, the four rows around each loop-restoration stripe
+// boundary that falls inside the unit (tile/restoration_boundary.go:192-255):
+// the boundary-line save is fused into the CDEF pass instead of a separate
+// frame sweep.
+#include "pf_common.cuh"
+
+namespace pf {
+
+constexpr int kVeryLarge = 0x4000;
+constexpr int kSW = 80;   // smem row stride (64 + 2*8)
+constexpr int kSH = 68;   // smem rows (64 + 2*2)
+
+// (dy, dx) of the two taps of each CDEF direction entry, cdef/filter.go:53-66.
+__constant__ int8_t c_cdef_dir[12][2][2] = {
+    {{1, 0}, {2, 0}},   {{1, 0}, {2, -1}}, {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}},
+    {{0, 1}, {0, 2}},   {{0, 1}, {1, 2}},  {{1, 1}, {2, 2}},   {{1, 0}, {2, 1}},
+    {{1, 0}, {2, 0}},   {{1, 0}, {2, -1}}, {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}},
+};
+
+__device__ __forceinline__ int dir_off(int e, int k) { return c_cdef_dir[e][k][0] * kSW + c_cdef_dir[e][k][1]; }
+
+// Direction cost of direction D over one 8x8 block (cdef/direction.go:37-79
+// partial sums, :469-501 cost).  blk points at the block's top-left in smem.
+template <int D>
+__device__ __forceinline__ int32_t dir_cost(const uint16_t* blk, int shift) {
+  int32_t p[15];
+#pragma unroll
+  for (int k = 0; k < 15; k++) p[k] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int32_t x = (int32_t)(blk[i * kSW + j] >> shift) - 128;
+      if (D == 0) p[i + j] += x;
+      if (D == 1) p[i + (j >> 1)] += x;
+      if (D == 2) p[i] += x;
+      if (D == 3) p[3 + i - (j >> 1)] += x;
+      if (D == 4) p[7 + i - j] += x;
+      if (D == 5) p[3 - (i >> 1) + j] += x;
+      if (D == 6) p[j] += x;
+      if (D == 7) p[(i >> 1) + j] += x;
+    }
+  }
+  if (D == 2 || D == 6) {
+    int32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s += p[i] * p[i];
+    return s * 105;
+  }
+  if (D == 0 || D == 4) {
+    const int32_t div[8] = {840, 420, 280, 210, 168, 140, 120, 105};
+    int32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < 7; i++) s += (p[i] * p[i] + p[14 - i] * p[14 - i]) * div[i];
+    return s + p[7] * p[7] * 105;
+  }
+  return (p[3] * p[3] + p[4] * p[4] + p[5] * p[5] + p[6] * p[6] + p[7] * p[7]) * 105 +
+         (p[0] * p[0] + p[10] * p[10]) * 420 + (p[1] * p[1] + p[9] * p[9]) * 210 +
+         (p[2] * p[2] + p[8] * p[8]) * 140;
+}
+
+__device__ __forceinline__ int32_t dir_cost_any(int d, const uint16_t* blk, int shift) {
+  switch (d) {
+    case 0: return dir_cost<0>(blk, shift);
+    case 1: return dir_cost<1>(blk, shift);
+    case 2: return dir_cost<2>(blk, shift);
+    case 3: return dir_cost<3>(blk, shift);
+    case 4: return dir_cost<4>(blk, shift);
+    case 5: return dir_cost<5>(blk, shift);
+    case 6: return dir_cost<6>(blk, shift);
+    default: return dir_cost<7>(blk, shift);
+  }
+}
+
+__device__ __forceinline__ int constrain(int diff, int threshold, int shift) {
+  const int a = abs(diff);
+  const int l = imin(imax(threshold - (a >> shift), 0), a);
+  return diff < 0 ? -l : l;
+}
+
+__device__ __forceinline__ int constrain_shift(int threshold, int damping) {
+  if (threshold == 0) return 0;
+  return imax(damping - (31 - __clz(threshold)), 0);
+}
+
+__device__ __forceinline__ int adjust_strength(int strength, int32_t variance) {
+  if (variance == 0) return 0;
+  const int32_t v = variance >> 6;
+  const int i = v != 0 ? imin(31 - __clz(v), 12) : 0;
+  return (strength * (4 + i) + 8) >> 4;
+}
+
+// One sample of cdef/filter.go:79-169; c points at the centre sample in smem.
+__device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int sec, int dir, int damping,
+                                              int coeffShift) {
+  const int x = c[0];
+  if (pri == 0 && sec == 0) return x;
+  int sum = 0;
+  int hi = x, lo = x;
+  if (pri) {
+    const int t0 = ((pri >> coeffShift) & 1) ? 3 : 4;
+    const int t1 = ((pri >> coeffShift) & 1) ? 3 : 2;
+    const int sh = constrain_shift(pri, damping);
+    const int o0 = dir_off(dir + 2, 0), o1 = dir_off(dir + 2, 1);
+    const int a0 = c[o0], a1 = c[-o0], a2 = c[o1], a3 = c[-o1];
+    sum += t0 * (constrain(a0 - x, pri, sh) + constrain(a1 - x, pri, sh)) +
+           t1 * (constrain(a2 - x, pri, sh) + constrain(a3 - x, pri, sh));
+    if (sec) {
+      const int m = kVeryLarge - 1;
+      hi = imax(imax(imax(hi, a0 & m), imax(a1 & m, a2 & m)), a3 & m);
+      lo = imin(imin(imin(lo, a0), imin(a1, a2)), a3);
+    }
+  }
+  if (sec) {
+    const int sh = constrain_shift(sec, damping);
+    const int o0a = dir_off(dir + 4, 0), o0b = dir_off(dir + 4, 1);
+    const int o1a = dir_off(dir, 0), o1b = dir_off(dir, 1);
+    const int b0 = c[o0a], b1 = c[-o0a], b2 = c[o1a], b3 = c[-o1a];
+    const int b4 = c[o0b], b5 = c[-o0b], b6 = c[o1b], b7 = c[-o1b];
+    sum += 2 * (constrain(b0 - x, sec, sh) + constrain(b1 - x, sec, sh) + constrain(b2 - x, sec, sh) +
+                constrain(b3 - x, sec, sh)) +
+           constrain(b4 - x, sec, sh) + constrain(b5 - x, sec, sh) + constrain(b6 - x, sec, sh) +
+           constrain(b7 - x, sec, sh);
+    if (pri) {
+      const int m = kVeryLarge - 1;
+      hi = imax(hi, imax(imax(imax(b0 & m, b1 & m), imax(b2 & m, b3 & m)),
+                         imax(imax(b4 & m, b5 & m), imax(b6 & m, b7 & m))));
+      lo = imin(lo, imin(imin(imin(b0, b1), imin(b2, b3)), imin(imin(b4, b5), imin(b6, b7))));
+    }
+  }
+  int y = x + ((8 + sum - (sum < 0)) >> 4);
+  if (pri && sec) y = imin(imax(y, lo), hi);
+  return y;
+}
+
+struct CdefPlaneGeom {
+  int aw[3], ah[3];  // MI-aligned plane extents (frameWorkCDEFAlignedPlane)
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_cdef(DFrame in, DFrame out, CdefArgs a, CdefPlaneGeom g) {
+  __shared__ uint16_t s_in[kSH * kSW];
+  __shared__ uint8_t s_dir[64];
+  __shared__ int32_t s_var[64];
+  __shared__ int32_t s_cost[64 * 8];
+  const int uc = blockIdx.x, ur = blockIdx.y;
+  const int tid = threadIdx.x;
+  const int coeffShift = in.bd - 8;
+  const int mapOff = ur * a.index_stride + uc;
+  const bool rd = a.read[mapOff] != 0;
+  const int idx = a.index[mapOff];
+  uint64_t word = ~0ull;
+  if (a.noskip) {
+    const uint8_t* w = a.noskip + (size_t)(ur * a.ucols + uc) * 8;
+    word = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) word |= (uint64_t)w[i] << (8 * i);
+  }
+  const int nplanes = in.mono ? 1 : 3;
+  for (int plane = 0; plane < nplanes; plane++) {
+    const int xdec = plane ? in.ssx : 0, ydec = plane ? in.ssy : 0;
+    const int Wa = g.aw[plane], Ha = g.ah[plane];
+    const int unitX = (uc * 64) >> xdec, unitY = (ur * 64) >> ydec;
+    const int unitW = imin(64 >> xdec, Wa - unitX), unitH = imin(64 >> ydec, Ha - unitY);
+    if (unitW <= 0 || unitH <= 0) continue;
+    const DPlane& ip = in.pl[plane];
+    const DPlane& op = out.pl[plane];
+    // ---- activity of this (unit, plane), postfilter_cdef.go:936-956 ----
+    bool active = false, needPrimary = false, directionOnly = false;
+    int packed = 0;
+    if (a.filter && a.plane_process[plane] && rd && idx < a.strength_count) {
+      packed = plane == 0 ? a.y_strength[idx] : a.uv_strength[idx];
+      if (plane == 0)
+        needPrimary = (a.y_strength[idx] >> 2) != 0 || (a.chroma_filtering && (a.uv_strength[idx] >> 2) != 0);
+      else
+        needPrimary = (a.uv_strength[idx] >> 2) != 0;
+      directionOnly = plane == 0 && a.chroma_filtering && packed == 0 && (a.uv_strength[idx] >> 2) != 0;
+      active = packed != 0 || directionOnly;
+    }
+    const int bwLog2 = 3 - xdec, bhLog2 = 3 - ydec;
+    const int bcols = (unitW + (1 << bwLog2) - 1) >> bwLog2, brows = (unitH + (1 << bhLog2) - 1) >> bhLog2;
+    uint64_t listed = 0;
+    if (active) {
+      const uint64_t colMask = (1ull << bcols) - 1;
+      for (int by = 0; by < brows; by++) listed |= ((word >> (by * 8)) & colMask) << (by * 8);
+      if (listed == 0) active = false;
+    }
+    const int uwMax = 64 >> xdec;
+    const int rowStep = 256 / uwMax;
+    const int tx = tid % uwMax, ty0 = tid / uwMax;
+    if (!active) {
+      // Copy-through (inactive unit / plane or the CDEF stage is off).
+      if (tx < unitW)
+        for (int y = ty0; y < unitH; y += rowStep)
+          row_ptr<T>(op, unitY + y)[unitX + tx] = row_ptr<T>(ip, unitY + y)[unitX + tx];
+    } else {
+      // ---- stage the unit + halo (frameWorkFillCDEFInputSentinels /
+      //      frameWorkCopyCDEFInput with the replicate quirk) ----
+      const int srcX0 = imax(unitX - 8, 0), srcY0 = imax(unitY - 2, 0);
+      const int srcX1 = imin(unitX + unitW + 8, Wa), srcY1 = imin(unitY + unitH + 2, Ha);
+      const int wantY1 = unitY + unitH + 2, wantX1 = unitX + unitW + 8;
+      const bool rowExt = srcY1 < wantY1 && srcY1 > 0 && unitY + unitH < Ha;
+      const bool colExt = srcX1 < wantX1 && srcX1 > 0 && unitX + unitW < Wa;
+      const int extRowsEnd = srcY0 + (rowExt ? wantY1 - srcY0 : srcY1 - srcY0);
+      const int fillW = unitW + 16, fillH = unitH + 4;
+      for (int i = tid; i < fillH * fillW; i += 256) {
+        const int r = i / fillW, c = i - r * fillW;
+        const int sy = unitY - 2 + r, sx = unitX - 8 + c;
+        int v = kVeryLarge;
+        int ry = -1, rx = -1;
+        if (sy >= srcY0 && sy < srcY1) ry = sy;
+        else if (rowExt && sy >= srcY1 && sy < wantY1) ry = srcY1 - 1;
+        if (sx >= srcX0 && sx < srcX1) {
+          rx = sx;
+        } else if (colExt && sx >= srcX1 && sx < wantX1 && sy >= srcY0 && sy < extRowsEnd) {
+          rx = srcX1 - 1;
+          if (ry < 0) ry = srcY1 - 1;
+        }
+        if (ry >= 0 && rx >= 0) v = row_ptr<T>(ip, ry)[rx];
+        s_in[r * kSW + c] = (uint16_t)v;
+      }
+      __syncthreads();
+      // ---- luma direction search on listed blocks (needPrimary) ----
+      if (plane == 0 && needPrimary) {
+        for (int w = tid; w < 64 * 8; w += 256) {
+          const int b = w >> 3, d = w & 7;
+          const int by = b >> 3, bx = b & 7;
+          if ((listed >> b) & 1) s_cost[w] = dir_cost_any(d, &s_in[(2 + by * 8) * kSW + 8 + bx * 8], coeffShift);
+        }
+        __syncthreads();
+        if (tid < 64 && ((listed >> tid) & 1)) {
+          int best = 0;
+          int32_t bestCost = s_cost[tid * 8];
+          for (int d = 1; d < 8; d++) {
+            const int32_t c = s_cost[tid * 8 + d];
+            if (c > bestCost) {
+              best = d;
+              bestCost = c;
+            }
+          }
+          s_dir[tid] = (uint8_t)best;
+          s_var[tid] = (bestCost - s_cost[tid * 8 + ((best + 4) & 7)]) >> 10;
+        }
+        __syncthreads();
+      }
+      if (plane == 1 && needPrimary && xdec != ydec) {
+        // cdef/filter.go:614-633: U converts the shared grid in place (V reuses it).
+        if (tid < 64 && ((listed >> tid) & 1)) {
+          const uint8_t conv422[8] = {7, 0, 2, 4, 5, 6, 6, 6};
+          const uint8_t conv440[8] = {1, 2, 2, 2, 3, 4, 6, 0};
+          s_dir[tid] = xdec ? conv422[s_dir[tid]] : conv440[s_dir[tid]];
+        }
+        __syncthreads();
+      }
+      // ---- filter ----
+      int lvl, sec;
+      lvl = packed >> 2;
+      sec = packed & 3;
+      if (sec == 3) sec = 4;
+      const int pri = lvl << coeffShift;
+      sec <<= coeffShift;
+      int damping = a.damping + coeffShift;
+      if (plane != 0) damping--;
+      const bool lumaAdjust = plane == 0 && (needPrimary || pri != 0);
+      if (tx < unitW) {
+        for (int y = ty0; y < unitH; y += rowStep) {
+          const int b = ((y >> bhLog2) << 3) + (tx >> bwLog2);
+          const uint16_t* c = &s_in[(2 + y) * kSW + 8 + tx];
+          int v = c[0];
+          if (!directionOnly && ((listed >> b) & 1)) {
+            int strength = pri;
+            if (lumaAdjust) strength = adjust_strength(pri, s_var[b]);
+            const int dir = pri != 0 ? s_dir[b] : 0;
+            v = cdef_filter_px(c, strength, sec, dir, damping, coeffShift);
+          }
+          row_ptr<T>(op, unitY + y)[unitX + tx] = (T)v;
+        }
+      }
+      __syncthreads();
+    }
+    // ---- fused loop-restoration boundary-line save (pre-CDEF rows) ----
+    if (a.save_lines[plane]) {
+      const int Hc = ip.h, Wc = ip.w;
+      const int SHs = 64 >> ydec, off = 8 >> ydec;
+      for (int y = unitY; y < unitY + unitH && y < Hc; y++) {
+        const int k = (y + off + 2) / SHs;
+        const int b = k * SHs - off;
+        const int j = y - (b - 2);
+        if (k < 1 || b >= Hc || j < 0 || j > 3) continue;
+        const T* src = row_ptr<T>(ip, y);
+        for (int x = unitX + tid; x < unitX + unitW && x < Wc; x += 256) {
+          const T v = src[x];
+          reinterpret_cast<T*>(a.lines[plane] + (int64_t)(k * 4 + j) * a.line_stride[plane])[x] = v;
+          if (j == 2 && b + 1 >= Hc)
+            reinterpret_cast<T*>(a.lines[plane] + (int64_t)(k * 4 + 3) * a.line_stride[plane])[x] = v;
+        }
+      }
+    }
+  }
+}
+
+cudaError_t launch_cdef(const DFrame& in, const DFrame& out, const CdefArgs& a, cudaStream_t st) {
+  CdefPlaneGeom g;
+  for (int p = 0; p < 3; p++) {
+    const int xdec = p ? in.ssx : 0, ydec = p ? in.ssy : 0;
+    // MI-aligned extent (frameWorkCDEFAlignedPlane); the validated allocation
+    // always covers it.
+    const int aw = ((in.width + 7) & ~7) >> xdec, ah = ((in.height + 7) & ~7) >> ydec;
+    g.aw[p] = aw;
+    g.ah[p] = ah;
+  }
+  dim3 grd(a.ucols, a.urows);
+  if (in.bd == 8)
+    k_cdef<uint8_t><<<grd, 256, 0, st>>>(in, out, a, g);
+  else
+    k_cdef<uint16_t><<<grd, 256, 0, st>>>(in, out, a, g);
+  return cudaGetLastError();
+}
+
+}  // namespace pf

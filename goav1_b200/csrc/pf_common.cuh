@@ -1,0 +1,96 @@
+// pf_common.cuh - device-side frame views and launch parameter blocks shared
+// by the post-filter kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "goav1pf.h"
+
+namespace pf {
+
+// One plane in device memory.  stride in bytes; w/h cropped; aw/ah allocated.
+struct DPlane {
+  uint8_t* ptr;
+  int64_t stride;
+  int w, h, aw, ah;
+};
+
+struct DFrame {
+  DPlane pl[3];
+  int width, height;  // cropped luma
+  int bd, ssx, ssy, mono;
+};
+
+template <typename T>
+__device__ __forceinline__ T* row_ptr(const DPlane& p, int y) {
+  return reinterpret_cast<T*>(p.ptr + (int64_t)y * p.stride);
+}
+
+__host__ __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ int iclip(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ---- per-frame parameter blocks (passed by value to kernels) ----
+
+struct LfArgs {
+  const uint16_t* masks;
+  const uint8_t* level_cache;
+  int sb128_w, sb128_h, mi_cols, mi_rows;
+  int sharpness;
+  int gate_chroma[3];  // 1 = skip plane (chroma gating)
+};
+
+struct CdefArgs {
+  const uint8_t* index;
+  const uint8_t* read;
+  const uint8_t* noskip;  // may be null
+  int index_stride, ucols, urows;
+  int damping;
+  int filter;           // 0 = copy only (CDEF stage off)
+  int chroma_filtering;
+  int plane_process[3];
+  uint8_t y_strength[8], uv_strength[8];
+  int strength_count;
+  // Loop-restoration boundary lines (pre-CDEF rows), per plane.
+  uint8_t* lines[3];    // [boundary k][4 rows][stride] samples of T
+  int64_t line_stride[3];  // bytes per line row
+  int save_lines[3];
+};
+
+struct LrArgs {
+  const pf_lr_unit* units[3];
+  int type[3];          // frame type per plane
+  int unit_size[3];
+  int horz[3], vert[3];
+  const uint8_t* lines[3];
+  int64_t line_stride[3];
+};
+
+struct FgArgs {
+  int16_t* grain[3];      // 73*82 templates
+  const uint8_t* offsets; // [rows][blocks] offsets of the stripe LFSRs
+  int off_rows, off_cols;
+  uint8_t lut[3][256];
+  int active[3];
+  int scaling_shift;
+  int overlap;
+  int clip_restricted;
+  int matrix_identity;
+  int cfl;
+  int mult[3], luma_mult[3], offset[3];
+  int odd_luma;
+};
+
+struct FgTemplateArgs {
+  uint16_t seed;
+  int bd;
+  int num_y_points;
+  int grain_scale_shift;
+  int lag, coeff_shift;
+  int8_t coeffs[3][25];
+  int active[3];
+  int ssx, ssy;
+};
+
+}  // namespace pf

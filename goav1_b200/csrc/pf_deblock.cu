@@ -1,0 +1,194 @@
+// pf_deblock.cu - AV1 deblocking on the GPU.
+//
+// Follows goav1's mask-driven deblock: internal/av1/decoder/
+// postfilter_loopfilter_masks.go:229-268 (all vertical edges of the frame,
+// then all horizontal edges; chroma gated off when both luma frame levels or
+// the plane's base level are zero), postfilter_loopfilter_masks_sb.go:21-188
+// (the per-128x128-region bitmask walk, edges outside the 4-aligned crop and
+// column/row 0 dropped), loopfilter/sb.go:99-153 (width class from the mask
+// lanes, level fallback to the left/above cell) and sb.go:156-446 (the
+// 4/6/8/16-wide edge kernels).
+//
+// Same-direction edges never overlap (AV1 ties filter width to transform
+// spacing), so every 4-sample edge unit of one direction is independent: one
+// thread owns one unit (4 lines), warps run along the edge grid so the 32
+// threads of a warp touch one 128-byte span per row.
+#include "pf_common.cuh"
+
+namespace pf {
+
+// loopfilter/sb.go:348-446 (lpfUnit16); reduces to lpfUnit8 at bd == 8.
+// q points at q0 of the first line; sa steps along the edge, sb across it
+// (both in elements).
+template <typename T>
+__device__ __forceinline__ void lpf_unit(T* q, int sa, int sb, int bd, int E, int I, int H, int wd) {
+  const int bd8 = bd - 8;
+  const int F = 1 << bd8;
+  E <<= bd8;
+  I <<= bd8;
+  H <<= bd8;
+  const unsigned twoI = 2u * I, twoF = 2u * F, twoH = 2u * H;
+  const int maxPix = (1 << bd) - 1;
+  const int diffMin = -128 << bd8, diffMax = (128 << bd8) - 1;
+#pragma unroll 1
+  for (int i = 0; i < 4; i++, q += sa) {
+    const int p1 = q[-2 * sb], p0 = q[-sb], q0 = q[0], q1 = q[sb];
+    if ((unsigned)(p1 - p0 + I) > twoI || (unsigned)(q1 - q0 + I) > twoI ||
+        abs(p0 - q0) * 2 + (abs(p1 - q1) >> 1) > E)
+      continue;
+    int p2 = 0, q2 = 0, p3 = 0, q3 = 0;
+    if (wd > 4) {
+      p2 = q[-3 * sb];
+      q2 = q[2 * sb];
+      if ((unsigned)(p2 - p1 + I) > twoI || (unsigned)(q2 - q1 + I) > twoI) continue;
+      if (wd > 6) {
+        p3 = q[-4 * sb];
+        q3 = q[3 * sb];
+        if ((unsigned)(p3 - p2 + I) > twoI || (unsigned)(q3 - q2 + I) > twoI) continue;
+      }
+    }
+    bool flat8in = false;
+    if (wd >= 6) {
+      flat8in = (unsigned)(p2 - p0 + F) <= twoF && (unsigned)(p1 - p0 + F) <= twoF &&
+                (unsigned)(q1 - q0 + F) <= twoF && (unsigned)(q2 - q0 + F) <= twoF;
+      if (wd >= 8 && flat8in) flat8in = (unsigned)(p3 - p0 + F) <= twoF && (unsigned)(q3 - q0 + F) <= twoF;
+    }
+    if (flat8in) {
+      if (wd >= 16) {
+        const int p6 = q[-7 * sb], p5 = q[-6 * sb], p4 = q[-5 * sb];
+        const int q4 = q[4 * sb], q5 = q[5 * sb], q6 = q[6 * sb];
+        if ((unsigned)(p6 - p0 + F) <= twoF && (unsigned)(p5 - p0 + F) <= twoF &&
+            (unsigned)(p4 - p0 + F) <= twoF && (unsigned)(q4 - q0 + F) <= twoF &&
+            (unsigned)(q5 - q0 + F) <= twoF && (unsigned)(q6 - q0 + F) <= twoF) {
+          q[-6 * sb] = (T)((p6 * 7 + p5 * 2 + p4 * 2 + p3 + p2 + p1 + p0 + q0 + 8) >> 4);
+          q[-5 * sb] = (T)((p6 * 5 + p5 * 2 + p4 * 2 + p3 * 2 + p2 + p1 + p0 + q0 + q1 + 8) >> 4);
+          q[-4 * sb] = (T)((p6 * 4 + p5 + p4 * 2 + p3 * 2 + p2 * 2 + p1 + p0 + q0 + q1 + q2 + 8) >> 4);
+          q[-3 * sb] = (T)((p6 * 3 + p5 + p4 + p3 * 2 + p2 * 2 + p1 * 2 + p0 + q0 + q1 + q2 + q3 + 8) >> 4);
+          q[-2 * sb] = (T)((p6 * 2 + p5 + p4 + p3 + p2 * 2 + p1 * 2 + p0 * 2 + q0 + q1 + q2 + q3 + q4 + 8) >> 4);
+          q[-sb] = (T)((p6 + p5 + p4 + p3 + p2 + p1 * 2 + p0 * 2 + q0 * 2 + q1 + q2 + q3 + q4 + q5 + 8) >> 4);
+          q[0] = (T)((p5 + p4 + p3 + p2 + p1 + p0 * 2 + q0 * 2 + q1 * 2 + q2 + q3 + q4 + q5 + q6 + 8) >> 4);
+          q[sb] = (T)((p4 + p3 + p2 + p1 + p0 + q0 * 2 + q1 * 2 + q2 * 2 + q3 + q4 + q5 + q6 * 2 + 8) >> 4);
+          q[2 * sb] = (T)((p3 + p2 + p1 + p0 + q0 + q1 * 2 + q2 * 2 + q3 * 2 + q4 + q5 + q6 * 3 + 8) >> 4);
+          q[3 * sb] = (T)((p2 + p1 + p0 + q0 + q1 + q2 * 2 + q3 * 2 + q4 * 2 + q5 + q6 * 4 + 8) >> 4);
+          q[4 * sb] = (T)((p1 + p0 + q0 + q1 + q2 + q3 * 2 + q4 * 2 + q5 * 2 + q6 * 5 + 8) >> 4);
+          q[5 * sb] = (T)((p0 + q0 + q1 + q2 + q3 + q4 * 2 + q5 * 2 + q6 * 7 + 8) >> 4);
+          continue;
+        }
+      }
+      if (wd >= 8) {
+        q[-3 * sb] = (T)((p3 * 3 + p2 * 2 + p1 + p0 + q0 + 4) >> 3);
+        q[-2 * sb] = (T)((p3 * 2 + p2 + p1 * 2 + p0 + q0 + q1 + 4) >> 3);
+        q[-sb] = (T)((p3 + p2 + p1 + p0 * 2 + q0 + q1 + q2 + 4) >> 3);
+        q[0] = (T)((p2 + p1 + p0 + q0 * 2 + q1 + q2 + q3 + 4) >> 3);
+        q[sb] = (T)((p1 + p0 + q0 + q1 * 2 + q2 + q3 * 2 + 4) >> 3);
+        q[2 * sb] = (T)((p0 + q0 + q1 + q2 * 2 + q3 * 3 + 4) >> 3);
+        continue;
+      }
+      q[-2 * sb] = (T)((p2 * 3 + p1 * 2 + p0 * 2 + q0 + 4) >> 3);
+      q[-sb] = (T)((p2 + p1 * 2 + p0 * 2 + q0 * 2 + q1 + 4) >> 3);
+      q[0] = (T)((p1 + p0 * 2 + q0 * 2 + q1 * 2 + q2 + 4) >> 3);
+      q[sb] = (T)((p0 + q0 * 2 + q1 * 2 + q2 * 3 + 4) >> 3);
+      continue;
+    }
+    const bool hev = (unsigned)(p1 - p0 + H) > twoH || (unsigned)(q1 - q0 + H) > twoH;
+    int f;
+    if (hev)
+      f = imin(imax(imin(imax(p1 - q1, diffMin), diffMax) + 3 * (q0 - p0), diffMin), diffMax);
+    else
+      f = imin(imax(3 * (q0 - p0), diffMin), diffMax);
+    const int f1 = imin(f + 4, diffMax) >> 3;
+    const int f2 = imin(f + 3, diffMax) >> 3;
+    q[-sb] = (T)imin(imax(p0 + f2, 0), maxPix);
+    q[0] = (T)imin(imax(q0 - f1, 0), maxPix);
+    if (!hev) {
+      f = (f1 + 1) >> 1;
+      q[-2 * sb] = (T)imin(imax(p1 + f, 0), maxPix);
+      q[sb] = (T)imin(imax(q1 - f, 0), maxPix);
+    }
+  }
+}
+
+// One thread per 4x4 edge unit (c4, r4) of plane blockIdx.z; dir 0 filters
+// the unit's left (vertical) edge, dir 1 its top (horizontal) edge.
+template <typename T>
+__global__ void __launch_bounds__(256) k_deblock(DFrame f, LfArgs a, int dir) {
+  const int plane = blockIdx.z;
+  if (a.gate_chroma[plane]) return;
+  const int c4 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r4 = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ssx = plane ? f.ssx : 0, ssy = plane ? f.ssy : 0;
+  // frameWorkLoopFilterPlaneSize: edge positions inside the 4-aligned crop.
+  const int w4 = ((plane ? (f.width + ssx) >> ssx : f.width) + 3) >> 2;
+  const int h4 = ((plane ? (f.height + ssy) >> ssy : f.height) + 3) >> 2;
+  if (c4 >= w4 || r4 >= h4) return;
+  if (dir == 0 ? c4 == 0 : r4 == 0) return;
+  const bool luma = plane == 0;
+  const int regionW = 32 >> ssx, regionH = 32 >> ssy;
+  const int rCol = c4 / regionW, rRow = r4 / regionH;
+  const int pcol = c4 - rCol * regionW, prow = r4 - rRow * regionH;
+  const uint16_t* region = a.masks + (size_t)(rRow * a.sb128_w + rCol) * PF_LF_MASK_WORDS;
+  const int pos = dir == 0 ? pcol : prow;
+  const int bit = dir == 0 ? prow : pcol;
+  int k = -1;
+  if (luma) {
+    const int half = bit >> 4, b = bit & 15;
+#pragma unroll
+    for (int kk = 2; kk >= 0; kk--) {
+      if (k < 0 && ((region[((dir * 32 + pos) * 3 + kk) * 2 + half] >> b) & 1)) k = kk;
+    }
+  } else {
+    const int lane = dir == 0 ? (16 >> ssy) : (16 >> ssx);
+    const int half = bit / lane, b = bit - half * lane;
+#pragma unroll
+    for (int kk = 1; kk >= 0; kk--) {
+      if (k < 0 && ((region[384 + ((dir * 32 + pos) * 2 + kk) * 2 + half] >> b) & 1)) k = kk;
+    }
+  }
+  if (k < 0) return;
+  const int wd = k == 2 ? 16 : (k == 1 ? (luma ? 8 : 6) : 4);
+  // Level with the left / above fallback (sb.go:122-128, :142-148).
+  const int comp = luma ? dir : plane + 1;
+  const int li = r4 * a.mi_cols + c4;
+  int L = a.level_cache[4 * li + comp];
+  if (L == 0) L = a.level_cache[4 * (dir == 0 ? li - 1 : li - a.mi_cols) + comp];
+  if (L == 0) return;
+  // loopfilter/threshold.go:18-47.
+  const int sh = a.sharpness;
+  int limit = L >> ((sh > 0) + (sh > 4));
+  if (sh > 0 && limit > 9 - sh) limit = 9 - sh;
+  if (limit < 1) limit = 1;
+  const int E = 2 * (L + 2) + limit, I = limit, H = L >> 4;
+  const DPlane& pl = f.pl[plane];
+  // The masks are trusted like the reference trusts them, but an edge whose
+  // taps would leave the allocated plane (only a malformed mask can ask for
+  // one; the reference would fault on it) is skipped instead of touched.
+  const int reachP = wd == 16 ? 7 : (wd == 8 ? 4 : (wd == 6 ? 3 : 2));
+  const int reachQ = wd == 16 ? 6 : (wd == 8 ? 3 : (wd == 6 ? 2 : 1));
+  const int pos0 = dir == 0 ? c4 * 4 : r4 * 4;
+  const int lim = dir == 0 ? pl.aw : pl.ah;
+  const int along = dir == 0 ? r4 * 4 + 3 : c4 * 4 + 3;
+  const int alongLim = dir == 0 ? pl.ah : pl.aw;
+  if (pos0 - reachP < 0 || pos0 + reachQ >= lim || along >= alongLim) return;
+  const int sstride = (int)(pl.stride / sizeof(T));
+  T* q = row_ptr<T>(pl, r4 * 4) + c4 * 4;
+  if (dir == 0)
+    lpf_unit<T>(q, sstride, 1, f.bd, E, I, H, wd);
+  else
+    lpf_unit<T>(q, 1, sstride, f.bd, E, I, H, wd);
+}
+
+// Host launcher: vertical edges of all planes, then horizontal edges.
+cudaError_t launch_deblock(const DFrame& f, const LfArgs& a, cudaStream_t st) {
+  const int w4 = (f.width + 3) >> 2, h4 = (f.height + 3) >> 2;
+  dim3 blk(32, 8);
+  dim3 grd((w4 + 31) / 32, (h4 + 7) / 8, f.mono ? 1 : 3);
+  for (int dir = 0; dir < 2; dir++) {
+    if (f.bd == 8)
+      k_deblock<uint8_t><<<grd, blk, 0, st>>>(f, a, dir);
+    else
+      k_deblock<uint16_t><<<grd, blk, 0, st>>>(f, a, dir);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pf

@@ -1,0 +1,250 @@
+// pf_fg.cu - film-grain synthesis and reference-frame border extension.
+//
+// Film grain follows goav1's publication path: internal/av1/decoder/
+// postfilter_filmgrain.go:192-263 (plane activity), :516-628 (LUTs, luma then
+// chroma templates, chroma planes then luma, into a display copy) and the
+// filmgrain package: random.go:15-72 (LFSR, stripe seeds), luma.go:24-158 and
+// chroma.go:29-241 (templates with the AR recursion), scaling.go:18-121,
+// apply.go:72-343, :414-546 and blend.go:16-25 (per-32x32 block offsets drawn
+// in order from each stripe's LFSR, overlap blends, noise and clipping).
+//
+// GPU shape: the 82x73 templates are generated by one CTA per frame: the
+// Gaussian fill is a serial LFSR walk, the AR filter runs as a wavefront over
+// t = x + 4y (every AR input of sample (y, x) has a smaller t), one warp per
+// template.  Offsets come from one thread per 32-row stripe.  The apply is
+// one thread per output sample.
+#include "pf_common.cuh"
+#include "pf_tables.h"
+
+namespace pf {
+
+__constant__ int16_t c_gauss[2048];
+
+constexpr int kGW = 82, kGH = 73;
+
+__device__ __forceinline__ int rpow2(int v, int bits) { return bits <= 0 ? v : (v + (1 << (bits - 1))) >> bits; }
+
+__device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
+  const uint16_t bit = ((reg >> 0) ^ (reg >> 1) ^ (reg >> 3) ^ (reg >> 12)) & 1;
+  reg = (uint16_t)((reg >> 1) | (bit << 15));
+  return (uint16_t)((reg >> (16 - bits)) & ((1 << bits) - 1));
+}
+
+// AR recursion of one template (luma.go:83-158 / chroma.go:92-199 generic
+// form) as a wavefront.  One warp; lanes take rows.
+__device__ void ar_wavefront(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h) {
+  const int lane = threadIdx.x & 31;
+  const int lag = p.lag, cs = p.coeff_shift, ro = 1 << (cs - 1);
+  const int gmin = -(1 << (p.bd - 1)), gmax = (1 << (p.bd - 1)) - 1;
+  const int8_t* co = p.coeffs[plane];
+  const int tmax = (w - 4) + 4 * (h - 1);
+  for (int t = 3 + 4 * 3; t <= tmax; t++) {
+    for (int y = 3 + lane; y < h; y += 32) {
+      const int x = t - 4 * y;
+      if (x < 3 || x >= w - 3) continue;
+      int sum = 0, pos = 0;
+      for (int dr = -lag; dr <= 0; dr++) {
+        for (int dc = -lag; dc <= lag; dc++) {
+          if (dr == 0 && dc == 0) {
+            if (plane != 0 && p.num_y_points != 0) {
+              const int sx = plane ? p.ssx : 0, sy = plane ? p.ssy : 0;
+              const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
+              int s = 0;
+              for (int dy = 0; dy <= sy; dy++)
+                for (int dx = 0; dx <= sx; dx++) s += luma[(ly + dy) * kGW + lx + dx];
+              sum += rpow2(s, sx + sy) * co[pos];
+            }
+            break;
+          }
+          sum += co[pos++] * g[(y + dr) * kGW + x + dc];
+        }
+      }
+      g[y * kGW + x] = (int16_t)iclip(g[y * kGW + x] + ((sum + ro) >> cs), gmin, gmax);
+    }
+    __syncwarp();
+  }
+}
+
+// One CTA (3 warps) per frame: luma template, then both chroma templates.
+__global__ void k_fg_templates(FgTemplateArgs p, int16_t* gy, int16_t* gu, int16_t* gv) {
+  __shared__ int16_t s_g[3][kGW * kGH];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int16_t* outs[3] = {gy, gu, gv};
+  // Gaussian fill: one serial LFSR walk per template (lane 0 of its warp).
+  if (warp < 3) {
+    int16_t* g = s_g[warp];
+    for (int i = lane; i < kGW * kGH; i += 32) g[i] = 0;
+    __syncwarp();
+    const bool active = warp == 0 ? p.num_y_points != 0 : p.active[warp];
+    if (active && lane == 0) {
+      const int w = warp == 0 ? kGW : (p.ssx ? 44 : kGW);
+      const int h = warp == 0 ? kGH : (p.ssy ? 38 : kGH);
+      uint16_t reg = warp == 0 ? p.seed : (uint16_t)(p.seed ^ (warp == 1 ? 0xb524 : 0x49d8));
+      const int shift = 12 - p.bd + p.grain_scale_shift;
+      for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) g[y * kGW + x] = (int16_t)rpow2(c_gauss[lfsr(reg, 11)], shift);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  if (warp == 0 && p.num_y_points != 0 && p.lag != 0) ar_wavefront(s_g[0], nullptr, p, 0, kGW, kGH);
+  __syncthreads();
+  if (warp == 1 || warp == 2) {
+    const bool run = p.active[warp] && !(p.lag == 0 && p.num_y_points == 0);
+    if (run) ar_wavefront(s_g[warp], s_g[0], p, warp, p.ssx ? 44 : kGW, p.ssy ? 38 : kGH);
+  }
+  __syncthreads();
+  for (int pl = 0; pl < 3; pl++)
+    if (outs[pl])
+      for (int i = threadIdx.x; i < kGW * kGH; i += blockDim.x) outs[pl][i] = s_g[pl][i];
+}
+
+// Offsets of every 32x32 block: row r uses the LFSR seeded by stripe r
+// (random.go:39-49), one Number(8) per block in order (apply.go:72-125).
+__global__ void k_fg_offsets(uint16_t seed, int rows, int cols, uint8_t* out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int n = r;  // lumaLine >> 5 with lumaLine = 32 r
+  uint16_t reg = seed;
+  reg ^= (uint16_t)(((n * 37 + 178) & 255) << 8);
+  reg ^= (uint16_t)((n * 173 + 105) & 255);
+  for (int b = 0; b < cols; b++) out[r * cols + b] = (uint8_t)lfsr(reg, 8);
+}
+
+__device__ __forceinline__ int scale_lut(const uint8_t* lut, int index, int bd) {
+  index = iclip(index, 0, (1 << bd) - 1);
+  const int shift = bd - 8;
+  const int x = index >> shift;
+  if (bd == 8 || x == 255) return lut[x];
+  const int rem = index - (x << shift);
+  const int start = lut[x], end = lut[x + 1];
+  return (uint8_t)(start + rpow2((end - start) * rem, shift));
+}
+
+__device__ __forceinline__ int blend_w(int prev, int cur, int pw, int cw, int bd) {
+  return iclip(rpow2(prev * pw + cur * cw, 5), -(1 << (bd - 1)), (1 << (bd - 1)) - 1);
+}
+
+// Display = reference with grain added on the cropped area of active planes;
+// every allocated sample of the display frame is written.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fg_apply(DFrame ref, DFrame disp, FgArgs a) {
+  const int plane = blockIdx.z;
+  if (plane > 0 && ref.mono) return;
+  const DPlane& sp = ref.pl[plane];
+  const DPlane& dp = disp.pl[plane];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= sp.aw || y >= sp.ah) return;
+  const int s = row_ptr<T>(sp, y)[x];
+  if (!a.active[plane] || x >= sp.w || y >= sp.h) {
+    row_ptr<T>(dp, y)[x] = (T)s;
+    return;
+  }
+  const int bd = ref.bd;
+  const int sx = plane ? ref.ssx : 0, sy = plane ? ref.ssy : 0;
+  const int bw = 32 >> sx, bh = 32 >> sy;
+  const int row = y / bh, bcol = x / bw;
+  const int xi = x - bcol * bw, yi = y - row * bh;
+  const int ovl = 2;
+  const int xStart = (a.overlap && bcol > 0) ? imin(sp.w - bcol * bw, ovl >> sx) : 0;
+  const int yStart = (a.overlap && row > 0) ? imin(sp.h - row * bh, ovl >> sy) : 0;
+  const uint8_t* offs = a.offsets;
+  const int16_t* gr = a.grain[plane];
+  auto gidx = [&](int offset, int bc, int br) {
+    const int col = 3 + (ovl >> sx) * (3 + (offset >> 4)) + xi + bw * bc;
+    const int rr = 3 + (ovl >> sy) * (3 + (offset & 15)) + yi + bh * br;
+    return rr * kGW + col;
+  };
+  const int o00 = offs[row * a.off_cols + bcol];
+  int g = gr[gidx(o00, 0, 0)];
+  // Horizontal blend weights: luma 27/17 then 17/27; subsampled chroma 23/22.
+  const int hpw = sx ? 23 : (xi == 1 ? 17 : 27), hcw = sx ? 22 : (xi == 1 ? 27 : 17);
+  if (xi < xStart) {
+    const int o10 = offs[row * a.off_cols + bcol - 1];
+    g = blend_w(gr[gidx(o10, 1, 0)], g, hpw, hcw, bd);
+  }
+  if (yi < yStart) {
+    const int o01 = offs[(row - 1) * a.off_cols + bcol];
+    int top = gr[gidx(o01, 0, 1)];
+    if (xi < xStart) {
+      const int o11 = offs[(row - 1) * a.off_cols + bcol - 1];
+      top = blend_w(gr[gidx(o11, 1, 1)], top, hpw, hcw, bd);
+    }
+    const int vpw = sy ? 23 : (yi == 1 ? 17 : 27), vcw = sy ? 22 : (yi == 1 ? 27 : 17);
+    g = blend_w(top, g, vpw, vcw, bd);
+  }
+  int idx;
+  if (plane == 0) {
+    idx = s;
+  } else {
+    // chromaScalingIndex (apply.go:501-520) on the un-grained luma.
+    const DPlane& lp = ref.pl[0];
+    const int lx = x << sx, ly = y << sy;
+    int avg = row_ptr<T>(lp, ly)[lx];
+    if (sx && !(a.odd_luma && x == sp.w - 1)) avg = (avg + row_ptr<T>(lp, ly)[lx + 1] + 1) >> 1;
+    if (a.cfl) {
+      idx = avg;
+    } else {
+      const int combined = avg * (a.luma_mult[plane] - 128) + s * (a.mult[plane] - 128);
+      idx = iclip((combined >> 6) + ((a.offset[plane] << (bd - 8)) - (1 << bd)), 0, (1 << bd) - 1);
+    }
+  }
+  const int scale = scale_lut(a.lut[plane], idx, bd);
+  const int noise = rpow2(scale * g, a.scaling_shift);
+  int minV = 0, maxV = (256 << (bd - 8)) - 1;
+  if (a.clip_restricted) {
+    minV = 16 << (bd - 8);
+    maxV = (plane == 0 ? 235 : (a.matrix_identity ? 235 : 240)) << (bd - 8);
+  }
+  row_ptr<T>(dp, y)[x] = (T)iclip(s + noise, minV, maxV);
+}
+
+// frame/buffer.go:339-400: replicate the last visible column into the padding
+// columns of every visible row, then the last visible row into padding rows.
+template <typename T>
+__global__ void k_extend(DFrame f) {
+  const int plane = blockIdx.z;
+  if (plane > 0 && f.mono) return;
+  const DPlane& p = f.pl[plane];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= p.aw || y >= p.ah) return;
+  if (x < p.w && y < p.h) return;
+  const int h = imin(p.h, p.ah);
+  row_ptr<T>(p, y)[x] = row_ptr<T>(p, imin(y, h - 1))[imin(x, p.w - 1)];
+}
+
+cudaError_t fg_upload_tables() { return cudaMemcpyToSymbol(c_gauss, pf_gaussian_sequence, sizeof(pf_gaussian_sequence)); }
+
+cudaError_t launch_fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, cudaStream_t st) {
+  k_fg_templates<<<1, 96, 0, st>>>(p, gy, gu, gv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fg_offsets(uint16_t seed, int rows, int cols, uint8_t* out, cudaStream_t st) {
+  k_fg_offsets<<<(rows + 63) / 64, 64, 0, st>>>(seed, rows, cols, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fg_apply(const DFrame& ref, const DFrame& disp, const FgArgs& a, cudaStream_t st) {
+  dim3 blk(64, 4);
+  dim3 grd((ref.pl[0].aw + 63) / 64, (ref.pl[0].ah + 3) / 4, ref.mono ? 1 : 3);
+  if (ref.bd == 8)
+    k_fg_apply<uint8_t><<<grd, blk, 0, st>>>(ref, disp, a);
+  else
+    k_fg_apply<uint16_t><<<grd, blk, 0, st>>>(ref, disp, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_extend(const DFrame& f, cudaStream_t st) {
+  dim3 blk(64, 4);
+  dim3 grd((f.pl[0].aw + 63) / 64, (f.pl[0].ah + 3) / 4, f.mono ? 1 : 3);
+  if (f.bd == 8)
+    k_extend<uint8_t><<<grd, blk, 0, st>>>(f);
+  else
+    k_extend<uint16_t><<<grd, blk, 0, st>>>(f);
+  return cudaGetLastError();
+}
+
+}  // namespace pf

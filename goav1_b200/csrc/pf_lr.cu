@@ -1,0 +1,270 @@
+// pf_lr.cu - loop restoration (Wiener / SGRproj) on the GPU.
+//
+// One CTA per (64-wide processing column, restoration stripe, plane).  The
+// geometry is goav1's: tile/restoration_schedule.go:61-109, :400-409 (unit
+// grid), tile/restoration_geometry.go:54-236 (unit rects shifted up by 8/4
+// rows, stripes of 64/32 rows with the first one 8/4 rows shorter, 64-wide
+// processing units).  Each stripe reads the post-CDEF plane with a 3-sample
+// replicated frame border (restoration_boundary.go:126-180) and, across
+// interior stripe boundaries, the pre-CDEF rows the CDEF kernel saved
+// (setupRestorationStripeBoundaryFromSaved, restoration_boundary.go:553-614:
+// rows above = saved[max(i+2,0)], rows below = saved[min(i,1)]).  The
+// filters are restoration/wiener.go:59-211 and restoration/selfguided.go:
+// 111-390 (box sums, a/b tables, 6/5 and 4/3 weights, projection with the
+// int16 wrap).  Visible output columns depend only on +/-3 source columns,
+// so the reference's rounding of the last Wiener unit width up to 16 changes
+// no stored sample and is not replicated.
+//
+// Every sample of the tile inside the MI-aligned plane is written to the
+// destination: restored samples where a Wiener/SGR unit covers the cropped
+// plane, the post-CDEF sample everywhere else.
+#include "pf_common.cuh"
+#include "pf_tables.h"
+
+namespace pf {
+
+__constant__ int16_t c_sgr_params[16][4];
+__constant__ uint16_t c_x_by_xplus1[256];
+__constant__ uint16_t c_one_by_x[25];
+
+constexpr int kWin = 70;  // 64 + 2*3
+
+struct LrGeom {
+  int aw[3], ah[3];
+};
+
+__device__ __forceinline__ int32_t rpot(int32_t v, int bits) {
+  return bits <= 0 ? v : (v + (int32_t)(1 << (bits - 1))) >> bits;
+}
+__device__ __forceinline__ uint32_t rpotu(uint32_t v, int bits) {
+  return bits <= 0 ? v : (v + (1u << (bits - 1))) >> bits;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_lr(DFrame src, DFrame dst, LrArgs a, LrGeom g, int enabled) {
+  __shared__ uint16_t s_win[kWin * kWin];
+  __shared__ int32_t s_A[66 * 66];
+  __shared__ int32_t s_B[66 * 66];
+  const int plane = blockIdx.z;
+  if (plane > 0 && src.mono) return;
+  const int ssx = plane ? src.ssx : 0, ssy = plane ? src.ssy : 0;
+  const int PW = 64 >> ssx, SH = 64 >> ssy, off = 8 >> ssy;
+  const int Wa = g.aw[plane], Ha = g.ah[plane];
+  const DPlane& sp = src.pl[plane];
+  const DPlane& dp = dst.pl[plane];
+  const int Wc = sp.w, Hc = sp.h;
+  const int s = blockIdx.y, j = blockIdx.x;
+  const int x0 = j * PW;
+  const int y0 = imax(0, s * SH - off);
+  if (x0 >= Wa || y0 >= Ha) return;
+  const int x1 = imin(x0 + PW, Wa), y1 = imin((s + 1) * SH - off, Ha);
+  const int tid = threadIdx.x;
+  const int tx = tid % PW, ty0 = tid / PW, rowStep = 256 / PW;
+  const int bd = src.bd;
+
+  // Which restoration unit (if any) covers this tile.
+  const pf_lr_unit* u = nullptr;
+  const int xf1 = imin(x1, Wc), yf1 = imin(y1, Hc);
+  if (enabled && a.type[plane] != PF_LR_NONE && x0 < Wc && y0 < Hc) {
+    const int us = a.unit_size[plane];
+    const int ur = imin((y0 + off) / us, a.vert[plane] - 1);
+    const int uc = imin(x0 / us, a.horz[plane] - 1);
+    const pf_lr_unit* cand = &a.units[plane][ur * a.horz[plane] + uc];
+    if (cand->type == PF_LR_WIENER || cand->type == PF_LR_SGRPROJ) u = cand;
+  }
+  if (!u) {
+    if (tx < x1 - x0)
+      for (int y = y0 + ty0; y < y1; y += rowStep) row_ptr<T>(dp, y)[x0 + tx] = row_ptr<T>(sp, y)[x0 + tx];
+    return;
+  }
+  const int h = yf1 - y0, w = xf1 - x0;
+  // ---- stage the (h+6) x (w+6) source window ----
+  const int nominal = SH - (y0 == 0 ? off : 0);
+  const bool copyAbove = y0 != 0, copyBelow = y0 + nominal < Hc;
+  const int kAbove = s, kBelow = s + 1;  // boundary indices of the saved lines
+  const int ww = w + 6, wh = h + 6;
+  for (int i = tid; i < ww * wh; i += 256) {
+    const int r = i / ww, c = i - r * ww;
+    const int yy = y0 - 3 + r;
+    const int xx = iclip(x0 - 3 + c, 0, Wc - 1);
+    int v;
+    if (yy < y0 && copyAbove) {
+      const int li = imax(yy - y0 + 2, 0);
+      v = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kAbove * 4 + li) * a.line_stride[plane])[xx];
+    } else if (yy >= yf1 && copyBelow) {
+      const int li = 2 + imin(yy - yf1, 1);
+      v = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kBelow * 4 + li) * a.line_stride[plane])[xx];
+    } else {
+      v = row_ptr<T>(sp, iclip(yy, 0, Hc - 1))[xx];
+    }
+    s_win[r * kWin + c] = (uint16_t)v;
+  }
+  __syncthreads();
+
+  // Pixels of the tile outside the cropped plane are copied through.
+  if (tx < x1 - x0)
+    for (int y = y0 + ty0; y < y1; y += rowStep)
+      if (x0 + tx >= Wc || y >= Hc) row_ptr<T>(dp, y)[x0 + tx] = row_ptr<T>(sp, y)[x0 + tx];
+
+  const int maxv = (1 << bd) - 1;
+  if (u->type == PF_LR_WIENER) {
+    // restoration/wiener.go:202-211 (wienerRounds), :132-196.
+    int round0 = 3, round1 = 11;
+    const int range = bd + 7 - round0 + 2;
+    if (range > 16) {
+      round0 += range - 16;
+      round1 -= range - 16;
+    }
+    const int hv0 = u->wiener_h[0], hv1 = u->wiener_h[1], hv2 = u->wiener_h[2];
+    const int hf[7] = {hv0, hv1, hv2, -2 * (hv0 + hv1 + hv2), hv2, hv1, hv0};
+    const int vv0 = u->wiener_v[0], vv1 = u->wiener_v[1], vv2 = u->wiener_v[2];
+    const int vf[7] = {vv0, vv1, vv2, -2 * (vv0 + vv1 + vv2), vv2, vv1, vv0};
+    const int32_t limit = 1 << (bd + 1 + 7 - round0);
+    const int32_t offH = 1 << (bd + 7 - 1);
+    uint16_t* temp = reinterpret_cast<uint16_t*>(s_A);  // (h+6) x 64
+    for (int i = tid; i < wh * w; i += 256) {
+      const int r = i / w, c = i - r * w;
+      const uint16_t* sw = &s_win[r * kWin + c];
+      int32_t sum = ((int32_t)sw[3] << 7) + offH;
+#pragma unroll
+      for (int k = 0; k < 7; k++) sum += (int32_t)sw[k] * hf[k];
+      temp[r * 64 + c] = (uint16_t)imin(imax(rpot(sum, round0), 0), limit - 1);
+    }
+    __syncthreads();
+    const int32_t offV = 1 << (bd + round1 - 1);
+    if (tx < w)
+      for (int y = ty0; y < h; y += rowStep) {
+        int32_t c3 = temp[(y + 3) * 64 + tx];
+        int32_t sum = (c3 << 7) - offV;
+#pragma unroll
+        for (int k = 0; k < 7; k++) sum += (int32_t)temp[(y + k) * 64 + tx] * vf[k];
+        row_ptr<T>(dp, y0 + y)[x0 + tx] = (T)imin(imax(rpot(sum, round1), 0), maxv);
+      }
+    return;
+  }
+
+  // ---- SGRproj (restoration/selfguided.go:132-359) ----
+  const int set = u->sgr_set;
+  const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][1];
+  int32_t flt0[16], flt1[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    flt0[k] = 0;
+    flt1[k] = 0;
+  }
+  for (int pass = 0; pass < 2; pass++) {
+    const int r = pass == 0 ? r0 : r1;
+    if (r == 0) continue;
+    const int sv = c_sgr_params[set][2 + pass];
+    const uint32_t n = (uint32_t)((2 * r + 1) * (2 * r + 1));
+    const int step = pass == 0 ? 2 : 1;  // r=2 pass computes every other row
+    // a/b for rows -1..h (step), cols -1..w, stored at [(row+1)*66 + col+1].
+    const int nrows = h + 2, ncols = w + 2;
+    for (int i = tid; i < nrows * ncols; i += 256) {
+      const int rr = i / ncols, cc = i - rr * ncols;
+      const int row = rr - 1, col = cc - 1;
+      if (step == 2 && ((row + 1) & 1)) continue;  // rows -1, 1, 3, ...
+      int32_t sum = 0, sq = 0;
+      for (int dy = -r; dy <= r; dy++)
+        for (int dx = -r; dx <= r; dx++) {
+          const int32_t v = s_win[(row + 3 + dy) * kWin + col + 3 + dx];
+          sum += v;
+          sq += v * v;
+        }
+      const uint32_t av = (uint32_t)rpot(sq, 2 * (bd - 8));
+      const uint32_t bv = (uint32_t)rpot(sum, bd - 8);
+      uint32_t p = 0;
+      if (av * n >= bv * bv) p = av * n - bv * bv;
+      uint32_t z = rpotu(p * (uint32_t)sv, 20);
+      if (z > 255) z = 255;
+      const int32_t A = c_x_by_xplus1[z];
+      s_A[rr * 66 + cc] = A;
+      s_B[rr * 66 + cc] = (int32_t)rpotu((uint32_t)(256 - A) * (uint32_t)sum * (uint32_t)c_one_by_x[n - 1], 12);
+    }
+    __syncthreads();
+    if (tx < w) {
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        const int y = ty0 + k * rowStep;
+        if (y >= h) break;
+        const int32_t* A = &s_A[(y + 1) * 66 + tx + 1];
+        const int32_t* B = &s_B[(y + 1) * 66 + tx + 1];
+        const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
+        int32_t av, bv, shift;
+        if (pass == 0) {
+          if ((y & 1) == 0) {
+            av = (A[-66] + A[66]) * 6 + (A[-67] + A[-65] + A[65] + A[67]) * 5;
+            bv = (B[-66] + B[66]) * 6 + (B[-67] + B[-65] + B[65] + B[67]) * 5;
+            shift = 9;
+          } else {
+            av = A[0] * 6 + (A[-1] + A[1]) * 5;
+            bv = B[0] * 6 + (B[-1] + B[1]) * 5;
+            shift = 8;
+          }
+          flt0[k] = rpot(av * dg + bv, shift);
+        } else {
+          av = (A[0] + A[-1] + A[1] + A[-66] + A[66]) * 4 + (A[-67] + A[65] + A[-65] + A[67]) * 3;
+          bv = (B[0] + B[-1] + B[1] + B[-66] + B[66]) * 4 + (B[-67] + B[65] + B[-65] + B[67]) * 3;
+          flt1[k] = rpot(av * dg + bv, 9);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // restoration/selfguided.go:111-127 (DecodeSGRXQ), :233-247 (projection).
+  int xq0, xq1;
+  if (r0 == 0) {
+    xq0 = 0;
+    xq1 = 128 - u->sgr_xqd[1];
+  } else if (r1 == 0) {
+    xq0 = u->sgr_xqd[0];
+    xq1 = 0;
+  } else {
+    xq0 = u->sgr_xqd[0];
+    xq1 = 128 - xq0 - u->sgr_xqd[1];
+  }
+  if (tx < w) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      const int y = ty0 + k * rowStep;
+      if (y >= h) break;
+      const int32_t uu = (int32_t)s_win[(y + 3) * kWin + tx + 3] << 4;
+      int32_t v = uu << 7;
+      v += xq0 * (flt0[k] - uu);
+      v += xq1 * (flt1[k] - uu);
+      const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
+      row_ptr<T>(dp, y0 + y)[x0 + tx] = (T)imin(imax(wv, 0), maxv);
+    }
+  }
+}
+
+cudaError_t lr_upload_tables() {
+  cudaError_t e = cudaMemcpyToSymbol(c_sgr_params, pf_sgr_params, sizeof(pf_sgr_params));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_x_by_xplus1, pf_sgr_x_by_xplus1, sizeof(pf_sgr_x_by_xplus1));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_one_by_x, pf_sgr_one_by_x, sizeof(pf_sgr_one_by_x));
+  return e;
+}
+
+cudaError_t launch_lr(const DFrame& src, const DFrame& dst, const LrArgs& a, int enabled, cudaStream_t st) {
+  LrGeom g;
+  int maxCols = 0, maxStripes = 0;
+  for (int p = 0; p < (src.mono ? 1 : 3); p++) {
+    const int xdec = p ? src.ssx : 0, ydec = p ? src.ssy : 0;
+    // MI-aligned extent (frameWorkCDEFAlignedPlane); the validated allocation
+    // always covers it.
+    const int aw = ((src.width + 7) & ~7) >> xdec, ah = ((src.height + 7) & ~7) >> ydec;
+    g.aw[p] = aw;
+    g.ah[p] = ah;
+    const int PW = 64 >> xdec, SH = 64 >> ydec, off = 8 >> ydec;
+    maxCols = imax(maxCols, (aw + PW - 1) / PW);
+    maxStripes = imax(maxStripes, (ah + off + SH - 1) / SH);
+  }
+  dim3 grd(maxCols, maxStripes, src.mono ? 1 : 3);
+  if (src.bd == 8)
+    k_lr<uint8_t><<<grd, 256, 0, st>>>(src, dst, a, g, enabled);
+  else
+    k_lr<uint16_t><<<grd, 256, 0, st>>>(src, dst, a, g, enabled);
+  return cudaGetLastError();
+}
+
+}  // namespace pf

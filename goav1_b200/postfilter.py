@@ -1,0 +1,214 @@
+"""Host-side mirror of goav1's post-filter runner, over the C ABI.
+
+PostFilterRunner mirrors decoderFrameWorkReusableSupportedPostFilterRunner
+(decoder_postfilter_bind.go:398-440): apply() takes the frame and the
+decode-time side information of one completed frame, leaves the frame as the
+publishable reference (deblock, CDEF, loop restoration, border extension,
+in place) and, when film grain applies, produces the display picture that
+post_filter_output() returns (decoder_postfilter_bind.go:252-256, :434-439).
+Errors are raised as the reference's sentinel errors (ErrInvalidCDEF,
+ErrInvalidFilter, ErrInvalidPlan, ErrUnsupportedPostFilter, ErrShortBuffer).
+
+DeviceFrame / device_side keep frames and side information resident in HBM
+(torch tensors are used only as device allocations).
+"""
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi, lib
+
+
+class PostFilterError(Exception):
+    code = None
+
+
+class ErrInvalidCDEF(PostFilterError):
+    code = abi.PF_ERR_INVALID_CDEF
+
+
+class ErrInvalidFilter(PostFilterError):
+    code = abi.PF_ERR_INVALID_FILTER
+
+
+class ErrInvalidPlan(PostFilterError):
+    code = abi.PF_ERR_INVALID_PLAN
+
+
+class ErrUnsupportedPostFilter(PostFilterError):
+    code = abi.PF_ERR_UNSUPPORTED
+
+
+class ErrShortBuffer(PostFilterError):
+    code = abi.PF_ERR_SHORT_BUFFER
+
+
+class ErrInvalidFormat(PostFilterError):
+    code = abi.PF_ERR_INVALID_FORMAT
+
+
+class ErrInvalidArgument(PostFilterError):
+    code = abi.PF_ERR_INVALID_ARG
+
+
+class ErrDevice(PostFilterError):
+    code = abi.PF_ERR_DEVICE
+
+
+class ErrTimeout(PostFilterError):
+    code = abi.PF_ERR_TIMEOUT
+
+
+class ErrNoDevice(PostFilterError):
+    code = abi.PF_ERR_NO_DEVICE
+
+
+_ERRORS = {cls.code: cls for cls in (ErrInvalidCDEF, ErrInvalidFilter, ErrInvalidPlan, ErrUnsupportedPostFilter,
+                                     ErrShortBuffer, ErrInvalidFormat, ErrInvalidArgument, ErrDevice, ErrTimeout,
+                                     ErrNoDevice)}
+
+
+def check(status):
+    if status != abi.PF_OK:
+        msg = lib().pf_status_string(status).decode()
+        raise _ERRORS.get(status, PostFilterError)(msg)
+    return status
+
+
+def validate(frame, side, display=None):
+    """The status pf_frame_apply would return before touching anything."""
+    return lib().pf_frame_validate(C.byref(frame), C.byref(side), C.byref(display) if display is not None else None)
+
+
+class PostFilterRunner:
+    """One post-filter runner per decoder; calls are serialised by the caller."""
+
+    def __init__(self, device=0, timing=False):
+        L = lib()
+        cfg = abi.pf_config(device=device, timing=1 if timing else 0)
+        st = C.c_int(0)
+        h = L.pf_create(C.byref(cfg), C.byref(st))
+        if not h:
+            check(st.value or abi.PF_ERR_NO_DEVICE)
+        self._h = h
+        self._display = None
+        self.stats = abi.pf_stats()
+
+    def apply(self, frame, side, display=None):
+        """Runs side.stages on frame (in place) and grain into display."""
+        st = lib().pf_frame_apply(self._h, C.byref(frame), C.byref(side),
+                                  C.byref(display) if display is not None else None, C.byref(self.stats))
+        check(st)
+        self._display = display if (side.stages & abi.PF_STAGE_FILM_GRAIN) else None
+        return self.stats
+
+    def apply_batch(self, items):
+        """items: list of (frame, side, display) device-resident triples."""
+        arr = (abi.pf_batch_item * len(items))()
+        for i, (f, s, d) in enumerate(items):
+            arr[i].frame = C.pointer(f)
+            arr[i].side = C.pointer(s)
+            arr[i].display = C.pointer(d) if d is not None else None
+        check(lib().pf_batch_apply(self._h, arr, len(items), C.byref(self.stats)))
+        return self.stats
+
+    def post_filter_output(self):
+        """(display frame, True) after a grain-applying apply(), else (None, False)."""
+        return (self._display, self._display is not None)
+
+    def sync(self):
+        check(lib().pf_sync(self._h))
+
+    @property
+    def stream(self):
+        return lib().pf_stream(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Device residency helpers (torch tensors as plain device allocations).
+
+
+class DeviceFrame:
+    """A frame whose planes live in device memory, same geometry as a HostFrame."""
+
+    def __init__(self, host, device="cuda"):
+        import torch
+
+        self.host = host
+        dt = torch.uint8 if host.bit_depth == 8 else torch.int16
+        self.tensors = []
+        for p in host.planes:
+            t = torch.empty(p.shape, dtype=dt, device=device)
+            self.tensors.append(t)
+        self.upload(host)
+
+    def upload(self, host, non_blocking=False):
+        import torch
+
+        for t, p in zip(self.tensors, host.planes):
+            src = torch.from_numpy(p.view(np.int16) if p.dtype == np.uint16 else p)
+            t.copy_(src, non_blocking=non_blocking)
+
+    def download(self, host=None):
+        host = host or self.host.like()
+        for t, p in zip(self.tensors, host.planes):
+            a = t.cpu().numpy()
+            p[:] = a.view(np.uint16) if p.dtype == np.uint16 else a
+        return host
+
+    def pf(self):
+        bps = 1 if self.host.bit_depth == 8 else 2
+        f = self.host.pf(memory=abi.PF_MEM_DEVICE, ptrs=[t.data_ptr() for t in self.tensors])
+        for i, t in enumerate(self.tensors):
+            f.plane[i].stride = t.stride(0) * bps
+        return f
+
+    def nbytes(self):
+        return sum(t.numel() * t.element_size() for t in self.tensors)
+
+
+def device_side(si, frame, device="cuda"):
+    """Copy of a SideInfo (for HostFrame `frame`) whose arrays are device
+    resident (side_memory=DEVICE)."""
+    import torch
+
+    s = abi.pf_frame_side()
+    C.memmove(C.byref(s), C.byref(si.side), C.sizeof(s))
+    s.side_memory = abi.PF_MEM_DEVICE
+    keep = []
+
+    def up(ptr, nbytes):
+        if not ptr or nbytes == 0:
+            return ptr
+        buf = (C.c_uint8 * nbytes).from_address(ptr)
+        t = torch.frombuffer(bytearray(buf), dtype=torch.uint8).to(device)
+        keep.append(t)
+        return t.data_ptr()
+
+    lf = si.side.lf
+    s.lf.masks = up(lf.masks, lf.sb128_w * lf.sb128_h * abi.PF_LF_MASK_WORDS * 2)
+    s.lf.level_cache = up(lf.level_cache, 4 * lf.mi_cols * lf.mi_rows)
+    cd = si.side.cdef
+    n = cd.index_stride * cd.index_rows
+    s.cdef.index = up(cd.index, n)
+    s.cdef.read = up(cd.read, n)
+    ucols, urows = (frame.width + 63) // 64, (frame.height + 63) // 64
+    s.cdef.noskip = up(cd.noskip, ucols * urows * 8) if cd.noskip else None
+    for p in range(3):
+        if si.side.lr.units[p]:
+            s.lr.units[p] = up(si.side.lr.units[p], si.side.lr.unit_count[p] * C.sizeof(abi.pf_lr_unit))
+    from .synth import SideInfo
+
+    return SideInfo(side=s, keep=keep + [si], blocks=si.blocks)

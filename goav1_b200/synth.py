@@ -181,28 +181,18 @@ def build_lf_masks(frame, blocks, mi_cols, mi_rows):
     sb128_w = (mi_cols + 31) // 32
     sb128_h = (mi_rows + 31) // 32
     masks = np.zeros((sb128_h * sb128_w, abi.PF_LF_MASK_WORDS), np.uint16)
-    # Luma transform grid: tx width/height (4-px units) and tx origin per cell.
-    txs = np.zeros((mi_rows, mi_cols), np.int32)
-    tx0x = np.zeros((mi_rows, mi_cols), np.int32)
-    tx0y = np.zeros((mi_rows, mi_cols), np.int32)
-    bsz = np.zeros((mi_rows, mi_cols), np.int32)
-    b0x = np.zeros((mi_rows, mi_cols), np.int32)
-    b0y = np.zeros((mi_rows, mi_cols), np.int32)
-    for (x4, y4, s4, t4) in blocks:
-        ys, xs = slice(y4, min(y4 + s4, mi_rows)), slice(x4, min(x4 + s4, mi_cols))
-        bsz[ys, xs] = s4
-        b0x[ys, xs] = x4
-        b0y[ys, xs] = y4
-        txs[ys, xs] = t4
-        gy, gx = np.mgrid[ys, xs]
-        tx0x[ys, xs] = x4 + ((gx - x4) // t4) * t4
-        tx0y[ys, xs] = y4 + ((gy - y4) // t4) * t4
+    # Luma transform grid: tx size (4-px units) and tx origin per cell.
+    owner = _owner_grid(blocks, mi_cols, mi_rows)
+    barr = np.asarray(blocks, np.int32).reshape(-1, 4)
+    b0x, b0y, bsz, txs = (barr[owner, k] for k in range(4))
+    gy, gx = np.mgrid[0:mi_rows, 0:mi_cols]
+    tx0x = b0x + ((gx - b0x) // txs) * txs
+    tx0y = b0y + ((gy - b0y) // txs) * txs
 
     def put(region_idx, word_idx, bit):
         np.bitwise_or.at(masks, (region_idx, word_idx), (1 << bit).astype(np.uint16))
 
     cls = _class_luma(txs)
-    gy, gx = np.mgrid[0:mi_rows, 0:mi_cols]
     # vertical edges (dir 0): left side of a tx, x4 > 0
     sel = (tx0x == gx) & (gx > 0)
     y, x = gy[sel], gx[sel]
@@ -263,25 +253,28 @@ def calc_lf_values(level_y, level_u, level_v, seg_deltas):
     return out
 
 
+def _owner_grid(blocks, mi_cols, mi_rows):
+    owner = np.zeros((mi_rows, mi_cols), np.int32)
+    for bi, (x4, y4, s4, _t4) in enumerate(blocks):
+        owner[y4:y4 + s4, x4:x4 + s4] = bi
+    return owner
+
+
 def build_level_cache(frame, blocks, mi_cols, mi_rows, seg_of_block, seg_levels):
     """Level cache: 4 bytes per MI cell [YV, YH, U, V]; chroma cells at chroma
     coordinates with the luma stride (postfilter_loopfilter_masks.go:135-228)."""
     lc = np.zeros((mi_rows, mi_cols, 4), np.uint8)
     ssx, ssy = frame.ss_x, frame.ss_y
-    for bi, (x4, y4, s4, _t4) in enumerate(blocks):
-        lv = seg_levels[seg_of_block[bi]]
-        lc[y4:y4 + s4, x4:x4 + s4, 0] = lv[0]
-        lc[y4:y4 + s4, x4:x4 + s4, 1] = lv[1]
+    owner = _owner_grid(blocks, mi_cols, mi_rows)
+    lv = np.asarray(seg_levels, np.uint8)[np.asarray(seg_of_block)]  # [nblocks, 4]
+    lc[:, :, 0] = lv[owner, 0]
+    lc[:, :, 1] = lv[owner, 1]
     cc, cr = (mi_cols + ssx) >> ssx, (mi_rows + ssy) >> ssy
-    owner = np.zeros((mi_rows, mi_cols), np.int32)
-    for bi, (x4, y4, s4, _t4) in enumerate(blocks):
-        owner[y4:y4 + s4, x4:x4 + s4] = bi
-    for cy in range(cr):
-        for cx in range(cc):
-            bi = owner[min(cy << ssy, mi_rows - 1), min(cx << ssx, mi_cols - 1)]
-            lv = seg_levels[seg_of_block[bi]]
-            lc[cy, cx, 2] = lv[2]
-            lc[cy, cx, 3] = lv[3]
+    cy = np.minimum(np.arange(cr) << ssy, mi_rows - 1)
+    cx = np.minimum(np.arange(cc) << ssx, mi_cols - 1)
+    co = owner[np.ix_(cy, cx)]
+    lc[:cr, :cc, 2] = lv[co, 2]
+    lc[:cr, :cc, 3] = lv[co, 3]
     return lc
 
 
@@ -290,21 +283,19 @@ def build_noskip(blocks, skip, mi_cols, mi_rows):
     64x64 unit, bit by*8+bx set when the 8x8 block carries residual; bits of
     blocks outside the frame are preset."""
     ucols, urows = (mi_cols + 15) >> 4, (mi_rows + 15) >> 4
-    ns = np.zeros((urows, ucols, 8), np.uint8)
+    owner = _owner_grid(blocks, mi_cols, mi_rows)
+    coded = ~np.asarray(skip, bool)[owner]  # per 4x4 cell
+    c8 = np.zeros((urows * 8, ucols * 8), bool)
+    r8, k8 = (mi_rows + 1) >> 1, (mi_cols + 1) >> 1
+    pad = np.zeros((r8 * 2, k8 * 2), bool)
+    pad[:mi_rows, :mi_cols] = coded
+    c8[:r8, :k8] = pad.reshape(r8, 2, k8, 2).any(axis=(1, 3))
     valid_c, valid_r = mi_cols >> 1, mi_rows >> 1
-    if valid_c & 7:
-        ns[:, ucols - 1, :] |= np.uint8((0xFF << (valid_c & 7)) & 0xFF)
-    if valid_r & 7:
-        ns[urows - 1, :, (valid_r & 7):] = 0xFF
-    for bi, (x4, y4, s4, _t4) in enumerate(blocks):
-        if skip[bi]:
-            continue
-        x0, y0 = x4 >> 1, y4 >> 1
-        x1, y1 = (min(x4 + s4, mi_cols) + 1) >> 1, (min(y4 + s4, mi_rows) + 1) >> 1
-        for y in range(y0, y1):
-            for x in range(x0, x1):
-                ns[y >> 3, x >> 3, y & 7] |= np.uint8(1 << (x & 7))
-    return ns
+    c8[:, valid_c:] = True
+    c8[valid_r:, :] = True
+    bits = c8.reshape(urows, 8, ucols, 8).transpose(0, 2, 1, 3)  # [ur, uc, by, bx]
+    ns = np.packbits(bits, axis=-1, bitorder="little")[..., 0]
+    return np.ascontiguousarray(ns.astype(np.uint8))
 
 
 # ---------------------------------------------------------------------------
@@ -389,14 +380,11 @@ def make_frame(config, seed, frame_index=0, texture=None, width=None, height=Non
     noskip = build_noskip(blocks, skip, mi_cols, mi_rows)
     index = rng.integers(0, cd.strength_count, size=(urows, ucols)).astype(np.uint8)
     # Read=false for units whose in-frame 8x8 blocks are all skip.
-    read = np.zeros((urows, ucols), np.uint8)
-    for ur in range(urows):
-        for uc in range(ucols):
-            bc = min(8, (mi_cols >> 1) - uc * 8)
-            br = min(8, (mi_rows >> 1) - ur * 8)
-            word = noskip[ur, uc]
-            any_ns = any(int(word[by]) & ((1 << bc) - 1) for by in range(br))
-            read[ur, uc] = 1 if any_ns else 0
+    bits = np.unpackbits(noskip, axis=-1, bitorder="little").astype(bool).reshape(urows, ucols, 8, 8)
+    gy = np.arange(urows)[:, None, None, None] * 8 + np.arange(8)[None, None, :, None]
+    gx = np.arange(ucols)[None, :, None, None] * 8 + np.arange(8)[None, None, None, :]
+    inside = (gy < (mi_rows >> 1)) & (gx < (mi_cols >> 1))
+    read = (bits & inside).any(axis=(2, 3)).astype(np.uint8)
     keep += [noskip, index, read]
     cd.index, cd.read = index.ctypes.data, read.ctypes.data
     cd.index_stride, cd.index_rows = ucols, urows

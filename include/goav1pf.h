@@ -191,7 +191,9 @@ typedef struct pf_film_grain {
  * work.go:85-101, reduced to its post-filter inputs). */
 typedef struct pf_frame_side {
   uint32_t stages;       /* PF_STAGE_* still to run */
-  uint32_t reserved;
+  uint32_t side_memory;  /* PF_MEM_HOST: the side-info arrays below are host
+                            memory (copied up each call); PF_MEM_DEVICE: they
+                            are already device resident */
   pf_loop_filter lf;
   pf_cdef cdef;
   pf_restoration lr;
