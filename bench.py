@@ -234,15 +234,14 @@ def main():
             flush.fill_(1)
 
     def step():
-        for f, s, d in pf_frames:
-            runner.apply(f, s, d)
+        runner.apply_batch(pf_frames)
 
     # Warm-up.
     for _ in range(max(args.warmup, 3)):
         reset()
         step()
     torch.cuda.synchronize()
-    launches_per_frame = 8
+    launches_per_step = 7  # one launch per stage for the whole batch
     clocks = ClockSampler(local)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if world > 1:
@@ -267,12 +266,16 @@ def main():
     px = sum(fr.luma_pixels for fr, _ in frames)
     value = world * px / (ms / 1e3) / 1e6
 
-    # Per-stage device times (CUDA events recorded by the library on its stream).
+    # Per-stage device times of the batched launches (CUDA events the library
+    # records on its stream), averaged over a few batches.
     trunner = PostFilterRunner(device=local, timing=True)
     stage = np.zeros(5)
-    for (f, s, d) in pf_frames:
-        st = trunner.apply(f, s, d)
-        stage += np.array(list(st.stage_ms))
+    reps = 3
+    for _ in range(reps + 1):
+        reset()
+        st = trunner.apply_batch(pf_frames)
+        if _ > 0:
+            stage += np.array(list(st.stage_ms)) / reps
     trunner.close()
     stage_names = ["deblock", "cdef", "restoration", "extend", "film_grain"]
     per_frame = stage / n
@@ -338,7 +341,7 @@ def main():
                            "l2": "inputs (%.0f MB per rank) larger than L2, and a 256 MB L2 flush between steps"
                                  % (sum(fr.nbytes() for fr, _ in frames) / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-                "gpu_launches": launches_per_frame * n * args.steps}
+                "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))
     runner.close()
     if world > 1:

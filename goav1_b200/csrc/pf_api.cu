@@ -21,15 +21,15 @@
 #include "pf_common.cuh"
 
 namespace pf {
-cudaError_t launch_deblock(const DFrame& f, const LfArgs& a, cudaStream_t st);
-cudaError_t launch_cdef(const DFrame& in, const DFrame& out, const CdefArgs& a, cudaStream_t st);
-cudaError_t launch_lr(const DFrame& src, const DFrame& dst, const LrArgs& a, int enabled, cudaStream_t st);
+cudaError_t launch_deblock_batch(const BatchArgs& b, int total, int grid, int dir, cudaStream_t st);
+cudaError_t launch_cdef_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
+cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
+cudaError_t launch_fg_templates_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
+cudaError_t launch_fg_offsets_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
+cudaError_t launch_fg_apply_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
+cudaError_t launch_extend_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
 cudaError_t lr_upload_tables();
 cudaError_t fg_upload_tables();
-cudaError_t launch_fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, cudaStream_t st);
-cudaError_t launch_fg_offsets(uint16_t seed, int rows, int cols, uint8_t* out, cudaStream_t st);
-cudaError_t launch_fg_apply(const DFrame& ref, const DFrame& disp, const FgArgs& a, cudaStream_t st);
-cudaError_t launch_extend(const DFrame& f, cudaStream_t st);
 }  // namespace pf
 
 using namespace pf;
@@ -62,11 +62,21 @@ int bps_of(const pf_frame* f) { return f->bit_depth > 8 ? 2 : 1; }
 
 struct pf_ctx {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;  // main stream (returned by pf_stream)
+  cudaStream_t side = nullptr;    // film-grain templates/offsets overlap the chain here
   int timing = 0;
-  cudaEvent_t ev[6] = {};
-  DevBuf io, disp, scratch, lines, grain, offsets;
-  DevBuf masks, lc, index, read, noskip, units[3];
+  cudaEvent_t ev[8] = {};
+  cudaEvent_t fork = nullptr, join = nullptr;
+  DevBuf io, disp;           // staging of host frames
+  DevBuf arena;              // per-frame scratch: CDEF output, LR lines, grain, offsets
+  DevBuf sidebuf;            // host side information copied up
+  DevBuf jobs, bases, counters;
+  std::vector<FrameJob> hjobs;
+  std::vector<int> hbase;
+  std::vector<uint8_t> hside;
+  // Persistent-CTA count per stage (0 = one CTA per work item).
+  int persistent[ST_COUNT] = {};
 };
 
 // ---------------------------------------------------------------------------
@@ -234,15 +244,6 @@ static cudaError_t layout_like(const pf_frame* f, DevBuf& buf, void** ptrs, int6
   return cudaSuccess;
 }
 
-template <typename TT>
-static const TT* side_ptr(pf_ctx* c, DevBuf& b, const TT* src, size_t bytes, bool host, cudaError_t* e) {
-  if (!host || !src) return src;
-  *e = b.ensure(bytes);
-  if (*e != cudaSuccess) return nullptr;
-  *e = cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, c->stream);
-  return (const TT*)b.p;
-}
-
 static void build_scaling_lut(uint8_t* dst, const uint8_t (*pts)[2], int n) {
   // filmgrain/scaling.go:18-48 (BuildScalingLUT).
   memset(dst, 0, 256);
@@ -313,7 +314,11 @@ extern "C" pf_ctx* pf_create(const pf_config* cfg, int* status) {
     if (status) *status = PF_ERR_DEVICE;
     return nullptr;
   }
-  for (int i = 0; i < 6; i++) cudaEventCreate(&c->ev[i]);
+  for (int i = 0; i < 8; i++) cudaEventCreate(&c->ev[i]);
+  cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
+  cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+  c->sm_count = prop.multiProcessorCount;
   if (status) *status = PF_OK;
   return c;
 }
@@ -322,11 +327,14 @@ extern "C" void pf_destroy(pf_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->io, &c->disp, &c->scratch, &c->lines, &c->grain, &c->offsets, &c->masks,
-                    &c->lc, &c->index, &c->read, &c->noskip, &c->units[0], &c->units[1], &c->units[2]};
+  cudaStreamSynchronize(c->side);
+  DevBuf* bufs[] = {&c->io, &c->disp, &c->arena, &c->sidebuf, &c->jobs, &c->bases, &c->counters};
   for (DevBuf* b : bufs) b->release();
-  for (int i = 0; i < 6; i++)
+  for (int i = 0; i < 8; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  cudaEventDestroy(c->fork);
+  cudaEventDestroy(c->join);
+  cudaStreamDestroy(c->side);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -338,180 +346,245 @@ extern "C" int pf_sync(pf_ctx* c) {
 
 extern "C" void* pf_stream(pf_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
-// Queues the chain for one validated frame whose planes are at io (device).
-static int run_chain(pf_ctx* c, const pf_frame* f, const DFrame& io, const pf_frame_side* s, const DFrame* disp,
-                     pf_stats* stats) {
-  const cudaStream_t st = c->stream;
-  const bool host = s->side_memory == PF_MEM_HOST;
+
+// ---------------------------------------------------------------------------
+// Job preparation.
+
+struct FrameRef {
+  const pf_frame* f;
+  const pf_frame_side* s;
+  const pf_frame* display;  // may be null
+  void* io[3];
+  int64_t ioStride[3];
+  void* dp[3];
+  int64_t dStride[3];
+};
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+static bool cdef_any(const pf_frame* f, const pf_frame_side* s) {
+  if (!(s->stages & PF_STAGE_CDEF)) return false;
+  for (int i = 0; i < std::min((int)s->cdef.strength_count, 8); i++)
+    if (s->cdef.y_strength[i] || (!f->mono && s->cdef.uv_strength[i])) return true;
+  return false;
+}
+
+static bool lr_any(const pf_frame_side* s) {
+  return (s->stages & PF_STAGE_LOOP_RESTORATION) &&
+         (s->lr.type[0] != PF_LR_NONE || s->lr.type[1] != PF_LR_NONE || s->lr.type[2] != PF_LR_NONE);
+}
+
+static bool fg_active(const pf_frame* f, const pf_frame_side* s, int act[3]) {
+  const pf_film_grain& g = s->fg;
+  act[0] = g.apply && g.num_y_points != 0;
+  act[1] = g.apply && !f->mono && (g.num_cb_points != 0 || g.chroma_scaling_from_luma);
+  act[2] = g.apply && !f->mono && (g.num_cr_points != 0 || g.chroma_scaling_from_luma);
+  return (s->stages & PF_STAGE_FILM_GRAIN) && (act[0] || act[1] || act[2]);
+}
+
+// Scratch bytes one frame needs in the arena.
+static size_t frame_scratch(const pf_frame* f, const pf_frame_side* s) {
   const int bps = bps_of(f);
-  cudaError_t e = cudaSuccess;
+  size_t n = 0;
+  if (cdef_any(f, s) || lr_any(s)) {
+    for (int p = 0; p < 3; p++)
+      n += align256((size_t)align256((size_t)f->plane[p].alloc_width * bps) * f->plane[p].alloc_height);
+  }
+  if (lr_any(s)) {
+    for (int p = 0; p < 3; p++) {
+      if (s->lr.type[p] == PF_LR_NONE) continue;
+      const int sy = p ? f->ss_y : 0;
+      const int nb = (f->plane[p].height + (8 >> sy)) / (64 >> sy) + 2;
+      n += align256((size_t)nb * 4 * align256((size_t)f->plane[p].width * bps));
+    }
+  }
+  int act[3];
+  if (fg_active(f, s, act)) {
+    n += align256(3 * 82 * 73 * sizeof(int16_t));
+    n += align256((size_t)((f->height + 31) / 32) * ((f->width + 31) / 32));
+  }
+  return n;
+}
+
+// Host side-information bytes to copy up for one frame.
+static size_t frame_side_bytes(const pf_frame* f, const pf_frame_side* s) {
+  if (s->side_memory != PF_MEM_HOST) return 0;
+  size_t n = 0;
   const int miCols = ((f->width + 7) >> 3) << 1, miRows = ((f->height + 7) >> 3) << 1;
   const int ucols = (f->width + 63) / 64, urows = (f->height + 63) / 64;
-  uint32_t done = 0;
-  if (c->timing) cudaEventRecord(c->ev[0], st);
+  if (s->stages & PF_STAGE_LOOP_FILTER)
+    n += align256((size_t)s->lf.sb128_w * s->lf.sb128_h * PF_LF_MASK_WORDS * 2) + align256((size_t)4 * miCols * miRows);
+  if (cdef_any(f, s))
+    n += 2 * align256((size_t)s->cdef.index_stride * s->cdef.index_rows) + align256((size_t)ucols * urows * 8);
+  if (lr_any(s))
+    for (int p = 0; p < 3; p++)
+      if (s->lr.type[p] != PF_LR_NONE) n += align256(sizeof(pf_lr_unit) * s->lr.unit_count[p]);
+  return n;
+}
 
-  // ---- deblocking ----
+struct Cursor {
+  uint8_t* base;
+  size_t off;
+  void* take(size_t n) {
+    void* p = base + off;
+    off += align256(n);
+    return p;
+  }
+};
+
+static const void* put_side(std::vector<uint8_t>& hs, Cursor& dev, const void* src, size_t n) {
+  if (!src || n == 0) return src;
+  void* d = dev.take(n);
+  const size_t at = (uint8_t*)d - dev.base;
+  if (hs.size() < at + n) hs.resize(at + n);
+  memcpy(hs.data() + at, src, n);
+  return d;
+}
+
+static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, std::vector<uint8_t>& hs, FrameJob& J,
+                     int counts[ST_COUNT]) {
+  const pf_frame* f = r.f;
+  const pf_frame_side* s = r.s;
+  const int bps = bps_of(f);
+  const bool host = s->side_memory == PF_MEM_HOST;
+  memset(&J, 0, sizeof(J));
+  J.io = dframe_from(f, r.io, r.ioStride);
+  const int miCols = ((f->width + 7) >> 3) << 1, miRows = ((f->height + 7) >> 3) << 1;
+  const int ucols = (f->width + 63) / 64, urows = (f->height + 63) / 64;
+  for (int p = 0; p < 3; p++) {
+    const int xdec = p ? f->ss_x : 0, ydec = p ? f->ss_y : 0;
+    J.aw[p] = ((f->width + 7) & ~7) >> xdec;
+    J.ah[p] = ((f->height + 7) & ~7) >> ydec;
+  }
+  for (int k = 0; k < ST_COUNT; k++) counts[k] = 0;
+
+  // Deblocking.
   if (s->stages & PF_STAGE_LOOP_FILTER) {
     const pf_loop_filter& lf = s->lf;
-    LfArgs a;
-    memset(&a, 0, sizeof(a));
-    a.masks = side_ptr(c, c->masks, lf.masks, (size_t)lf.sb128_w * lf.sb128_h * PF_LF_MASK_WORDS * 2, host, &e);
-    CK(e);
-    a.level_cache = side_ptr(c, c->lc, lf.level_cache, (size_t)4 * miCols * miRows, host, &e);
-    CK(e);
+    LfArgs& a = J.lf;
+    a.masks = host ? (const uint16_t*)put_side(hs, side, lf.masks, (size_t)lf.sb128_w * lf.sb128_h * PF_LF_MASK_WORDS * 2)
+                   : lf.masks;
+    a.level_cache = host ? (const uint8_t*)put_side(hs, side, lf.level_cache, (size_t)4 * miCols * miRows) : lf.level_cache;
     a.sb128_w = lf.sb128_w;
     a.sb128_h = lf.sb128_h;
     a.mi_cols = lf.mi_cols;
     a.mi_rows = lf.mi_rows;
     a.sharpness = lf.sharpness;
     const bool lumaZero = lf.level_y[0] == 0 && lf.level_y[1] == 0;
-    a.gate_chroma[0] = 0;
     a.gate_chroma[1] = f->mono || lumaZero || lf.level_u == 0;
     a.gate_chroma[2] = f->mono || lumaZero || lf.level_v == 0;
-    CK(launch_deblock(io, a, st));
-    done |= PF_STAGE_LOOP_FILTER;
+    int tiles = 0;
+    for (int p = 0; p < 3; p++) {
+      if (a.gate_chroma[p]) continue;
+      const int sx = p ? f->ss_x : 0, sy = p ? f->ss_y : 0;
+      const int w4 = (((f->width + sx) >> sx) + 3) >> 2, h4 = (((f->height + sy) >> sy) + 3) >> 2;
+      J.db_tx[p] = (w4 + 31) / 32;
+      J.db_ty[p] = (h4 + 7) / 8;
+      tiles += J.db_tx[p] * J.db_ty[p];
+    }
+    counts[ST_DEBLOCK_V] = counts[ST_DEBLOCK_H] = tiles;
   }
-  if (c->timing) cudaEventRecord(c->ev[1], st);
 
-  // ---- CDEF (+ LR boundary lines) ----
-  const bool doLR = (s->stages & PF_STAGE_LOOP_RESTORATION) &&
-                    (s->lr.type[0] != PF_LR_NONE || s->lr.type[1] != PF_LR_NONE || s->lr.type[2] != PF_LR_NONE);
-  bool cdefAny = false;
-  const pf_cdef& cd = s->cdef;
-  if (s->stages & PF_STAGE_CDEF) {
-    for (int i = 0; i < std::min((int)cd.strength_count, 8); i++)
-      if (cd.y_strength[i] || (!f->mono && cd.uv_strength[i])) cdefAny = true;
-  }
-  void* sptr[3];
-  int64_t sstride[3];
-  DFrame B;
-  if (cdefAny || doLR) {
-    CK(layout_like(f, c->scratch, sptr, sstride));
-    B = dframe_from(f, sptr, sstride);
-    CdefArgs a;
-    memset(&a, 0, sizeof(a));
-    a.filter = cdefAny ? 1 : 0;
+  // CDEF (+ restoration boundary lines) and restoration (or copy back).
+  const bool cdefOn = cdef_any(f, s), lrOn = lr_any(s);
+  if (cdefOn || lrOn) {
+    void* sp[3];
+    int64_t ss[3];
+    for (int p = 0; p < 3; p++) {
+      ss[p] = (int64_t)align256((size_t)f->plane[p].alloc_width * bps);
+      sp[p] = arena.take((size_t)ss[p] * f->plane[p].alloc_height);
+    }
+    J.scr = dframe_from(f, sp, ss);
+    CdefArgs& a = J.cdef;
+    const pf_cdef& cd = s->cdef;
+    a.filter = cdefOn ? 1 : 0;
     a.ucols = ucols;
     a.urows = urows;
-    std::vector<uint8_t> zeros;
-    if (cdefAny) {
-      a.index = side_ptr(c, c->index, cd.index, (size_t)cd.index_stride * cd.index_rows, host, &e);
-      CK(e);
-      a.read = side_ptr(c, c->read, cd.read, (size_t)cd.index_stride * cd.index_rows, host, &e);
-      CK(e);
-      a.noskip = cd.noskip ? side_ptr(c, c->noskip, cd.noskip, (size_t)ucols * urows * 8, host, &e) : nullptr;
-      CK(e);
+    if (cdefOn) {
+      const size_t n = (size_t)cd.index_stride * cd.index_rows;
+      a.index = host ? (const uint8_t*)put_side(hs, side, cd.index, n) : cd.index;
+      a.read = host ? (const uint8_t*)put_side(hs, side, cd.read, n) : cd.read;
+      a.noskip = cd.noskip ? (host ? (const uint8_t*)put_side(hs, side, cd.noskip, (size_t)ucols * urows * 8) : cd.noskip)
+                           : nullptr;
       a.index_stride = cd.index_stride;
-    } else {
-      // Copy-only pass: an all-zero Read map (no unit filters).
-      CK(c->read.ensure((size_t)ucols * urows));
-      CK(cudaMemsetAsync(c->read.p, 0, (size_t)ucols * urows, st));
-      a.read = (const uint8_t*)c->read.p;
-      a.index = (const uint8_t*)c->read.p;
-      a.index_stride = ucols;
     }
     a.damping = cd.damping;
-    a.strength_count = cd.strength_count;
+    a.strength_count = cdefOn ? cd.strength_count : 0;
+    bool uvAny = false, yAny = false;
     for (int i = 0; i < 8; i++) {
       a.y_strength[i] = cd.y_strength[i];
       a.uv_strength[i] = cd.uv_strength[i];
     }
-    bool uvAny = false, yAny = false;
     for (int i = 0; i < std::min((int)cd.strength_count, 8); i++) {
       uvAny |= cd.uv_strength[i] != 0;
       yAny |= cd.y_strength[i] != 0;
     }
-    a.chroma_filtering = !f->mono && uvAny;
-    a.plane_process[0] = yAny || a.chroma_filtering;
-    a.plane_process[1] = a.plane_process[2] = uvAny;
-    if (doLR) {
-      size_t total = 0;
-      size_t offs[3];
+    a.chroma_filtering = cdefOn && !f->mono && uvAny;
+    a.plane_process[0] = cdefOn && (yAny || a.chroma_filtering);
+    a.plane_process[1] = a.plane_process[2] = cdefOn && uvAny;
+    J.do_lr = lrOn ? 1 : 0;
+    if (lrOn) {
       for (int p = 0; p < 3; p++) {
-        offs[p] = total;
         if (s->lr.type[p] == PF_LR_NONE) continue;
         const int sy = p ? f->ss_y : 0;
-        const int SH = 64 >> sy, off = 8 >> sy;
-        const int nb = (f->plane[p].height + off) / SH + 2;
-        const int64_t ls = ((int64_t)f->plane[p].width * bps + 255) & ~(int64_t)255;
-        a.line_stride[p] = ls;
-        total += (size_t)nb * 4 * ls;
-      }
-      CK(c->lines.ensure(total));
-      for (int p = 0; p < 3; p++) {
-        if (s->lr.type[p] == PF_LR_NONE) continue;
-        a.lines[p] = (uint8_t*)c->lines.p + offs[p];
+        const int nb = (f->plane[p].height + (8 >> sy)) / (64 >> sy) + 2;
+        a.line_stride[p] = (int64_t)align256((size_t)f->plane[p].width * bps);
+        a.lines[p] = (uint8_t*)arena.take((size_t)nb * 4 * a.line_stride[p]);
         a.save_lines[p] = 1;
-      }
-    }
-    CK(launch_cdef(io, B, a, st));
-    if (cdefAny) done |= PF_STAGE_CDEF;
-    if (c->timing) cudaEventRecord(c->ev[2], st);
-    // ---- loop restoration (or copy back) ----
-    LrArgs la;
-    memset(&la, 0, sizeof(la));
-    if (doLR) {
-      for (int p = 0; p < 3; p++) {
-        la.type[p] = s->lr.type[p];
-        if (la.type[p] == PF_LR_NONE) continue;
+        LrArgs& l = J.lr;
+        l.type[p] = s->lr.type[p];
         int horz, vert, us;
         lr_grid(f, s->lr, p, &horz, &vert, &us);
-        la.horz[p] = horz;
-        la.vert[p] = vert;
-        la.unit_size[p] = us;
-        la.units[p] = side_ptr(c, c->units[p], s->lr.units[p], sizeof(pf_lr_unit) * horz * vert, host, &e);
-        CK(e);
-        la.lines[p] = a.lines[p];
-        la.line_stride[p] = a.line_stride[p];
+        l.horz[p] = horz;
+        l.vert[p] = vert;
+        l.unit_size[p] = us;
+        l.units[p] = host ? (const pf_lr_unit*)put_side(hs, side, s->lr.units[p], sizeof(pf_lr_unit) * horz * vert)
+                          : s->lr.units[p];
+        l.lines[p] = a.lines[p];
+        l.line_stride[p] = a.line_stride[p];
       }
     }
-    CK(launch_lr(B, io, la, doLR ? 1 : 0, st));
-    if (doLR) done |= PF_STAGE_LOOP_RESTORATION;
-  } else if (c->timing) {
-    cudaEventRecord(c->ev[2], st);
+    counts[ST_CDEF] = ucols * urows;
+    int tiles = 0;
+    for (int p = 0; p < (f->mono ? 1 : 3); p++) {
+      const int sx = p ? f->ss_x : 0, sy = p ? f->ss_y : 0;
+      const int PW = 64 >> sx, SH = 64 >> sy, off = 8 >> sy;
+      J.lr_cols[p] = (J.aw[p] + PW - 1) / PW;
+      J.lr_rows[p] = (J.ah[p] + off + SH - 1) / SH;
+      tiles += J.lr_cols[p] * J.lr_rows[p];
+    }
+    counts[ST_LR] = tiles;
   }
-  if (c->timing) cudaEventRecord(c->ev[3], st);
 
-  // ---- border extension ----
+  // Border extension.
   if (s->stages & PF_STAGE_EXTEND_BORDERS) {
-    CK(launch_extend(io, st));
-    done |= PF_STAGE_EXTEND_BORDERS;
+    int tiles = 0;
+    for (int p = 0; p < (f->mono ? 1 : 3); p++) {
+      const pf_plane& pl = f->plane[p];
+      J.ext_r[p][0] = (pl.alloc_width - pl.width + 63) / 64;
+      J.ext_r[p][1] = J.ext_r[p][0] ? (pl.height + 3) / 4 : 0;
+      J.ext_b[p][0] = (pl.alloc_width + 63) / 64;
+      J.ext_b[p][1] = (pl.alloc_height - pl.height + 3) / 4;
+      tiles += J.ext_r[p][0] * J.ext_r[p][1] + J.ext_b[p][0] * J.ext_b[p][1];
+    }
+    counts[ST_EXTEND] = tiles;
   }
-  if (c->timing) cudaEventRecord(c->ev[4], st);
 
-  // ---- film grain into the display frame ----
-  if ((s->stages & PF_STAGE_FILM_GRAIN) && disp) {
-    const pf_film_grain& g = s->fg;
-    FgArgs a;
-    memset(&a, 0, sizeof(a));
-    a.active[0] = g.apply && g.num_y_points != 0;
-    a.active[1] = g.apply && !f->mono && (g.num_cb_points != 0 || g.chroma_scaling_from_luma);
-    a.active[2] = g.apply && !f->mono && (g.num_cr_points != 0 || g.chroma_scaling_from_luma);
-    if (a.active[0] || a.active[1] || a.active[2]) {
-      CK(c->grain.ensure(3 * 82 * 73 * sizeof(int16_t)));
-      int16_t* gbase = (int16_t*)c->grain.p;
-      FgTemplateArgs t;
-      memset(&t, 0, sizeof(t));
-      t.seed = g.seed;
-      t.bd = f->bit_depth;
-      t.num_y_points = g.num_y_points;
-      t.grain_scale_shift = g.grain_scale_shift;
-      t.lag = g.ar_coeff_lag;
-      t.coeff_shift = g.ar_coeff_shift;
-      memcpy(t.coeffs[0], g.ar_coeffs_y, 24);
-      memcpy(t.coeffs[1], g.ar_coeffs_cb, 25);
-      memcpy(t.coeffs[2], g.ar_coeffs_cr, 25);
-      t.active[0] = a.active[0];
-      t.active[1] = a.active[1];
-      t.active[2] = a.active[2];
-      t.ssx = f->ss_x;
-      t.ssy = f->ss_y;
-      CK(launch_fg_templates(t, gbase, gbase + 82 * 73, gbase + 2 * 82 * 73, st));
+  // Film grain into the display frame.
+  if ((s->stages & PF_STAGE_FILM_GRAIN) && r.display) {
+    J.disp = dframe_from(r.display, r.dp, r.dStride);
+    int act[3];
+    const bool on = fg_active(f, s, act);
+    FgArgs& a = J.fg;
+    if (on) {
+      const pf_film_grain& g = s->fg;
+      int16_t* gbase = (int16_t*)arena.take(3 * 82 * 73 * sizeof(int16_t));
       const int rows = (f->height + 31) / 32, cols = (f->width + 31) / 32;
-      CK(c->offsets.ensure((size_t)rows * cols));
-      CK(launch_fg_offsets(g.seed, rows, cols, (uint8_t*)c->offsets.p, st));
-      for (int p = 0; p < 3; p++) a.grain[p] = gbase + p * 82 * 73;
-      a.offsets = (const uint8_t*)c->offsets.p;
+      a.offsets = (const uint8_t*)arena.take((size_t)rows * cols);
+      for (int p = 0; p < 3; p++) {
+        a.grain[p] = gbase + p * 82 * 73;
+        a.active[p] = act[p];
+      }
       a.off_rows = rows;
       a.off_cols = cols;
       build_scaling_lut(a.lut[0], g.y_points, g.num_y_points);
@@ -534,18 +607,118 @@ static int run_chain(pf_ctx* c, const pf_frame* f, const DFrame& io, const pf_fr
       a.luma_mult[2] = g.cr_luma_mult;
       a.offset[2] = g.cr_offset;
       a.odd_luma = f->ss_x && (f->width & 1);
-      CK(launch_fg_apply(io, *disp, a, st));
-      done |= PF_STAGE_FILM_GRAIN;
-    } else {
-      // No-op grain: the display picture is the reference picture.
-      FgArgs z;
-      memset(&z, 0, sizeof(z));
-      CK(launch_fg_apply(io, *disp, z, st));
+      FgTemplateArgs& t = J.fgt;
+      t.seed = g.seed;
+      t.bd = f->bit_depth;
+      t.num_y_points = g.num_y_points;
+      t.grain_scale_shift = g.grain_scale_shift;
+      t.lag = g.ar_coeff_lag;
+      t.coeff_shift = g.ar_coeff_shift;
+      memcpy(t.coeffs[0], g.ar_coeffs_y, 24);
+      memcpy(t.coeffs[1], g.ar_coeffs_cb, 25);
+      memcpy(t.coeffs[2], g.ar_coeffs_cr, 25);
+      for (int p = 0; p < 3; p++) t.active[p] = act[p];
+      t.ssx = f->ss_x;
+      t.ssy = f->ss_y;
+      counts[ST_FG_TEMPLATES] = 1;
+      counts[ST_FG_OFFSETS] = (rows + 63) / 64;
     }
+    int tiles = 0;
+    for (int p = 0; p < (f->mono ? 1 : 3); p++) {
+      J.fg_tx[p] = (f->plane[p].alloc_width + 63) / 64;
+      J.fg_ty[p] = (f->plane[p].alloc_height + 15) / 16;
+      tiles += J.fg_tx[p] * J.fg_ty[p];
+    }
+    counts[ST_FG_APPLY] = tiles;
   }
-  if (c->timing) cudaEventRecord(c->ev[5], st);
+}
+
+// Builds the job table for n validated frames and queues every stage.
+static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats) {
+  const cudaStream_t st = c->stream;
+  size_t arenaBytes = 0, sideBytes = 0;
+  for (int i = 0; i < n; i++) {
+    arenaBytes += frame_scratch(refs[i].f, refs[i].s);
+    sideBytes += frame_side_bytes(refs[i].f, refs[i].s);
+  }
+  CK(c->arena.ensure(arenaBytes + 256));
+  CK(c->sidebuf.ensure(sideBytes + 256));
+  Cursor arena{(uint8_t*)c->arena.p, 0}, side{(uint8_t*)c->sidebuf.p, 0};
+  c->hjobs.resize(n);
+  c->hbase.assign((size_t)ST_COUNT * (n + 1), 0);
+  c->hside.clear();
+  uint32_t done = 0;
+  for (int i = 0; i < n; i++) {
+    int counts[ST_COUNT];
+    fill_job(refs[i], arena, side, c->hside, c->hjobs[i], counts);
+    for (int k = 0; k < ST_COUNT; k++) c->hbase[(size_t)k * (n + 1) + i + 1] = c->hbase[(size_t)k * (n + 1) + i] + counts[k];
+    const pf_frame_side* s = refs[i].s;
+    if (counts[ST_DEBLOCK_V]) done |= PF_STAGE_LOOP_FILTER;
+    if (cdef_any(refs[i].f, s)) done |= PF_STAGE_CDEF;
+    if (lr_any(s)) done |= PF_STAGE_LOOP_RESTORATION;
+    if (s->stages & PF_STAGE_EXTEND_BORDERS) done |= PF_STAGE_EXTEND_BORDERS;
+    if (counts[ST_FG_TEMPLATES]) done |= PF_STAGE_FILM_GRAIN;
+  }
+  if (!c->hside.empty()) CK(cudaMemcpyAsync(c->sidebuf.p, c->hside.data(), c->hside.size(), cudaMemcpyHostToDevice, st));
+  CK(c->jobs.ensure(sizeof(FrameJob) * n));
+  CK(c->bases.ensure(sizeof(int) * c->hbase.size()));
+  CK(c->counters.ensure(sizeof(int) * ST_COUNT));
+  CK(cudaMemcpyAsync(c->jobs.p, c->hjobs.data(), sizeof(FrameJob) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->bases.p, c->hbase.data(), sizeof(int) * c->hbase.size(), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(c->counters.p, 0, sizeof(int) * ST_COUNT, st));
+  BatchArgs b;
+  b.jobs = (const FrameJob*)c->jobs.p;
+  b.base = (const int*)c->bases.p;
+  b.n = n;
+  auto total = [&](int k) { return c->hbase[(size_t)k * (n + 1) + n]; };
+  auto args = [&](int k, int* grid) {
+    BatchArgs a = b;
+    const int t = total(k);
+    if (c->persistent[k] > 0 && t > c->persistent[k]) {
+      *grid = c->persistent[k];
+      a.counters = (int*)c->counters.p;
+    } else {
+      *grid = t;
+      a.counters = nullptr;
+    }
+    return a;
+  };
+  int g;
+  // Film-grain templates and offsets depend on nothing else: side stream.
+  const bool fg = total(ST_FG_TEMPLATES) > 0;
+  if (fg) {
+    CK(cudaEventRecord(c->fork, st));
+    CK(cudaStreamWaitEvent(c->side, c->fork, 0));
+    BatchArgs a = args(ST_FG_TEMPLATES, &g);
+    CK(launch_fg_templates_batch(a, total(ST_FG_TEMPLATES), g, c->side));
+    a = args(ST_FG_OFFSETS, &g);
+    CK(launch_fg_offsets_batch(a, total(ST_FG_OFFSETS), g, c->side));
+    CK(cudaEventRecord(c->join, c->side));
+  }
+  if (c->timing) CK(cudaEventRecord(c->ev[0], st));
+  BatchArgs a = args(ST_DEBLOCK_V, &g);
+  CK(launch_deblock_batch(a, total(ST_DEBLOCK_V), g, 0, st));
+  a = args(ST_DEBLOCK_H, &g);
+  CK(launch_deblock_batch(a, total(ST_DEBLOCK_H), g, 1, st));
+  if (c->timing) CK(cudaEventRecord(c->ev[1], st));
+  a = args(ST_CDEF, &g);
+  CK(launch_cdef_batch(a, total(ST_CDEF), g, st));
+  if (c->timing) CK(cudaEventRecord(c->ev[2], st));
+  a = args(ST_LR, &g);
+  CK(launch_lr_batch(a, total(ST_LR), g, st));
+  if (c->timing) CK(cudaEventRecord(c->ev[3], st));
+  a = args(ST_EXTEND, &g);
+  CK(launch_extend_batch(a, total(ST_EXTEND), g, st));
+  if (c->timing) CK(cudaEventRecord(c->ev[4], st));
+  if (fg) CK(cudaStreamWaitEvent(st, c->join, 0));
+  a = args(ST_FG_APPLY, &g);
+  CK(launch_fg_apply_batch(a, total(ST_FG_APPLY), g, st));
+  if (c->timing) CK(cudaEventRecord(c->ev[5], st));
   if (stats) {
     stats->completed = done;
+    stats->cdef_units = total(ST_CDEF);
+    stats->lr_units = total(ST_LR);
+    stats->fg_rows = total(ST_FG_OFFSETS);
   }
   return PF_OK;
 }
@@ -567,50 +740,47 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
   CK(cudaSetDevice(c->device));
   if (stats) memset(stats, 0, sizeof(*stats));
   const int bps = bps_of(f);
-  void* ioPtr[3];
-  int64_t ioStride[3];
+  FrameRef r;
+  memset(&r, 0, sizeof(r));
+  r.f = f;
+  r.s = s;
+  const bool wantDisp = (s->stages & PF_STAGE_FILM_GRAIN) && display;
+  r.display = wantDisp ? display : nullptr;
   if (f->memory == PF_MEM_HOST) {
-    CK(layout_like(f, c->io, ioPtr, ioStride));
+    CK(layout_like(f, c->io, r.io, r.ioStride));
     for (int p = 0; p < 3; p++)
-      CK(cudaMemcpy2DAsync(ioPtr[p], ioStride[p], f->plane[p].data, f->plane[p].stride,
+      CK(cudaMemcpy2DAsync(r.io[p], r.ioStride[p], f->plane[p].data, f->plane[p].stride,
                            (size_t)f->plane[p].alloc_width * bps, f->plane[p].alloc_height, cudaMemcpyHostToDevice,
                            c->stream));
   } else {
     for (int p = 0; p < 3; p++) {
-      ioPtr[p] = f->plane[p].data;
-      ioStride[p] = f->plane[p].stride;
+      r.io[p] = f->plane[p].data;
+      r.ioStride[p] = f->plane[p].stride;
     }
   }
-  DFrame io = dframe_from(f, ioPtr, ioStride);
-  const bool wantDisp = (s->stages & PF_STAGE_FILM_GRAIN) && display;
-  DFrame disp;
-  void* dPtr[3];
-  int64_t dStride[3];
   if (wantDisp) {
     if (display->memory == PF_MEM_HOST) {
-      CK(layout_like(display, c->disp, dPtr, dStride));
+      CK(layout_like(display, c->disp, r.dp, r.dStride));
     } else {
       for (int p = 0; p < 3; p++) {
-        dPtr[p] = display->plane[p].data;
-        dStride[p] = display->plane[p].stride;
+        r.dp[p] = display->plane[p].data;
+        r.dStride[p] = display->plane[p].stride;
       }
     }
-    disp = dframe_from(display, dPtr, dStride);
   }
-  st = run_chain(c, f, io, s, wantDisp ? &disp : nullptr, stats);
+  st = run_batch(c, &r, 1, stats);
   if (st != PF_OK) return st;
   if (f->memory == PF_MEM_HOST)
     for (int p = 0; p < 3; p++)
-      CK(cudaMemcpy2DAsync(f->plane[p].data, f->plane[p].stride, ioPtr[p], ioStride[p],
+      CK(cudaMemcpy2DAsync(f->plane[p].data, f->plane[p].stride, r.io[p], r.ioStride[p],
                            (size_t)f->plane[p].alloc_width * bps, f->plane[p].alloc_height, cudaMemcpyDeviceToHost,
                            c->stream));
   if (wantDisp && display->memory == PF_MEM_HOST)
     for (int p = 0; p < 3; p++)
-      CK(cudaMemcpy2DAsync(display->plane[p].data, display->plane[p].stride, dPtr[p], dStride[p],
+      CK(cudaMemcpy2DAsync(display->plane[p].data, display->plane[p].stride, r.dp[p], r.dStride[p],
                            (size_t)display->plane[p].alloc_width * bps, display->plane[p].alloc_height,
                            cudaMemcpyDeviceToHost, c->stream));
-  if (f->memory == PF_MEM_HOST || (wantDisp && display->memory == PF_MEM_HOST) || s->side_memory == PF_MEM_HOST ||
-      c->timing) {
+  if (f->memory == PF_MEM_HOST || (wantDisp && display->memory == PF_MEM_HOST) || c->timing) {
     CK(cudaStreamSynchronize(c->stream));
     read_stage_times(c, stats);
   }
@@ -620,15 +790,40 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
 
 extern "C" int pf_batch_apply(pf_ctx* c, const pf_batch_item* items, int32_t n, pf_stats* stats) {
   if (!c || (!items && n > 0) || n < 0) return PF_ERR_INVALID_ARG;
+  if (n > 65535) return PF_ERR_INVALID_ARG;
+  std::vector<FrameRef> refs((size_t)n);
   for (int i = 0; i < n; i++) {
-    int st = pf_frame_validate(items[i].frame, items[i].side, items[i].display);
+    const pf_batch_item& it = items[i];
+    int st = pf_frame_validate(it.frame, it.side, it.display);
     if (st != PF_OK) return st;
-    if (items[i].frame->memory != PF_MEM_DEVICE || items[i].side->side_memory != PF_MEM_DEVICE) return PF_ERR_INVALID_ARG;
+    const bool wantDisp = (it.side->stages & PF_STAGE_FILM_GRAIN) && it.display;
+    if (it.frame->memory != PF_MEM_DEVICE || (wantDisp && it.display->memory != PF_MEM_DEVICE))
+      return PF_ERR_INVALID_ARG;
+    FrameRef& r = refs[i];
+    memset(&r, 0, sizeof(r));
+    r.f = it.frame;
+    r.s = it.side;
+    r.display = wantDisp ? it.display : nullptr;
+    for (int p = 0; p < 3; p++) {
+      r.io[p] = it.frame->plane[p].data;
+      r.ioStride[p] = it.frame->plane[p].stride;
+      if (wantDisp) {
+        r.dp[p] = it.display->plane[p].data;
+        r.dStride[p] = it.display->plane[p].stride;
+      }
+    }
   }
-  for (int i = 0; i < n; i++) {
-    int st = pf_frame_apply(c, items[i].frame, items[i].side, items[i].display, stats);
-    if (st != PF_OK) return st;
+  CK(cudaSetDevice(c->device));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  int st = run_batch(c, refs.data(), n, stats);
+  if (st != PF_OK) return st;
+  bool hostSide = false;
+  for (int i = 0; i < n; i++) hostSide |= items[i].side->side_memory == PF_MEM_HOST;
+  if (hostSide || c->timing) {
+    CK(cudaStreamSynchronize(c->stream));
+    read_stage_times(c, stats);
   }
+  CK(cudaGetLastError());
   return PF_OK;
 }
 

@@ -147,17 +147,22 @@ __device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int se
   return y;
 }
 
-struct CdefPlaneGeom {
-  int aw[3], ah[3];  // MI-aligned plane extents (frameWorkCDEFAlignedPlane)
+struct CdefSmem {
+  uint16_t in[kSH * kSW];
+  int32_t cost[64 * 8];
+  int32_t var[64];
+  uint8_t dir[64];
 };
 
+// One 64x64 filter unit (uc, ur), all planes.  aw/ah: MI-aligned extents
+// (frameWorkCDEFAlignedPlane).
 template <typename T>
-__global__ void __launch_bounds__(256) k_cdef(DFrame in, DFrame out, CdefArgs a, CdefPlaneGeom g) {
-  __shared__ uint16_t s_in[kSH * kSW];
-  __shared__ uint8_t s_dir[64];
-  __shared__ int32_t s_var[64];
-  __shared__ int32_t s_cost[64 * 8];
-  const int uc = blockIdx.x, ur = blockIdx.y;
+__device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a, const int* aw, const int* ah,
+                          int uc, int ur, CdefSmem& sm) {
+  uint16_t* s_in = sm.in;
+  uint8_t* s_dir = sm.dir;
+  int32_t* s_var = sm.var;
+  int32_t* s_cost = sm.cost;
   const int tid = threadIdx.x;
   const int coeffShift = in.bd - 8;
   const int mapOff = ur * a.index_stride + uc;
@@ -173,7 +178,7 @@ __global__ void __launch_bounds__(256) k_cdef(DFrame in, DFrame out, CdefArgs a,
   const int nplanes = in.mono ? 1 : 3;
   for (int plane = 0; plane < nplanes; plane++) {
     const int xdec = plane ? in.ssx : 0, ydec = plane ? in.ssy : 0;
-    const int Wa = g.aw[plane], Ha = g.ah[plane];
+    const int Wa = aw[plane], Ha = ah[plane];
     const int unitX = (uc * 64) >> xdec, unitY = (ur * 64) >> ydec;
     const int unitW = imin(64 >> xdec, Wa - unitX), unitH = imin(64 >> ydec, Ha - unitY);
     if (unitW <= 0 || unitH <= 0) continue;
@@ -313,21 +318,25 @@ __global__ void __launch_bounds__(256) k_cdef(DFrame in, DFrame out, CdefArgs a,
   }
 }
 
-cudaError_t launch_cdef(const DFrame& in, const DFrame& out, const CdefArgs& a, cudaStream_t st) {
-  CdefPlaneGeom g;
-  for (int p = 0; p < 3; p++) {
-    const int xdec = p ? in.ssx : 0, ydec = p ? in.ssy : 0;
-    // MI-aligned extent (frameWorkCDEFAlignedPlane); the validated allocation
-    // always covers it.
-    const int aw = ((in.width + 7) & ~7) >> xdec, ah = ((in.height + 7) & ~7) >> ydec;
-    g.aw[p] = aw;
-    g.ah[p] = ah;
-  }
-  dim3 grd(a.ucols, a.urows);
-  if (in.bd == 8)
-    k_cdef<uint8_t><<<grd, 256, 0, st>>>(in, out, a, g);
-  else
-    k_cdef<uint16_t><<<grd, 256, 0, st>>>(in, out, a, g);
+// Batched CDEF: each work item is one 64x64 unit of one frame.
+__global__ void __launch_bounds__(256) k_cdef_batch(BatchArgs b) {
+  __shared__ CdefSmem sm;
+  const int* base = b.base + ST_CDEF * (b.n + 1);
+  for_each_item(base[b.n], b.counters ? b.counters + ST_CDEF : nullptr, [&](int item) {
+    const int fi = find_frame(base, b.n, item);
+    const FrameJob& J = b.jobs[fi];
+    const int local = item - base[fi];
+    const int uc = local % J.cdef.ucols, ur = local / J.cdef.ucols;
+    if (J.io.bd == 8)
+      cdef_unit<uint8_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, sm);
+    else
+      cdef_unit<uint16_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, sm);
+  });
+}
+
+cudaError_t launch_cdef_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  k_cdef_batch<<<grid, 256, 0, st>>>(b);
   return cudaGetLastError();
 }
 

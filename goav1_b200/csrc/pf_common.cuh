@@ -93,4 +93,72 @@ struct FgTemplateArgs {
   int ssx, ssy;
 };
 
+// ---- batched execution: one launch per stage over the frames of a batch ----
+
+enum Stage {
+  ST_FG_TEMPLATES = 0,
+  ST_DEBLOCK_V,
+  ST_DEBLOCK_H,
+  ST_CDEF,
+  ST_LR,
+  ST_EXTEND,
+  ST_FG_OFFSETS,
+  ST_FG_APPLY,
+  ST_COUNT
+};
+
+// Work items of a stage are numbered frame after frame; base[f] is the first
+// item of frame f (base[n] = total).  Each stage decodes its local index.
+struct FrameJob {
+  DFrame io;    // the frame, filtered in place
+  DFrame scr;   // CDEF output scratch (same geometry)
+  DFrame disp;  // film-grain display frame
+  LfArgs lf;
+  CdefArgs cdef;
+  LrArgs lr;
+  FgArgs fg;
+  FgTemplateArgs fgt;
+  int aw[3], ah[3];          // MI-aligned plane extents
+  int db_tx[3], db_ty[3];    // deblock tiles (32x8 edge units) per plane (0 = gated)
+  int lr_cols[3], lr_rows[3];  // restoration tiles (processing column x stripe)
+  int fg_tx[3], fg_ty[3];    // 64x16-sample tiles of the display planes
+  int ext_r[3][2], ext_b[3][2];  // extension tiles: right strip, bottom strip
+  int do_lr;
+};
+
+struct BatchArgs {
+  const FrameJob* jobs;
+  const int* base;  // ST_COUNT arrays of n+1 ints, stage-major
+  int n;
+  int* counters;    // ST_COUNT work counters (persistent mode), or null
+};
+
+__device__ __forceinline__ int find_frame(const int* base, int n, int item) {
+  int lo = 0, hi = n;  // base[lo] <= item < base[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(&base[mid]) <= item) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Runs f(item) for the CTA's work items: one item per CTA (grid = total), or
+// a persistent CTA draining the stage's queue through an atomic counter.
+template <typename F>
+__device__ __forceinline__ void for_each_item(int total, int* counter, F f) {
+  if (counter == nullptr) {
+    if ((int)blockIdx.x < total) f((int)blockIdx.x);
+    return;
+  }
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= total) break;
+    f(it);
+  }
+}
+
 }  // namespace pf

@@ -108,14 +108,11 @@ __device__ __forceinline__ void lpf_unit(T* q, int sa, int sb, int bd, int E, in
   }
 }
 
-// One thread per 4x4 edge unit (c4, r4) of plane blockIdx.z; dir 0 filters
-// the unit's left (vertical) edge, dir 1 its top (horizontal) edge.
+// One thread per 4x4 edge unit (c4, r4) of `plane`; dir 0 filters the
+// unit's left (vertical) edge, dir 1 its top (horizontal) edge.
 template <typename T>
-__global__ void __launch_bounds__(256) k_deblock(DFrame f, LfArgs a, int dir) {
-  const int plane = blockIdx.z;
+__device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, int dir, int plane, int c4, int r4) {
   if (a.gate_chroma[plane]) return;
-  const int c4 = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r4 = blockIdx.y * blockDim.y + threadIdx.y;
   const int ssx = plane ? f.ssx : 0, ssy = plane ? f.ssy : 0;
   // frameWorkLoopFilterPlaneSize: edge positions inside the 4-aligned crop.
   const int w4 = ((plane ? (f.width + ssx) >> ssx : f.width) + 3) >> 2;
@@ -134,14 +131,14 @@ __global__ void __launch_bounds__(256) k_deblock(DFrame f, LfArgs a, int dir) {
     const int half = bit >> 4, b = bit & 15;
 #pragma unroll
     for (int kk = 2; kk >= 0; kk--) {
-      if (k < 0 && ((region[((dir * 32 + pos) * 3 + kk) * 2 + half] >> b) & 1)) k = kk;
+      if (k < 0 && ((__ldg(&region[((dir * 32 + pos) * 3 + kk) * 2 + half]) >> b) & 1)) k = kk;
     }
   } else {
     const int lane = dir == 0 ? (16 >> ssy) : (16 >> ssx);
     const int half = bit / lane, b = bit - half * lane;
 #pragma unroll
     for (int kk = 1; kk >= 0; kk--) {
-      if (k < 0 && ((region[384 + ((dir * 32 + pos) * 2 + kk) * 2 + half] >> b) & 1)) k = kk;
+      if (k < 0 && ((__ldg(&region[384 + ((dir * 32 + pos) * 2 + kk) * 2 + half]) >> b) & 1)) k = kk;
     }
   }
   if (k < 0) return;
@@ -149,8 +146,8 @@ __global__ void __launch_bounds__(256) k_deblock(DFrame f, LfArgs a, int dir) {
   // Level with the left / above fallback (sb.go:122-128, :142-148).
   const int comp = luma ? dir : plane + 1;
   const int li = r4 * a.mi_cols + c4;
-  int L = a.level_cache[4 * li + comp];
-  if (L == 0) L = a.level_cache[4 * (dir == 0 ? li - 1 : li - a.mi_cols) + comp];
+  int L = __ldg(&a.level_cache[4 * li + comp]);
+  if (L == 0) L = __ldg(&a.level_cache[4 * (dir == 0 ? li - 1 : li - a.mi_cols) + comp]);
   if (L == 0) return;
   // loopfilter/threshold.go:18-47.
   const int sh = a.sharpness;
@@ -177,17 +174,32 @@ __global__ void __launch_bounds__(256) k_deblock(DFrame f, LfArgs a, int dir) {
     lpf_unit<T>(q, 1, sstride, f.bd, E, I, H, wd);
 }
 
-// Host launcher: vertical edges of all planes, then horizontal edges.
-cudaError_t launch_deblock(const DFrame& f, const LfArgs& a, cudaStream_t st) {
-  const int w4 = (f.width + 3) >> 2, h4 = (f.height + 3) >> 2;
-  dim3 blk(32, 8);
-  dim3 grd((w4 + 31) / 32, (h4 + 7) / 8, f.mono ? 1 : 3);
-  for (int dir = 0; dir < 2; dir++) {
-    if (f.bd == 8)
-      k_deblock<uint8_t><<<grd, blk, 0, st>>>(f, a, dir);
+// Batched deblocking: each work item is one 32x8 tile of edge units of one
+// plane of one frame; 256 threads, one edge unit each.
+__global__ void __launch_bounds__(256) k_deblock_batch(BatchArgs b, int dir) {
+  const int stage = dir == 0 ? ST_DEBLOCK_V : ST_DEBLOCK_H;
+  const int* base = b.base + stage * (b.n + 1);
+  for_each_item(base[b.n], b.counters ? b.counters + stage : nullptr, [&](int item) {
+    const int fi = find_frame(base, b.n, item);
+    const FrameJob& J = b.jobs[fi];
+    int local = item - base[fi];
+    int plane = 0;
+    while (plane < 2 && local >= J.db_tx[plane] * J.db_ty[plane]) {
+      local -= J.db_tx[plane] * J.db_ty[plane];
+      plane++;
+    }
+    const int tx = local % J.db_tx[plane], ty = local / J.db_tx[plane];
+    const int c4 = tx * 32 + (threadIdx.x & 31), r4 = ty * 8 + (threadIdx.x >> 5);
+    if (J.io.bd == 8)
+      deblock_unit<uint8_t>(J.io, J.lf, dir, plane, c4, r4);
     else
-      k_deblock<uint16_t><<<grd, blk, 0, st>>>(f, a, dir);
-  }
+      deblock_unit<uint16_t>(J.io, J.lf, dir, plane, c4, r4);
+  });
+}
+
+cudaError_t launch_deblock_batch(const BatchArgs& b, int total, int grid, int dir, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  k_deblock_batch<<<grid, 256, 0, st>>>(b, dir);
   return cudaGetLastError();
 }
 

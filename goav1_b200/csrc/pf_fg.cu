@@ -8,11 +8,13 @@
 // apply.go:72-343, :414-546 and blend.go:16-25 (per-32x32 block offsets drawn
 // in order from each stripe's LFSR, overlap blends, noise and clipping).
 //
-// GPU shape: the 82x73 templates are generated by one CTA per frame: the
-// Gaussian fill is a serial LFSR walk, the AR filter runs as a wavefront over
-// t = x + 4y (every AR input of sample (y, x) has a smaller t), one warp per
-// template.  Offsets come from one thread per 32-row stripe.  The apply is
-// one thread per output sample.
+// GPU shape: the 82x73 templates are generated by one CTA per frame.  The
+// Gaussian fill is split over 32 lanes: the LFSR is linear over GF(2)^16, so
+// lane k starts from M^(kL) * seed (jump matrices precomputed on the host) and
+// walks its L draws; the AR filter runs as a wavefront over t = x + 4y (every
+// AR input of sample (y, x) has a smaller t), one warp per template.  Offsets
+// come from one thread per 32-row stripe.  The apply is one thread per output
+// sample, 64x16-sample tiles per CTA.
 #include "pf_common.cuh"
 #include "pf_tables.h"
 
@@ -65,24 +67,55 @@ __device__ void ar_wavefront(int16_t* g, const int16_t* luma, const FgTemplateAr
   }
 }
 
-// One CTA (3 warps) per frame: luma template, then both chroma templates.
-__global__ void k_fg_templates(FgTemplateArgs p, int16_t* gy, int16_t* gu, int16_t* gv) {
-  __shared__ int16_t s_g[3][kGW * kGH];
+// Jump matrices: c_jump[t][k][c] = M^(k*L_t) e_c for the three template
+// shapes (t = 0: 82x73, 1: 44x73, 2: 44x38), L_t = ceil(samples / 32).
+__constant__ uint16_t c_jump[3][32][16];
+__constant__ int c_jump_len[3];
+
+__device__ __forceinline__ uint16_t gf2_apply(const uint16_t* cols, uint16_t v) {
+  uint16_t r = 0;
+#pragma unroll
+  for (int c = 0; c < 16; c++)
+    if ((v >> c) & 1) r ^= cols[c];
+  return r;
+}
+
+// Gaussian fill of one template (luma.go:32-38 / chroma.go:38-44): draw i of
+// the plane's LFSR goes to sample (i / w, i % w).  One warp.
+__device__ void gauss_fill(int16_t* g, uint16_t seed, int w, int h, int shape, int shift) {
+  const int lane = threadIdx.x & 31;
+  const int L = c_jump_len[shape];
+  uint16_t reg = gf2_apply(c_jump[shape][lane], seed);
+  const int n = w * h;
+  int i = lane * L;
+  const int iend = imin(i + L, n);
+  int y = i / w, x = i - y * w;
+  for (; i < iend; i++) {
+    g[y * kGW + x] = (int16_t)rpow2(c_gauss[lfsr(reg, 11)], shift);
+    if (++x == w) {
+      x = 0;
+      y++;
+    }
+  }
+}
+
+// One frame's templates: luma (warp 0), then Cb and Cr (warps 1, 2).
+__device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, int16_t (*s_g)[kGW * kGH]) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int16_t* outs[3] = {gy, gu, gv};
-  // Gaussian fill: one serial LFSR walk per template (lane 0 of its warp).
+  const int cw = p.ssx ? 44 : kGW, ch = p.ssy ? 38 : kGH;
+  const int cshape = p.ssx ? (p.ssy ? 2 : 1) : 0;
   if (warp < 3) {
     int16_t* g = s_g[warp];
     for (int i = lane; i < kGW * kGH; i += 32) g[i] = 0;
     __syncwarp();
     const bool active = warp == 0 ? p.num_y_points != 0 : p.active[warp];
-    if (active && lane == 0) {
-      const int w = warp == 0 ? kGW : (p.ssx ? 44 : kGW);
-      const int h = warp == 0 ? kGH : (p.ssy ? 38 : kGH);
-      uint16_t reg = warp == 0 ? p.seed : (uint16_t)(p.seed ^ (warp == 1 ? 0xb524 : 0x49d8));
-      const int shift = 12 - p.bd + p.grain_scale_shift;
-      for (int y = 0; y < h; y++)
-        for (int x = 0; x < w; x++) g[y * kGW + x] = (int16_t)rpow2(c_gauss[lfsr(reg, 11)], shift);
+    const int shift = 12 - p.bd + p.grain_scale_shift;
+    if (active) {
+      if (warp == 0)
+        gauss_fill(g, p.seed, kGW, kGH, 0, shift);
+      else
+        gauss_fill(g, (uint16_t)(p.seed ^ (warp == 1 ? 0xb524 : 0x49d8)), cw, ch, cshape, shift);
     }
     __syncwarp();
   }
@@ -91,7 +124,7 @@ __global__ void k_fg_templates(FgTemplateArgs p, int16_t* gy, int16_t* gu, int16
   __syncthreads();
   if (warp == 1 || warp == 2) {
     const bool run = p.active[warp] && !(p.lag == 0 && p.num_y_points == 0);
-    if (run) ar_wavefront(s_g[warp], s_g[0], p, warp, p.ssx ? 44 : kGW, p.ssy ? 38 : kGH);
+    if (run) ar_wavefront(s_g[warp], s_g[0], p, warp, cw, ch);
   }
   __syncthreads();
   for (int pl = 0; pl < 3; pl++)
@@ -101,9 +134,7 @@ __global__ void k_fg_templates(FgTemplateArgs p, int16_t* gy, int16_t* gu, int16
 
 // Offsets of every 32x32 block: row r uses the LFSR seeded by stripe r
 // (random.go:39-49), one Number(8) per block in order (apply.go:72-125).
-__global__ void k_fg_offsets(uint16_t seed, int rows, int cols, uint8_t* out) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= rows) return;
+__device__ __forceinline__ void fg_offsets_row(uint16_t seed, int r, int cols, uint8_t* out) {
   const int n = r;  // lumaLine >> 5 with lumaLine = 32 r
   uint16_t reg = seed;
   reg ^= (uint16_t)(((n * 37 + 178) & 255) << 8);
@@ -128,13 +159,10 @@ __device__ __forceinline__ int blend_w(int prev, int cur, int pw, int cw, int bd
 // Display = reference with grain added on the cropped area of active planes;
 // every allocated sample of the display frame is written.
 template <typename T>
-__global__ void __launch_bounds__(256) k_fg_apply(DFrame ref, DFrame disp, FgArgs a) {
-  const int plane = blockIdx.z;
-  if (plane > 0 && ref.mono) return;
+__device__ __forceinline__ void fg_apply_px(const DFrame& ref, const DFrame& disp, const FgArgs& a, int plane, int x,
+                                            int y) {
   const DPlane& sp = ref.pl[plane];
   const DPlane& dp = disp.pl[plane];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= sp.aw || y >= sp.ah) return;
   const int s = row_ptr<T>(sp, y)[x];
   if (!a.active[plane] || x >= sp.w || y >= sp.h) {
@@ -203,47 +231,142 @@ __global__ void __launch_bounds__(256) k_fg_apply(DFrame ref, DFrame disp, FgArg
 // frame/buffer.go:339-400: replicate the last visible column into the padding
 // columns of every visible row, then the last visible row into padding rows.
 template <typename T>
-__global__ void k_extend(DFrame f) {
-  const int plane = blockIdx.z;
-  if (plane > 0 && f.mono) return;
+__device__ __forceinline__ void extend_px(const DFrame& f, int plane, int x, int y) {
   const DPlane& p = f.pl[plane];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= p.aw || y >= p.ah) return;
   if (x < p.w && y < p.h) return;
   const int h = imin(p.h, p.ah);
   row_ptr<T>(p, y)[x] = row_ptr<T>(p, imin(y, h - 1))[imin(x, p.w - 1)];
 }
 
-cudaError_t fg_upload_tables() { return cudaMemcpyToSymbol(c_gauss, pf_gaussian_sequence, sizeof(pf_gaussian_sequence)); }
+// ---- batched kernels ----
 
-cudaError_t launch_fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, cudaStream_t st) {
-  k_fg_templates<<<1, 96, 0, st>>>(p, gy, gu, gv);
+__global__ void __launch_bounds__(96) k_fg_templates_batch(BatchArgs b) {
+  __shared__ int16_t s_g[3][kGW * kGH];
+  const int* base = b.base + ST_FG_TEMPLATES * (b.n + 1);
+  for_each_item(base[b.n], b.counters ? b.counters + ST_FG_TEMPLATES : nullptr, [&](int item) {
+    const FrameJob& J = b.jobs[find_frame(base, b.n, item)];
+    fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], s_g);
+  });
+}
+
+__global__ void __launch_bounds__(64) k_fg_offsets_batch(BatchArgs b) {
+  const int* base = b.base + ST_FG_OFFSETS * (b.n + 1);
+  for_each_item(base[b.n], b.counters ? b.counters + ST_FG_OFFSETS : nullptr, [&](int item) {
+    const int fi = find_frame(base, b.n, item);
+    const FrameJob& J = b.jobs[fi];
+    const int r = (item - base[fi]) * 64 + threadIdx.x;
+    if (r < J.fg.off_rows) fg_offsets_row(J.fgt.seed, r, J.fg.off_cols, const_cast<uint8_t*>(J.fg.offsets));
+  });
+}
+
+// Display frame: 64x16-sample tiles of each plane, 256 threads x 4 rows.
+__global__ void __launch_bounds__(256) k_fg_apply_batch(BatchArgs b) {
+  const int* base = b.base + ST_FG_APPLY * (b.n + 1);
+  for_each_item(base[b.n], b.counters ? b.counters + ST_FG_APPLY : nullptr, [&](int item) {
+    const int fi = find_frame(base, b.n, item);
+    const FrameJob& J = b.jobs[fi];
+    int local = item - base[fi];
+    int plane = 0;
+    while (plane < 2 && local >= J.fg_tx[plane] * J.fg_ty[plane]) {
+      local -= J.fg_tx[plane] * J.fg_ty[plane];
+      plane++;
+    }
+    const int tx = local % J.fg_tx[plane], ty = local / J.fg_tx[plane];
+    const int x = tx * 64 + (threadIdx.x & 63);
+    for (int k = 0; k < 4; k++) {
+      const int y = ty * 16 + (threadIdx.x >> 6) * 4 + k;
+      if (J.io.bd == 8)
+        fg_apply_px<uint8_t>(J.io, J.disp, J.fg, plane, x, y);
+      else
+        fg_apply_px<uint16_t>(J.io, J.disp, J.fg, plane, x, y);
+    }
+  });
+}
+
+// Border extension: 64x4-sample tiles of the right strip [w, aw) x [0, h)
+// then of the bottom strip [0, aw) x [h, ah), per plane.
+__global__ void __launch_bounds__(256) k_extend_batch(BatchArgs b) {
+  const int* base = b.base + ST_EXTEND * (b.n + 1);
+  for_each_item(base[b.n], b.counters ? b.counters + ST_EXTEND : nullptr, [&](int item) {
+    const int fi = find_frame(base, b.n, item);
+    const FrameJob& J = b.jobs[fi];
+    int local = item - base[fi];
+    for (int plane = 0; plane < 3; plane++) {
+      const int nr = J.ext_r[plane][0] * J.ext_r[plane][1], nb = J.ext_b[plane][0] * J.ext_b[plane][1];
+      if (local >= nr + nb) {
+        local -= nr + nb;
+        continue;
+      }
+      const DPlane& p = J.io.pl[plane];
+      int x, y;
+      if (local < nr) {
+        x = p.w + (local % J.ext_r[plane][0]) * 64 + (threadIdx.x & 63);
+        y = (local / J.ext_r[plane][0]) * 4 + (threadIdx.x >> 6);
+        if (y >= p.h) return;
+      } else {
+        local -= nr;
+        x = (local % J.ext_b[plane][0]) * 64 + (threadIdx.x & 63);
+        y = p.h + (local / J.ext_b[plane][0]) * 4 + (threadIdx.x >> 6);
+      }
+      if (J.io.bd == 8)
+        extend_px<uint8_t>(J.io, plane, x, y);
+      else
+        extend_px<uint16_t>(J.io, plane, x, y);
+      return;
+    }
+  });
+}
+
+// LFSR step as a GF(2)^16 map, for the host-side jump tables.
+static uint16_t lfsr_step_host(uint16_t reg) {
+  const uint16_t bit = ((reg >> 0) ^ (reg >> 1) ^ (reg >> 3) ^ (reg >> 12)) & 1;
+  return (uint16_t)((reg >> 1) | (bit << 15));
+}
+
+cudaError_t fg_upload_tables() {
+  cudaError_t e = cudaMemcpyToSymbol(c_gauss, pf_gaussian_sequence, sizeof(pf_gaussian_sequence));
+  if (e != cudaSuccess) return e;
+  static uint16_t jump[3][32][16];
+  int lens[3];
+  const int samples[3] = {82 * 73, 44 * 73, 44 * 38};
+  for (int t = 0; t < 3; t++) {
+    const int L = (samples[t] + 31) / 32;
+    lens[t] = L;
+    uint16_t cols[16];
+    for (int c = 0; c < 16; c++) cols[c] = (uint16_t)(1u << c);
+    for (int k = 0; k < 32; k++) {
+      for (int c = 0; c < 16; c++) jump[t][k][c] = cols[c];
+      for (int c = 0; c < 16; c++)
+        for (int s = 0; s < L; s++) cols[c] = lfsr_step_host(cols[c]);
+    }
+  }
+  e = cudaMemcpyToSymbol(c_jump, jump, sizeof(jump));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_jump_len, lens, sizeof(lens));
+  return e;
+}
+
+cudaError_t launch_fg_templates_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  k_fg_templates_batch<<<grid, 96, 0, st>>>(b);
   return cudaGetLastError();
 }
 
-cudaError_t launch_fg_offsets(uint16_t seed, int rows, int cols, uint8_t* out, cudaStream_t st) {
-  k_fg_offsets<<<(rows + 63) / 64, 64, 0, st>>>(seed, rows, cols, out);
+cudaError_t launch_fg_offsets_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  k_fg_offsets_batch<<<grid, 64, 0, st>>>(b);
   return cudaGetLastError();
 }
 
-cudaError_t launch_fg_apply(const DFrame& ref, const DFrame& disp, const FgArgs& a, cudaStream_t st) {
-  dim3 blk(64, 4);
-  dim3 grd((ref.pl[0].aw + 63) / 64, (ref.pl[0].ah + 3) / 4, ref.mono ? 1 : 3);
-  if (ref.bd == 8)
-    k_fg_apply<uint8_t><<<grd, blk, 0, st>>>(ref, disp, a);
-  else
-    k_fg_apply<uint16_t><<<grd, blk, 0, st>>>(ref, disp, a);
+cudaError_t launch_fg_apply_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  k_fg_apply_batch<<<grid, 256, 0, st>>>(b);
   return cudaGetLastError();
 }
 
-cudaError_t launch_extend(const DFrame& f, cudaStream_t st) {
-  dim3 blk(64, 4);
-  dim3 grd((f.pl[0].aw + 63) / 64, (f.pl[0].ah + 3) / 4, f.mono ? 1 : 3);
-  if (f.bd == 8)
-    k_extend<uint8_t><<<grd, blk, 0, st>>>(f);
-  else
-    k_extend<uint16_t><<<grd, blk, 0, st>>>(f);
+cudaError_t launch_extend_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  k_extend_batch<<<grid, 256, 0, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -29,8 +29,10 @@ __constant__ uint16_t c_one_by_x[25];
 
 constexpr int kWin = 70;  // 64 + 2*3
 
-struct LrGeom {
-  int aw[3], ah[3];
+struct LrSmem {
+  uint16_t win[kWin * kWin];
+  int32_t A[66 * 66];
+  int32_t B[66 * 66];
 };
 
 __device__ __forceinline__ int32_t rpot(int32_t v, int bits) {
@@ -40,20 +42,19 @@ __device__ __forceinline__ uint32_t rpotu(uint32_t v, int bits) {
   return bits <= 0 ? v : (v + (1u << (bits - 1))) >> bits;
 }
 
+// One restoration tile: processing column j of stripe s of `plane`.
 template <typename T>
-__global__ void __launch_bounds__(256) k_lr(DFrame src, DFrame dst, LrArgs a, LrGeom g, int enabled) {
-  __shared__ uint16_t s_win[kWin * kWin];
-  __shared__ int32_t s_A[66 * 66];
-  __shared__ int32_t s_B[66 * 66];
-  const int plane = blockIdx.z;
-  if (plane > 0 && src.mono) return;
+__device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, const int* aw, const int* ah,
+                        int enabled, int plane, int j, int s, LrSmem& sm) {
+  uint16_t* s_win = sm.win;
+  int32_t* s_A = sm.A;
+  int32_t* s_B = sm.B;
   const int ssx = plane ? src.ssx : 0, ssy = plane ? src.ssy : 0;
   const int PW = 64 >> ssx, SH = 64 >> ssy, off = 8 >> ssy;
-  const int Wa = g.aw[plane], Ha = g.ah[plane];
+  const int Wa = aw[plane], Ha = ah[plane];
   const DPlane& sp = src.pl[plane];
   const DPlane& dp = dst.pl[plane];
   const int Wc = sp.w, Hc = sp.h;
-  const int s = blockIdx.y, j = blockIdx.x;
   const int x0 = j * PW;
   const int y0 = imax(0, s * SH - off);
   if (x0 >= Wa || y0 >= Ha) return;
@@ -245,25 +246,32 @@ cudaError_t lr_upload_tables() {
   return e;
 }
 
-cudaError_t launch_lr(const DFrame& src, const DFrame& dst, const LrArgs& a, int enabled, cudaStream_t st) {
-  LrGeom g;
-  int maxCols = 0, maxStripes = 0;
-  for (int p = 0; p < (src.mono ? 1 : 3); p++) {
-    const int xdec = p ? src.ssx : 0, ydec = p ? src.ssy : 0;
-    // MI-aligned extent (frameWorkCDEFAlignedPlane); the validated allocation
-    // always covers it.
-    const int aw = ((src.width + 7) & ~7) >> xdec, ah = ((src.height + 7) & ~7) >> ydec;
-    g.aw[p] = aw;
-    g.ah[p] = ah;
-    const int PW = 64 >> xdec, SH = 64 >> ydec, off = 8 >> ydec;
-    maxCols = imax(maxCols, (aw + PW - 1) / PW);
-    maxStripes = imax(maxStripes, (ah + off + SH - 1) / SH);
-  }
-  dim3 grd(maxCols, maxStripes, src.mono ? 1 : 3);
-  if (src.bd == 8)
-    k_lr<uint8_t><<<grd, 256, 0, st>>>(src, dst, a, g, enabled);
-  else
-    k_lr<uint16_t><<<grd, 256, 0, st>>>(src, dst, a, g, enabled);
+// Batched restoration: each work item is one (processing column, stripe)
+// tile of one plane of one frame.  Frames without restoration get the copy
+// of the CDEF output back into the frame.
+__global__ void __launch_bounds__(256) k_lr_batch(BatchArgs b) {
+  __shared__ LrSmem sm;
+  const int* base = b.base + ST_LR * (b.n + 1);
+  for_each_item(base[b.n], b.counters ? b.counters + ST_LR : nullptr, [&](int item) {
+    const int fi = find_frame(base, b.n, item);
+    const FrameJob& J = b.jobs[fi];
+    int local = item - base[fi];
+    int plane = 0;
+    while (plane < 2 && local >= J.lr_cols[plane] * J.lr_rows[plane]) {
+      local -= J.lr_cols[plane] * J.lr_rows[plane];
+      plane++;
+    }
+    const int j = local % J.lr_cols[plane], s = local / J.lr_cols[plane];
+    if (J.io.bd == 8)
+      lr_tile<uint8_t>(J.scr, J.io, J.lr, J.aw, J.ah, J.do_lr, plane, j, s, sm);
+    else
+      lr_tile<uint16_t>(J.scr, J.io, J.lr, J.aw, J.ah, J.do_lr, plane, j, s, sm);
+  });
+}
+
+cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  k_lr_batch<<<grid, 256, 0, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -132,3 +132,25 @@ def test_repeated_calls_are_deterministic(runner):
     b, db = _gpu(runner, fr, si)
     _assert_same(a, b, "repeat")
     _assert_same(da, db, "repeat display")
+
+
+def test_batch_mixed_sizes_depths_formats(runner):
+    """One pf_batch_apply over frames of different size, bit depth and chroma
+    format equals per-frame oracle runs."""
+    from goav1_b200.postfilter import DeviceFrame, device_side
+
+    specs = [dict(width=320, height=180), dict(width=320, height=180), dict(width=640, height=360, bit_depth=10),
+             dict(width=256, height=144, ss=(0, 0)), dict(width=200, height=130, bit_depth=12, ss=(1, 0)),
+             dict(width=66, height=66)]
+    frames = [synth.make_frame(1, 100 + i, **kw) for i, kw in enumerate(specs)]
+    items, keep = [], []
+    for fr, si in frames:
+        d, dd, ds = DeviceFrame(fr), DeviceFrame(fr.like()), device_side(si, fr)
+        keep.append((d, dd, ds))
+        items.append((d.pf(), ds.side, dd.pf()))
+    runner.apply_batch(items)
+    runner.sync()
+    for (fr, si), (d, dd, _) in zip(frames, keep):
+        ref, rdisp = _oracle(fr, si)
+        _assert_same(ref, d.download(), "batch reference")
+        _assert_same(rdisp, dd.download(), "batch display")
