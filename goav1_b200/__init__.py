@@ -28,6 +28,7 @@ def lib():
     L.pf_abi_version.restype = C.c_int
     L.pf_status_string.argtypes = [C.c_int]
     L.pf_status_string.restype = C.c_char_p
+    L.pf_status_detail.restype = C.c_char_p
     L.pf_create.argtypes = [C.POINTER(abi.pf_config), C.POINTER(C.c_int)]
     L.pf_create.restype = C.c_void_p
     L.pf_destroy.argtypes = [C.c_void_p]

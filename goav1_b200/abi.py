@@ -209,6 +209,7 @@ class pf_cdef_search_result(C.Structure):
 EXPORTED_SYMBOLS = (
     "pf_abi_version",
     "pf_status_string",
+    "pf_status_detail",
     "pf_create",
     "pf_destroy",
     "pf_frame_apply",

@@ -257,18 +257,25 @@ static void build_scaling_lut(uint8_t* dst, const uint8_t (*pts)[2], int n) {
   for (int x = pts[n - 1][0]; x < 256; x++) dst[x] = pts[n - 1][1];
 }
 
-#define CK(expr)                       \
-  do {                                 \
-    cudaError_t _e = (expr);           \
-    if (_e != cudaSuccess) {           \
-      last_error(_e);                  \
-      return PF_ERR_DEVICE;            \
-    }                                  \
+// The last failing CUDA call of this thread, for pf_status_detail().
+static thread_local char g_detail[256];
+
+static void last_error(cudaError_t e, const char* expr, int line) {
+  snprintf(g_detail, sizeof(g_detail), "%s (%s) at pf_api.cu:%d: %s", cudaGetErrorName(e), cudaGetErrorString(e),
+           line, expr);
+  if (getenv("PF_DEBUG")) fprintf(stderr, "goav1pf: %s\n", g_detail);
+}
+
+#define CK(expr)                        \
+  do {                                  \
+    cudaError_t _e = (expr);            \
+    if (_e != cudaSuccess) {            \
+      last_error(_e, #expr, __LINE__);  \
+      return PF_ERR_DEVICE;             \
+    }                                   \
   } while (0)
 
-static void last_error(cudaError_t e) {
-  if (getenv("PF_DEBUG")) fprintf(stderr, "goav1pf: CUDA error %s\n", cudaGetErrorString(e));
-}
+extern "C" const char* pf_status_detail(void) { return g_detail; }
 
 extern "C" int pf_abi_version(void) { return PF_ABI_VERSION; }
 
@@ -727,7 +734,10 @@ static void read_stage_times(pf_ctx* c, pf_stats* stats) {
   if (!stats || !c->timing) return;
   for (int i = 0; i < 5; i++) {
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]);
+    if (cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]) != cudaSuccess) {
+      ms = -1.f;
+      (void)cudaGetLastError();  // a timing read is not a device fault
+    }
     stats->stage_ms[i] = ms;
   }
 }

@@ -72,6 +72,8 @@ _ERRORS = {cls.code: cls for cls in (ErrInvalidCDEF, ErrInvalidFilter, ErrInvali
 def check(status):
     if status != abi.PF_OK:
         msg = lib().pf_status_string(status).decode()
+        if status == abi.PF_ERR_DEVICE:
+            msg += ": " + lib().pf_status_detail().decode()
         raise _ERRORS.get(status, PostFilterError)(msg)
     return status
 

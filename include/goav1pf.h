@@ -221,6 +221,9 @@ typedef struct pf_ctx pf_ctx;
 /* Library identity. */
 int pf_abi_version(void);
 const char* pf_status_string(int status);
+/* The failing CUDA call behind the last PF_ERR_DEVICE of this thread
+ * (call, source line, CUDA error), or "" if none. */
+const char* pf_status_detail(void);
 
 /* Context life cycle.  One context per decoder; calls on one context are
  * serialised by the caller (the reference calls Apply once per frame on the
