@@ -165,11 +165,13 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
   int32_t* s_cost = sm.cost;
   const int tid = threadIdx.x;
   const int coeffShift = in.bd - 8;
+  // The index map is only present when CDEF filters; the copy-only pass (CDEF
+  // off, loop restoration on) reads no side information.
   const int mapOff = ur * a.index_stride + uc;
-  const bool rd = a.read[mapOff] != 0;
-  const int idx = a.index[mapOff];
+  const bool rd = a.filter && a.read[mapOff] != 0;
+  const int idx = a.filter ? a.index[mapOff] : 0;
   uint64_t word = ~0ull;
-  if (a.noskip) {
+  if (a.filter && a.noskip) {
     const uint8_t* w = a.noskip + (size_t)(ur * a.ucols + uc) * 8;
     word = 0;
 #pragma unroll
