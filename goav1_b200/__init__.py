@@ -43,6 +43,8 @@ def lib():
     L.pf_cdef_search.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame), C.c_void_p,
                                  C.POINTER(abi.pf_cdef_search_params), C.c_void_p, C.c_void_p,
                                  C.POINTER(abi.pf_cdef_search_result)]
+    L.pf_film_grain_static.argtypes = [C.POINTER(abi.pf_frame), C.POINTER(abi.pf_film_grain),
+                                       C.POINTER(abi.pf_frame), C.c_void_p]
     if L.pf_abi_version() != 1:
         raise RuntimeError("goav1_b200: ABI version mismatch")
     _lib = L

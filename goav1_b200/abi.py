@@ -218,4 +218,5 @@ EXPORTED_SYMBOLS = (
     "pf_stream",
     "pf_batch_apply",
     "pf_cdef_search",
+    "pf_film_grain_static",
 )

@@ -293,6 +293,33 @@ int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
                    uint64_t* mse_out, uint8_t* fb_index_out,
                    pf_cdef_search_result* result);
 
+/* ---- film grain with no allocation ----
+ * No counterpart in the reference; this entry point exists for callers that
+ * cannot call cudaMalloc: a presentation thread adding grain right before
+ * display, which must not stall on an allocation that can synchronise the
+ * device, or an application whose device memory is already owned by another
+ * allocator.  It writes display = ref with film grain applied, exactly as
+ * pf_frame_apply with only PF_STAGE_FILM_GRAIN does, but allocates nothing:
+ * its scratch (grain templates, block offsets, the job record) is one
+ * file-scope device array of PF_GRAIN_STATIC_SCRATCH_BYTES that every GPU
+ * loading the library holds until the process exits.
+ *   - ref and display are device frames (PF_MEM_DEVICE) of equal geometry on
+ *     the current CUDA device; fg is the frame's grain parameters.
+ *   - Frames with more than PF_GRAIN_STATIC_MAX_BLOCKS 32x32 luma blocks
+ *     (ceil(width/32) * ceil(height/32), e.g. 8192x8192) are rejected with
+ *     PF_ERR_SHORT_BUFFER before anything is queued.
+ *   - The first call on a device sets up that device (looks up the array's
+ *     device address and loads the grain tables into constant memory, a
+ *     synchronous copy); make that first call before any stream capture.
+ *   - Work is queued on `stream` (a cudaStream_t, or NULL for the legacy
+ *     default stream); the call returns without waiting for it.
+ *   - Every call shares the one array and it keeps the last call's contents;
+ *     calls whose work overlaps on the GPU race, so order them (one stream).
+ */
+#define PF_GRAIN_STATIC_SCRATCH_BYTES 131072
+#define PF_GRAIN_STATIC_MAX_BLOCKS 65536
+int pf_film_grain_static(const pf_frame* ref, const pf_film_grain* fg, const pf_frame* display, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
