@@ -105,20 +105,19 @@ __device__ __forceinline__ int adjust_strength(int strength, int32_t variance) {
 }
 
 // One sample of cdef/filter.go:79-169; c points at the centre sample in smem.
-__device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int sec, int dir, int damping,
-                                              int coeffShift) {
+// po/so: the primary tap offsets (entry dir+2) and the two secondary entries
+// (dir+4, dir) as smem offsets; the constrain shifts are precomputed.
+__device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int priShift, int sec, int secShift,
+                                              int2 po, int2 s0, int2 s1, int coeffShift) {
   const int x = c[0];
-  if (pri == 0 && sec == 0) return x;
   int sum = 0;
   int hi = x, lo = x;
   if (pri) {
-    const int t0 = ((pri >> coeffShift) & 1) ? 3 : 4;
-    const int t1 = ((pri >> coeffShift) & 1) ? 3 : 2;
-    const int sh = constrain_shift(pri, damping);
-    const int o0 = dir_off(dir + 2, 0), o1 = dir_off(dir + 2, 1);
-    const int a0 = c[o0], a1 = c[-o0], a2 = c[o1], a3 = c[-o1];
-    sum += t0 * (constrain(a0 - x, pri, sh) + constrain(a1 - x, pri, sh)) +
-           t1 * (constrain(a2 - x, pri, sh) + constrain(a3 - x, pri, sh));
+    const int odd = (pri >> coeffShift) & 1;
+    const int t0 = odd ? 3 : 4, t1 = odd ? 3 : 2;
+    const int a0 = c[po.x], a1 = c[-po.x], a2 = c[po.y], a3 = c[-po.y];
+    sum += t0 * (constrain(a0 - x, pri, priShift) + constrain(a1 - x, pri, priShift)) +
+           t1 * (constrain(a2 - x, pri, priShift) + constrain(a3 - x, pri, priShift));
     if (sec) {
       const int m = kVeryLarge - 1;
       hi = imax(imax(imax(hi, a0 & m), imax(a1 & m, a2 & m)), a3 & m);
@@ -126,15 +125,12 @@ __device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int se
     }
   }
   if (sec) {
-    const int sh = constrain_shift(sec, damping);
-    const int o0a = dir_off(dir + 4, 0), o0b = dir_off(dir + 4, 1);
-    const int o1a = dir_off(dir, 0), o1b = dir_off(dir, 1);
-    const int b0 = c[o0a], b1 = c[-o0a], b2 = c[o1a], b3 = c[-o1a];
-    const int b4 = c[o0b], b5 = c[-o0b], b6 = c[o1b], b7 = c[-o1b];
-    sum += 2 * (constrain(b0 - x, sec, sh) + constrain(b1 - x, sec, sh) + constrain(b2 - x, sec, sh) +
-                constrain(b3 - x, sec, sh)) +
-           constrain(b4 - x, sec, sh) + constrain(b5 - x, sec, sh) + constrain(b6 - x, sec, sh) +
-           constrain(b7 - x, sec, sh);
+    const int b0 = c[s0.x], b1 = c[-s0.x], b2 = c[s1.x], b3 = c[-s1.x];
+    const int b4 = c[s0.y], b5 = c[-s0.y], b6 = c[s1.y], b7 = c[-s1.y];
+    sum += 2 * (constrain(b0 - x, sec, secShift) + constrain(b1 - x, sec, secShift) +
+                constrain(b2 - x, sec, secShift) + constrain(b3 - x, sec, secShift)) +
+           constrain(b4 - x, sec, secShift) + constrain(b5 - x, sec, secShift) + constrain(b6 - x, sec, secShift) +
+           constrain(b7 - x, sec, secShift);
     if (pri) {
       const int m = kVeryLarge - 1;
       hi = imax(hi, imax(imax(imax(b0 & m, b1 & m), imax(b2 & m, b3 & m)),
@@ -151,6 +147,8 @@ struct CdefSmem {
   uint16_t in[kSH * kSW];
   int32_t cost[64 * 8];
   int32_t var[64];
+  int32_t blk[64];   // per block: filter flag << 16 | priShift << 12 | strength << 4 | dir
+  int2 ofs[12];      // direction tap offsets in smem units (cdef/filter.go:53-66)
   uint8_t dir[64];
 };
 
@@ -164,6 +162,7 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
   int32_t* s_var = sm.var;
   int32_t* s_cost = sm.cost;
   const int tid = threadIdx.x;
+  if (tid < 12) sm.ofs[tid] = make_int2(dir_off(tid, 0), dir_off(tid, 1));
   const int coeffShift = in.bd - 8;
   // The index map is only present when CDEF filters; the copy-only pass (CDEF
   // off, loop restoration on) reads no side information.
@@ -224,21 +223,34 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
       const bool colExt = srcX1 < wantX1 && srcX1 > 0 && unitX + unitW < Wa;
       const int extRowsEnd = srcY0 + (rowExt ? wantY1 - srcY0 : srcY1 - srcY0);
       const int fillW = unitW + 16, fillH = unitH + 4;
-      for (int i = tid; i < fillH * fillW; i += 256) {
-        const int r = i / fillW, c = i - r * fillW;
-        const int sy = unitY - 2 + r, sx = unitX - 8 + c;
-        int v = kVeryLarge;
-        int ry = -1, rx = -1;
-        if (sy >= srcY0 && sy < srcY1) ry = sy;
-        else if (rowExt && sy >= srcY1 && sy < wantY1) ry = srcY1 - 1;
-        if (sx >= srcX0 && sx < srcX1) {
-          rx = sx;
-        } else if (colExt && sx >= srcX1 && sx < wantX1 && sy >= srcY0 && sy < extRowsEnd) {
-          rx = srcX1 - 1;
-          if (ry < 0) ry = srcY1 - 1;
+      const int warp = tid >> 5, lane = tid & 31;
+      if (srcX0 == unitX - 8 && srcX1 == wantX1 && srcY0 == unitY - 2 && srcY1 == wantY1) {
+        // Interior unit: the whole halo is frame data.
+        for (int r = warp; r < fillH; r += 8) {
+          const T* src = row_ptr<T>(ip, unitY - 2 + r) + (unitX - 8);
+          uint16_t* dst = &s_in[r * kSW];
+          for (int c = lane; c < fillW; c += 32) dst[c] = src[c];
         }
-        if (ry >= 0 && rx >= 0) v = row_ptr<T>(ip, ry)[rx];
-        s_in[r * kSW + c] = (uint16_t)v;
+      } else {
+        for (int r = warp; r < fillH; r += 8) {
+          const int sy = unitY - 2 + r;
+          int ry = -1;
+          if (sy >= srcY0 && sy < srcY1) ry = sy;
+          else if (rowExt && sy >= srcY1 && sy < wantY1) ry = srcY1 - 1;
+          const bool extRow = colExt && sy >= srcY0 && sy < extRowsEnd;
+          const int ryExt = ry < 0 ? srcY1 - 1 : ry;
+          uint16_t* dst = &s_in[r * kSW];
+          for (int c = lane; c < fillW; c += 32) {
+            const int sx = unitX - 8 + c;
+            int v = kVeryLarge;
+            if (sx >= srcX0 && sx < srcX1) {
+              if (ry >= 0) v = row_ptr<T>(ip, ry)[sx];
+            } else if (extRow && sx >= srcX1 && sx < wantX1) {
+              v = row_ptr<T>(ip, ryExt)[srcX1 - 1];
+            }
+            dst[c] = (uint16_t)v;
+          }
+        }
       }
       __syncthreads();
       // ---- luma direction search on listed blocks (needPrimary) ----
@@ -274,25 +286,38 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
         __syncthreads();
       }
       // ---- filter ----
-      int lvl, sec;
-      lvl = packed >> 2;
-      sec = packed & 3;
+      int lvl = packed >> 2, sec = packed & 3;
       if (sec == 3) sec = 4;
       const int pri = lvl << coeffShift;
       sec <<= coeffShift;
       int damping = a.damping + coeffShift;
       if (plane != 0) damping--;
       const bool lumaAdjust = plane == 0 && (needPrimary || pri != 0);
+      // Per-block parameters once (cdef/filter.go:490-543): adjusted luma
+      // strength, direction (0 when the primary strength is zero), shift.
+      if (tid < 64) {
+        const int b = tid;
+        int pk = 0;
+        if (!directionOnly && ((listed >> b) & 1)) {
+          const int strength = lumaAdjust ? adjust_strength(pri, s_var[b]) : pri;
+          const int dir = pri != 0 ? s_dir[b] : 0;
+          pk = (1 << 16) | (constrain_shift(strength, damping) << 12) | (strength << 4) | dir;
+        }
+        sm.blk[b] = pk;
+      }
+      __syncthreads();
+      const int secShift = constrain_shift(sec, damping);
       if (tx < unitW) {
         for (int y = ty0; y < unitH; y += rowStep) {
           const int b = ((y >> bhLog2) << 3) + (tx >> bwLog2);
           const uint16_t* c = &s_in[(2 + y) * kSW + 8 + tx];
+          const int pk = sm.blk[b];
           int v = c[0];
-          if (!directionOnly && ((listed >> b) & 1)) {
-            int strength = pri;
-            if (lumaAdjust) strength = adjust_strength(pri, s_var[b]);
-            const int dir = pri != 0 ? s_dir[b] : 0;
-            v = cdef_filter_px(c, strength, sec, dir, damping, coeffShift);
+          if (pk >> 16) {
+            const int strength = (pk >> 4) & 255, dir = pk & 7;
+            if (strength | sec)
+              v = cdef_filter_px(c, strength, (pk >> 12) & 15, sec, secShift, sm.ofs[dir + 2], sm.ofs[dir + 4],
+                                 sm.ofs[dir], coeffShift);
           }
           row_ptr<T>(op, unitY + y)[unitX + tx] = (T)v;
         }

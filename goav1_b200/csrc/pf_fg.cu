@@ -158,74 +158,98 @@ __device__ __forceinline__ int blend_w(int prev, int cur, int pw, int cw, int bd
 
 // Display = reference with grain added on the cropped area of active planes;
 // every allocated sample of the display frame is written.
+// One column x of up to 4 rows y0.. of one display plane (all inside one
+// 32-row grain block row): per-block values once, then per sample.
 template <typename T>
-__device__ __forceinline__ void fg_apply_px(const DFrame& ref, const DFrame& disp, const FgArgs& a, int plane, int x,
-                                            int y) {
+__device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& disp, const FgArgs& a, int plane, int x,
+                                             int y0, int nrows) {
   const DPlane& sp = ref.pl[plane];
   const DPlane& dp = disp.pl[plane];
-  if (x >= sp.aw || y >= sp.ah) return;
-  const int s = row_ptr<T>(sp, y)[x];
-  if (!a.active[plane] || x >= sp.w || y >= sp.h) {
-    row_ptr<T>(dp, y)[x] = (T)s;
+  if (x >= sp.aw) return;
+  const int yend = imin(y0 + nrows, sp.ah);
+  if (!a.active[plane] || x >= sp.w) {
+    for (int y = y0; y < yend; y++) row_ptr<T>(dp, y)[x] = row_ptr<T>(sp, y)[x];
     return;
   }
   const int bd = ref.bd;
   const int sx = plane ? ref.ssx : 0, sy = plane ? ref.ssy : 0;
-  const int bw = 32 >> sx, bh = 32 >> sy;
-  const int row = y / bh, bcol = x / bw;
-  const int xi = x - bcol * bw, yi = y - row * bh;
+  const int bwl = 5 - sx, bhl = 5 - sy;
+  const int bw = 1 << bwl, bh = 1 << bhl;
+  const int row = y0 >> bhl, bcol = x >> bwl;
+  const int xi = x - (bcol << bwl);
   const int ovl = 2;
-  const int xStart = (a.overlap && bcol > 0) ? imin(sp.w - bcol * bw, ovl >> sx) : 0;
-  const int yStart = (a.overlap && row > 0) ? imin(sp.h - row * bh, ovl >> sy) : 0;
-  const uint8_t* offs = a.offsets;
+  const int xStart = (a.overlap && bcol > 0) ? imin(sp.w - (bcol << bwl), ovl >> sx) : 0;
+  const int yStart = (a.overlap && row > 0) ? imin(sp.h - (row << bhl), ovl >> sy) : 0;
+  const uint8_t* offs = a.offsets + row * a.off_cols + bcol;
   const int16_t* gr = a.grain[plane];
-  auto gidx = [&](int offset, int bc, int br) {
-    const int col = 3 + (ovl >> sx) * (3 + (offset >> 4)) + xi + bw * bc;
-    const int rr = 3 + (ovl >> sy) * (3 + (offset & 15)) + yi + bh * br;
-    return rr * kGW + col;
-  };
-  const int o00 = offs[row * a.off_cols + bcol];
-  int g = gr[gidx(o00, 0, 0)];
+  // Template column / row origins of the current, left, top and top-left blocks.
+  auto gcol = [&](int offset, int bc) { return 3 + (ovl >> sx) * (3 + (offset >> 4)) + xi + bw * bc; };
+  auto grow = [&](int offset, int br) { return 3 + (ovl >> sy) * (3 + (offset & 15)) + bh * br; };
+  const int o00 = offs[0];
+  const int c00 = gcol(o00, 0), r00 = grow(o00, 0);
+  const bool left = xi < xStart;
+  int c10 = 0, r10 = 0, c01 = 0, r01 = 0, c11 = 0, r11 = 0;
+  if (left) {
+    const int o10 = offs[-1];
+    c10 = gcol(o10, 1);
+    r10 = grow(o10, 0);
+  }
+  if (yStart > 0) {
+    const int o01 = offs[-a.off_cols];
+    c01 = gcol(o01, 0);
+    r01 = grow(o01, 1);
+    if (left) {
+      const int o11 = offs[-a.off_cols - 1];
+      c11 = gcol(o11, 1);
+      r11 = grow(o11, 1);
+    }
+  }
   // Horizontal blend weights: luma 27/17 then 17/27; subsampled chroma 23/22.
   const int hpw = sx ? 23 : (xi == 1 ? 17 : 27), hcw = sx ? 22 : (xi == 1 ? 27 : 17);
-  if (xi < xStart) {
-    const int o10 = offs[row * a.off_cols + bcol - 1];
-    g = blend_w(gr[gidx(o10, 1, 0)], g, hpw, hcw, bd);
-  }
-  if (yi < yStart) {
-    const int o01 = offs[(row - 1) * a.off_cols + bcol];
-    int top = gr[gidx(o01, 0, 1)];
-    if (xi < xStart) {
-      const int o11 = offs[(row - 1) * a.off_cols + bcol - 1];
-      top = blend_w(gr[gidx(o11, 1, 1)], top, hpw, hcw, bd);
-    }
-    const int vpw = sy ? 23 : (yi == 1 ? 17 : 27), vcw = sy ? 22 : (yi == 1 ? 27 : 17);
-    g = blend_w(top, g, vpw, vcw, bd);
-  }
-  int idx;
-  if (plane == 0) {
-    idx = s;
-  } else {
-    // chromaScalingIndex (apply.go:501-520) on the un-grained luma.
-    const DPlane& lp = ref.pl[0];
-    const int lx = x << sx, ly = y << sy;
-    int avg = row_ptr<T>(lp, ly)[lx];
-    if (sx && !(a.odd_luma && x == sp.w - 1)) avg = (avg + row_ptr<T>(lp, ly)[lx + 1] + 1) >> 1;
-    if (a.cfl) {
-      idx = avg;
-    } else {
-      const int combined = avg * (a.luma_mult[plane] - 128) + s * (a.mult[plane] - 128);
-      idx = iclip((combined >> 6) + ((a.offset[plane] << (bd - 8)) - (1 << bd)), 0, (1 << bd) - 1);
-    }
-  }
-  const int scale = scale_lut(a.lut[plane], idx, bd);
-  const int noise = rpow2(scale * g, a.scaling_shift);
+  const uint8_t* lut = a.lut[plane];
+  const int shift = a.scaling_shift;
   int minV = 0, maxV = (256 << (bd - 8)) - 1;
   if (a.clip_restricted) {
     minV = 16 << (bd - 8);
     maxV = (plane == 0 ? 235 : (a.matrix_identity ? 235 : 240)) << (bd - 8);
   }
-  row_ptr<T>(dp, y)[x] = (T)iclip(s + noise, minV, maxV);
+  const int yclip = imin(yend, sp.h);
+  for (int y = y0; y < yend; y++) {
+    const int s = row_ptr<T>(sp, y)[x];
+    if (y >= yclip) {
+      row_ptr<T>(dp, y)[x] = (T)s;
+      continue;
+    }
+    const int yi = y - (row << bhl);
+    int g = gr[(r00 + yi) * kGW + c00];
+    if (left) g = blend_w(gr[(r10 + yi) * kGW + c10], g, hpw, hcw, bd);
+    if (yi < yStart) {
+      int top = gr[(r01 + yi) * kGW + c01];
+      if (left) top = blend_w(gr[(r11 + yi) * kGW + c11], top, hpw, hcw, bd);
+      const int vpw = sy ? 23 : (yi == 1 ? 17 : 27), vcw = sy ? 22 : (yi == 1 ? 27 : 17);
+      g = blend_w(top, g, vpw, vcw, bd);
+    }
+    int idx;
+    if (plane == 0) {
+      idx = s;
+    } else {
+      // chromaScalingIndex (apply.go:501-520) on the un-grained luma.
+      const DPlane& lp = ref.pl[0];
+      const T* lrow = row_ptr<T>(lp, y << sy);
+      const int lx = x << sx;
+      int avg = lrow[lx];
+      if (sx && !(a.odd_luma && x == sp.w - 1)) avg = (avg + lrow[lx + 1] + 1) >> 1;
+      if (a.cfl) {
+        idx = avg;
+      } else {
+        const int combined = avg * (a.luma_mult[plane] - 128) + s * (a.mult[plane] - 128);
+        idx = iclip((combined >> 6) + ((a.offset[plane] << (bd - 8)) - (1 << bd)), 0, (1 << bd) - 1);
+      }
+    }
+    const int scale = scale_lut(lut, idx, bd);
+    const int noise = rpow2(scale * g, shift);
+    row_ptr<T>(dp, y)[x] = (T)iclip(s + noise, minV, maxV);
+  }
 }
 
 // frame/buffer.go:339-400: replicate the last visible column into the padding
@@ -274,13 +298,11 @@ __global__ void __launch_bounds__(256) k_fg_apply_batch(BatchArgs b) {
     }
     const int tx = local % J.fg_tx[plane], ty = local / J.fg_tx[plane];
     const int x = tx * 64 + (threadIdx.x & 63);
-    for (int k = 0; k < 4; k++) {
-      const int y = ty * 16 + (threadIdx.x >> 6) * 4 + k;
-      if (J.io.bd == 8)
-        fg_apply_px<uint8_t>(J.io, J.disp, J.fg, plane, x, y);
-      else
-        fg_apply_px<uint16_t>(J.io, J.disp, J.fg, plane, x, y);
-    }
+    const int y0 = ty * 16 + (threadIdx.x >> 6) * 4;
+    if (J.io.bd == 8)
+      fg_apply_col<uint8_t>(J.io, J.disp, J.fg, plane, x, y0, 4);
+    else
+      fg_apply_col<uint16_t>(J.io, J.disp, J.fg, plane, x, y0, 4);
   });
 }
 

@@ -31,8 +31,11 @@ constexpr int kWin = 70;  // 64 + 2*3
 
 struct LrSmem {
   uint16_t win[kWin * kWin];
+  uint16_t vsum[66 * kWin];  // SGR vertical box sums of the window columns
+  uint32_t vsq[66 * kWin];   // ... and of the squares
   int32_t A[66 * 66];
   int32_t B[66 * 66];
+  uint16_t x_by_xplus1[256];  // data-dependent lookup: smem, not constant memory
 };
 
 __device__ __forceinline__ int32_t rpot(int32_t v, int bits) {
@@ -49,6 +52,7 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
   uint16_t* s_win = sm.win;
   int32_t* s_A = sm.A;
   int32_t* s_B = sm.B;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ssx = plane ? src.ssx : 0, ssy = plane ? src.ssy : 0;
   const int PW = 64 >> ssx, SH = 64 >> ssy, off = 8 >> ssy;
   const int Wa = aw[plane], Ha = ah[plane];
@@ -84,22 +88,19 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
   const bool copyAbove = y0 != 0, copyBelow = y0 + nominal < Hc;
   const int kAbove = s, kBelow = s + 1;  // boundary indices of the saved lines
   const int ww = w + 6, wh = h + 6;
-  for (int i = tid; i < ww * wh; i += 256) {
-    const int r = i / ww, c = i - r * ww;
+  for (int r = warp; r < wh; r += 8) {
     const int yy = y0 - 3 + r;
-    const int xx = iclip(x0 - 3 + c, 0, Wc - 1);
-    int v;
+    const T* srow;
     if (yy < y0 && copyAbove) {
-      const int li = imax(yy - y0 + 2, 0);
-      v = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kAbove * 4 + li) * a.line_stride[plane])[xx];
+      srow = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kAbove * 4 + imax(yy - y0 + 2, 0)) * a.line_stride[plane]);
     } else if (yy >= yf1 && copyBelow) {
-      const int li = 2 + imin(yy - yf1, 1);
-      v = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kBelow * 4 + li) * a.line_stride[plane])[xx];
+      srow = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kBelow * 4 + 2 + imin(yy - yf1, 1)) * a.line_stride[plane]);
     } else {
-      v = row_ptr<T>(sp, iclip(yy, 0, Hc - 1))[xx];
+      srow = row_ptr<T>(sp, iclip(yy, 0, Hc - 1));
     }
-    s_win[r * kWin + c] = (uint16_t)v;
+    for (int c = lane; c < ww; c += 32) s_win[r * kWin + c] = (uint16_t)srow[iclip(x0 - 3 + c, 0, Wc - 1)];
   }
+  for (int i = tid; i < 256; i += 256) sm.x_by_xplus1[i] = c_x_by_xplus1[i];
   __syncthreads();
 
   // Pixels of the tile outside the cropped plane are copied through.
@@ -123,13 +124,14 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
     const int32_t limit = 1 << (bd + 1 + 7 - round0);
     const int32_t offH = 1 << (bd + 7 - 1);
     uint16_t* temp = reinterpret_cast<uint16_t*>(s_A);  // (h+6) x 64
-    for (int i = tid; i < wh * w; i += 256) {
-      const int r = i / w, c = i - r * w;
-      const uint16_t* sw = &s_win[r * kWin + c];
-      int32_t sum = ((int32_t)sw[3] << 7) + offH;
+    for (int r = warp; r < wh; r += 8) {
+      for (int c = lane; c < w; c += 32) {
+        const uint16_t* sw = &s_win[r * kWin + c];
+        int32_t sum = ((int32_t)sw[3] << 7) + offH;
 #pragma unroll
-      for (int k = 0; k < 7; k++) sum += (int32_t)sw[k] * hf[k];
-      temp[r * 64 + c] = (uint16_t)imin(imax(rpot(sum, round0), 0), limit - 1);
+        for (int k = 0; k < 7; k++) sum += (int32_t)sw[k] * hf[k];
+        temp[r * 64 + c] = (uint16_t)imin(imax(rpot(sum, round0), 0), limit - 1);
+      }
     }
     __syncthreads();
     const int32_t offV = 1 << (bd + round1 - 1);
@@ -159,28 +161,44 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
     const int sv = c_sgr_params[set][2 + pass];
     const uint32_t n = (uint32_t)((2 * r + 1) * (2 * r + 1));
     const int step = pass == 0 ? 2 : 1;  // r=2 pass computes every other row
-    // a/b for rows -1..h (step), cols -1..w, stored at [(row+1)*66 + col+1].
+    // a/b for rows -1..h (every other row for r = 2), cols -1..w, stored at
+    // [(row+1)*66 + col+1]; box sums separably: column sums, then row sums.
     const int nrows = h + 2, ncols = w + 2;
-    for (int i = tid; i < nrows * ncols; i += 256) {
-      const int rr = i / ncols, cc = i - rr * ncols;
-      const int row = rr - 1, col = cc - 1;
-      if (step == 2 && ((row + 1) & 1)) continue;  // rows -1, 1, 3, ...
-      int32_t sum = 0, sq = 0;
-      for (int dy = -r; dy <= r; dy++)
-        for (int dx = -r; dx <= r; dx++) {
-          const int32_t v = s_win[(row + 3 + dy) * kWin + col + 3 + dx];
-          sum += v;
-          sq += v * v;
+    for (int rr = warp; rr < nrows; rr += 8) {
+      if (step == 2 && (rr & 1)) continue;  // rows -1, 1, 3, ...
+      const uint16_t* wcol = &s_win[(rr + 2 - r) * kWin];
+      for (int c = lane; c < ww; c += 32) {
+        uint32_t vs = 0, vq = 0;
+        for (int dy = 0; dy <= 2 * r; dy++) {
+          const uint32_t v = wcol[dy * kWin + c];
+          vs += v;
+          vq += v * v;
         }
-      const uint32_t av = (uint32_t)rpot(sq, 2 * (bd - 8));
-      const uint32_t bv = (uint32_t)rpot(sum, bd - 8);
-      uint32_t p = 0;
-      if (av * n >= bv * bv) p = av * n - bv * bv;
-      uint32_t z = rpotu(p * (uint32_t)sv, 20);
-      if (z > 255) z = 255;
-      const int32_t A = c_x_by_xplus1[z];
-      s_A[rr * 66 + cc] = A;
-      s_B[rr * 66 + cc] = (int32_t)rpotu((uint32_t)(256 - A) * (uint32_t)sum * (uint32_t)c_one_by_x[n - 1], 12);
+        sm.vsum[rr * kWin + c] = (uint16_t)vs;
+        sm.vsq[rr * kWin + c] = vq;
+      }
+    }
+    __syncthreads();
+    for (int rr = warp; rr < nrows; rr += 8) {
+      if (step == 2 && (rr & 1)) continue;
+      const uint16_t* vsr = &sm.vsum[rr * kWin];
+      const uint32_t* vqr = &sm.vsq[rr * kWin];
+      for (int cc = lane; cc < ncols; cc += 32) {
+        int32_t sum = 0, sq = 0;
+        for (int dx = 0; dx <= 2 * r; dx++) {
+          sum += vsr[cc + 2 - r + dx];
+          sq += (int32_t)vqr[cc + 2 - r + dx];
+        }
+        const uint32_t av = (uint32_t)rpot(sq, 2 * (bd - 8));
+        const uint32_t bv = (uint32_t)rpot(sum, bd - 8);
+        uint32_t p = 0;
+        if (av * n >= bv * bv) p = av * n - bv * bv;
+        uint32_t z = rpotu(p * (uint32_t)sv, 20);
+        if (z > 255) z = 255;
+        const int32_t A = sm.x_by_xplus1[z];
+        s_A[rr * 66 + cc] = A;
+        s_B[rr * 66 + cc] = (int32_t)rpotu((uint32_t)(256 - A) * (uint32_t)sum * (uint32_t)c_one_by_x[n - 1], 12);
+      }
     }
     __syncthreads();
     if (tx < w) {
@@ -250,7 +268,8 @@ cudaError_t lr_upload_tables() {
 // tile of one plane of one frame.  Frames without restoration get the copy
 // of the CDEF output back into the frame.
 __global__ void __launch_bounds__(256) k_lr_batch(BatchArgs b) {
-  __shared__ LrSmem sm;
+  extern __shared__ __align__(16) uint8_t lr_smem_raw[];
+  LrSmem& sm = *reinterpret_cast<LrSmem*>(lr_smem_raw);
   const int* base = b.base + ST_LR * (b.n + 1);
   for_each_item(base[b.n], b.counters ? b.counters + ST_LR : nullptr, [&](int item) {
     const int fi = find_frame(base, b.n, item);
@@ -271,7 +290,13 @@ __global__ void __launch_bounds__(256) k_lr_batch(BatchArgs b) {
 
 cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
-  k_lr_batch<<<grid, 256, 0, st>>>(b);
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_lr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LrSmem));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  k_lr_batch<<<grid, 256, sizeof(LrSmem), st>>>(b);
   return cudaGetLastError();
 }
 
