@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--frames", type=int, default=N_FRAMES)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-search", action="store_true")
     return ap.parse_args()
 
 
@@ -330,6 +331,37 @@ def main():
         e2e = {"value": world * px / es / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "note": "pinned host frames, one pf_frame_apply call per frame"}
 
+    # Encoder CDEF strength search (BASELINE's second metric): 64x64 filter
+    # blocks searched per second, exhaustive level-1 search (64 luma x 64
+    # chroma strengths) plus the greedy 8-preset selection, on a 1080p 8-bit
+    # 4:2:0 source/reconstruction pair resident in HBM.
+    search = None
+    if not args.no_search:
+        from goav1_b200 import synth as _s
+
+        src, rec, sside, sigma = _s.make_search_pair(2000, 1920, 1080)
+        lf_runner = PostFilterRunner(device=local)
+        lf_runner.apply(rec.pf(), sside.side)  # deblock the reconstruction (library, host path)
+        lf_runner.close()
+        dsrc, drec = DeviceFrame(src), DeviceFrame(rec)
+        ucols, urows = (rec.width + 63) // 64, (rec.height + 63) // 64
+        ns = np.ctypeslib.as_array((C.c_uint8 * (ucols * urows * 8)).from_address(sside.side.cdef.noskip)).copy()
+        sp, rp = dsrc.pf(), drec.pf()
+        for _ in range(2):
+            runner.cdef_search(sp, rp, ns, 128, 4000.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        reps = max(3, args.steps)
+        for _ in range(reps):
+            res, _mse, _idx = runner.cdef_search(sp, rp, ns, 128, 4000.0)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / reps
+        nfb = ucols * urows
+        search = {"metric": "CDEF search blocks/s", "value": nfb / dt, "unit": "blocks/s", "ms_per_frame": dt * 1e3,
+                  "config": "1920x1080 8-bit 4:2:0, level-1 exhaustive (64 luma x 64 chroma strengths) + "
+                            "greedy preset selection, qindex 128, noise sigma %g" % sigma,
+                  "presets": int(res.strength_count)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(frames[:8], seconds=10.0)
@@ -340,7 +372,7 @@ def main():
                 "config": {"workload": CONFIG_NAME, "frames_per_rank": n, "parallelism": "frame-shard x%d" % world,
                            "l2": "inputs (%.0f MB per rank) larger than L2, and a 256 MB L2 flush between steps"
                                  % (sum(fr.nbytes() for fr, _ in frames) / 1e6)},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "cdef_search": search,
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))
     runner.close()

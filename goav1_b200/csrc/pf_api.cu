@@ -72,6 +72,7 @@ struct pf_ctx {
   DevBuf arena;              // per-frame scratch: CDEF output, LR lines, grain, offsets
   DevBuf sidebuf;            // host side information copied up
   DevBuf jobs, bases, counters;
+  DevBuf search;             // encoder CDEF search scratch
   std::vector<FrameJob> hjobs;
   std::vector<int> hbase;
   std::vector<uint8_t> hside;
@@ -335,7 +336,7 @@ extern "C" void pf_destroy(pf_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   cudaStreamSynchronize(c->side);
-  DevBuf* bufs[] = {&c->io, &c->disp, &c->arena, &c->sidebuf, &c->jobs, &c->bases, &c->counters};
+  DevBuf* bufs[] = {&c->io, &c->disp, &c->arena, &c->sidebuf, &c->jobs, &c->bases, &c->counters, &c->search};
   for (DevBuf* b : bufs) b->release();
   for (int i = 0; i < 8; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -837,16 +838,9 @@ extern "C" int pf_batch_apply(pf_ctx* c, const pf_batch_item* items, int32_t n, 
   return PF_OK;
 }
 
-extern "C" int pf_cdef_search(pf_ctx* c, const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
-                              const pf_cdef_search_params* params, uint64_t* mse_out, uint8_t* fb_index_out,
-                              pf_cdef_search_result* result) {
-  (void)c;
-  (void)source;
-  (void)recon;
-  (void)noskip;
-  (void)params;
-  (void)mse_out;
-  (void)fb_index_out;
-  (void)result;
-  return PF_ERR_UNSUPPORTED;
+// Scratch and stream of a context for the encoder search (pf_search.cu).
+void* pf_internal_search_scratch(pf_ctx* c, size_t bytes) {
+  if (c->search.ensure(bytes) != cudaSuccess) return nullptr;
+  return c->search.p;
 }
+void* pf_internal_stream(pf_ctx* c) { return (void*)c->stream; }

@@ -16,132 +16,9 @@
 // boundary that falls inside the unit (tile/restoration_boundary.go:192-255):
 // the boundary-line save is fused into the CDEF pass instead of a separate
 // frame sweep.
-#include "pf_common.cuh"
+#include "pf_cdef_dev.cuh"
 
 namespace pf {
-
-constexpr int kVeryLarge = 0x4000;
-constexpr int kSW = 80;   // smem row stride (64 + 2*8)
-constexpr int kSH = 68;   // smem rows (64 + 2*2)
-
-// (dy, dx) of the two taps of each CDEF direction entry, cdef/filter.go:53-66.
-__constant__ int8_t c_cdef_dir[12][2][2] = {
-    {{1, 0}, {2, 0}},   {{1, 0}, {2, -1}}, {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}},
-    {{0, 1}, {0, 2}},   {{0, 1}, {1, 2}},  {{1, 1}, {2, 2}},   {{1, 0}, {2, 1}},
-    {{1, 0}, {2, 0}},   {{1, 0}, {2, -1}}, {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}},
-};
-
-__device__ __forceinline__ int dir_off(int e, int k) { return c_cdef_dir[e][k][0] * kSW + c_cdef_dir[e][k][1]; }
-
-// Direction cost of direction D over one 8x8 block (cdef/direction.go:37-79
-// partial sums, :469-501 cost).  blk points at the block's top-left in smem.
-template <int D>
-__device__ __forceinline__ int32_t dir_cost(const uint16_t* blk, int shift) {
-  int32_t p[15];
-#pragma unroll
-  for (int k = 0; k < 15; k++) p[k] = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int32_t x = (int32_t)(blk[i * kSW + j] >> shift) - 128;
-      if (D == 0) p[i + j] += x;
-      if (D == 1) p[i + (j >> 1)] += x;
-      if (D == 2) p[i] += x;
-      if (D == 3) p[3 + i - (j >> 1)] += x;
-      if (D == 4) p[7 + i - j] += x;
-      if (D == 5) p[3 - (i >> 1) + j] += x;
-      if (D == 6) p[j] += x;
-      if (D == 7) p[(i >> 1) + j] += x;
-    }
-  }
-  if (D == 2 || D == 6) {
-    int32_t s = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) s += p[i] * p[i];
-    return s * 105;
-  }
-  if (D == 0 || D == 4) {
-    const int32_t div[8] = {840, 420, 280, 210, 168, 140, 120, 105};
-    int32_t s = 0;
-#pragma unroll
-    for (int i = 0; i < 7; i++) s += (p[i] * p[i] + p[14 - i] * p[14 - i]) * div[i];
-    return s + p[7] * p[7] * 105;
-  }
-  return (p[3] * p[3] + p[4] * p[4] + p[5] * p[5] + p[6] * p[6] + p[7] * p[7]) * 105 +
-         (p[0] * p[0] + p[10] * p[10]) * 420 + (p[1] * p[1] + p[9] * p[9]) * 210 +
-         (p[2] * p[2] + p[8] * p[8]) * 140;
-}
-
-__device__ __forceinline__ int32_t dir_cost_any(int d, const uint16_t* blk, int shift) {
-  switch (d) {
-    case 0: return dir_cost<0>(blk, shift);
-    case 1: return dir_cost<1>(blk, shift);
-    case 2: return dir_cost<2>(blk, shift);
-    case 3: return dir_cost<3>(blk, shift);
-    case 4: return dir_cost<4>(blk, shift);
-    case 5: return dir_cost<5>(blk, shift);
-    case 6: return dir_cost<6>(blk, shift);
-    default: return dir_cost<7>(blk, shift);
-  }
-}
-
-__device__ __forceinline__ int constrain(int diff, int threshold, int shift) {
-  const int a = abs(diff);
-  const int l = imin(imax(threshold - (a >> shift), 0), a);
-  return diff < 0 ? -l : l;
-}
-
-__device__ __forceinline__ int constrain_shift(int threshold, int damping) {
-  if (threshold == 0) return 0;
-  return imax(damping - (31 - __clz(threshold)), 0);
-}
-
-__device__ __forceinline__ int adjust_strength(int strength, int32_t variance) {
-  if (variance == 0) return 0;
-  const int32_t v = variance >> 6;
-  const int i = v != 0 ? imin(31 - __clz(v), 12) : 0;
-  return (strength * (4 + i) + 8) >> 4;
-}
-
-// One sample of cdef/filter.go:79-169; c points at the centre sample in smem.
-// po/so: the primary tap offsets (entry dir+2) and the two secondary entries
-// (dir+4, dir) as smem offsets; the constrain shifts are precomputed.
-__device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int priShift, int sec, int secShift,
-                                              int2 po, int2 s0, int2 s1, int coeffShift) {
-  const int x = c[0];
-  int sum = 0;
-  int hi = x, lo = x;
-  if (pri) {
-    const int odd = (pri >> coeffShift) & 1;
-    const int t0 = odd ? 3 : 4, t1 = odd ? 3 : 2;
-    const int a0 = c[po.x], a1 = c[-po.x], a2 = c[po.y], a3 = c[-po.y];
-    sum += t0 * (constrain(a0 - x, pri, priShift) + constrain(a1 - x, pri, priShift)) +
-           t1 * (constrain(a2 - x, pri, priShift) + constrain(a3 - x, pri, priShift));
-    if (sec) {
-      const int m = kVeryLarge - 1;
-      hi = imax(imax(imax(hi, a0 & m), imax(a1 & m, a2 & m)), a3 & m);
-      lo = imin(imin(imin(lo, a0), imin(a1, a2)), a3);
-    }
-  }
-  if (sec) {
-    const int b0 = c[s0.x], b1 = c[-s0.x], b2 = c[s1.x], b3 = c[-s1.x];
-    const int b4 = c[s0.y], b5 = c[-s0.y], b6 = c[s1.y], b7 = c[-s1.y];
-    sum += 2 * (constrain(b0 - x, sec, secShift) + constrain(b1 - x, sec, secShift) +
-                constrain(b2 - x, sec, secShift) + constrain(b3 - x, sec, secShift)) +
-           constrain(b4 - x, sec, secShift) + constrain(b5 - x, sec, secShift) + constrain(b6 - x, sec, secShift) +
-           constrain(b7 - x, sec, secShift);
-    if (pri) {
-      const int m = kVeryLarge - 1;
-      hi = imax(hi, imax(imax(imax(b0 & m, b1 & m), imax(b2 & m, b3 & m)),
-                         imax(imax(b4 & m, b5 & m), imax(b6 & m, b7 & m))));
-      lo = imin(lo, imin(imin(imin(b0, b1), imin(b2, b3)), imin(imin(b4, b5), imin(b6, b7))));
-    }
-  }
-  int y = x + ((8 + sum - (sum < 0)) >> 4);
-  if (pri && sec) y = imin(imax(y, lo), hi);
-  return y;
-}
 
 struct CdefSmem {
   uint16_t in[kSH * kSW];
@@ -224,7 +101,8 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
       const int extRowsEnd = srcY0 + (rowExt ? wantY1 - srcY0 : srcY1 - srcY0);
       const int fillW = unitW + 16, fillH = unitH + 4;
       const int warp = tid >> 5, lane = tid & 31;
-      if (srcX0 == unitX - 8 && srcX1 == wantX1 && srcY0 == unitY - 2 && srcY1 == wantY1) {
+      const bool interior = srcX0 == unitX - 8 && srcX1 == wantX1 && srcY0 == unitY - 2 && srcY1 == wantY1;
+      if (interior) {
         // Interior unit: the whole halo is frame data.
         for (int r = warp; r < fillH; r += 8) {
           const T* src = row_ptr<T>(ip, unitY - 2 + r) + (unitX - 8);
@@ -315,9 +193,14 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
           int v = c[0];
           if (pk >> 16) {
             const int strength = (pk >> 4) & 255, dir = pk & 7;
-            if (strength | sec)
-              v = cdef_filter_px(c, strength, (pk >> 12) & 15, sec, secShift, sm.ofs[dir + 2], sm.ofs[dir + 4],
-                                 sm.ofs[dir], coeffShift);
+            if (strength | sec) {
+              if (interior)  // no VeryLarge sentinel anywhere in the halo
+                v = cdef_filter_px<false>(c, strength, (pk >> 12) & 15, sec, secShift, sm.ofs[dir + 2],
+                                          sm.ofs[dir + 4], sm.ofs[dir], coeffShift);
+              else
+                v = cdef_filter_px<true>(c, strength, (pk >> 12) & 15, sec, secShift, sm.ofs[dir + 2],
+                                         sm.ofs[dir + 4], sm.ofs[dir], coeffShift);
+            }
           }
           row_ptr<T>(op, unitY + y)[unitX + tx] = (T)v;
         }

@@ -31,9 +31,8 @@ constexpr int kWin = 70;  // 64 + 2*3
 
 struct LrSmem {
   uint16_t win[kWin * kWin];
-  uint16_t vsum[66 * kWin];  // SGR vertical box sums of the window columns
-  uint32_t vsq[66 * kWin];   // ... and of the squares
-  int32_t A[66 * 66];
+  int32_t flt0[64 * 64];     // SGR radius-2 filter output between the passes (Wiener: row-pass temp)
+  uint16_t A[66 * 66];       // SGR a (<= 256)
   int32_t B[66 * 66];
   uint16_t x_by_xplus1[256];  // data-dependent lookup: smem, not constant memory
 };
@@ -50,7 +49,7 @@ template <typename T>
 __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, const int* aw, const int* ah,
                         int enabled, int plane, int j, int s, LrSmem& sm) {
   uint16_t* s_win = sm.win;
-  int32_t* s_A = sm.A;
+  uint16_t* s_A = sm.A;
   int32_t* s_B = sm.B;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ssx = plane ? src.ssx : 0, ssy = plane ? src.ssy : 0;
@@ -123,7 +122,7 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
     const int vf[7] = {vv0, vv1, vv2, -2 * (vv0 + vv1 + vv2), vv2, vv1, vv0};
     const int32_t limit = 1 << (bd + 1 + 7 - round0);
     const int32_t offH = 1 << (bd + 7 - 1);
-    uint16_t* temp = reinterpret_cast<uint16_t*>(s_A);  // (h+6) x 64
+    uint16_t* temp = reinterpret_cast<uint16_t*>(sm.flt0);  // (h+6) x 64
     for (int r = warp; r < wh; r += 8) {
       for (int c = lane; c < w; c += 32) {
         const uint16_t* sw = &s_win[r * kWin + c];
@@ -149,88 +148,7 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
   // ---- SGRproj (restoration/selfguided.go:132-359) ----
   const int set = u->sgr_set;
   const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][1];
-  int32_t flt0[16], flt1[16];
-#pragma unroll
-  for (int k = 0; k < 16; k++) {
-    flt0[k] = 0;
-    flt1[k] = 0;
-  }
-  for (int pass = 0; pass < 2; pass++) {
-    const int r = pass == 0 ? r0 : r1;
-    if (r == 0) continue;
-    const int sv = c_sgr_params[set][2 + pass];
-    const uint32_t n = (uint32_t)((2 * r + 1) * (2 * r + 1));
-    const int step = pass == 0 ? 2 : 1;  // r=2 pass computes every other row
-    // a/b for rows -1..h (every other row for r = 2), cols -1..w, stored at
-    // [(row+1)*66 + col+1]; box sums separably: column sums, then row sums.
-    const int nrows = h + 2, ncols = w + 2;
-    for (int rr = warp; rr < nrows; rr += 8) {
-      if (step == 2 && (rr & 1)) continue;  // rows -1, 1, 3, ...
-      const uint16_t* wcol = &s_win[(rr + 2 - r) * kWin];
-      for (int c = lane; c < ww; c += 32) {
-        uint32_t vs = 0, vq = 0;
-        for (int dy = 0; dy <= 2 * r; dy++) {
-          const uint32_t v = wcol[dy * kWin + c];
-          vs += v;
-          vq += v * v;
-        }
-        sm.vsum[rr * kWin + c] = (uint16_t)vs;
-        sm.vsq[rr * kWin + c] = vq;
-      }
-    }
-    __syncthreads();
-    for (int rr = warp; rr < nrows; rr += 8) {
-      if (step == 2 && (rr & 1)) continue;
-      const uint16_t* vsr = &sm.vsum[rr * kWin];
-      const uint32_t* vqr = &sm.vsq[rr * kWin];
-      for (int cc = lane; cc < ncols; cc += 32) {
-        int32_t sum = 0, sq = 0;
-        for (int dx = 0; dx <= 2 * r; dx++) {
-          sum += vsr[cc + 2 - r + dx];
-          sq += (int32_t)vqr[cc + 2 - r + dx];
-        }
-        const uint32_t av = (uint32_t)rpot(sq, 2 * (bd - 8));
-        const uint32_t bv = (uint32_t)rpot(sum, bd - 8);
-        uint32_t p = 0;
-        if (av * n >= bv * bv) p = av * n - bv * bv;
-        uint32_t z = rpotu(p * (uint32_t)sv, 20);
-        if (z > 255) z = 255;
-        const int32_t A = sm.x_by_xplus1[z];
-        s_A[rr * 66 + cc] = A;
-        s_B[rr * 66 + cc] = (int32_t)rpotu((uint32_t)(256 - A) * (uint32_t)sum * (uint32_t)c_one_by_x[n - 1], 12);
-      }
-    }
-    __syncthreads();
-    if (tx < w) {
-#pragma unroll
-      for (int k = 0; k < 16; k++) {
-        const int y = ty0 + k * rowStep;
-        if (y >= h) break;
-        const int32_t* A = &s_A[(y + 1) * 66 + tx + 1];
-        const int32_t* B = &s_B[(y + 1) * 66 + tx + 1];
-        const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
-        int32_t av, bv, shift;
-        if (pass == 0) {
-          if ((y & 1) == 0) {
-            av = (A[-66] + A[66]) * 6 + (A[-67] + A[-65] + A[65] + A[67]) * 5;
-            bv = (B[-66] + B[66]) * 6 + (B[-67] + B[-65] + B[65] + B[67]) * 5;
-            shift = 9;
-          } else {
-            av = A[0] * 6 + (A[-1] + A[1]) * 5;
-            bv = B[0] * 6 + (B[-1] + B[1]) * 5;
-            shift = 8;
-          }
-          flt0[k] = rpot(av * dg + bv, shift);
-        } else {
-          av = (A[0] + A[-1] + A[1] + A[-66] + A[66]) * 4 + (A[-67] + A[65] + A[-65] + A[67]) * 3;
-          bv = (B[0] + B[-1] + B[1] + B[-66] + B[66]) * 4 + (B[-67] + B[65] + B[-65] + B[67]) * 3;
-          flt1[k] = rpot(av * dg + bv, 9);
-        }
-      }
-    }
-    __syncthreads();
-  }
-  // restoration/selfguided.go:111-127 (DecodeSGRXQ), :233-247 (projection).
+  // restoration/selfguided.go:111-127 (DecodeSGRXQ).
   int xq0, xq1;
   if (r0 == 0) {
     xq0 = 0;
@@ -242,15 +160,104 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
     xq0 = u->sgr_xqd[0];
     xq1 = 128 - xq0 - u->sgr_xqd[1];
   }
-  if (tx < w) {
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-      const int y = ty0 + k * rowStep;
-      if (y >= h) break;
+  int32_t* flt0 = sm.flt0;  // [y * 64 + x]
+  if (r0 == 0)
+    for (int y = warp; y < h; y += 8)
+      for (int x = lane; x < w; x += 32) flt0[y * 64 + x] = 0;
+  const int nrows = h + 2, ncols = w + 2;
+  for (int pass = 0; pass < 2; pass++) {
+    const int r = pass == 0 ? r0 : r1;
+    if (r == 0) continue;
+    const int sv = c_sgr_params[set][2 + pass];
+    const uint32_t n = (uint32_t)((2 * r + 1) * (2 * r + 1));
+    const int step = pass == 0 ? 2 : 1;  // the r = 2 pass computes rows -1, 1, 3, ...
+    // a/b for rows -1..h and cols -1..w at [(row+1)*66 + col+1].  Box sums:
+    // each lane slides a (2r+1)-row column sum down its window column; the
+    // (2r+1)-wide row sum comes from the neighbouring lanes by shuffles, so
+    // a warp yields 32-2r output columns per row.
+    const int outPer = 32 - 2 * r;
+    const int nch = (ncols + outPer - 1) / outPer;
+    const int nseg = (nrows + 15) / 16;
+    for (int item = warp; item < nch * nseg; item += 8) {
+      const int q = item % nch, seg = item / nch;
+      const int cc = q * outPer + lane - r;   // output column of this lane
+      const int wc = cc + 2;                  // its window column (centre)
+      const bool colIn = wc >= 0 && wc < ww;
+      const int rs = seg * 16, re = imin(rs + 16, nrows);
+      int rr = rs + (step == 2 ? (rs & 1) : 0);
+      uint32_t vs = 0, vq = 0;
+      if (colIn && rr < re)
+        for (int dy = -r; dy <= r; dy++) {
+          const uint32_t v = s_win[(rr + 2 + dy) * kWin + wc];
+          vs += v;
+          vq += v * v;
+        }
+      for (; rr < re; rr += step) {
+        uint32_t bs = 0, bq = 0;
+        for (int dx = -r; dx <= r; dx++) {
+          bs += __shfl_sync(0xffffffffu, vs, imin(imax(lane + dx, 0), 31));
+          bq += __shfl_sync(0xffffffffu, vq, imin(imax(lane + dx, 0), 31));
+        }
+        if (lane >= r && lane < 32 - r && cc < ncols) {
+          const int32_t sum = (int32_t)bs, sq = (int32_t)bq;
+          const uint32_t av = (uint32_t)rpot(sq, 2 * (bd - 8));
+          const uint32_t bv = (uint32_t)rpot(sum, bd - 8);
+          uint32_t p = 0;
+          if (av * n >= bv * bv) p = av * n - bv * bv;
+          uint32_t z = rpotu(p * (uint32_t)sv, 20);
+          if (z > 255) z = 255;
+          const int32_t A = sm.x_by_xplus1[z];
+          s_A[rr * 66 + cc] = (uint16_t)A;
+          s_B[rr * 66 + cc] = (int32_t)rpotu((uint32_t)(256 - A) * (uint32_t)sum * (uint32_t)c_one_by_x[n - 1], 12);
+        }
+        // Slide the column sums down to the next computed row.
+        if (colIn && rr + step < re) {
+          for (int k = 0; k < step; k++) {
+            const uint32_t vin = s_win[(rr + 2 + r + 1 + k) * kWin + wc];
+            const uint32_t vout = s_win[(rr + 2 - r + k) * kWin + wc];
+            vs += vin - vout;
+            vq += vin * vin - vout * vout;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (tx < w) {
+      for (int y = ty0; y < h; y += rowStep) {
+        const uint16_t* A = &s_A[(y + 1) * 66 + tx + 1];
+        const int32_t* B = &s_B[(y + 1) * 66 + tx + 1];
+        const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
+        if (pass == 0) {
+          int32_t av, bv, shift;
+          if ((y & 1) == 0) {
+            av = (A[-66] + A[66]) * 6 + (A[-67] + A[-65] + A[65] + A[67]) * 5;
+            bv = (B[-66] + B[66]) * 6 + (B[-67] + B[-65] + B[65] + B[67]) * 5;
+            shift = 9;
+          } else {
+            av = A[0] * 6 + (A[-1] + A[1]) * 5;
+            bv = B[0] * 6 + (B[-1] + B[1]) * 5;
+            shift = 8;
+          }
+          flt0[y * 64 + tx] = rpot(av * dg + bv, shift);
+        } else {
+          // restoration/selfguided.go:233-247: projection with the int16 wrap.
+          const int32_t av = (A[0] + A[-1] + A[1] + A[-66] + A[66]) * 4 + (A[-67] + A[65] + A[-65] + A[67]) * 3;
+          const int32_t bv = (B[0] + B[-1] + B[1] + B[-66] + B[66]) * 4 + (B[-67] + B[65] + B[-65] + B[67]) * 3;
+          const int32_t f1 = rpot(av * dg + bv, 9);
+          const int32_t uu = dg << 4;
+          const int32_t v = (uu << 7) + xq0 * (flt0[y * 64 + tx] - uu) + xq1 * (f1 - uu);
+          const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
+          row_ptr<T>(dp, y0 + y)[x0 + tx] = (T)imin(imax(wv, 0), maxv);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (r1 == 0 && tx < w) {
+    // Only the radius-2 filter: project with xq1 = 0.
+    for (int y = ty0; y < h; y += rowStep) {
       const int32_t uu = (int32_t)s_win[(y + 3) * kWin + tx + 3] << 4;
-      int32_t v = uu << 7;
-      v += xq0 * (flt0[k] - uu);
-      v += xq1 * (flt1[k] - uu);
+      const int32_t v = (uu << 7) + xq0 * (flt0[y * 64 + tx] - uu);
       const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
       row_ptr<T>(dp, y0 + y)[x0 + tx] = (T)imin(imax(wv, 0), maxv);
     }
@@ -267,7 +274,7 @@ cudaError_t lr_upload_tables() {
 // Batched restoration: each work item is one (processing column, stripe)
 // tile of one plane of one frame.  Frames without restoration get the copy
 // of the CDEF output back into the frame.
-__global__ void __launch_bounds__(256) k_lr_batch(BatchArgs b) {
+__global__ void __launch_bounds__(256, 4) k_lr_batch(BatchArgs b) {
   extern __shared__ __align__(16) uint8_t lr_smem_raw[];
   LrSmem& sm = *reinterpret_cast<LrSmem*>(lr_smem_raw);
   const int* base = b.base + ST_LR * (b.n + 1);

@@ -115,6 +115,22 @@ class PostFilterRunner:
         check(lib().pf_batch_apply(self._h, arr, len(items), C.byref(self.stats)))
         return self.stats
 
+    def cdef_search(self, source, recon, noskip, qindex, lam, max_presets=8, damping=0):
+        """Encoder CDEF strength search (cdefSearcher.search + finish,
+        internal/av1/encoder/cdef_search.go:580-945) on 8-bit 4:2:0 frames.
+        Returns (pf_cdef_search_result, mse uint64[2, nfb, 64], fb_index uint8[nfb])."""
+        w, h = recon.width, recon.height
+        mi_cols, mi_rows = ((w + 7) >> 3) << 1, ((h + 7) >> 3) << 1
+        nfb = ((mi_cols + 15) // 16) * ((mi_rows + 15) // 16)
+        mse = np.zeros((2, nfb, 64), np.uint64)
+        idx = np.zeros(nfb, np.uint8)
+        res = abi.pf_cdef_search_result()
+        prm = abi.pf_cdef_search_params(qindex=qindex, damping=damping, max_presets=max_presets, lam=lam)
+        ns = noskip.ctypes.data if noskip is not None else None
+        check(lib().pf_cdef_search(self._h, C.byref(source), C.byref(recon), ns, C.byref(prm), mse.ctypes.data,
+                                   idx.ctypes.data, C.byref(res)))
+        return res, mse, idx
+
     def post_filter_output(self):
         """(display frame, True) after a grain-applying apply(), else (None, False)."""
         return (self._display, self._display is not None)

@@ -452,3 +452,20 @@ def make_frame(config, seed, frame_index=0, texture=None, width=None, height=Non
 
     si = SideInfo(side=side, keep=keep, blocks=dict(blocks=blocks, skip=skip))
     return fr, si
+
+
+def make_search_pair(seed, width=1920, height=1080, sigma=None):
+    """CDEF-search workload (8-bit 4:2:0): the source is the cosine-gradient
+    texture without noise; the reconstruction adds per-8x8 DC offsets in
+    +/-12 and Gaussian noise with sigma drawn from {2, 4, 8}.  Returns
+    (source, recon, side) where side is config-1 style side information for
+    the same frame (its loop-filter part deblocks the reconstruction and its
+    noskip words drive the search's block lists)."""
+    rng = np.random.default_rng([seed, 0x5EA2C4])
+    src = HostFrame.alloc(width, height, 8)
+    params = gen_content(rng, src, 0.0, 0)
+    rec = HostFrame.alloc(width, height, 8)
+    sig = float(sigma if sigma is not None else rng.choice([2.0, 4.0, 8.0]))
+    gen_content(rng, rec, sig, 12, params=params)
+    _, side = make_frame(1, seed, width=width, height=height, stages=abi.PF_STAGE_LOOP_FILTER)
+    return src, rec, side, sig

@@ -51,7 +51,6 @@ def lib():
         _lib.oracle_sgr.restype = None
         _lib.oracle_cdef_adjust_strength.argtypes = [C.c_int, C.c_int32]
         _lib.oracle_cdef_search.argtypes = [C.c_void_p] * 7
-        _lib.oracle_cdef_unit_sse.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_int] * 5 + [C.c_void_p]
     return _lib
 
 

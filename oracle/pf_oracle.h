@@ -70,11 +70,6 @@ int oracle_cdef_search(const pf_frame* source, const pf_frame* recon, const uint
                        const pf_cdef_search_params* params, uint64_t* mse_out,
                        uint8_t* fb_index_out, pf_cdef_search_result* result);
 
-/* Per-unit SSE for one strength (the search's inner trial). */
-int oracle_cdef_unit_sse(const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
-                         int damping, int plane, int unit_row, int unit_col,
-                         int packed_strength, uint64_t* sse);
-
 #ifdef __cplusplus
 }
 #endif

@@ -94,3 +94,14 @@ def test_runner_without_device_raises():
 
     with pytest.raises(postfilter.ErrNoDevice):
         postfilter.PostFilterRunner()
+
+
+def test_library_has_no_undefined_project_symbols():
+    """Every pf:: function the library calls is defined in it (a missing one
+    only shows up when the library is loaded)."""
+    import subprocess
+
+    import goav1_b200
+
+    out = subprocess.run(["nm", "-D", "--undefined-only", goav1_b200.LIB_PATH], capture_output=True, text=True).stdout
+    assert "_ZN2pf" not in out, out
