@@ -95,6 +95,7 @@ __device__ int32_t dir_cost8_any(int d, const uint8_t* blk, int64_t stride) {
 __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   __shared__ uint16_t s_in[kSH * kSW];
   __shared__ uint8_t s_src[64 * 64];
+  __shared__ uint8_t s_rec[64 * 64];  // the reconstruction itself (unfiltered trials measure it)
   __shared__ int32_t s_cost[64 * 8];
   __shared__ uint8_t s_dir[64];
   __shared__ int8_t s_ai[64];   // adjustStrength index, -1 for zero variance
@@ -150,7 +151,10 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
       }
     }
     for (int r = warp; r < h; r += 8)
-      for (int c = lane; c < w; c += 32) s_src[r * 64 + c] = row_ptr<uint8_t>(sp, y0 + r)[x0 + c];
+      for (int c = lane; c < w; c += 32) {
+        s_src[r * 64 + c] = row_ptr<uint8_t>(sp, y0 + r)[x0 + c];
+        s_rec[r * 64 + c] = row_ptr<uint8_t>(rp, y0 + r)[x0 + c];
+      }
     if (pli == 0) {
       // Luma directions of the listed blocks, from the reconstruction.
       for (int wi = tid; wi < 64 * 8; wi += 256) {
@@ -199,11 +203,16 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
             strength = ai < 0 ? 0 : (pri * (4 + ai) + 8) >> 4;
           }
           const uint16_t* c = &s_in[(2 + yy) * kSW + 8 + xx];
-          int v = c[0];
+          // An unfiltered block keeps the reconstruction (cdefDist8 against
+          // recon / the copyFB trial buffer), which below the crop is not the
+          // VeryLarge-padded input.
+          int v = s_rec[yy * 64 + xx];
           if (strength | sec) {
             const int dir = pri != 0 ? s_dir[b] : 0;
-            v = cdef_filter_px(c, strength, constrain_shift(strength, dmp), sec, secShift, s_ofs[dir + 2],
-                               s_ofs[dir + 4], s_ofs[dir], 0);
+            // The 8-bit trial buffer keeps the low byte (cdef/filter_u8.go:151),
+            // which matters only below the crop where the centre is VeryLarge.
+            v = (uint8_t)cdef_filter_px(c, strength, constrain_shift(strength, dmp), sec, secShift, s_ofs[dir + 2],
+                                        s_ofs[dir + 4], s_ofs[dir], 0);
           }
           const int e = (int)s_src[yy * 64 + xx] - v;
           sse += (uint32_t)(e * e);
@@ -549,9 +558,11 @@ extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_fram
       rS[p] = recon->plane[p].stride;
     }
   }
-  const uint8_t* ns = noskip;
-  if (noskip && host) {
-    if (e == cudaSuccess) e = cudaMemcpyAsync(base + oNs, noskip, (size_t)nfb * 8, cudaMemcpyHostToDevice, st);
+  // The noskip words may live in host or device memory: copy them into the
+  // scratch either way (cudaMemcpyDefault resolves the direction).
+  const uint8_t* ns = nullptr;
+  if (noskip) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + oNs, noskip, (size_t)nfb * 8, cudaMemcpyDefault, st);
     ns = base + oNs;
   }
   if (e != cudaSuccess) return PF_ERR_DEVICE;

@@ -287,7 +287,13 @@ typedef struct pf_cdef_search_result {
  * `recon` (luma, and U+V summed for chroma) is written to mse_out
  * (uint64, [2][n_fb][64]); then the greedy preset selection picks the frame
  * presets and fb_index_out gets each unit's preset.  recon is the deblocked
- * frame; noskip as in pf_cdef. */
+ * frame; source and recon are both host or both device frames.  noskip is
+ * as in pf_cdef, in host or device memory (it is copied), or NULL to search
+ * every 8x8 block.  Entry i of the 64 trials is the packed strength of the
+ * reference's level-1 list: 4*i for i < 16, then 4*(k/3) + k%3 + 1 for
+ * k = i - 16.  Only 8-bit 4:2:0 frames are searched (goav1's
+ * SourceFrame420); others get PF_ERR_UNSUPPORTED.  mse_out and fb_index_out
+ * are host buffers (either may be NULL). */
 int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
                    const uint8_t* noskip, const pf_cdef_search_params* params,
                    uint64_t* mse_out, uint8_t* fb_index_out,

@@ -290,8 +290,8 @@ extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, cons
                 int v;
                 if (strength == 0 && sec == 0)
                   v = rp.at(x0 + xx, y0 + yy);
-                else
-                  v = filter_px(in.data(), origin + yy * kBS + xx, strength, sec, d, dmp);
+                else  // the 8-bit trial buffer stores byte(...) (cdef/filter_u8.go:151)
+                  v = (uint8_t)filter_px(in.data(), origin + yy * kBS + xx, strength, sec, d, dmp);
                 const int e = sp.at(x0 + xx, y0 + yy) - v;
                 sse += (uint64_t)(e * e);
               }
