@@ -43,7 +43,7 @@ N_FRAMES = 60
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=N_FRAMES)
@@ -93,9 +93,12 @@ def side_bytes(si, fr):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons, sampled every 50 ms from before the
+    warm-up to after the timed region; the summary keeps the samples whose
+    timestamps fall inside the timed window (all load samples when the window
+    is shorter than the sampling period)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -103,42 +106,59 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+        self.window = None
 
     def start(self):
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            t_end = time.time() + 5.0
+            while time.time() < t_end and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
+
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
 
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.1)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.fh.close()
-        sm, smax, reasons = [], [], set()
+        import datetime
+
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(f[2]), float(f[3]),
+                             [nm for nm, v in zip(names, f[6:10]) if v.lower().startswith("active")]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = rows
+        scope = "all samples from warm-up to the end of the timed region"
+        if self.window:
+            w = [r for r in rows if self.window[0] - 0.05 <= r[0] <= self.window[1] + 0.05]
+            if len(w) >= 3:
+                inside, scope = w, "timed region"
+        sm = [r[1] for r in inside]
+        reasons = sorted({x for r in inside for x in r[3]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(r[2] for r in inside) if inside else None,
+                "reasons": reasons, "samples": len(sm), "scope": scope}
 
 
 def cpu_baseline(frames, seconds=10.0):
@@ -237,24 +257,26 @@ def main():
     def step():
         runner.apply_batch(pf_frames)
 
+    clocks = ClockSampler(local)
+    clocks.start()
     # Warm-up.
     for _ in range(max(args.warmup, 3)):
         reset()
         step()
     torch.cuda.synchronize()
     launches_per_step = 7  # one launch per stage for the whole batch
-    clocks = ClockSampler(local)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    t_on = time.time()
     for k in range(args.steps):
         reset()
         ev[k][0].record(stream)
         step()
         ev[k][1].record(stream)
     torch.cuda.synchronize()
+    clocks.mark(t_on, time.time())
     if world > 1:
         torch.distributed.barrier()
     clk = clocks.stop()
@@ -294,8 +316,18 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = algo[stage_names[dom]] / (per_frame[dom] / 1e3) / 1e9
+    # DRAM bytes (read + write) per frame of each batched kernel from one ncu
+    # capture of a 60-frame launch (profiles/postfilter_kernels_1080p8_60frames_ncu.md),
+    # scaled to this launch's frame count; with the ALU-pipe utilisation of
+    # the same capture, the ceiling that binds.
+    ncu_per_frame = {"deblock": (221.8e6 + 123.1e6 + 206.6e6 + 54.6e6) / 60, "cdef": (188.3e6 + 167.4e6) / 60,
+                     "restoration": (206.9e6 + 156.1e6) / 60, "film_grain": (189.7e6 + 158.9e6) / 60}
+    alu_pct = {"deblock": 27.2, "cdef": 74.0, "restoration": 44.0, "film_grain": 43.0}
+    traffic = ncu_per_frame.get(stage_names[dom])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": stage_names[dom],
+                "traffic": traffic * n if traffic else None, "kernel": stage_names[dom],
+                "algorithmic_bytes_per_launch": algo[stage_names[dom]] * n, "frames_per_launch": n,
+                "int_pipe": {"alu_pipe_pct_of_peak": alu_pct.get(stage_names[dom]), "source": "ncu, same kernel, 60 frames"},
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "stage_ms_per_frame": dict(zip(stage_names, [round(float(x), 4) for x in per_frame])),
                 "chain_algorithmic_bytes_per_px": 3 * c + 0.33,

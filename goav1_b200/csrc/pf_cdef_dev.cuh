@@ -111,8 +111,8 @@ __device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int pr
            t1 * (constrain(a2 - x, pri, priShift) + constrain(a3 - x, pri, priShift));
     if (sec) {
       const int m = kMask ? kVeryLarge - 1 : 0xffff;
-      hi = imax(imax(imax(hi, a0 & m), imax(a1 & m, a2 & m)), a3 & m);
-      lo = imin(imin(imin(lo, a0), imin(a1, a2)), a3);
+      hi = __vimax3_s32(__vimax3_s32(hi, a0 & m, a1 & m), a2 & m, a3 & m);
+      lo = __vimin3_s32(__vimin3_s32(lo, a0, a1), a2, a3);
     }
   }
   if (sec) {
@@ -123,10 +123,11 @@ __device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int pr
            constrain(b4 - x, sec, secShift) + constrain(b5 - x, sec, secShift) + constrain(b6 - x, sec, secShift) +
            constrain(b7 - x, sec, secShift);
     if (pri) {
+      // 3-way DPX min/max: half the instructions of a two-operand chain.
       const int m = kMask ? kVeryLarge - 1 : 0xffff;
-      hi = imax(hi, imax(imax(imax(b0 & m, b1 & m), imax(b2 & m, b3 & m)),
-                         imax(imax(b4 & m, b5 & m), imax(b6 & m, b7 & m))));
-      lo = imin(lo, imin(imin(imin(b0, b1), imin(b2, b3)), imin(imin(b4, b5), imin(b6, b7))));
+      hi = __vimax3_s32(__vimax3_s32(hi, b0 & m, b1 & m), __vimax3_s32(b2 & m, b3 & m, b4 & m),
+                        __vimax3_s32(b5 & m, b6 & m, b7 & m));
+      lo = __vimin3_s32(__vimin3_s32(lo, b0, b1), __vimin3_s32(b2, b3, b4), __vimin3_s32(b5, b6, b7));
     }
   }
   int y = x + ((8 + sum - (sum < 0)) >> 4);

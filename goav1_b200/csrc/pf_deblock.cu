@@ -60,18 +60,32 @@ __device__ __forceinline__ void lpf_unit(T* q, int sa, int sb, int bd, int E, in
         if ((unsigned)(p6 - p0 + F) <= twoF && (unsigned)(p5 - p0 + F) <= twoF &&
             (unsigned)(p4 - p0 + F) <= twoF && (unsigned)(q4 - q0 + F) <= twoF &&
             (unsigned)(q5 - q0 + F) <= twoF && (unsigned)(q6 - q0 + F) <= twoF) {
-          q[-6 * sb] = (T)((p6 * 7 + p5 * 2 + p4 * 2 + p3 + p2 + p1 + p0 + q0 + 8) >> 4);
-          q[-5 * sb] = (T)((p6 * 5 + p5 * 2 + p4 * 2 + p3 * 2 + p2 + p1 + p0 + q0 + q1 + 8) >> 4);
-          q[-4 * sb] = (T)((p6 * 4 + p5 + p4 * 2 + p3 * 2 + p2 * 2 + p1 + p0 + q0 + q1 + q2 + 8) >> 4);
-          q[-3 * sb] = (T)((p6 * 3 + p5 + p4 + p3 * 2 + p2 * 2 + p1 * 2 + p0 + q0 + q1 + q2 + q3 + 8) >> 4);
-          q[-2 * sb] = (T)((p6 * 2 + p5 + p4 + p3 + p2 * 2 + p1 * 2 + p0 * 2 + q0 + q1 + q2 + q3 + q4 + 8) >> 4);
-          q[-sb] = (T)((p6 + p5 + p4 + p3 + p2 + p1 * 2 + p0 * 2 + q0 * 2 + q1 + q2 + q3 + q4 + q5 + 8) >> 4);
-          q[0] = (T)((p5 + p4 + p3 + p2 + p1 + p0 * 2 + q0 * 2 + q1 * 2 + q2 + q3 + q4 + q5 + q6 + 8) >> 4);
-          q[sb] = (T)((p4 + p3 + p2 + p1 + p0 + q0 * 2 + q1 * 2 + q2 * 2 + q3 + q4 + q5 + q6 * 2 + 8) >> 4);
-          q[2 * sb] = (T)((p3 + p2 + p1 + p0 + q0 + q1 * 2 + q2 * 2 + q3 * 2 + q4 + q5 + q6 * 3 + 8) >> 4);
-          q[3 * sb] = (T)((p2 + p1 + p0 + q0 + q1 + q2 * 2 + q3 * 2 + q4 * 2 + q5 + q6 * 4 + 8) >> 4);
-          q[4 * sb] = (T)((p1 + p0 + q0 + q1 + q2 + q3 * 2 + q4 * 2 + q5 * 2 + q6 * 5 + 8) >> 4);
-          q[5 * sb] = (T)((p0 + q0 + q1 + q2 + q3 + q4 * 2 + q5 * 2 + q6 * 7 + 8) >> 4);
+          // The twelve outputs as one running sum: each output's 16-weight
+          // window differs from the previous one by two samples in, two out.
+          int t = p6 * 7 + p5 * 2 + p4 * 2 + p3 + p2 + p1 + p0 + q0 + 8;
+          q[-6 * sb] = (T)(t >> 4);
+          t += p3 + q1 - 2 * p6;
+          q[-5 * sb] = (T)(t >> 4);
+          t += p2 + q2 - p6 - p5;
+          q[-4 * sb] = (T)(t >> 4);
+          t += p1 + q3 - p6 - p4;
+          q[-3 * sb] = (T)(t >> 4);
+          t += p0 + q4 - p6 - p3;
+          q[-2 * sb] = (T)(t >> 4);
+          t += q0 + q5 - p6 - p2;
+          q[-sb] = (T)(t >> 4);
+          t += q1 + q6 - p6 - p1;
+          q[0] = (T)(t >> 4);
+          t += q2 + q6 - p5 - p0;
+          q[sb] = (T)(t >> 4);
+          t += q3 + q6 - p4 - q0;
+          q[2 * sb] = (T)(t >> 4);
+          t += q4 + q6 - p3 - q1;
+          q[3 * sb] = (T)(t >> 4);
+          t += q5 + q6 - p2 - q2;
+          q[4 * sb] = (T)(t >> 4);
+          t += 2 * q6 - p1 - q3;
+          q[5 * sb] = (T)(t >> 4);
           continue;
         }
       }
@@ -176,7 +190,7 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
 
 // Batched deblocking: each work item is one 32x8 tile of edge units of one
 // plane of one frame; 256 threads, one edge unit each.
-__global__ void __launch_bounds__(256) k_deblock_batch(BatchArgs b, int dir) {
+__global__ void __launch_bounds__(256, 3) k_deblock_batch(BatchArgs b, int dir) {
   const int stage = dir == 0 ? ST_DEBLOCK_V : ST_DEBLOCK_H;
   const int* base = b.base + stage * (b.n + 1);
   for_each_item(base[b.n], b.counters ? b.counters + stage : nullptr, [&](int item) {
