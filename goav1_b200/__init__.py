@@ -45,6 +45,17 @@ def lib():
                                  C.POINTER(abi.pf_cdef_search_result)]
     L.pf_film_grain_static.argtypes = [C.POINTER(abi.pf_frame), C.POINTER(abi.pf_film_grain),
                                        C.POINTER(abi.pf_frame), C.c_void_p]
+    L.pf_cdef_features.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.c_void_p, C.c_int32, C.c_int32,
+                                   C.c_void_p]
+    L.pf_cdef_mlp_forward.argtypes = [C.c_void_p, C.POINTER(abi.pf_cdef_mlp), C.c_void_p, C.c_int32, C.c_void_p]
+    L.pf_cdef_mlp_gradients.argtypes = [C.c_void_p, C.POINTER(abi.pf_cdef_mlp), C.c_void_p, C.c_void_p, C.c_int32,
+                                        C.POINTER(C.c_float), C.POINTER(abi.pf_cdef_mlp_grads)]
+    L.pf_cdef_mlp_train.argtypes = [C.c_void_p, C.POINTER(abi.pf_cdef_mlp), C.c_void_p, C.c_void_p, C.c_int32,
+                                    C.POINTER(abi.pf_cdef_mlp_train_params), C.c_void_p]
+    L.pf_cdef_search_learned.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame), C.c_void_p,
+                                         C.POINTER(abi.pf_cdef_search_params), C.POINTER(abi.pf_cdef_mlp), C.c_float,
+                                         C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(abi.pf_cdef_search_result),
+                                         C.POINTER(abi.pf_cdef_learned_stats)]
     if L.pf_abi_version() != 1:
         raise RuntimeError("goav1_b200: ABI version mismatch")
     _lib = L

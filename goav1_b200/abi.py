@@ -205,6 +205,60 @@ class pf_cdef_search_result(C.Structure):
     ]
 
 
+PF_MLP_FEATURES = 40
+PF_MLP_HIDDEN = 64
+PF_MLP_CLASSES = 64
+PF_MLP_OUTPUTS = 2 * PF_MLP_CLASSES
+PF_MLP_PARAMS = (PF_MLP_HIDDEN * PF_MLP_FEATURES + PF_MLP_HIDDEN * PF_MLP_HIDDEN + PF_MLP_OUTPUTS * PF_MLP_HIDDEN
+                 + 2 * PF_MLP_HIDDEN + PF_MLP_OUTPUTS)
+
+
+class pf_cdef_mlp(C.Structure):
+    _fields_ = [
+        ("w1", C.c_uint16 * (PF_MLP_HIDDEN * PF_MLP_FEATURES)),
+        ("w2", C.c_uint16 * (PF_MLP_HIDDEN * PF_MLP_HIDDEN)),
+        ("w3", C.c_uint16 * (PF_MLP_OUTPUTS * PF_MLP_HIDDEN)),
+        ("b1", C.c_float * PF_MLP_HIDDEN),
+        ("b2", C.c_float * PF_MLP_HIDDEN),
+        ("b3", C.c_float * PF_MLP_OUTPUTS),
+        ("feat_shift", C.c_float * PF_MLP_FEATURES),
+        ("feat_scale", C.c_float * PF_MLP_FEATURES),
+    ]
+
+
+class pf_cdef_mlp_grads(C.Structure):
+    _fields_ = [
+        ("w1", C.c_float * (PF_MLP_HIDDEN * PF_MLP_FEATURES)),
+        ("w2", C.c_float * (PF_MLP_HIDDEN * PF_MLP_HIDDEN)),
+        ("w3", C.c_float * (PF_MLP_OUTPUTS * PF_MLP_HIDDEN)),
+        ("b1", C.c_float * PF_MLP_HIDDEN),
+        ("b2", C.c_float * PF_MLP_HIDDEN),
+        ("b3", C.c_float * PF_MLP_OUTPUTS),
+    ]
+
+
+class pf_cdef_mlp_train_params(C.Structure):
+    _fields_ = [
+        ("epochs", C.c_int32),
+        ("batch", C.c_int32),
+        ("lr", C.c_float),
+        ("beta1", C.c_float),
+        ("beta2", C.c_float),
+        ("eps", C.c_float),
+        ("weight_decay", C.c_float),
+        ("seed", C.c_uint32),
+    ]
+
+
+class pf_cdef_learned_stats(C.Structure):
+    _fields_ = [
+        ("blocks", C.c_int32),
+        ("fallback", C.c_int32),
+        ("trials_luma", C.c_int32),
+        ("trials_chroma", C.c_int32),
+    ]
+
+
 # Every symbol include/goav1pf.h declares (checked by tests/test_abi.py).
 EXPORTED_SYMBOLS = (
     "pf_abi_version",
@@ -219,4 +273,9 @@ EXPORTED_SYMBOLS = (
     "pf_batch_apply",
     "pf_cdef_search",
     "pf_film_grain_static",
+    "pf_cdef_features",
+    "pf_cdef_mlp_forward",
+    "pf_cdef_mlp_gradients",
+    "pf_cdef_mlp_train",
+    "pf_cdef_search_learned",
 )

@@ -6,91 +6,35 @@
 //   k_cdef_search   one CTA per 64x64 filter block: the noskip 8x8 list
 //                   (computeCDEFList, :410-447), the VeryLarge-padded input
 //                   (loadCDEFInput, :479-506), luma directions from the
-//                   reconstruction, then for each of the 64 trials the SSE of
+//                   reconstruction, then for each tested trial the SSE of
 //                   the filtered block against the source (searchRow,
 //                   :649-745; FilterBlocksU8SubsampledTrusted with row step 1,
-//                   cdef/filter_search.go:20-74).  Warps own trials, lanes own
-//                   pixels, the SSE is a warp reduction.
-//   k_sel_*         finish (:886-945): jointStrengthSearchDual / searchOneDual
-//                   (:780-869) for nb = 1, 2, 4, 8 as a chain of GPU steps.
-//                   sav[j][k] = sum_i max(0, best_i - m0[i][j] - m1[i][k]) is
-//                   the reference's savings form; FB chunks add their partial
-//                   sums atomically, one CTA picks the argmax.
+//                   cdef/filter_search.go:20-74).  The work is split into
+//                   (trial, 8-row group) tasks spread over the warps, so a
+//                   block that tests few trials (the learned search) still
+//                   keeps every warp busy.  An untested trial gets the
+//                   reference's untested-chroma figure (cdefDefaultMSEUV*64,
+//                   :669-672) in both planes.
+//   k_sel_greedy    finish (:886-945): jointStrengthSearchDual /
+//                   searchOneDual (:780-869) for one nb = 1 << cluster index,
+//                   all 5*nb greedy and refinement steps inside one launch.
+//                   Eight CTAs of a thread-block cluster each own a slice of
+//                   the filter blocks (SSE rows in shared memory), compute
+//                   partial savings sav[j][k] = sum_i max(0, best_i -
+//                   m0[i][j] - m1[i][k]) (the reference's form), and reduce
+//                   them through distributed shared memory.
 //   k_sel_finish    the RD choice of nb and the per-block preset index.
+#include <cooperative_groups.h>
 #include <string.h>
 
 #include <vector>
 
 #include "pf_cdef_dev.cuh"
+#include "pf_search.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace pf {
-
-struct SearchArgs {
-  DFrame src, rec;          // 8-bit 4:2:0
-  const uint8_t* noskip;    // 8 bytes per filter block, or null (all blocks)
-  int miCols, miRows, nhfb, nvfb;
-  int damping;
-  uint64_t* mse;            // [2][nfb][64]
-  uint8_t* skip;            // [nfb]
-};
-
-// Trial gi -> packed strength (level-1 lists, svtPfGI then pf+1..pf+3).
-__host__ __device__ __forceinline__ int trial_strength(int g) {
-  if (g < 16) return g * 4;
-  const int k = g - 16;
-  return (k / 3) * 4 + (k % 3) + 1;
-}
-
-// Direction cost of direction D over an 8-bit 8x8 block in global memory.
-template <int D>
-__device__ __forceinline__ int32_t dir_cost8(const uint8_t* blk, int64_t stride) {
-  int32_t p[15];
-#pragma unroll
-  for (int k = 0; k < 15; k++) p[k] = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int32_t x = (int32_t)blk[i * stride + j] - 128;
-      if (D == 0) p[i + j] += x;
-      if (D == 1) p[i + (j >> 1)] += x;
-      if (D == 2) p[i] += x;
-      if (D == 3) p[3 + i - (j >> 1)] += x;
-      if (D == 4) p[7 + i - j] += x;
-      if (D == 5) p[3 - (i >> 1) + j] += x;
-      if (D == 6) p[j] += x;
-      if (D == 7) p[(i >> 1) + j] += x;
-    }
-  }
-  if (D == 2 || D == 6) {
-    int32_t s = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) s += p[i] * p[i];
-    return s * 105;
-  }
-  if (D == 0 || D == 4) {
-    const int32_t div[8] = {840, 420, 280, 210, 168, 140, 120, 105};
-    int32_t s = 0;
-#pragma unroll
-    for (int i = 0; i < 7; i++) s += (p[i] * p[i] + p[14 - i] * p[14 - i]) * div[i];
-    return s + p[7] * p[7] * 105;
-  }
-  return (p[3] * p[3] + p[4] * p[4] + p[5] * p[5] + p[6] * p[6] + p[7] * p[7]) * 105 +
-         (p[0] * p[0] + p[10] * p[10]) * 420 + (p[1] * p[1] + p[9] * p[9]) * 210 + (p[2] * p[2] + p[8] * p[8]) * 140;
-}
-
-__device__ int32_t dir_cost8_any(int d, const uint8_t* blk, int64_t stride) {
-  switch (d) {
-    case 0: return dir_cost8<0>(blk, stride);
-    case 1: return dir_cost8<1>(blk, stride);
-    case 2: return dir_cost8<2>(blk, stride);
-    case 3: return dir_cost8<3>(blk, stride);
-    case 4: return dir_cost8<4>(blk, stride);
-    case 5: return dir_cost8<5>(blk, stride);
-    case 6: return dir_cost8<6>(blk, stride);
-    default: return dir_cost8<7>(blk, stride);
-  }
-}
 
 __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   __shared__ uint16_t s_in[kSH * kSW];
@@ -100,7 +44,9 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   __shared__ uint8_t s_dir[64];
   __shared__ int8_t s_ai[64];   // adjustStrength index, -1 for zero variance
   __shared__ int2 s_ofs[12];
-  __shared__ uint32_t s_m1[64];  // U+V SSE per trial
+  __shared__ uint32_t s_sse[2][64];  // luma; U+V
+  __shared__ uint8_t s_list[2][64];  // tested trials, ascending
+  __shared__ int s_cnt[2];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int fb = blockIdx.x;
   const int fbr = fb / a.nhfb, fbc = fb - fbr * a.nhfb;
@@ -109,18 +55,7 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   const int nfb = a.nhfb * a.nvfb;
   uint64_t* m0 = a.mse + (size_t)fb * 64;
   uint64_t* m1 = a.mse + (size_t)nfb * 64 + (size_t)fb * 64;
-  uint64_t word = ~0ull;
-  if (a.noskip) {
-    word = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) word |= (uint64_t)a.noskip[(size_t)fb * 8 + i] << (8 * i);
-  }
-  uint64_t listed = 0;
-  for (int r = 0; r < imin(a.miRows - lr, 16); r += 2)
-    for (int c = 0; c < imin(a.miCols - lc, 16); c += 2) {
-      const int b = (r >> 1) * 8 + (c >> 1);
-      listed |= word & (1ull << b);
-    }
+  const uint64_t listed = fb_listed(a, fb, lr, lc);
   if (listed == 0) {
     if (tid < 64) {
       m0[tid] = 0;
@@ -129,17 +64,30 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
     if (tid == 0) a.skip[fb] = 1;
     return;
   }
-  if (tid == 0) a.skip[fb] = 0;
+  const uint64_t mask0 = a.tmask ? a.tmask[2 * fb] : ~0ull;
+  const uint64_t mask1 = a.tmask ? a.tmask[2 * fb + 1] : ~0ull;
+  if (tid == 0) {
+    a.skip[fb] = 0;
+    int c0 = 0, c1 = 0;
+    for (int g = 0; g < 64; g++) {
+      if ((mask0 >> g) & 1) s_list[0][c0++] = (uint8_t)g;
+      if ((mask1 >> g) & 1) s_list[1][c1++] = (uint8_t)g;
+    }
+    s_cnt[0] = c0;
+    s_cnt[1] = c1;
+  }
   if (tid < 12) s_ofs[tid] = make_int2(dir_off(tid, 0), dir_off(tid, 1));
-  if (tid < 64) s_m1[tid] = 0;
+  if (tid < 128) s_sse[tid >> 6][tid & 63] = 0;
   const int damping = a.damping;
   for (int pli = 0; pli < 3; pli++) {
     const int dec = pli ? 1 : 0;
+    const int P = pli ? 1 : 0;
     const int x0 = (lc * 4) >> dec, y0 = (lr * 4) >> dec;
     const int w = (nhb * 4) >> dec, h = (nvb * 4) >> dec;
     const DPlane& rp = a.rec.pl[pli];
     const DPlane& sp = a.src.pl[pli];
     const int planeW = rp.w, planeH = rp.h;
+    __syncthreads();  // the previous plane's tasks are done with the buffers
     // loadCDEFInput: frame samples where they exist, VeryLarge elsewhere.
     for (int r = warp; r < h + 4; r += 8) {
       const int yy = y0 - 2 + r;
@@ -160,7 +108,7 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
       for (int wi = tid; wi < 64 * 8; wi += 256) {
         const int b = wi >> 3, d = wi & 7;
         if ((listed >> b) & 1)
-          s_cost[wi] = dir_cost8_any(d, row_ptr<uint8_t>(rp, y0 + (b >> 3) * 8) + x0 + (b & 7) * 8, rp.stride);
+          s_cost[wi] = dir_cost8_dev(d, row_ptr<uint8_t>(rp, y0 + (b >> 3) * 8) + x0 + (b & 7) * 8, rp.stride);
       }
       __syncthreads();
       if (tid < 64 && ((listed >> tid) & 1)) {
@@ -185,214 +133,270 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
     __syncthreads();
     const int bl = 3 - dec;
     const int dmp = pli ? damping - 1 : damping;
-    for (int t = 0; t < 8; t++) {
-      const int g = warp + 8 * t;
+    const int ngrp = (h + 7) >> 3;
+    const int ntask = s_cnt[P] * ngrp;
+    for (int task = warp; task < ntask; task += 8) {
+      const int g = s_list[P][task / ngrp];
+      const int grp = task - (task / ngrp) * ngrp;
       const int packed = trial_strength(g);
       const int pri = packed >> 2;
       int sec = packed & 3;
       if (sec == 3) sec = 4;
       const int secShift = constrain_shift(sec, dmp);
       uint32_t sse = 0;
-      for (int yy = 0; yy < h; yy++) {
-        for (int xx = lane; xx < w; xx += 32) {
-          const int b = ((yy >> bl) << 3) + (xx >> bl);
+      for (int xx = lane; xx < w; xx += 32) {
+        for (int yb = grp * 8; yb < imin(grp * 8 + 8, h); yb += 1 << bl) {
+          const int b = ((yb >> bl) << 3) + (xx >> bl);
           if (!((listed >> b) & 1)) continue;
           int strength = pri;
           if (pli == 0 && pri != 0) {
             const int ai = s_ai[b];
             strength = ai < 0 ? 0 : (pri * (4 + ai) + 8) >> 4;
           }
-          const uint16_t* c = &s_in[(2 + yy) * kSW + 8 + xx];
-          // An unfiltered block keeps the reconstruction (cdefDist8 against
-          // recon / the copyFB trial buffer), which below the crop is not the
-          // VeryLarge-padded input.
-          int v = s_rec[yy * 64 + xx];
-          if (strength | sec) {
-            const int dir = pri != 0 ? s_dir[b] : 0;
-            // The 8-bit trial buffer keeps the low byte (cdef/filter_u8.go:151),
-            // which matters only below the crop where the centre is VeryLarge.
-            v = (uint8_t)cdef_filter_px(c, strength, constrain_shift(strength, dmp), sec, secShift, s_ofs[dir + 2],
-                                        s_ofs[dir + 4], s_ofs[dir], 0);
+          const bool filt = (strength | sec) != 0;
+          const int dir = pri != 0 ? s_dir[b] : 0;
+          const int priShift = constrain_shift(strength, dmp);
+          const int2 po = s_ofs[dir + 2], q0 = s_ofs[dir + 4], q1 = s_ofs[dir];
+          for (int yy = yb; yy < yb + (1 << bl); yy++) {
+            // An unfiltered block keeps the reconstruction (cdefDist8 against
+            // recon / the copyFB trial buffer), which below the crop is not
+            // the VeryLarge-padded input.
+            int v = s_rec[yy * 64 + xx];
+            if (filt)
+              // The 8-bit trial buffer keeps the low byte (cdef/filter_u8.go:151),
+              // which matters only below the crop where the centre is VeryLarge.
+              v = (uint8_t)cdef_filter_px(&s_in[(2 + yy) * kSW + 8 + xx], strength, priShift, sec, secShift, po, q0,
+                                          q1, 0);
+            const int e = (int)s_src[yy * 64 + xx] - v;
+            sse += (uint32_t)(e * e);
           }
-          const int e = (int)s_src[yy * 64 + xx] - v;
-          sse += (uint32_t)(e * e);
         }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) sse += __shfl_xor_sync(0xffffffffu, sse, o);
-      if (lane == 0) {
-        if (pli == 0)
-          m0[g] = sse;
-        else
-          s_m1[g] += sse;
-      }
+      if (lane == 0) atomicAdd(&s_sse[P][g], sse);
     }
-    __syncthreads();
   }
-  if (tid < 64) m1[tid] = s_m1[tid];
+  __syncthreads();
+  if (tid < 64) {
+    m0[tid] = ((mask0 >> tid) & 1) ? (uint64_t)s_sse[0][tid] : (uint64_t)kUntestedMSE;
+    m1[tid] = ((mask1 >> tid) & 1) ? (uint64_t)s_sse[1][tid] : (uint64_t)kUntestedMSE;
+  }
 }
 
 // ---- greedy preset selection (finish) ----
 
-struct SelState {
-  int lev0[4][8], lev1[4][8];     // per configuration nb = 1 << c
-  unsigned long long tot[4];
-  unsigned long long sav[4][64 * 64];
-  unsigned long long sumBest[4];
-  unsigned long long colsum[4][2][64];
+// Savings-matrix slice each cluster CTA reduces.
+constexpr int kSelPairsPerCta = 4096 / kSelCluster;
+
+struct SelShared {
+  unsigned long long part[4096];       // this CTA's partial savings (or column sums)
+  unsigned long long col[128];
+  unsigned long long candV[2], candSB[2];
+  int candI[2];
+  unsigned long long redV[kSelThreads / 32];
+  int redI[kSelThreads / 32];
+  unsigned long long redS[kSelThreads / 32];
+  int lev0[8], lev1[8];
+  unsigned long long tot;
 };
 
-struct SelArgs {
-  const uint64_t* mse;   // [2][nfb][64]
-  const int* sb;         // non-skip filter blocks
-  int n, nfb;
-  SelState* st;
-};
-
-// One step's partial sums over a chunk of filter blocks: for nbCur == 0 the
-// per-strength column sums, else sumBest and the savings matrix.
-__global__ void __launch_bounds__(256) k_sel_accum(SelArgs a, int cfg, int nbCur) {
-  SelState* st = a.st;
-  const int per = (a.n + gridDim.x - 1) / gridDim.x;
-  const int i0 = blockIdx.x * per, i1 = imin(a.n, i0 + per);
-  if (i0 >= i1) return;
-  const uint64_t* M0 = a.mse;
-  const uint64_t* M1 = a.mse + (size_t)a.nfb * 64;
-  if (nbCur == 0) {
-    if (threadIdx.x < 128) {
-      const int pl = threadIdx.x >> 6, j = threadIdx.x & 63;
-      const uint64_t* M = pl ? M1 : M0;
-      unsigned long long s = 0;
-      for (int i = i0; i < i1; i++) s += M[(size_t)a.sb[i] * 64 + j];
-      atomicAdd(&st->colsum[cfg][pl][j], s);
+// One cluster per configuration nb = 1 << (blockIdx.x / kSelCluster).
+// kRows: the filter blocks' SSE rows (as 32-bit values; an 8-bit 64x64
+// block's SSE is below 2^28) are copied into shared memory.
+template <bool kRows>
+__global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(kSelThreads)
+    k_sel_greedy(SelArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  SelShared& S = *reinterpret_cast<SelShared*>(smem);
+  uint32_t* s_best = reinterpret_cast<uint32_t*>(smem + sizeof(SelShared));
+  uint32_t* s_min1 = s_best + a.cap;
+  uint32_t* s_rows = s_min1 + a.cap;  // [cap][128] when kRows
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int cfg = blockIdx.x / kSelCluster;
+  const int nb = 1 << cfg;
+  const int t = threadIdx.x;
+  const int n = *a.n;
+  SelOut* out = a.out;
+  if (n == 0) {
+    if (rank == 0 && t == 0) {
+      for (int g = 0; g < 8; g++) out->lev0[cfg][g] = out->lev1[cfg][g] = 0;
+      out->tot[cfg] = 0;
     }
     return;
   }
-  __shared__ unsigned long long s_best[256];
-  __shared__ unsigned long long s_part;
-  if (threadIdx.x == 0) s_part = 0;
+  const int per = (n + kSelCluster - 1) / kSelCluster;
+  const int i0 = imin(n, rank * per), i1 = imin(n, i0 + per), cnt = i1 - i0;
+  const uint64_t* M0 = a.mse;
+  const uint64_t* M1 = a.mse + (size_t)a.nfb * 64;
+  auto row = [&](int il, int pl, int j) -> uint32_t {
+    if (kRows) return s_rows[il * 128 + pl * 64 + j];
+    const int fb = a.sb[i0 + il];
+    return (uint32_t)(pl ? M1 : M0)[(size_t)fb * 64 + j];
+  };
+  if (kRows)
+    for (int e = t; e < cnt * 128; e += kSelThreads) {
+      const int il = e >> 7, pl = (e >> 6) & 1, j = e & 63;
+      const int fb = a.sb[i0 + il];
+      s_rows[e] = (uint32_t)(pl ? M1 : M0)[(size_t)fb * 64 + j];
+    }
   __syncthreads();
-  unsigned long long localSav[16];
-#pragma unroll
-  for (int q = 0; q < 16; q++) localSav[q] = 0;
-  for (int base = i0; base < i1; base += 256) {
-    const int cnt = imin(256, i1 - base);
-    __syncthreads();
-    if ((int)threadIdx.x < cnt) {
-      const int fb = a.sb[base + threadIdx.x];
-      unsigned long long best = M0[(size_t)fb * 64 + st->lev0[cfg][0]] + M1[(size_t)fb * 64 + st->lev1[cfg][0]];
-      for (int g = 1; g < nbCur; g++) {
-        const unsigned long long c = M0[(size_t)fb * 64 + st->lev0[cfg][g]] + M1[(size_t)fb * 64 + st->lev1[cfg][g]];
-        if (c < best) best = c;
-      }
-      s_best[threadIdx.x] = best;
-      atomicAdd(&s_part, best);
-    }
-    __syncthreads();
-    for (int ii = 0; ii < cnt; ii++) {
-      const int fb = a.sb[base + ii];
-      const unsigned long long best = s_best[ii];
-#pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int p = threadIdx.x + 256 * q;
-        const int j = p >> 6, k = p & 63;
-        const unsigned long long v0 = M0[(size_t)fb * 64 + j];
-        if (v0 >= best) continue;
-        const unsigned long long rem = best - v0, v1 = M1[(size_t)fb * 64 + k];
-        if (v1 < rem) localSav[q] += rem - v1;
-      }
-    }
+  for (int il = t; il < cnt; il += kSelThreads) {
+    uint32_t m = 0xffffffffu;
+    for (int k = 0; k < 64; k++) m = min(m, row(il, 1, k));
+    s_min1[il] = m;
   }
-#pragma unroll
-  for (int q = 0; q < 16; q++)
-    if (localSav[q]) atomicAdd(&st->sav[cfg][threadIdx.x + 256 * q], localSav[q]);
+  if (t < 8) S.lev0[t] = S.lev1[t] = 0;
   __syncthreads();
-  if (threadIdx.x == 0) atomicAdd(&st->sumBest[cfg], s_part);
-}
-
-// Picks the step's winner, clears the accumulators, and shifts the selected
-// list left when the next step is a refinement pass.
-__global__ void __launch_bounds__(1024) k_sel_pick(SelArgs a, int cfg, int nbCur, int shiftAfter, int nb) {
-  SelState* st = a.st;
-  __shared__ unsigned long long s_v[1024];
-  __shared__ int s_i[1024];
-  const int t = threadIdx.x;
-  if (a.n == 0) {
-    if (t == 0) {
-      st->lev0[cfg][nbCur] = st->lev1[cfg][nbCur] = 0;
-      st->tot[cfg] = 0;
-    }
-  } else if (nbCur == 0) {
-    if (t == 0) {
-      int b0 = 0, b1 = 0;
-      for (int j = 1; j < 64; j++) {
-        if (st->colsum[cfg][0][j] < st->colsum[cfg][0][b0]) b0 = j;
-        if (st->colsum[cfg][1][j] < st->colsum[cfg][1][b1]) b1 = j;
+  const int steps = 5 * nb;
+  for (int k = 0; k < steps; k++) {
+    const int nbCur = k < nb ? k : nb - 1;
+    const int par = k & 1;
+    if (nbCur == 0) {
+      // First pick: the luma and chroma strengths with the least total SSE.
+      if (t < 128) {
+        unsigned long long s = 0;
+        for (int il = 0; il < cnt; il++) s += row(il, t >> 6, t & 63);
+        S.part[t] = s;
       }
-      st->lev0[cfg][0] = b0;
-      st->lev1[cfg][0] = b1;
-      st->tot[cfg] = st->colsum[cfg][0][b0] + st->colsum[cfg][1][b1];
-    }
-  } else {
-    // argmax over row-major (j, k), the first maximum wins (strict >).
-    unsigned long long bv = 0;
-    int bi = 0x7fffffff;
-    for (int p = t; p < 4096; p += 1024) {
-      const unsigned long long v = st->sav[cfg][p];
-      if (bi == 0x7fffffff || v > bv) {
-        bv = v;
-        bi = p;
-      }
-    }
-    s_v[t] = bv;
-    s_i[t] = bi;
-    __syncthreads();
-    for (int o = 512; o > 0; o >>= 1) {
-      if (t < o) {
-        const unsigned long long v2 = s_v[t + o];
-        const int i2 = s_i[t + o];
-        if (v2 > s_v[t] || (v2 == s_v[t] && i2 < s_i[t])) {
-          s_v[t] = v2;
-          s_i[t] = i2;
-        }
+      cl.sync();
+      if (t < 128) {
+        unsigned long long s = 0;
+        for (int r = 0; r < kSelCluster; r++) s += cl.map_shared_rank(&S.part[0], r)[t];
+        S.col[t] = s;
       }
       __syncthreads();
+      if (t == 0) {
+        int b0 = 0, b1 = 0;
+        for (int j = 1; j < 64; j++) {
+          if (S.col[j] < S.col[b0]) b0 = j;
+          if (S.col[64 + j] < S.col[64 + b1]) b1 = j;
+        }
+        S.lev0[0] = b0;
+        S.lev1[0] = b1;
+        S.tot = S.col[b0] + S.col[64 + b1];
+      }
+      cl.sync();  // every CTA has read the others' column sums
+    } else {
+      // best_i over the strengths selected so far, and its sum.
+      unsigned long long sb = 0;
+      for (int il = t; il < cnt; il += kSelThreads) {
+        uint32_t best = row(il, 0, S.lev0[0]) + row(il, 1, S.lev1[0]);
+        for (int g = 1; g < nbCur; g++) best = min(best, row(il, 0, S.lev0[g]) + row(il, 1, S.lev1[g]));
+        s_best[il] = best;
+        sb += best;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sb += __shfl_xor_sync(0xffffffffu, sb, o);
+      if ((t & 31) == 0) S.redS[t >> 5] = sb;
+      __syncthreads();
+      if (t == 0) {
+        unsigned long long s = 0;
+        for (int w = 0; w < kSelThreads / 32; w++) s += S.redS[w];
+        S.candSB[par] = s;
+      }
+      // Partial savings of this CTA's blocks: thread t owns (j, k0..k0+7).
+      const int j = t >> 3, k0 = (t & 7) * 8;
+      unsigned long long acc[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) acc[q] = 0;
+      for (int il = 0; il < cnt; il++) {
+        const uint32_t bi = s_best[il], a0 = row(il, 0, j);
+        if (a0 + s_min1[il] >= bi) continue;  // no k can save anything
+        const uint32_t rem = bi - a0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const uint32_t v = row(il, 1, k0 + q);
+          if (v < rem) acc[q] += rem - v;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 8; q++) S.part[j * 64 + k0 + q] = acc[q];
+      cl.sync();
+      // Reduce this CTA's slice across the cluster; first maximum wins.
+      unsigned long long bv = 0;
+      int bi = 0x7fffffff;
+      for (int e = rank * kSelPairsPerCta + t; e < (rank + 1) * kSelPairsPerCta; e += kSelThreads) {
+        unsigned long long v = 0;
+        for (int r = 0; r < kSelCluster; r++) v += cl.map_shared_rank(&S.part[0], r)[e];
+        if (bi == 0x7fffffff || v > bv) {
+          bv = v;
+          bi = e;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (v2 > bv || (v2 == bv && i2 < bi)) {
+          bv = v2;
+          bi = i2;
+        }
+      }
+      if ((t & 31) == 0) {
+        S.redV[t >> 5] = bv;
+        S.redI[t >> 5] = bi;
+      }
+      __syncthreads();
+      if (t == 0) {
+        for (int w = 1; w < kSelThreads / 32; w++)
+          if (S.redV[w] > bv || (S.redV[w] == bv && S.redI[w] < bi)) {
+            bv = S.redV[w];
+            bi = S.redI[w];
+          }
+        S.candV[par] = bv;
+        S.candI[par] = bi;
+      }
+      cl.sync();
+      if (t == 0) {
+        unsigned long long wv = 0, sumBest = 0;
+        int wi = 0x7fffffff;
+        for (int r = 0; r < kSelCluster; r++) {
+          const SelShared* R = cl.map_shared_rank(&S, r);
+          const unsigned long long v = R->candV[par];
+          const int i = R->candI[par];
+          sumBest += R->candSB[par];
+          if (wi == 0x7fffffff || v > wv || (v == wv && i < wi)) {
+            wv = v;
+            wi = i;
+          }
+        }
+        S.lev0[nbCur] = wi >> 6;
+        S.lev1[nbCur] = wi & 63;
+        S.tot = sumBest - wv;
+      }
     }
-    if (t == 0) {
-      st->lev0[cfg][nbCur] = s_i[0] >> 6;
-      st->lev1[cfg][nbCur] = s_i[0] & 63;
-      st->tot[cfg] = st->sumBest[cfg] - s_v[0];
-    }
+    // Refinement passes drop the oldest pick (jointStrengthSearchDual).
+    if (t == 0 && k + 1 >= nb && k + 1 < steps)
+      for (int g = 0; g < nb - 1; g++) {
+        S.lev0[g] = S.lev0[g + 1];
+        S.lev1[g] = S.lev1[g + 1];
+      }
+    __syncthreads();
   }
-  __syncthreads();
-  for (int p = t; p < 4096; p += 1024) st->sav[cfg][p] = 0;
-  if (t < 128) st->colsum[cfg][t >> 6][t & 63] = 0;
-  if (t == 0) st->sumBest[cfg] = 0;
-  if (shiftAfter && t == 0) {
-    for (int j = 0; j < nb - 1; j++) {
-      st->lev0[cfg][j] = st->lev0[cfg][j + 1];
-      st->lev1[cfg][j] = st->lev1[cfg][j + 1];
+  if (rank == 0 && t == 0) {
+    for (int g = 0; g < 8; g++) {
+      out->lev0[cfg][g] = g < nb ? S.lev0[g] : 0;
+      out->lev1[cfg][g] = g < nb ? S.lev1[g] : 0;
     }
+    out->tot[cfg] = S.tot;
   }
+  cl.sync();  // no CTA leaves while another may still read its shared memory
 }
-
-struct FinishOut {
-  int bits;
-  int ys[8], uvs[8];
-  unsigned long long cost;
-};
 
 // RD choice of nb (finish, :914-931) and the per-block preset index.
 __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsigned long long lambda, uint8_t* fbIndex,
-                                                    FinishOut* out) {
+                                                    FinishOut* fo) {
   __shared__ int s_best;
-  const SelState* st = a.st;
+  const SelOut* st = a.out;
+  const int n = *a.n;
   if (threadIdx.x == 0) {
     unsigned long long bestTot = 1ull << 63;
     int best = 0;
     for (int c = 0; c <= maxCfg; c++) {
       const int nb = 1 << c;
-      const long long rate = (long long)(a.n * c + nb * 6 * 2) << 9;
+      const long long rate = (long long)(n * c + nb * 6 * 2) << 9;
       const unsigned long long cost =
           (unsigned long long)((rate * (long long)lambda + (1 << 8)) >> 9) + ((st->tot[c] * 16ull) << 7);
       if (cost < bestTot) {
@@ -402,11 +406,11 @@ __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsig
     }
     s_best = best;
     if (blockIdx.x == 0) {
-      out->bits = best;
-      out->cost = bestTot;
+      fo->bits = best;
+      fo->cost = bestTot;
       for (int j = 0; j < (1 << best); j++) {
-        out->ys[j] = st->lev0[best][j];
-        out->uvs[j] = st->lev1[best][j];
+        fo->ys[j] = st->lev0[best][j];
+        fo->uvs[j] = st->lev1[best][j];
       }
     }
   }
@@ -415,7 +419,7 @@ __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsig
   const uint64_t* M0 = a.mse;
   const uint64_t* M1 = a.mse + (size_t)a.nfb * 64;
   for (int fb = blockIdx.x * blockDim.x + threadIdx.x; fb < a.nfb; fb += gridDim.x * blockDim.x) fbIndex[fb] = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int fb = a.sb[i];
     int bg = 0;
     unsigned long long bm = 1ull << 63;
@@ -431,13 +435,58 @@ __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsig
 }
 
 // Compacts the non-skip filter blocks into a list (order preserved).
-__global__ void k_sel_list(const uint8_t* skip, int nfb, int* sb, int* n) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    int c = 0;
-    for (int fb = 0; fb < nfb; fb++)
-      if (!skip[fb]) sb[c++] = fb;
-    *n = c;
+__global__ void __launch_bounds__(1024) k_sel_list(const uint8_t* skip, int nfb, int* sb, int* n) {
+  __shared__ int s_warp[32];
+  __shared__ int s_base;
+  const int t = threadIdx.x;
+  if (t == 0) s_base = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < nfb; b0 += 1024) {
+    const int fb = b0 + t;
+    const bool keep = fb < nfb && !skip[fb];
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if ((t & 31) == 0) s_warp[t >> 5] = __popc(m);
+    __syncthreads();
+    int off = s_base;
+    for (int w = 0; w < (t >> 5); w++) off += s_warp[w];
+    off += __popc(m & ((1u << (t & 31)) - 1));
+    if (keep) sb[off] = fb;
+    __syncthreads();
+    if (t == 0)
+      for (int w = 0; w < 32; w++) s_base += s_warp[w];
+    __syncthreads();
   }
+  if (t == 0) *n = s_base;
+}
+
+size_t sel_smem_bytes(int nfb, bool rows) {
+  const int cap = (nfb + kSelCluster - 1) / kSelCluster;
+  return sizeof(SelShared) + (size_t)cap * 8 + (rows ? (size_t)cap * 512 : 0);
+}
+
+cudaError_t launch_search(const SearchArgs& a, cudaStream_t st) {
+  k_cdef_search<<<a.nhfb * a.nvfb, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_select(SelArgs s, int maxCfg, unsigned long long lambda, uint8_t* fbIndex, FinishOut* fo,
+                          cudaStream_t st) {
+  k_sel_list<<<1, 1024, 0, st>>>(s.skip, s.nfb, s.sb_w, s.n_w);
+  s.cap = (s.nfb + kSelCluster - 1) / kSelCluster;
+  const bool rows = sel_smem_bytes(s.nfb, true) <= kSelMaxSmem;
+  const size_t bytes = sel_smem_bytes(s.nfb, rows);
+  if (bytes > kSelMaxSmem) return cudaErrorInvalidValue;
+  cudaError_t e;
+  if (rows) {
+    e = cudaFuncSetAttribute(k_sel_greedy<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) k_sel_greedy<true><<<kSelCluster * (maxCfg + 1), kSelThreads, bytes, st>>>(s);
+  } else {
+    e = cudaFuncSetAttribute(k_sel_greedy<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) k_sel_greedy<false><<<kSelCluster * (maxCfg + 1), kSelThreads, bytes, st>>>(s);
+  }
+  if (e != cudaSuccess) return e;
+  k_sel_finish<<<imax(1, (s.nfb + 255) / 256), 256, 0, st>>>(s, maxCfg, lambda, fbIndex, fo);
+  return cudaGetLastError();
 }
 
 }  // namespace pf
@@ -445,16 +494,8 @@ __global__ void k_sel_list(const uint8_t* skip, int nfb, int* sb, int* n) {
 using namespace pf;
 
 // ---------------------------------------------------------------------------
-// Host side: the search entry point.  Scratch comes from a small cache the
-// entry point keeps per process (grown, never shrunk); frames are staged like
-// pf_frame_apply's.
-
-namespace {
-struct SearchBufs {
-  void* p = nullptr;
-  size_t n = 0;
-};
-}  // namespace
+// Host side: the search entry points.  Scratch comes from a cache the context
+// keeps (grown, never shrunk); host frames are staged like pf_frame_apply's.
 
 void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
 void* pf_internal_stream(pf_ctx* c);
@@ -493,36 +534,51 @@ static DFrame search_dframe(const pf_frame* f, uint8_t* const* ptrs, const int64
   return d;
 }
 
-extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
-                              const pf_cdef_search_params* params, uint64_t* mse_out, uint8_t* fb_index_out,
-                              pf_cdef_search_result* result) {
-  if (!ctx || !source || !recon || !params) return PF_ERR_INVALID_ARG;
+// Validation, staging and scratch shared by the search entry points.
+// Scratch: [staged src | staged rec | noskip | mse | skip | sb list | n |
+//           SelOut | FinishOut | fbIndex | caller's extra bytes].
+struct Staged {
+  SearchArgs a;
+  SelArgs s;
+  uint8_t* idx;
+  FinishOut* fo;
+  uint8_t* extra;
+  int nfb, maxCfg;
+  cudaStream_t st;
+};
+
+static int check_search_frame(const pf_frame* f, const pf_frame* recon) {
   // goav1's searcher works on 8-bit 4:2:0 pictures (SourceFrame420).
-  if (recon->bit_depth != 8 || source->bit_depth != 8 || recon->ss_x != 1 || recon->ss_y != 1 || recon->mono ||
-      source->width != recon->width || source->height != recon->height || source->ss_x != 1 || source->ss_y != 1)
+  if (f->bit_depth != 8 || f->ss_x != 1 || f->ss_y != 1 || f->mono || f->width != recon->width ||
+      f->height != recon->height)
     return PF_ERR_UNSUPPORTED;
-  if (recon->memory != source->memory || recon->memory > PF_MEM_DEVICE) return PF_ERR_INVALID_ARG;
+  if (f->memory != recon->memory || f->memory > PF_MEM_DEVICE) return PF_ERR_INVALID_ARG;
   for (int p = 0; p < 3; p++) {
     const int w = p ? (recon->width + 1) >> 1 : recon->width, h = p ? (recon->height + 1) >> 1 : recon->height;
     const int aw8 = ((recon->width + 7) & ~7) >> (p ? 1 : 0), ah8 = ((recon->height + 7) & ~7) >> (p ? 1 : 0);
-    for (const pf_frame* f : {source, recon}) {
-      const pf_plane& pl = f->plane[p];
-      if (!pl.data || pl.width != w || pl.height != h || pl.alloc_width < aw8 || pl.alloc_height < ah8 ||
-          pl.stride < pl.alloc_width)
-        return PF_ERR_SHORT_BUFFER;
-    }
+    const pf_plane& pl = f->plane[p];
+    if (!pl.data || pl.width != w || pl.height != h || pl.alloc_width < aw8 || pl.alloc_height < ah8 ||
+        pl.stride < pl.alloc_width)
+      return PF_ERR_SHORT_BUFFER;
   }
+  return PF_OK;
+}
+
+// source may be null (features only: the source is never read).
+static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
+                        int damping, int maxCfg, size_t extra, Staged* S) {
+  int stt = check_search_frame(recon, recon);
+  if (stt == PF_OK && source) stt = check_search_frame(source, recon);
+  if (stt != PF_OK) return stt;
+  if (damping < 3 || damping > 6) return PF_ERR_INVALID_CDEF;
   const int miCols = ((recon->width + 7) >> 3) << 1, miRows = ((recon->height + 7) >> 3) << 1;
   const int nhfb = (miCols + 15) / 16, nvfb = (miRows + 15) / 16, nfb = nhfb * nvfb;
-  const int damping = params->damping ? params->damping : 3 + (params->qindex >> 6);
-  if (damping < 3 || damping > 6) return PF_ERR_INVALID_CDEF;
-  const int maxCfg = params->max_presets >= 8 ? 3 : params->max_presets >= 4 ? 2 : params->max_presets >= 2 ? 1 : 0;
+  if (sel_smem_bytes(nfb, false) > kSelMaxSmem) return PF_ERR_UNSUPPORTED;
   const cudaStream_t st = (cudaStream_t)pf_internal_stream(ctx);
   const bool host = recon->memory == PF_MEM_HOST;
-  // Scratch: [staged src | staged rec | noskip | mse | skip | sb list | n | SelState | FinishOut | fbIndex].
-  int64_t sS[3], rS[3];
+  int64_t sS[3] = {0, 0, 0}, rS[3];
   cudaError_t e = cudaSuccess;
-  const size_t srcBytes = host ? (size_t)stage_frame(source, nullptr, sS, st, &e) : 0;
+  const size_t srcBytes = host && source ? (size_t)stage_frame(source, nullptr, sS, st, &e) : 0;
   const size_t recBytes = host ? (size_t)stage_frame(recon, nullptr, rS, st, &e) : 0;
   auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
   size_t off = 0;
@@ -533,27 +589,32 @@ extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_fram
   const size_t oSkip = off; off += al(nfb);
   const size_t oSb = off; off += al((size_t)nfb * 4);
   const size_t oN = off; off += 256;
-  const size_t oSel = off; off += al(sizeof(SelState));
+  const size_t oSel = off; off += al(sizeof(SelOut));
   const size_t oFin = off; off += al(sizeof(FinishOut));
   const size_t oIdx = off; off += al(nfb);
+  const size_t oExtra = off; off += al(extra);
   uint8_t* base = (uint8_t*)pf_internal_search_scratch(ctx, off);
   if (!base) return PF_ERR_DEVICE;
-  uint8_t* sp[3];
+  uint8_t* sp[3] = {nullptr, nullptr, nullptr};
   uint8_t* rpp[3];
   if (host) {
-    stage_frame(source, base + oSrc, sS, st, &e);
+    if (source) stage_frame(source, base + oSrc, sS, st, &e);
     stage_frame(recon, base + oRec, rS, st, &e);
     size_t o1 = 0, o2 = 0;
     for (int p = 0; p < 3; p++) {
-      sp[p] = base + oSrc + o1;
+      if (source) {
+        sp[p] = base + oSrc + o1;
+        o1 += (size_t)sS[p] * source->plane[p].alloc_height;
+      }
       rpp[p] = base + oRec + o2;
-      o1 += (size_t)sS[p] * source->plane[p].alloc_height;
       o2 += (size_t)rS[p] * recon->plane[p].alloc_height;
     }
   } else {
     for (int p = 0; p < 3; p++) {
-      sp[p] = (uint8_t*)source->plane[p].data;
-      sS[p] = source->plane[p].stride;
+      if (source) {
+        sp[p] = (uint8_t*)source->plane[p].data;
+        sS[p] = source->plane[p].stride;
+      }
       rpp[p] = (uint8_t*)recon->plane[p].data;
       rS[p] = recon->plane[p].stride;
     }
@@ -566,10 +627,11 @@ extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_fram
     ns = base + oNs;
   }
   if (e != cudaSuccess) return PF_ERR_DEVICE;
-  SearchArgs a;
-  a.src = search_dframe(source, sp, sS);
+  SearchArgs& a = S->a;
+  a.src = source ? search_dframe(source, sp, sS) : search_dframe(recon, rpp, rS);
   a.rec = search_dframe(recon, rpp, rS);
   a.noskip = ns;
+  a.tmask = nullptr;
   a.miCols = miCols;
   a.miRows = miRows;
   a.nhfb = nhfb;
@@ -577,41 +639,47 @@ extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_fram
   a.damping = damping;
   a.mse = (uint64_t*)(base + oMse);
   a.skip = base + oSkip;
-  k_cdef_search<<<nfb, 256, 0, st>>>(a);
-  k_sel_list<<<1, 32, 0, st>>>(a.skip, nfb, (int*)(base + oSb), (int*)(base + oN));
-  if (cudaMemsetAsync(base + oSel, 0, sizeof(SelState), st) != cudaSuccess) return PF_ERR_DEVICE;
-  // The number of non-skip blocks is needed on the host to size the steps.
-  int n = 0;
-  if (cudaMemcpyAsync(&n, base + oN, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    return PF_ERR_DEVICE;
-  SelArgs s;
+  SelArgs& s = S->s;
   s.mse = a.mse;
-  s.sb = (const int*)(base + oSb);
-  s.n = n;
+  s.skip = a.skip;
+  s.sb_w = (int*)(base + oSb);
+  s.n_w = (int*)(base + oN);
+  s.sb = s.sb_w;
+  s.n = s.n_w;
   s.nfb = nfb;
-  s.st = (SelState*)(base + oSel);
-  const int grid = imax(1, imin(148, n));
-  for (int c = 0; c <= maxCfg; c++) {
-    const int nb = 1 << c;
-    // jointStrengthSearchDual: nb greedy steps, then 4*nb refinements.
-    const int steps = nb + 4 * nb;
-    for (int k = 0; k < steps; k++) {
-      const int nbCur = k < nb ? k : nb - 1;
-      const int shiftAfter = (k + 1 >= nb && k + 1 < steps) ? 1 : 0;
-      k_sel_accum<<<grid, 256, 0, st>>>(s, c, nbCur);
-      k_sel_pick<<<1, 1024, 0, st>>>(s, c, nbCur, shiftAfter, nb);
-    }
-  }
-  k_sel_finish<<<imax(1, (nfb + 255) / 256), 256, 0, st>>>(s, maxCfg, (unsigned long long)params->lambda,
-                                                           base + oIdx, (FinishOut*)(base + oFin));
-  if (cudaGetLastError() != cudaSuccess) return PF_ERR_DEVICE;
-  FinishOut fo;
-  if (cudaMemcpyAsync(&fo, base + oFin, sizeof(fo), cudaMemcpyDeviceToHost, st) != cudaSuccess) return PF_ERR_DEVICE;
-  if (mse_out &&
-      cudaMemcpyAsync(mse_out, a.mse, (size_t)2 * nfb * 64 * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+  s.cap = 0;
+  s.out = (SelOut*)(base + oSel);
+  S->idx = base + oIdx;
+  S->fo = (FinishOut*)(base + oFin);
+  S->extra = base + oExtra;
+  S->nfb = nfb;
+  S->maxCfg = maxCfg;
+  S->st = st;
+  return PF_OK;
+}
+
+static int search_damping(const pf_cdef_search_params* params) {
+  return params->damping ? params->damping : 3 + (params->qindex >> 6);
+}
+
+static int search_max_cfg(const pf_cdef_search_params* params) {
+  return params->max_presets >= 8 ? 3 : params->max_presets >= 4 ? 2 : params->max_presets >= 2 ? 1 : 0;
+}
+
+// Search (with S.a.tmask already set by the caller, or null), selection,
+// results to the host.
+static int search_finish(Staged& S, const pf_cdef_search_params* params, uint64_t* mse_out, uint8_t* fb_index_out,
+                         pf_cdef_search_result* result) {
+  const cudaStream_t st = S.st;
+  if (launch_search(S.a, st) != cudaSuccess) return PF_ERR_DEVICE;
+  if (launch_select(S.s, S.maxCfg, (unsigned long long)params->lambda, S.idx, S.fo, st) != cudaSuccess)
     return PF_ERR_DEVICE;
-  if (fb_index_out && cudaMemcpyAsync(fb_index_out, base + oIdx, nfb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+  FinishOut fo;
+  if (cudaMemcpyAsync(&fo, S.fo, sizeof(fo), cudaMemcpyDeviceToHost, st) != cudaSuccess) return PF_ERR_DEVICE;
+  if (mse_out &&
+      cudaMemcpyAsync(mse_out, S.a.mse, (size_t)2 * S.nfb * 64 * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return PF_ERR_DEVICE;
+  if (fb_index_out && cudaMemcpyAsync(fb_index_out, S.idx, S.nfb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return PF_ERR_DEVICE;
   if (cudaStreamSynchronize(st) != cudaSuccess) return PF_ERR_DEVICE;
   if (result) {
@@ -623,6 +691,83 @@ extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_fram
       result->uv_strength[j] = (uint8_t)trial_strength(fo.uvs[j]);
     }
     result->cost = (double)fo.cost;
+  }
+  return PF_OK;
+}
+
+extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
+                              const pf_cdef_search_params* params, uint64_t* mse_out, uint8_t* fb_index_out,
+                              pf_cdef_search_result* result) {
+  if (!ctx || !source || !recon || !params) return PF_ERR_INVALID_ARG;
+  Staged S;
+  const int stt = stage_search(ctx, source, recon, noskip, search_damping(params), search_max_cfg(params), 0, &S);
+  if (stt != PF_OK) return stt;
+  return search_finish(S, params, mse_out, fb_index_out, result);
+}
+
+extern "C" int pf_cdef_features(pf_ctx* ctx, const pf_frame* recon, const uint8_t* noskip, int32_t qindex,
+                                int32_t damping, float* features) {
+  if (!ctx || !recon || !features) return PF_ERR_INVALID_ARG;
+  if (qindex < 0 || qindex > 255) return PF_ERR_INVALID_ARG;
+  const int dmp = damping ? damping : 3 + (qindex >> 6);
+  Staged S;
+  const int miCols = ((recon->width + 7) >> 3) << 1, miRows = ((recon->height + 7) >> 3) << 1;
+  const int nfb = ((miCols + 15) / 16) * ((miRows + 15) / 16);
+  const size_t xBytes = (size_t)nfb * PF_MLP_FEATURES * sizeof(float);
+  const int stt = stage_search(ctx, nullptr, recon, noskip, dmp, 0, xBytes, &S);
+  if (stt != PF_OK) return stt;
+  float* X = (float*)S.extra;
+  if (launch_features(S.a, qindex, X, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  if (cudaMemcpyAsync(features, X, xBytes, cudaMemcpyDeviceToHost, S.st) != cudaSuccess ||
+      cudaStreamSynchronize(S.st) != cudaSuccess)
+    return PF_ERR_DEVICE;
+  return PF_OK;
+}
+
+extern "C" int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
+                                      const uint8_t* noskip, const pf_cdef_search_params* params,
+                                      const pf_cdef_mlp* model, float threshold, int32_t candidates,
+                                      uint64_t* mse_out, uint8_t* fb_index_out, pf_cdef_search_result* result,
+                                      pf_cdef_learned_stats* stats) {
+  if (!ctx || !source || !recon || !params || !model) return PF_ERR_INVALID_ARG;
+  if (candidates < 1 || candidates > 8 || !(threshold >= 0.f)) return PF_ERR_INVALID_ARG;
+  if (params->qindex < 0 || params->qindex > 255) return PF_ERR_INVALID_ARG;
+  const int miCols = ((recon->width + 7) >> 3) << 1, miRows = ((recon->height + 7) >> 3) << 1;
+  const int nfb = ((miCols + 15) / 16) * ((miRows + 15) / 16);
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t xBytes = al((size_t)nfb * PF_MLP_FEATURES * sizeof(float));
+  const size_t mBytes = al((size_t)nfb * 2 * sizeof(uint64_t));
+  const size_t wBytes = al(sizeof(pf_cdef_mlp));
+  Staged S;
+  const int stt = stage_search(ctx, source, recon, noskip, search_damping(params), search_max_cfg(params),
+                               xBytes + mBytes + wBytes, &S);
+  if (stt != PF_OK) return stt;
+  float* X = (float*)S.extra;
+  uint64_t* masks = (uint64_t*)(S.extra + xBytes);
+  pf_cdef_mlp* dmodel = (pf_cdef_mlp*)(S.extra + xBytes + mBytes);
+  if (cudaMemcpyAsync(dmodel, model, sizeof(pf_cdef_mlp), cudaMemcpyHostToDevice, S.st) != cudaSuccess)
+    return PF_ERR_DEVICE;
+  if (launch_features(S.a, params->qindex, X, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  if (launch_mlp_masks(dmodel, X, nfb, threshold, candidates, masks, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  S.a.tmask = masks;
+  std::vector<uint64_t> hm;
+  if (stats) hm.resize((size_t)nfb * 2);
+  if (stats && cudaMemcpyAsync(hm.data(), masks, (size_t)nfb * 16, cudaMemcpyDeviceToHost, S.st) != cudaSuccess)
+    return PF_ERR_DEVICE;
+  const int r = search_finish(S, params, mse_out, fb_index_out, result);
+  if (r != PF_OK) return r;
+  if (stats) {
+    std::vector<uint8_t> skip(nfb);
+    if (cudaMemcpy(skip.data(), S.a.skip, nfb, cudaMemcpyDeviceToHost) != cudaSuccess) return PF_ERR_DEVICE;
+    memset(stats, 0, sizeof(*stats));
+    for (int fb = 0; fb < nfb; fb++) {
+      if (skip[fb]) continue;
+      stats->blocks++;
+      const int c0 = __builtin_popcountll(hm[2 * fb]), c1 = __builtin_popcountll(hm[2 * fb + 1]);
+      if (c0 == 64 && c1 == 64) stats->fallback++;
+      stats->trials_luma += c0;
+      stats->trials_chroma += c1;
+    }
   }
   return PF_OK;
 }

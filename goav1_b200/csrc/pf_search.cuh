@@ -1,0 +1,141 @@
+// pf_search.cuh - shared declarations of the encoder CDEF strength search
+// (pf_search.cu) and the learned strength selection built on it (pf_mlp.cu).
+#pragma once
+
+#include "pf_common.cuh"
+
+namespace pf {
+
+// goav1's cdefDefaultMSEUV * 64 (encoder/cdef_search.go:669-672): the SSE
+// recorded for a trial that was not measured.
+constexpr uint32_t kUntestedMSE = 1040400u * 64u;
+
+constexpr int kSelCluster = 8;     // CTAs per greedy-selection cluster
+constexpr int kSelThreads = 512;
+constexpr size_t kSelMaxSmem = 200 * 1024;
+
+// Trial gi -> packed strength (level-1 lists: svtPfGI = 4*i for i < 16, then
+// pf+1..pf+3 for each first-pass pf; encoder/cdef_search.go:72-110).
+__host__ __device__ __forceinline__ int trial_strength(int g) {
+  if (g < 16) return g * 4;
+  const int k = g - 16;
+  return (k / 3) * 4 + (k % 3) + 1;
+}
+
+struct SearchArgs {
+  DFrame src, rec;          // 8-bit 4:2:0
+  const uint8_t* noskip;    // 8 bytes per filter block, or null (all blocks)
+  const uint64_t* tmask;    // [nfb][2] tested luma / chroma trials, or null (all 64)
+  int miCols, miRows, nhfb, nvfb;
+  int damping;
+  uint64_t* mse;            // [2][nfb][64]
+  uint8_t* skip;            // [nfb]
+};
+
+struct SelOut {
+  int lev0[4][8], lev1[4][8];  // per configuration nb = 1 << c
+  unsigned long long tot[4];
+};
+
+struct FinishOut {
+  int bits;
+  int ys[8], uvs[8];
+  unsigned long long cost;
+};
+
+struct SelArgs {
+  const uint64_t* mse;   // [2][nfb][64]
+  const uint8_t* skip;   // [nfb]
+  int* sb_w;             // non-skip filter blocks (written by the list kernel)
+  int* n_w;              // their count (device)
+  const int* sb;
+  const int* n;
+  int nfb, cap;
+  SelOut* out;
+};
+
+// The 8x8 luma blocks of filter block fb that the search measures
+// (computeCDEFList, encoder/cdef_search.go:410-447: noskip blocks inside the
+// MI grid), as a bit per block (bit = 8 * row + column).
+__device__ __forceinline__ uint64_t fb_listed(const SearchArgs& a, int fb, int lr, int lc) {
+  uint64_t word = ~0ull;
+  if (a.noskip) {
+    word = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) word |= (uint64_t)a.noskip[(size_t)fb * 8 + i] << (8 * i);
+  }
+  uint64_t listed = 0;
+  for (int r = 0; r < imin(a.miRows - lr, 16); r += 2)
+    for (int c = 0; c < imin(a.miCols - lc, 16); c += 2) {
+      const int b = (r >> 1) * 8 + (c >> 1);
+      listed |= word & (1ull << b);
+    }
+  return listed;
+}
+
+// cdef/direction.go:37-79 (partial sums) and :469-501 (cost), 8-bit samples
+// read straight from the frame; shared by the search and the features.
+template <int D>
+__device__ __forceinline__ int32_t dir_cost8(const uint8_t* blk, int64_t stride) {
+  int32_t p[15];
+#pragma unroll
+  for (int k = 0; k < 15; k++) p[k] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int32_t x = (int32_t)blk[i * stride + j] - 128;
+      if (D == 0) p[i + j] += x;
+      if (D == 1) p[i + (j >> 1)] += x;
+      if (D == 2) p[i] += x;
+      if (D == 3) p[3 + i - (j >> 1)] += x;
+      if (D == 4) p[7 + i - j] += x;
+      if (D == 5) p[3 - (i >> 1) + j] += x;
+      if (D == 6) p[j] += x;
+      if (D == 7) p[(i >> 1) + j] += x;
+    }
+  }
+  if (D == 2 || D == 6) {
+    int32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s += p[i] * p[i];
+    return s * 105;
+  }
+  if (D == 0 || D == 4) {
+    const int32_t div[8] = {840, 420, 280, 210, 168, 140, 120, 105};
+    int32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < 7; i++) s += (p[i] * p[i] + p[14 - i] * p[14 - i]) * div[i];
+    return s + p[7] * p[7] * 105;
+  }
+  return (p[3] * p[3] + p[4] * p[4] + p[5] * p[5] + p[6] * p[6] + p[7] * p[7]) * 105 +
+         (p[0] * p[0] + p[10] * p[10]) * 420 + (p[1] * p[1] + p[9] * p[9]) * 210 + (p[2] * p[2] + p[8] * p[8]) * 140;
+}
+
+__device__ __forceinline__ int32_t dir_cost8_dev(int d, const uint8_t* blk, int64_t stride) {
+  switch (d) {
+    case 0: return dir_cost8<0>(blk, stride);
+    case 1: return dir_cost8<1>(blk, stride);
+    case 2: return dir_cost8<2>(blk, stride);
+    case 3: return dir_cost8<3>(blk, stride);
+    case 4: return dir_cost8<4>(blk, stride);
+    case 5: return dir_cost8<5>(blk, stride);
+    case 6: return dir_cost8<6>(blk, stride);
+    default: return dir_cost8<7>(blk, stride);
+  }
+}
+
+size_t sel_smem_bytes(int nfb, bool rows);
+cudaError_t launch_search(const SearchArgs& a, cudaStream_t st);
+// Non-skip list, the greedy selection for nb = 1..(1 << maxCfg) and the RD
+// finish; everything stays on the device (no host round trip).
+cudaError_t launch_select(SelArgs s, int maxCfg, unsigned long long lambda, uint8_t* fbIndex, FinishOut* fo,
+                          cudaStream_t st);
+
+// pf_mlp.cu: per-filter-block features of a.rec (X: [nfb][PF_MLP_FEATURES]).
+cudaError_t launch_features(const SearchArgs& a, int qindex, float* X, cudaStream_t st);
+// pf_mlp.cu: the network over X and the tested-trial masks ([nfb][2]).
+cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, const float* X, int nfb, float threshold, int candidates,
+                             uint64_t* masks, cudaStream_t st);
+
+}  // namespace pf

@@ -78,6 +78,12 @@ def check(status):
     return status
 
 
+def _nfb(w, h):
+    """Number of 64x64 filter blocks over the MI grid of a w x h frame."""
+    mi_cols, mi_rows = ((w + 7) >> 3) << 1, ((h + 7) >> 3) << 1
+    return ((mi_cols + 15) // 16) * ((mi_rows + 15) // 16)
+
+
 def validate(frame, side, display=None):
     """The status pf_frame_apply would return before touching anything."""
     return lib().pf_frame_validate(C.byref(frame), C.byref(side), C.byref(display) if display is not None else None)
@@ -119,9 +125,7 @@ class PostFilterRunner:
         """Encoder CDEF strength search (cdefSearcher.search + finish,
         internal/av1/encoder/cdef_search.go:580-945) on 8-bit 4:2:0 frames.
         Returns (pf_cdef_search_result, mse uint64[2, nfb, 64], fb_index uint8[nfb])."""
-        w, h = recon.width, recon.height
-        mi_cols, mi_rows = ((w + 7) >> 3) << 1, ((h + 7) >> 3) << 1
-        nfb = ((mi_cols + 15) // 16) * ((mi_rows + 15) // 16)
+        nfb = _nfb(recon.width, recon.height)
         mse = np.zeros((2, nfb, 64), np.uint64)
         idx = np.zeros(nfb, np.uint8)
         res = abi.pf_cdef_search_result()
@@ -130,6 +134,62 @@ class PostFilterRunner:
         check(lib().pf_cdef_search(self._h, C.byref(source), C.byref(recon), ns, C.byref(prm), mse.ctypes.data,
                                    idx.ctypes.data, C.byref(res)))
         return res, mse, idx
+
+    def cdef_features(self, recon, noskip, qindex, damping=0):
+        """Per-filter-block features (float32[nfb, 40]) of an 8-bit 4:2:0
+        deblocked reconstruction, as the learned search computes them."""
+        nfb = _nfb(recon.width, recon.height)
+        X = np.zeros((nfb, abi.PF_MLP_FEATURES), np.float32)
+        ns = noskip.ctypes.data if noskip is not None else None
+        check(lib().pf_cdef_features(self._h, C.byref(recon), ns, qindex, damping, X.ctypes.data))
+        return X
+
+    def mlp_forward(self, model, X):
+        """Softmax outputs float32[n, 128] (luma trials, then chroma trials)."""
+        X = np.ascontiguousarray(X, np.float32)
+        P = np.zeros((X.shape[0], abi.PF_MLP_OUTPUTS), np.float32)
+        check(lib().pf_cdef_mlp_forward(self._h, C.byref(model), X.ctypes.data, X.shape[0], P.ctypes.data))
+        return P
+
+    def mlp_gradients(self, model, X, labels):
+        """(mean loss, pf_cdef_mlp_grads) of the training kernels over one batch."""
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(labels, np.uint8)
+        loss = C.c_float()
+        g = abi.pf_cdef_mlp_grads()
+        check(lib().pf_cdef_mlp_gradients(self._h, C.byref(model), X.ctypes.data, Y.ctypes.data, X.shape[0],
+                                          C.byref(loss), C.byref(g)))
+        return loss.value, g
+
+    def mlp_train(self, model, X, labels, epochs, batch=256, lr=2e-3, beta1=0.9, beta2=0.999, eps=1e-8,
+                  weight_decay=1e-4, seed=1):
+        """Adam training on the GPU, model updated in place; returns the
+        per-epoch mean loss."""
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(labels, np.uint8)
+        prm = abi.pf_cdef_mlp_train_params(epochs=epochs, batch=batch, lr=lr, beta1=beta1, beta2=beta2, eps=eps,
+                                           weight_decay=weight_decay, seed=seed)
+        losses = np.zeros(epochs, np.float32)
+        check(lib().pf_cdef_mlp_train(self._h, C.byref(model), X.ctypes.data, Y.ctypes.data, X.shape[0],
+                                      C.byref(prm), losses.ctypes.data))
+        return losses
+
+    def cdef_search_learned(self, source, recon, noskip, qindex, lam, model, threshold=0.5, candidates=2,
+                            max_presets=8, damping=0):
+        """The learned search: the network's top trials per block, all trials
+        where it is unsure, then the reference's greedy selection.  Returns
+        (pf_cdef_search_result, mse uint64[2, nfb, 64], fb_index, pf_cdef_learned_stats)."""
+        nfb = _nfb(recon.width, recon.height)
+        mse = np.zeros((2, nfb, 64), np.uint64)
+        idx = np.zeros(nfb, np.uint8)
+        res = abi.pf_cdef_search_result()
+        st = abi.pf_cdef_learned_stats()
+        prm = abi.pf_cdef_search_params(qindex=qindex, damping=damping, max_presets=max_presets, lam=lam)
+        ns = noskip.ctypes.data if noskip is not None else None
+        check(lib().pf_cdef_search_learned(self._h, C.byref(source), C.byref(recon), ns, C.byref(prm),
+                                           C.byref(model), threshold, candidates, mse.ctypes.data, idx.ctypes.data,
+                                           C.byref(res), C.byref(st)))
+        return res, mse, idx, st
 
     def post_filter_output(self):
         """(display frame, True) after a grain-applying apply(), else (None, False)."""

@@ -80,11 +80,48 @@ class HostFrame:
 
 @dataclass
 class SideInfo:
-    """Side information arrays plus the pf_frame_side struct pointing at them."""
+    """Side information arrays plus the pf_frame_side struct pointing at them.
+
+    Picklable (for process pools): the struct travels as bytes with each
+    pointer recorded as an index into `keep`, and is re-pointed on arrival."""
 
     side: abi.pf_frame_side
     keep: list = field(default_factory=list)  # arrays the struct points into
     blocks: dict = field(default_factory=dict)  # generator bookkeeping
+
+    _PTRS = (("lf", "masks"), ("lf", "level_cache"), ("cdef", "index"), ("cdef", "read"), ("cdef", "noskip"))
+
+    def __getstate__(self):
+        addrs = [k.ctypes.data if isinstance(k, np.ndarray) else C.addressof(k) for k in self.keep]
+
+        def find(a):
+            if not a:
+                return None
+            if a not in addrs:
+                raise ValueError("pf_frame_side points outside its kept arrays")
+            return addrs.index(a)
+
+        ptrs = {"%s.%s" % sf: find(getattr(getattr(self.side, sf[0]), sf[1])) for sf in self._PTRS}
+        for p in range(3):
+            ptrs["lr.units.%d" % p] = find(self.side.lr.units[p])
+        keep = [k if isinstance(k, np.ndarray) else (type(k)._type_, type(k)._length_, bytes(k)) for k in self.keep]
+        return {"side": bytes(self.side), "ptrs": ptrs, "keep": keep, "blocks": self.blocks}
+
+    def __setstate__(self, st):
+        self.keep = [k if isinstance(k, np.ndarray) else (k[0] * k[1]).from_buffer_copy(k[2]) for k in st["keep"]]
+        self.blocks = st["blocks"]
+        self.side = abi.pf_frame_side.from_buffer_copy(st["side"])
+
+        def addr(i):
+            if i is None:
+                return None
+            k = self.keep[i]
+            return k.ctypes.data if isinstance(k, np.ndarray) else C.addressof(k)
+
+        for s, f in self._PTRS:
+            setattr(getattr(self.side, s), f, addr(st["ptrs"]["%s.%s" % (s, f)]))
+        for p in range(3):
+            self.side.lr.units[p] = addr(st["ptrs"]["lr.units.%d" % p])
 
 
 # ---------------------------------------------------------------------------

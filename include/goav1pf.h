@@ -326,6 +326,105 @@ int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
 #define PF_GRAIN_STATIC_MAX_BLOCKS 65536
 int pf_film_grain_static(const pf_frame* ref, const pf_film_grain* fg, const pf_frame* display, void* stream);
 
+/* ---- learned CDEF strength selection ----
+ * No counterpart in the reference.  A small network predicts, per 64x64
+ * filter block, which of the 64 level-1 trials (the pf_cdef_search order)
+ * is best for luma and for chroma, from 40 statistics of the deblocked
+ * reconstruction.  pf_cdef_search_learned then measures only the predicted
+ * trials of a confident block, the full 64 + 64 of a block whose top-1
+ * probability is below the threshold, and runs the same greedy preset
+ * selection and RD choice as pf_cdef_search over that table; the bitstream
+ * syntax (CDEFParams and the per-block index) is unchanged.
+ *
+ * Network: 40 features -> 64 ReLU -> 64 ReLU -> 64 luma + 64 chroma logits,
+ * two softmax heads.  Weights are bf16 (bit patterns in uint16_t, row-major
+ * [out][in]), biases and arithmetic fp32 (fused multiply-add over the inputs
+ * in index order).  Features are normalised as (x - feat_shift) * feat_scale
+ * before the first layer. */
+#define PF_MLP_FEATURES 40
+#define PF_MLP_HIDDEN 64
+#define PF_MLP_CLASSES 64
+#define PF_MLP_OUTPUTS (2 * PF_MLP_CLASSES)
+#define PF_MLP_PARAMS                                                            \
+  (PF_MLP_HIDDEN * PF_MLP_FEATURES + PF_MLP_HIDDEN * PF_MLP_HIDDEN +             \
+   PF_MLP_OUTPUTS * PF_MLP_HIDDEN + 2 * PF_MLP_HIDDEN + PF_MLP_OUTPUTS)
+
+typedef struct pf_cdef_mlp {
+  uint16_t w1[PF_MLP_HIDDEN * PF_MLP_FEATURES];
+  uint16_t w2[PF_MLP_HIDDEN * PF_MLP_HIDDEN];
+  uint16_t w3[PF_MLP_OUTPUTS * PF_MLP_HIDDEN]; /* rows 0..63 luma, 64..127 chroma */
+  float b1[PF_MLP_HIDDEN];
+  float b2[PF_MLP_HIDDEN];
+  float b3[PF_MLP_OUTPUTS];
+  float feat_shift[PF_MLP_FEATURES];
+  float feat_scale[PF_MLP_FEATURES];
+} pf_cdef_mlp;
+
+/* Gradients of the mean loss with respect to every parameter, fp32, in the
+ * order w1, w2, w3, b1, b2, b3 (PF_MLP_PARAMS floats). */
+typedef struct pf_cdef_mlp_grads {
+  float w1[PF_MLP_HIDDEN * PF_MLP_FEATURES];
+  float w2[PF_MLP_HIDDEN * PF_MLP_HIDDEN];
+  float w3[PF_MLP_OUTPUTS * PF_MLP_HIDDEN];
+  float b1[PF_MLP_HIDDEN];
+  float b2[PF_MLP_HIDDEN];
+  float b3[PF_MLP_OUTPUTS];
+} pf_cdef_mlp_grads;
+
+typedef struct pf_cdef_mlp_train_params {
+  int32_t epochs;
+  int32_t batch;        /* samples per Adam step (a multiple of 32) */
+  float lr;             /* Adam step size */
+  float beta1, beta2, eps;
+  float weight_decay;   /* decoupled, on the weights only */
+  uint32_t seed;        /* shuffling */
+} pf_cdef_mlp_train_params;
+
+typedef struct pf_cdef_learned_stats {
+  int32_t blocks;         /* non-skip filter blocks */
+  int32_t fallback;       /* blocks searched with all 64 + 64 trials */
+  int32_t trials_luma;    /* luma trials measured, all blocks */
+  int32_t trials_chroma;  /* chroma trials measured, all blocks */
+} pf_cdef_learned_stats;
+
+/* Per-filter-block features of an 8-bit 4:2:0 deblocked reconstruction
+ * (host or device frame; noskip as in pf_cdef_search).  features is a host
+ * buffer of n_fb * PF_MLP_FEATURES floats, n_fb = ceil(w/64) * ceil(h/64);
+ * a block with no searched 8x8 block gets zeros in its first 33 features. */
+int pf_cdef_features(pf_ctx* ctx, const pf_frame* recon, const uint8_t* noskip,
+                     int32_t qindex, int32_t damping, float* features);
+
+/* Forward pass over n host feature rows; probs (host, n * PF_MLP_OUTPUTS)
+ * receives the two softmax heads. */
+int pf_cdef_mlp_forward(pf_ctx* ctx, const pf_cdef_mlp* model, const float* features,
+                        int32_t n, float* probs);
+
+/* Mean cross-entropy of both heads over n samples (labels: n pairs of luma,
+ * chroma trial indices) and its gradients, computed by the training
+ * kernels in one batch. */
+int pf_cdef_mlp_gradients(pf_ctx* ctx, const pf_cdef_mlp* model, const float* features,
+                          const uint8_t* labels, int32_t n, float* loss,
+                          pf_cdef_mlp_grads* grads);
+
+/* Adam training on the GPU from `model` (updated in place: bf16 weights are
+ * the rounded fp32 master weights).  epoch_loss (host, epochs floats, may be
+ * NULL) receives each epoch's mean loss. */
+int pf_cdef_mlp_train(pf_ctx* ctx, pf_cdef_mlp* model, const float* features,
+                      const uint8_t* labels, int32_t n, const pf_cdef_mlp_train_params* params,
+                      float* epoch_loss);
+
+/* The learned search: arguments and outputs as pf_cdef_search, plus the
+ * network, the confidence threshold (a block falls back to all trials when
+ * either head's top-1 probability is below it; above 1 every block falls
+ * back) and the number of top trials measured per head for a confident
+ * block (1..8).  Unmeasured entries of mse_out hold 66585600 (the
+ * reference's untested-trial figure). */
+int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
+                           const uint8_t* noskip, const pf_cdef_search_params* params,
+                           const pf_cdef_mlp* model, float threshold, int32_t candidates,
+                           uint64_t* mse_out, uint8_t* fb_index_out,
+                           pf_cdef_search_result* result, pf_cdef_learned_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,15 @@ int oracle_cdef_search(const pf_frame* source, const pf_frame* recon, const uint
                        const pf_cdef_search_params* params, uint64_t* mse_out,
                        uint8_t* fb_index_out, pf_cdef_search_result* result);
 
+/* Learned CDEF selection (oracle/learned_oracle.cpp); see pf_cdef_features
+ * and the pf_cdef_mlp_* entry points.  grads: PF_MLP_PARAMS floats. */
+int oracle_cdef_features(const pf_frame* recon, const uint8_t* noskip, int qindex, int damping, float* X);
+void oracle_mlp_forward(const pf_cdef_mlp* m, const float* X, int n, float* probs);
+void oracle_mlp_gradients(const pf_cdef_mlp* m, const float* X, const uint8_t* labels, int n, float* loss,
+                          float* grads);
+void oracle_mlp_loss_grad_f64(const double* params, const double* shift, const double* scale, const float* X,
+                              const uint8_t* labels, int n, double* loss, double* grads);
+
 #ifdef __cplusplus
 }
 #endif
