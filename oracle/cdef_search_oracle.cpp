@@ -304,14 +304,21 @@ extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, cons
       }
     }
   }
-  // finish (cdef_search.go:886-945).
+  return oracle_cdef_select(mse_out, skipFB.data(), nfb, prm, fb_index_out, result);
+}
+
+// finish (cdef_search.go:886-945) over a given SSE table.
+extern "C" int oracle_cdef_select(const uint64_t* mse, const uint8_t* skip, int nfb, const pf_cdef_search_params* prm,
+                                  uint8_t* fb_index_out, pf_cdef_search_result* result) {
+  int8_t fs[64];
+  trial_list(fs);
   std::vector<const uint64_t*> s0, s1;
   std::vector<int> sbIndex;
   for (int fb = 0; fb < nfb; fb++) {
     if (fb_index_out) fb_index_out[fb] = 0;
-    if (skipFB[fb]) continue;
-    s0.push_back(mse_out + (size_t)fb * 64);
-    s1.push_back(mse_out + (size_t)nfb * 64 + (size_t)fb * 64);
+    if (skip[fb]) continue;
+    s0.push_back(mse + (size_t)fb * 64);
+    s1.push_back(mse + (size_t)nfb * 64 + (size_t)fb * 64);
     sbIndex.push_back(fb);
   }
   const int sbCount = (int)s0.size();

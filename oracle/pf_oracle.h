@@ -70,6 +70,11 @@ int oracle_cdef_search(const pf_frame* source, const pf_frame* recon, const uint
                        const pf_cdef_search_params* params, uint64_t* mse_out,
                        uint8_t* fb_index_out, pf_cdef_search_result* result);
 
+/* finish() alone (encoder/cdef_search.go:886-945) over a given SSE table
+ * ([2][nfb][64]; skip[fb] != 0 leaves a block out). */
+int oracle_cdef_select(const uint64_t* mse, const uint8_t* skip, int nfb, const pf_cdef_search_params* params,
+                       uint8_t* fb_index_out, pf_cdef_search_result* result);
+
 /* Learned CDEF selection (oracle/learned_oracle.cpp); see pf_cdef_features
  * and the pf_cdef_mlp_* entry points.  grads: PF_MLP_PARAMS floats. */
 int oracle_cdef_features(const pf_frame* recon, const uint8_t* noskip, int qindex, int damping, float* X);

@@ -151,3 +151,21 @@ def test_committed_network_on_eval_frames(runner):
         assert st.blocks > 0
     assert max(inc_net) <= 0.005, inc_net
     assert np.mean(inc_net) <= np.mean(inc_prior), (inc_net, inc_prior)
+
+
+@pytest.mark.parametrize("w,h,cand", [(640, 360, 1), (1280, 720, 2)])
+def test_learned_selection_matches_oracle_finish(runner, oracle, w, h, cand):
+    """The greedy selection over the learned search's own table (tested
+    trials measured, the rest at the untested figure) equals the oracle's
+    finish() over that table."""
+    src, rec, ns = _pair(runner, 90 + w, w, h)
+    model = learned.load_model()
+    res, mse, idx, st = runner.cdef_search_learned(src.pf(), rec.pf(), ns, 128, 4000.0, model, candidates=cand)
+    skip = (mse[0].sum(1) == 0).astype(np.uint8)
+    res_o = abi.pf_cdef_search_result()
+    idx_o = np.zeros_like(idx)
+    prm = abi.pf_cdef_search_params(qindex=128, damping=0, max_presets=8, lam=4000.0)
+    assert oracle.oracle_cdef_select(mse.ctypes.data, skip.ctypes.data, mse.shape[1], C.byref(prm), idx_o.ctypes.data,
+                                     C.byref(res_o)) == 0
+    assert bytes(res) == bytes(res_o) and np.array_equal(idx, idx_o)
+    assert st.trials_luma < 64 * st.blocks
