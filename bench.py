@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-search", action="store_true")
+    ap.add_argument("--search-frames", type=int, default=8)
     return ap.parse_args()
 
 
@@ -363,36 +364,64 @@ def main():
         e2e = {"value": world * px / es / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "note": "pinned host frames, one pf_frame_apply call per frame"}
 
-    # Encoder CDEF strength search (BASELINE's second metric): 64x64 filter
-    # blocks searched per second, exhaustive level-1 search (64 luma x 64
-    # chroma strengths) plus the greedy 8-preset selection, on a 1080p 8-bit
-    # 4:2:0 source/reconstruction pair resident in HBM.
-    search = None
-    if not args.no_search:
-        from goav1_b200 import synth as _s
+    # Encoder CDEF strength search, exhaustive and learned, on the held-out
+    # learned-selection frames (1080p 8-bit 4:2:0, seeds 2000..): source
+    # without noise, reconstruction with 8x8 DC offsets and noise, deblocked
+    # by the library, both frames resident in HBM.  Blocks/s = the frame's
+    # 64x64 filter blocks (all of them, as the search visits them) per second
+    # of one search call, host round trip included (the call returns the
+    # decision).  The learned search's luma SSE increase is read from the
+    # exhaustive search's table.  Rank 0 only.
+    search = learned_leg = None
+    if not args.no_search and rank == 0:
+        from goav1_b200 import learned as _l
 
-        src, rec, sside, sigma = _s.make_search_pair(2000, 1920, 1080)
-        lf_runner = PostFilterRunner(device=local)
-        lf_runner.apply(rec.pf(), sside.side)  # deblock the reconstruction (library, host path)
-        lf_runner.close()
-        dsrc, drec = DeviceFrame(src), DeviceFrame(rec)
-        ucols, urows = (rec.width + 63) // 64, (rec.height + 63) // 64
-        ns = np.ctypeslib.as_array((C.c_uint8 * (ucols * urows * 8)).from_address(sside.side.cdef.noskip)).copy()
-        sp, rp = dsrc.pf(), drec.pf()
-        for _ in range(2):
-            runner.cdef_search(sp, rp, ns, 128, 4000.0)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        reps = max(3, args.steps)
-        for _ in range(reps):
-            res, _mse, _idx = runner.cdef_search(sp, rp, ns, 128, 4000.0)
-        torch.cuda.synchronize()
-        dt = (time.perf_counter() - t0) / reps
-        nfb = ucols * urows
-        search = {"metric": "CDEF search blocks/s", "value": nfb / dt, "unit": "blocks/s", "ms_per_frame": dt * 1e3,
-                  "config": "1920x1080 8-bit 4:2:0, level-1 exhaustive (64 luma x 64 chroma strengths) + "
-                            "greedy preset selection, qindex 128, noise sigma %g" % sigma,
-                  "presets": int(res.strength_count)}
+        model = _l.load_model()
+        rows = []
+        for seed, src, rec, sside, sigma in _l.search_frames(range(2000, 2000 + args.search_frames), 1920, 1080,
+                                                             workers=min(8, args.search_frames)):
+            runner.apply(rec.pf(), sside.side)  # deblock (loop-filter-only side info)
+            ns = _l.noskip_of(sside, rec)
+            q = _l.frame_qindex(seed)
+            dsrc, drec = DeviceFrame(src), DeviceFrame(rec)
+            sp, rp = dsrc.pf(), drec.pf()
+            r0, m0, i0 = runner.cdef_search(sp, rp, ns, q, _l.LAMBDA)
+            r1, _, i1, st = runner.cdef_search_learned(sp, rp, ns, q, _l.LAMBDA, model)
+
+            def timed(fn, reps=max(3, args.steps // 4)):
+                fn()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for _ in range(reps):
+                    fn()
+                torch.cuda.synchronize()
+                return (time.perf_counter() - t0) / reps
+
+            te = timed(lambda: runner.cdef_search(sp, rp, ns, q, _l.LAMBDA, want_mse=False))
+            tl = timed(lambda: runner.cdef_search_learned(sp, rp, ns, q, _l.LAMBDA, model, want_mse=False,
+                                                         want_stats=False))
+            base = _l.luma_sse(r0, i0, m0)
+            rows.append(dict(nfb=m0.shape[1], te=te, tl=tl, inc=_l.luma_sse(r1, i1, m0) / base - 1,
+                             blocks=st.blocks, fbl=st.fallback_luma, fbc=st.fallback_chroma,
+                             trials=(st.trials_luma * 4096 + st.trials_chroma * 2048) / (st.blocks * 64 * 6144)))
+        nfb = sum(r["nfb"] for r in rows)
+        te = sum(r["te"] for r in rows)
+        tl = sum(r["tl"] for r in rows)
+        blocks = sum(r["blocks"] for r in rows)
+        cfg = ("%d frames 1920x1080 8-bit 4:2:0 (seeds 2000-%d), qindex per frame in {64..192}, noise sigma in "
+               "{2,4,8}, device-resident, lambda %g" % (len(rows), 1999 + len(rows), _l.LAMBDA))
+        search = {"metric": "CDEF search blocks/s", "value": nfb / te, "unit": "blocks/s",
+                  "ms_per_frame": te / len(rows) * 1e3,
+                  "config": "level-1 exhaustive (64 luma x 64 chroma strengths) + greedy preset selection; " + cfg}
+        learned_leg = {"metric": "learned CDEF search blocks/s", "value": nfb / tl, "unit": "blocks/s",
+                       "ms_per_frame": tl / len(rows) * 1e3, "speedup_vs_exhaustive": te / tl,
+                       "luma_sse_increase_mean": float(np.mean([r["inc"] for r in rows])),
+                       "luma_sse_increase_max": float(np.max([r["inc"] for r in rows])),
+                       "fallback_luma_frac": sum(r["fbl"] for r in rows) / blocks,
+                       "fallback_chroma_frac": sum(r["fbc"] for r in rows) / blocks,
+                       "trial_work_frac": float(np.mean([r["trials"] for r in rows])),
+                       "config": "network goav1_b200/data/cdef_mlp_1080p.bin, threshold 0.5, 3 candidates per "
+                                 "head; " + cfg}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -405,6 +434,7 @@ def main():
                            "l2": "inputs (%.0f MB per rank) larger than L2, and a 256 MB L2 flush between steps"
                                  % (sum(fr.nbytes() for fr, _ in frames) / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "cdef_search": search,
+                "cdef_search_learned": learned_leg,
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))
     runner.close()

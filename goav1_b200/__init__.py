@@ -54,7 +54,8 @@ def lib():
                                     C.POINTER(abi.pf_cdef_mlp_train_params), C.c_void_p]
     L.pf_cdef_search_learned.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame), C.c_void_p,
                                          C.POINTER(abi.pf_cdef_search_params), C.POINTER(abi.pf_cdef_mlp), C.c_float,
-                                         C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(abi.pf_cdef_search_result),
+                                         C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                         C.POINTER(abi.pf_cdef_search_result),
                                          C.POINTER(abi.pf_cdef_learned_stats)]
     if L.pf_abi_version() != 1:
         raise RuntimeError("goav1_b200: ABI version mismatch")

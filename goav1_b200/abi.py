@@ -205,6 +205,7 @@ class pf_cdef_search_result(C.Structure):
     ]
 
 
+PF_LEARNED_REFINE = 1
 PF_MLP_FEATURES = 40
 PF_MLP_HIDDEN = 64
 PF_MLP_CLASSES = 64
@@ -253,7 +254,8 @@ class pf_cdef_mlp_train_params(C.Structure):
 class pf_cdef_learned_stats(C.Structure):
     _fields_ = [
         ("blocks", C.c_int32),
-        ("fallback", C.c_int32),
+        ("fallback_luma", C.c_int32),
+        ("fallback_chroma", C.c_int32),
         ("trials_luma", C.c_int32),
         ("trials_chroma", C.c_int32),
     ]

@@ -73,6 +73,11 @@ struct pf_ctx {
   DevBuf sidebuf;            // host side information copied up
   DevBuf jobs, bases, counters;
   DevBuf search;             // encoder CDEF search scratch
+  DevBuf model;              // the learned search's network, uploaded when it changes
+  std::vector<uint8_t> model_shadow;  // host copy of what `model` holds
+  void* pinned = nullptr;    // page-locked staging for small host inputs
+  size_t pinned_n = 0;
+  void* model_pin = nullptr; // page-locked staging of the network upload
   std::vector<FrameJob> hjobs;
   std::vector<int> hbase;
   std::vector<uint8_t> hside;
@@ -338,6 +343,9 @@ extern "C" void pf_destroy(pf_ctx* c) {
   cudaStreamSynchronize(c->side);
   DevBuf* bufs[] = {&c->io, &c->disp, &c->arena, &c->sidebuf, &c->jobs, &c->bases, &c->counters, &c->search};
   for (DevBuf* b : bufs) b->release();
+  c->model.release();
+  if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->model_pin) cudaFreeHost(c->model_pin);
   for (int i = 0; i < 8; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   cudaEventDestroy(c->fork);
@@ -844,3 +852,38 @@ void* pf_internal_search_scratch(pf_ctx* c, size_t bytes) {
   return c->search.p;
 }
 void* pf_internal_stream(pf_ctx* c) { return (void*)c->stream; }
+
+// Page-locked host staging of at least `bytes` (grown, never shrunk), so
+// small host inputs go up with an asynchronous copy.  Valid until the next
+// call; the entry points using it end with a stream synchronisation.
+void* pf_internal_pinned(pf_ctx* c, size_t bytes) {
+  if (bytes > c->pinned_n) {
+    if (c->pinned) cudaFreeHost(c->pinned);
+    c->pinned = nullptr;
+    c->pinned_n = 0;
+    const size_t n = (bytes + 4095) & ~(size_t)4095;
+    if (cudaMallocHost(&c->pinned, n) != cudaSuccess) return nullptr;
+    c->pinned_n = n;
+  }
+  return c->pinned;
+}
+
+// Device copy of `bytes` of host data that rarely changes (the learned
+// search's network): uploaded only when it differs from the last upload.
+void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, cudaStream_t st) {
+  if (c->model.ensure(bytes) != cudaSuccess) return nullptr;
+  if (c->model_shadow.size() == bytes && memcmp(c->model_shadow.data(), host, bytes) == 0) return c->model.p;
+  if (c->model_shadow.size() != bytes) {
+    if (c->model_pin) cudaFreeHost(c->model_pin);
+    c->model_pin = nullptr;
+    if (cudaMallocHost(&c->model_pin, bytes) != cudaSuccess) return nullptr;
+  }
+  c->model_shadow.assign((const uint8_t*)host, (const uint8_t*)host + bytes);
+  memcpy(c->model_pin, host, bytes);
+  if (cudaMemcpyAsync(c->model.p, c->model_pin, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    c->model_shadow.clear();
+    return nullptr;
+  }
+  return c->model.p;
+}

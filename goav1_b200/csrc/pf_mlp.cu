@@ -11,8 +11,8 @@
 //   k_feat_frame     frame means of seven of them (features 33..39).
 //   k_mlp_masks      forward pass per 32 blocks, softmax heads, and the
 //                    tested-trial masks: the top `candidates` trials of each
-//                    head, or all 64 + 64 when a head's top-1 probability is
-//                    below the threshold.
+//                    head, or all 64 trials of a head whose top-1
+//                    probability is below the threshold.
 //   k_mlp_train_step forward + backward over 32 samples per CTA, partial
 //                    gradients per CTA (no atomics: the reduction order is
 //                    fixed, so training is deterministic).
@@ -59,10 +59,11 @@ __device__ __forceinline__ void acc_add(unsigned long long* p, unsigned long lon
   if (v) atomicAdd(p, v);
 }
 
-__global__ void __launch_bounds__(256) k_cdef_features(SearchArgs a, int qindex, float* X) {
+__global__ void __launch_bounds__(256, 4) k_cdef_features(SearchArgs a, int qindex, float* X) {
   __shared__ FeatAcc A;
   __shared__ int32_t s_cost[64 * 8];
-  __shared__ int s_bsum[64], s_bsq[64];
+  __shared__ uint8_t s_y[64 * 64];      // the filter block's luma (allocated part)
+  __shared__ uint8_t s_c[2][32 * 32];   // and chroma
   const int tid = threadIdx.x;
   const int fb = blockIdx.x;
   const int fbr = fb / a.nhfb, fbc = fb - fbr * a.nhfb;
@@ -77,54 +78,109 @@ __global__ void __launch_bounds__(256) k_cdef_features(SearchArgs a, int qindex,
     unsigned long long* z = reinterpret_cast<unsigned long long*>(&A);
     for (int i = tid; i < (int)(sizeof(FeatAcc) / 8); i += 256) z[i] = 0;
   }
-  if (tid < 64) s_bsum[tid] = s_bsq[tid] = 0;
-  __syncthreads();
   const DPlane& Y = a.rec.pl[0];
   const int x0 = lc * 4, y0 = lr * 4;
   const int W = a.rec.width, H = a.rec.height;
   const int wc = imin(64, W - x0), hc = imin(64, H - y0);
-  // Direction costs of the searched blocks (the search's own arithmetic).
-  for (int wi = tid; wi < 64 * 8; wi += 256) {
-    const int b = wi >> 3, d = wi & 7;
-    if ((listed >> b) & 1)
-      s_cost[wi] = dir_cost8_dev(d, row_ptr<uint8_t>(Y, y0 + (b >> 3) * 8) + x0 + (b & 7) * 8, Y.stride);
-  }
-  // Block sums for the 8x8 luma block variance (one row of a block per item).
-  for (int wi = tid; wi < 64 * 8; wi += 256) {
-    const int b = wi >> 3, r = wi & 7;
-    if ((listed >> b) & 1) {
-      const uint8_t* row = row_ptr<uint8_t>(Y, y0 + (b >> 3) * 8 + r) + x0 + (b & 7) * 8;
-      int s = 0, q = 0;
-      for (int j = 0; j < 8; j++) {
-        s += row[j];
-        q += row[j] * row[j];
+  const int x0c = x0 >> 1, y0c = y0 >> 1;
+  const int wcc = imin(32, a.rec.pl[1].w - x0c), hcc = imin(32, a.rec.pl[1].h - y0c);
+  // Stage the block once, row-coalesced: every statistic reads shared memory.
+  {
+    const int rh = imin(64, Y.ah - y0), rw = imin(64, Y.aw - x0);
+    for (int e = tid; e < rh * 64; e += 256) {
+      const int i = e >> 6, j = e & 63;
+      s_y[e] = j < rw ? row_ptr<uint8_t>(Y, y0 + i)[x0 + j] : 0;
+    }
+    for (int pl = 1; pl < 3; pl++) {
+      const DPlane& Cp = a.rec.pl[pl];
+      const int ch = imin(32, Cp.ah - y0c), cw = imin(32, Cp.aw - x0c);
+      for (int e = tid; e < ch * 32; e += 256) {
+        const int i = e >> 5, j = e & 31;
+        s_c[pl - 1][e] = j < cw ? row_ptr<uint8_t>(Cp, y0c + i)[x0c + j] : 0;
       }
-      atomicAdd(&s_bsum[b], s);
-      atomicAdd(&s_bsq[b], q);
     }
   }
   __syncthreads();
-  if (tid < 64 && ((listed >> tid) & 1)) {
+  // Direction costs of the searched blocks (the search's own arithmetic).
+  for (int wi = tid; wi < 64 * 8; wi += 256) {
+    const int b = wi >> 3, d = wi & 7;
+    if ((listed >> b) & 1) s_cost[wi] = dir_cost8_dev(d, &s_y[(b >> 3) * 8 * 64 + (b & 7) * 8], 64);
+  }
+  __syncthreads();
+  if (tid < 64) {
+    // Per searched 8x8 block (two warps, a lane per block), then warp sums:
+    // one shared atomic per warp and counter.
+    const bool on = (listed >> tid) & 1;
+    unsigned long long dc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long var64 = 0, nvar0 = 0, adj = 0, bvar = 0, cv[2] = {0, 0};
     int best = 0;
-    int32_t bc = s_cost[tid * 8];
-    for (int d = 1; d < 8; d++)
-      if (s_cost[tid * 8 + d] > bc) {
-        best = d;
-        bc = s_cost[tid * 8 + d];
+    if (on) {
+      int32_t bc = s_cost[tid * 8];
+      for (int d = 1; d < 8; d++)
+        if (s_cost[tid * 8 + d] > bc) {
+          best = d;
+          bc = s_cost[tid * 8 + d];
+        }
+      const int32_t var = (bc - s_cost[tid * 8 + ((best + 4) & 7)]) >> 10;
+      for (int d = 0; d < 8; d++) dc[d] = (unsigned long long)s_cost[tid * 8 + d];
+      var64 = (unsigned long long)var;
+      int ai = -1;
+      if (var == 0) {
+        nvar0 = 1;
+      } else {
+        const int32_t v = var >> 6;
+        ai = v ? imin(31 - __clz(v), 12) : 0;
+        adj = (unsigned long long)(4 + ai);
       }
-    const int32_t var = (bc - s_cost[tid * 8 + ((best + 4) & 7)]) >> 10;
-    for (int d = 0; d < 8; d++) atomicAdd(&A.dcost[d], (unsigned long long)s_cost[tid * 8 + d]);
-    atomicAdd(&A.dhist[best], 1ull);
-    acc_add(&A.varsum, (unsigned long long)var);
-    if (var == 0) {
-      atomicAdd(&A.nvar0, 1ull);
-    } else {
-      const int32_t v = var >> 6;
-      const int ai = v ? imin(31 - __clz(v), 12) : 0;
-      atomicAdd(&A.adjsum, (unsigned long long)(4 + ai));
+      if (a.dirs) {
+        a.dirs[(size_t)fb * 64 + tid] = (uint8_t)best;
+        a.ais[(size_t)fb * 64 + tid] = (int8_t)ai;
+      }
+      // 8x8 luma variance and 4x4 chroma variances of the block.
+      const uint8_t* by = &s_y[(tid >> 3) * 8 * 64 + (tid & 7) * 8];
+      long long s = 0, q = 0;
+      for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 8; j++) {
+          const int x = by[i * 64 + j];
+          s += x;
+          q += x * x;
+        }
+      bvar = (unsigned long long)(64 * q - s * s);
+      for (int pl = 0; pl < 2; pl++) {
+        const uint8_t* bc2 = &s_c[pl][(tid >> 3) * 4 * 32 + (tid & 7) * 4];
+        int cs = 0, cq = 0;
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++) {
+            const int x = bc2[i * 32 + j];
+            cs += x;
+            cq += x * x;
+          }
+        cv[pl] = (unsigned long long)(16 * cq - cs * cs);
+      }
     }
-    const long long bs = s_bsum[tid];
-    acc_add(&A.bvar, (unsigned long long)(64ll * s_bsq[tid] - bs * bs));
+    // Direction histogram: each lane's best direction as a ballot per value.
+    unsigned long long hist[8];
+#pragma unroll
+    for (int d = 0; d < 8; d++) hist[d] = __popc(__ballot_sync(0xffffffffu, on && best == d));
+    unsigned long long v[15] = {dc[0], dc[1], dc[2], dc[3], dc[4], dc[5], dc[6], dc[7], var64, nvar0, adj, bvar,
+                                cv[0], cv[1], 0};
+#pragma unroll
+    for (int k = 0; k < 14; k++)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if ((tid & 31) == 0) {
+#pragma unroll
+      for (int d = 0; d < 8; d++) {
+        acc_add(&A.dcost[d], v[d]);
+        acc_add(&A.dhist[d], hist[d]);
+      }
+      acc_add(&A.varsum, v[8]);
+      acc_add(&A.nvar0, v[9]);
+      acc_add(&A.adjsum, v[10]);
+      acc_add(&A.bvar, v[11]);
+      acc_add(&A.uvar, v[12]);
+      acc_add(&A.vvar, v[13]);
+    }
   }
   // Pixel statistics over the cropped luma region.
   {
@@ -133,7 +189,7 @@ __global__ void __launch_bounds__(256) k_cdef_features(SearchArgs a, int qindex,
     for (int e = tid; e < hc * 64; e += 256) {
       const int i = e >> 6, j = e & 63;
       if (j >= wc) continue;
-      const uint8_t* r0 = row_ptr<uint8_t>(Y, y0 + i) + x0;
+      const uint8_t* r0 = &s_y[i * 64];
       const int x = r0[j];
       sy += x;
       if (j + 1 < wc) {
@@ -146,7 +202,7 @@ __global__ void __launch_bounds__(256) k_cdef_features(SearchArgs a, int qindex,
         }
       }
       if (i + 1 < hc) {
-        const unsigned d = abs(row_ptr<uint8_t>(Y, y0 + i + 1)[x0 + j] - x);
+        const unsigned d = abs(r0[64 + j] - x);
         gV += d;
         cV++;
         if (((y0 + i + 1) & 7) == 0) {
@@ -155,74 +211,51 @@ __global__ void __launch_bounds__(256) k_cdef_features(SearchArgs a, int qindex,
         }
       }
       if (i >= 1 && i + 1 < hc && j >= 1 && j + 1 < wc) {
-        const uint8_t* ru = row_ptr<uint8_t>(Y, y0 + i - 1) + x0;
-        const uint8_t* rd = row_ptr<uint8_t>(Y, y0 + i + 1) + x0;
+        const uint8_t* ru = r0 - 64;
+        const uint8_t* rd = r0 + 64;
         const int L = ru[j - 1] - 2 * ru[j] + ru[j + 1] - 2 * r0[j - 1] + 4 * x - 2 * r0[j + 1] + rd[j - 1] -
                       2 * rd[j] + rd[j + 1];
         lap += (unsigned)abs(L);
         clap++;
       }
     }
-    acc_add(&A.gH, gH);
-    acc_add(&A.cH, cH);
-    acc_add(&A.gV, gV);
-    acc_add(&A.cV, cV);
-    acc_add(&A.bH, bH);
-    acc_add(&A.cbH, cbH);
-    acc_add(&A.bV, bV);
-    acc_add(&A.cbV, cbV);
-    acc_add(&A.lap, lap);
-    acc_add(&A.clap, clap);
-    acc_add(&A.sumY, sy);
-  }
-  // Chroma: 4x4 block variances of the searched blocks, Laplacian and
-  // neighbour differences over the cropped region of U and V.
-  {
-    const int x0c = x0 >> 1, y0c = y0 >> 1;
-    const int Wc = a.rec.pl[1].w, Hc = a.rec.pl[1].h;
-    const int wcc = imin(32, Wc - x0c), hcc = imin(32, Hc - y0c);
+    // Chroma: Laplacian and neighbour differences over the cropped region.
     unsigned long long cl = 0, ccl = 0, cg = 0, ccg = 0;
-    for (int pl = 1; pl < 3; pl++) {
-      const DPlane& Cp = a.rec.pl[pl];
-      if (tid < 64 && ((listed >> tid) & 1)) {
-        const int b = tid;
-        int s = 0, q = 0;
-        for (int i = 0; i < 4; i++) {
-          const uint8_t* row = row_ptr<uint8_t>(Cp, y0c + (b >> 3) * 4 + i) + x0c + (b & 7) * 4;
-          for (int j = 0; j < 4; j++) {
-            s += row[j];
-            q += row[j] * row[j];
-          }
-        }
-        acc_add(pl == 1 ? &A.uvar : &A.vvar, (unsigned long long)(16 * q - s * s));
+    for (int e = tid; e < 2 * hcc * 32; e += 256) {
+      const int pl = e / (hcc * 32), r = e - pl * hcc * 32;
+      const int i = r >> 5, j = r & 31;
+      if (j >= wcc) continue;
+      const uint8_t* r0 = &s_c[pl][i * 32];
+      const int x = r0[j];
+      if (j + 1 < wcc) {
+        cg += (unsigned)abs(r0[j + 1] - x);
+        ccg++;
       }
-      for (int e = tid; e < hcc * 32; e += 256) {
-        const int i = e >> 5, j = e & 31;
-        if (j >= wcc) continue;
-        const uint8_t* r0 = row_ptr<uint8_t>(Cp, y0c + i) + x0c;
-        const int x = r0[j];
-        if (j + 1 < wcc) {
-          cg += (unsigned)abs(r0[j + 1] - x);
-          ccg++;
-        }
-        if (i + 1 < hcc) {
-          cg += (unsigned)abs(row_ptr<uint8_t>(Cp, y0c + i + 1)[x0c + j] - x);
-          ccg++;
-        }
-        if (i >= 1 && i + 1 < hcc && j >= 1 && j + 1 < wcc) {
-          const uint8_t* ru = row_ptr<uint8_t>(Cp, y0c + i - 1) + x0c;
-          const uint8_t* rd = row_ptr<uint8_t>(Cp, y0c + i + 1) + x0c;
-          const int L = ru[j - 1] - 2 * ru[j] + ru[j + 1] - 2 * r0[j - 1] + 4 * x - 2 * r0[j + 1] + rd[j - 1] -
-                        2 * rd[j] + rd[j + 1];
-          cl += (unsigned)abs(L);
-          ccl++;
-        }
+      if (i + 1 < hcc) {
+        cg += (unsigned)abs(r0[32 + j] - x);
+        ccg++;
+      }
+      if (i >= 1 && i + 1 < hcc && j >= 1 && j + 1 < wcc) {
+        const uint8_t* ru = r0 - 32;
+        const uint8_t* rd = r0 + 32;
+        const int L = ru[j - 1] - 2 * ru[j] + ru[j + 1] - 2 * r0[j - 1] + 4 * x - 2 * r0[j + 1] + rd[j - 1] -
+                      2 * rd[j] + rd[j + 1];
+        cl += (unsigned)abs(L);
+        ccl++;
       }
     }
-    acc_add(&A.clapUV, cl);
-    acc_add(&A.cclapUV, ccl);
-    acc_add(&A.cgUV, cg);
-    acc_add(&A.ccgUV, ccg);
+    // Warp sums first: one shared atomic per warp and counter.
+    unsigned long long v[15] = {gH, cH, gV, cV, bH, cbH, bV, cbV, lap, clap, sy, cl, ccl, cg, ccg};
+#pragma unroll
+    for (int k = 0; k < 15; k++)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if ((tid & 31) == 0) {
+      unsigned long long* dst[15] = {&A.gH, &A.cH, &A.gV, &A.cV, &A.bH, &A.cbH, &A.bV, &A.cbV, &A.lap, &A.clap,
+                                     &A.sumY, &A.clapUV, &A.cclapUV, &A.cgUV, &A.ccgUV};
+#pragma unroll
+      for (int k = 0; k < 15; k++) acc_add(dst[k], v[k]);
+    }
   }
   __syncthreads();
   if (tid == 0) {
@@ -253,14 +286,19 @@ __global__ void __launch_bounds__(256) k_cdef_features(SearchArgs a, int qindex,
 }
 
 // Frame means of features 16, 19, 22, 23, 24, 25, 27 over the searched
-// blocks, written as features 33..39 of every block.  Fixed-order sums.
+// blocks (features 33..39 of every block).  Fixed-order sums: 256 threads
+// stride over the blocks, then a tree in shared memory, so every caller gets
+// the same bits.
 __constant__ int c_frame_feat[7] = {16, 19, 22, 23, 24, 25, 27};
 
-__global__ void __launch_bounds__(256) k_feat_frame(float* X, int nfb) {
-  __shared__ double s_sum[7][256];
-  __shared__ int s_cnt[256];
-  __shared__ float s_mean[7];
-  const int t = threadIdx.x;
+struct FrameMeanSmem {
+  double sum[7][256];
+  int cnt[256];
+  float mean[7];
+};
+
+__device__ void frame_means(const float* X, int nfb, FrameMeanSmem& M) {
+  const int t = threadIdx.x;  // blockDim.x == 256
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   int c = 0;
   for (int fb = t; fb < nfb; fb += 256) {
@@ -270,36 +308,46 @@ __global__ void __launch_bounds__(256) k_feat_frame(float* X, int nfb) {
       for (int i = 0; i < 7; i++) acc[i] += (double)f[c_frame_feat[i]];
     }
   }
-  for (int i = 0; i < 7; i++) s_sum[i][t] = acc[i];
-  s_cnt[t] = c;
+  for (int i = 0; i < 7; i++) M.sum[i][t] = acc[i];
+  M.cnt[t] = c;
   __syncthreads();
   for (int o = 128; o > 0; o >>= 1) {
     if (t < o) {
-      for (int i = 0; i < 7; i++) s_sum[i][t] += s_sum[i][t + o];
-      s_cnt[t] += s_cnt[t + o];
+      for (int i = 0; i < 7; i++) M.sum[i][t] += M.sum[i][t + o];
+      M.cnt[t] += M.cnt[t + o];
     }
     __syncthreads();
   }
-  if (t < 7) s_mean[t] = s_cnt[0] ? (float)(s_sum[t][0] / (double)s_cnt[0]) : 0.f;
+  if (t < 7) M.mean[t] = M.cnt[0] ? (float)(M.sum[t][0] / (double)M.cnt[0]) : 0.f;
   __syncthreads();
-  for (int e = t; e < nfb * 7; e += 256) X[(size_t)(e / 7) * kF + kPerFb + e % 7] = s_mean[e % 7];
+}
+
+__global__ void __launch_bounds__(256) k_feat_frame(float* X, int nfb) {
+  __shared__ FrameMeanSmem M;
+  frame_means(X, nfb, M);
+  for (int e = threadIdx.x; e < nfb * 7; e += 256) X[(size_t)(e / 7) * kF + kPerFb + e % 7] = M.mean[e % 7];
 }
 
 // ---------------------------------------------------------------------------
 // The network.
 
-struct MlpTile {
+template <int TILE>
+struct MlpTileT {
   float w1[kNW1], w2[kNW2], w3[kNW3];
   float b1[kH], b2[kH], b3[kO];
-  float x[kTile][kF + 1];
-  float h1[kTile][kH + 1];
-  float h2[kTile][kH + 1];
-  float z[kTile][kO + 1];   // logits, then probabilities, then dL/dz
-  float dh2[kTile][kH + 1];
-  float dh1[kTile][kH + 1];
-  float loss[kTile];
-  int y[kTile][2];
+  float x[TILE][kF + 1];
+  float h1[TILE][kH + 1];
+  float h2[TILE][kH + 1];
+  float z[TILE][kO + 1];   // logits, then probabilities, then dL/dz
+  float dh2[TILE][kH + 1];
+  float dh1[TILE][kH + 1];
+  float lossh[TILE][2];
+  float loss[TILE];
+  int y[TILE][2];
 };
+using MlpTile = MlpTileT<kTile>;  // training tile
+constexpr int kInferTile = 8;    // inference: more CTAs, less serial work each
+using MlpInfer = MlpTileT<kInferTile>;
 
 __device__ __forceinline__ float bf16_to_f(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
 
@@ -307,43 +355,72 @@ __device__ __forceinline__ float bf16_to_f(uint16_t b) { return __uint_as_float(
 // samples (rows[first + s], or first + s), then the three layers.  Lanes of
 // a warp are samples, warps are output groups: a weight is a broadcast and
 // an activation row a conflict-free column.
-__device__ void mlp_forward(MlpTile& T, const pf_cdef_mlp* M, const float* X, const int* rows, int first, int count) {
+// Weights widened once to fp32 for the inference kernels: [w1 | w2 | w3 |
+// b1 | b2 | b3 | feat_shift | feat_scale], the layout of MlpTileT's weight
+// block followed by the normalisation.
+constexpr int kExpanded = kNP + 2 * kF;
+
+__global__ void k_mlp_expand(const pf_cdef_mlp* M, float* W) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kExpanded) return;
+  if (p < kNW)
+    W[p] = bf16_to_f(reinterpret_cast<const uint16_t*>(M)[p]);
+  else if (p < kNP)
+    W[p] = reinterpret_cast<const float*>(&M->b1[0])[p - kNW];
+  else
+    W[p] = reinterpret_cast<const float*>(&M->feat_shift[0])[p - kNP];  // shift, then scale
+}
+
+template <int TILE>
+__device__ void mlp_forward(MlpTileT<TILE>& T, const pf_cdef_mlp* M, const float* X, const int* rows, int first, int count,
+                            const float* means = nullptr, const float* Wf = nullptr) {
   const int t = threadIdx.x;
-  for (int e = t; e < kNW1; e += kMlpThreads) T.w1[e] = bf16_to_f(M->w1[e]);
-  for (int e = t; e < kNW2; e += kMlpThreads) T.w2[e] = bf16_to_f(M->w2[e]);
-  for (int e = t; e < kNW3; e += kMlpThreads) T.w3[e] = bf16_to_f(M->w3[e]);
-  if (t < kH) {
-    T.b1[t] = M->b1[t];
-    T.b2[t] = M->b2[t];
+  const float* shift = M ? M->feat_shift : Wf + kNP;
+  const float* scale = M ? M->feat_scale : Wf + kNP + kF;
+  if (Wf) {
+    // fp32 weights and biases, contiguous like the tile's: 16-byte copies.
+    const float4* src = reinterpret_cast<const float4*>(Wf);
+    float4* dst = reinterpret_cast<float4*>(&T.w1[0]);
+    for (int e = t; e < kNP / 4; e += kMlpThreads) dst[e] = src[e];
+  } else {
+    for (int e = t; e < kNW1; e += kMlpThreads) T.w1[e] = bf16_to_f(M->w1[e]);
+    for (int e = t; e < kNW2; e += kMlpThreads) T.w2[e] = bf16_to_f(M->w2[e]);
+    for (int e = t; e < kNW3; e += kMlpThreads) T.w3[e] = bf16_to_f(M->w3[e]);
+    if (t < kH) {
+      T.b1[t] = M->b1[t];
+      T.b2[t] = M->b2[t];
+    }
+    if (t < kO) T.b3[t] = M->b3[t];
   }
-  if (t < kO) T.b3[t] = M->b3[t];
-  for (int e = t; e < kTile * kF; e += kMlpThreads) {
+  for (int e = t; e < TILE * kF; e += kMlpThreads) {
     const int s = e / kF, k = e - s * kF;
     float v = 0.f;
     if (s < count) {
       const int r = rows ? rows[first + s] : first + s;
-      v = (X[(size_t)r * kF + k] - M->feat_shift[k]) * M->feat_scale[k];
+      const float f = (means && k >= kPerFb) ? means[k - kPerFb] : X[(size_t)r * kF + k];
+      v = (f - shift[k]) * scale[k];
     }
     T.x[s][k] = v;
   }
   __syncthreads();
-  const int s = t & 31, og = t >> 5;
-  for (int q = 0; q < kH / 8; q++) {
-    const int o = og * (kH / 8) + q;
+  constexpr int G = kMlpThreads / TILE;  // output groups
+  const int s = t % TILE, og = t / TILE;
+  for (int q = 0; q < kH / G; q++) {
+    const int o = og * (kH / G) + q;
     float acc = T.b1[o];
     for (int k = 0; k < kF; k++) acc = __fmaf_rn(T.w1[o * kF + k], T.x[s][k], acc);
     T.h1[s][o] = acc > 0.f ? acc : 0.f;
   }
   __syncthreads();
-  for (int q = 0; q < kH / 8; q++) {
-    const int o = og * (kH / 8) + q;
+  for (int q = 0; q < kH / G; q++) {
+    const int o = og * (kH / G) + q;
     float acc = T.b2[o];
     for (int k = 0; k < kH; k++) acc = __fmaf_rn(T.w2[o * kH + k], T.h1[s][k], acc);
     T.h2[s][o] = acc > 0.f ? acc : 0.f;
   }
   __syncthreads();
-  for (int q = 0; q < kO / 8; q++) {
-    const int o = og * (kO / 8) + q;
+  for (int q = 0; q < kO / G; q++) {
+    const int o = og * (kO / G) + q;
     float acc = T.b3[o];
     for (int k = 0; k < kH; k++) acc = __fmaf_rn(T.w3[o * kH + k], T.h2[s][k], acc);
     T.z[s][o] = acc;
@@ -351,68 +428,95 @@ __device__ void mlp_forward(MlpTile& T, const pf_cdef_mlp* M, const float* X, co
   __syncthreads();
 }
 
-// Softmax of both heads in place; with labels, the per-sample loss
-// (log-sum-exp minus the label's logit, both heads).
-__device__ void mlp_softmax(MlpTile& T, bool withLoss) {
-  const int t = threadIdx.x;
-  if (t < 2 * kTile) {
-    const int s = t & 31, hd = t >> 5;
+// Softmax of both heads in place, one warp per (sample, head): lane l holds
+// classes l and l + 32; the maximum and the sum are butterfly reductions
+// (sum order: e[l] + e[l+32], then xor-partners at distances 16..1).  With
+// labels, the per-sample loss (log-sum-exp minus the label's logit, both
+// heads).
+template <int TILE>
+__device__ void mlp_softmax(MlpTileT<TILE>& T, bool withLoss) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int task = warp; task < 2 * TILE; task += kMlpThreads / 32) {
+    const int s = task >> 1, hd = task & 1;
     float* z = &T.z[s][hd * kC];
-    float m = z[0];
-    for (int o = 1; o < kC; o++) m = fmaxf(m, z[o]);
-    float sum = 0.f;
-    for (int o = 0; o < kC; o++) sum += expf(z[o] - m);
-    if (withLoss) T.dh1[s][hd] = m + logf(sum) - z[T.y[s][hd]];  // dh1 is free until backward
+    const float z0 = z[lane], z1 = z[lane + 32];
+    float m = fmaxf(z0, z1);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const float e0 = expf(z0 - m), e1 = expf(z1 - m);
+    float sum = e0 + e1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (withLoss && lane == 0) T.lossh[s][hd] = m + logf(sum) - z[T.y[s][hd]];
+    __syncwarp();
     const float inv = 1.f / sum;
-    for (int o = 0; o < kC; o++) z[o] = expf(z[o] - m) * inv;
+    z[lane] = e0 * inv;
+    z[lane + 32] = e1 * inv;
   }
   __syncthreads();
-  if (withLoss && t < kTile) T.loss[t] = T.dh1[t][0] + T.dh1[t][1];
+  if (withLoss && threadIdx.x < TILE) T.loss[threadIdx.x] = T.lossh[threadIdx.x][0] + T.lossh[threadIdx.x][1];
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_masks(const pf_cdef_mlp* M, const float* X, int nfb,
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_masks(const float* W, const float* X, int nfb,
                                                            float threshold, int candidates, uint64_t* masks) {
   extern __shared__ __align__(16) unsigned char smem[];
-  MlpTile& T = *reinterpret_cast<MlpTile*>(smem);
-  __shared__ uint64_t s_m[kTile][2];
-  __shared__ int s_conf[kTile][2];
-  const int first = blockIdx.x * kTile, count = imin(kTile, nfb - first);
-  mlp_forward(T, M, X, nullptr, first, count);
+  MlpInfer& T = *reinterpret_cast<MlpInfer*>(smem);
+  __shared__ FrameMeanSmem FM;
+  __shared__ uint64_t s_m[kInferTile][2];
+  __shared__ int s_conf[kInferTile][2];
+  const int first = blockIdx.x * kInferTile, count = imin(kInferTile, nfb - first);
+  frame_means(X, nfb, FM);  // features 33..39 (the features kernel leaves them unset)
+  mlp_forward(T, nullptr, X, nullptr, first, count, FM.mean, W);
   mlp_softmax(T, false);
-  const int t = threadIdx.x;
-  if (t < 2 * kTile) {
-    const int s = t & 31, hd = t >> 5;
-    const float* p = &T.z[s][hd * kC];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int task = warp; task < 2 * kInferTile; task += kMlpThreads / 32) {
+    const int s = task >> 1, hd = task & 1;
+    float p0 = T.z[s][hd * kC + lane], p1 = T.z[s][hd * kC + lane + 32];
     uint64_t m = 0;
     float top = 0.f;
     for (int c = 0; c < candidates; c++) {
-      int bi = 0;
-      float bv = -1.f;
-      for (int o = 0; o < kC; o++)
-        if (!((m >> o) & 1) && p[o] > bv) {
-          bv = p[o];
-          bi = o;
+      // Largest remaining probability, the lower class on ties.
+      float v = p0;
+      int i = lane;
+      if (p1 > v) {
+        v = p1;
+        i = lane + 32;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+        if (v2 > v || (v2 == v && i2 < i)) {
+          v = v2;
+          i = i2;
         }
-      if (c == 0) top = bv;
-      m |= 1ull << bi;
+      }
+      if (c == 0) top = v;
+      m |= 1ull << i;
+      if (i == lane) p0 = -1.f;
+      if (i == lane + 32) p1 = -1.f;
     }
-    s_m[s][hd] = m;
-    s_conf[s][hd] = top >= threshold;
+    if (lane == 0) {
+      s_m[s][hd] = m;
+      s_conf[s][hd] = top >= threshold;
+    }
   }
   __syncthreads();
+  const int t = threadIdx.x;
   if (t < count) {
-    const bool conf = s_conf[t][0] && s_conf[t][1];
-    masks[2 * (size_t)(first + t)] = conf ? s_m[t][0] : ~0ull;
-    masks[2 * (size_t)(first + t) + 1] = conf ? s_m[t][1] : ~0ull;
+    // Each head falls back on its own: an unsure luma head measures all 64
+    // luma trials while a confident chroma head keeps its candidates.
+    masks[2 * (size_t)(first + t)] = s_conf[t][0] ? s_m[t][0] : ~0ull;
+    masks[2 * (size_t)(first + t) + 1] = s_conf[t][1] ? s_m[t][1] : ~0ull;
   }
 }
 
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_probs(const pf_cdef_mlp* M, const float* X, int n, float* P) {
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_probs(const float* W, const float* X, int n, float* P) {
   extern __shared__ __align__(16) unsigned char smem[];
-  MlpTile& T = *reinterpret_cast<MlpTile*>(smem);
-  const int first = blockIdx.x * kTile, count = imin(kTile, n - first);
-  mlp_forward(T, M, X, nullptr, first, count);
+  MlpInfer& T = *reinterpret_cast<MlpInfer*>(smem);
+  const int first = blockIdx.x * kInferTile, count = imin(kInferTile, n - first);
+  mlp_forward(T, nullptr, X, nullptr, first, count, nullptr, W);
   mlp_softmax(T, false);
   for (int e = threadIdx.x; e < count * kO; e += kMlpThreads) P[(size_t)first * kO + e] = T.z[e / kO][e % kO];
 }
@@ -560,23 +664,32 @@ __global__ void k_master_init(const pf_cdef_mlp* M, float* master) {
                       : reinterpret_cast<const float*>(&M->b1[0])[p - kNW];
 }
 
-static cudaError_t set_tile_smem(const void* fn) {
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpTile));
+static cudaError_t set_tile_smem(const void* fn, size_t bytes = sizeof(MlpTile)) {
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-cudaError_t launch_features(const SearchArgs& a, int qindex, float* X, cudaStream_t st) {
+cudaError_t launch_features(const SearchArgs& a, int qindex, float* X, bool frameMeans, cudaStream_t st) {
   const int nfb = a.nhfb * a.nvfb;
   k_cdef_features<<<nfb, 256, 0, st>>>(a, qindex, X);
-  k_feat_frame<<<1, 256, 0, st>>>(X, nfb);
+  if (frameMeans) k_feat_frame<<<1, 256, 0, st>>>(X, nfb);
   return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, const float* X, int nfb, float threshold, int candidates,
-                             uint64_t* masks, cudaStream_t st) {
-  const cudaError_t e = set_tile_smem((const void*)k_mlp_masks);
-  if (e != cudaSuccess) return e;
-  k_mlp_masks<<<(nfb + kTile - 1) / kTile, kMlpThreads, sizeof(MlpTile), st>>>(dmodel, X, nfb, threshold, candidates,
-                                                                               masks);
+size_t mlp_expanded_bytes() { return (size_t)kExpanded * sizeof(float); }
+
+cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, float* W, const float* X, int nfb, float threshold,
+                             int candidates, uint64_t* masks, cudaStream_t st) {
+  static thread_local int ready = -1;  // device whose attribute is set
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (ready != dev) {
+    const cudaError_t e = set_tile_smem((const void*)k_mlp_masks, sizeof(MlpInfer));
+    if (e != cudaSuccess) return e;
+    ready = dev;
+  }
+  k_mlp_expand<<<(kExpanded + 255) / 256, 256, 0, st>>>(dmodel, W);
+  k_mlp_masks<<<(nfb + kInferTile - 1) / kInferTile, kMlpThreads, sizeof(MlpInfer), st>>>(W, X, nfb, threshold,
+                                                                                       candidates, masks);
   return cudaGetLastError();
 }
 
@@ -627,14 +740,16 @@ extern "C" int pf_cdef_mlp_forward(pf_ctx* ctx, const pf_cdef_mlp* model, const 
   const cudaStream_t st = (cudaStream_t)pf_internal_stream(ctx);
   Scratch S;
   pf_cdef_mlp* dm = S.get<pf_cdef_mlp>(1);
+  float* W = S.get<float>(kExpanded);
   float* X = S.get<float>((size_t)n * kF);
   float* P = S.get<float>((size_t)n * kO);
   if (S.err != cudaSuccess) return PF_ERR_DEVICE;
   if (cudaMemcpyAsync(dm, model, sizeof(*model), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(X, features, (size_t)n * kF * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      set_tile_smem((const void*)k_mlp_probs) != cudaSuccess)
+      set_tile_smem((const void*)k_mlp_probs, sizeof(MlpInfer)) != cudaSuccess)
     return PF_ERR_DEVICE;
-  k_mlp_probs<<<(n + kTile - 1) / kTile, kMlpThreads, sizeof(MlpTile), st>>>(dm, X, n, P);
+  k_mlp_expand<<<(kExpanded + 255) / 256, 256, 0, st>>>(dm, W);
+  k_mlp_probs<<<(n + kInferTile - 1) / kInferTile, kMlpThreads, sizeof(MlpInfer), st>>>(W, X, n, P);
   if (cudaGetLastError() != cudaSuccess ||
       cudaMemcpyAsync(probs, P, (size_t)n * kO * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)

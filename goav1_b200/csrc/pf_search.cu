@@ -38,8 +38,8 @@ namespace pf {
 
 __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   __shared__ uint16_t s_in[kSH * kSW];
-  __shared__ uint8_t s_src[64 * 64];
-  __shared__ uint8_t s_rec[64 * 64];  // the reconstruction itself (unfiltered trials measure it)
+  __shared__ __align__(16) uint8_t s_src[64 * 64];
+  __shared__ __align__(16) uint8_t s_rec[64 * 64];  // the reconstruction itself (unfiltered trials measure it)
   __shared__ int32_t s_cost[64 * 8];
   __shared__ uint8_t s_dir[64];
   __shared__ int8_t s_ai[64];   // adjustStrength index, -1 for zero variance
@@ -89,21 +89,52 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
     const int planeW = rp.w, planeH = rp.h;
     __syncthreads();  // the previous plane's tasks are done with the buffers
     // loadCDEFInput: frame samples where they exist, VeryLarge elsewhere.
+    // A row wholly inside the plane whose start is 4-byte aligned is read
+    // four samples at a time (w + 16 is a multiple of 4).
     for (int r = warp; r < h + 4; r += 8) {
       const int yy = y0 - 2 + r;
       const bool rowIn = yy >= 0 && yy < planeH;
       const uint8_t* srow = rowIn ? row_ptr<uint8_t>(rp, yy) : nullptr;
-      for (int c = lane; c < w + 16; c += 32) {
-        const int xx = x0 - 8 + c;
-        s_in[r * kSW + c] = (rowIn && xx >= 0 && xx < planeW) ? srow[xx] : (uint16_t)kVeryLarge;
+      const int xs = x0 - 8;
+      if (rowIn && xs >= 0 && xs + w + 16 <= planeW && (((uintptr_t)(srow + xs)) & 3) == 0) {
+        const uint32_t* q = reinterpret_cast<const uint32_t*>(srow + xs);
+        for (int c4 = lane; c4 < (w + 16) >> 2; c4 += 32) {
+          const uint32_t v = q[c4];
+          uint16_t* d = &s_in[r * kSW + 4 * c4];
+          d[0] = v & 0xff;
+          d[1] = (v >> 8) & 0xff;
+          d[2] = (v >> 16) & 0xff;
+          d[3] = v >> 24;
+        }
+      } else {
+        for (int c = lane; c < w + 16; c += 32) {
+          const int xx = xs + c;
+          s_in[r * kSW + c] = (rowIn && xx >= 0 && xx < planeW) ? srow[xx] : (uint16_t)kVeryLarge;
+        }
       }
     }
-    for (int r = warp; r < h; r += 8)
-      for (int c = lane; c < w; c += 32) {
-        s_src[r * 64 + c] = row_ptr<uint8_t>(sp, y0 + r)[x0 + c];
-        s_rec[r * 64 + c] = row_ptr<uint8_t>(rp, y0 + r)[x0 + c];
+    for (int r = warp; r < h; r += 8) {
+      const uint8_t* srow = row_ptr<uint8_t>(sp, y0 + r) + x0;
+      const uint8_t* rrow = row_ptr<uint8_t>(rp, y0 + r) + x0;
+      if ((((uintptr_t)srow | (uintptr_t)rrow) & 3) == 0) {
+        for (int c4 = lane; c4 < w >> 2; c4 += 32) {
+          reinterpret_cast<uint32_t*>(&s_src[r * 64])[c4] = reinterpret_cast<const uint32_t*>(srow)[c4];
+          reinterpret_cast<uint32_t*>(&s_rec[r * 64])[c4] = reinterpret_cast<const uint32_t*>(rrow)[c4];
+        }
+      } else {
+        for (int c = lane; c < w; c += 32) {
+          s_src[r * 64 + c] = srow[c];
+          s_rec[r * 64 + c] = rrow[c];
+        }
       }
-    if (pli == 0) {
+    }
+    if (pli == 0 && a.dirs) {
+      // Directions already found by the features kernel (same arithmetic).
+      if (tid < 64 && ((listed >> tid) & 1)) {
+        s_dir[tid] = a.dirs[(size_t)fb * 64 + tid];
+        s_ai[tid] = a.ais[(size_t)fb * 64 + tid];
+      }
+    } else if (pli == 0) {
       // Luma directions of the listed blocks, from the reconstruction.
       for (int wi = tid; wi < 64 * 8; wi += 256) {
         const int b = wi >> 3, d = wi & 7;
@@ -186,9 +217,6 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
 
 // ---- greedy preset selection (finish) ----
 
-// Savings-matrix slice each cluster CTA reduces.
-constexpr int kSelPairsPerCta = 4096 / kSelCluster;
-
 struct SelShared {
   unsigned long long part[4096];       // this CTA's partial savings (or column sums)
   unsigned long long col[128];
@@ -201,22 +229,31 @@ struct SelShared {
   unsigned long long tot;
 };
 
-// One cluster per configuration nb = 1 << (blockIdx.x / kSelCluster).
-// kRows: the filter blocks' SSE rows (as 32-bit values; an 8-bit 64x64
-// block's SSE is below 2^28) are copied into shared memory.
+// First maximum wins: larger value, or equal value at a lower index.
+__device__ __forceinline__ void argmax_merge(unsigned long long& v, int& i, unsigned long long v2, int i2) {
+  if (i == 0x7fffffff || v2 > v || (v2 == v && i2 < i)) {
+    v = v2;
+    i = i2;
+  }
+}
+
+// One cluster per configuration nb = 1 << (blockIdx.x / cluster size); the
+// cluster size (16, or 8 where a 16-CTA cluster cannot be placed) is read at
+// run time.  kRows: the filter blocks' SSE rows (as 32-bit values; an 8-bit
+// 64x64 block's SSE is below 2^28) are copied into shared memory.
 template <bool kRows>
-__global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(kSelThreads)
-    k_sel_greedy(SelArgs a) {
+__global__ void __launch_bounds__(kSelThreads) k_sel_greedy(SelArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   SelShared& S = *reinterpret_cast<SelShared*>(smem);
   uint32_t* s_best = reinterpret_cast<uint32_t*>(smem + sizeof(SelShared));
   uint32_t* s_min1 = s_best + a.cap;
   uint32_t* s_rows = s_min1 + a.cap;  // [cap][128] when kRows
   cg::cluster_group cl = cg::this_cluster();
+  const int CS = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
-  const int cfg = blockIdx.x / kSelCluster;
+  const int cfg = blockIdx.x / CS;
   const int nb = 1 << cfg;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int n = *a.n;
   SelOut* out = a.out;
   if (n == 0) {
@@ -226,8 +263,9 @@ __global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(kSelThread
     }
     return;
   }
-  const int per = (n + kSelCluster - 1) / kSelCluster;
+  const int per = (n + CS - 1) / CS;
   const int i0 = imin(n, rank * per), i1 = imin(n, i0 + per), cnt = i1 - i0;
+  const int pairs = 4096 / CS;
   const uint64_t* M0 = a.mse;
   const uint64_t* M1 = a.mse + (size_t)a.nfb * 64;
   auto row = [&](int il, int pl, int j) -> uint32_t {
@@ -249,7 +287,7 @@ __global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(kSelThread
   }
   if (t < 8) S.lev0[t] = S.lev1[t] = 0;
   __syncthreads();
-  const int steps = 5 * nb;
+  const int steps = a.refine ? 5 * nb : nb;
   for (int k = 0; k < steps; k++) {
     const int nbCur = k < nb ? k : nb - 1;
     const int par = k & 1;
@@ -262,9 +300,14 @@ __global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(kSelThread
       }
       cl.sync();
       if (t < 128) {
-        unsigned long long s = 0;
-        for (int r = 0; r < kSelCluster; r++) s += cl.map_shared_rank(&S.part[0], r)[t];
-        S.col[t] = s;
+        unsigned long long s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int r = 0; r < CS; r += 4) {
+          s0 += cl.map_shared_rank(&S.part[0], r)[t];
+          s1 += cl.map_shared_rank(&S.part[0], r + 1)[t];
+          s2 += cl.map_shared_rank(&S.part[0], r + 2)[t];
+          s3 += cl.map_shared_rank(&S.part[0], r + 3)[t];
+        }
+        S.col[t] = (s0 + s1) + (s2 + s3);
       }
       __syncthreads();
       if (t == 0) {
@@ -289,26 +332,38 @@ __global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(kSelThread
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) sb += __shfl_xor_sync(0xffffffffu, sb, o);
-      if ((t & 31) == 0) S.redS[t >> 5] = sb;
+      if (lane == 0) S.redS[warp] = sb;
       __syncthreads();
-      if (t == 0) {
-        unsigned long long s = 0;
-        for (int w = 0; w < kSelThreads / 32; w++) s += S.redS[w];
-        S.candSB[par] = s;
+      if (warp == 0) {
+        unsigned long long v = lane < kSelThreads / 32 ? S.redS[lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) S.candSB[par] = v;
       }
       // Partial savings of this CTA's blocks: thread t owns (j, k0..k0+7).
+      // A block saves below 2^29, so eight blocks sum exactly in 32 bits
+      // before joining the 64-bit totals.
       const int j = t >> 3, k0 = (t & 7) * 8;
       unsigned long long acc[8];
+      uint32_t acc32[8];
 #pragma unroll
-      for (int q = 0; q < 8; q++) acc[q] = 0;
-      for (int il = 0; il < cnt; il++) {
-        const uint32_t bi = s_best[il], a0 = row(il, 0, j);
-        if (a0 + s_min1[il] >= bi) continue;  // no k can save anything
-        const uint32_t rem = bi - a0;
+      for (int q = 0; q < 8; q++) acc[q] = acc32[q] = 0;
+      for (int il0 = 0; il0 < cnt; il0 += 8) {
+        const int il1 = imin(cnt, il0 + 8);
+        for (int il = il0; il < il1; il++) {
+          const uint32_t bi = s_best[il], a0 = row(il, 0, j);
+          if (a0 + s_min1[il] >= bi) continue;  // no k can save anything
+          const uint32_t rem = bi - a0;
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const uint32_t v = row(il, 1, k0 + q);
+            acc32[q] += v < rem ? rem - v : 0u;
+          }
+        }
 #pragma unroll
         for (int q = 0; q < 8; q++) {
-          const uint32_t v = row(il, 1, k0 + q);
-          if (v < rem) acc[q] += rem - v;
+          acc[q] += acc32[q];
+          acc32[q] = 0;
         }
       }
 #pragma unroll
@@ -317,54 +372,69 @@ __global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(kSelThread
       // Reduce this CTA's slice across the cluster; first maximum wins.
       unsigned long long bv = 0;
       int bi = 0x7fffffff;
-      for (int e = rank * kSelPairsPerCta + t; e < (rank + 1) * kSelPairsPerCta; e += kSelThreads) {
-        unsigned long long v = 0;
-        for (int r = 0; r < kSelCluster; r++) v += cl.map_shared_rank(&S.part[0], r)[e];
-        if (bi == 0x7fffffff || v > bv) {
-          bv = v;
-          bi = e;
+      for (int e = rank * pairs + t; e < (rank + 1) * pairs; e += kSelThreads) {
+        // Four independent remote reads in flight (CS is a multiple of 4).
+        unsigned long long v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+        for (int r = 0; r < CS; r += 4) {
+          v0 += cl.map_shared_rank(&S.part[0], r)[e];
+          v1 += cl.map_shared_rank(&S.part[0], r + 1)[e];
+          v2 += cl.map_shared_rank(&S.part[0], r + 2)[e];
+          v3 += cl.map_shared_rank(&S.part[0], r + 3)[e];
         }
+        argmax_merge(bv, bi, (v0 + v1) + (v2 + v3), e);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long v2 = __shfl_xor_sync(0xffffffffu, bv, o);
         const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (v2 > bv || (v2 == bv && i2 < bi)) {
-          bv = v2;
-          bi = i2;
-        }
+        argmax_merge(bv, bi, v2, i2);
       }
-      if ((t & 31) == 0) {
-        S.redV[t >> 5] = bv;
-        S.redI[t >> 5] = bi;
+      if (lane == 0) {
+        S.redV[warp] = bv;
+        S.redI[warp] = bi;
       }
       __syncthreads();
-      if (t == 0) {
-        for (int w = 1; w < kSelThreads / 32; w++)
-          if (S.redV[w] > bv || (S.redV[w] == bv && S.redI[w] < bi)) {
-            bv = S.redV[w];
-            bi = S.redI[w];
-          }
-        S.candV[par] = bv;
-        S.candI[par] = bi;
+      if (warp == 0) {
+        unsigned long long v = 0;
+        int i = 0x7fffffff;
+        if (lane < kSelThreads / 32) {
+          v = S.redV[lane];
+          i = S.redI[lane];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const unsigned long long v2 = __shfl_xor_sync(0xffffffffu, v, o);
+          const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+          argmax_merge(v, i, v2, i2);
+        }
+        if (lane == 0) {
+          S.candV[par] = v;
+          S.candI[par] = i;
+        }
       }
       cl.sync();
-      if (t == 0) {
-        unsigned long long wv = 0, sumBest = 0;
-        int wi = 0x7fffffff;
-        for (int r = 0; r < kSelCluster; r++) {
-          const SelShared* R = cl.map_shared_rank(&S, r);
-          const unsigned long long v = R->candV[par];
-          const int i = R->candI[par];
-          sumBest += R->candSB[par];
-          if (wi == 0x7fffffff || v > wv || (v == wv && i < wi)) {
-            wv = v;
-            wi = i;
-          }
+      if (warp == 0) {
+        // Lane r reads rank r's candidate and partial sum of best_i.
+        unsigned long long v = 0, sbr = 0;
+        int i = 0x7fffffff;
+        if (lane < CS) {
+          const SelShared* R = cl.map_shared_rank(&S, lane);
+          v = R->candV[par];
+          i = R->candI[par];
+          sbr = R->candSB[par];
         }
-        S.lev0[nbCur] = wi >> 6;
-        S.lev1[nbCur] = wi & 63;
-        S.tot = sumBest - wv;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const unsigned long long v2 = __shfl_xor_sync(0xffffffffu, v, o);
+          const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+          argmax_merge(v, i, v2, i2);
+          sbr += __shfl_xor_sync(0xffffffffu, sbr, o);
+        }
+        if (lane == 0) {
+          S.lev0[nbCur] = i >> 6;
+          S.lev1[nbCur] = i & 63;
+          S.tot = sbr - v;
+        }
       }
     }
     // Refinement passes drop the oldest pick (jointStrengthSearchDual).
@@ -460,7 +530,7 @@ __global__ void __launch_bounds__(1024) k_sel_list(const uint8_t* skip, int nfb,
 }
 
 size_t sel_smem_bytes(int nfb, bool rows) {
-  const int cap = (nfb + kSelCluster - 1) / kSelCluster;
+  const int cap = (nfb + kSelMinCluster - 1) / kSelMinCluster;
   return sizeof(SelShared) + (size_t)cap * 8 + (rows ? (size_t)cap * 512 : 0);
 }
 
@@ -469,21 +539,72 @@ cudaError_t launch_search(const SearchArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Launches k_sel_greedy with 16-CTA clusters when the device can place one
+// with this much shared memory, else with 8-CTA clusters.
+template <bool kRows>
+static cudaError_t launch_greedy(const SelArgs& s, int maxCfg, size_t bytes, cudaStream_t st) {
+  const void* fn = (const void*)k_sel_greedy<kRows>;
+  // The attributes and the cluster size are settled once per device and
+  // shared-memory size (host queries cost more than the short launches).
+  static thread_local int lastDev = -1;
+  static thread_local size_t lastBytes = 0;
+  static thread_local int lastCs = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev == lastDev && bytes <= lastBytes && lastCs) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = lastCs;
+    attr[0].val.clusterDim.y = attr[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(lastCs * (maxCfg + 1));
+    cfg.blockDim = dim3(kSelThreads);
+    cfg.dynamicSmemBytes = bytes;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_sel_greedy<kRows>, s);
+  }
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  cudaLaunchConfig_t cfg = {};
+  cfg.blockDim = dim3(kSelThreads);
+  cfg.dynamicSmemBytes = bytes;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int cs = kSelMaxCluster;
+  for (; cs > kSelMinCluster; cs >>= 1) {
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cs * (maxCfg + 1));
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) == cudaSuccess && nclusters >= 1) break;
+    cudaGetLastError();  // a refused query leaves no sticky error
+  }
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(cs * (maxCfg + 1));
+  e = cudaLaunchKernelEx(&cfg, k_sel_greedy<kRows>, s);
+  if (e == cudaSuccess) {
+    lastDev = dev;
+    lastBytes = bytes;
+    lastCs = cs;
+  }
+  return e;
+}
+
 cudaError_t launch_select(SelArgs s, int maxCfg, unsigned long long lambda, uint8_t* fbIndex, FinishOut* fo,
                           cudaStream_t st) {
   k_sel_list<<<1, 1024, 0, st>>>(s.skip, s.nfb, s.sb_w, s.n_w);
-  s.cap = (s.nfb + kSelCluster - 1) / kSelCluster;
+  s.cap = (s.nfb + kSelMinCluster - 1) / kSelMinCluster;
   const bool rows = sel_smem_bytes(s.nfb, true) <= kSelMaxSmem;
   const size_t bytes = sel_smem_bytes(s.nfb, rows);
   if (bytes > kSelMaxSmem) return cudaErrorInvalidValue;
-  cudaError_t e;
-  if (rows) {
-    e = cudaFuncSetAttribute(k_sel_greedy<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess) k_sel_greedy<true><<<kSelCluster * (maxCfg + 1), kSelThreads, bytes, st>>>(s);
-  } else {
-    e = cudaFuncSetAttribute(k_sel_greedy<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess) k_sel_greedy<false><<<kSelCluster * (maxCfg + 1), kSelThreads, bytes, st>>>(s);
-  }
+  const cudaError_t e = rows ? launch_greedy<true>(s, maxCfg, bytes, st) : launch_greedy<false>(s, maxCfg, bytes, st);
   if (e != cudaSuccess) return e;
   k_sel_finish<<<imax(1, (s.nfb + 255) / 256), 256, 0, st>>>(s, maxCfg, lambda, fbIndex, fo);
   return cudaGetLastError();
@@ -499,6 +620,8 @@ using namespace pf;
 
 void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
 void* pf_internal_stream(pf_ctx* c);
+void* pf_internal_pinned(pf_ctx* c, size_t bytes);
+void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, cudaStream_t st);
 
 static void* stage_frame(const pf_frame* f, void* dst, int64_t* strides, cudaStream_t st, cudaError_t* e) {
   size_t off = 0;
@@ -620,10 +743,22 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
     }
   }
   // The noskip words may live in host or device memory: copy them into the
-  // scratch either way (cudaMemcpyDefault resolves the direction).
+  // scratch either way; host words go through page-locked staging so the
+  // copy does not hold the host.
   const uint8_t* ns = nullptr;
-  if (noskip) {
-    if (e == cudaSuccess) e = cudaMemcpyAsync(base + oNs, noskip, (size_t)nfb * 8, cudaMemcpyDefault, st);
+  if (noskip && e == cudaSuccess) {
+    cudaPointerAttributes at;
+    const bool dev = cudaPointerGetAttributes(&at, noskip) == cudaSuccess &&
+                     (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    if (dev) {
+      e = cudaMemcpyAsync(base + oNs, noskip, (size_t)nfb * 8, cudaMemcpyDeviceToDevice, st);
+    } else {
+      void* pin = pf_internal_pinned(ctx, (size_t)nfb * 8);
+      if (!pin) return PF_ERR_DEVICE;
+      memcpy(pin, noskip, (size_t)nfb * 8);
+      e = cudaMemcpyAsync(base + oNs, pin, (size_t)nfb * 8, cudaMemcpyHostToDevice, st);
+    }
     ns = base + oNs;
   }
   if (e != cudaSuccess) return PF_ERR_DEVICE;
@@ -639,6 +774,8 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
   a.damping = damping;
   a.mse = (uint64_t*)(base + oMse);
   a.skip = base + oSkip;
+  a.dirs = nullptr;
+  a.ais = nullptr;
   SelArgs& s = S->s;
   s.mse = a.mse;
   s.skip = a.skip;
@@ -648,6 +785,7 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
   s.n = s.n_w;
   s.nfb = nfb;
   s.cap = 0;
+  s.refine = 1;
   s.out = (SelOut*)(base + oSel);
   S->idx = base + oIdx;
   S->fo = (FinishOut*)(base + oFin);
@@ -717,7 +855,7 @@ extern "C" int pf_cdef_features(pf_ctx* ctx, const pf_frame* recon, const uint8_
   const int stt = stage_search(ctx, nullptr, recon, noskip, dmp, 0, xBytes, &S);
   if (stt != PF_OK) return stt;
   float* X = (float*)S.extra;
-  if (launch_features(S.a, qindex, X, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  if (launch_features(S.a, qindex, X, true, S.st) != cudaSuccess) return PF_ERR_DEVICE;
   if (cudaMemcpyAsync(features, X, xBytes, cudaMemcpyDeviceToHost, S.st) != cudaSuccess ||
       cudaStreamSynchronize(S.st) != cudaSuccess)
     return PF_ERR_DEVICE;
@@ -727,9 +865,10 @@ extern "C" int pf_cdef_features(pf_ctx* ctx, const pf_frame* recon, const uint8_
 extern "C" int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
                                       const uint8_t* noskip, const pf_cdef_search_params* params,
                                       const pf_cdef_mlp* model, float threshold, int32_t candidates,
-                                      uint64_t* mse_out, uint8_t* fb_index_out, pf_cdef_search_result* result,
-                                      pf_cdef_learned_stats* stats) {
+                                      int32_t flags, uint64_t* mse_out, uint8_t* fb_index_out,
+                                      pf_cdef_search_result* result, pf_cdef_learned_stats* stats) {
   if (!ctx || !source || !recon || !params || !model) return PF_ERR_INVALID_ARG;
+  if (flags & ~PF_LEARNED_REFINE) return PF_ERR_INVALID_ARG;
   if (candidates < 1 || candidates > 8 || !(threshold >= 0.f)) return PF_ERR_INVALID_ARG;
   if (params->qindex < 0 || params->qindex > 255) return PF_ERR_INVALID_ARG;
   const int miCols = ((recon->width + 7) >> 3) << 1, miRows = ((recon->height + 7) >> 3) << 1;
@@ -737,34 +876,40 @@ extern "C" int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const
   auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
   const size_t xBytes = al((size_t)nfb * PF_MLP_FEATURES * sizeof(float));
   const size_t mBytes = al((size_t)nfb * 2 * sizeof(uint64_t));
-  const size_t wBytes = al(sizeof(pf_cdef_mlp));
+  const size_t dBytes = al((size_t)nfb * 128);
+  const size_t wBytes = al(mlp_expanded_bytes());
   Staged S;
   const int stt = stage_search(ctx, source, recon, noskip, search_damping(params), search_max_cfg(params),
-                               xBytes + mBytes + wBytes, &S);
+                               xBytes + mBytes + dBytes + wBytes, &S);
   if (stt != PF_OK) return stt;
   float* X = (float*)S.extra;
   uint64_t* masks = (uint64_t*)(S.extra + xBytes);
-  pf_cdef_mlp* dmodel = (pf_cdef_mlp*)(S.extra + xBytes + mBytes);
-  if (cudaMemcpyAsync(dmodel, model, sizeof(pf_cdef_mlp), cudaMemcpyHostToDevice, S.st) != cudaSuccess)
-    return PF_ERR_DEVICE;
-  if (launch_features(S.a, params->qindex, X, S.st) != cudaSuccess) return PF_ERR_DEVICE;
-  if (launch_mlp_masks(dmodel, X, nfb, threshold, candidates, masks, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  const pf_cdef_mlp* dmodel = (const pf_cdef_mlp*)pf_internal_cached_upload(ctx, model, sizeof(pf_cdef_mlp), S.st);
+  if (!dmodel) return PF_ERR_DEVICE;
+  S.a.dirs = S.extra + xBytes + mBytes;
+  S.a.ais = (int8_t*)(S.extra + xBytes + mBytes + (size_t)nfb * 64);
+  if (launch_features(S.a, params->qindex, X, false, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  float* W = (float*)(S.extra + xBytes + mBytes + dBytes);
+  if (launch_mlp_masks(dmodel, W, X, nfb, threshold, candidates, masks, S.st) != cudaSuccess) return PF_ERR_DEVICE;
   S.a.tmask = masks;
-  std::vector<uint64_t> hm;
-  if (stats) hm.resize((size_t)nfb * 2);
-  if (stats && cudaMemcpyAsync(hm.data(), masks, (size_t)nfb * 16, cudaMemcpyDeviceToHost, S.st) != cudaSuccess)
-    return PF_ERR_DEVICE;
+  S.s.refine = (flags & PF_LEARNED_REFINE) ? 1 : 0;
   const int r = search_finish(S, params, mse_out, fb_index_out, result);
   if (r != PF_OK) return r;
+  // The statistics are read back after the search (no host wait between the
+  // network and the search it steers).
   if (stats) {
+    std::vector<uint64_t> hm((size_t)nfb * 2);
     std::vector<uint8_t> skip(nfb);
-    if (cudaMemcpy(skip.data(), S.a.skip, nfb, cudaMemcpyDeviceToHost) != cudaSuccess) return PF_ERR_DEVICE;
+    if (cudaMemcpy(hm.data(), masks, (size_t)nfb * 16, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(skip.data(), S.a.skip, nfb, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return PF_ERR_DEVICE;
     memset(stats, 0, sizeof(*stats));
     for (int fb = 0; fb < nfb; fb++) {
       if (skip[fb]) continue;
       stats->blocks++;
       const int c0 = __builtin_popcountll(hm[2 * fb]), c1 = __builtin_popcountll(hm[2 * fb + 1]);
-      if (c0 == 64 && c1 == 64) stats->fallback++;
+      if (c0 == 64) stats->fallback_luma++;
+      if (c1 == 64) stats->fallback_chroma++;
       stats->trials_luma += c0;
       stats->trials_chroma += c1;
     }

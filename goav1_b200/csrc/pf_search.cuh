@@ -10,7 +10,8 @@ namespace pf {
 // recorded for a trial that was not measured.
 constexpr uint32_t kUntestedMSE = 1040400u * 64u;
 
-constexpr int kSelCluster = 8;     // CTAs per greedy-selection cluster
+constexpr int kSelMaxCluster = 16;  // CTAs per greedy-selection cluster (non-portable size)
+constexpr int kSelMinCluster = 8;   // fallback where a 16-CTA cluster cannot be placed
 constexpr int kSelThreads = 512;
 constexpr size_t kSelMaxSmem = 200 * 1024;
 
@@ -30,6 +31,12 @@ struct SearchArgs {
   int damping;
   uint64_t* mse;            // [2][nfb][64]
   uint8_t* skip;            // [nfb]
+  // Per 8x8 luma block of each filter block: CDEF direction and
+  // adjustStrength index (-1 for zero variance).  Written by the features
+  // kernel when non-null; read by the search instead of its own direction
+  // pass when non-null.
+  uint8_t* dirs;            // [nfb][64]
+  int8_t* ais;              // [nfb][64]
 };
 
 struct SelOut {
@@ -51,6 +58,7 @@ struct SelArgs {
   const int* sb;
   const int* n;
   int nfb, cap;
+  int refine;            // 1: the reference's 4*nb refinement passes after the nb greedy picks
   SelOut* out;
 };
 
@@ -132,10 +140,13 @@ cudaError_t launch_search(const SearchArgs& a, cudaStream_t st);
 cudaError_t launch_select(SelArgs s, int maxCfg, unsigned long long lambda, uint8_t* fbIndex, FinishOut* fo,
                           cudaStream_t st);
 
-// pf_mlp.cu: per-filter-block features of a.rec (X: [nfb][PF_MLP_FEATURES]).
-cudaError_t launch_features(const SearchArgs& a, int qindex, float* X, cudaStream_t st);
+// pf_mlp.cu: per-filter-block features of a.rec (X: [nfb][PF_MLP_FEATURES]);
+// the frame means (features 33..39) only with frameMeans (the mask kernel
+// computes them itself).
+cudaError_t launch_features(const SearchArgs& a, int qindex, float* X, bool frameMeans, cudaStream_t st);
 // pf_mlp.cu: the network over X and the tested-trial masks ([nfb][2]).
-cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, const float* X, int nfb, float threshold, int candidates,
-                             uint64_t* masks, cudaStream_t st);
+size_t mlp_expanded_bytes();  // fp32 copy of the network's parameters
+cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, float* W, const float* X, int nfb, float threshold,
+                             int candidates, uint64_t* masks, cudaStream_t st);
 
 }  // namespace pf

@@ -121,18 +121,18 @@ class PostFilterRunner:
         check(lib().pf_batch_apply(self._h, arr, len(items), C.byref(self.stats)))
         return self.stats
 
-    def cdef_search(self, source, recon, noskip, qindex, lam, max_presets=8, damping=0):
+    def cdef_search(self, source, recon, noskip, qindex, lam, max_presets=8, damping=0, want_mse=True):
         """Encoder CDEF strength search (cdefSearcher.search + finish,
         internal/av1/encoder/cdef_search.go:580-945) on 8-bit 4:2:0 frames.
         Returns (pf_cdef_search_result, mse uint64[2, nfb, 64], fb_index uint8[nfb])."""
         nfb = _nfb(recon.width, recon.height)
-        mse = np.zeros((2, nfb, 64), np.uint64)
-        idx = np.zeros(nfb, np.uint8)
+        mse = np.empty((2, nfb, 64), np.uint64) if want_mse else None
+        idx = np.empty(nfb, np.uint8)
         res = abi.pf_cdef_search_result()
         prm = abi.pf_cdef_search_params(qindex=qindex, damping=damping, max_presets=max_presets, lam=lam)
         ns = noskip.ctypes.data if noskip is not None else None
-        check(lib().pf_cdef_search(self._h, C.byref(source), C.byref(recon), ns, C.byref(prm), mse.ctypes.data,
-                                   idx.ctypes.data, C.byref(res)))
+        check(lib().pf_cdef_search(self._h, C.byref(source), C.byref(recon), ns, C.byref(prm),
+                                   mse.ctypes.data if want_mse else None, idx.ctypes.data, C.byref(res)))
         return res, mse, idx
 
     def cdef_features(self, recon, noskip, qindex, damping=0):
@@ -174,21 +174,24 @@ class PostFilterRunner:
                                       C.byref(prm), losses.ctypes.data))
         return losses
 
-    def cdef_search_learned(self, source, recon, noskip, qindex, lam, model, threshold=0.5, candidates=2,
-                            max_presets=8, damping=0):
+    def cdef_search_learned(self, source, recon, noskip, qindex, lam, model, threshold=0.5, candidates=3,
+                            max_presets=8, damping=0, want_mse=True, want_stats=True, refine=False):
         """The learned search: the network's top trials per block, all trials
-        where it is unsure, then the reference's greedy selection.  Returns
+        where it is unsure, then the reference's greedy selection (its
+        refinement passes only with refine=True).  Returns
         (pf_cdef_search_result, mse uint64[2, nfb, 64], fb_index, pf_cdef_learned_stats)."""
         nfb = _nfb(recon.width, recon.height)
-        mse = np.zeros((2, nfb, 64), np.uint64)
-        idx = np.zeros(nfb, np.uint8)
+        mse = np.empty((2, nfb, 64), np.uint64) if want_mse else None
+        idx = np.empty(nfb, np.uint8)
         res = abi.pf_cdef_search_result()
         st = abi.pf_cdef_learned_stats()
         prm = abi.pf_cdef_search_params(qindex=qindex, damping=damping, max_presets=max_presets, lam=lam)
         ns = noskip.ctypes.data if noskip is not None else None
         check(lib().pf_cdef_search_learned(self._h, C.byref(source), C.byref(recon), ns, C.byref(prm),
-                                           C.byref(model), threshold, candidates, mse.ctypes.data, idx.ctypes.data,
-                                           C.byref(res), C.byref(st)))
+                                           C.byref(model), threshold, candidates,
+                                           abi.PF_LEARNED_REFINE if refine else 0,
+                                           mse.ctypes.data if want_mse else None, idx.ctypes.data,
+                                           C.byref(res), C.byref(st) if want_stats else None))
         return res, mse, idx, st
 
     def post_filter_output(self):

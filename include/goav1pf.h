@@ -331,7 +331,7 @@ int pf_film_grain_static(const pf_frame* ref, const pf_film_grain* fg, const pf_
  * filter block, which of the 64 level-1 trials (the pf_cdef_search order)
  * is best for luma and for chroma, from 40 statistics of the deblocked
  * reconstruction.  pf_cdef_search_learned then measures only the predicted
- * trials of a confident block, the full 64 + 64 of a block whose top-1
+ * trials of a confident head, all 64 trials of a head whose top-1
  * probability is below the threshold, and runs the same greedy preset
  * selection and RD choice as pf_cdef_search over that table; the bitstream
  * syntax (CDEFParams and the per-block index) is unchanged.
@@ -381,10 +381,11 @@ typedef struct pf_cdef_mlp_train_params {
 } pf_cdef_mlp_train_params;
 
 typedef struct pf_cdef_learned_stats {
-  int32_t blocks;         /* non-skip filter blocks */
-  int32_t fallback;       /* blocks searched with all 64 + 64 trials */
-  int32_t trials_luma;    /* luma trials measured, all blocks */
-  int32_t trials_chroma;  /* chroma trials measured, all blocks */
+  int32_t blocks;           /* non-skip filter blocks */
+  int32_t fallback_luma;    /* blocks whose luma head measured all 64 trials */
+  int32_t fallback_chroma;  /* blocks whose chroma head measured all 64 trials */
+  int32_t trials_luma;      /* luma trials measured, all blocks */
+  int32_t trials_chroma;    /* chroma trials measured, all blocks */
 } pf_cdef_learned_stats;
 
 /* Per-filter-block features of an 8-bit 4:2:0 deblocked reconstruction
@@ -414,15 +415,20 @@ int pf_cdef_mlp_train(pf_ctx* ctx, pf_cdef_mlp* model, const float* features,
                       float* epoch_loss);
 
 /* The learned search: arguments and outputs as pf_cdef_search, plus the
- * network, the confidence threshold (a block falls back to all trials when
- * either head's top-1 probability is below it; above 1 every block falls
- * back) and the number of top trials measured per head for a confident
- * block (1..8).  Unmeasured entries of mse_out hold 66585600 (the
- * reference's untested-trial figure). */
+ * network, the confidence threshold (a head falls back to all 64 trials
+ * when its top-1 probability is below it; above 1 every head falls back)
+ * and the number of top trials measured by a confident head (1..8).
+ * Unmeasured entries of mse_out hold 66585600 (the reference's
+ * untested-trial figure).  The preset selection is the reference's greedy
+ * over that table; without PF_LEARNED_REFINE in flags it stops after the nb
+ * greedy picks (no 4*nb refinement passes: 8 sequential steps instead of 40
+ * for 8 presets; on the evaluation frames the refinement changed no
+ * frame's luma SSE by more than 0.001 %). */
+#define PF_LEARNED_REFINE 1
 int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
                            const uint8_t* noskip, const pf_cdef_search_params* params,
                            const pf_cdef_mlp* model, float threshold, int32_t candidates,
-                           uint64_t* mse_out, uint8_t* fb_index_out,
+                           int32_t flags, uint64_t* mse_out, uint8_t* fb_index_out,
                            pf_cdef_search_result* result, pf_cdef_learned_stats* stats);
 
 #ifdef __cplusplus

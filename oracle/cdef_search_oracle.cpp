@@ -307,9 +307,21 @@ extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, cons
   return oracle_cdef_select(mse_out, skipFB.data(), nfb, prm, fb_index_out, result);
 }
 
+extern "C" int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, int nfb,
+                                     const pf_cdef_search_params* prm, int refine, uint8_t* fb_index_out,
+                                     pf_cdef_search_result* result);
+
 // finish (cdef_search.go:886-945) over a given SSE table.
 extern "C" int oracle_cdef_select(const uint64_t* mse, const uint8_t* skip, int nfb, const pf_cdef_search_params* prm,
                                   uint8_t* fb_index_out, pf_cdef_search_result* result) {
+  return oracle_cdef_select_ex(mse, skip, nfb, prm, 1, fb_index_out, result);
+}
+
+// refine = 0 stops each configuration after its nb greedy picks (the
+// learned search's selection); refine = 1 is finish() itself.
+extern "C" int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, int nfb,
+                                     const pf_cdef_search_params* prm, int refine, uint8_t* fb_index_out,
+                                     pf_cdef_search_result* result) {
   int8_t fs[64];
   trial_list(fs);
   std::vector<const uint64_t*> s0, s1;
@@ -331,7 +343,7 @@ extern "C" int oracle_cdef_select(const uint64_t* mse, const uint8_t* skip, int 
     const int nb = 1 << i;
     uint64_t tot = (uint64_t)1 << 63;
     for (int k = 0; k < nb; k++) tot = search_one_dual(s0, s1, lev0, lev1, k, 64);
-    for (int k = 0; k < 4 * nb; k++) {
+    for (int k = 0; refine && k < 4 * nb; k++) {
       for (int j = 0; j < nb - 1; j++) {
         lev0[j] = lev0[j + 1];
         lev1[j] = lev1[j + 1];

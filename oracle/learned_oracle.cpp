@@ -10,7 +10,8 @@
 //                             rest are integer pixel statistics.
 //   oracle_mlp_forward        the network (bf16 weights widened to fp32,
 //                             fused multiply-adds over the inputs in index
-//                             order, ReLU, two softmax heads).
+//                             order, ReLU, two softmax heads summed in the
+//                             GPU warp's butterfly order).
 //   oracle_mlp_gradients      mean two-head cross-entropy and its gradients,
 //                             accumulated in the GPU kernels' order (tiles of
 //                             32 samples, fused multiply-adds), so fp32
@@ -290,11 +291,18 @@ void forward(const float* P, const float* shift, const float* scale, const float
     const float* z = A.z + hd * kC;
     float m = z[0];
     for (int o = 1; o < kC; o++) m = fmaxf(m, z[o]);
-    float sum = 0.f;
-    for (int o = 0; o < kC; o++) sum += expf(z[o] - m);
+    // The GPU's warp order: e[l] + e[l+32] per lane, then xor butterflies.
+    float e[kC], v[32], nv[32];
+    for (int o = 0; o < kC; o++) e[o] = expf(z[o] - m);
+    for (int i = 0; i < 32; i++) v[i] = e[i] + e[i + 32];
+    for (int d = 16; d > 0; d >>= 1) {
+      for (int i = 0; i < 32; i++) nv[i] = v[i] + v[i ^ d];
+      memcpy(v, nv, sizeof(v));
+    }
+    const float sum = v[0];
     if (y) l[hd] = m + logf(sum) - z[y[hd]];
     const float inv = 1.f / sum;
-    for (int o = 0; o < kC; o++) A.p[hd * kC + o] = expf(z[o] - m) * inv;
+    for (int o = 0; o < kC; o++) A.p[hd * kC + o] = e[o] * inv;
   }
   if (y) A.loss = l[0] + l[1];
 }

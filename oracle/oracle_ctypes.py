@@ -52,6 +52,8 @@ def lib():
         _lib.oracle_cdef_adjust_strength.argtypes = [C.c_int, C.c_int32]
         _lib.oracle_cdef_search.argtypes = [C.c_void_p] * 7
         _lib.oracle_cdef_select.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.oracle_cdef_select_ex.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                               C.c_void_p]
         _lib.oracle_cdef_features.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         _lib.oracle_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         _lib.oracle_mlp_forward.restype = None

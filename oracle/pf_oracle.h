@@ -74,6 +74,10 @@ int oracle_cdef_search(const pf_frame* source, const pf_frame* recon, const uint
  * ([2][nfb][64]; skip[fb] != 0 leaves a block out). */
 int oracle_cdef_select(const uint64_t* mse, const uint8_t* skip, int nfb, const pf_cdef_search_params* params,
                        uint8_t* fb_index_out, pf_cdef_search_result* result);
+/* The same with the refinement passes switched by `refine` (0: stop after
+ * the nb greedy picks, as the learned search does by default). */
+int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, int nfb, const pf_cdef_search_params* params,
+                          int refine, uint8_t* fb_index_out, pf_cdef_search_result* result);
 
 /* Learned CDEF selection (oracle/learned_oracle.cpp); see pf_cdef_features
  * and the pf_cdef_mlp_* entry points.  grads: PF_MLP_PARAMS floats. */

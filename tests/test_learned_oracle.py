@@ -102,6 +102,19 @@ def test_canonical_labels_break_near_ties_by_prior():
     assert y[0, 0] == 20 and y[1, 0] == 10 and (y[:, 1] == 5).all()
 
 
+def test_default_labels_follow_the_frame_ranking():
+    mse = np.full((2, 3, 64), 1000000, np.uint64)
+    # Block 0 prefers 10 by 0.4 %, blocks 1 and 2 prefer 20 by a lot: the
+    # frame ranks 20 first, so block 0's near-tie goes to 20.
+    mse[0, 0, 10], mse[0, 0, 20] = 500000, 502000
+    mse[0, 1, 20], mse[0, 2, 20] = 100000, 100000
+    mse[1, :, 7] = 5
+    keep = np.ones(3, bool)
+    y = learned.canonical_labels(mse, keep, tie=0.01)
+    assert (y[:, 0] == 20).all() and (y[:, 1] == 7).all()
+    assert learned.canonical_labels(mse, keep, tie=0.001)[0, 0] == 10
+
+
 def test_argmin_prior_orders_by_frequency():
     mse = np.full((2, 4, 64), 10, np.uint64)
     mse[0, 0, 3] = mse[0, 1, 3] = mse[0, 2, 7] = 1
