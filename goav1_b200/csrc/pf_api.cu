@@ -869,10 +869,17 @@ void* pf_internal_pinned(pf_ctx* c, size_t bytes) {
 }
 
 // Device copy of `bytes` of host data that rarely changes (the learned
-// search's network): uploaded only when it differs from the last upload.
-void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, cudaStream_t st) {
-  if (c->model.ensure(bytes) != cudaSuccess) return nullptr;
+// search's network): uploaded only when it differs from the last upload
+// (*changed = 1 then).  `extra` device bytes follow it (256-aligned) for
+// data derived from it, which the caller refreshes when it changed.
+void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, size_t extra, cudaStream_t st,
+                                int* changed) {
+  *changed = 0;
+  const size_t need = ((bytes + 255) & ~(size_t)255) + extra;
+  if (need > c->model.n) c->model_shadow.clear();  // a new buffer holds nothing yet
+  if (c->model.ensure(need) != cudaSuccess) return nullptr;
   if (c->model_shadow.size() == bytes && memcmp(c->model_shadow.data(), host, bytes) == 0) return c->model.p;
+  *changed = 1;
   if (c->model_shadow.size() != bytes) {
     if (c->model_pin) cudaFreeHost(c->model_pin);
     c->model_pin = nullptr;

@@ -258,30 +258,40 @@ __global__ void __launch_bounds__(256, 4) k_cdef_features(SearchArgs a, int qind
     }
   }
   __syncthreads();
-  if (tid == 0) {
+  if (tid < kPerFb) {
+    // Thread i writes feature i (same expressions as the oracle's).
     const float nb = (float)__popcll(listed);
-    unsigned long long ds = 0;
-    for (int d = 0; d < 8; d++) ds += A.dcost[d];
-    for (int d = 0; d < 8; d++) out[d] = ds ? (float)A.dcost[d] / (float)ds : 0.125f;
-    for (int d = 0; d < 8; d++) out[8 + d] = (float)A.dhist[d] / nb;
     auto cnt = [](unsigned long long c) { return (float)(c ? c : 1ull); };
-    out[16] = log2f(1.f + (float)A.varsum / nb);
-    out[17] = (float)A.nvar0 / nb;
-    out[18] = (float)A.adjsum / (16.f * nb);
-    out[19] = log2f(1.f + (float)A.bvar / (4096.f * nb));
-    out[20] = log2f(1.f + (float)A.gH / cnt(A.cH));
-    out[21] = log2f(1.f + (float)A.gV / cnt(A.cV));
-    out[22] = log2f(1.f + (float)A.lap / cnt(A.clap));
-    out[23] = ((float)A.bH / cnt(A.cbH) - (float)(A.gH - A.bH) / cnt(A.cH - A.cbH)) / 8.f;
-    out[24] = ((float)A.bV / cnt(A.cbV) - (float)(A.gV - A.bV) / cnt(A.cV - A.cbV)) / 8.f;
-    out[25] = log2f(1.f + (float)A.uvar / (256.f * nb));
-    out[26] = log2f(1.f + (float)A.vvar / (256.f * nb));
-    out[27] = log2f(1.f + (float)A.clapUV / cnt(A.cclapUV));
-    out[28] = log2f(1.f + (float)A.cgUV / cnt(A.ccgUV));
-    out[29] = nb / 64.f;
-    out[30] = (float)qindex / 255.f;
-    out[31] = (float)(a.damping - 3) / 3.f;
-    out[32] = (float)A.sumY / (255.f * (float)(wc * hc));
+    float f;
+    const int i = tid;
+    if (i < 8) {
+      unsigned long long ds = 0;
+      for (int d = 0; d < 8; d++) ds += A.dcost[d];
+      f = ds ? (float)A.dcost[i] / (float)ds : 0.125f;
+    } else if (i < 16) {
+      f = (float)A.dhist[i - 8] / nb;
+    } else {
+      switch (i) {
+        case 16: f = log2f(1.f + (float)A.varsum / nb); break;
+        case 17: f = (float)A.nvar0 / nb; break;
+        case 18: f = (float)A.adjsum / (16.f * nb); break;
+        case 19: f = log2f(1.f + (float)A.bvar / (4096.f * nb)); break;
+        case 20: f = log2f(1.f + (float)A.gH / cnt(A.cH)); break;
+        case 21: f = log2f(1.f + (float)A.gV / cnt(A.cV)); break;
+        case 22: f = log2f(1.f + (float)A.lap / cnt(A.clap)); break;
+        case 23: f = ((float)A.bH / cnt(A.cbH) - (float)(A.gH - A.bH) / cnt(A.cH - A.cbH)) / 8.f; break;
+        case 24: f = ((float)A.bV / cnt(A.cbV) - (float)(A.gV - A.bV) / cnt(A.cV - A.cbV)) / 8.f; break;
+        case 25: f = log2f(1.f + (float)A.uvar / (256.f * nb)); break;
+        case 26: f = log2f(1.f + (float)A.vvar / (256.f * nb)); break;
+        case 27: f = log2f(1.f + (float)A.clapUV / cnt(A.cclapUV)); break;
+        case 28: f = log2f(1.f + (float)A.cgUV / cnt(A.ccgUV)); break;
+        case 29: f = nb / 64.f; break;
+        case 30: f = (float)qindex / 255.f; break;
+        case 31: f = (float)(a.damping - 3) / 3.f; break;
+        default: f = (float)A.sumY / (255.f * (float)(wc * hc)); break;
+      }
+    }
+    out[i] = f;
   }
 }
 
@@ -677,8 +687,8 @@ cudaError_t launch_features(const SearchArgs& a, int qindex, float* X, bool fram
 
 size_t mlp_expanded_bytes() { return (size_t)kExpanded * sizeof(float); }
 
-cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, float* W, const float* X, int nfb, float threshold,
-                             int candidates, uint64_t* masks, cudaStream_t st) {
+cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, float* W, bool expand, const float* X, int nfb,
+                             float threshold, int candidates, uint64_t* masks, cudaStream_t st) {
   static thread_local int ready = -1;  // device whose attribute is set
   int dev = 0;
   cudaGetDevice(&dev);
@@ -687,7 +697,7 @@ cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, float* W, const float* X
     if (e != cudaSuccess) return e;
     ready = dev;
   }
-  k_mlp_expand<<<(kExpanded + 255) / 256, 256, 0, st>>>(dmodel, W);
+  if (expand) k_mlp_expand<<<(kExpanded + 255) / 256, 256, 0, st>>>(dmodel, W);
   k_mlp_masks<<<(nfb + kInferTile - 1) / kInferTile, kMlpThreads, sizeof(MlpInfer), st>>>(W, X, nfb, threshold,
                                                                                        candidates, masks);
   return cudaGetLastError();

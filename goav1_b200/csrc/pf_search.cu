@@ -237,6 +237,29 @@ __device__ __forceinline__ void argmax_merge(unsigned long long& v, int& i, unsi
   }
 }
 
+// The non-skip filter blocks in order (computeCDEFList's non-empty units):
+// a ballot per warp and a running base; returns their count.  All threads
+// of the block call it; `wsum` is one int per warp of scratch.
+__device__ int compact_blocks(const uint8_t* skip, int nfb, int* list, int* wsum) {
+  const int t = threadIdx.x, nw = blockDim.x >> 5;
+  int base = 0;
+  for (int b0 = 0; b0 < nfb; b0 += blockDim.x) {
+    const int fb = b0 + t;
+    const bool keep = fb < nfb && !skip[fb];
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    __syncthreads();  // the previous round is done with wsum
+    if ((t & 31) == 0) wsum[t >> 5] = __popc(m);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < (t >> 5); w++) off += wsum[w];
+    off += __popc(m & ((1u << (t & 31)) - 1));
+    if (keep) list[off] = fb;
+    for (int w = 0; w < nw; w++) base += wsum[w];
+  }
+  __syncthreads();
+  return base;
+}
+
 // One cluster per configuration nb = 1 << (blockIdx.x / cluster size); the
 // cluster size (16, or 8 where a 16-CTA cluster cannot be placed) is read at
 // run time.  kRows: the filter blocks' SSE rows (as 32-bit values; an 8-bit
@@ -245,7 +268,8 @@ template <bool kRows>
 __global__ void __launch_bounds__(kSelThreads) k_sel_greedy(SelArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   SelShared& S = *reinterpret_cast<SelShared*>(smem);
-  uint32_t* s_best = reinterpret_cast<uint32_t*>(smem + sizeof(SelShared));
+  int* s_sb = reinterpret_cast<int*>(smem + sizeof(SelShared));  // [nfb] non-skip blocks
+  uint32_t* s_best = reinterpret_cast<uint32_t*>(s_sb + ((a.nfb + 3) & ~3));
   uint32_t* s_min1 = s_best + a.cap;
   uint32_t* s_rows = s_min1 + a.cap;  // [cap][128] when kRows
   cg::cluster_group cl = cg::this_cluster();
@@ -254,7 +278,7 @@ __global__ void __launch_bounds__(kSelThreads) k_sel_greedy(SelArgs a) {
   const int cfg = blockIdx.x / CS;
   const int nb = 1 << cfg;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int n = *a.n;
+  const int n = compact_blocks(a.skip, a.nfb, s_sb, S.redI);
   SelOut* out = a.out;
   if (n == 0) {
     if (rank == 0 && t == 0) {
@@ -270,13 +294,13 @@ __global__ void __launch_bounds__(kSelThreads) k_sel_greedy(SelArgs a) {
   const uint64_t* M1 = a.mse + (size_t)a.nfb * 64;
   auto row = [&](int il, int pl, int j) -> uint32_t {
     if (kRows) return s_rows[il * 128 + pl * 64 + j];
-    const int fb = a.sb[i0 + il];
+    const int fb = s_sb[i0 + il];
     return (uint32_t)(pl ? M1 : M0)[(size_t)fb * 64 + j];
   };
   if (kRows)
     for (int e = t; e < cnt * 128; e += kSelThreads) {
       const int il = e >> 7, pl = (e >> 6) & 1, j = e & 63;
-      const int fb = a.sb[i0 + il];
+      const int fb = s_sb[i0 + il];
       s_rows[e] = (uint32_t)(pl ? M1 : M0)[(size_t)fb * 64 + j];
     }
   __syncthreads();
@@ -458,9 +482,18 @@ __global__ void __launch_bounds__(kSelThreads) k_sel_greedy(SelArgs a) {
 // RD choice of nb (finish, :914-931) and the per-block preset index.
 __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsigned long long lambda, uint8_t* fbIndex,
                                                     FinishOut* fo) {
-  __shared__ int s_best;
+  __shared__ int s_best, s_n;
   const SelOut* st = a.out;
-  const int n = *a.n;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  {
+    int c = 0;
+    for (int fb = threadIdx.x; fb < a.nfb; fb += blockDim.x) c += !a.skip[fb];
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_n, c);
+  }
+  __syncthreads();
+  const int n = s_n;
   if (threadIdx.x == 0) {
     unsigned long long bestTot = 1ull << 63;
     int best = 0;
@@ -488,9 +521,11 @@ __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsig
   const int c = s_best, nb = 1 << c;
   const uint64_t* M0 = a.mse;
   const uint64_t* M1 = a.mse + (size_t)a.nfb * 64;
-  for (int fb = blockIdx.x * blockDim.x + threadIdx.x; fb < a.nfb; fb += gridDim.x * blockDim.x) fbIndex[fb] = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int fb = a.sb[i];
+  for (int fb = blockIdx.x * blockDim.x + threadIdx.x; fb < a.nfb; fb += gridDim.x * blockDim.x) {
+    if (a.skip[fb]) {
+      fbIndex[fb] = 0;
+      continue;
+    }
     int bg = 0;
     unsigned long long bm = 1ull << 63;
     for (int g = 0; g < nb; g++) {
@@ -504,34 +539,9 @@ __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsig
   }
 }
 
-// Compacts the non-skip filter blocks into a list (order preserved).
-__global__ void __launch_bounds__(1024) k_sel_list(const uint8_t* skip, int nfb, int* sb, int* n) {
-  __shared__ int s_warp[32];
-  __shared__ int s_base;
-  const int t = threadIdx.x;
-  if (t == 0) s_base = 0;
-  __syncthreads();
-  for (int b0 = 0; b0 < nfb; b0 += 1024) {
-    const int fb = b0 + t;
-    const bool keep = fb < nfb && !skip[fb];
-    const unsigned m = __ballot_sync(0xffffffffu, keep);
-    if ((t & 31) == 0) s_warp[t >> 5] = __popc(m);
-    __syncthreads();
-    int off = s_base;
-    for (int w = 0; w < (t >> 5); w++) off += s_warp[w];
-    off += __popc(m & ((1u << (t & 31)) - 1));
-    if (keep) sb[off] = fb;
-    __syncthreads();
-    if (t == 0)
-      for (int w = 0; w < 32; w++) s_base += s_warp[w];
-    __syncthreads();
-  }
-  if (t == 0) *n = s_base;
-}
-
 size_t sel_smem_bytes(int nfb, bool rows) {
   const int cap = (nfb + kSelMinCluster - 1) / kSelMinCluster;
-  return sizeof(SelShared) + (size_t)cap * 8 + (rows ? (size_t)cap * 512 : 0);
+  return sizeof(SelShared) + (size_t)((nfb + 3) & ~3) * 4 + (size_t)cap * 8 + (rows ? (size_t)cap * 512 : 0);
 }
 
 cudaError_t launch_search(const SearchArgs& a, cudaStream_t st) {
@@ -599,7 +609,6 @@ static cudaError_t launch_greedy(const SelArgs& s, int maxCfg, size_t bytes, cud
 
 cudaError_t launch_select(SelArgs s, int maxCfg, unsigned long long lambda, uint8_t* fbIndex, FinishOut* fo,
                           cudaStream_t st) {
-  k_sel_list<<<1, 1024, 0, st>>>(s.skip, s.nfb, s.sb_w, s.n_w);
   s.cap = (s.nfb + kSelMinCluster - 1) / kSelMinCluster;
   const bool rows = sel_smem_bytes(s.nfb, true) <= kSelMaxSmem;
   const size_t bytes = sel_smem_bytes(s.nfb, rows);
@@ -621,7 +630,8 @@ using namespace pf;
 void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
 void* pf_internal_stream(pf_ctx* c);
 void* pf_internal_pinned(pf_ctx* c, size_t bytes);
-void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, cudaStream_t st);
+void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, size_t extra, cudaStream_t st,
+                                int* changed);
 
 static void* stage_frame(const pf_frame* f, void* dst, int64_t* strides, cudaStream_t st, cudaError_t* e) {
   size_t off = 0;
@@ -658,8 +668,8 @@ static DFrame search_dframe(const pf_frame* f, uint8_t* const* ptrs, const int64
 }
 
 // Validation, staging and scratch shared by the search entry points.
-// Scratch: [staged src | staged rec | noskip | mse | skip | sb list | n |
-//           SelOut | FinishOut | fbIndex | caller's extra bytes].
+// Scratch: [staged src | staged rec | noskip | mse | skip | SelOut |
+//           FinishOut | fbIndex | caller's extra bytes].
 struct Staged {
   SearchArgs a;
   SelArgs s;
@@ -710,8 +720,6 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
   const size_t oNs = off; off += al((size_t)nfb * 8);
   const size_t oMse = off; off += al((size_t)2 * nfb * 64 * 8);
   const size_t oSkip = off; off += al(nfb);
-  const size_t oSb = off; off += al((size_t)nfb * 4);
-  const size_t oN = off; off += 256;
   const size_t oSel = off; off += al(sizeof(SelOut));
   const size_t oFin = off; off += al(sizeof(FinishOut));
   const size_t oIdx = off; off += al(nfb);
@@ -779,10 +787,6 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
   SelArgs& s = S->s;
   s.mse = a.mse;
   s.skip = a.skip;
-  s.sb_w = (int*)(base + oSb);
-  s.n_w = (int*)(base + oN);
-  s.sb = s.sb_w;
-  s.n = s.n_w;
   s.nfb = nfb;
   s.cap = 0;
   s.refine = 1;
@@ -877,20 +881,23 @@ extern "C" int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const
   const size_t xBytes = al((size_t)nfb * PF_MLP_FEATURES * sizeof(float));
   const size_t mBytes = al((size_t)nfb * 2 * sizeof(uint64_t));
   const size_t dBytes = al((size_t)nfb * 128);
-  const size_t wBytes = al(mlp_expanded_bytes());
   Staged S;
   const int stt = stage_search(ctx, source, recon, noskip, search_damping(params), search_max_cfg(params),
-                               xBytes + mBytes + dBytes + wBytes, &S);
+                               xBytes + mBytes + dBytes, &S);
   if (stt != PF_OK) return stt;
   float* X = (float*)S.extra;
   uint64_t* masks = (uint64_t*)(S.extra + xBytes);
-  const pf_cdef_mlp* dmodel = (const pf_cdef_mlp*)pf_internal_cached_upload(ctx, model, sizeof(pf_cdef_mlp), S.st);
-  if (!dmodel) return PF_ERR_DEVICE;
+  int changed = 0;
+  uint8_t* mbase = (uint8_t*)pf_internal_cached_upload(ctx, model, sizeof(pf_cdef_mlp), mlp_expanded_bytes(), S.st,
+                                                       &changed);
+  if (!mbase) return PF_ERR_DEVICE;
+  const pf_cdef_mlp* dmodel = (const pf_cdef_mlp*)mbase;
+  float* W = (float*)(mbase + ((sizeof(pf_cdef_mlp) + 255) & ~(size_t)255));
   S.a.dirs = S.extra + xBytes + mBytes;
   S.a.ais = (int8_t*)(S.extra + xBytes + mBytes + (size_t)nfb * 64);
   if (launch_features(S.a, params->qindex, X, false, S.st) != cudaSuccess) return PF_ERR_DEVICE;
-  float* W = (float*)(S.extra + xBytes + mBytes + dBytes);
-  if (launch_mlp_masks(dmodel, W, X, nfb, threshold, candidates, masks, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  if (launch_mlp_masks(dmodel, W, changed != 0, X, nfb, threshold, candidates, masks, S.st) != cudaSuccess)
+    return PF_ERR_DEVICE;
   S.a.tmask = masks;
   S.s.refine = (flags & PF_LEARNED_REFINE) ? 1 : 0;
   const int r = search_finish(S, params, mse_out, fb_index_out, result);

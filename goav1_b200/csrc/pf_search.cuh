@@ -52,11 +52,7 @@ struct FinishOut {
 
 struct SelArgs {
   const uint64_t* mse;   // [2][nfb][64]
-  const uint8_t* skip;   // [nfb]
-  int* sb_w;             // non-skip filter blocks (written by the list kernel)
-  int* n_w;              // their count (device)
-  const int* sb;
-  const int* n;
+  const uint8_t* skip;   // [nfb]; the kernels list the non-skip blocks themselves
   int nfb, cap;
   int refine;            // 1: the reference's 4*nb refinement passes after the nb greedy picks
   SelOut* out;
@@ -135,8 +131,8 @@ __device__ __forceinline__ int32_t dir_cost8_dev(int d, const uint8_t* blk, int6
 
 size_t sel_smem_bytes(int nfb, bool rows);
 cudaError_t launch_search(const SearchArgs& a, cudaStream_t st);
-// Non-skip list, the greedy selection for nb = 1..(1 << maxCfg) and the RD
-// finish; everything stays on the device (no host round trip).
+// The greedy selection for nb = 1..(1 << maxCfg) and the RD finish;
+// everything stays on the device (no host round trip).
 cudaError_t launch_select(SelArgs s, int maxCfg, unsigned long long lambda, uint8_t* fbIndex, FinishOut* fo,
                           cudaStream_t st);
 
@@ -146,7 +142,8 @@ cudaError_t launch_select(SelArgs s, int maxCfg, unsigned long long lambda, uint
 cudaError_t launch_features(const SearchArgs& a, int qindex, float* X, bool frameMeans, cudaStream_t st);
 // pf_mlp.cu: the network over X and the tested-trial masks ([nfb][2]).
 size_t mlp_expanded_bytes();  // fp32 copy of the network's parameters
-cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, float* W, const float* X, int nfb, float threshold,
-                             int candidates, uint64_t* masks, cudaStream_t st);
+// W: the fp32 copy, refreshed from dmodel first when `expand` is set.
+cudaError_t launch_mlp_masks(const pf_cdef_mlp* dmodel, float* W, bool expand, const float* X, int nfb,
+                             float threshold, int candidates, uint64_t* masks, cudaStream_t st);
 
 }  // namespace pf
