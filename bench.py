@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-search", action="store_true")
     ap.add_argument("--search-frames", type=int, default=8)
+    ap.add_argument("--no-mixed", action="store_true")
     return ap.parse_args()
 
 
@@ -80,6 +81,101 @@ def make_batch(n, rank, pinned=False):
                 fr.planes[k] = a
                 fr._pin = getattr(fr, "_pin", []) + [t]
     return frames
+
+
+# The mixed batched workload: 48 frames, seeds 100-147, each with full-chain
+# side information of the 1080p workload's kind.
+MIXED_SPECS = ([dict(width=640, height=360)] * 16 + [dict(width=1280, height=720)] * 16 +
+               [dict(width=1920, height=1080, bit_depth=10)] * 8 + [dict(width=1280, height=720, ss=(0, 0))] * 8)
+
+
+def _mixed_frame(i):
+    from goav1_b200 import synth
+
+    return synth.make_frame(1, 100 + i, **MIXED_SPECS[i])
+
+
+def mixed_leg(local, steps, warmup):
+    """48 frames of mixed size, bit depth and chroma format: one batched call
+    (autotuned persistent settings, CUDA graph replay) against the same
+    frames one call each on a plain context.  Inputs reset and L2 flushed
+    between steps, CUDA events on the library stream around the calls."""
+    import multiprocessing as mp
+
+    import torch
+
+    from goav1_b200.postfilter import DeviceFrame, PostFilterRunner, device_side
+
+    with mp.get_context("spawn").Pool(8) as pool:
+        frames = pool.map(_mixed_frame, range(len(MIXED_SPECS)))
+    px = sum(fr.luma_pixels for fr, _ in frames)
+    dev = [(DeviceFrame(fr), DeviceFrame(fr.like()), device_side(si, fr)) for fr, si in frames]
+    pristine = [[t.clone() for t in d.tensors] for d, _, _ in dev]
+    items = [(d.pf(), s.side, dd.pf()) for d, dd, s in dev]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    tuned = PostFilterRunner(device=local)
+    scratch = [(DeviceFrame(fr), DeviceFrame(fr.like()), device_side(si, fr)) for fr, si in frames]
+    tune = tuned.autotune([(d.pf(), s.side, dd.pf()) for d, dd, s in scratch], reps=2)
+    del scratch
+    tuned.batch_graphs(True)
+    plain = PostFilterRunner(device=local)
+    arr = tuned.batch_items(items)
+    singles = [plain.batch_items([it]) for it in items]
+
+    def timed(runner, run):
+        stream = torch.cuda.ExternalStream(runner.stream)
+
+        def reset():
+            with torch.cuda.stream(stream):
+                for (d, _, _), src in zip(dev, pristine):
+                    for t, s0 in zip(d.tensors, src):
+                        t.copy_(s0, non_blocking=True)
+                flush.fill_(1)
+
+        for _ in range(max(warmup, 3)):
+            reset()
+            run()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev:
+            reset()
+            a.record(stream)
+            run()
+            b.record(stream)
+        torch.cuda.synchronize()
+        return statistics.mean(a.elapsed_time(b) for a, b in ev)
+
+    def run_singles():
+        for one in singles:
+            plain.apply_batch(one)
+
+    ms_b = timed(tuned, lambda: tuned.apply_batch(arr))
+    ms_s = timed(plain, run_singles)
+    # Each kind of frame batched on its own (same settings): the mixed queue
+    # against the sum of these is its cost of mixing.
+    kinds = {}
+    for i, spec in enumerate(MIXED_SPECS):
+        kinds.setdefault(tuple(sorted(spec.items())), []).append(i)
+    ms_kinds = 0.0
+    for idx in kinds.values():
+        sub = tuned.batch_items([items[i] for i in idx])
+        ms_kinds += timed(tuned, lambda sub=sub: tuned.apply_batch(sub))
+    tuned.close()
+    plain.close()
+    names = ["deblock", "cdef", "restoration", "film_grain"]
+    return {"metric": "mixed batch Mpix/s", "value": px / (ms_b / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms_b,
+            "single_stream_value": px / (ms_s / 1e3) / 1e6, "single_stream_ms_per_step": ms_s,
+            "batched_over_single_stream": ms_s / ms_b,
+            "homogeneous_batches_ms_sum": ms_kinds, "mixed_rate_over_homogeneous": ms_kinds / ms_b,
+            "autotune": {n: {"ctas": int(tune.ctas[i]), "ms": round(float(tune.ms[i]), 4),
+                             "ms_one_cta_per_item": round(float(tune.ms_default[i]), 4)}
+                         for i, n in enumerate(names)},
+            "config": "48 frames, seeds 100-147: 16x640x360 8-bit 4:2:0, 16x1280x720 8-bit 4:2:0, "
+                      "8x1920x1080 10-bit 4:2:0, 8x1280x720 8-bit 4:4:4, full chain; batched = one pf_batch_apply "
+                      "(autotuned persistent CTAs, CUDA graph replay), single stream = one call per frame, "
+                      "homogeneous = each of the four kinds batched alone; "
+                      "256 MB L2 flush between steps; %.1f Mpix per step" % (px / 1e6)}
 
 
 def side_bytes(si, fr):
@@ -423,6 +519,11 @@ def main():
                        "config": "network goav1_b200/data/cdef_mlp_1080p.bin, threshold 0.5, 3 candidates per "
                                  "head; " + cfg}
 
+    mixed = None
+    if rank == 0 and not args.no_mixed:
+        mixed = mixed_leg(local, args.steps, args.warmup)
+        mixed["per_pixel_rate_vs_1080p_workload"] = mixed["value"] / value * world
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(frames[:8], seconds=10.0)
@@ -434,7 +535,7 @@ def main():
                            "l2": "inputs (%.0f MB per rank) larger than L2, and a 256 MB L2 flush between steps"
                                  % (sum(fr.nbytes() for fr, _ in frames) / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "cdef_search": search,
-                "cdef_search_learned": learned_leg,
+                "cdef_search_learned": learned_leg, "mixed_batch": mixed,
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))
     runner.close()

@@ -57,6 +57,10 @@ def lib():
                                          C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                          C.POINTER(abi.pf_cdef_search_result),
                                          C.POINTER(abi.pf_cdef_learned_stats)]
+    L.pf_batch_graphs.argtypes = [C.c_void_p, C.c_int32]
+    L.pf_set_persistent.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+    L.pf_autotune.argtypes = [C.c_void_p, C.POINTER(abi.pf_batch_item), C.c_int32, C.c_int32,
+                              C.POINTER(abi.pf_tune_result)]
     if L.pf_abi_version() != 1:
         raise RuntimeError("goav1_b200: ABI version mismatch")
     _lib = L

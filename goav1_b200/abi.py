@@ -206,6 +206,16 @@ class pf_cdef_search_result(C.Structure):
 
 
 PF_LEARNED_REFINE = 1
+PF_TUNE_DEBLOCK, PF_TUNE_CDEF, PF_TUNE_RESTORATION, PF_TUNE_FILM_GRAIN, PF_TUNE_GROUPS = 0, 1, 2, 3, 4
+
+
+class pf_tune_result(C.Structure):
+    _fields_ = [
+        ("ctas", C.c_int32 * PF_TUNE_GROUPS),
+        ("ms", C.c_float * PF_TUNE_GROUPS),
+        ("ms_default", C.c_float * PF_TUNE_GROUPS),
+    ]
+
 PF_MLP_FEATURES = 40
 PF_MLP_HIDDEN = 64
 PF_MLP_CLASSES = 64
@@ -280,4 +290,7 @@ EXPORTED_SYMBOLS = (
     "pf_cdef_mlp_gradients",
     "pf_cdef_mlp_train",
     "pf_cdef_search_learned",
+    "pf_batch_graphs",
+    "pf_set_persistent",
+    "pf_autotune",
 )

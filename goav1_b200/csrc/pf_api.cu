@@ -83,6 +83,43 @@ struct pf_ctx {
   std::vector<uint8_t> hside;
   // Persistent-CTA count per stage (0 = one CTA per work item).
   int persistent[ST_COUNT] = {};
+  // CUDA graphs of pf_batch_apply, one per batch signature (see run_batch).
+  int graphs = 0;
+  std::vector<struct GraphEntry*> gcache;
+  uint64_t gclock = 0;
+};
+
+// One captured batch signature, in two slots used in turn: each slot is a
+// graph and the page-locked copies of the job table, prefix arrays and side
+// information its copy nodes read when it runs.  A replay waits for the
+// slot's previous run (its event) before rewriting those buffers, so the host
+// can prepare one batch while the previous one is still on the GPU.
+struct GraphSlot {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t done = nullptr;
+  void* pjobs = nullptr;
+  void* pbase = nullptr;
+  void* pside = nullptr;
+};
+
+struct GraphEntry {
+  std::vector<int64_t> key;
+  void* bufs[5] = {};  // the context scratch the captured kernels address
+  GraphSlot slot[2];
+  int next = 0;
+  uint64_t used = 0;
+  ~GraphEntry() {
+    for (GraphSlot& g : slot) {
+      if (g.done) cudaEventSynchronize(g.done);
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      if (g.graph) cudaGraphDestroy(g.graph);
+      if (g.done) cudaEventDestroy(g.done);
+      if (g.pjobs) cudaFreeHost(g.pjobs);
+      if (g.pbase) cudaFreeHost(g.pbase);
+      if (g.pside) cudaFreeHost(g.pside);
+    }
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -344,6 +381,8 @@ extern "C" void pf_destroy(pf_ctx* c) {
   DevBuf* bufs[] = {&c->io, &c->disp, &c->arena, &c->sidebuf, &c->jobs, &c->bases, &c->counters, &c->search};
   for (DevBuf* b : bufs) b->release();
   c->model.release();
+  for (GraphEntry* g : c->gcache) delete g;
+  c->gcache.clear();
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->model_pin) cudaFreeHost(c->model_pin);
   for (int i = 0; i < 8; i++)
@@ -649,44 +688,19 @@ static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, std::vector
   }
 }
 
-// Builds the job table for n validated frames and queues every stage.
-static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats) {
+// Queues the copies of the host tables (from the given host buffers) and
+// every stage's launch on the context's streams.
+static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, const uint8_t* hside, int n, bool fg) {
   const cudaStream_t st = c->stream;
-  size_t arenaBytes = 0, sideBytes = 0;
-  for (int i = 0; i < n; i++) {
-    arenaBytes += frame_scratch(refs[i].f, refs[i].s);
-    sideBytes += frame_side_bytes(refs[i].f, refs[i].s);
-  }
-  CK(c->arena.ensure(arenaBytes + 256));
-  CK(c->sidebuf.ensure(sideBytes + 256));
-  Cursor arena{(uint8_t*)c->arena.p, 0}, side{(uint8_t*)c->sidebuf.p, 0};
-  c->hjobs.resize(n);
-  c->hbase.assign((size_t)ST_COUNT * (n + 1), 0);
-  c->hside.clear();
-  uint32_t done = 0;
-  for (int i = 0; i < n; i++) {
-    int counts[ST_COUNT];
-    fill_job(refs[i], arena, side, c->hside, c->hjobs[i], counts);
-    for (int k = 0; k < ST_COUNT; k++) c->hbase[(size_t)k * (n + 1) + i + 1] = c->hbase[(size_t)k * (n + 1) + i] + counts[k];
-    const pf_frame_side* s = refs[i].s;
-    if (counts[ST_DEBLOCK_V]) done |= PF_STAGE_LOOP_FILTER;
-    if (cdef_any(refs[i].f, s)) done |= PF_STAGE_CDEF;
-    if (lr_any(s)) done |= PF_STAGE_LOOP_RESTORATION;
-    if (s->stages & PF_STAGE_EXTEND_BORDERS) done |= PF_STAGE_EXTEND_BORDERS;
-    if (counts[ST_FG_TEMPLATES]) done |= PF_STAGE_FILM_GRAIN;
-  }
-  if (!c->hside.empty()) CK(cudaMemcpyAsync(c->sidebuf.p, c->hside.data(), c->hside.size(), cudaMemcpyHostToDevice, st));
-  CK(c->jobs.ensure(sizeof(FrameJob) * n));
-  CK(c->bases.ensure(sizeof(int) * c->hbase.size()));
-  CK(c->counters.ensure(sizeof(int) * ST_COUNT));
-  CK(cudaMemcpyAsync(c->jobs.p, c->hjobs.data(), sizeof(FrameJob) * n, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(c->bases.p, c->hbase.data(), sizeof(int) * c->hbase.size(), cudaMemcpyHostToDevice, st));
+  if (!c->hside.empty()) CK(cudaMemcpyAsync(c->sidebuf.p, hside, c->hside.size(), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->jobs.p, hjobs, sizeof(FrameJob) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->bases.p, hbase, sizeof(int) * c->hbase.size(), cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync(c->counters.p, 0, sizeof(int) * ST_COUNT, st));
   BatchArgs b;
   b.jobs = (const FrameJob*)c->jobs.p;
   b.base = (const int*)c->bases.p;
   b.n = n;
-  auto total = [&](int k) { return c->hbase[(size_t)k * (n + 1) + n]; };
+  auto total = [&](int k) { return hbase[(size_t)k * (n + 1) + n]; };
   auto args = [&](int k, int* grid) {
     BatchArgs a = b;
     const int t = total(k);
@@ -701,7 +715,6 @@ static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats) {
   };
   int g;
   // Film-grain templates and offsets depend on nothing else: side stream.
-  const bool fg = total(ST_FG_TEMPLATES) > 0;
   if (fg) {
     CK(cudaEventRecord(c->fork, st));
     CK(cudaStreamWaitEvent(c->side, c->fork, 0));
@@ -730,6 +743,113 @@ static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats) {
   a = args(ST_FG_APPLY, &g);
   CK(launch_fg_apply_batch(a, total(ST_FG_APPLY), g, st));
   if (c->timing) CK(cudaEventRecord(c->ev[5], st));
+  return PF_OK;
+}
+
+// The batch signature: everything that shapes the launch sequence (grid
+// sizes follow from the prefix arrays and the persistent settings, copy
+// sizes from n and the side-information bytes).
+static std::vector<int64_t> batch_key(const pf_ctx* c, int n, bool fg) {
+  std::vector<int64_t> k;
+  k.reserve(8 + ST_COUNT + c->hbase.size());
+  k.push_back(n);
+  k.push_back((int64_t)c->hside.size());
+  k.push_back(fg);
+  for (int i = 0; i < ST_COUNT; i++) k.push_back(c->persistent[i]);
+  for (int v : c->hbase) k.push_back(v);
+  return k;
+}
+
+// Replays the graph captured for this batch signature (capturing the slot on
+// its first use; at most 8 signatures kept, least recently used dropped).  A
+// graph addresses the context's scratch buffers, so it is recaptured after
+// any of them moved.
+static int replay_or_capture(pf_ctx* c, int n, bool fg) {
+  const cudaStream_t st = c->stream;
+  const std::vector<int64_t> key = batch_key(c, n, fg);
+  void* bufs[5] = {c->arena.p, c->sidebuf.p, c->jobs.p, c->bases.p, c->counters.p};
+  const size_t nj = sizeof(FrameJob) * n, nb = sizeof(int) * c->hbase.size(), ns = c->hside.size();
+  GraphEntry* e = nullptr;
+  for (GraphEntry* x : c->gcache)
+    if (x->key == key && memcmp(x->bufs, bufs, sizeof(bufs)) == 0) e = x;
+  if (!e) {
+    if (c->gcache.size() >= 8) {
+      auto lru = std::min_element(c->gcache.begin(), c->gcache.end(),
+                                  [](const GraphEntry* a, const GraphEntry* b) { return a->used < b->used; });
+      delete *lru;
+      c->gcache.erase(lru);
+    }
+    e = new GraphEntry();
+    e->key = key;
+    memcpy(e->bufs, bufs, sizeof(bufs));
+    c->gcache.push_back(e);
+  }
+  e->used = ++c->gclock;
+  GraphSlot& g = e->slot[e->next];
+  e->next ^= 1;
+  if (!g.exec) {
+    if (cudaMallocHost(&g.pjobs, nj + 16) != cudaSuccess || cudaMallocHost(&g.pbase, nb + 16) != cudaSuccess ||
+        cudaMallocHost(&g.pside, ns + 16) != cudaSuccess)
+      return PF_ERR_DEVICE;
+    CK(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+  } else {
+    CK(cudaEventSynchronize(g.done));  // the slot's previous run has read its tables
+  }
+  memcpy(g.pjobs, c->hjobs.data(), nj);
+  memcpy(g.pbase, c->hbase.data(), nb);
+  if (ns) memcpy(g.pside, c->hside.data(), ns);
+  if (!g.exec) {
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int est = enqueue_batch(c, (const FrameJob*)g.pjobs, (const int*)g.pbase, (const uint8_t*)g.pside, n, fg);
+    const cudaError_t ce = cudaStreamEndCapture(st, &g.graph);
+    cudaError_t ie = cudaSuccess;
+    if (est == PF_OK && ce == cudaSuccess) ie = cudaGraphInstantiate(&g.exec, g.graph, 0);
+    if (est != PF_OK || ce != cudaSuccess || ie != cudaSuccess) {
+      if (g.graph) cudaGraphDestroy(g.graph);
+      g.graph = nullptr;
+      g.exec = nullptr;
+      if (est != PF_OK) return est;
+      CK(ce != cudaSuccess ? ce : ie);
+    }
+  }
+  CK(cudaGraphLaunch(g.exec, st));
+  CK(cudaEventRecord(g.done, st));
+  return PF_OK;
+}
+
+// Builds the job table for n validated frames and queues every stage.
+static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats, bool useGraph = false) {
+  size_t arenaBytes = 0, sideBytes = 0;
+  for (int i = 0; i < n; i++) {
+    arenaBytes += frame_scratch(refs[i].f, refs[i].s);
+    sideBytes += frame_side_bytes(refs[i].f, refs[i].s);
+  }
+  CK(c->arena.ensure(arenaBytes + 256));
+  CK(c->sidebuf.ensure(sideBytes + 256));
+  Cursor arena{(uint8_t*)c->arena.p, 0}, side{(uint8_t*)c->sidebuf.p, 0};
+  c->hjobs.resize(n);
+  c->hbase.assign((size_t)ST_COUNT * (n + 1), 0);
+  c->hside.clear();
+  uint32_t done = 0;
+  for (int i = 0; i < n; i++) {
+    int counts[ST_COUNT];
+    fill_job(refs[i], arena, side, c->hside, c->hjobs[i], counts);
+    for (int k = 0; k < ST_COUNT; k++) c->hbase[(size_t)k * (n + 1) + i + 1] = c->hbase[(size_t)k * (n + 1) + i] + counts[k];
+    const pf_frame_side* s = refs[i].s;
+    if (counts[ST_DEBLOCK_V]) done |= PF_STAGE_LOOP_FILTER;
+    if (cdef_any(refs[i].f, s)) done |= PF_STAGE_CDEF;
+    if (lr_any(s)) done |= PF_STAGE_LOOP_RESTORATION;
+    if (s->stages & PF_STAGE_EXTEND_BORDERS) done |= PF_STAGE_EXTEND_BORDERS;
+    if (counts[ST_FG_TEMPLATES]) done |= PF_STAGE_FILM_GRAIN;
+  }
+  CK(c->jobs.ensure(sizeof(FrameJob) * n));
+  CK(c->bases.ensure(sizeof(int) * c->hbase.size()));
+  CK(c->counters.ensure(sizeof(int) * ST_COUNT));
+  const bool fg = c->hbase[(size_t)ST_FG_TEMPLATES * (n + 1) + n] > 0;
+  const int est = (useGraph && !c->timing) ? replay_or_capture(c, n, fg)
+                                           : enqueue_batch(c, c->hjobs.data(), c->hbase.data(), c->hside.data(), n, fg);
+  if (est != PF_OK) return est;
+  auto total = [&](int k) { return c->hbase[(size_t)k * (n + 1) + n]; };
   if (stats) {
     stats->completed = done;
     stats->cdef_units = total(ST_CDEF);
@@ -834,7 +954,7 @@ extern "C" int pf_batch_apply(pf_ctx* c, const pf_batch_item* items, int32_t n, 
   }
   CK(cudaSetDevice(c->device));
   if (stats) memset(stats, 0, sizeof(*stats));
-  int st = run_batch(c, refs.data(), n, stats);
+  int st = run_batch(c, refs.data(), n, stats, c->graphs != 0);
   if (st != PF_OK) return st;
   bool hostSide = false;
   for (int i = 0; i < n; i++) hostSide |= items[i].side->side_memory == PF_MEM_HOST;
@@ -893,4 +1013,65 @@ void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, size_
     return nullptr;
   }
   return c->model.p;
+}
+
+// ---------------------------------------------------------------------------
+// Batch scheduling: graphs, persistent CTAs and the autotuner.
+
+extern "C" int pf_batch_graphs(pf_ctx* c, int32_t enable) {
+  if (!c || (enable != 0 && enable != 1)) return PF_ERR_INVALID_ARG;
+  c->graphs = enable;
+  if (!enable) {
+    for (GraphEntry* g : c->gcache) delete g;
+    c->gcache.clear();
+  }
+  return PF_OK;
+}
+
+// The stages each tunable group sets.
+static const int kTuneStages[PF_TUNE_GROUPS][2] = {
+    {ST_DEBLOCK_V, ST_DEBLOCK_H}, {ST_CDEF, -1}, {ST_LR, -1}, {ST_FG_APPLY, -1}};
+static const int kTuneStatIndex[PF_TUNE_GROUPS] = {0, 1, 2, 4};  // pf_stats.stage_ms
+
+extern "C" int pf_set_persistent(pf_ctx* c, int32_t group, int32_t ctas) {
+  if (!c || group < 0 || group >= PF_TUNE_GROUPS || ctas < 0 || ctas > (1 << 20)) return PF_ERR_INVALID_ARG;
+  for (int k : kTuneStages[group])
+    if (k >= 0) c->persistent[k] = ctas;
+  return PF_OK;
+}
+
+extern "C" int pf_autotune(pf_ctx* c, const pf_batch_item* items, int32_t n, int32_t reps, pf_tune_result* out) {
+  if (!c || !items || n <= 0 || reps <= 0 || reps > 1000 || !out) return PF_ERR_INVALID_ARG;
+  const int savedTiming = c->timing;
+  c->timing = 1;  // per-stage CUDA events; no graphs while timing
+  memset(out, 0, sizeof(*out));
+  static const int kMult[] = {0, 1, 2, 4, 8, 16};  // x SM count; 0 = one CTA per work item
+  int status = PF_OK;
+  for (int gi = 0; gi < PF_TUNE_GROUPS && status == PF_OK; gi++) {
+    float best = 3.4e38f;
+    int bestCtas = 0;
+    for (int m : kMult) {
+      const int ctas = m * c->sm_count;
+      pf_set_persistent(c, gi, ctas);
+      std::vector<float> t;
+      for (int r = 0; r <= reps && status == PF_OK; r++) {  // run 0 warms up
+        pf_stats st;
+        status = pf_batch_apply(c, items, n, &st);
+        if (r > 0 && status == PF_OK) t.push_back(st.stage_ms[kTuneStatIndex[gi]]);
+      }
+      if (status != PF_OK) break;
+      std::sort(t.begin(), t.end());
+      const float med = t[t.size() / 2];
+      if (m == 0) out->ms_default[gi] = med;
+      if (med < best) {
+        best = med;
+        bestCtas = ctas;
+      }
+    }
+    pf_set_persistent(c, gi, bestCtas);
+    out->ctas[gi] = bestCtas;
+    out->ms[gi] = best;
+  }
+  c->timing = savedTiming;
+  return status;
 }

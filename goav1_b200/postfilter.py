@@ -111,15 +111,38 @@ class PostFilterRunner:
         self._display = display if (side.stages & abi.PF_STAGE_FILM_GRAIN) else None
         return self.stats
 
-    def apply_batch(self, items):
-        """items: list of (frame, side, display) device-resident triples."""
+    @staticmethod
+    def batch_items(items):
+        """ctypes array of pf_batch_item from (frame, side, display) triples."""
         arr = (abi.pf_batch_item * len(items))()
         for i, (f, s, d) in enumerate(items):
             arr[i].frame = C.pointer(f)
             arr[i].side = C.pointer(s)
             arr[i].display = C.pointer(d) if d is not None else None
-        check(lib().pf_batch_apply(self._h, arr, len(items), C.byref(self.stats)))
+        return arr
+
+    def apply_batch(self, items):
+        """items: list of (frame, side, display) device-resident triples, or
+        an array from batch_items()."""
+        arr = items if isinstance(items, C.Array) else self.batch_items(items)
+        check(lib().pf_batch_apply(self._h, arr, len(arr), C.byref(self.stats)))
         return self.stats
+
+    def batch_graphs(self, enable=True):
+        """Capture pf_batch_apply as CUDA graphs per batch signature."""
+        check(lib().pf_batch_graphs(self._h, int(enable)))
+
+    def set_persistent(self, group, ctas):
+        """Persistent CTA count of a stage group (abi.PF_TUNE_*); 0 = one CTA per item."""
+        check(lib().pf_set_persistent(self._h, group, ctas))
+
+    def autotune(self, items, reps=3):
+        """Picks each stage group's persistent setting on this batch (run in
+        place: pass copies).  Returns pf_tune_result."""
+        arr = items if isinstance(items, C.Array) else self.batch_items(items)
+        out = abi.pf_tune_result()
+        check(lib().pf_autotune(self._h, arr, len(arr), reps, C.byref(out)))
+        return out
 
     def cdef_search(self, source, recon, noskip, qindex, lam, max_presets=8, damping=0, want_mse=True):
         """Encoder CDEF strength search (cdefSearcher.search + finish,

@@ -265,6 +265,38 @@ typedef struct pf_batch_item {
  * CTAs (one per SM).  Equivalent to n pf_frame_apply calls. */
 int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats* stats);
 
+/* ---- batch scheduling (no counterpart in the reference) ----
+ * pf_batch_apply queues one launch per stage for all frames of a batch; each
+ * work item (a tile or unit of one plane of one frame) is found from per-stage
+ * prefix counts.  Two knobs shape those launches:
+ *   - CUDA graphs (pf_batch_graphs): the first batch of a given signature
+ *     (frame count, each frame's work per stage, side-information bytes and
+ *     the persistent settings) is captured as a graph and later batches of
+ *     that signature replay it, with only their job tables refreshed.  Up to
+ *     8 signatures are kept; a change of the context's scratch buffers
+ *     recaptures.  Graphs are not used while the context times stages.
+ *   - Persistent CTAs (pf_set_persistent): per stage group, a fixed number
+ *     of CTAs draining the stage's items through an atomic counter instead
+ *     of one CTA per item (0).
+ * pf_autotune picks the persistent setting of each group on a given batch:
+ * for each group it runs the batch reps + 1 times per candidate (one CTA per
+ * item, then 1, 2, 4, 8 and 16 CTAs per SM), keeps the candidate with the
+ * lowest median stage time, and leaves the winners set on the context.  It
+ * runs the batch in place, so pass frames whose contents may be overwritten
+ * (copies).  out->ms_default is the one-CTA-per-item time of each group. */
+enum { PF_TUNE_DEBLOCK = 0, PF_TUNE_CDEF = 1, PF_TUNE_RESTORATION = 2, PF_TUNE_FILM_GRAIN = 3, PF_TUNE_GROUPS = 4 };
+
+typedef struct pf_tune_result {
+  int32_t ctas[PF_TUNE_GROUPS];      /* chosen persistent CTA count (0 = one per item) */
+  float ms[PF_TUNE_GROUPS];          /* its median stage time */
+  float ms_default[PF_TUNE_GROUPS];  /* one CTA per item */
+} pf_tune_result;
+
+int pf_batch_graphs(pf_ctx* ctx, int32_t enable);
+int pf_set_persistent(pf_ctx* ctx, int32_t group, int32_t ctas);
+int pf_autotune(pf_ctx* ctx, const pf_batch_item* items, int32_t n, int32_t reps,
+                pf_tune_result* out);
+
 /* ---- encoder CDEF strength search (cdef_search.go) ---- */
 typedef struct pf_cdef_search_params {
   int32_t qindex;        /* frame base_q_idx */

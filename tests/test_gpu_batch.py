@@ -1,0 +1,120 @@
+"""Batch scheduling on the GPU: CUDA-graph capture and replay, persistent
+CTAs and the autotuner must not change a single sample.
+
+The batch is a reduced form of the mixed workload (640x360 and 1280x720
+8-bit 4:2:0, 1920x1080 10-bit 4:2:0, 1280x720 8-bit 4:4:4, each with its own
+seed and full-chain side information); every frame is compared bit-exactly
+with the oracle (tolerance zero, integer arithmetic)."""
+
+import numpy as np
+import pytest
+
+from goav1_b200 import abi, synth
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [dict(width=640, height=360)] * 3 + [dict(width=1280, height=720)] * 2 + \
+        [dict(width=1920, height=1080, bit_depth=10)] + [dict(width=1280, height=720, ss=(0, 0))] * 2
+
+
+def mixed_frames(seed0=100):
+    return [synth.make_frame(1, seed0 + i, **kw) for i, kw in enumerate(SPECS)]
+
+
+@pytest.fixture(scope="module")
+def frames():
+    return mixed_frames()
+
+
+@pytest.fixture(scope="module")
+def expected(frames):
+    import oracle_ctypes
+
+    out = []
+    for fr, si in frames:
+        ref, disp = fr.copy(), fr.like()
+        assert oracle_ctypes.frame_apply(ref.pf(), si.side, disp.pf()) == 0
+        out.append((ref, disp))
+    return out
+
+
+class Batch:
+    """Device copies of the frames, displays and side information."""
+
+    def __init__(self, frames):
+        from goav1_b200.postfilter import DeviceFrame, device_side
+
+        self.frames = frames
+        self.dev = [(DeviceFrame(fr), DeviceFrame(fr.like()), device_side(si, fr)) for fr, si in frames]
+        self.items = [(d.pf(), s.side, dd.pf()) for d, dd, s in self.dev]
+
+    def reset(self):
+        for (fr, _), (d, _, _) in zip(self.frames, self.dev):
+            d.upload(fr)
+
+
+def assert_batch(batch, expected, what):
+    for i, ((ref, disp), (d, dd, _)) in enumerate(zip(expected, batch.dev)):
+        for name, a, b in (("reference", ref, d.download()), ("display", disp, dd.download())):
+            for p, (pa, pb) in enumerate(zip(a.planes, b.planes)):
+                assert np.array_equal(pa, pb), "%s: frame %d %s plane %d differs in %d samples" % (
+                    what, i, name, p, int((pa != pb).sum()))
+
+
+def test_graph_capture_and_replays_match_oracle(frames, expected):
+    from goav1_b200.postfilter import PostFilterRunner
+
+    r = PostFilterRunner()
+    r.batch_graphs(True)
+    b = Batch(frames)
+    # Run 1 captures slot A, run 2 slot B, runs 3 and 4 replay them.
+    for run in range(4):
+        b.reset()
+        r.apply_batch(b.items)
+        r.sync()
+        assert_batch(b, expected, "graph run %d" % run)
+    r.close()
+
+
+def test_persistent_ctas_match_oracle(frames, expected):
+    from goav1_b200.postfilter import PostFilterRunner
+
+    r = PostFilterRunner()
+    for g in range(abi.PF_TUNE_GROUPS):
+        r.set_persistent(g, 296)
+    b = Batch(frames)
+    r.apply_batch(b.items)
+    r.sync()
+    assert_batch(b, expected, "persistent")
+    r.close()
+
+
+def test_autotune_then_graphs_match_oracle(frames, expected):
+    from goav1_b200.postfilter import PostFilterRunner
+
+    r = PostFilterRunner()
+    scratch = Batch(frames)  # the tuner filters these in place
+    res = r.autotune(scratch.items, reps=1)
+    assert all(c >= 0 for c in res.ctas) and all(m > 0 for m in res.ms)
+    assert all(m <= d for m, d in zip(res.ms, res.ms_default))
+    r.batch_graphs(True)
+    b = Batch(frames)
+    for run in range(2):
+        b.reset()
+        r.apply_batch(b.items)
+        r.sync()
+        assert_batch(b, expected, "tuned run %d" % run)
+    r.close()
+
+
+def test_scheduling_arguments_are_checked():
+    from goav1_b200.postfilter import ErrInvalidArgument, PostFilterRunner
+
+    r = PostFilterRunner()
+    with pytest.raises(ErrInvalidArgument):
+        r.set_persistent(abi.PF_TUNE_GROUPS, 10)
+    with pytest.raises(ErrInvalidArgument):
+        r.set_persistent(0, -1)
+    with pytest.raises(ErrInvalidArgument):
+        r.batch_graphs(2)
+    r.close()
