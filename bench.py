@@ -56,10 +56,9 @@ def parse():
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from goav1_b200 import dist
+
+    return dist.env()
 
 
 def make_batch(n, rank, pinned=False):
@@ -67,8 +66,10 @@ def make_batch(n, rank, pinned=False):
 
     frames = []
     tex = None
-    for i in range(n):
-        fr, si = synth.make_frame(1, 2, frame_index=rank * n + i, texture=tex)
+    from goav1_b200 import dist
+
+    for i in dist.shard(n, rank):
+        fr, si = synth.make_frame(1, 2, frame_index=i, texture=tex)
         frames.append((fr, si))
     if pinned:
         import torch
@@ -325,13 +326,11 @@ def main():
     rank, world, local = dist_env()
     import torch
 
+    from goav1_b200 import dist
+
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init("nccl")
     from goav1_b200 import abi
     from goav1_b200.postfilter import DeviceFrame, PostFilterRunner, device_side
 
@@ -363,8 +362,7 @@ def main():
     torch.cuda.synchronize()
     launches_per_step = 7  # one launch per stage for the whole batch
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
+    dist.barrier(world)
     torch.cuda.synchronize()
     t_on = time.time()
     for k in range(args.steps):
@@ -374,15 +372,10 @@ def main():
         ev[k][1].record(stream)
     torch.cuda.synchronize()
     clocks.mark(t_on, time.time())
-    if world > 1:
-        torch.distributed.barrier()
+    dist.barrier(world)
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    ms = statistics.mean(step_ms)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = dist.max_over_ranks(statistics.mean(step_ms), world, device="cuda")
     px = sum(fr.luma_pixels for fr, _ in frames)
     value = world * px / (ms / 1e3) / 1e6
 
@@ -452,11 +445,7 @@ def main():
                 runner.apply(out.pf(), si.side, disp.pf())
             torch.cuda.synchronize()
             ehost.append(time.perf_counter() - t0)
-        es = statistics.mean(ehost)
-        if world > 1:
-            t = torch.tensor([es], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            es = float(t.item())
+        es = dist.max_over_ranks(statistics.mean(ehost), world, device="cuda")
         e2e = {"value": world * px / es / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "note": "pinned host frames, one pf_frame_apply call per frame"}
 
@@ -540,6 +529,8 @@ def main():
         print(json.dumps(line))
     runner.close()
     if world > 1:
+        import torch.distributed
+
         torch.distributed.destroy_process_group()
 
 
