@@ -161,8 +161,8 @@ __device__ __forceinline__ int blend_w(int prev, int cur, int pw, int cw, int bd
 // One column x of up to 4 rows y0.. of one display plane (all inside one
 // 32-row grain block row): per-block values once, then per sample.
 template <typename T>
-__device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& disp, const FgArgs& a, int plane, int x,
-                                             int y0, int nrows) {
+__device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& disp, const FgArgs& a, const uint8_t* lut,
+                                             int plane, int x, int y0, int nrows) {
   const DPlane& sp = ref.pl[plane];
   const DPlane& dp = disp.pl[plane];
   if (x >= sp.aw) return;
@@ -206,7 +206,6 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
   }
   // Horizontal blend weights: luma 27/17 then 17/27; subsampled chroma 23/22.
   const int hpw = sx ? 23 : (xi == 1 ? 17 : 27), hcw = sx ? 22 : (xi == 1 ? 27 : 17);
-  const uint8_t* lut = a.lut[plane];
   const int shift = a.scaling_shift;
   int minV = 0, maxV = (256 << (bd - 8)) - 1;
   if (a.clip_restricted) {
@@ -284,8 +283,11 @@ __global__ void __launch_bounds__(64) k_fg_offsets_batch(BatchArgs b) {
   });
 }
 
-// Display frame: 64x16-sample tiles of each plane, 256 threads x 4 rows.
+// Display frame: 64x32-sample tiles of each plane, 256 threads x 8 rows (a
+// thread's rows stay inside one grain block: blocks are 32 or 16 rows high).
+// The plane's scaling table is staged in shared memory per tile.
 __global__ void __launch_bounds__(256) k_fg_apply_batch(BatchArgs b) {
+  __shared__ uint8_t s_lut[256];
   const int* base = b.base + ST_FG_APPLY * (b.n + 1);
   for_each_item(base[b.n], b.counters ? b.counters + ST_FG_APPLY : nullptr, [&](int item) {
     const int fi = find_frame(base, b.n, item);
@@ -296,13 +298,16 @@ __global__ void __launch_bounds__(256) k_fg_apply_batch(BatchArgs b) {
       local -= J.fg_tx[plane] * J.fg_ty[plane];
       plane++;
     }
+    s_lut[threadIdx.x] = J.fg.lut[plane][threadIdx.x];
+    __syncthreads();
     const int tx = local % J.fg_tx[plane], ty = local / J.fg_tx[plane];
     const int x = tx * 64 + (threadIdx.x & 63);
-    const int y0 = ty * 16 + (threadIdx.x >> 6) * 4;
+    const int y0 = ty * 32 + (threadIdx.x >> 6) * 8;
     if (J.io.bd == 8)
-      fg_apply_col<uint8_t>(J.io, J.disp, J.fg, plane, x, y0, 4);
+      fg_apply_col<uint8_t>(J.io, J.disp, J.fg, s_lut, plane, x, y0, 8);
     else
-      fg_apply_col<uint16_t>(J.io, J.disp, J.fg, plane, x, y0, 4);
+      fg_apply_col<uint16_t>(J.io, J.disp, J.fg, s_lut, plane, x, y0, 8);
+    __syncthreads();  // the table is rewritten by the next tile (persistent CTAs)
   });
 }
 
