@@ -318,6 +318,29 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def cpu_baseline_lr_search(pair, seconds=5.0):
+    """The LR search oracle (C++ restatement of goav1's Go search) on one
+    host thread, repeated on one 1080p frame for about `seconds`."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_ctypes
+
+    from goav1_b200 import abi
+
+    src, rec, _ = pair
+    horz, vert = abi.lr_unit_grid(rec.width, rec.height)
+    units = (abi.pf_lr_search_unit * (horz * vert))()
+    out = rec.copy()
+    lib = oracle_ctypes.lib()
+    t0 = time.perf_counter()
+    calls = 0
+    while calls == 0 or time.perf_counter() - t0 < seconds:
+        assert lib.oracle_lr_search(C.byref(src.pf()), C.byref(rec.pf()), C.byref(out.pf()), units, len(units)) == 0
+        calls += 1
+    dt = time.perf_counter() - t0
+    return {"value": calls * len(units) / dt, "unit": "units/s", "ms_per_frame": dt / calls * 1e3, "cores": 1,
+            "kind": "port", "sample": "%d calls on one 1920x1080 frame (seed 2000) in %.1f s, one thread" % (calls, dt)}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -508,6 +531,45 @@ def main():
                        "config": "network goav1_b200/data/cdef_mlp_1080p.bin, threshold 0.5, 3 candidates per "
                                  "head; " + cfg}
 
+    # Encoder loop-restoration search (pf_lr_search: every 64x64 luma unit
+    # searched with the six Wiener tap sets and the four SGR presets, the
+    # decision applied into an output frame) on 1080p 8-bit 4:2:0 frames
+    # (seeds 2000..), both frames resident in HBM.  Units/s per call, host
+    # round trip of the unit records included.  The oracle's time on one
+    # frame (one host thread) is reported beside it.  Rank 0 only.
+    lr_leg = None
+    if not args.no_search and rank == 0:
+        from goav1_b200 import synth
+
+        n_lr = max(1, args.search_frames)
+        times, units_total, kinds = [], 0, [0, 0, 0, 0]
+        for i in range(n_lr):
+            src, rec, _ = synth.make_lr_search_pair(2000 + i, 1920, 1080)
+            dsrc, drec, dout = DeviceFrame(src), DeviceFrame(rec), DeviceFrame(rec.like())
+            sp, rp, op = dsrc.pf(), drec.pf(), dout.pf()
+            units = runner.lr_search(sp, rp, op)
+            units_total += len(units)
+            for u in units:
+                kinds[u.unit.type] += 1
+            reps = max(3, args.steps // 4)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                runner.lr_search(sp, rp, op)
+            torch.cuda.synchronize()
+            times.append((time.perf_counter() - t0) / reps)
+        per_frame = statistics.mean(times)
+        lr_leg = {"metric": "LR search units/s", "value": units_total / sum(times), "unit": "units/s",
+                  "ms_per_frame": per_frame * 1e3, "mpix_per_s": 1920 * 1080 / per_frame / 1e6,
+                  "decisions": {"none": kinds[abi.PF_LR_NONE], "wiener": kinds[abi.PF_LR_WIENER],
+                                "sgrproj": kinds[abi.PF_LR_SGRPROJ]},
+                  "config": "%d frames 1920x1080 8-bit 4:2:0 (seeds 2000-%d, make_lr_search_pair), 510 luma units "
+                            "of 64 per frame, 6 Wiener sets + 4 SGR presets per unit, decision applied into an "
+                            "output frame, device-resident, host round trip of the unit records per call"
+                            % (n_lr, 1999 + n_lr)}
+        if world == 1 and not args.no_cpu:
+            lr_leg["cpu_baseline"] = cpu_baseline_lr_search(synth.make_lr_search_pair(2000, 1920, 1080))
+
     mixed = None
     if rank == 0 and not args.no_mixed:
         mixed = mixed_leg(local, args.steps, args.warmup)
@@ -524,7 +586,7 @@ def main():
                            "l2": "inputs (%.0f MB per rank) larger than L2, and a 256 MB L2 flush between steps"
                                  % (sum(fr.nbytes() for fr, _ in frames) / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "cdef_search": search,
-                "cdef_search_learned": learned_leg, "mixed_batch": mixed,
+                "cdef_search_learned": learned_leg, "lr_search": lr_leg, "mixed_batch": mixed,
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))
     runner.close()

@@ -271,6 +271,33 @@ class pf_cdef_learned_stats(C.Structure):
     ]
 
 
+PF_LR_WIENER_CANDIDATES = 6
+PF_LR_SGR_PRESETS = 4
+
+
+class pf_lr_search_unit(C.Structure):
+    _fields_ = [
+        ("x0", C.c_int32),
+        ("y0", C.c_int32),
+        ("x1", C.c_int32),
+        ("y1", C.c_int32),
+        ("base_sse", C.c_uint64),
+        ("sse", C.c_uint64),
+        ("wiener_sse", C.c_uint64),
+        ("sgr_sse", C.c_uint64),
+        ("wiener_candidate", C.c_int8),
+        ("sgr_preset", C.c_int8),
+        ("reserved", C.c_uint8 * 2),
+        ("unit", pf_lr_unit),
+    ]
+
+
+def lr_unit_grid(width, height):
+    """(horz, vert) luma restoration units of 64 samples
+    (tile/restoration_schedule.go:400-409)."""
+    return max((width + 32) // 64, 1), max((height + 32) // 64, 1)
+
+
 # Every symbol include/goav1pf.h declares (checked by tests/test_abi.py).
 EXPORTED_SYMBOLS = (
     "pf_abi_version",
@@ -293,4 +320,5 @@ EXPORTED_SYMBOLS = (
     "pf_batch_graphs",
     "pf_set_persistent",
     "pf_autotune",
+    "pf_lr_search",
 )

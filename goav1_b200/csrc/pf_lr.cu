@@ -44,121 +44,76 @@ __device__ __forceinline__ uint32_t rpotu(uint32_t v, int bits) {
   return bits <= 0 ? v : (v + (1u << (bits - 1))) >> bits;
 }
 
-// One restoration tile: processing column j of stripe s of `plane`.
-template <typename T>
-__device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, const int* aw, const int* ah,
-                        int enabled, int plane, int j, int s, LrSmem& sm) {
-  uint16_t* s_win = sm.win;
+// Wiener filter of the staged window (restoration/wiener.go:132-211): the
+// block's sample (0,0) sits at sm.win[3 * kWin + 3], w x h <= 64 x 64, with
+// the 3-sample halo around it.  hf/vf are the 7 horizontal / vertical taps.
+// out(y, x, v) receives every output sample; threads map to samples as
+// x = tid % PW, y = tid / PW + k * (256 / PW).  Every thread of the CTA calls
+// it; it leaves the window untouched and ends without a barrier.
+template <class Out>
+__device__ __forceinline__ void lr_wiener_window(LrSmem& sm, int w, int h, int bd, const int* hf, const int* vf, int PW,
+                                 Out&& out) {
+  const uint16_t* s_win = sm.win;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tid = threadIdx.x, tx = tid % PW, ty0 = tid / PW, rowStep = 256 / PW;
+  const int wh = h + 6;
+  const int maxv = (1 << bd) - 1;
+  // restoration/wiener.go:202-211 (wienerRounds), :132-196.
+  int round0 = 3, round1 = 11;
+  const int range = bd + 7 - round0 + 2;
+  if (range > 16) {
+    round0 += range - 16;
+    round1 -= range - 16;
+  }
+  const int32_t limit = 1 << (bd + 1 + 7 - round0);
+  const int32_t offH = 1 << (bd + 7 - 1);
+  uint16_t* temp = reinterpret_cast<uint16_t*>(sm.flt0);  // (h+6) x 64
+  for (int r = warp; r < wh; r += 8) {
+    for (int c = lane; c < w; c += 32) {
+      const uint16_t* sw = &s_win[r * kWin + c];
+      int32_t sum = ((int32_t)sw[3] << 7) + offH;
+#pragma unroll
+      for (int k = 0; k < 7; k++) sum += (int32_t)sw[k] * hf[k];
+      temp[r * 64 + c] = (uint16_t)imin(imax(rpot(sum, round0), 0), limit - 1);
+    }
+  }
+  __syncthreads();
+  const int32_t offV = 1 << (bd + round1 - 1);
+  if (tx < w)
+    for (int y = ty0; y < h; y += rowStep) {
+      int32_t c3 = temp[(y + 3) * 64 + tx];
+      int32_t sum = (c3 << 7) - offV;
+#pragma unroll
+      for (int k = 0; k < 7; k++) sum += (int32_t)temp[(y + k) * 64 + tx] * vf[k];
+      out(y, tx, imin(imax(rpot(sum, round1), 0), maxv));
+    }
+}
+
+// Self-guided filter of the staged window (restoration/selfguided.go:111-390)
+// with parameter set `set` and the coded xqd pair; same window, thread
+// mapping and out() contract as lr_wiener_window.  sm.x_by_xplus1 must hold
+// the table.  Ends with a barrier.
+template <class Out>
+__device__ __forceinline__ void lr_sgr_window(LrSmem& sm, int w, int h, int bd, int set, int xqd0, int xqd1, int PW, Out&& out) {
+  const uint16_t* s_win = sm.win;
   uint16_t* s_A = sm.A;
   int32_t* s_B = sm.B;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ssx = plane ? src.ssx : 0, ssy = plane ? src.ssy : 0;
-  const int PW = 64 >> ssx, SH = 64 >> ssy, off = 8 >> ssy;
-  const int Wa = aw[plane], Ha = ah[plane];
-  const DPlane& sp = src.pl[plane];
-  const DPlane& dp = dst.pl[plane];
-  const int Wc = sp.w, Hc = sp.h;
-  const int x0 = j * PW;
-  const int y0 = imax(0, s * SH - off);
-  if (x0 >= Wa || y0 >= Ha) return;
-  const int x1 = imin(x0 + PW, Wa), y1 = imin((s + 1) * SH - off, Ha);
-  const int tid = threadIdx.x;
-  const int tx = tid % PW, ty0 = tid / PW, rowStep = 256 / PW;
-  const int bd = src.bd;
-
-  // Which restoration unit (if any) covers this tile.
-  const pf_lr_unit* u = nullptr;
-  const int xf1 = imin(x1, Wc), yf1 = imin(y1, Hc);
-  if (enabled && a.type[plane] != PF_LR_NONE && x0 < Wc && y0 < Hc) {
-    const int us = a.unit_size[plane];
-    const int ur = imin((y0 + off) / us, a.vert[plane] - 1);
-    const int uc = imin(x0 / us, a.horz[plane] - 1);
-    const pf_lr_unit* cand = &a.units[plane][ur * a.horz[plane] + uc];
-    if (cand->type == PF_LR_WIENER || cand->type == PF_LR_SGRPROJ) u = cand;
-  }
-  if (!u) {
-    if (tx < x1 - x0)
-      for (int y = y0 + ty0; y < y1; y += rowStep) row_ptr<T>(dp, y)[x0 + tx] = row_ptr<T>(sp, y)[x0 + tx];
-    return;
-  }
-  const int h = yf1 - y0, w = xf1 - x0;
-  // ---- stage the (h+6) x (w+6) source window ----
-  const int nominal = SH - (y0 == 0 ? off : 0);
-  const bool copyAbove = y0 != 0, copyBelow = y0 + nominal < Hc;
-  const int kAbove = s, kBelow = s + 1;  // boundary indices of the saved lines
-  const int ww = w + 6, wh = h + 6;
-  for (int r = warp; r < wh; r += 8) {
-    const int yy = y0 - 3 + r;
-    const T* srow;
-    if (yy < y0 && copyAbove) {
-      srow = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kAbove * 4 + imax(yy - y0 + 2, 0)) * a.line_stride[plane]);
-    } else if (yy >= yf1 && copyBelow) {
-      srow = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kBelow * 4 + 2 + imin(yy - yf1, 1)) * a.line_stride[plane]);
-    } else {
-      srow = row_ptr<T>(sp, iclip(yy, 0, Hc - 1));
-    }
-    for (int c = lane; c < ww; c += 32) s_win[r * kWin + c] = (uint16_t)srow[iclip(x0 - 3 + c, 0, Wc - 1)];
-  }
-  for (int i = tid; i < 256; i += 256) sm.x_by_xplus1[i] = c_x_by_xplus1[i];
-  __syncthreads();
-
-  // Pixels of the tile outside the cropped plane are copied through.
-  if (tx < x1 - x0)
-    for (int y = y0 + ty0; y < y1; y += rowStep)
-      if (x0 + tx >= Wc || y >= Hc) row_ptr<T>(dp, y)[x0 + tx] = row_ptr<T>(sp, y)[x0 + tx];
-
+  const int tid = threadIdx.x, tx = tid % PW, ty0 = tid / PW, rowStep = 256 / PW;
+  const int ww = w + 6;
   const int maxv = (1 << bd) - 1;
-  if (u->type == PF_LR_WIENER) {
-    // restoration/wiener.go:202-211 (wienerRounds), :132-196.
-    int round0 = 3, round1 = 11;
-    const int range = bd + 7 - round0 + 2;
-    if (range > 16) {
-      round0 += range - 16;
-      round1 -= range - 16;
-    }
-    const int hv0 = u->wiener_h[0], hv1 = u->wiener_h[1], hv2 = u->wiener_h[2];
-    const int hf[7] = {hv0, hv1, hv2, -2 * (hv0 + hv1 + hv2), hv2, hv1, hv0};
-    const int vv0 = u->wiener_v[0], vv1 = u->wiener_v[1], vv2 = u->wiener_v[2];
-    const int vf[7] = {vv0, vv1, vv2, -2 * (vv0 + vv1 + vv2), vv2, vv1, vv0};
-    const int32_t limit = 1 << (bd + 1 + 7 - round0);
-    const int32_t offH = 1 << (bd + 7 - 1);
-    uint16_t* temp = reinterpret_cast<uint16_t*>(sm.flt0);  // (h+6) x 64
-    for (int r = warp; r < wh; r += 8) {
-      for (int c = lane; c < w; c += 32) {
-        const uint16_t* sw = &s_win[r * kWin + c];
-        int32_t sum = ((int32_t)sw[3] << 7) + offH;
-#pragma unroll
-        for (int k = 0; k < 7; k++) sum += (int32_t)sw[k] * hf[k];
-        temp[r * 64 + c] = (uint16_t)imin(imax(rpot(sum, round0), 0), limit - 1);
-      }
-    }
-    __syncthreads();
-    const int32_t offV = 1 << (bd + round1 - 1);
-    if (tx < w)
-      for (int y = ty0; y < h; y += rowStep) {
-        int32_t c3 = temp[(y + 3) * 64 + tx];
-        int32_t sum = (c3 << 7) - offV;
-#pragma unroll
-        for (int k = 0; k < 7; k++) sum += (int32_t)temp[(y + k) * 64 + tx] * vf[k];
-        row_ptr<T>(dp, y0 + y)[x0 + tx] = (T)imin(imax(rpot(sum, round1), 0), maxv);
-      }
-    return;
-  }
-
-  // ---- SGRproj (restoration/selfguided.go:132-359) ----
-  const int set = u->sgr_set;
   const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][1];
   // restoration/selfguided.go:111-127 (DecodeSGRXQ).
   int xq0, xq1;
   if (r0 == 0) {
     xq0 = 0;
-    xq1 = 128 - u->sgr_xqd[1];
+    xq1 = 128 - xqd1;
   } else if (r1 == 0) {
-    xq0 = u->sgr_xqd[0];
+    xq0 = xqd0;
     xq1 = 0;
   } else {
-    xq0 = u->sgr_xqd[0];
-    xq1 = 128 - xq0 - u->sgr_xqd[1];
+    xq0 = xqd0;
+    xq1 = 128 - xq0 - xqd1;
   }
   int32_t* flt0 = sm.flt0;  // [y * 64 + x]
   if (r0 == 0)
@@ -247,7 +202,7 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
           const int32_t uu = dg << 4;
           const int32_t v = (uu << 7) + xq0 * (flt0[y * 64 + tx] - uu) + xq1 * (f1 - uu);
           const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
-          row_ptr<T>(dp, y0 + y)[x0 + tx] = (T)imin(imax(wv, 0), maxv);
+          out(y, tx, imin(imax(wv, 0), maxv));
         }
       }
     }
@@ -259,9 +214,83 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
       const int32_t uu = (int32_t)s_win[(y + 3) * kWin + tx + 3] << 4;
       const int32_t v = (uu << 7) + xq0 * (flt0[y * 64 + tx] - uu);
       const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
-      row_ptr<T>(dp, y0 + y)[x0 + tx] = (T)imin(imax(wv, 0), maxv);
+      out(y, tx, imin(imax(wv, 0), maxv));
     }
   }
+}
+
+// One restoration tile: processing column j of stripe s of `plane`.
+template <typename T>
+__device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, const int* aw, const int* ah,
+                        int enabled, int plane, int j, int s, LrSmem& sm) {
+  uint16_t* s_win = sm.win;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ssx = plane ? src.ssx : 0, ssy = plane ? src.ssy : 0;
+  const int PW = 64 >> ssx, SH = 64 >> ssy, off = 8 >> ssy;
+  const int Wa = aw[plane], Ha = ah[plane];
+  const DPlane& sp = src.pl[plane];
+  const DPlane& dp = dst.pl[plane];
+  const int Wc = sp.w, Hc = sp.h;
+  const int x0 = j * PW;
+  const int y0 = imax(0, s * SH - off);
+  if (x0 >= Wa || y0 >= Ha) return;
+  const int x1 = imin(x0 + PW, Wa), y1 = imin((s + 1) * SH - off, Ha);
+  const int tid = threadIdx.x;
+  const int tx = tid % PW, ty0 = tid / PW, rowStep = 256 / PW;
+  const int bd = src.bd;
+
+  // Which restoration unit (if any) covers this tile.
+  const pf_lr_unit* u = nullptr;
+  const int xf1 = imin(x1, Wc), yf1 = imin(y1, Hc);
+  if (enabled && a.type[plane] != PF_LR_NONE && x0 < Wc && y0 < Hc) {
+    const int us = a.unit_size[plane];
+    const int ur = imin((y0 + off) / us, a.vert[plane] - 1);
+    const int uc = imin(x0 / us, a.horz[plane] - 1);
+    const pf_lr_unit* cand = &a.units[plane][ur * a.horz[plane] + uc];
+    if (cand->type == PF_LR_WIENER || cand->type == PF_LR_SGRPROJ) u = cand;
+  }
+  if (!u) {
+    if (tx < x1 - x0)
+      for (int y = y0 + ty0; y < y1; y += rowStep) row_ptr<T>(dp, y)[x0 + tx] = row_ptr<T>(sp, y)[x0 + tx];
+    return;
+  }
+  const int h = yf1 - y0, w = xf1 - x0;
+  // ---- stage the (h+6) x (w+6) source window ----
+  const int nominal = SH - (y0 == 0 ? off : 0);
+  const bool copyAbove = y0 != 0, copyBelow = y0 + nominal < Hc;
+  const int kAbove = s, kBelow = s + 1;  // boundary indices of the saved lines
+  const int ww = w + 6, wh = h + 6;
+  for (int r = warp; r < wh; r += 8) {
+    const int yy = y0 - 3 + r;
+    const T* srow;
+    if (yy < y0 && copyAbove) {
+      srow = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kAbove * 4 + imax(yy - y0 + 2, 0)) * a.line_stride[plane]);
+    } else if (yy >= yf1 && copyBelow) {
+      srow = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kBelow * 4 + 2 + imin(yy - yf1, 1)) * a.line_stride[plane]);
+    } else {
+      srow = row_ptr<T>(sp, iclip(yy, 0, Hc - 1));
+    }
+    for (int c = lane; c < ww; c += 32) s_win[r * kWin + c] = (uint16_t)srow[iclip(x0 - 3 + c, 0, Wc - 1)];
+  }
+  for (int i = tid; i < 256; i += 256) sm.x_by_xplus1[i] = c_x_by_xplus1[i];
+  __syncthreads();
+
+  // Pixels of the tile outside the cropped plane are copied through.
+  if (tx < x1 - x0)
+    for (int y = y0 + ty0; y < y1; y += rowStep)
+      if (x0 + tx >= Wc || y >= Hc) row_ptr<T>(dp, y)[x0 + tx] = row_ptr<T>(sp, y)[x0 + tx];
+
+  auto store = [&](int y, int x, int v) { row_ptr<T>(dp, y0 + y)[x0 + x] = (T)v; };
+  if (u->type == PF_LR_WIENER) {
+    const int hv0 = u->wiener_h[0], hv1 = u->wiener_h[1], hv2 = u->wiener_h[2];
+    const int hf[7] = {hv0, hv1, hv2, -2 * (hv0 + hv1 + hv2), hv2, hv1, hv0};
+    const int vv0 = u->wiener_v[0], vv1 = u->wiener_v[1], vv2 = u->wiener_v[2];
+    const int vf[7] = {vv0, vv1, vv2, -2 * (vv0 + vv1 + vv2), vv2, vv1, vv0};
+    lr_wiener_window(sm, w, h, bd, hf, vf, PW, store);
+    return;
+  }
+  // ---- SGRproj (restoration/selfguided.go:132-359) ----
+  lr_sgr_window(sm, w, h, bd, u->sgr_set, u->sgr_xqd[0], u->sgr_xqd[1], PW, store);
 }
 
 cudaError_t lr_upload_tables() {
@@ -307,4 +336,399 @@ cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_
   return cudaGetLastError();
 }
 
+// ---- encoder loop-restoration unit search ----
+// encoder/restoration.go:149-210 (SearchWienerUnitU8), :216-263
+// (SearchSGRProjUnitU8) and the unit loops of EncodeLoopRestorationKeyframe
+// (encoder/keyframe_lossy.go:2313-2383, :2422-2453), luma of 8-bit frames.
+//
+// Two launches.  k_lr_search_sse: one CTA per (unit, job); job 0 measures
+// the unfiltered SSE, the six horizontal-only Wiener candidates and the
+// exact Wiener filter of the pick, jobs 1..4 one exact SGR preset each, into
+// a table of 32-bit SSEs (a unit holds at most 95 x 95 samples, so every sum
+// stays below 2^32).  k_lr_search_decide: one CTA per unit replays the
+// reference's decisions over the table, writes the unit record and, when
+// asked, filters the unit with the winner into the output plane.
+
+// The candidate tap sets and presets of encoder/restoration.go:166-173 and
+// :235-240, in the reference's order (first strictly better wins).
+__constant__ int8_t c_lrs_wiener[PF_LR_WIENER_CANDIDATES][3] = {
+    {0, -3, 12}, {0, -5, 18}, {0, -2, 8}, {0, 2, 10}, {1, 4, 14}, {0, -1, 4}};
+__constant__ int8_t c_lrs_sgr[PF_LR_SGR_PRESETS][3] = {{0, 8, 24}, {2, 16, 40}, {10, 0, 48}, {14, 24, 72}};
+
+constexpr uint32_t kLrsNone = 0xffffffffu;
+
+struct LrsSse {
+  uint32_t base;
+  uint32_t wiener[PF_LR_WIENER_CANDIDATES];  // horizontal approximation
+  uint32_t wexact;                           // exact Wiener of the pick
+  uint32_t sgr[PF_LR_SGR_PRESETS];
+  int32_t wpick;
+};
+
+struct LrsArgs {
+  const uint8_t* src;
+  int64_t sstride;
+  const uint8_t* rec;
+  int64_t rstride;
+  uint8_t* dst;  // null: search only
+  int64_t dstride;
+  int W, H, horz, vert;
+  LrsSse* table;
+  pf_lr_search_unit* out;
+};
+
+struct LrsSmem {
+  LrSmem lr;
+  uint8_t src[64 * 64];
+  uint32_t red[8 * 8];
+};
+
+// tile/restoration_geometry.go:54-92 for luma units of 64.
+__device__ __forceinline__ void lrs_rect(const LrsArgs& a, int col, int row, int& x0, int& y0, int& x1, int& y1) {
+  x0 = col * 64;
+  x1 = col + 1 == a.horz ? a.W : x0 + 64;
+  y0 = row * 64;
+  y1 = row + 1 == a.vert ? a.H : y0 + 64;
+  if (y0 > 0) y0 -= 8;
+  if (y1 < a.H) y1 -= 8;
+}
+
+// Sums N per-thread values over the CTA; every thread gets the totals.
+template <int N>
+__device__ __forceinline__ void lrs_block_sum(uint32_t (&v)[N], uint32_t* red) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    uint32_t x = v[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) red[warp * N + i] = x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    uint32_t x = 0;
+    for (int k = 0; k < 8; k++) x += red[k * N + i];
+    v[i] = x;
+  }
+  __syncthreads();
+}
+
+// The unit's recon window with a 3-sample edge-clamped border (the bordered
+// copy of keyframe_lossy.go:2313-2330) into sm.lr.win; the SGR table when
+// `tables`; the unit's source samples into sm.src when `source`.
+__device__ __forceinline__ void lrs_stage(const LrsArgs& a, LrsSmem& sm, int x0, int y0, int w, int h, bool tables,
+                                          bool source) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = warp; r < h + 6; r += 8) {
+    const uint8_t* row = a.rec + (int64_t)iclip(y0 - 3 + r, 0, a.H - 1) * a.rstride;
+    for (int c = lane; c < w + 6; c += 32) sm.lr.win[r * kWin + c] = row[iclip(x0 - 3 + c, 0, a.W - 1)];
+  }
+  if (source)
+    for (int r = warp; r < h; r += 8) {
+      const uint8_t* row = a.src + (int64_t)(y0 + r) * a.sstride + x0;
+      for (int c = lane; c < w; c += 32) sm.src[r * 64 + c] = row[c];
+    }
+  if (tables) sm.lr.x_by_xplus1[threadIdx.x] = c_x_by_xplus1[threadIdx.x];
+  __syncthreads();
+}
+
+// The same sets as compile-time values, for the unrolled candidate loop.
+__host__ __device__ constexpr int lrs_tap(int c, int k) {
+  constexpr int8_t t[PF_LR_WIENER_CANDIDATES][3] = {{0, -3, 12}, {0, -5, 18}, {0, -2, 8},
+                                                    {0, 2, 10},  {1, 4, 14},  {0, -1, 4}};
+  return t[c][k];
+}
+
+// One candidate's horizontal-only prediction (encoder/restoration.go:181-198)
+// from the symmetric pair sums p06, p15, p24 and the centre p3.
+template <int C>
+__device__ __forceinline__ int lrs_hpred(int p06, int p15, int p24, int p3) {
+  constexpr int t0 = lrs_tap(C, 0), t1 = lrs_tap(C, 1), t2 = lrs_tap(C, 2), t3 = -2 * (t0 + t1 + t2);
+  const int hs = t0 * p06 + t1 * p15 + t2 * p24 + t3 * p3;
+  return iclip((hs + 64) >> 7, 0, 255);
+}
+
+template <int C>
+__device__ __forceinline__ void lrs_hsse(uint32_t* acc, int s, int p06, int p15, int p24, int p3) {
+  const int d = s - lrs_hpred<C>(p06, p15, p24, p3);
+  acc[1 + C] += (uint32_t)(d * d);
+  if constexpr (C + 1 < PF_LR_WIENER_CANDIDATES) lrs_hsse<C + 1>(acc, s, p06, p15, p24, p3);
+}
+
+__device__ __forceinline__ void lrs_taps(int c, int* f) {
+  const int t0 = c_lrs_wiener[c][0], t1 = c_lrs_wiener[c][1], t2 = c_lrs_wiener[c][2];
+  f[0] = f[6] = t0;
+  f[1] = f[5] = t1;
+  f[2] = f[4] = t2;
+  f[3] = -2 * (t0 + t1 + t2);  // restoration/wiener.go:44-47 (NewWienerFilter)
+}
+
+// SearchWienerUnitU8's choice over the table (encoder/restoration.go:161-209).
+__device__ __forceinline__ int lrs_wiener_pick(const uint32_t* cand, uint32_t base, int area) {
+  int pick = -1;
+  uint64_t best = base;
+  if (base != 0)
+    for (int c = 0; c < PF_LR_WIENER_CANDIDATES; c++)
+      if ((uint64_t)cand[c] + (uint64_t)area < best) {
+        best = cand[c];
+        pick = c;
+      }
+  return pick;
+}
+
+__global__ void __launch_bounds__(256, 2) k_lr_search_sse(LrsArgs a) {
+  extern __shared__ __align__(16) uint8_t lrs_smem_raw[];
+  LrsSmem& sm = *reinterpret_cast<LrsSmem*>(lrs_smem_raw);
+  const int unit = blockIdx.x, job = blockIdx.y;
+  int x0, y0, x1, y1;
+  lrs_rect(a, unit % a.horz, unit / a.horz, x0, y0, x1, y1);
+  const int w = x1 - x0, h = y1 - y0;
+  const bool fits = w <= 64 && h <= 64;  // restoration/wiener.go:198-200
+  LrsSse& T = a.table[unit];
+  const int tid = threadIdx.x;
+  if (job > 0) {
+    // SearchSGRProjUnitU8, one preset (encoder/restoration.go:242-261).
+    const int p = job - 1;
+    if (!fits) {
+      if (tid == 0) T.sgr[p] = kLrsNone;
+      return;
+    }
+    lrs_stage(a, sm, x0, y0, w, h, true, true);
+    uint32_t acc[1] = {0};
+    lr_sgr_window(sm.lr, w, h, 8, c_lrs_sgr[p][0], c_lrs_sgr[p][1], c_lrs_sgr[p][2], 64, [&](int y, int x, int v) {
+      const int d = (int)sm.src[y * 64 + x] - v;
+      acc[0] += (uint32_t)(d * d);
+    });
+    lrs_block_sum(acc, sm.red);
+    if (tid == 0) T.sgr[p] = acc[0];
+    return;
+  }
+  // Job 0: SearchWienerUnitU8 (encoder/restoration.go:149-210).
+  uint32_t acc[1 + PF_LR_WIENER_CANDIDATES];
+#pragma unroll
+  for (int i = 0; i <= PF_LR_WIENER_CANDIDATES; i++) acc[i] = 0;
+  if (fits) {
+    lrs_stage(a, sm, x0, y0, w, h, false, true);
+    const int tx = tid & 63;
+    if (tx < w)
+      for (int y = tid >> 6; y < h; y += 4) {
+        const uint16_t* wr = &sm.lr.win[(y + 3) * kWin + tx];
+        const int s = sm.src[y * 64 + tx];
+        const int d0 = s - (int)wr[3];
+        acc[0] += (uint32_t)(d0 * d0);
+        lrs_hsse<0>(acc, s, wr[0] + wr[6], wr[1] + wr[5], wr[2] + wr[4], wr[3]);
+      }
+  } else {
+    // Units larger than 64x64 (the last row or column of some frame sizes):
+    // the search still runs on them, straight from the frame.
+    for (int i = tid; i < w * h; i += 256) {
+      const int y = y0 + i / w, x = x0 + i % w;
+      const uint8_t* rr = a.rec + (int64_t)y * a.rstride;
+      const int s = a.src[(int64_t)y * a.sstride + x];
+      const int d0 = s - (int)rr[x];
+      acc[0] += (uint32_t)(d0 * d0);
+      int px[7];
+#pragma unroll
+      for (int k = 0; k < 7; k++) px[k] = rr[iclip(x + k - 3, 0, a.W - 1)];
+      lrs_hsse<0>(acc, s, px[0] + px[6], px[1] + px[5], px[2] + px[4], px[3]);
+    }
+  }
+  lrs_block_sum(acc, sm.red);
+  const int pick = lrs_wiener_pick(acc + 1, acc[0], w * h);
+  uint32_t ex[1] = {kLrsNone};
+  if (pick >= 0 && fits) {
+    // The exact filter of the pick (keyframe_lossy.go:2344-2366).
+    int fv[7];
+    lrs_taps(pick, fv);
+    ex[0] = 0;
+    lr_wiener_window(sm.lr, w, h, 8, fv, fv, 64, [&](int y, int x, int v) {
+      const int d = (int)sm.src[y * 64 + x] - v;
+      ex[0] += (uint32_t)(d * d);
+    });
+    lrs_block_sum(ex, sm.red);
+  }
+  if (tid == 0) {
+    T.base = acc[0];
+    for (int c = 0; c < PF_LR_WIENER_CANDIDATES; c++) T.wiener[c] = acc[1 + c];
+    T.wexact = ex[0];
+    T.wpick = pick;
+  }
+}
+
+// The unit's decision (keyframe_lossy.go:2338-2382) and, with a.dst, the
+// unit filtered by it (:2422-2453).
+__global__ void __launch_bounds__(256) k_lr_search_decide(LrsArgs a) {
+  extern __shared__ __align__(16) uint8_t lrs_smem_raw[];
+  LrsSmem& sm = *reinterpret_cast<LrsSmem*>(lrs_smem_raw);
+  const int unit = blockIdx.x, tid = threadIdx.x;
+  int x0, y0, x1, y1;
+  lrs_rect(a, unit % a.horz, unit / a.horz, x0, y0, x1, y1);
+  const int w = x1 - x0, h = y1 - y0;
+  const bool fits = w <= 64 && h <= 64;
+  const LrsSse& T = a.table[unit];
+  const uint64_t base = T.base;
+  const int wpick = T.wpick;
+  uint64_t best = ~0ull;
+  int type = PF_LR_NONE;
+  if (wpick >= 0 && fits) {
+    best = T.wexact;
+    type = PF_LR_WIENER;
+  }
+  int spick = -1;
+  uint64_t sbest = fits ? base : ~0ull;
+  if (fits && base != 0)
+    for (int p = 0; p < PF_LR_SGR_PRESETS; p++)
+      if ((uint64_t)T.sgr[p] + (uint64_t)(w * h) < sbest) {
+        sbest = T.sgr[p];
+        spick = p;
+      }
+  if (spick >= 0 && sbest < best) {
+    best = sbest;
+    type = PF_LR_SGRPROJ;
+  }
+  if (tid == 0) {
+    pf_lr_search_unit r;
+    memset(&r, 0, sizeof(r));
+    r.x0 = x0;
+    r.y0 = y0;
+    r.x1 = x1;
+    r.y1 = y1;
+    r.base_sse = base;
+    r.sse = type == PF_LR_NONE ? base : best;
+    r.wiener_sse = wpick >= 0 && fits ? (uint64_t)T.wexact : ~0ull;
+    r.sgr_sse = sbest;
+    r.wiener_candidate = (int8_t)wpick;
+    r.sgr_preset = (int8_t)spick;
+    r.unit.type = (uint8_t)type;
+    if (type == PF_LR_WIENER)
+      for (int k = 0; k < 3; k++) r.unit.wiener_v[k] = r.unit.wiener_h[k] = c_lrs_wiener[wpick][k];
+    if (type == PF_LR_SGRPROJ) {
+      r.unit.sgr_set = (uint8_t)c_lrs_sgr[spick][0];
+      r.unit.sgr_xqd[0] = c_lrs_sgr[spick][1];
+      r.unit.sgr_xqd[1] = c_lrs_sgr[spick][2];
+    }
+    a.out[unit] = r;
+  }
+  if (!a.dst) return;
+  if (type == PF_LR_NONE) {
+    for (int i = tid; i < w * h; i += 256) {
+      const int y = y0 + i / w, x = x0 + i % w;
+      a.dst[(int64_t)y * a.dstride + x] = a.rec[(int64_t)y * a.rstride + x];
+    }
+    return;
+  }
+  lrs_stage(a, sm, x0, y0, w, h, type == PF_LR_SGRPROJ, false);
+  auto store = [&](int y, int x, int v) { a.dst[(int64_t)(y0 + y) * a.dstride + x0 + x] = (uint8_t)v; };
+  if (type == PF_LR_WIENER) {
+    int fv[7];
+    lrs_taps(wpick, fv);
+    lr_wiener_window(sm.lr, w, h, 8, fv, fv, 64, store);
+  } else {
+    lr_sgr_window(sm.lr, w, h, 8, c_lrs_sgr[spick][0], c_lrs_sgr[spick][1], c_lrs_sgr[spick][2], 64, store);
+  }
+}
+
+static int lrs_check(const pf_frame* f, const pf_frame* ref) {
+  // goav1's keyframe encoder works on 8-bit 4:2:0 pictures (SourceFrame420).
+  if (f->bit_depth != 8 || f->ss_x != 1 || f->ss_y != 1 || f->mono || f->width != ref->width ||
+      f->height != ref->height)
+    return PF_ERR_UNSUPPORTED;
+  if (f->memory != ref->memory || f->memory > PF_MEM_DEVICE) return PF_ERR_INVALID_ARG;
+  const pf_plane& pl = f->plane[0];
+  if (!pl.data || pl.width != ref->width || pl.height != ref->height || pl.stride < pl.width)
+    return PF_ERR_SHORT_BUFFER;
+  return PF_OK;
+}
+
 }  // namespace pf
+
+void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
+void* pf_internal_stream(pf_ctx* c);
+void* pf_internal_pinned(pf_ctx* c, size_t bytes);
+
+extern "C" int pf_lr_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const pf_frame* restored,
+                            pf_lr_search_unit* units, int32_t max_units) {
+  using namespace pf;
+  if (!ctx || !source || !recon) return PF_ERR_INVALID_ARG;
+  if (recon->width <= 0 || recon->height <= 0) return PF_ERR_INVALID_ARG;
+  int stt = lrs_check(recon, recon);
+  if (stt == PF_OK) stt = lrs_check(source, recon);
+  if (stt == PF_OK && restored) stt = lrs_check(restored, recon);
+  if (stt != PF_OK) return stt;
+  const int W = recon->width, H = recon->height;
+  const int horz = imax((W + 32) / 64, 1), vert = imax((H + 32) / 64, 1), n = horz * vert;
+  if (units && max_units < n) return PF_ERR_SHORT_BUFFER;
+  const cudaStream_t st = (cudaStream_t)pf_internal_stream(ctx);
+  const bool host = recon->memory == PF_MEM_HOST;
+  const pf_plane &sp = source->plane[0], &rp = recon->plane[0];
+  // In place (restored's luma is recon's): the unit filters read a copy.
+  const bool alias = restored && restored->plane[0].data == rp.data;
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t plane = al((size_t)W * H);
+  size_t off = 0;
+  const size_t oTab = off;
+  off += al(sizeof(LrsSse) * n);
+  const size_t oOut = off;
+  off += al(sizeof(pf_lr_search_unit) * n);
+  const size_t oSrc = off;
+  off += host ? plane : 0;
+  const size_t oRec = off;
+  off += host || alias ? plane : 0;
+  const size_t oDst = off;
+  off += host && restored ? plane : 0;
+  uint8_t* base = (uint8_t*)pf_internal_search_scratch(ctx, off);
+  if (!base) return PF_ERR_DEVICE;
+  LrsArgs a;
+  a.W = W;
+  a.H = H;
+  a.horz = horz;
+  a.vert = vert;
+  a.table = (LrsSse*)(base + oTab);
+  a.out = (pf_lr_search_unit*)(base + oOut);
+  cudaError_t e = cudaSuccess;
+  const cudaMemcpyKind up = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  if (host) {
+    a.src = base + oSrc;
+    a.sstride = W;
+    e = cudaMemcpy2DAsync(base + oSrc, W, sp.data, sp.stride, W, H, up, st);
+  } else {
+    a.src = (const uint8_t*)sp.data;
+    a.sstride = sp.stride;
+  }
+  if (host || alias) {
+    a.rec = base + oRec;
+    a.rstride = W;
+    if (e == cudaSuccess) e = cudaMemcpy2DAsync(base + oRec, W, rp.data, rp.stride, W, H, up, st);
+  } else {
+    a.rec = (const uint8_t*)rp.data;
+    a.rstride = rp.stride;
+  }
+  a.dst = nullptr;
+  a.dstride = 0;
+  if (restored) {
+    a.dst = host ? base + oDst : (uint8_t*)restored->plane[0].data;
+    a.dstride = host ? W : restored->plane[0].stride;
+  }
+  if (e != cudaSuccess) return PF_ERR_DEVICE;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(k_lr_search_sse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LrsSmem)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_lr_search_decide, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(LrsSmem)) != cudaSuccess)
+      return PF_ERR_DEVICE;
+    configured = true;
+  }
+  k_lr_search_sse<<<dim3(n, 1 + PF_LR_SGR_PRESETS), 256, sizeof(LrsSmem), st>>>(a);
+  k_lr_search_decide<<<n, 256, sizeof(LrsSmem), st>>>(a);
+  e = cudaGetLastError();
+  if (e == cudaSuccess && host && restored)
+    e = cudaMemcpy2DAsync(restored->plane[0].data, restored->plane[0].stride, a.dst, W, W, H,
+                          cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && units)
+    e = cudaMemcpyAsync(units, a.out, sizeof(pf_lr_search_unit) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? PF_OK : PF_ERR_DEVICE;
+}
+

@@ -158,6 +158,21 @@ class PostFilterRunner:
                                    mse.ctypes.data if want_mse else None, idx.ctypes.data, C.byref(res)))
         return res, mse, idx
 
+    def lr_search(self, source, recon, restored=None):
+        """Encoder loop-restoration unit search on the luma of 8-bit 4:2:0
+        frames: SearchWienerUnitU8 and SearchSGRProjUnitU8 per 64x64 unit
+        (internal/av1/encoder/restoration.go:149-263) with the Wiener / SGRProj
+        / none decision of EncodeLoopRestorationKeyframe
+        (encoder/keyframe_lossy.go:2332-2383); with `restored`, its luma gets
+        the decided filters applied (:2422-2453).  source, recon and restored
+        are pf_frame views (all host or all device; restored may be recon).
+        Returns the pf_lr_search_unit records in raster order."""
+        horz, vert = abi.lr_unit_grid(recon.width, recon.height)
+        units = (abi.pf_lr_search_unit * (horz * vert))()
+        check(lib().pf_lr_search(self._h, C.byref(source), C.byref(recon),
+                                 C.byref(restored) if restored is not None else None, units, horz * vert))
+        return units
+
     def cdef_features(self, recon, noskip, qindex, damping=0):
         """Per-filter-block features (float32[nfb, 40]) of an 8-bit 4:2:0
         deblocked reconstruction, as the learned search computes them."""

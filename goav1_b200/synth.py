@@ -506,3 +506,36 @@ def make_search_pair(seed, width=1920, height=1080, sigma=None):
     gen_content(rng, rec, sig, 12, params=params)
     _, side = make_frame(1, seed, width=width, height=height, stages=abi.PF_STAGE_LOOP_FILTER)
     return src, rec, side, sig
+
+
+def make_lr_search_pair(seed, width=1920, height=1080, sigma=None):
+    """Loop-restoration search workload (8-bit 4:2:0, luma searched): the
+    source is the cosine-gradient texture; the reconstruction adds per-8x8
+    DC offsets in +/-6 and Gaussian noise (sigma from {2, 4, 8}).  About one
+    luma restoration unit in eight is made dark in the source (0..3) with
+    the reconstruction 16..40 above it, the content on which the reference's
+    horizontal-only Wiener scoring (taps without the centre's 128) can win,
+    and about one in sixteen is reconstructed exactly (zero unfiltered SSE).
+    Returns (source, recon, sigma)."""
+    rng = np.random.default_rng([seed, 0x1E57A9])
+    src = HostFrame.alloc(width, height, 8)
+    params = gen_content(rng, src, 0.0, 0)
+    rec = HostFrame.alloc(width, height, 8)
+    sig = float(sigma if sigma is not None else rng.choice([2.0, 4.0, 8.0]))
+    gen_content(rng, rec, sig, 6, params=params)
+    horz, vert = abi.lr_unit_grid(width, height)
+    for row in range(vert):
+        for col in range(horz):
+            x0, x1 = col * 64, (width if col + 1 == horz else col * 64 + 64)
+            y0, y1 = row * 64, (height if row + 1 == vert else row * 64 + 64)
+            y0 -= 8 if y0 > 0 else 0
+            y1 -= 8 if y1 < height else 0
+            s = src.planes[0][y0:y1, x0:x1]
+            r = rec.planes[0][y0:y1, x0:x1]
+            u = rng.random()
+            if u < 0.125:
+                s[:] = rng.integers(0, 4, size=s.shape)
+                r[:] = np.clip(s.astype(np.int32) + rng.integers(16, 41, size=s.shape), 0, 255)
+            elif u < 0.1875:
+                r[:] = s
+    return src, rec, sig

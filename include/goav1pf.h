@@ -15,6 +15,10 @@
  *                          (decoder_postfilter_bind.go:252-256, :434-439).
  *   - pf_cdef_search      internal/av1/encoder/cdef_search.go:580-634
  *                          (cdefSearcher.search) + :886-945 (finish).
+ *   - pf_lr_search        internal/av1/encoder/restoration.go:149-263
+ *                          (SearchWienerUnitU8, SearchSGRProjUnitU8) and the
+ *                          unit loops of EncodeLoopRestorationKeyframe,
+ *                          encoder/keyframe_lossy.go:2313-2383, :2422-2453.
  *   - status codes        sentinel errors: cdef.ErrInvalidCDEF
  *                          (cdef/direction.go:11), loopfilter.ErrInvalidFilter,
  *                          tile.ErrInvalidPlan, decoder.ErrUnsupportedPostFilter,
@@ -462,6 +466,56 @@ int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const pf_frame* 
                            const pf_cdef_mlp* model, float threshold, int32_t candidates,
                            int32_t flags, uint64_t* mse_out, uint8_t* fb_index_out,
                            pf_cdef_search_result* result, pf_cdef_learned_stats* stats);
+
+/* ---- encoder loop-restoration unit search (encoder/restoration.go) ----
+ * Replaces the per-unit loop of EncodeLoopRestorationKeyframe
+ * (internal/av1/encoder/keyframe_lossy.go:2313-2383, the bordered copy and
+ * the search, and
+ * :2422-2453, the application): luma restoration units of 64 samples
+ * (tile.RestorationPlaneGrid, tile/restoration_geometry.go:54-92: the last
+ * unit of a row or column takes the remainder, interior unit edges move up
+ * by 8 rows), each searched with
+ *   - SearchWienerUnitU8 (encoder/restoration.go:149-210): SSE of the
+ *     unfiltered recon, then the 6 fixed symmetric tap sets of
+ *     PF_LR_WIENER_CANDIDATES, scored by a horizontal-only 7-tap pass with
+ *     (sum + 64) >> 7 and edge-clamped columns; a set is taken when its SSE
+ *     + w*h is below the best so far;
+ *   - the exact Wiener filter (restoration/wiener_u8.go:36-56, both
+ *     directions the picked taps) on the 3-sample edge-clamped frame, whose
+ *     SSE becomes the unit's best;
+ *   - SearchSGRProjUnitU8 (encoder/restoration.go:216-263): the exact
+ *     self-guided filter (restoration/selfguided_u8.go:36) for each preset
+ *     of PF_LR_SGR_PRESETS under the same acceptance rule; SGRProj replaces
+ *     Wiener when its SSE is strictly lower.
+ * Units wider or taller than 64 stay PF_LR_NONE (the reference's filters
+ * reject them).  Only 8-bit 4:2:0 frames are searched (SourceFrame420);
+ * only luma is read or written.
+ * source, recon and restored (may be NULL) are all host or all device
+ * frames of equal geometry; restored may be recon itself.  When restored is
+ * given, its luma plane receives the reconstruction with every unit's
+ * decision applied (unfiltered samples for PF_LR_NONE units); its chroma
+ * planes are not touched.  units (host, may be NULL) receives one record
+ * per unit in raster order; max_units must cover horz*vert units, where
+ * horz = max((width + 32) / 64, 1) and vert = max((height + 32) / 64, 1). */
+#define PF_LR_WIENER_CANDIDATES 6
+#define PF_LR_SGR_PRESETS 4
+typedef struct pf_lr_search_unit {
+  int32_t x0, y0, x1, y1;   /* unit rectangle on the luma plane */
+  uint64_t base_sse;        /* unfiltered recon against source */
+  uint64_t sse;             /* SSE of the unit as decided (base_sse for NONE) */
+  uint64_t wiener_sse;      /* exact Wiener SSE of the search's pick; UINT64_MAX
+                               when the Wiener search took no set or the unit
+                               is larger than 64x64 */
+  uint64_t sgr_sse;         /* SearchSGRProjUnitU8's best SSE (base_sse when
+                               no preset was taken; UINT64_MAX when the unit
+                               is larger than 64x64) */
+  int8_t wiener_candidate;  /* index of the picked Wiener set, -1 = none */
+  int8_t sgr_preset;        /* index of the picked SGR preset, -1 = none */
+  uint8_t reserved[2];
+  pf_lr_unit unit;          /* the decision, as the bitstream codes it */
+} pf_lr_search_unit;
+int pf_lr_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const pf_frame* restored,
+                 pf_lr_search_unit* units, int32_t max_units);
 
 #ifdef __cplusplus
 }

@@ -61,6 +61,7 @@ def lib():
         _lib.oracle_mlp_gradients.restype = None
         _lib.oracle_mlp_loss_grad_f64.argtypes = [C.c_void_p] * 5 + [C.c_int, C.c_void_p, C.c_void_p]
         _lib.oracle_mlp_loss_grad_f64.restype = None
+        _lib.oracle_lr_search.argtypes = [C.c_void_p] * 4 + [C.c_int]
     return _lib
 
 

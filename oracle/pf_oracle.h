@@ -88,6 +88,11 @@ void oracle_mlp_gradients(const pf_cdef_mlp* m, const float* X, const uint8_t* l
 void oracle_mlp_loss_grad_f64(const double* params, const double* shift, const double* scale, const float* X,
                               const uint8_t* labels, int n, double* loss, double* grads);
 
+/* Encoder loop-restoration unit search and application
+ * (oracle/lr_search_oracle.cpp); see pf_lr_search.  Host frames. */
+int oracle_lr_search(const pf_frame* source, const pf_frame* recon, const pf_frame* restored,
+                     pf_lr_search_unit* units, int max_units);
+
 #ifdef __cplusplus
 }
 #endif
