@@ -318,6 +318,20 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def call_median(fn, reps):
+    """Median wall time of `reps` calls of a synchronous library call (each
+    returns after its work and its host copies are done)."""
+    import torch
+
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts)
+
+
 def cpu_baseline_lr_search(pair, seconds=5.0):
     """The LR search oracle (C++ restatement of goav1's Go search) on one
     host thread, repeated on one 1080p frame for about `seconds`."""
@@ -477,8 +491,8 @@ def main():
     # without noise, reconstruction with 8x8 DC offsets and noise, deblocked
     # by the library, both frames resident in HBM.  Blocks/s = the frame's
     # 64x64 filter blocks (all of them, as the search visits them) per second
-    # of one search call, host round trip included (the call returns the
-    # decision).  The learned search's luma SSE increase is read from the
+    # of one search call (median over the calls), host round trip included
+    # (the call returns the decision).  The learned search's luma SSE increase is read from the
     # exhaustive search's table.  Rank 0 only.
     search = learned_leg = None
     if not args.no_search and rank == 0:
@@ -496,14 +510,10 @@ def main():
             r0, m0, i0 = runner.cdef_search(sp, rp, ns, q, _l.LAMBDA)
             r1, _, i1, st = runner.cdef_search_learned(sp, rp, ns, q, _l.LAMBDA, model)
 
-            def timed(fn, reps=max(3, args.steps // 4)):
+            def timed(fn, reps=max(5, args.steps // 2)):
                 fn()
                 torch.cuda.synchronize()
-                t0 = time.perf_counter()
-                for _ in range(reps):
-                    fn()
-                torch.cuda.synchronize()
-                return (time.perf_counter() - t0) / reps
+                return call_median(fn, reps)
 
             te = timed(lambda: runner.cdef_search(sp, rp, ns, q, _l.LAMBDA, want_mse=False))
             tl = timed(lambda: runner.cdef_search_learned(sp, rp, ns, q, _l.LAMBDA, model, want_mse=False,
@@ -534,9 +544,10 @@ def main():
     # Encoder loop-restoration search (pf_lr_search: every 64x64 luma unit
     # searched with the six Wiener tap sets and the four SGR presets, the
     # decision applied into an output frame) on 1080p 8-bit 4:2:0 frames
-    # (seeds 2000..), both frames resident in HBM.  Units/s per call, host
-    # round trip of the unit records included.  The oracle's time on one
-    # frame (one host thread) is reported beside it.  Rank 0 only.
+    # (seeds 2000..), both frames resident in HBM.  Units/s per call (median
+    # over the calls), host round trip of the unit records included.  The
+    # oracle's time on one frame (one host thread) is reported beside it.
+    # Rank 0 only.
     lr_leg = None
     if not args.no_search and rank == 0:
         from goav1_b200 import synth
@@ -551,13 +562,8 @@ def main():
             units_total += len(units)
             for u in units:
                 kinds[u.unit.type] += 1
-            reps = max(3, args.steps // 4)
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            for _ in range(reps):
-                runner.lr_search(sp, rp, op)
-            torch.cuda.synchronize()
-            times.append((time.perf_counter() - t0) / reps)
+            times.append(call_median(lambda: runner.lr_search(sp, rp, op), max(5, args.steps // 2)))
         per_frame = statistics.mean(times)
         lr_leg = {"metric": "LR search units/s", "value": units_total / sum(times), "unit": "units/s",
                   "ms_per_frame": per_frame * 1e3, "mpix_per_s": 1920 * 1080 / per_frame / 1e6,

@@ -321,4 +321,5 @@ EXPORTED_SYMBOLS = (
     "pf_set_persistent",
     "pf_autotune",
     "pf_lr_search",
+    "pf_cdef_apply",
 )

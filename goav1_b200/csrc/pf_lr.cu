@@ -345,9 +345,12 @@ cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_
 // the unfiltered SSE, the six horizontal-only Wiener candidates and the
 // exact Wiener filter of the pick, jobs 1..4 one exact SGR preset each, into
 // a table of 32-bit SSEs (a unit holds at most 95 x 95 samples, so every sum
-// stays below 2^32).  k_lr_search_decide: one CTA per unit replays the
-// reference's decisions over the table, writes the unit record and, when
-// asked, filters the unit with the winner into the output plane.
+// stays below 2^32).  When the output is wanted, each exact filter also
+// stores its filtered unit in a candidate buffer ([unit][job][64 x 64]
+// bytes, 10 MB at 1080p, so it stays in L2).  k_lr_search_decide: one CTA
+// per unit replays the reference's decisions over the table, writes the
+// unit record and copies the winner's samples (or the unfiltered ones) into
+// the output plane.
 
 // The candidate tap sets and presets of encoder/restoration.go:166-173 and
 // :235-240, in the reference's order (first strictly better wins).
@@ -375,7 +378,14 @@ struct LrsArgs {
   int W, H, horz, vert;
   LrsSse* table;
   pf_lr_search_unit* out;
+  uint8_t* cand;  // [unit][1 + PF_LR_SGR_PRESETS][64 * 64]; null: search only
 };
+
+constexpr int kLrsJobs = 1 + PF_LR_SGR_PRESETS;
+
+__device__ __forceinline__ uint8_t* lrs_cand(const LrsArgs& a, int unit, int job) {
+  return a.cand + ((size_t)unit * kLrsJobs + job) * 4096;
+}
 
 struct LrsSmem {
   LrSmem lr;
@@ -477,7 +487,7 @@ __device__ __forceinline__ int lrs_wiener_pick(const uint32_t* cand, uint32_t ba
   return pick;
 }
 
-__global__ void __launch_bounds__(256, 2) k_lr_search_sse(LrsArgs a) {
+__global__ void __launch_bounds__(256, 3) k_lr_search_sse(LrsArgs a) {
   extern __shared__ __align__(16) uint8_t lrs_smem_raw[];
   LrsSmem& sm = *reinterpret_cast<LrsSmem*>(lrs_smem_raw);
   const int unit = blockIdx.x, job = blockIdx.y;
@@ -496,9 +506,11 @@ __global__ void __launch_bounds__(256, 2) k_lr_search_sse(LrsArgs a) {
     }
     lrs_stage(a, sm, x0, y0, w, h, true, true);
     uint32_t acc[1] = {0};
+    uint8_t* keep = a.cand ? lrs_cand(a, unit, job) : nullptr;
     lr_sgr_window(sm.lr, w, h, 8, c_lrs_sgr[p][0], c_lrs_sgr[p][1], c_lrs_sgr[p][2], 64, [&](int y, int x, int v) {
       const int d = (int)sm.src[y * 64 + x] - v;
       acc[0] += (uint32_t)(d * d);
+      if (keep) keep[y * 64 + x] = (uint8_t)v;
     });
     lrs_block_sum(acc, sm.red);
     if (tid == 0) T.sgr[p] = acc[0];
@@ -542,9 +554,11 @@ __global__ void __launch_bounds__(256, 2) k_lr_search_sse(LrsArgs a) {
     int fv[7];
     lrs_taps(pick, fv);
     ex[0] = 0;
+    uint8_t* keep = a.cand ? lrs_cand(a, unit, 0) : nullptr;
     lr_wiener_window(sm.lr, w, h, 8, fv, fv, 64, [&](int y, int x, int v) {
       const int d = (int)sm.src[y * 64 + x] - v;
       ex[0] += (uint32_t)(d * d);
+      if (keep) keep[y * 64 + x] = (uint8_t)v;
     });
     lrs_block_sum(ex, sm.red);
   }
@@ -559,8 +573,6 @@ __global__ void __launch_bounds__(256, 2) k_lr_search_sse(LrsArgs a) {
 // The unit's decision (keyframe_lossy.go:2338-2382) and, with a.dst, the
 // unit filtered by it (:2422-2453).
 __global__ void __launch_bounds__(256) k_lr_search_decide(LrsArgs a) {
-  extern __shared__ __align__(16) uint8_t lrs_smem_raw[];
-  LrsSmem& sm = *reinterpret_cast<LrsSmem*>(lrs_smem_raw);
   const int unit = blockIdx.x, tid = threadIdx.x;
   int x0, y0, x1, y1;
   lrs_rect(a, unit % a.horz, unit / a.horz, x0, y0, x1, y1);
@@ -611,22 +623,19 @@ __global__ void __launch_bounds__(256) k_lr_search_decide(LrsArgs a) {
     a.out[unit] = r;
   }
   if (!a.dst) return;
-  if (type == PF_LR_NONE) {
-    for (int i = tid; i < w * h; i += 256) {
-      const int y = y0 + i / w, x = x0 + i % w;
-      a.dst[(int64_t)y * a.dstride + x] = a.rec[(int64_t)y * a.rstride + x];
-    }
+  // keyframe_lossy.go:2422-2453: the decided filter's samples, kept by the
+  // measuring CTA; NONE units keep the reconstruction.
+  const uint8_t* from = type == PF_LR_WIENER ? lrs_cand(a, unit, 0)
+                        : type == PF_LR_SGRPROJ ? lrs_cand(a, unit, 1 + spick) : nullptr;
+  if (from) {
+    const int x = tid & 63;
+    if (x < w)
+      for (int y = tid >> 6; y < h; y += 4) a.dst[(int64_t)(y0 + y) * a.dstride + x0 + x] = from[y * 64 + x];
     return;
   }
-  lrs_stage(a, sm, x0, y0, w, h, type == PF_LR_SGRPROJ, false);
-  auto store = [&](int y, int x, int v) { a.dst[(int64_t)(y0 + y) * a.dstride + x0 + x] = (uint8_t)v; };
-  if (type == PF_LR_WIENER) {
-    int fv[7];
-    lrs_taps(wpick, fv);
-    lr_wiener_window(sm.lr, w, h, 8, fv, fv, 64, store);
-  } else {
-    lr_sgr_window(sm.lr, w, h, 8, c_lrs_sgr[spick][0], c_lrs_sgr[spick][1], c_lrs_sgr[spick][2], 64, store);
-  }
+  for (int y = tid >> 5; y < h; y += 8)
+    for (int x = tid & 31; x < w; x += 32)
+      a.dst[(int64_t)(y0 + y) * a.dstride + x0 + x] = a.rec[(int64_t)(y0 + y) * a.rstride + x0 + x];
 }
 
 static int lrs_check(const pf_frame* f, const pf_frame* ref) {
@@ -677,6 +686,8 @@ extern "C" int pf_lr_search(pf_ctx* ctx, const pf_frame* source, const pf_frame*
   off += host || alias ? plane : 0;
   const size_t oDst = off;
   off += host && restored ? plane : 0;
+  const size_t oCand = off;
+  off += restored ? (size_t)n * kLrsJobs * 4096 : 0;
   uint8_t* base = (uint8_t*)pf_internal_search_scratch(ctx, off);
   if (!base) return PF_ERR_DEVICE;
   LrsArgs a;
@@ -686,6 +697,7 @@ extern "C" int pf_lr_search(pf_ctx* ctx, const pf_frame* source, const pf_frame*
   a.vert = vert;
   a.table = (LrsSse*)(base + oTab);
   a.out = (pf_lr_search_unit*)(base + oOut);
+  a.cand = restored ? base + oCand : nullptr;
   cudaError_t e = cudaSuccess;
   const cudaMemcpyKind up = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   if (host) {
@@ -714,14 +726,12 @@ extern "C" int pf_lr_search(pf_ctx* ctx, const pf_frame* source, const pf_frame*
   static bool configured = false;
   if (!configured) {
     if (cudaFuncSetAttribute(k_lr_search_sse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LrsSmem)) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_lr_search_decide, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(LrsSmem)) != cudaSuccess)
+        cudaSuccess)
       return PF_ERR_DEVICE;
     configured = true;
   }
   k_lr_search_sse<<<dim3(n, 1 + PF_LR_SGR_PRESETS), 256, sizeof(LrsSmem), st>>>(a);
-  k_lr_search_decide<<<n, 256, sizeof(LrsSmem), st>>>(a);
+  k_lr_search_decide<<<n, 256, 0, st>>>(a);
   e = cudaGetLastError();
   if (e == cudaSuccess && host && restored)
     e = cudaMemcpy2DAsync(restored->plane[0].data, restored->plane[0].stride, a.dst, W, W, H,

@@ -847,6 +847,73 @@ extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_fram
   return search_finish(S, params, mse_out, fb_index_out, result);
 }
 
+// Host or device bytes into a host vector.
+static bool read_small(const uint8_t* p, size_t n, std::vector<uint8_t>* out) {
+  out->resize(n);
+  cudaPointerAttributes at;
+  const bool dev = cudaPointerGetAttributes(&at, p) == cudaSuccess &&
+                   (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged);
+  cudaGetLastError();
+  if (!dev) {
+    memcpy(out->data(), p, n);
+    return true;
+  }
+  return cudaMemcpy(out->data(), p, n, cudaMemcpyDeviceToHost) == cudaSuccess;
+}
+
+extern "C" int pf_cdef_apply(pf_ctx* ctx, const pf_frame* recon, const uint8_t* noskip,
+                             const pf_cdef_search_params* params, const pf_cdef_search_result* result,
+                             const uint8_t* fb_index) {
+  if (!ctx || !recon || !params || !result) return PF_ERR_INVALID_ARG;
+  const int stt = check_search_frame(recon, recon);
+  if (stt != PF_OK) return stt;
+  if (result->bits > 3) return PF_ERR_INVALID_CDEF;
+  const int count = 1 << result->bits;
+  // cdef_apply.go:262-271: nothing to do when every strength is zero.
+  bool zero = true;
+  for (int i = 0; i < count; i++)
+    if (result->y_strength[i] || result->uv_strength[i]) zero = false;
+  if (zero) return PF_OK;
+  const int ucols = (recon->width + 63) / 64, urows = (recon->height + 63) / 64, n = ucols * urows;
+  std::vector<uint8_t> ns, idx, read(n, 1), index(n, 0);
+  if (noskip && !read_small(noskip, (size_t)n * 8, &ns)) return PF_ERR_DEVICE;
+  if (fb_index && !read_small(fb_index, n, &idx)) return PF_ERR_DEVICE;
+  // cdef_apply.go:202-235 (markFromLoopFilterMap, noskip-grid branch): a
+  // unit is coded, with its searched index, when an in-frame 8x8 block of it
+  // carries residual.
+  const int cols8 = (recon->width + 7) >> 3, rows8 = (recon->height + 7) >> 3;
+  for (int uy = 0; uy < urows; uy++)
+    for (int ux = 0; ux < ucols; ux++) {
+      const int u = uy * ucols + ux;
+      if (noskip) {
+        uint64_t inFrame = 0, word = 0;
+        for (int by = 0; by < 8 && uy * 8 + by < rows8; by++)
+          for (int bx = 0; bx < 8 && ux * 8 + bx < cols8; bx++) inFrame |= 1ull << (by * 8 + bx);
+        for (int b = 0; b < 8; b++) word |= (uint64_t)ns[(size_t)u * 8 + b] << (8 * b);
+        read[u] = (word & inFrame) != 0;
+      }
+      index[u] = read[u] && fb_index ? idx[u] : 0;
+    }
+  pf_frame_side side;
+  memset(&side, 0, sizeof(side));
+  side.stages = PF_STAGE_CDEF;
+  side.side_memory = PF_MEM_HOST;
+  pf_cdef& c = side.cdef;
+  c.damping = (uint8_t)search_damping(params);
+  c.bits = result->bits;
+  c.strength_count = (uint8_t)count;
+  memcpy(c.y_strength, result->y_strength, 8);
+  memcpy(c.uv_strength, result->uv_strength, 8);
+  c.index = index.data();
+  c.read = read.data();
+  c.index_stride = ucols;
+  c.index_rows = urows;
+  c.noskip = noskip ? ns.data() : nullptr;
+  const int r = pf_frame_apply(ctx, recon, &side, nullptr, nullptr);
+  if (r != PF_OK) return r;
+  return pf_sync(ctx);
+}
+
 extern "C" int pf_cdef_features(pf_ctx* ctx, const pf_frame* recon, const uint8_t* noskip, int32_t qindex,
                                 int32_t damping, float* features) {
   if (!ctx || !recon || !features) return PF_ERR_INVALID_ARG;

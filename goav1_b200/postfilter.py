@@ -158,6 +158,17 @@ class PostFilterRunner:
                                    mse.ctypes.data if want_mse else None, idx.ctypes.data, C.byref(res)))
         return res, mse, idx
 
+    def cdef_apply(self, recon, noskip, qindex, result, fb_index, damping=0):
+        """The encoder's CDEF application (cdefApplier.apply,
+        internal/av1/encoder/cdef_apply.go:202-371): filters the 8-bit 4:2:0
+        `recon` (pf_frame view, host or device) in place with a search's
+        pf_cdef_search_result and per-block indices (uint8[nfb] or None), the
+        units coded as the decoder rebuilds them from the noskip words."""
+        prm = abi.pf_cdef_search_params(qindex=qindex, damping=damping, max_presets=8, lam=0.0)
+        check(lib().pf_cdef_apply(self._h, C.byref(recon), noskip.ctypes.data if noskip is not None else None,
+                                  C.byref(prm), C.byref(result),
+                                  fb_index.ctypes.data if fb_index is not None else None))
+
     def lr_search(self, source, recon, restored=None):
         """Encoder loop-restoration unit search on the luma of 8-bit 4:2:0
         frames: SearchWienerUnitU8 and SearchSGRProjUnitU8 per 64x64 unit

@@ -15,6 +15,8 @@
  *                          (decoder_postfilter_bind.go:252-256, :434-439).
  *   - pf_cdef_search      internal/av1/encoder/cdef_search.go:580-634
  *                          (cdefSearcher.search) + :886-945 (finish).
+ *   - pf_cdef_apply       internal/av1/encoder/cdef_apply.go:202-371
+ *                          (cdefApplier.markFromLoopFilterMap + apply).
  *   - pf_lr_search        internal/av1/encoder/restoration.go:149-263
  *                          (SearchWienerUnitU8, SearchSGRProjUnitU8) and the
  *                          unit loops of EncodeLoopRestorationKeyframe,
@@ -334,6 +336,22 @@ int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
                    const uint8_t* noskip, const pf_cdef_search_params* params,
                    uint64_t* mse_out, uint8_t* fb_index_out,
                    pf_cdef_search_result* result);
+
+/* The encoder's CDEF application (cdefApplier.apply,
+ * internal/av1/encoder/cdef_apply.go:258-371): filters `recon` in place with
+ * the searched parameters, leaving it equal to the decoder's post-CDEF
+ * output.  The per-unit index map is the one the decoder rebuilds while
+ * parsing (markFromLoopFilterMap, :202-235): a 64x64 unit is filtered, with
+ * fb_index[unit] (0 when fb_index is NULL, as for result->bits == 0), when
+ * any of its in-frame 8x8 blocks has its noskip bit set; noskip NULL
+ * filters every unit.  Damping is params->damping, or 3 + (qindex >> 6)
+ * when 0 (cdef_frame.go:62).  A result whose strengths are all zero leaves
+ * recon untouched (:262-271).  8-bit 4:2:0 frames only; recon is a host or
+ * device frame, noskip and fb_index host or device memory.  Returns when
+ * the frame is filtered. */
+int pf_cdef_apply(pf_ctx* ctx, const pf_frame* recon, const uint8_t* noskip,
+                  const pf_cdef_search_params* params, const pf_cdef_search_result* result,
+                  const uint8_t* fb_index);
 
 /* ---- film grain with no allocation ----
  * No counterpart in the reference; this entry point exists for callers that
