@@ -16,6 +16,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <new>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "pf_common.cuh"
@@ -58,6 +61,33 @@ struct DevBuf {
 
 int bps_of(const pf_frame* f) { return f->bit_depth > 8 ? 2 : 1; }
 
+// Page-locked host allocator whose element construction leaves bytes as they
+// are (staging that is always overwritten is not zero-filled first).
+template <class T>
+struct PinnedAlloc {
+  using value_type = T;
+  PinnedAlloc() = default;
+  template <class U>
+  PinnedAlloc(const PinnedAlloc<U>&) {}
+  T* allocate(size_t n) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, n * sizeof(T)) != cudaSuccess) throw std::bad_alloc();
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t) { cudaFreeHost(p); }
+  template <class U>
+  void construct(U* p) {
+    ::new ((void*)p) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new ((void*)p) U(std::forward<A>(a)...);
+  }
+  bool operator==(const PinnedAlloc&) const { return true; }
+  bool operator!=(const PinnedAlloc&) const { return false; }
+};
+using PinnedBytes = std::vector<uint8_t, PinnedAlloc<uint8_t>>;
+
 }  // namespace
 
 struct pf_ctx {
@@ -87,6 +117,22 @@ struct pf_ctx {
   int graphs = 0;
   std::vector<struct GraphEntry*> gcache;
   uint64_t gclock = 0;
+  // Host-frame batches (run_host_pipeline): copy streams and a ring of
+  // staging slots, each a chunk of frames on the device with the page-locked
+  // tables of its launch.
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  struct HostSlot {
+    DevBuf io, disp;
+    void* pjobs = nullptr;
+    size_t njobs = 0;
+    void* pbase = nullptr;
+    size_t nbase = 0;
+    PinnedBytes side;  // the chunk's side information, written in place
+    DevBuf djobs, dbases, dside;  // the chunk's tables on the device
+    cudaEvent_t up = nullptr, comp = nullptr, down = nullptr;
+    bool used = false;
+  } hslot[3];
+  int host_chunk = 4;
 };
 
 // One captured batch signature, in two slots used in turn: each slot is a
@@ -124,6 +170,21 @@ struct GraphEntry {
 
 // ---------------------------------------------------------------------------
 // Validation (no device work; mirrors the reference's error taxonomy).
+
+// Whether any of n bytes exceeds 63 (bit 6 or 7 set), read 8 bytes at a
+// time without an early exit so the compiler vectorises the scan of a
+// frame's level cache (half a megabyte at 1080p).
+static bool any_byte_above_63(const uint8_t* p, size_t n) {
+  uint64_t acc = 0;
+  size_t i = 0;
+  for (; i + 8 <= n; i += 8) {
+    uint64_t w;
+    memcpy(&w, p + i, 8);
+    acc |= w;
+  }
+  for (; i < n; i++) acc |= p[i];
+  return (acc & 0xC0C0C0C0C0C0C0C0ull) != 0;
+}
 
 static int plane_dims_ok(const pf_frame* f) {
   if (f->bit_depth != 8 && f->bit_depth != 10 && f->bit_depth != 12) return 0;
@@ -178,10 +239,7 @@ extern "C" int pf_frame_validate(const pf_frame* f, const pf_frame_side* s, cons
     if (!lf.masks || !lf.level_cache || lf.mi_cols != miCols || lf.mi_rows != miRows ||
         lf.sb128_w != (miCols + 31) / 32 || lf.sb128_h != (miRows + 31) / 32)
       return PF_ERR_INVALID_FILTER;
-    if (hostSide) {
-      for (int i = 0; i < 4 * miCols * miRows; i++)
-        if (lf.level_cache[i] > 63) return PF_ERR_INVALID_FILTER;
-    }
+    if (hostSide && any_byte_above_63(lf.level_cache, (size_t)4 * miCols * miRows)) return PF_ERR_INVALID_FILTER;
   }
   const int ucols = (f->width + 63) / 64, urows = (f->height + 63) / 64;
   if (s->stages & PF_STAGE_CDEF) {
@@ -378,8 +436,25 @@ extern "C" void pf_destroy(pf_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   cudaStreamSynchronize(c->side);
+  if (c->h2d) cudaStreamSynchronize(c->h2d);
+  if (c->d2h) cudaStreamSynchronize(c->d2h);
   DevBuf* bufs[] = {&c->io, &c->disp, &c->arena, &c->sidebuf, &c->jobs, &c->bases, &c->counters, &c->search};
   for (DevBuf* b : bufs) b->release();
+  for (pf_ctx::HostSlot& h : c->hslot) {
+    h.io.release();
+    h.disp.release();
+    if (h.pjobs) cudaFreeHost(h.pjobs);
+    if (h.pbase) cudaFreeHost(h.pbase);
+    PinnedBytes().swap(h.side);
+    h.djobs.release();
+    h.dbases.release();
+    h.dside.release();
+    if (h.up) cudaEventDestroy(h.up);
+    if (h.comp) cudaEventDestroy(h.comp);
+    if (h.down) cudaEventDestroy(h.down);
+  }
+  if (c->h2d) cudaStreamDestroy(c->h2d);
+  if (c->d2h) cudaStreamDestroy(c->d2h);
   c->model.release();
   for (GraphEntry* g : c->gcache) delete g;
   c->gcache.clear();
@@ -487,7 +562,8 @@ struct Cursor {
   }
 };
 
-static const void* put_side(std::vector<uint8_t>& hs, Cursor& dev, const void* src, size_t n) {
+template <class Bytes>
+static const void* put_side(Bytes& hs, Cursor& dev, const void* src, size_t n) {
   if (!src || n == 0) return src;
   void* d = dev.take(n);
   const size_t at = (uint8_t*)d - dev.base;
@@ -496,8 +572,8 @@ static const void* put_side(std::vector<uint8_t>& hs, Cursor& dev, const void* s
   return d;
 }
 
-static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, std::vector<uint8_t>& hs, FrameJob& J,
-                     int counts[ST_COUNT]) {
+template <class Bytes>
+static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, Bytes& hs, FrameJob& J, int counts[ST_COUNT]) {
   const pf_frame* f = r.f;
   const pf_frame_side* s = r.s;
   const int bps = bps_of(f);
@@ -690,15 +766,24 @@ static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, std::vector
 
 // Queues the copies of the host tables (from the given host buffers) and
 // every stage's launch on the context's streams.
-static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, const uint8_t* hside, int n, bool fg) {
+// djobs / dbases: device copies of the tables when the caller uploaded them
+// already (null: copy hjobs / hbase / hside into the context's buffers here).
+static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, const uint8_t* hside, size_t nside,
+                         int n, bool fg, const void* djobs = nullptr, const void* dbases = nullptr) {
   const cudaStream_t st = c->stream;
-  if (!c->hside.empty()) CK(cudaMemcpyAsync(c->sidebuf.p, hside, c->hside.size(), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(c->jobs.p, hjobs, sizeof(FrameJob) * n, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(c->bases.p, hbase, sizeof(int) * c->hbase.size(), cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(c->counters.p, 0, sizeof(int) * ST_COUNT, st));
+  if (!djobs) {
+    if (nside) CK(cudaMemcpyAsync(c->sidebuf.p, hside, nside, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->jobs.p, hjobs, sizeof(FrameJob) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->bases.p, hbase, sizeof(int) * c->hbase.size(), cudaMemcpyHostToDevice, st));
+    djobs = c->jobs.p;
+    dbases = c->bases.p;
+  }
+  bool persistent = false;
+  for (int k = 0; k < ST_COUNT; k++) persistent |= c->persistent[k] > 0;
+  if (persistent) CK(cudaMemsetAsync(c->counters.p, 0, sizeof(int) * ST_COUNT, st));
   BatchArgs b;
-  b.jobs = (const FrameJob*)c->jobs.p;
-  b.base = (const int*)c->bases.p;
+  b.jobs = (const FrameJob*)djobs;
+  b.base = (const int*)dbases;
   b.n = n;
   auto total = [&](int k) { return hbase[(size_t)k * (n + 1) + n]; };
   auto args = [&](int k, int* grid) {
@@ -800,7 +885,8 @@ static int replay_or_capture(pf_ctx* c, int n, bool fg) {
   if (ns) memcpy(g.pside, c->hside.data(), ns);
   if (!g.exec) {
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int est = enqueue_batch(c, (const FrameJob*)g.pjobs, (const int*)g.pbase, (const uint8_t*)g.pside, n, fg);
+    const int est =
+        enqueue_batch(c, (const FrameJob*)g.pjobs, (const int*)g.pbase, (const uint8_t*)g.pside, ns, n, fg);
     const cudaError_t ce = cudaStreamEndCapture(st, &g.graph);
     cudaError_t ie = cudaSuccess;
     if (est == PF_OK && ce == cudaSuccess) ie = cudaGraphInstantiate(&g.exec, g.graph, 0);
@@ -817,23 +903,29 @@ static int replay_or_capture(pf_ctx* c, int n, bool fg) {
   return PF_OK;
 }
 
-// Builds the job table for n validated frames and queues every stage.
-static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats, bool useGraph = false) {
+// Builds the job table and prefix arrays of n validated frames into c->hjobs
+// / hbase and their host side information into hs (the device buffers they
+// address are sized here); *fg tells whether any frame has film grain.
+// sideDev: where the side information goes on the device (the context's
+// buffer, or a host-pipeline slot's).
+template <class Bytes>
+static int prepare_batch(pf_ctx* c, const FrameRef* refs, int n, Bytes& hs, DevBuf& sideDev, uint32_t* completed,
+                         bool* fg) {
   size_t arenaBytes = 0, sideBytes = 0;
   for (int i = 0; i < n; i++) {
     arenaBytes += frame_scratch(refs[i].f, refs[i].s);
     sideBytes += frame_side_bytes(refs[i].f, refs[i].s);
   }
   CK(c->arena.ensure(arenaBytes + 256));
-  CK(c->sidebuf.ensure(sideBytes + 256));
-  Cursor arena{(uint8_t*)c->arena.p, 0}, side{(uint8_t*)c->sidebuf.p, 0};
+  CK(sideDev.ensure(sideBytes + 256));
+  Cursor arena{(uint8_t*)c->arena.p, 0}, side{(uint8_t*)sideDev.p, 0};
   c->hjobs.resize(n);
   c->hbase.assign((size_t)ST_COUNT * (n + 1), 0);
-  c->hside.clear();
+  hs.clear();
   uint32_t done = 0;
   for (int i = 0; i < n; i++) {
     int counts[ST_COUNT];
-    fill_job(refs[i], arena, side, c->hside, c->hjobs[i], counts);
+    fill_job(refs[i], arena, side, hs, c->hjobs[i], counts);
     for (int k = 0; k < ST_COUNT; k++) c->hbase[(size_t)k * (n + 1) + i + 1] = c->hbase[(size_t)k * (n + 1) + i] + counts[k];
     const pf_frame_side* s = refs[i].s;
     if (counts[ST_DEBLOCK_V]) done |= PF_STAGE_LOOP_FILTER;
@@ -845,17 +937,35 @@ static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats, bo
   CK(c->jobs.ensure(sizeof(FrameJob) * n));
   CK(c->bases.ensure(sizeof(int) * c->hbase.size()));
   CK(c->counters.ensure(sizeof(int) * ST_COUNT));
-  const bool fg = c->hbase[(size_t)ST_FG_TEMPLATES * (n + 1) + n] > 0;
-  const int est = (useGraph && !c->timing) ? replay_or_capture(c, n, fg)
-                                           : enqueue_batch(c, c->hjobs.data(), c->hbase.data(), c->hside.data(), n, fg);
-  if (est != PF_OK) return est;
+  *fg = c->hbase[(size_t)ST_FG_TEMPLATES * (n + 1) + n] > 0;
+  *completed = done;
+  return PF_OK;
+}
+
+static void add_stats(const pf_ctx* c, int n, uint32_t done, pf_stats* stats) {
+  if (!stats) return;
   auto total = [&](int k) { return c->hbase[(size_t)k * (n + 1) + n]; };
+  stats->completed |= done;
+  stats->cdef_units += total(ST_CDEF);
+  stats->lr_units += total(ST_LR);
+  stats->fg_rows += total(ST_FG_OFFSETS);
+}
+
+// Builds the job table for n validated frames and queues every stage.
+static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats, bool useGraph = false) {
+  uint32_t done = 0;
+  bool fg = false;
+  int st = prepare_batch(c, refs, n, c->hside, c->sidebuf, &done, &fg);
+  if (st != PF_OK) return st;
+  const int est = (useGraph && !c->timing)
+                      ? replay_or_capture(c, n, fg)
+                      : enqueue_batch(c, c->hjobs.data(), c->hbase.data(), c->hside.data(), c->hside.size(), n, fg);
+  if (est != PF_OK) return est;
   if (stats) {
-    stats->completed = done;
-    stats->cdef_units = total(ST_CDEF);
-    stats->lr_units = total(ST_LR);
-    stats->fg_rows = total(ST_FG_OFFSETS);
+    stats->completed = 0;
+    stats->cdef_units = stats->lr_units = stats->fg_rows = 0;
   }
+  add_stats(c, n, done, stats);
   return PF_OK;
 }
 
@@ -927,17 +1037,207 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
   return PF_OK;
 }
 
+static cudaError_t pinned_ensure(void** p, size_t* n, size_t need) {
+  if (need <= *n) return cudaSuccess;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *n = 0;
+  need = (need + 4095) & ~(size_t)4095;
+  const cudaError_t e = cudaMallocHost(p, need);
+  if (e == cudaSuccess) *n = need;
+  return e;
+}
+
+// Device layout of a host frame's planes at `base`: the host row pitch when
+// rows are packed (pitch = row bytes, a multiple of 16: each plane then moves
+// as one contiguous copy), else rows padded to 256 bytes.
+static size_t host_frame_layout(const pf_frame* f, uint8_t* base, void** ptrs, int64_t* strides) {
+  const int bps = bps_of(f);
+  size_t total = 0;
+  for (int p = 0; p < 3; p++) {
+    const pf_plane& pl = f->plane[p];
+    const int64_t row = (int64_t)pl.alloc_width * bps;
+    strides[p] = pl.stride == row && row % 16 == 0 ? row : (row + 255) & ~(int64_t)255;
+    if (ptrs) ptrs[p] = base + total;
+    total = align256(total + (size_t)strides[p] * pl.alloc_height);
+  }
+  return total;
+}
+
+static cudaError_t copy_planes(const pf_frame* f, void* const* dev, const int64_t* ds, bool up, cudaStream_t st) {
+  const int bps = bps_of(f);
+  for (int p = 0; p < 3; p++) {
+    const pf_plane& pl = f->plane[p];
+    const size_t w = (size_t)pl.alloc_width * bps;
+    cudaError_t e;
+    if (ds[p] == pl.stride && (size_t)pl.stride == w) {
+      const size_t bytes = w * pl.alloc_height;
+      e = up ? cudaMemcpyAsync(dev[p], pl.data, bytes, cudaMemcpyHostToDevice, st)
+             : cudaMemcpyAsync(pl.data, dev[p], bytes, cudaMemcpyDeviceToHost, st);
+    } else {
+      e = up ? cudaMemcpy2DAsync(dev[p], ds[p], pl.data, pl.stride, w, pl.alloc_height, cudaMemcpyHostToDevice, st)
+             : cudaMemcpy2DAsync(pl.data, pl.stride, dev[p], ds[p], w, pl.alloc_height, cudaMemcpyDeviceToHost, st);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// A batch of host frames: chunks of c->host_chunk frames flow through a
+// ring of three device slots, the upload of one chunk (stream h2d), the
+// filtering of the previous one (the main stream) and the download of the
+// one before (stream d2h) overlapping.  The chain itself is run_batch's,
+// unchanged; only the frames' home differs.  Page-locked host frames let the
+// copies run asynchronously; pageable ones are still correct, copied
+// synchronously.
+static int run_host_pipeline(pf_ctx* c, const pf_batch_item* items, int n, pf_stats* stats) {
+  if (!c->h2d) {
+    CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+    for (pf_ctx::HostSlot& h : c->hslot) {
+      CK(cudaEventCreateWithFlags(&h.up, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&h.comp, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&h.down, cudaEventDisableTiming));
+    }
+  }
+  const int chunk = std::max(1, c->host_chunk);
+  const int nchunks = (n + chunk - 1) / chunk;
+  // The shared scratch is sized for the largest chunk before anything is
+  // queued, so it never moves while a chunk is in flight.
+  size_t maxArena = 0, maxSide = 0;
+  for (int k = 0; k < nchunks; k++) {
+    size_t a = 0, b = 0;
+    for (int i = k * chunk; i < std::min(n, (k + 1) * chunk); i++) {
+      a += frame_scratch(items[i].frame, items[i].side);
+      b += frame_side_bytes(items[i].frame, items[i].side);
+    }
+    maxArena = std::max(maxArena, a);
+    maxSide = std::max(maxSide, b);
+  }
+  CK(c->arena.ensure(maxArena + 256));
+  for (pf_ctx::HostSlot& h : c->hslot)
+    if (h.dside.n < maxSide + 256) {
+      if (h.used) CK(cudaEventSynchronize(h.comp));
+      CK(h.dside.ensure(maxSide + 256));
+    }
+  if (stats) memset(stats, 0, sizeof(*stats));
+  std::vector<FrameRef> refs((size_t)chunk);
+  for (int k = 0; k < nchunks; k++) {
+    pf_ctx::HostSlot& h = c->hslot[k % 3];
+    const int i0 = k * chunk, m = std::min(chunk, n - i0);
+    // The slot's tables were read by its previous chunk's launch.
+    if (h.used) CK(cudaEventSynchronize(h.comp));
+    size_t ioBytes = 0, dBytes = 0;
+    for (int i = 0; i < m; i++) {
+      const pf_batch_item& it = items[i0 + i];
+      int64_t st[3];
+      ioBytes += host_frame_layout(it.frame, nullptr, nullptr, st);
+      if ((it.side->stages & PF_STAGE_FILM_GRAIN) && it.display)
+        dBytes += host_frame_layout(it.display, nullptr, nullptr, st);
+    }
+    if (h.used && (ioBytes > h.io.n || dBytes > h.disp.n)) CK(cudaEventSynchronize(h.down));
+    CK(h.io.ensure(ioBytes + 256));
+    CK(h.disp.ensure(dBytes + 256));
+    if (h.used) CK(cudaStreamWaitEvent(c->h2d, h.down, 0));
+    size_t oi = 0, od = 0;
+    for (int i = 0; i < m; i++) {
+      const pf_batch_item& it = items[i0 + i];
+      FrameRef& r = refs[i];
+      memset(&r, 0, sizeof(r));
+      r.f = it.frame;
+      r.s = it.side;
+      const bool wantDisp = (it.side->stages & PF_STAGE_FILM_GRAIN) && it.display;
+      r.display = wantDisp ? it.display : nullptr;
+      oi += host_frame_layout(it.frame, (uint8_t*)h.io.p + oi, r.io, r.ioStride);
+      if (wantDisp) od += host_frame_layout(it.display, (uint8_t*)h.disp.p + od, r.dp, r.dStride);
+      CK(copy_planes(it.frame, r.io, r.ioStride, true, c->h2d));
+    }
+    // The chunk's tables go up with its frames, on the upload stream, into
+    // the slot's own device buffers: the launch then waits for nothing but
+    // the upload event, and no small copy queues behind the next chunk's
+    // frames on the copy engine.
+    uint32_t done = 0;
+    bool fg = false;
+    int st;
+    try {
+      st = prepare_batch(c, refs.data(), m, h.side, h.dside, &done, &fg);  // side information straight into pinned memory
+    } catch (const std::bad_alloc&) {
+      return PF_ERR_DEVICE;
+    }
+    if (st != PF_OK) return st;
+    const size_t nj = sizeof(FrameJob) * m, nb = sizeof(int) * c->hbase.size();
+    CK(pinned_ensure(&h.pjobs, &h.njobs, nj + 16));
+    CK(pinned_ensure(&h.pbase, &h.nbase, nb + 16));
+    CK(h.djobs.ensure(nj + 16));
+    CK(h.dbases.ensure(nb + 16));
+    memcpy(h.pjobs, c->hjobs.data(), nj);
+    memcpy(h.pbase, c->hbase.data(), nb);
+    if (!h.side.empty()) CK(cudaMemcpyAsync(h.dside.p, h.side.data(), h.side.size(), cudaMemcpyHostToDevice, c->h2d));
+    CK(cudaMemcpyAsync(h.djobs.p, h.pjobs, nj, cudaMemcpyHostToDevice, c->h2d));
+    CK(cudaMemcpyAsync(h.dbases.p, h.pbase, nb, cudaMemcpyHostToDevice, c->h2d));
+    CK(cudaEventRecord(h.up, c->h2d));
+    CK(cudaStreamWaitEvent(c->stream, h.up, 0));
+    st = enqueue_batch(c, (const FrameJob*)h.pjobs, (const int*)h.pbase, nullptr, 0, m, fg, h.djobs.p, h.dbases.p);
+    if (st != PF_OK) return st;
+    add_stats(c, m, done, stats);
+    CK(cudaEventRecord(h.comp, c->stream));
+    CK(cudaStreamWaitEvent(c->d2h, h.comp, 0));
+    for (int i = 0; i < m; i++) {
+      CK(copy_planes(refs[i].f, refs[i].io, refs[i].ioStride, false, c->d2h));
+      if (refs[i].display) CK(copy_planes(refs[i].display, refs[i].dp, refs[i].dStride, false, c->d2h));
+    }
+    CK(cudaEventRecord(h.down, c->d2h));
+    h.used = true;
+  }
+  CK(cudaStreamSynchronize(c->d2h));
+  CK(cudaStreamSynchronize(c->stream));
+  read_stage_times(c, stats);
+  CK(cudaGetLastError());
+  return PF_OK;
+}
+
+// Validates a batch's frames on up to 8 host threads (the level-cache scan of
+// a host frame is half a megabyte at 1080p) and returns the status of the
+// first failing frame in batch order, as a serial scan would.
+static int validate_items(const pf_batch_item* items, int n) {
+  std::vector<int> st((size_t)n, PF_OK);
+  int threads = std::min(8, (n + 3) / 4);
+  threads = std::min(threads, (int)std::max(1u, std::thread::hardware_concurrency()));
+  bool serial = threads <= 1;
+  if (!serial) {
+    std::vector<std::thread> pool;
+    try {
+      for (int t = 0; t < threads; t++)
+        pool.emplace_back([&st, items, n, threads, t] {
+          for (int i = t; i < n; i += threads) st[i] = pf_frame_validate(items[i].frame, items[i].side, items[i].display);
+        });
+    } catch (...) {
+      serial = true;
+    }
+    for (std::thread& th : pool) th.join();
+    if (serial)
+      for (int i = 0; i < n; i++) st[i] = PF_OK;
+  }
+  for (int i = 0; i < n; i++) {
+    if (serial) st[i] = pf_frame_validate(items[i].frame, items[i].side, items[i].display);
+    if (st[i] != PF_OK) return st[i];
+  }
+  return PF_OK;
+}
+
 extern "C" int pf_batch_apply(pf_ctx* c, const pf_batch_item* items, int32_t n, pf_stats* stats) {
   if (!c || (!items && n > 0) || n < 0) return PF_ERR_INVALID_ARG;
   if (n > 65535) return PF_ERR_INVALID_ARG;
+  const int vst = validate_items(items, n);
+  if (vst != PF_OK) return vst;
   std::vector<FrameRef> refs((size_t)n);
   for (int i = 0; i < n; i++) {
     const pf_batch_item& it = items[i];
-    int st = pf_frame_validate(it.frame, it.side, it.display);
-    if (st != PF_OK) return st;
     const bool wantDisp = (it.side->stages & PF_STAGE_FILM_GRAIN) && it.display;
-    if (it.frame->memory != PF_MEM_DEVICE || (wantDisp && it.display->memory != PF_MEM_DEVICE))
-      return PF_ERR_INVALID_ARG;
+    // Every frame and display of a batch lives on the same side: all in
+    // device memory, or all in host memory (run_host_pipeline).
+    const int home = items[0].frame->memory;
+    if (it.frame->memory != home || (wantDisp && it.display->memory != home)) return PF_ERR_INVALID_ARG;
     FrameRef& r = refs[i];
     memset(&r, 0, sizeof(r));
     r.f = it.frame;
@@ -953,6 +1253,7 @@ extern "C" int pf_batch_apply(pf_ctx* c, const pf_batch_item* items, int32_t n, 
     }
   }
   CK(cudaSetDevice(c->device));
+  if (n > 0 && items[0].frame->memory == PF_MEM_HOST) return run_host_pipeline(c, items, n, stats);
   if (stats) memset(stats, 0, sizeof(*stats));
   int st = run_batch(c, refs.data(), n, stats, c->graphs != 0);
   if (st != PF_OK) return st;

@@ -33,37 +33,53 @@ __device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
 }
 
 // AR recursion of one template (luma.go:83-158 / chroma.go:92-199 generic
-// form) as a wavefront.  One warp; lanes take rows.
+// form) as a wavefront.  One warp; lanes take rows.  Row y computes column
+// t - 4y at step t, so every causal neighbour (rows above up to x + LAG,
+// LAG <= 3) was written at an earlier step.  The LAG is a template argument:
+// the coefficients sit in registers and the tap loops unroll.
+template <int LAG>
 __device__ void ar_wavefront(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h) {
+  constexpr int kTaps = 2 * LAG * (LAG + 1);  // causal neighbours before the centre
   const int lane = threadIdx.x & 31;
-  const int lag = p.lag, cs = p.coeff_shift, ro = 1 << (cs - 1);
+  const int cs = p.coeff_shift, ro = 1 << (cs - 1);
   const int gmin = -(1 << (p.bd - 1)), gmax = (1 << (p.bd - 1)) - 1;
-  const int8_t* co = p.coeffs[plane];
+  int co[kTaps + 1];
+#pragma unroll
+  for (int i = 0; i <= kTaps; i++) co[i] = p.coeffs[plane][i];
+  const bool lumaTerm = plane != 0 && p.num_y_points != 0;
+  const int sx = plane ? p.ssx : 0, sy = plane ? p.ssy : 0;
   const int tmax = (w - 4) + 4 * (h - 1);
   for (int t = 3 + 4 * 3; t <= tmax; t++) {
     for (int y = 3 + lane; y < h; y += 32) {
       const int x = t - 4 * y;
       if (x < 3 || x >= w - 3) continue;
-      int sum = 0, pos = 0;
-      for (int dr = -lag; dr <= 0; dr++) {
-        for (int dc = -lag; dc <= lag; dc++) {
-          if (dr == 0 && dc == 0) {
-            if (plane != 0 && p.num_y_points != 0) {
-              const int sx = plane ? p.ssx : 0, sy = plane ? p.ssy : 0;
-              const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
-              int s = 0;
-              for (int dy = 0; dy <= sy; dy++)
-                for (int dx = 0; dx <= sx; dx++) s += luma[(ly + dy) * kGW + lx + dx];
-              sum += rpow2(s, sx + sy) * co[pos];
-            }
-            break;
-          }
-          sum += co[pos++] * g[(y + dr) * kGW + x + dc];
-        }
+      int sum = 0;
+      const int16_t* c = &g[y * kGW + x];
+#pragma unroll
+      for (int dr = -LAG; dr <= 0; dr++)
+#pragma unroll
+        for (int dc = -LAG; dc <= (dr < 0 ? LAG : -1); dc++)
+          sum += co[(dr + LAG) * (2 * LAG + 1) + dc + LAG] * c[dr * kGW + dc];
+      if (lumaTerm) {
+        const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
+        int s = 0;
+        for (int dy = 0; dy <= sy; dy++)
+          for (int dx = 0; dx <= sx; dx++) s += luma[(ly + dy) * kGW + lx + dx];
+        sum += rpow2(s, sx + sy) * co[kTaps];
       }
-      g[y * kGW + x] = (int16_t)iclip(g[y * kGW + x] + ((sum + ro) >> cs), gmin, gmax);
+      g[y * kGW + x] = (int16_t)iclip(c[0] + ((sum + ro) >> cs), gmin, gmax);
     }
     __syncwarp();
+  }
+}
+
+__device__ void ar_wavefront_lag(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w,
+                                 int h) {
+  switch (p.lag) {
+    case 0: ar_wavefront<0>(g, luma, p, plane, w, h); break;
+    case 1: ar_wavefront<1>(g, luma, p, plane, w, h); break;
+    case 2: ar_wavefront<2>(g, luma, p, plane, w, h); break;
+    default: ar_wavefront<3>(g, luma, p, plane, w, h); break;
   }
 }
 
@@ -82,7 +98,7 @@ __device__ __forceinline__ uint16_t gf2_apply(const uint16_t* cols, uint16_t v) 
 
 // Gaussian fill of one template (luma.go:32-38 / chroma.go:38-44): draw i of
 // the plane's LFSR goes to sample (i / w, i % w).  One warp.
-__device__ void gauss_fill(int16_t* g, uint16_t seed, int w, int h, int shape, int shift) {
+__device__ void gauss_fill(int16_t* g, const int16_t* gauss, uint16_t seed, int w, int h, int shape, int shift) {
   const int lane = threadIdx.x & 31;
   const int L = c_jump_len[shape];
   uint16_t reg = gf2_apply(c_jump[shape][lane], seed);
@@ -91,7 +107,7 @@ __device__ void gauss_fill(int16_t* g, uint16_t seed, int w, int h, int shape, i
   const int iend = imin(i + L, n);
   int y = i / w, x = i - y * w;
   for (; i < iend; i++) {
-    g[y * kGW + x] = (int16_t)rpow2(c_gauss[lfsr(reg, 11)], shift);
+    g[y * kGW + x] = (int16_t)rpow2(gauss[lfsr(reg, 11)], shift);
     if (++x == w) {
       x = 0;
       y++;
@@ -100,7 +116,10 @@ __device__ void gauss_fill(int16_t* g, uint16_t seed, int w, int h, int shape, i
 }
 
 // One frame's templates: luma (warp 0), then Cb and Cr (warps 1, 2).
-__device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, int16_t (*s_g)[kGW * kGH]) {
+// s_gauss holds the Gaussian sequence (lanes draw different entries, which
+// constant memory would serialise).
+__device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, int16_t (*s_g)[kGW * kGH],
+                             const int16_t* s_gauss) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int16_t* outs[3] = {gy, gu, gv};
   const int cw = p.ssx ? 44 : kGW, ch = p.ssy ? 38 : kGH;
@@ -113,18 +132,18 @@ __device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, 
     const int shift = 12 - p.bd + p.grain_scale_shift;
     if (active) {
       if (warp == 0)
-        gauss_fill(g, p.seed, kGW, kGH, 0, shift);
+        gauss_fill(g, s_gauss, p.seed, kGW, kGH, 0, shift);
       else
-        gauss_fill(g, (uint16_t)(p.seed ^ (warp == 1 ? 0xb524 : 0x49d8)), cw, ch, cshape, shift);
+        gauss_fill(g, s_gauss, (uint16_t)(p.seed ^ (warp == 1 ? 0xb524 : 0x49d8)), cw, ch, cshape, shift);
     }
     __syncwarp();
   }
   __syncthreads();
-  if (warp == 0 && p.num_y_points != 0 && p.lag != 0) ar_wavefront(s_g[0], nullptr, p, 0, kGW, kGH);
+  if (warp == 0 && p.num_y_points != 0 && p.lag != 0) ar_wavefront_lag(s_g[0], nullptr, p, 0, kGW, kGH);
   __syncthreads();
   if (warp == 1 || warp == 2) {
     const bool run = p.active[warp] && !(p.lag == 0 && p.num_y_points == 0);
-    if (run) ar_wavefront(s_g[warp], s_g[0], p, warp, cw, ch);
+    if (run) ar_wavefront_lag(s_g[warp], s_g[0], p, warp, cw, ch);
   }
   __syncthreads();
   for (int pl = 0; pl < 3; pl++)
@@ -266,10 +285,13 @@ __device__ __forceinline__ void extend_px(const DFrame& f, int plane, int x, int
 
 __global__ void __launch_bounds__(96) k_fg_templates_batch(BatchArgs b) {
   __shared__ int16_t s_g[3][kGW * kGH];
+  __shared__ int16_t s_gauss[2048];
+  for (int i = threadIdx.x; i < 2048; i += blockDim.x) s_gauss[i] = c_gauss[i];
+  __syncthreads();
   const int* base = b.base + ST_FG_TEMPLATES * (b.n + 1);
   for_each_item(base[b.n], b.counters ? b.counters + ST_FG_TEMPLATES : nullptr, [&](int item) {
     const FrameJob& J = b.jobs[find_frame(base, b.n, item)];
-    fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], s_g);
+    fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], s_g, s_gauss);
   });
 }
 

@@ -266,9 +266,17 @@ typedef struct pf_batch_item {
   const pf_frame* display;
 } pf_batch_item;
 
-/* Filters n device-resident frames of any size, bit depth and chroma format.
- * Work units of all frames share one queue per stage, drained by persistent
- * CTAs (one per SM).  Equivalent to n pf_frame_apply calls. */
+/* Filters n frames of any size, bit depth and chroma format; equivalent to
+ * n pf_frame_apply calls.  Device-resident frames: work units of all frames
+ * share one launch per stage (see batch scheduling below); the call returns
+ * once the work is queued (host side information: once it is done).
+ * Host-resident frames (every frame and display of the batch in host
+ * memory): the frames go through in chunks of 4, the upload of one chunk,
+ * the filtering of the previous one and the download of the one before that
+ * overlapping on three streams; the call returns when every frame and
+ * display is back in host memory.  Page-locked host memory lets the copies
+ * overlap; pageable memory works, with synchronous copies.  A batch mixing
+ * host and device frames gets PF_ERR_INVALID_ARG. */
 int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats* stats);
 
 /* ---- batch scheduling (no counterpart in the reference) ----

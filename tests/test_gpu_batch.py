@@ -118,3 +118,57 @@ def test_scheduling_arguments_are_checked():
     with pytest.raises(ErrInvalidArgument):
         r.batch_graphs(2)
     r.close()
+
+
+def _host_copy(fr, pinned, like=False):
+    """A host copy of a frame (or a zeroed frame of its geometry), in
+    page-locked memory when `pinned`."""
+    out = fr.like() if like else fr.copy()
+    if pinned:
+        import torch
+
+        keep = []
+        for k, p in enumerate(out.planes):
+            t = torch.empty(p.shape, dtype=torch.uint8 if p.dtype == np.uint8 else torch.int16, pin_memory=True)
+            a = t.numpy().view(p.dtype)
+            a[:] = p
+            out.planes[k] = a
+            keep.append(t)
+        out._pin = keep
+    return out
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_frame_batches_match_oracle(frames, expected, pinned):
+    """Host frames through pf_batch_apply's chunked copy/compute pipeline:
+    13 frames (four chunks, so the three staging slots wrap) in two calls."""
+    from goav1_b200.postfilter import PostFilterRunner
+
+    order = list(range(len(frames))) + list(range(5))
+    r = PostFilterRunner()
+    for call in range(2):
+        hosts = [(_host_copy(frames[i][0], pinned), _host_copy(frames[i][0], pinned, like=True)) for i in order]
+        items = [(h.pf(), frames[i][1].side, d.pf()) for (h, d), i in zip(hosts, order)]
+        stats = r.apply_batch(items)
+        assert stats.completed == abi.PF_STAGES_ALL
+        for k, ((h, d), i) in enumerate(zip(hosts, order)):
+            ref, disp = expected[i]
+            for name, a, b in (("reference", ref, h), ("display", disp, d)):
+                for p, (pa, pb) in enumerate(zip(a.planes, b.planes)):
+                    assert np.array_equal(pa, pb), "call %d item %d %s plane %d differs in %d samples" % (
+                        call, k, name, p, int((pa != pb).sum()))
+    r.close()
+
+
+def test_mixed_host_and_device_batch_is_rejected(frames):
+    from goav1_b200.postfilter import DeviceFrame, ErrInvalidArgument, PostFilterRunner
+
+    r = PostFilterRunner()
+    (f0, s0), (f1, s1) = frames[0], frames[1]
+    d1 = DeviceFrame(f1)
+    dd1 = DeviceFrame(f1.like())
+    h0, hd0 = f0.copy(), f0.like()
+    with pytest.raises(ErrInvalidArgument):
+        r.apply_batch([(h0.pf(), s0.side, hd0.pf()), (d1.pf(), s1.side, dd1.pf())])
+    assert np.array_equal(h0.planes[0], f0.planes[0])
+    r.close()

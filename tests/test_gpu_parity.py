@@ -154,3 +154,24 @@ def test_batch_mixed_sizes_depths_formats(runner):
         ref, rdisp = _oracle(fr, si)
         _assert_same(ref, d.download(), "batch reference")
         _assert_same(rdisp, dd.download(), "batch display")
+
+
+@pytest.mark.parametrize("lag", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", ["all", "no_luma_points", "cfl", "422_10bit", "444"])
+def test_film_grain_ar_lags(runner, lag, variant):
+    """The grain templates' AR recursion for every lag (compiled per lag),
+    with and without luma scaling points (the chroma luma term), chroma
+    scaling from luma, and each chroma layout."""
+    kw = dict(width=160, height=96, stages=abi.PF_STAGE_FILM_GRAIN)
+    if variant == "422_10bit":
+        kw.update(ss=(1, 0), bit_depth=10)
+    if variant == "444":
+        kw.update(ss=(0, 0))
+    fr, si = synth.make_frame(1, 40 + lag, **kw)
+    fg = si.side.fg
+    fg.ar_coeff_lag = lag
+    if variant == "no_luma_points":
+        fg.num_y_points = 0
+    if variant == "cfl":
+        fg.chroma_scaling_from_luma = 1
+    _check(runner, fr, si)
