@@ -20,13 +20,23 @@
 
 namespace pf {
 
+// 8-bit units without sentinels read constrain() from tables: one per
+// primary strength used in the unit (8-bit strengths are 1..15) and one for
+// the secondary strength, 511 entries each (differences -255..255).
+constexpr int kTabLen = 512;
+constexpr int kSecTab = 16;
+
 struct CdefSmem {
-  uint16_t in[kSH * kSW];
+  alignas(16) uint16_t in[kSH * kSW];
   int32_t cost[64 * 8];
   int32_t var[64];
   int32_t blk[64];   // per block: filter flag << 16 | priShift << 12 | strength << 4 | dir
   int2 ofs[12];      // direction tap offsets in smem units (cdef/filter.go:53-66)
   uint8_t dir[64];
+  int16_t tab[kSecTab + 1][kTabLen];
+  uint32_t strengths;    // bit k: a block of the plane filters with primary strength k
+  int8_t slot[16];       // table of each primary strength
+  int8_t slot_str[16];   // strength of each table
 };
 
 // One 64x64 filter unit (uc, ur), all planes.  aw/ah: MI-aligned extents
@@ -102,7 +112,34 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
       const int fillW = unitW + 16, fillH = unitH + 4;
       const int warp = tid >> 5, lane = tid & 31;
       const bool interior = srcX0 == unitX - 8 && srcX1 == wantX1 && srcY0 == unitY - 2 && srcY1 == wantY1;
-      if (interior) {
+      const uint8_t* tile0 = reinterpret_cast<const uint8_t*>(row_ptr<T>(ip, unitY - 2) + (unitX - 8));
+      // Words of 8 samples: 8 bytes (8-bit, rows start 8 bytes before a
+      // 64-sample unit) or 16 bytes (10/12-bit).
+      constexpr int kWord = 8 * sizeof(T);
+      if (interior && fillW % 8 == 0 &&
+          ((reinterpret_cast<uintptr_t>(tile0) | (uintptr_t)ip.stride) & (kWord - 1)) == 0) {
+        // Interior unit with aligned rows: the whole halo is frame data, a
+        // thread's few words unrolled so their loads are in flight together.
+        const int wpr = fillW / 8, total = fillH * wpr;
+        constexpr int kMaxItems = (kSH * (kSW / 8) + 255) / 256;
+#pragma unroll
+        for (int k = 0; k < kMaxItems; k++) {
+          const int i = tid + 256 * k;
+          if (i < total) {
+            const int r = i / wpr, cw = i - r * wpr;
+            const uint8_t* src = tile0 + (int64_t)r * ip.stride + cw * kWord;
+            uint4 v;
+            if (sizeof(T) == 1) {
+              const uint2 w = *reinterpret_cast<const uint2*>(src);
+              v = make_uint4(__byte_perm(w.x, 0, 0x4140), __byte_perm(w.x, 0, 0x4342), __byte_perm(w.y, 0, 0x4140),
+                             __byte_perm(w.y, 0, 0x4342));
+            } else {
+              v = *reinterpret_cast<const uint4*>(src);
+            }
+            *reinterpret_cast<uint4*>(&s_in[r * kSW + cw * 8]) = v;
+          }
+        }
+      } else if (interior) {
         // Interior unit: the whole halo is frame data.
         for (int r = warp; r < fillH; r += 8) {
           const T* src = row_ptr<T>(ip, unitY - 2 + r) + (unitX - 8);
@@ -173,6 +210,10 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
       const bool lumaAdjust = plane == 0 && (needPrimary || pri != 0);
       // Per-block parameters once (cdef/filter.go:490-543): adjusted luma
       // strength, direction (0 when the primary strength is zero), shift.
+      // 8-bit units whose halo is all frame data: constrain() from tables.
+      const bool useTab = sizeof(T) == 1 && interior;
+      if (tid == 0) sm.strengths = 0;
+      __syncthreads();
       if (tid < 64) {
         const int b = tid;
         int pk = 0;
@@ -180,11 +221,33 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
           const int strength = lumaAdjust ? adjust_strength(pri, s_var[b]) : pri;
           const int dir = pri != 0 ? s_dir[b] : 0;
           pk = (1 << 16) | (constrain_shift(strength, damping) << 12) | (strength << 4) | dir;
+          if (useTab && strength) atomicOr(&sm.strengths, 1u << strength);
         }
         sm.blk[b] = pk;
       }
       __syncthreads();
       const int secShift = constrain_shift(sec, damping);
+      if (useTab) {
+        const uint32_t used = sm.strengths;
+        const int ntab = __popc(used);
+        if (tid < 16) {
+          const bool on = (used >> tid) & 1;
+          const int k = __popc(used & ((1u << tid) - 1));
+          sm.slot[tid] = on ? (int8_t)k : (int8_t)-1;
+          if (on) sm.slot_str[k] = (int8_t)tid;
+        }
+        __syncthreads();
+        for (int i = tid; i < (ntab + 1) * 511; i += 256) {
+          const int t = i / 511, d = i - t * 511 - 255;
+          if (t < ntab) {
+            const int st = sm.slot_str[t];
+            sm.tab[t][d + 255] = (int16_t)constrain(d, st, constrain_shift(st, damping));
+          } else {
+            sm.tab[kSecTab][d + 255] = (int16_t)(sec ? constrain(d, sec, secShift) : 0);
+          }
+        }
+        __syncthreads();
+      }
       if (tx < unitW) {
         for (int y = ty0; y < unitH; y += rowStep) {
           const int b = ((y >> bhLog2) << 3) + (tx >> bwLog2);
@@ -193,7 +256,11 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
           int v = c[0];
           if (pk >> 16) {
             const int strength = (pk >> 4) & 255, dir = pk & 7;
-            if (strength | sec) {
+            if (useTab) {
+              if (strength | sec)
+                v = cdef_filter_px_tab(c, strength, strength ? &sm.tab[sm.slot[strength]][255] : nullptr, sec,
+                                       &sm.tab[kSecTab][255], sm.ofs[dir + 2], sm.ofs[dir + 4], sm.ofs[dir]);
+            } else if (strength | sec) {
               if (interior)  // no VeryLarge sentinel anywhere in the halo
                 v = cdef_filter_px<false>(c, strength, (pk >> 12) & 15, sec, secShift, sm.ofs[dir + 2],
                                           sm.ofs[dir + 4], sm.ofs[dir], coeffShift);
@@ -208,20 +275,27 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
       __syncthreads();
     }
     // ---- fused loop-restoration boundary-line save (pre-CDEF rows) ----
+    // Rows b-2 .. b+1 around each stripe boundary b = k*SH - off (k >= 1)
+    // inside the unit; the rows of one boundary are spread over the CTA.
     if (a.save_lines[plane]) {
       const int Hc = ip.h, Wc = ip.w;
       const int SHs = 64 >> ydec, off = 8 >> ydec;
-      for (int y = unitY; y < unitY + unitH && y < Hc; y++) {
-        const int k = (y + off + 2) / SHs;
-        const int b = k * SHs - off;
-        const int j = y - (b - 2);
-        if (k < 1 || b >= Hc || j < 0 || j > 3) continue;
-        const T* src = row_ptr<T>(ip, y);
-        for (int x = unitX + tid; x < unitX + unitW && x < Wc; x += 256) {
-          const T v = src[x];
-          reinterpret_cast<T*>(a.lines[plane] + (int64_t)(k * 4 + j) * a.line_stride[plane])[x] = v;
-          if (j == 2 && b + 1 >= Hc)
-            reinterpret_cast<T*>(a.lines[plane] + (int64_t)(k * 4 + 3) * a.line_stride[plane])[x] = v;
+      const int yEnd = imin(unitY + unitH, Hc);
+      if (unitY < yEnd) {
+        const int k0 = imax((unitY + off + 2) / SHs, 1), k1 = (yEnd - 1 + off + 2) / SHs;
+        for (int k = k0; k <= k1; k++) {
+          const int b = k * SHs - off;
+          if (b >= Hc) break;
+          const int ya = imax(unitY, b - 2), yb = imin(yEnd - 1, b + 1);
+          for (int i = tid; i < (yb - ya + 1) * unitW; i += 256) {
+            const int y = ya + i / unitW, x = unitX + i % unitW;
+            if (x >= Wc) continue;
+            const int j = y - (b - 2);
+            const T v = row_ptr<T>(ip, y)[x];
+            reinterpret_cast<T*>(a.lines[plane] + (int64_t)(k * 4 + j) * a.line_stride[plane])[x] = v;
+            if (j == 2 && b + 1 >= Hc)
+              reinterpret_cast<T*>(a.lines[plane] + (int64_t)(k * 4 + 3) * a.line_stride[plane])[x] = v;
+          }
         }
       }
     }
@@ -229,7 +303,7 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
 }
 
 // Batched CDEF: each work item is one 64x64 unit of one frame.
-__global__ void __launch_bounds__(256) k_cdef_batch(BatchArgs b) {
+__global__ void __launch_bounds__(256, 4) k_cdef_batch(BatchArgs b) {
   __shared__ CdefSmem sm;
   const int* base = b.base + ST_CDEF * (b.n + 1);
   for_each_item(base[b.n], b.counters ? b.counters + ST_CDEF : nullptr, [&](int item) {

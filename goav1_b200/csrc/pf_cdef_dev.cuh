@@ -135,4 +135,38 @@ __device__ __forceinline__ int cdef_filter_px(const uint16_t* c, int pri, int pr
   return y;
 }
 
+// cdef_filter_px for 8-bit input without sentinels, with constrain() read
+// from tables: tp (primary, the block's strength) and ts (secondary) point at
+// the entry for a difference of 0 of 511-entry tables covering -255..255,
+// built from constrain() itself, so the result is the same sample.
+__device__ __forceinline__ int cdef_filter_px_tab(const uint16_t* c, int pri, const int16_t* tp, int sec,
+                                                  const int16_t* ts, int2 po, int2 s0, int2 s1) {
+  const int x = c[0];
+  int sum = 0;
+  int hi = x, lo = x;
+  if (pri) {
+    const int odd = pri & 1;
+    const int t0 = odd ? 3 : 4, t1 = odd ? 3 : 2;
+    const int a0 = c[po.x], a1 = c[-po.x], a2 = c[po.y], a3 = c[-po.y];
+    sum += t0 * (tp[a0 - x] + tp[a1 - x]) + t1 * (tp[a2 - x] + tp[a3 - x]);
+    if (sec) {
+      hi = __vimax3_s32(__vimax3_s32(hi, a0, a1), a2, a3);
+      lo = __vimin3_s32(__vimin3_s32(lo, a0, a1), a2, a3);
+    }
+  }
+  if (sec) {
+    const int b0 = c[s0.x], b1 = c[-s0.x], b2 = c[s1.x], b3 = c[-s1.x];
+    const int b4 = c[s0.y], b5 = c[-s0.y], b6 = c[s1.y], b7 = c[-s1.y];
+    sum += 2 * (ts[b0 - x] + ts[b1 - x] + ts[b2 - x] + ts[b3 - x]) + ts[b4 - x] + ts[b5 - x] + ts[b6 - x] +
+           ts[b7 - x];
+    if (pri) {
+      hi = __vimax3_s32(__vimax3_s32(hi, b0, b1), __vimax3_s32(b2, b3, b4), __vimax3_s32(b5, b6, b7));
+      lo = __vimin3_s32(__vimin3_s32(lo, b0, b1), __vimin3_s32(b2, b3, b4), __vimin3_s32(b5, b6, b7));
+    }
+  }
+  int y = x + ((8 + sum - (sum < 0)) >> 4);
+  if (pri && sec) y = imin(imax(y, lo), hi);
+  return y;
+}
+
 }  // namespace pf
