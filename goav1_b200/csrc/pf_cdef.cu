@@ -97,9 +97,7 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
     const int tx = tid % uwMax, ty0 = tid / uwMax;
     if (!active) {
       // Copy-through (inactive unit / plane or the CDEF stage is off).
-      if (tx < unitW)
-        for (int y = ty0; y < unitH; y += rowStep)
-          row_ptr<T>(op, unitY + y)[unitX + tx] = row_ptr<T>(ip, unitY + y)[unitX + tx];
+      if (tx < unitW) copy_column<T>(ip, op, unitX + tx, unitY + ty0, unitY + unitH, rowStep);
     } else {
       // ---- stage the unit + halo (frameWorkFillCDEFInputSentinels /
       //      frameWorkCopyCDEFInput with the replicate quirk) ----

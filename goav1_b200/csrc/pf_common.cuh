@@ -27,6 +27,21 @@ __device__ __forceinline__ T* row_ptr(const DPlane& p, int y) {
   return reinterpret_cast<T*>(p.ptr + (int64_t)y * p.stride);
 }
 
+// Copies column x of rows y, y+step, ... < yEnd from one plane to another,
+// four rows' loads issued before their stores (the planes may not alias).
+template <typename T>
+__device__ __forceinline__ void copy_column(const DPlane& from, const DPlane& to, int x, int y, int yEnd, int step) {
+  for (; y < yEnd; y += 4 * step) {
+    T v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (y + k * step < yEnd) v[k] = row_ptr<T>(from, y + k * step)[x];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (y + k * step < yEnd) row_ptr<T>(to, y + k * step)[x] = v[k];
+  }
+}
+
 __host__ __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 __host__ __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ __forceinline__ int iclip(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }

@@ -250,8 +250,7 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
     if (cand->type == PF_LR_WIENER || cand->type == PF_LR_SGRPROJ) u = cand;
   }
   if (!u) {
-    if (tx < x1 - x0)
-      for (int y = y0 + ty0; y < y1; y += rowStep) row_ptr<T>(dp, y)[x0 + tx] = row_ptr<T>(sp, y)[x0 + tx];
+    if (tx < x1 - x0) copy_column<T>(sp, dp, x0 + tx, y0 + ty0, y1, rowStep);
     return;
   }
   const int h = yf1 - y0, w = xf1 - x0;
@@ -260,17 +259,35 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
   const bool copyAbove = y0 != 0, copyBelow = y0 + nominal < Hc;
   const int kAbove = s, kBelow = s + 1;  // boundary indices of the saved lines
   const int ww = w + 6, wh = h + 6;
-  for (int r = warp; r < wh; r += 8) {
+  auto srcRow = [&](int r) -> const T* {
     const int yy = y0 - 3 + r;
-    const T* srow;
-    if (yy < y0 && copyAbove) {
-      srow = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kAbove * 4 + imax(yy - y0 + 2, 0)) * a.line_stride[plane]);
-    } else if (yy >= yf1 && copyBelow) {
-      srow = reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kBelow * 4 + 2 + imin(yy - yf1, 1)) * a.line_stride[plane]);
-    } else {
-      srow = row_ptr<T>(sp, iclip(yy, 0, Hc - 1));
+    if (yy < y0 && copyAbove)
+      return reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kAbove * 4 + imax(yy - y0 + 2, 0)) * a.line_stride[plane]);
+    if (yy >= yf1 && copyBelow)
+      return reinterpret_cast<const T*>(a.lines[plane] + (int64_t)(kBelow * 4 + 2 + imin(yy - yf1, 1)) * a.line_stride[plane]);
+    return row_ptr<T>(sp, iclip(yy, 0, Hc - 1));
+  };
+  // A warp's rows r and r+8 and each lane's three columns are loaded before
+  // any is stored: six loads in flight per lane (ww <= 70 < 96).
+  for (int r0 = warp; r0 < wh; r0 += 16) {
+    uint16_t v[2][3];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int r = r0 + 8 * q;
+      if (r < wh) {
+        const T* srow = srcRow(r);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const int c = lane + 32 * k;
+          if (c < ww) v[q][k] = (uint16_t)srow[iclip(x0 - 3 + c, 0, Wc - 1)];
+        }
+      }
     }
-    for (int c = lane; c < ww; c += 32) s_win[r * kWin + c] = (uint16_t)srow[iclip(x0 - 3 + c, 0, Wc - 1)];
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (r0 + 8 * q < wh && lane + 32 * k < ww) s_win[(r0 + 8 * q) * kWin + lane + 32 * k] = v[q][k];
   }
   for (int i = tid; i < 256; i += 256) sm.x_by_xplus1[i] = c_x_by_xplus1[i];
   __syncthreads();
@@ -430,9 +447,24 @@ __device__ __forceinline__ void lrs_block_sum(uint32_t (&v)[N], uint32_t* red) {
 __device__ __forceinline__ void lrs_stage(const LrsArgs& a, LrsSmem& sm, int x0, int y0, int w, int h, bool tables,
                                           bool source) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int r = warp; r < h + 6; r += 8) {
-    const uint8_t* row = a.rec + (int64_t)iclip(y0 - 3 + r, 0, a.H - 1) * a.rstride;
-    for (int c = lane; c < w + 6; c += 32) sm.lr.win[r * kWin + c] = row[iclip(x0 - 3 + c, 0, a.W - 1)];
+  // Six loads in flight per lane, as in lr_tile.
+  for (int r0 = warp; r0 < h + 6; r0 += 16) {
+    uint8_t v[2][3];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int r = r0 + 8 * q;
+      if (r < h + 6) {
+        const uint8_t* row = a.rec + (int64_t)iclip(y0 - 3 + r, 0, a.H - 1) * a.rstride;
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+          if (lane + 32 * k < w + 6) v[q][k] = row[iclip(x0 - 3 + lane + 32 * k, 0, a.W - 1)];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (r0 + 8 * q < h + 6 && lane + 32 * k < w + 6) sm.lr.win[(r0 + 8 * q) * kWin + lane + 32 * k] = v[q][k];
   }
   if (source)
     for (int r = warp; r < h; r += 8) {
