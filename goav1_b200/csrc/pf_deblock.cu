@@ -30,20 +30,32 @@ __device__ __forceinline__ void lpf_unit(T* q, int sa, int sb, int bd, int E, in
   const unsigned twoI = 2u * I, twoF = 2u * F, twoH = 2u * H;
   const int maxPix = (1 << bd) - 1;
   const int diffMin = -128 << bd8, diffMax = (128 << bd8) - 1;
-#pragma unroll 1
+  // The four lines never overlap, so the inner samples of all four (p3..q3
+  // as far as the width reaches) are read before any line is filtered: one
+  // round trip to memory instead of one per line.
+  const int nIn = wd > 6 ? 4 : (wd > 4 ? 3 : 2);
+  int P[4][4], Q[4][4];  // P[i][k] = p_k, Q[i][k] = q_k of line i
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      P[i][k] = k < nIn ? q[i * sa - (k + 1) * sb] : 0;
+      Q[i][k] = k < nIn ? q[i * sa + k * sb] : 0;
+    }
+#pragma unroll
   for (int i = 0; i < 4; i++, q += sa) {
-    const int p1 = q[-2 * sb], p0 = q[-sb], q0 = q[0], q1 = q[sb];
+    const int p1 = P[i][1], p0 = P[i][0], q0 = Q[i][0], q1 = Q[i][1];
     if ((unsigned)(p1 - p0 + I) > twoI || (unsigned)(q1 - q0 + I) > twoI ||
         abs(p0 - q0) * 2 + (abs(p1 - q1) >> 1) > E)
       continue;
     int p2 = 0, q2 = 0, p3 = 0, q3 = 0;
     if (wd > 4) {
-      p2 = q[-3 * sb];
-      q2 = q[2 * sb];
+      p2 = P[i][2];
+      q2 = Q[i][2];
       if ((unsigned)(p2 - p1 + I) > twoI || (unsigned)(q2 - q1 + I) > twoI) continue;
       if (wd > 6) {
-        p3 = q[-4 * sb];
-        q3 = q[3 * sb];
+        p3 = P[i][3];
+        q3 = Q[i][3];
         if ((unsigned)(p3 - p2 + I) > twoI || (unsigned)(q3 - q2 + I) > twoI) continue;
       }
     }
@@ -160,8 +172,11 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
   // Level with the left / above fallback (sb.go:122-128, :142-148).
   const int comp = luma ? dir : plane + 1;
   const int li = r4 * a.mi_cols + c4;
-  int L = __ldg(&a.level_cache[4 * li + comp]);
-  if (L == 0) L = __ldg(&a.level_cache[4 * (dir == 0 ? li - 1 : li - a.mi_cols) + comp]);
+  // Both levels are read together; the neighbour's is used when this
+  // cell's is 0 (c4 > 0 for vertical, r4 > 0 for horizontal edges here).
+  const int L0 = __ldg(&a.level_cache[4 * li + comp]);
+  const int L1 = __ldg(&a.level_cache[4 * (dir == 0 ? li - 1 : li - a.mi_cols) + comp]);
+  const int L = L0 != 0 ? L0 : L1;
   if (L == 0) return;
   // loopfilter/threshold.go:18-47.
   const int sh = a.sharpness;
