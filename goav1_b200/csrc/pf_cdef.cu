@@ -225,6 +225,10 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
       }
       __syncthreads();
       const int secShift = constrain_shift(sec, damping);
+      // The output row base in registers: the plane descriptor sits in the
+      // job table, which the compiler would re-read after every store.
+      uint8_t* const obase = op.ptr;
+      const int64_t ostride = op.stride;
       if (useTab) {
         const uint32_t used = sm.strengths;
         const int ntab = __popc(used);
@@ -267,7 +271,7 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
                                          sm.ofs[dir + 4], sm.ofs[dir], coeffShift);
             }
           }
-          row_ptr<T>(op, unitY + y)[unitX + tx] = (T)v;
+          reinterpret_cast<T*>(obase + (int64_t)(unitY + y) * ostride)[unitX + tx] = (T)v;
         }
       }
       __syncthreads();

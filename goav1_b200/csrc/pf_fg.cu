@@ -182,8 +182,10 @@ __device__ __forceinline__ int blend_w(int prev, int cur, int pw, int cw, int bd
 template <typename T>
 __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& disp, const FgArgs& a, const uint8_t* lut,
                                              int plane, int x, int y0, int nrows) {
-  const DPlane& sp = ref.pl[plane];
-  const DPlane& dp = disp.pl[plane];
+  // Plane descriptors and parameters by value: they live in the job table in
+  // global memory, which the compiler would re-read after every store.
+  const DPlane sp = ref.pl[plane];
+  const DPlane dp = disp.pl[plane];
   if (x >= sp.aw) return;
   const int yend = imin(y0 + nrows, sp.ah);
   if (!a.active[plane] || x >= sp.w) {
@@ -232,6 +234,10 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
     maxV = (plane == 0 ? 235 : (a.matrix_identity ? 235 : 240)) << (bd - 8);
   }
   const int yclip = imin(yend, sp.h);
+  const DPlane lp = ref.pl[0];
+  const bool cfl = a.cfl, oddLuma = a.odd_luma;
+  const int lumaMult = a.luma_mult[plane] - 128, mult = a.mult[plane] - 128;
+  const int offs0 = (a.offset[plane] << (bd - 8)) - (1 << bd);
   for (int y = y0; y < yend; y++) {
     const int s = row_ptr<T>(sp, y)[x];
     if (y >= yclip) {
@@ -252,16 +258,15 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
       idx = s;
     } else {
       // chromaScalingIndex (apply.go:501-520) on the un-grained luma.
-      const DPlane& lp = ref.pl[0];
       const T* lrow = row_ptr<T>(lp, y << sy);
       const int lx = x << sx;
       int avg = lrow[lx];
-      if (sx && !(a.odd_luma && x == sp.w - 1)) avg = (avg + lrow[lx + 1] + 1) >> 1;
-      if (a.cfl) {
+      if (sx && !(oddLuma && x == sp.w - 1)) avg = (avg + lrow[lx + 1] + 1) >> 1;
+      if (cfl) {
         idx = avg;
       } else {
-        const int combined = avg * (a.luma_mult[plane] - 128) + s * (a.mult[plane] - 128);
-        idx = iclip((combined >> 6) + ((a.offset[plane] << (bd - 8)) - (1 << bd)), 0, (1 << bd) - 1);
+        const int combined = avg * lumaMult + s * mult;
+        idx = iclip((combined >> 6) + offs0, 0, (1 << bd) - 1);
       }
     }
     const int scale = scale_lut(lut, idx, bd);
