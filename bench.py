@@ -461,13 +461,15 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = algo[stage_names[dom]] / (per_frame[dom] / 1e3) / 1e9
-    # DRAM bytes (read + write) per frame of each batched kernel from one ncu
-    # capture of a 60-frame launch (profiles/postfilter_kernels_1080p8_60frames_ncu.md),
+    # DRAM bytes (read + write) per frame of each batched kernel from ncu
+    # captures of a 60-frame launch (profiles/postfilter_kernels_1080p8_60frames_ncu.md:
+    # CDEF and restoration from the capture after their staging changes, the
+    # grain apply from its own section, deblocking from the first capture),
     # scaled to this launch's frame count; with the ALU-pipe utilisation of
-    # the same capture, the ceiling that binds.
-    ncu_per_frame = {"deblock": (221.8e6 + 123.1e6 + 206.6e6 + 54.6e6) / 60, "cdef": (188.3e6 + 167.4e6) / 60,
-                     "restoration": (206.9e6 + 156.1e6) / 60, "film_grain": (189.7e6 + 158.9e6) / 60}
-    alu_pct = {"deblock": 27.2, "cdef": 74.0, "restoration": 44.0, "film_grain": 43.0}
+    # the same captures, the ceiling that binds.
+    ncu_per_frame = {"deblock": (221.8e6 + 123.1e6 + 206.6e6 + 54.6e6) / 60, "cdef": (187.1e6 + 167.6e6) / 60,
+                     "restoration": (207.1e6 + 156.5e6) / 60, "film_grain": (189.6e6 + 159.9e6) / 60}
+    alu_pct = {"deblock": 27.2, "cdef": 72.5, "restoration": 50.9, "film_grain": 36.9}
     traffic = ncu_per_frame.get(stage_names[dom])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic * n if traffic else None, "kernel": stage_names[dom],
