@@ -757,7 +757,7 @@ static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, Bytes& hs, 
     int tiles = 0;
     for (int p = 0; p < (f->mono ? 1 : 3); p++) {
       J.fg_tx[p] = (f->plane[p].alloc_width + 63) / 64;
-      J.fg_ty[p] = (f->plane[p].alloc_height + 31) / 32;
+      J.fg_ty[p] = (f->plane[p].alloc_height + 63) / 64;
       tiles += J.fg_tx[p] * J.fg_ty[p];
     }
     counts[ST_FG_APPLY] = tiles;

@@ -136,7 +136,7 @@ struct FrameJob {
   int aw[3], ah[3];          // MI-aligned plane extents
   int db_tx[3], db_ty[3];    // deblock tiles (32x8 edge units) per plane (0 = gated)
   int lr_cols[3], lr_rows[3];  // restoration tiles (processing column x stripe)
-  int fg_tx[3], fg_ty[3];    // 64x32-sample tiles of the display planes
+  int fg_tx[3], fg_ty[3];    // 64x64-sample tiles of the display planes
   int ext_r[3][2], ext_b[3][2];  // extension tiles: right strip, bottom strip
   int do_lr;
 };

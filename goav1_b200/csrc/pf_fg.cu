@@ -310,8 +310,9 @@ __global__ void __launch_bounds__(64) k_fg_offsets_batch(BatchArgs b) {
   });
 }
 
-// Display frame: 64x32-sample tiles of each plane, 256 threads x 8 rows (a
-// thread's rows stay inside one grain block: blocks are 32 or 16 rows high).
+// Display frame: 64x64-sample tiles of each plane, 256 threads x 16 rows (a
+// thread's rows stay inside one grain block: blocks are 32 or 16 rows high,
+// and a thread's per-column set-up is spread over 16 samples).
 // The plane's scaling table is staged in shared memory per tile.
 __global__ void __launch_bounds__(256) k_fg_apply_batch(BatchArgs b) {
   __shared__ uint8_t s_lut[256];
@@ -329,11 +330,11 @@ __global__ void __launch_bounds__(256) k_fg_apply_batch(BatchArgs b) {
     __syncthreads();
     const int tx = local % J.fg_tx[plane], ty = local / J.fg_tx[plane];
     const int x = tx * 64 + (threadIdx.x & 63);
-    const int y0 = ty * 32 + (threadIdx.x >> 6) * 8;
+    const int y0 = ty * 64 + (threadIdx.x >> 6) * 16;
     if (J.io.bd == 8)
-      fg_apply_col<uint8_t>(J.io, J.disp, J.fg, s_lut, plane, x, y0, 8);
+      fg_apply_col<uint8_t>(J.io, J.disp, J.fg, s_lut, plane, x, y0, 16);
     else
-      fg_apply_col<uint16_t>(J.io, J.disp, J.fg, s_lut, plane, x, y0, 8);
+      fg_apply_col<uint16_t>(J.io, J.disp, J.fg, s_lut, plane, x, y0, 16);
     __syncthreads();  // the table is rewritten by the next tile (persistent CTAs)
   });
 }

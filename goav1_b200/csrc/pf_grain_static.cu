@@ -182,7 +182,7 @@ extern "C" int pf_film_grain_static(const pf_frame* ref, const pf_film_grain* fg
   int tiles = 0;
   for (int p = 0; p < (ref->mono ? 1 : 3); p++) {
     J.fg_tx[p] = (ref->plane[p].alloc_width + 63) / 64;
-    J.fg_ty[p] = (ref->plane[p].alloc_height + 31) / 32;
+    J.fg_ty[p] = (ref->plane[p].alloc_height + 63) / 64;
     tiles += J.fg_tx[p] * J.fg_ty[p];
   }
   counts[ST_FG_APPLY] = tiles;
