@@ -168,10 +168,13 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
       __syncthreads();
       // ---- luma direction search on listed blocks (needPrimary) ----
       if (plane == 0 && needPrimary) {
+        // A warp takes one direction for 32 blocks, so the direction's
+        // template runs without divergence.
         for (int w = tid; w < 64 * 8; w += 256) {
-          const int b = w >> 3, d = w & 7;
+          const int d = w >> 6, b = w & 63;
           const int by = b >> 3, bx = b & 7;
-          if ((listed >> b) & 1) s_cost[w] = dir_cost_any(d, &s_in[(2 + by * 8) * kSW + 8 + bx * 8], coeffShift);
+          if ((listed >> b) & 1)
+            s_cost[b * 8 + d] = dir_cost_any(d, &s_in[(2 + by * 8) * kSW + 8 + bx * 8], coeffShift);
         }
         __syncthreads();
         if (tid < 64 && ((listed >> tid) & 1)) {

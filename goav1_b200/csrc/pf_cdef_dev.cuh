@@ -22,7 +22,8 @@ static __constant__ int8_t c_cdef_dir[12][2][2] = {
 __device__ __forceinline__ int dir_off(int e, int k) { return c_cdef_dir[e][k][0] * kSW + c_cdef_dir[e][k][1]; }
 
 // Direction cost of direction D over one 8x8 block (cdef/direction.go:37-79
-// partial sums, :469-501 cost).  blk points at the block's top-left in smem.
+// partial sums, :469-501 cost).  blk points at the block's top-left in smem
+// (16-byte aligned: each row is read as one 16-byte word).
 template <int D>
 __device__ __forceinline__ int32_t dir_cost(const uint16_t* blk, int shift) {
   int32_t p[15];
@@ -30,9 +31,11 @@ __device__ __forceinline__ int32_t dir_cost(const uint16_t* blk, int shift) {
   for (int k = 0; k < 15; k++) p[k] = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
+    const uint4 row = *reinterpret_cast<const uint4*>(blk + i * kSW);
+    const uint32_t rw[4] = {row.x, row.y, row.z, row.w};
 #pragma unroll
     for (int j = 0; j < 8; j++) {
-      const int32_t x = (int32_t)(blk[i * kSW + j] >> shift) - 128;
+      const int32_t x = (int32_t)(((rw[j >> 1] >> (16 * (j & 1))) & 0xffffu) >> shift) - 128;
       if (D == 0) p[i + j] += x;
       if (D == 1) p[i + (j >> 1)] += x;
       if (D == 2) p[i] += x;
