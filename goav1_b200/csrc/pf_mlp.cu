@@ -102,9 +102,11 @@ __global__ void __launch_bounds__(256, 4) k_cdef_features(SearchArgs a, int qind
   }
   __syncthreads();
   // Direction costs of the searched blocks (the search's own arithmetic).
+  // A warp takes one direction for 32 blocks (no divergence between the
+  // eight direction templates).
   for (int wi = tid; wi < 64 * 8; wi += 256) {
-    const int b = wi >> 3, d = wi & 7;
-    if ((listed >> b) & 1) s_cost[wi] = dir_cost8_dev(d, &s_y[(b >> 3) * 8 * 64 + (b & 7) * 8], 64);
+    const int d = wi >> 6, b = wi & 63;
+    if ((listed >> b) & 1) s_cost[b * 8 + d] = dir_cost8_dev(d, &s_y[(b >> 3) * 8 * 64 + (b & 7) * 8], 64);
   }
   __syncthreads();
   if (tid < 64) {

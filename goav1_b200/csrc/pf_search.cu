@@ -136,10 +136,12 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
       }
     } else if (pli == 0) {
       // Luma directions of the listed blocks, from the reconstruction.
+      // A warp takes one direction for 32 blocks (no divergence between
+      // the eight direction templates).
       for (int wi = tid; wi < 64 * 8; wi += 256) {
-        const int b = wi >> 3, d = wi & 7;
+        const int d = wi >> 6, b = wi & 63;
         if ((listed >> b) & 1)
-          s_cost[wi] = dir_cost8_dev(d, row_ptr<uint8_t>(rp, y0 + (b >> 3) * 8) + x0 + (b & 7) * 8, rp.stride);
+          s_cost[b * 8 + d] = dir_cost8_dev(d, row_ptr<uint8_t>(rp, y0 + (b >> 3) * 8) + x0 + (b & 7) * 8, rp.stride);
       }
       __syncthreads();
       if (tid < 64 && ((listed >> tid) & 1)) {
