@@ -172,4 +172,42 @@ __device__ __forceinline__ int cdef_filter_px_tab(const uint16_t* c, int pri, co
   return y;
 }
 
+// cdef_filter_px for 8-bit input that may hold the VeryLarge sentinel, with
+// constrain() read from 513-entry tables: tp / ts point at the entry for a
+// difference of 0, and differences beyond +/-255 (only a sentinel makes one,
+// and at 8-bit strengths <= 15 constrain() is 0 there) clamp to the end
+// entries, which hold 0.  The clamp-range masking is cdef_filter_px's.
+__device__ __forceinline__ int cdef_filter_px_tab8(const uint16_t* c, int pri, const int16_t* tp, int sec,
+                                                   const int16_t* ts, int2 po, int2 s0, int2 s1) {
+  const int x = c[0];
+  auto lut = [](const int16_t* t, int d) { return (int)t[imin(imax(d, -256), 256)]; };
+  int sum = 0;
+  int hi = x, lo = x;
+  constexpr int m = kVeryLarge - 1;
+  if (pri) {
+    const int odd = pri & 1;
+    const int t0 = odd ? 3 : 4, t1 = odd ? 3 : 2;
+    const int a0 = c[po.x], a1 = c[-po.x], a2 = c[po.y], a3 = c[-po.y];
+    sum += t0 * (lut(tp, a0 - x) + lut(tp, a1 - x)) + t1 * (lut(tp, a2 - x) + lut(tp, a3 - x));
+    if (sec) {
+      hi = __vimax3_s32(__vimax3_s32(hi, a0 & m, a1 & m), a2 & m, a3 & m);
+      lo = __vimin3_s32(__vimin3_s32(lo, a0, a1), a2, a3);
+    }
+  }
+  if (sec) {
+    const int b0 = c[s0.x], b1 = c[-s0.x], b2 = c[s1.x], b3 = c[-s1.x];
+    const int b4 = c[s0.y], b5 = c[-s0.y], b6 = c[s1.y], b7 = c[-s1.y];
+    sum += 2 * (lut(ts, b0 - x) + lut(ts, b1 - x) + lut(ts, b2 - x) + lut(ts, b3 - x)) + lut(ts, b4 - x) +
+           lut(ts, b5 - x) + lut(ts, b6 - x) + lut(ts, b7 - x);
+    if (pri) {
+      hi = __vimax3_s32(__vimax3_s32(hi, b0 & m, b1 & m), __vimax3_s32(b2 & m, b3 & m, b4 & m),
+                        __vimax3_s32(b5 & m, b6 & m, b7 & m));
+      lo = __vimin3_s32(__vimin3_s32(lo, b0, b1), __vimin3_s32(b2, b3, b4), __vimin3_s32(b5, b6, b7));
+    }
+  }
+  int y = x + ((8 + sum - (sum < 0)) >> 4);
+  if (pri && sec) y = imin(imax(y, lo), hi);
+  return y;
+}
+
 }  // namespace pf

@@ -47,6 +47,10 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   __shared__ uint32_t s_sse[2][64];  // luma; U+V
   __shared__ uint8_t s_list[2][64];  // tested trials, ascending
   __shared__ int s_cnt[2];
+  // constrain() of the plane's damping: primary strength k at row k (0..15),
+  // secondary strengths 1, 2, 4 at rows 16..18; entry 256 is a difference of
+  // 0, entries 0 and 512 stand for every difference beyond +/-255.
+  __shared__ int16_t s_tab[19][513];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int fb = blockIdx.x;
   const int fbr = fb / a.nhfb, fbc = fb - fbr * a.nhfb;
@@ -163,9 +167,15 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
         s_ai[tid] = (int8_t)ai;
       }
     }
-    __syncthreads();
     const int bl = 3 - dec;
     const int dmp = pli ? damping - 1 : damping;
+    if (pli < 2)  // chroma planes share one damping
+      for (int i = tid; i < 19 * 513; i += 256) {
+        const int t = i / 513, d = i - t * 513 - 256;
+        const int k = t < 16 ? t : (t == 16 ? 1 : (t == 17 ? 2 : 4));
+        s_tab[t][i - t * 513] = (int16_t)(d < -255 || d > 255 ? 0 : constrain(d, k, constrain_shift(k, dmp)));
+      }
+    __syncthreads();
     const int ngrp = (h + 7) >> 3;
     const int ntask = s_cnt[P] * ngrp;
     for (int task = warp; task < ntask; task += 8) {
@@ -175,7 +185,7 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
       const int pri = packed >> 2;
       int sec = packed & 3;
       if (sec == 3) sec = 4;
-      const int secShift = constrain_shift(sec, dmp);
+      const int16_t* ts = &s_tab[sec == 1 ? 16 : (sec == 2 ? 17 : 18)][256];
       uint32_t sse = 0;
       for (int xx = lane; xx < w; xx += 32) {
         for (int yb = grp * 8; yb < imin(grp * 8 + 8, h); yb += 1 << bl) {
@@ -188,7 +198,7 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
           }
           const bool filt = (strength | sec) != 0;
           const int dir = pri != 0 ? s_dir[b] : 0;
-          const int priShift = constrain_shift(strength, dmp);
+          const int16_t* tp = &s_tab[strength][256];
           const int2 po = s_ofs[dir + 2], q0 = s_ofs[dir + 4], q1 = s_ofs[dir];
           for (int yy = yb; yy < yb + (1 << bl); yy++) {
             // An unfiltered block keeps the reconstruction (cdefDist8 against
@@ -198,8 +208,7 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
             if (filt)
               // The 8-bit trial buffer keeps the low byte (cdef/filter_u8.go:151),
               // which matters only below the crop where the centre is VeryLarge.
-              v = (uint8_t)cdef_filter_px(&s_in[(2 + yy) * kSW + 8 + xx], strength, priShift, sec, secShift, po, q0,
-                                          q1, 0);
+              v = (uint8_t)cdef_filter_px_tab8(&s_in[(2 + yy) * kSW + 8 + xx], strength, tp, sec, ts, po, q0, q1);
             const int e = (int)s_src[yy * 64 + xx] - v;
             sse += (uint32_t)(e * e);
           }
