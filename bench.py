@@ -463,13 +463,13 @@ def main():
     achieved = algo[stage_names[dom]] / (per_frame[dom] / 1e3) / 1e9
     # DRAM bytes (read + write) per frame of each batched kernel from ncu
     # captures of a 60-frame launch (profiles/postfilter_kernels_1080p8_60frames_ncu.md:
-    # CDEF and restoration from the capture after their staging changes, the
-    # grain apply from its own section, deblocking from the first capture),
+    # restoration from the capture after its staging change, deblocking, CDEF
+    # and the grain apply from the capture of the current kernels),
     # scaled to this launch's frame count; with the ALU-pipe utilisation of
     # the same captures, the ceiling that binds.
-    ncu_per_frame = {"deblock": (221.8e6 + 123.1e6 + 206.6e6 + 54.6e6) / 60, "cdef": (187.1e6 + 167.6e6) / 60,
-                     "restoration": (207.1e6 + 156.5e6) / 60, "film_grain": (189.6e6 + 159.9e6) / 60}
-    alu_pct = {"deblock": 27.2, "cdef": 72.5, "restoration": 50.9, "film_grain": 36.9}
+    ncu_per_frame = {"deblock": (221.8e6 + 122.2e6 + 206.4e6 + 54.6e6) / 60, "cdef": (187.2e6 + 168.5e6) / 60,
+                     "restoration": (207.1e6 + 156.5e6) / 60, "film_grain": (189.6e6 + 155.8e6) / 60}
+    alu_pct = {"deblock": 53.6, "cdef": 65.2, "restoration": 50.9, "film_grain": 34.5}
     traffic = ncu_per_frame.get(stage_names[dom])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic * n if traffic else None, "kernel": stage_names[dom],
