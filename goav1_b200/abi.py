@@ -322,4 +322,5 @@ EXPORTED_SYMBOLS = (
     "pf_autotune",
     "pf_lr_search",
     "pf_cdef_apply",
+    "pf_superres_upscale",
 )

@@ -1,11 +1,13 @@
 """Generate pf_tables.h: the normative AV1 data tables the post-filter chain needs.
 
-The tables are AV1 spec data (the 2048-entry film-grain Gaussian sequence and
-the self-guided restoration tables).  They must match goav1 value for value,
-so they are parsed straight out of the reference sources:
+The tables are AV1 spec data (the 2048-entry film-grain Gaussian sequence,
+the self-guided restoration tables and the super-resolution upscale filter).
+They must match goav1 value for value, so they are parsed straight out of the
+reference sources:
 
   internal/av1/filmgrain/gaussian.go        gaussianSequence
   internal/av1/restoration/selfguided.go    SGRParameterTable, xByXPlus1, oneByX
+  internal/av1/superres/superres.go         upscaleFilter
 
 Run once where the reference checkout exists; the generated header is
 committed, so builds elsewhere never read the reference.  The film-grain
@@ -53,10 +55,12 @@ def parse(ref):
         params.append((r[0], r[1], s[0], s[1]))
     xby = _ints(_block(sg, r"var xByXPlus1 = \[256\]uint16\{"))
     oneby = _ints(_block(sg, r"var oneByX = \[25\]uint16\{"))
-    return gauss, params, xby, oneby
+    sr = open(os.path.join(ref, "internal/av1/superres/superres.go")).read()
+    upf = _ints(_block(sr, r"var upscaleFilter = \[FilterShifts\]\[FilterTaps\]int16\{"))
+    return gauss, params, xby, oneby, upf
 
 
-def check(gauss, params, xby, oneby):
+def check(gauss, params, xby, oneby, upf):
     assert len(gauss) == 2048, len(gauss)
     s = sum(gauss)
     a = sum(abs(v) for v in gauss)
@@ -64,12 +68,15 @@ def check(gauss, params, xby, oneby):
     if (s, a, w) != (1120, 837192, -8011268):
         raise SystemExit("gaussian checksum mismatch: %r" % ((s, a, w),))
     assert len(params) == 16 and len(xby) == 256 and len(oneby) == 25
+    # 64 phases of 8 taps, each phase summing to 128 (unity gain).
+    assert len(upf) == 64 * 8 and all(sum(upf[8 * i:8 * i + 8]) == 128 for i in range(64))
 
 
-def emit(gauss, params, xby, oneby):
+def emit(gauss, params, xby, oneby, upf):
     out = []
     out.append("/* Generated by gen_tables.py from goav1's normative AV1 tables")
-    out.append(" * (internal/av1/filmgrain/gaussian.go, internal/av1/restoration/selfguided.go).")
+    out.append(" * (internal/av1/filmgrain/gaussian.go, internal/av1/restoration/selfguided.go,")
+    out.append(" * internal/av1/superres/superres.go).")
     out.append(" * Do not edit by hand. */")
     out.append("#ifndef PF_TABLES_H")
     out.append("#define PF_TABLES_H")
@@ -94,6 +101,12 @@ def emit(gauss, params, xby, oneby):
     out.append("")
     out.append("static const uint16_t pf_sgr_one_by_x[25] = {")
     out.append("  " + ", ".join(str(v) for v in oneby) + ",")
+    out.append("};")
+    out.append("")
+    out.append("/* Super-resolution upscale filter: 64 subpel phases x 8 taps. */")
+    out.append("static const int16_t pf_superres_filter[64][8] = {")
+    for i in range(64):
+        out.append("  {" + ", ".join(str(v) for v in upf[8 * i:8 * i + 8]) + "},")
     out.append("};")
     out.append("")
     out.append("#endif /* PF_TABLES_H */")

@@ -169,6 +169,13 @@ class PostFilterRunner:
                                   C.byref(prm), C.byref(result),
                                   fb_index.ctypes.data if fb_index is not None else None))
 
+    def superres_upscale(self, coded, upscaled):
+        """The normative super-resolution upscale (superres.UpscalePlaneCoded,
+        internal/av1/superres/superres.go:40-107) of every plane of `coded`
+        (width = FrameSize.CodedWidth) into `upscaled` (width =
+        FrameSize.UpscaledWidth); pf_frame views, both host or both device."""
+        check(lib().pf_superres_upscale(self._h, C.byref(coded), C.byref(upscaled)))
+
     def lr_search(self, source, recon, restored=None):
         """Encoder loop-restoration unit search on the luma of 8-bit 4:2:0
         frames: SearchWienerUnitU8 and SearchSGRProjUnitU8 per 64x64 unit

@@ -17,6 +17,8 @@
  *                          (cdefSearcher.search) + :886-945 (finish).
  *   - pf_cdef_apply       internal/av1/encoder/cdef_apply.go:202-371
  *                          (cdefApplier.markFromLoopFilterMap + apply).
+ *   - pf_superres_upscale internal/av1/superres/superres.go:40-107 as called
+ *                          from decoder/postfilter_superres.go:206-283.
  *   - pf_lr_search        internal/av1/encoder/restoration.go:149-263
  *                          (SearchWienerUnitU8, SearchSGRProjUnitU8) and the
  *                          unit loops of EncodeLoopRestorationKeyframe,
@@ -99,8 +101,9 @@ typedef struct pf_plane {
 } pf_plane;
 
 /* A frame (frame.Frame, frame/buffer.go:128-141).  width/height are the
- * cropped luma size (FrameSize.CodedWidth x Height; super-res is not
- * supported).  Chroma planes are ((width+ss_x)>>ss_x) x ((height+ss_y)>>ss_y). */
+ * cropped luma size (FrameSize.CodedWidth x Height: the chain filters coded
+ * frames; pf_superres_upscale resamples one to FrameSize.UpscaledWidth).
+ * Chroma planes are ((width+ss_x)>>ss_x) x ((height+ss_y)>>ss_y). */
 typedef struct pf_frame {
   int32_t width;
   int32_t height;
@@ -360,6 +363,22 @@ int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
 int pf_cdef_apply(pf_ctx* ctx, const pf_frame* recon, const uint8_t* noskip,
                   const pf_cdef_search_params* params, const pf_cdef_search_result* result,
                   const uint8_t* fb_index);
+
+/* ---- super-resolution upscale (superres.UpscalePlaneCoded) ----
+ * The normative horizontal upscaler the decoder runs between CDEF and loop
+ * restoration on super-resolved frames (internal/av1/superres/superres.go:
+ * 40-107, called from internal/av1/decoder/postfilter_superres.go:206-283).
+ * For each plane, the coded frame's samples over the MI-aligned span
+ * (((width + 7) & ~7) >> ss_x columns, so the columns past the crop are the
+ * coded buffer's own samples) and the crop height are resampled to the
+ * upscaled plane width with the 8-tap, 64-phase filter; the step and the
+ * initial phase come from the cropped coded width.  coded->width is
+ * FrameSize.CodedWidth, upscaled->width FrameSize.UpscaledWidth (greater);
+ * both frames have the same height, bit depth and chroma layout and are both
+ * host or both device frames.  The cropped upscaled planes are written.
+ * Mismatched frames give PF_ERR_INVALID_FORMAT (frame.ErrInvalidFormat /
+ * ErrInvalidPlane), planes too small for that geometry PF_ERR_SHORT_BUFFER. */
+int pf_superres_upscale(pf_ctx* ctx, const pf_frame* coded, const pf_frame* upscaled);
 
 /* ---- film grain with no allocation ----
  * No counterpart in the reference; this entry point exists for callers that

@@ -62,6 +62,9 @@ def lib():
         _lib.oracle_mlp_loss_grad_f64.argtypes = [C.c_void_p] * 5 + [C.c_int, C.c_void_p, C.c_void_p]
         _lib.oracle_mlp_loss_grad_f64.restype = None
         _lib.oracle_lr_search.argtypes = [C.c_void_p] * 4 + [C.c_int]
+        _lib.oracle_superres_row.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
+        _lib.oracle_superres_row.restype = None
+        _lib.oracle_superres_upscale.argtypes = [C.c_void_p, C.c_void_p]
     return _lib
 
 

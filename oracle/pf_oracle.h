@@ -93,6 +93,12 @@ void oracle_mlp_loss_grad_f64(const double* params, const double* shift, const d
 int oracle_lr_search(const pf_frame* source, const pf_frame* recon, const pf_frame* restored,
                      pf_lr_search_unit* units, int max_units);
 
+/* Super-resolution upscale (oracle/superres_oracle.cpp): one row, and every
+ * plane of a host frame as pf_superres_upscale takes it. */
+void oracle_superres_row(const uint16_t* src, int src_width, int coded_width, uint16_t* dst, int dst_width,
+                         int bit_depth);
+int oracle_superres_upscale(const pf_frame* coded, const pf_frame* upscaled);
+
 #ifdef __cplusplus
 }
 #endif

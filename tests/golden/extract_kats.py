@@ -79,6 +79,22 @@ def main():
     out["wiener"] = {"src": "%s:%d" % (p, lineno(t, m.start())), "default": ints(m.group(1)),
                      "rounds": {int(k): ints(v) for k, v in re.findall(r"(\d+):\s*\{([^}]*)\}", m.group(2))}}
 
+    p = "internal/av1/superres/superres_test.go"
+    t = open(os.path.join(ref, p)).read()
+    m = re.search(r"func TestUpscalePlaneMatchesNormativeRows", t)
+    cases = [{"name": n, "bit_depth": int(b), "src": ints(s_), "dst_width": int(w), "want": ints(wa)}
+             for n, b, s_, w, wa in re.findall(
+                 r"name:\s*\"([^\"]+)\",\s*bitDepth: (\d+),\s*src:\s*\[\]uint16\{([^}]*)\},\s*dstWidth: (\d+),"
+                 r"\s*want:\s*\[\]uint16\{([^}]*)\}", t[m.start():], re.S)]
+    out["superres_rows"] = {"src": "%s:%d" % (p, lineno(t, m.start())), "cases": cases}
+    p = "internal/av1/superres/superres_aligned_libaom_test.go"
+    t = open(os.path.join(ref, p)).read()
+    m = re.search(r"func TestUpscalePlaneCodedMatchesLibaomAlignedRow.*?src := \[\]uint16\{([^}]*)\}.*?want := "
+                  r"\[\]uint16\{([^}]*)\}.*?codedWidth = (\d+).*?alignedWidth = (\d+).*?upscaledWidth = (\d+)", t, re.S)
+    out["superres_libaom_row"] = {"src": "%s:%d" % (p, lineno(t, m.start())), "src_row": ints(m.group(1)),
+                                  "want": ints(m.group(2)), "coded_width": int(m.group(3)),
+                                  "aligned_width": int(m.group(4)), "upscaled_width": int(m.group(5)), "bit_depth": 8}
+
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kats.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)

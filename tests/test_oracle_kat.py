@@ -108,3 +108,32 @@ def test_wiener_default_identity_on_flat(oracle, kats):
         oracle.oracle_wiener(src.ctypes.data + 2 * (3 * stride + 3), stride, dst.ctypes.data, w, w, h,
                              f.ctypes.data, f.ctypes.data, bd)
         assert (dst == 100 << (bd - 8)).all()
+
+
+def test_superres_rows(oracle, kats):
+    """superres_test.go:10-47: the normative rows, 8- and 10-bit."""
+    for case in kats["superres_rows"]["cases"]:
+        src = np.array(case["src"], np.uint16)
+        dst = np.zeros(case["dst_width"], np.uint16)
+        oracle.oracle_superres_row(src.ctypes.data, len(src), len(src), dst.ctypes.data, len(dst), case["bit_depth"])
+        assert list(dst) == case["want"], case["name"]
+
+
+def test_superres_libaom_aligned_row(oracle, kats):
+    """superres_aligned_libaom_test.go:17-51: libaom's row for a coded width of
+    107 read over the 112-column MI-aligned span, upscaled to 160."""
+    r = kats["superres_libaom_row"]
+    src = np.array(r["src_row"], np.uint16)
+    dst = np.zeros(r["upscaled_width"], np.uint16)
+    oracle.oracle_superres_row(src.ctypes.data, r["aligned_width"], r["coded_width"], dst.ctypes.data, len(dst), 8)
+    assert list(dst) == r["want"]
+
+
+def test_superres_constant_rows_stay_constant(oracle):
+    """superres_test.go:49-70: unity-gain phases keep a flat row flat."""
+    for value, bd in ((100, 8), (200, 8), (700, 10), (4095, 12)):
+        src = np.full(16, value, np.uint16)
+        for dw in (17, 20, 32):
+            dst = np.zeros(dw, np.uint16)
+            oracle.oracle_superres_row(src.ctypes.data, 16, 16, dst.ctypes.data, dw, bd)
+            assert (dst == value).all()
