@@ -617,6 +617,35 @@ def main():
                   "ms_per_frame": t_sr * 1e3, "achieved_gbs": sr_bytes / t_sr / 1e9,
                   "config": "8 frames 1280x1080 -> 1920x1080 8-bit 4:2:0 (denominator 12), device-resident, one "
                             "call per frame with its synchronisation, output Mpix/s"}
+        # The whole chain on a super-resolved frame (pf_frame_apply_superres):
+        # the 1080p workload's side information for a coded 1280x1080 frame,
+        # restoration units of the 1920x1080 grid, frames device-resident,
+        # reset from pristine copies outside the timing.
+        import ctypes as _C
+
+        cf, csi = synth.make_frame(1, 2, width=1280, height=1080)
+        uf, usi = synth.make_frame(1, 3, width=1920, height=1080)
+        side = abi.pf_frame_side()
+        _C.memmove(_C.byref(side), _C.byref(csi.side), _C.sizeof(side))
+        side.lr = usi.side.lr
+        dc, du, dd = DeviceFrame(cf), DeviceFrame(uf.like()), DeviceFrame(uf.like())
+        pristine = [t.clone() for t in dc.tensors]
+
+        def sr_chain():
+            for t, t0 in zip(dc.tensors, pristine):
+                t.copy_(t0)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            runner.apply_superres(dc.pf(), side, du.pf(), dd.pf())
+            return time.perf_counter() - t1
+
+        sr_chain()
+        t_chain = statistics.median(sr_chain() for _ in range(max(5, args.steps // 2)))
+        sr_leg["chain"] = {"metric": "super-resolved chain Mpix/s", "value": 1920 * 1080 / t_chain / 1e6,
+                           "unit": "Mpix/s", "ms_per_frame": t_chain * 1e3,
+                           "config": "one 1280x1080 -> 1920x1080 8-bit 4:2:0 frame, full chain (deblock, CDEF, "
+                                     "boundary rows and frame upscaled, restoration, border extension, grain), "
+                                     "device-resident, one call with its synchronisation, upscaled Mpix/s"}
 
     lr_leg = None
     if not args.no_search and rank == 0:

@@ -63,6 +63,8 @@ def lib():
                               C.POINTER(abi.pf_tune_result)]
     L.pf_cdef_apply.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.c_void_p, C.POINTER(abi.pf_cdef_search_params),
                                 C.POINTER(abi.pf_cdef_search_result), C.c_void_p]
+    L.pf_frame_apply_superres.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame_side),
+                                          C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame), C.POINTER(abi.pf_stats)]
     L.pf_superres_upscale.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame)]
     L.pf_lr_search.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame),
                                C.POINTER(abi.pf_frame), C.c_void_p, C.c_int32]

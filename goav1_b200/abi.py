@@ -323,4 +323,5 @@ EXPORTED_SYMBOLS = (
     "pf_lr_search",
     "pf_cdef_apply",
     "pf_superres_upscale",
+    "pf_frame_apply_superres",
 )

@@ -33,6 +33,11 @@ cudaError_t launch_fg_apply_batch(const BatchArgs& b, int total, int grid, cudaS
 cudaError_t launch_extend_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
 cudaError_t lr_upload_tables();
 cudaError_t fg_upload_tables();
+cudaError_t launch_superres_frame(const uint8_t* const* src, const int64_t* sstride, uint8_t* const* dst,
+                                  const int64_t* dstride, const pf_frame* coded, int upW, cudaStream_t st);
+cudaError_t launch_superres_lines(const uint8_t* const* src, const int64_t* sstride, uint8_t* const* lines,
+                                  const int64_t* lstride, const int* nb, const pf_frame* coded, int upW,
+                                  cudaStream_t st);
 }  // namespace pf
 
 using namespace pf;
@@ -99,6 +104,7 @@ struct pf_ctx {
   cudaEvent_t ev[8] = {};
   cudaEvent_t fork = nullptr, join = nullptr;
   DevBuf io, disp;           // staging of host frames
+  DevBuf sr_up, sr_lines;    // super-resolved frames: upscaled staging, upscaled boundary rows
   DevBuf arena;              // per-frame scratch: CDEF output, LR lines, grain, offsets
   DevBuf sidebuf;            // host side information copied up
   DevBuf jobs, bases, counters;
@@ -438,7 +444,8 @@ extern "C" void pf_destroy(pf_ctx* c) {
   cudaStreamSynchronize(c->side);
   if (c->h2d) cudaStreamSynchronize(c->h2d);
   if (c->d2h) cudaStreamSynchronize(c->d2h);
-  DevBuf* bufs[] = {&c->io, &c->disp, &c->arena, &c->sidebuf, &c->jobs, &c->bases, &c->counters, &c->search};
+  DevBuf* bufs[] = {&c->io,   &c->disp,  &c->arena,    &c->sidebuf, &c->jobs,
+                    &c->bases, &c->counters, &c->search, &c->sr_up,   &c->sr_lines};
   for (DevBuf* b : bufs) b->release();
   for (pf_ctx::HostSlot& h : c->hslot) {
     h.io.release();
@@ -488,6 +495,10 @@ struct FrameRef {
   int64_t ioStride[3];
   void* dp[3];
   int64_t dStride[3];
+  // Restoration stripe-boundary rows made elsewhere (a super-resolved frame's
+  // upscaled deblock rows); null: the CDEF pass saves them.
+  uint8_t* ext_lines[3];
+  int64_t ext_line_stride[3];
 };
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -659,9 +670,15 @@ static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, Bytes& hs, 
         if (s->lr.type[p] == PF_LR_NONE) continue;
         const int sy = p ? f->ss_y : 0;
         const int nb = (f->plane[p].height + (8 >> sy)) / (64 >> sy) + 2;
-        a.line_stride[p] = (int64_t)align256((size_t)f->plane[p].width * bps);
-        a.lines[p] = (uint8_t*)arena.take((size_t)nb * 4 * a.line_stride[p]);
-        a.save_lines[p] = 1;
+        if (r.ext_lines[p]) {
+          a.line_stride[p] = r.ext_line_stride[p];
+          a.lines[p] = r.ext_lines[p];
+          a.save_lines[p] = 0;
+        } else {
+          a.line_stride[p] = (int64_t)align256((size_t)f->plane[p].width * bps);
+          a.lines[p] = (uint8_t*)arena.take((size_t)nb * 4 * a.line_stride[p]);
+          a.save_lines[p] = 1;
+        }
         LrArgs& l = J.lr;
         l.type[p] = s->lr.type[p];
         int horz, vert, us;
@@ -1192,6 +1209,143 @@ static int run_host_pipeline(pf_ctx* c, const pf_batch_item* items, int n, pf_st
   CK(cudaStreamSynchronize(c->d2h));
   CK(cudaStreamSynchronize(c->stream));
   read_stage_times(c, stats);
+  CK(cudaGetLastError());
+  return PF_OK;
+}
+
+// A super-resolved frame (FrameSize.SuperResEnabled): the decoder's order,
+// internal/av1/decoder/postfilter.go:336-345 and postfilter_superres.go:
+// deblock and CDEF on the coded frame, the restoration stripe-boundary rows
+// saved from the deblocked coded rows and upscaled
+// (tile/restoration_boundary.go:257-406), the CDEF output upscaled
+// (superres.UpscalePlaneCoded), then restoration, border extension and grain
+// on the upscaled frame.
+extern "C" int pf_frame_apply_superres(pf_ctx* c, const pf_frame* coded, const pf_frame_side* s,
+                                       const pf_frame* up, const pf_frame* display, pf_stats* stats) {
+  if (!c || !coded || !s || !up) return PF_ERR_INVALID_ARG;
+  if (s->stages & ~0x1Fu) return PF_ERR_UNSUPPORTED;
+  if (coded->memory > PF_MEM_DEVICE || up->memory != coded->memory) return PF_ERR_INVALID_ARG;
+  if (up->bit_depth != coded->bit_depth || up->ss_x != coded->ss_x || up->ss_y != coded->ss_y ||
+      up->mono != coded->mono || up->height != coded->height || up->width <= coded->width || up->width > 16384)
+    return PF_ERR_INVALID_FORMAT;
+  pf_frame_side sa = *s, sb = *s;
+  sa.stages = s->stages & (PF_STAGE_LOOP_FILTER | PF_STAGE_CDEF);
+  sb.stages = s->stages & (PF_STAGE_LOOP_RESTORATION | PF_STAGE_EXTEND_BORDERS | PF_STAGE_FILM_GRAIN);
+  const bool wantDisp = (sb.stages & PF_STAGE_FILM_GRAIN) && display;
+  if (wantDisp && display->memory != up->memory) return PF_ERR_INVALID_ARG;
+  int st = pf_frame_validate(coded, &sa, nullptr);
+  if (st == PF_OK) st = pf_frame_validate(up, &sb, display);
+  if (st != PF_OK) return st;
+  CK(cudaSetDevice(c->device));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  const int bps = bps_of(coded);
+  const int nplanes = coded->mono ? 1 : 3;
+  const bool host = coded->memory == PF_MEM_HOST;
+  const cudaStream_t cs = c->stream;
+  void *cio[3] = {}, *uio[3] = {}, *dio[3] = {};
+  int64_t cst[3] = {}, ust[3] = {}, dst3[3] = {};
+  if (host) {
+    CK(layout_like(coded, c->io, cio, cst));
+    CK(layout_like(up, c->sr_up, uio, ust));
+    if (wantDisp) CK(layout_like(display, c->disp, dio, dst3));
+    // Both frames go up: the upscale writes only the upscaled crop, and what
+    // lies around it must come back as the caller left it.
+    for (int p = 0; p < 3; p++) {
+      CK(cudaMemcpy2DAsync(cio[p], cst[p], coded->plane[p].data, coded->plane[p].stride,
+                           (size_t)coded->plane[p].alloc_width * bps, coded->plane[p].alloc_height,
+                           cudaMemcpyHostToDevice, cs));
+      CK(cudaMemcpy2DAsync(uio[p], ust[p], up->plane[p].data, up->plane[p].stride,
+                           (size_t)up->plane[p].alloc_width * bps, up->plane[p].alloc_height,
+                           cudaMemcpyHostToDevice, cs));
+    }
+  } else {
+    for (int p = 0; p < 3; p++) {
+      cio[p] = coded->plane[p].data;
+      cst[p] = coded->plane[p].stride;
+      uio[p] = up->plane[p].data;
+      ust[p] = up->plane[p].stride;
+      if (wantDisp) {
+        dio[p] = display->plane[p].data;
+        dst3[p] = display->plane[p].stride;
+      }
+    }
+  }
+  auto ref_of = [](const pf_frame* f, const pf_frame_side* side, void* const* io, const int64_t* ios) {
+    FrameRef x;
+    memset(&x, 0, sizeof(x));
+    x.f = f;
+    x.s = side;
+    for (int p = 0; p < 3; p++) {
+      x.io[p] = io[p];
+      x.ioStride[p] = ios[p];
+    }
+    return x;
+  };
+  uint32_t done = 0;
+  if (sa.stages & PF_STAGE_LOOP_FILTER) {
+    pf_frame_side s1 = sa;
+    s1.stages = PF_STAGE_LOOP_FILTER;
+    const FrameRef x = ref_of(coded, &s1, cio, cst);
+    if ((st = run_batch(c, &x, 1, nullptr)) != PF_OK) return st;
+    done |= PF_STAGE_LOOP_FILTER;
+  }
+  // The deblocked coded rows around the stripe boundaries, upscaled.
+  uint8_t* lines[3] = {};
+  int64_t lstride[3] = {};
+  if (lr_any(&sb)) {
+    int nb[3] = {};
+    size_t total = 0, off[3] = {};
+    for (int p = 0; p < nplanes; p++) {
+      if (sb.lr.type[p] == PF_LR_NONE) continue;
+      const int sy = p ? up->ss_y : 0;
+      nb[p] = (up->plane[p].height + (8 >> sy)) / (64 >> sy) + 2;
+      lstride[p] = (int64_t)align256((size_t)up->plane[p].width * bps);
+      off[p] = total;
+      total += align256((size_t)nb[p] * 4 * lstride[p]);
+    }
+    CK(c->sr_lines.ensure(total + 256));
+    for (int p = 0; p < nplanes; p++)
+      if (nb[p]) lines[p] = (uint8_t*)c->sr_lines.p + off[p];
+    CK(launch_superres_lines((const uint8_t* const*)cio, cst, lines, lstride, nb, coded, up->width, cs));
+  }
+  if ((sa.stages & PF_STAGE_CDEF) && cdef_any(coded, &sa)) {
+    pf_frame_side s2 = sa;
+    s2.stages = PF_STAGE_CDEF;
+    const FrameRef x = ref_of(coded, &s2, cio, cst);
+    if ((st = run_batch(c, &x, 1, nullptr)) != PF_OK) return st;
+    done |= PF_STAGE_CDEF;
+  }
+  CK(launch_superres_frame((const uint8_t* const*)cio, cst, (uint8_t* const*)uio, ust, coded, up->width, cs));
+  if (sb.stages) {
+    FrameRef x = ref_of(up, &sb, uio, ust);
+    x.display = wantDisp ? display : nullptr;
+    for (int p = 0; p < 3; p++) {
+      x.dp[p] = dio[p];
+      x.dStride[p] = dst3[p];
+      x.ext_lines[p] = lines[p];
+      x.ext_line_stride[p] = lstride[p];
+    }
+    if ((st = run_batch(c, &x, 1, stats)) != PF_OK) return st;
+  }
+  if (host) {
+    auto down = [&](const pf_frame* f, void* const* dev, const int64_t* ds) -> cudaError_t {
+      for (int p = 0; p < nplanes; p++) {
+        const cudaError_t e = cudaMemcpy2DAsync(f->plane[p].data, f->plane[p].stride, dev[p], ds[p],
+                                                (size_t)f->plane[p].alloc_width * bps, f->plane[p].alloc_height,
+                                                cudaMemcpyDeviceToHost, cs);
+        if (e != cudaSuccess) return e;
+      }
+      return cudaSuccess;
+    };
+    CK(down(coded, cio, cst));
+    CK(down(up, uio, ust));
+    if (wantDisp) CK(down(display, dio, dst3));
+  }
+  CK(cudaStreamSynchronize(cs));
+  if (stats) {
+    stats->completed |= done;
+    read_stage_times(c, stats);
+  }
   CK(cudaGetLastError());
   return PF_OK;
 }

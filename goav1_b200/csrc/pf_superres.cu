@@ -40,9 +40,10 @@ struct SrArgs {
 // One output row.  The source row (the MI-aligned span) is staged in shared
 // memory first; each output reads its phase's 8 taps as one 16-byte word.
 template <typename T>
-__device__ __forceinline__ void sr_row(const SrPlane& p, int y, const int16_t (*f)[8], uint16_t* s_row, int maxv) {
-  const T* srow = reinterpret_cast<const T*>(p.src + (int64_t)y * p.sstride);
-  T* drow = reinterpret_cast<T*>(p.dst + (int64_t)y * p.dstride);
+__device__ __forceinline__ void sr_row(const SrPlane& p, const uint8_t* srcRow, uint8_t* dstRow, const int16_t (*f)[8],
+                                       uint16_t* s_row, int maxv) {
+  const T* srow = reinterpret_cast<const T*>(srcRow);
+  T* drow = reinterpret_cast<T*>(dstRow);
   const int last = p.srcWidth - 1;
   for (int x = threadIdx.x; x < p.srcWidth; x += blockDim.x) s_row[x] = srow[x];
   __syncthreads();
@@ -79,10 +80,141 @@ __global__ void __launch_bounds__(256) k_superres(SrArgs a) {
   while (p + 1 < a.nplanes && r >= a.rowBase[p + 1]) p++;
   const int y = r - a.rowBase[p];
   const int maxv = (1 << a.bd) - 1;
+  const SrPlane& q = a.pl[p];
+  const uint8_t* srow = q.src + (int64_t)y * q.sstride;
+  uint8_t* drow = q.dst + (int64_t)y * q.dstride;
   if (a.bd == 8)
-    sr_row<uint8_t>(a.pl[p], y, s_f, s_row, maxv);
+    sr_row<uint8_t>(q, srow, drow, s_f, s_row, maxv);
   else
-    sr_row<uint16_t>(a.pl[p], y, s_f, s_row, maxv);
+    sr_row<uint16_t>(q, srow, drow, s_f, s_row, maxv);
+}
+
+// Restoration stripe-boundary rows of a super-resolved frame
+// (tile/restoration_boundary.go:257-406, SaveRestorationBoundaryLinesFromFramePlaneSuperRes):
+// the deblocked coded rows b-2 .. b+1 around each stripe boundary b are
+// upscaled into the rows the restoration kernel reads (k*4 + j for boundary
+// k; when row b+1 is past the plane, row b stands in for it, as
+// finishRestorationBoundaryLines does).  One CTA per (plane, boundary, row).
+struct SrLinesArgs {
+  SrPlane pl[3];       // src: the deblocked coded plane; dst: the plane's lines, dstride per line
+  int nb[3];           // boundary slots per plane
+  int sh[3], off[3];   // stripe height and offset per plane
+  int nplanes, bd;
+  int16_t filter[64][8];
+};
+
+__global__ void __launch_bounds__(256) k_superres_lines(SrLinesArgs a) {
+  __shared__ __align__(16) int16_t s_f[64][8];
+  extern __shared__ uint16_t s_row[];
+  for (int i = threadIdx.x; i < 64 * 8; i += blockDim.x) s_f[i >> 3][i & 7] = a.filter[i >> 3][i & 7];
+  int r = blockIdx.x, p = 0;
+  while (p + 1 < a.nplanes && r >= a.nb[p] * 4) {
+    r -= a.nb[p] * 4;
+    p++;
+  }
+  const int k = r >> 2, j = r & 3;
+  const SrPlane& q = a.pl[p];
+  const int b = k * a.sh[p] - a.off[p], y = b - 2 + j;
+  // Block-uniform exits, before any barrier.
+  if (k < 1 || b >= q.rows || y >= q.rows) return;
+  const uint8_t* srow = q.src + (int64_t)y * q.sstride;
+  uint8_t* line = q.dst + (int64_t)(k * 4 + j) * q.dstride;
+  const int maxv = (1 << a.bd) - 1;
+  if (a.bd == 8)
+    sr_row<uint8_t>(q, srow, line, s_f, s_row, maxv);
+  else
+    sr_row<uint16_t>(q, srow, line, s_f, s_row, maxv);
+  if (j == 2 && b + 1 >= q.rows) {
+    // The stand-in row: copy what this CTA just wrote.
+    __syncthreads();
+    const int bps = a.bd == 8 ? 1 : 2;
+    for (int x = threadIdx.x; x < q.dstWidth * bps; x += blockDim.x) line[q.dstride + x] = line[x];
+  }
+}
+
+cudaError_t launch_superres_frame(const uint8_t* const* src, const int64_t* sstride, uint8_t* const* dst,
+                                  const int64_t* dstride, const pf_frame* coded, int upW, cudaStream_t st);
+cudaError_t launch_superres_lines(const uint8_t* const* src, const int64_t* sstride, uint8_t* const* lines,
+                                  const int64_t* lstride, const int* nb, const pf_frame* coded, int upW,
+                                  cudaStream_t st);
+
+// Per-plane geometry of an upscale from `coded` (its width the coded width)
+// to a plane width derived from upW.
+static void sr_planes(const pf_frame* coded, int upW, int* cw, int* aw, int* dw, int* rows) {
+  for (int p = 0; p < (coded->mono ? 1 : 3); p++) {
+    const int sx = p ? coded->ss_x : 0, sy = p ? coded->ss_y : 0;
+    cw[p] = (coded->width + sx) >> sx;
+    aw[p] = ((coded->width + 7) & ~7) >> sx;
+    dw[p] = (upW + sx) >> sx;
+    rows[p] = (coded->height + sy) >> sy;
+  }
+}
+
+static void sr_phase_dev(int coded, int dst, int* step, int* x0) {
+  const int s = ((coded << kSrScaleBits) + dst / 2) / dst;
+  const int err = dst * s - (coded << kSrScaleBits);
+  int x = ((-((dst - coded) << (kSrScaleBits - 1))) + dst / 2) / dst;
+  x += (1 << (kSrExtraBits - 1)) - err / 2;
+  *step = s;
+  *x0 = x & ((1 << kSrScaleBits) - 1);
+}
+
+cudaError_t launch_superres_lines(const uint8_t* const* src, const int64_t* sstride, uint8_t* const* lines,
+                                  const int64_t* lstride, const int* nb, const pf_frame* coded, int upW,
+                                  cudaStream_t st) {
+  SrLinesArgs a;
+  memset(&a, 0, sizeof(a));
+  memcpy(a.filter, pf_superres_filter, sizeof(a.filter));
+  int cw[3], aw[3], dw[3], rows[3], total = 0, span = 0;
+  sr_planes(coded, upW, cw, aw, dw, rows);
+  a.nplanes = coded->mono ? 1 : 3;
+  a.bd = coded->bit_depth;
+  for (int p = 0; p < a.nplanes; p++) {
+    SrPlane& q = a.pl[p];
+    sr_phase_dev(cw[p], dw[p], &q.step, &q.x0);
+    q.src = src[p];
+    q.sstride = sstride[p];
+    q.dst = lines[p];
+    q.dstride = lstride[p];
+    q.srcWidth = aw[p];
+    q.dstWidth = dw[p];
+    q.rows = rows[p];
+    const int sy = p ? coded->ss_y : 0;
+    a.sh[p] = 64 >> sy;
+    a.off[p] = 8 >> sy;
+    a.nb[p] = lines[p] ? nb[p] : 0;
+    total += a.nb[p] * 4;
+    span = aw[p] > span ? aw[p] : span;
+  }
+  if (total == 0) return cudaSuccess;
+  k_superres_lines<<<total, 256, (size_t)span * sizeof(uint16_t), st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_superres_frame(const uint8_t* const* src, const int64_t* sstride, uint8_t* const* dst,
+                                  const int64_t* dstride, const pf_frame* coded, int upW, cudaStream_t st) {
+  SrArgs a;
+  memset(&a, 0, sizeof(a));
+  memcpy(a.filter, pf_superres_filter, sizeof(a.filter));
+  int cw[3], aw[3], dw[3], rows[3], span = 0;
+  sr_planes(coded, upW, cw, aw, dw, rows);
+  a.nplanes = coded->mono ? 1 : 3;
+  a.bd = coded->bit_depth;
+  for (int p = 0; p < a.nplanes; p++) {
+    SrPlane& q = a.pl[p];
+    sr_phase_dev(cw[p], dw[p], &q.step, &q.x0);
+    q.src = src[p];
+    q.sstride = sstride[p];
+    q.dst = dst[p];
+    q.dstride = dstride[p];
+    q.srcWidth = aw[p];
+    q.dstWidth = dw[p];
+    q.rows = rows[p];
+    a.rowBase[p + 1] = a.rowBase[p] + rows[p];
+    span = aw[p] > span ? aw[p] : span;
+  }
+  k_superres<<<a.rowBase[a.nplanes], 256, (size_t)span * sizeof(uint16_t), st>>>(a);
+  return cudaGetLastError();
 }
 
 }  // namespace pf

@@ -169,6 +169,16 @@ class PostFilterRunner:
                                   C.byref(prm), C.byref(result),
                                   fb_index.ctypes.data if fb_index is not None else None))
 
+    def apply_superres(self, coded, side, upscaled, display=None):
+        """apply() for a super-resolved frame: deblock and CDEF on `coded`,
+        the upscale, then restoration, border extension and grain on
+        `upscaled` (grain into `display`)."""
+        check(lib().pf_frame_apply_superres(self._h, C.byref(coded), C.byref(side), C.byref(upscaled),
+                                            C.byref(display) if display is not None else None,
+                                            C.byref(self.stats)))
+        self._display = display if (side.stages & abi.PF_STAGE_FILM_GRAIN) else None
+        return self.stats
+
     def superres_upscale(self, coded, upscaled):
         """The normative super-resolution upscale (superres.UpscalePlaneCoded,
         internal/av1/superres/superres.go:40-107) of every plane of `coded`

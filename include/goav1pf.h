@@ -18,7 +18,9 @@
  *   - pf_cdef_apply       internal/av1/encoder/cdef_apply.go:202-371
  *                          (cdefApplier.markFromLoopFilterMap + apply).
  *   - pf_superres_upscale internal/av1/superres/superres.go:40-107 as called
- *                          from decoder/postfilter_superres.go:206-283.
+ *                          from decoder/postfilter_superres.go:206-283;
+ *     pf_frame_apply_superres  the runner's Apply for super-resolved frames
+ *                          (decoder/postfilter.go:336-345 stage order).
  *   - pf_lr_search        internal/av1/encoder/restoration.go:149-263
  *                          (SearchWienerUnitU8, SearchSGRProjUnitU8) and the
  *                          unit loops of EncodeLoopRestorationKeyframe,
@@ -379,6 +381,21 @@ int pf_cdef_apply(pf_ctx* ctx, const pf_frame* recon, const uint8_t* noskip,
  * Mismatched frames give PF_ERR_INVALID_FORMAT (frame.ErrInvalidFormat /
  * ErrInvalidPlane), planes too small for that geometry PF_ERR_SHORT_BUFFER. */
 int pf_superres_upscale(pf_ctx* ctx, const pf_frame* coded, const pf_frame* upscaled);
+
+/* pf_frame_apply for a super-resolved frame (FrameSize.SuperResEnabled): the
+ * decoder's stage order with the upscale between CDEF and restoration
+ * (internal/av1/decoder/postfilter.go:336-345, postfilter_superres.go).
+ * Deblocking and CDEF run on `coded` in place (its width the coded width,
+ * side->lf and side->cdef in its geometry); the restoration stripe-boundary
+ * rows are the deblocked coded rows, upscaled
+ * (tile/restoration_boundary.go:257-406); the CDEF output is upscaled into
+ * `upscaled` (width FrameSize.UpscaledWidth); restoration (side->lr on the
+ * upscaled grid), border extension and grain then run on `upscaled`, grain
+ * into `display` (upscaled geometry).  All frames host or all device; the
+ * same status codes as pf_frame_apply and pf_superres_upscale, returned
+ * before anything is touched.  Returns when the frames are filtered. */
+int pf_frame_apply_superres(pf_ctx* ctx, const pf_frame* coded, const pf_frame_side* side,
+                            const pf_frame* upscaled, const pf_frame* display, pf_stats* stats);
 
 /* ---- film grain with no allocation ----
  * No counterpart in the reference; this entry point exists for callers that

@@ -65,6 +65,7 @@ def lib():
         _lib.oracle_superres_row.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
         _lib.oracle_superres_row.restype = None
         _lib.oracle_superres_upscale.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.oracle_frame_apply_superres.argtypes = [C.c_void_p] * 4
     return _lib
 
 

@@ -653,7 +653,12 @@ struct LRLines {  // tile/restoration_boundary.go:20-31
 
 // tile/restoration_boundary.go:192-255 (SaveRestorationBoundaryLinesFromFramePlaneRows),
 // :454-521 (line saves) and :879-926 (finishRestorationBoundaryLines).
-void lr_save_lines(const pf_frame* fr, int plane, const LRGrid& g, LRLines& lines, bool afterCDEF) {
+// coded != null: a super-resolved frame's deblock save
+// (tile/restoration_boundary.go:257-406): each saved row is the coded frame's
+// row over its MI-aligned span, upscaled to the plane width g.W
+// (superres.UpscalePlaneCoded); fr is then only the geometry.
+void lr_save_lines(const pf_frame* fr, int plane, const LRGrid& g, LRLines& lines, bool afterCDEF,
+                   const pf_frame* coded = nullptr) {
   Plane pl = plane_of(fr, plane);
   const int stripeH = 64 >> g.ssy, off = kLRUnitOffset >> g.ssy;
   const int nStripes = (g.H + off) / stripeH + 2;
@@ -675,6 +680,14 @@ void lr_save_lines(const pf_frame* fr, int plane, const LRGrid& g, LRLines& line
   };
   auto save_row = [&](std::vector<uint16_t>& buf, int stripe, int ctxRow, int srcRow) {
     uint16_t* line = &buf[(size_t)(stripe * kLRCtxVert + ctxRow) * lines.stride];
+    if (coded) {
+      Plane cp = plane_of(coded, plane);
+      const int cw = (coded->width + g.ssx) >> g.ssx, aw = ((coded->width + 7) & ~7) >> g.ssx;
+      std::vector<uint16_t> row(aw);
+      for (int x = 0; x < aw; x++) row[x] = (uint16_t)cp.get(x, srcRow);
+      oracle_superres_row(row.data(), aw, cw, line + kLRExtraHorz, g.W, coded->bit_depth);
+      return;
+    }
     for (int x = 0; x < g.W; x++) line[kLRExtraHorz + x] = (uint16_t)pl.get(x, srcRow);
   };
   for (int s = 0;; s++) {
@@ -1310,6 +1323,42 @@ extern "C" int oracle_frame_apply(const pf_frame* fr, const pf_frame_side* side,
   if (side->stages & PF_STAGE_EXTEND_BORDERS) extend_borders(fr);
   if (side->stages & PF_STAGE_FILM_GRAIN) {
     if ((st = do_film_grain(fr, side->fg, disp)) != PF_OK) return st;
+  }
+  return PF_OK;
+}
+
+// The decoder's order for a super-resolved frame (decoder/postfilter.go:
+// 336-345, postfilter_superres.go:206-283): deblock, the deblock-row save
+// (upscaled), CDEF on the coded frame; the upscale; restoration, border
+// extension and grain on the upscaled frame.
+extern "C" int oracle_frame_apply_superres(const pf_frame* coded, const pf_frame_side* side, const pf_frame* up,
+                                           const pf_frame* disp) {
+  if (!coded || !side || !up) return PF_ERR_INVALID_ARG;
+  int st;
+  LRLines lines[3];
+  const bool lr = (side->stages & PF_STAGE_LOOP_RESTORATION) != 0;
+  if (side->stages & PF_STAGE_LOOP_FILTER) {
+    if ((st = do_loop_filter(coded, side)) != PF_OK) return st;
+  }
+  if (lr)
+    for (int p = 0; p < (up->mono ? 1 : 3); p++) {
+      LRGrid g = lr_grid(up, side->lr, p);
+      if (g.type != PF_LR_NONE) lr_save_lines(up, p, g, lines[p], false, coded);
+    }
+  if (side->stages & PF_STAGE_CDEF) {
+    if ((st = do_cdef(coded, side, nullptr)) != PF_OK) return st;
+  }
+  if ((st = oracle_superres_upscale(coded, up)) != PF_OK) return st;
+  if (lr) {
+    for (int p = 0; p < (up->mono ? 1 : 3); p++) {
+      LRGrid g = lr_grid(up, side->lr, p);
+      if (g.type != PF_LR_NONE) lr_save_lines(up, p, g, lines[p], true);
+    }
+    if ((st = do_loop_restoration(up, side, lines, nullptr)) != PF_OK) return st;
+  }
+  if (side->stages & PF_STAGE_EXTEND_BORDERS) extend_borders(up);
+  if (side->stages & PF_STAGE_FILM_GRAIN) {
+    if ((st = do_film_grain(up, side->fg, disp)) != PF_OK) return st;
   }
   return PF_OK;
 }

@@ -98,6 +98,9 @@ int oracle_lr_search(const pf_frame* source, const pf_frame* recon, const pf_fra
 void oracle_superres_row(const uint16_t* src, int src_width, int coded_width, uint16_t* dst, int dst_width,
                          int bit_depth);
 int oracle_superres_upscale(const pf_frame* coded, const pf_frame* upscaled);
+/* The chain on a super-resolved frame (see pf_frame_apply_superres). */
+int oracle_frame_apply_superres(const pf_frame* coded, const pf_frame_side* side, const pf_frame* upscaled,
+                                const pf_frame* display);
 
 #ifdef __cplusplus
 }
