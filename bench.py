@@ -647,6 +647,55 @@ def main():
                                      "boundary rows and frame upscaled, restoration, border extension, grain), "
                                      "device-resident, one call with its synchronisation, upscaled Mpix/s"}
 
+    # Deblocking masks and level cache from the block record map
+    # (pf_lf_build): 8 random 1080p maps (480x270 MI cells, 128x128
+    # superblocks, 4:2:0, segmentation + delta-lf + mode/ref deltas on).
+    # Device: records and outputs resident in HBM, one call per map with its
+    # synchronisation (the call returns the walk's status), median over the
+    # calls.  Host: records uploaded and outputs read back inside the call.
+    # The oracle (one host thread) on the same maps is reported beside it.
+    lf_leg = None
+    if not args.no_search and rank == 0:
+        from goav1_b200 import synth
+
+        maps = [synth.make_lf_map(100 + i, 480, 270) for i in range(8)]
+        lvs = [synth.make_lf_levels(100 + i, "deltas") for i in range(8)]
+        dev = [torch.from_numpy(m.view(np.uint8).reshape(270, 480, 32).copy()).cuda() for m, _ in maps]
+        outs = [runner.lf_build(d, lv) for d, lv in zip(dev, lvs)]
+        torch.cuda.synchronize()
+        reps = max(5, args.steps // 2)
+        t_dev = statistics.median(call_median(lambda d=d, lv=lv, o=o: runner.lf_build(d, lv, masks=o[0],
+                                                                                      level_cache=o[1]), reps)
+                                  for d, lv, o in zip(dev, lvs, outs))
+        t_host = statistics.median(call_median(lambda m=m, lv=lv: runner.lf_build(m, lv), reps)
+                                   for (m, _), lv in zip(maps, lvs))
+        cells = 480 * 270
+        lf_bytes = cells * (32 + 4) + 15 * 9 * abi.PF_LF_MASK_WORDS * 2
+        lf_leg = {"metric": "lf mask build Mcells/s", "value": cells / t_dev / 1e6, "unit": "Mcells/s",
+                  "ms_per_frame": t_dev * 1e3, "host_ms_per_frame": t_host * 1e3,
+                  "algorithmic_bytes_per_frame": lf_bytes,
+                  "config": "8 block record maps of 1920x1080 (480x270 MI cells, make_lf_map seeds 100-107), "
+                            "4:2:0, 128x128 superblocks, segmentation/delta-lf/mode-ref deltas on; device-resident "
+                            "records and outputs, one call per map with its synchronisation; host_ms_per_frame: "
+                            "host records and outputs copied inside the call"}
+        if world == 1 and not args.no_cpu:
+            import ctypes as _C
+
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle_ctypes
+
+            olib = oracle_ctypes.lib()
+            om = np.zeros((15 * 9, abi.PF_LF_MASK_WORDS), np.uint16)
+            ol = np.zeros((270, 480, 4), np.uint8)
+            ts = []
+            for (m, _), lv in zip(maps, lvs):
+                t0 = time.perf_counter()
+                olib.oracle_lf_build(m.ctypes.data, 480, 270, _C.byref(lv), 1, 1, 0, om.ctypes.data, ol.ctypes.data)
+                ts.append(time.perf_counter() - t0)
+            lf_leg["cpu_baseline"] = {"value": cells / statistics.median(ts) / 1e6, "unit": "Mcells/s", "cores": 1,
+                                      "kind": "port", "ms_per_frame": statistics.median(ts) * 1e3,
+                                      "sample": "the same 8 maps, oracle_lf_build, one host thread"}
+
     lr_leg = None
     if not args.no_search and rank == 0:
         from goav1_b200 import synth
@@ -691,7 +740,7 @@ def main():
                            "l2": "inputs (%.0f MB per rank) larger than L2, and a 256 MB L2 flush between steps"
                                  % (sum(fr.nbytes() for fr, _ in frames) / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "cdef_search": search,
-                "cdef_search_learned": learned_leg, "lr_search": lr_leg, "superres": sr_leg, "mixed_batch": mixed,
+                "cdef_search_learned": learned_leg, "lr_search": lr_leg, "superres": sr_leg, "lf_build": lf_leg, "mixed_batch": mixed,
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))
     runner.close()

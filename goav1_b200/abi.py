@@ -19,6 +19,7 @@ PF_ERR_INVALID_ARG = -7
 PF_ERR_DEVICE = -8
 PF_ERR_TIMEOUT = -9
 PF_ERR_NO_DEVICE = -10
+PF_ERR_INVALID_BATCH = -11
 
 PF_STAGE_LOOP_FILTER = 1 << 0
 PF_STAGE_CDEF = 1 << 1
@@ -298,6 +299,67 @@ def lr_unit_grid(width, height):
     return max((width + 32) // 64, 1), max((height + 32) // 64, 1)
 
 
+class pf_lf_record(C.Structure):
+    """threading.FrameWorkLoopFilterBlockRecord, one per MI cell (32 bytes)."""
+    _fields_ = [
+        ("mi_col", C.c_uint16),
+        ("mi_row", C.c_uint16),
+        ("mi_col_end", C.c_uint16),
+        ("mi_row_end", C.c_uint16),
+        ("block_size", C.c_uint8),
+        ("valid", C.c_uint8),
+        ("intra", C.c_uint8),
+        ("skip", C.c_uint8),
+        ("tx_y", C.c_uint8),
+        ("tx_uv", C.c_uint8),
+        ("has_uv", C.c_uint8),
+        ("segment_id", C.c_uint8),
+        ("ref_frame", C.c_uint8),
+        ("mode", C.c_uint8),
+        ("delta_lf_from_base", C.c_int8),
+        ("delta_lf", C.c_int8 * 4),
+        ("reserved0", C.c_uint8),
+        ("tx_split", C.c_uint16 * 2),
+        ("reserved1", C.c_uint32),
+    ]
+
+
+# The same record as a numpy dtype (record maps are built as arrays).
+LF_RECORD_DTYPE = None
+
+
+def lf_record_dtype():
+    import numpy as np
+
+    global LF_RECORD_DTYPE
+    if LF_RECORD_DTYPE is None:
+        LF_RECORD_DTYPE = np.dtype([
+            ("mi_col", "<u2"), ("mi_row", "<u2"), ("mi_col_end", "<u2"), ("mi_row_end", "<u2"),
+            ("block_size", "u1"), ("valid", "u1"), ("intra", "u1"), ("skip", "u1"), ("tx_y", "u1"),
+            ("tx_uv", "u1"), ("has_uv", "u1"), ("segment_id", "u1"), ("ref_frame", "u1"), ("mode", "u1"),
+            ("delta_lf_from_base", "i1"), ("delta_lf", "i1", (4,)), ("reserved0", "u1"),
+            ("tx_split", "<u2", (2,)), ("reserved1", "<u4")])
+        assert LF_RECORD_DTYPE.itemsize == C.sizeof(pf_lf_record) == 32
+    return LF_RECORD_DTYPE
+
+
+class pf_lf_levels(C.Structure):
+    """loopfilter.PrepareLevelResolver inputs."""
+    _fields_ = [
+        ("level_y", C.c_uint8 * 2),
+        ("level_u", C.c_uint8),
+        ("level_v", C.c_uint8),
+        ("delta_lf_present", C.c_uint8),
+        ("delta_lf_multi", C.c_uint8),
+        ("segmentation_enabled", C.c_uint8),
+        ("mode_ref_delta_enabled", C.c_uint8),
+        ("ref_delta", C.c_int8 * 8),
+        ("mode_delta", C.c_int8 * 2),
+        ("reserved", C.c_uint8 * 2),
+        ("segment_delta", (C.c_int16 * 4) * 8),
+    ]
+
+
 # Every symbol include/goav1pf.h declares (checked by tests/test_abi.py).
 EXPORTED_SYMBOLS = (
     "pf_abi_version",
@@ -324,4 +386,5 @@ EXPORTED_SYMBOLS = (
     "pf_cdef_apply",
     "pf_superres_upscale",
     "pf_frame_apply_superres",
+    "pf_lf_build",
 )

@@ -8,6 +8,9 @@ reference sources:
   internal/av1/filmgrain/gaussian.go        gaussianSequence
   internal/av1/restoration/selfguided.go    SGRParameterTable, xByXPlus1, oneByX
   internal/av1/superres/superres.go         upscaleFilter
+  internal/av1/tile/partition.go            blockDimensions
+  internal/av1/tile/tx_size.go              transformDimensions,
+                                            maxTransformSizeForBlock
 
 Run once where the reference checkout exists; the generated header is
 committed, so builds elsewhere never read the reference.  The film-grain
@@ -57,10 +60,30 @@ def parse(ref):
     oneby = _ints(_block(sg, r"var oneByX = \[25\]uint16\{"))
     sr = open(os.path.join(ref, "internal/av1/superres/superres.go")).read()
     upf = _ints(_block(sr, r"var upscaleFilter = \[FilterShifts\]\[FilterTaps\]int16\{"))
-    return gauss, params, xby, oneby, upf
+    tile = open(os.path.join(ref, "internal/av1/tile/partition.go")).read()
+    bdim = re.findall(r"BlockSize(\d+)x(\d+):\s*\{W4: (\d+), H4: (\d+), Log2W: (\d+), Log2H: (\d+)\}",
+                      _block(tile, r"var blockDimensions = \[blockSizeCount\]BlockDimensions\{"))
+    txf = open(os.path.join(ref, "internal/av1/tile/tx_size.go")).read()
+    consts = re.search(r"\tTransformSize4x4 TransformSize = iota\n(.*?)\ttransformSizeCount", txf, re.S).group(1)
+    order = ["TransformSize4x4"] + re.findall(r"^\t(TransformSize\d+x\d+)$", consts, re.M)
+    tdim = {}
+    for m in re.finditer(r"(TransformSize\d+x\d+):\s*\{([^}]*)\}",
+                         _block(txf, r"var transformDimensions = \[transformSizeCount\]TransformDimensions\{")):
+        f = dict(kv.split(":") for kv in m.group(2).replace(" ", "").split(","))
+        tdim[m.group(1)] = (int(f["W4"]), int(f["H4"]), int(f["Log2W"]), int(f["Log2H"]), f.get("Sub"))
+    tx = []
+    for name in order:
+        w4, h4, lw, lh, sub = tdim[name]
+        tx.append((w4, h4, lw, lh, order.index(sub) if sub else 0))
+    maxtx = []
+    for m in re.finditer(r"BlockSize(\d+)x(\d+):\s*\{([^}]*)\}",
+                         _block(txf, r"var maxTransformSizeForBlock = \[blockSizeCount\]\[4\]TransformSize\{")):
+        maxtx.append([order.index(v.strip()) for v in m.group(3).split(",")])
+    blocks = [tuple(int(v) for v in b[2:]) + (int(b[0]), int(b[1])) for b in bdim]
+    return gauss, params, xby, oneby, upf, blocks, tx, maxtx
 
 
-def check(gauss, params, xby, oneby, upf):
+def check(gauss, params, xby, oneby, upf, blocks, tx, maxtx):
     assert len(gauss) == 2048, len(gauss)
     s = sum(gauss)
     a = sum(abs(v) for v in gauss)
@@ -70,13 +93,25 @@ def check(gauss, params, xby, oneby, upf):
     assert len(params) == 16 and len(xby) == 256 and len(oneby) == 25
     # 64 phases of 8 taps, each phase summing to 128 (unity gain).
     assert len(upf) == 64 * 8 and all(sum(upf[8 * i:8 * i + 8]) == 128 for i in range(64))
+    # 22 block sizes and 19 transform sizes, each with its width and height in
+    # 4x4 units consistent with its name and log2 classes.
+    assert len(blocks) == 22 and len(tx) == 19 and len(maxtx) == 22
+    for w4, h4, lw, lh, pw, ph in blocks:
+        assert w4 * 4 == pw and h4 * 4 == ph and 1 << lw == w4 and 1 << lh == h4
+    for i, (w4, h4, lw, lh, sub) in enumerate(tx):
+        assert 1 << lw == w4 and 1 << lh == h4 and 0 <= sub < 19
+        # A split quarters a square transform and halves a rectangular one.
+        if i:
+            assert tx[sub][0] * tx[sub][1] * (4 if w4 == h4 else 2) == w4 * h4
+    assert all(len(r) == 4 and all(0 <= v < 19 for v in r) for r in maxtx)
 
 
-def emit(gauss, params, xby, oneby, upf):
+def emit(gauss, params, xby, oneby, upf, blocks, tx, maxtx):
     out = []
     out.append("/* Generated by gen_tables.py from goav1's normative AV1 tables")
     out.append(" * (internal/av1/filmgrain/gaussian.go, internal/av1/restoration/selfguided.go,")
-    out.append(" * internal/av1/superres/superres.go).")
+    out.append(" * internal/av1/superres/superres.go, internal/av1/tile/partition.go,")
+    out.append(" * internal/av1/tile/tx_size.go).")
     out.append(" * Do not edit by hand. */")
     out.append("#ifndef PF_TABLES_H")
     out.append("#define PF_TABLES_H")
@@ -107,6 +142,24 @@ def emit(gauss, params, xby, oneby, upf):
     out.append("static const int16_t pf_superres_filter[64][8] = {")
     for i in range(64):
         out.append("  {" + ", ".join(str(v) for v in upf[8 * i:8 * i + 8]) + "},")
+    out.append("};")
+    out.append("")
+    out.append("/* Block sizes in goav1's tile.BlockSize order: {W4, H4} in 4x4 units. */")
+    out.append("static const uint8_t pf_block_dims[22][2] = {")
+    for b in blocks:
+        out.append("  {%d, %d}," % b[:2])
+    out.append("};")
+    out.append("")
+    out.append("/* Transform sizes in tile.TransformSize order: {W4, H4, Log2W, Log2H, Sub}. */")
+    out.append("static const uint8_t pf_tx_dims[19][5] = {")
+    for t in tx:
+        out.append("  {%d, %d, %d, %d, %d}," % t)
+    out.append("};")
+    out.append("")
+    out.append("/* Largest transform per block size: luma, 4:2:0, 4:2:2, 4:4:4 chroma. */")
+    out.append("static const uint8_t pf_max_tx[22][4] = {")
+    for r in maxtx:
+        out.append("  {%d, %d, %d, %d}," % tuple(r))
     out.append("};")
     out.append("")
     out.append("#endif /* PF_TABLES_H */")

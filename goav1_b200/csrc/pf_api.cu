@@ -399,6 +399,7 @@ extern "C" const char* pf_status_string(int s) {
     case PF_ERR_DEVICE: return "CUDA error";
     case PF_ERR_TIMEOUT: return "device wait timed out";
     case PF_ERR_NO_DEVICE: return "no usable CUDA device";
+    case PF_ERR_INVALID_BATCH: return "threading: invalid batch";
     default: return "unknown status";
   }
 }

@@ -64,9 +64,13 @@ class ErrNoDevice(PostFilterError):
     code = abi.PF_ERR_NO_DEVICE
 
 
+class ErrInvalidBatch(PostFilterError):
+    code = abi.PF_ERR_INVALID_BATCH
+
+
 _ERRORS = {cls.code: cls for cls in (ErrInvalidCDEF, ErrInvalidFilter, ErrInvalidPlan, ErrUnsupportedPostFilter,
                                      ErrShortBuffer, ErrInvalidFormat, ErrInvalidArgument, ErrDevice, ErrTimeout,
-                                     ErrNoDevice)}
+                                     ErrNoDevice, ErrInvalidBatch)}
 
 
 def check(status):
@@ -185,6 +189,42 @@ class PostFilterRunner:
         (width = FrameSize.CodedWidth) into `upscaled` (width =
         FrameSize.UpscaledWidth); pf_frame views, both host or both device."""
         check(lib().pf_superres_upscale(self._h, C.byref(coded), C.byref(upscaled)))
+
+    def lf_build(self, records, levels, ss_x=1, ss_y=1, mono=False, masks=None, level_cache=None):
+        """Deblocking edge masks and level cache from the block record map:
+        FrameWorkLoopFilterMasks.BuildFromMap
+        (internal/av1/threading/loop_filter_masks.go:450-680) and
+        populateLoopFilterLevelCacheFromMap
+        (decoder/postfilter_loopfilter_masks.go:119-228), on the GPU.
+
+        records: the map, a uint8/record array of shape (mi_rows, mi_cols)
+        with dtype abi.lf_record_dtype(), or a torch CUDA tensor of shape
+        (mi_rows, mi_cols, 32) uint8 (device resident).  levels: pf_lf_levels.
+        With host records the outputs are numpy arrays (masks uint16
+        [sb128_h*sb128_w, 640], level_cache uint8 [mi_rows, mi_cols, 4]);
+        with device records they are torch CUDA tensors of those shapes
+        (or the given `masks` / `level_cache` tensors)."""
+        if hasattr(records, "data_ptr"):
+            import torch
+
+            rows, cols = records.shape[0], records.shape[1]
+            sbw, sbh = (cols + 31) // 32, (rows + 31) // 32
+            if masks is None:
+                masks = torch.empty((sbh * sbw, abi.PF_LF_MASK_WORDS), dtype=torch.int16, device=records.device)
+            if level_cache is None:
+                level_cache = torch.empty((rows, cols, 4), dtype=torch.uint8, device=records.device)
+            check(lib().pf_lf_build(self._h, records.data_ptr(), cols, rows, abi.PF_MEM_DEVICE, C.byref(levels),
+                                    ss_x, ss_y, int(mono), masks.data_ptr(), level_cache.data_ptr(),
+                                    abi.PF_MEM_DEVICE))
+            return masks, level_cache
+        rec = np.ascontiguousarray(records)
+        rows, cols = rec.shape
+        sbw, sbh = (cols + 31) // 32, (rows + 31) // 32
+        masks = np.empty((sbh * sbw, abi.PF_LF_MASK_WORDS), np.uint16)
+        level_cache = np.empty((rows, cols, 4), np.uint8)
+        check(lib().pf_lf_build(self._h, rec.ctypes.data, cols, rows, abi.PF_MEM_HOST, C.byref(levels), ss_x, ss_y,
+                                int(mono), masks.ctypes.data, level_cache.ctypes.data, abi.PF_MEM_HOST))
+        return masks, level_cache
 
     def lr_search(self, source, recon, restored=None):
         """Encoder loop-restoration unit search on the luma of 8-bit 4:2:0

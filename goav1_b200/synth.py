@@ -539,3 +539,149 @@ def make_lr_search_pair(seed, width=1920, height=1080, sigma=None):
             elif u < 0.1875:
                 r[:] = s
     return src, rec, sig
+
+
+# ---------------------------------------------------------------------------
+# Block record maps (threading.FrameWorkLoopFilterMap)
+
+_TABLES = None
+
+
+def av1_tables():
+    """(block_dims[22][2], tx_dims[19][5], max_tx[22][4]) from the generated
+    pf_tables.h: goav1's tile.BlockSize / TransformSize tables."""
+    global _TABLES
+    if _TABLES is None:
+        import os
+        import re
+
+        text = open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "pf_tables.h")).read()
+
+        def grab(name, cols):
+            body = re.search(name + r"\[[^\]]*\]\[\d+\] = \{(.*?)\n\};", text, re.S).group(1)
+            vals = [int(v) for v in re.findall(r"\d+", body)]
+            return [tuple(vals[i:i + cols]) for i in range(0, len(vals), cols)]
+
+        _TABLES = (grab("pf_block_dims", 2), grab("pf_tx_dims", 5), grab("pf_max_tx", 4))
+    return _TABLES
+
+
+# AV1 partitions of a square block of n 4x4 units, as (x, y, w, h) children
+# in decode order; "split" recurses into the four quadrants.
+def _partition_children(kind, n):
+    h = n // 2
+    q = n // 4
+    return {
+        "none": [(0, 0, n, n)],
+        "horz": [(0, 0, n, h), (0, h, n, h)],
+        "vert": [(0, 0, h, n), (h, 0, h, n)],
+        "horz_a": [(0, 0, h, h), (h, 0, h, h), (0, h, n, h)],
+        "horz_b": [(0, 0, n, h), (0, h, h, h), (h, h, h, h)],
+        "vert_a": [(0, 0, h, h), (0, h, h, h), (h, 0, h, n)],
+        "vert_b": [(0, 0, h, n), (h, 0, h, h), (h, h, h, h)],
+        "horz_4": [(0, i * q, n, q) for i in range(4)],
+        "vert_4": [(i * q, 0, q, n) for i in range(4)],
+    }[kind]
+
+
+def make_lf_map(seed, mi_cols, mi_rows, ss=(1, 1), mono=False, sb128=True, p_intra=0.3, p_skip=0.3, p_split=0.5,
+                p_vartx=0.6):
+    """A decoded block record map (threading.FrameWorkLoopFilterMap,
+    threading/loop_filter_map.go:46-72) for an mi_cols x mi_rows grid: each
+    64x64 or 128x128 superblock partitioned at random with AV1's partition
+    types (frame-edge blocks forced to split or halve as AV1 does), each
+    block intra (transform size reduced 0-2 steps) or inter (skip, or a
+    random var-tx split tree), its chroma transform the largest for the
+    layout (tile/tx_size.go:109-132), random segment, reference frame, mode
+    class and delta-lf values.  Returns (records[mi_rows, mi_cols] of
+    abi.lf_record_dtype(), decode-order origin cell indices)."""
+    bdims, txd, maxtx = av1_tables()
+    size_of = {d: i for i, d in enumerate(bdims)}
+    layout_col = 3 if ss[0] == 0 else (1 if ss[1] else 2)
+    rng = np.random.default_rng([seed, mi_cols, mi_rows, 0x1F3A])
+    rec = np.zeros((mi_rows, mi_cols), abi.lf_record_dtype())
+    order = []
+
+    def emit(x, y, w, h):
+        if x >= mi_cols or y >= mi_rows:
+            return
+        bs = size_of[(w, h)]
+        intra = rng.random() < p_intra
+        skip = (not intra) and rng.random() < p_skip
+        tx = maxtx[bs][0]
+        split = (0, 0)
+        if intra:
+            for _ in range(int(rng.integers(0, 3))):
+                tx = txd[tx][4] if tx else tx
+        elif not skip and tx and rng.random() < p_vartx:
+            split = (int(rng.integers(1, 1 << 16)), int(rng.integers(0, 1 << 16)))
+        x1, y1 = min(x + w, mi_cols), min(y + h, mi_rows)
+        r = rec[y:y1, x:x1]
+        r["mi_col"], r["mi_row"], r["mi_col_end"], r["mi_row_end"] = x, y, x1, y1
+        r["block_size"], r["valid"], r["intra"], r["skip"] = bs, 1, intra, skip
+        r["tx_y"], r["tx_uv"], r["has_uv"] = tx, maxtx[bs][layout_col], 0 if mono else 1
+        r["segment_id"] = rng.integers(0, 8)
+        r["ref_frame"] = 0 if intra else rng.integers(1, 8)
+        r["mode"] = 0 if intra else rng.integers(0, 2)
+        r["delta_lf_from_base"] = rng.integers(-12, 13)
+        r["delta_lf"] = rng.integers(-12, 13, size=4)
+        r["tx_split"] = split
+        order.append(y * mi_cols + x)
+
+    def part(x, y, n):
+        if x >= mi_cols or y >= mi_rows:
+            return
+        has_rows, has_cols = y + n // 2 < mi_rows, x + n // 2 < mi_cols
+        if n == 1:
+            emit(x, y, 1, 1)
+            return
+        if has_rows and has_cols:
+            kinds = ["none", "horz", "vert", "split"]
+            if n > 2:
+                kinds += ["horz_a", "horz_b", "vert_a", "vert_b"]
+            if 2 < n < 32:
+                kinds += ["horz_4", "vert_4"]
+            kind = "split" if rng.random() < p_split and n > 2 else kinds[int(rng.integers(0, len(kinds)))]
+        elif has_cols:
+            kind = "horz" if rng.random() < 0.5 and n > 2 else "split"
+        elif has_rows:
+            kind = "vert" if rng.random() < 0.5 and n > 2 else "split"
+        else:
+            kind = "split"
+        if kind == "split":
+            h = n // 2
+            for dy in (0, h):
+                for dx in (0, h):
+                    part(x + dx, y + dy, h)
+            return
+        for cx, cy, w, hh in _partition_children(kind, n):
+            emit(x + cx, y + cy, w, hh)
+
+    sb = 32 if sb128 else 16
+    for y in range(0, mi_rows, sb):
+        for x in range(0, mi_cols, sb):
+            part(x, y, sb)
+    return rec, np.array(order, np.int32)
+
+
+def make_lf_levels(seed, mode="plain"):
+    """pf_lf_levels: "plain" (frame levels only), "deltas" (segmentation,
+    delta_lf multi and mode/ref deltas on), "single" (delta_lf single),
+    "zero" (both luma levels 0)."""
+    rng = np.random.default_rng([seed, 0x1E7E])
+    lv = abi.pf_lf_levels()
+    lv.level_y[0], lv.level_y[1] = int(rng.integers(1, 64)), int(rng.integers(1, 64))
+    lv.level_u, lv.level_v = int(rng.integers(0, 64)), int(rng.integers(0, 64))
+    if mode == "zero":
+        lv.level_y[0] = lv.level_y[1] = 0
+    if mode in ("deltas", "single"):
+        lv.delta_lf_present = 1
+        lv.delta_lf_multi = 1 if mode == "deltas" else 0
+        lv.segmentation_enabled = 1
+        lv.mode_ref_delta_enabled = 1
+        for i in range(8):
+            lv.ref_delta[i] = int(rng.integers(-20, 21))
+            for k in range(4):
+                lv.segment_delta[i][k] = int(rng.integers(-20, 21))
+        lv.mode_delta[0], lv.mode_delta[1] = int(rng.integers(-20, 21)), int(rng.integers(-20, 21))
+    return lv

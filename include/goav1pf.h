@@ -25,6 +25,12 @@
  *                          (SearchWienerUnitU8, SearchSGRProjUnitU8) and the
  *                          unit loops of EncodeLoopRestorationKeyframe,
  *                          encoder/keyframe_lossy.go:2313-2383, :2422-2453.
+ *   - pf_lf_build         internal/av1/threading/loop_filter_masks.go:450-551
+ *                          (FrameWorkLoopFilterMasks.BuildFromMap) and
+ *                          decoder/postfilter_loopfilter_masks.go:119-228
+ *                          (populateLoopFilterLevelCacheFromMap), as the
+ *                          encoder's mask-driven deblock calls them
+ *                          (encoder/loopfilter_apply.go:576-589).
  *   - status codes        sentinel errors: cdef.ErrInvalidCDEF
  *                          (cdef/direction.go:11), loopfilter.ErrInvalidFilter,
  *                          tile.ErrInvalidPlan, decoder.ErrUnsupportedPostFilter,
@@ -66,7 +72,8 @@ enum {
   PF_ERR_INVALID_ARG = -7,       /* null pointer, bad size or enum */
   PF_ERR_DEVICE = -8,            /* a CUDA call failed */
   PF_ERR_TIMEOUT = -9,           /* a bounded device wait ran out */
-  PF_ERR_NO_DEVICE = -10         /* no usable sm_100 device */
+  PF_ERR_NO_DEVICE = -10,        /* no usable sm_100 device */
+  PF_ERR_INVALID_BATCH = -11     /* threading.ErrInvalidBatch (block record map) */
 };
 
 /* ---- stage bits (FrameWorkPostFilterStage, postfilter.go:13-21) ---- */
@@ -396,6 +403,83 @@ int pf_superres_upscale(pf_ctx* ctx, const pf_frame* coded, const pf_frame* upsc
  * before anything is touched.  Returns when the frames are filtered. */
 int pf_frame_apply_superres(pf_ctx* ctx, const pf_frame* coded, const pf_frame_side* side,
                             const pf_frame* upscaled, const pf_frame* display, pf_stats* stats);
+
+/* ---- deblocking masks and level cache from the block record map ----
+ * The record map is threading.FrameWorkLoopFilterMap
+ * (threading/loop_filter_map.go:46-72): one record per 4x4 MI cell, row-major
+ * with stride mi_cols, each block's record repeated in every cell it covers
+ * (its visible part).  pf_lf_build turns it into the two products
+ * pf_frame_apply's deblocking reads (pf_loop_filter.masks and .level_cache):
+ *   - the lfmask.FilterMask edge bitmasks of every 128x128 region, as
+ *     BuildFromMap builds them: each block's left/above edge width class is
+ *     the minimum of its own transform class and the neighbouring block's
+ *     right/bottom transform class read from the map (2 luma, 1 chroma at the
+ *     frame edge or next to an invalid cell); inner transform edges of intra
+ *     and non-skip inter blocks; chroma edges from the block that carries the
+ *     shared chroma (lfmask/build.go:60-100, :203-236, lfmask/mask.go);
+ *   - the level cache, each block's four levels (ResolveBlockLevels,
+ *     loopfilter/level.go:120-190) over its luma cells (bytes 0-1) and its
+ *     chroma cells (bytes 2-3, chroma coordinates with the luma stride),
+ *     blocks later in raster order of their origin overwriting earlier ones.
+ * Both outputs are overwritten whole: masks
+ * ceil(mi_cols/32)*ceil(mi_rows/32)*PF_LF_MASK_WORDS uint16, level_cache
+ * 4*mi_cols*mi_rows bytes.  A map whose records partition the grid (as the
+ * decoder writes it) gives the reference's output bit for bit. */
+typedef struct pf_lf_record {      /* threading.FrameWorkLoopFilterBlockRecord */
+  uint16_t mi_col;                 /* Block.MICol, MIRow: the block's origin cell */
+  uint16_t mi_row;
+  uint16_t mi_col_end;             /* Block.MIColEnd, MIRowEnd (exclusive, clamped to the grid) */
+  uint16_t mi_row_end;
+  uint8_t block_size;              /* tile.BlockSize: 0 = 128x128 ... 21 = 4x4 */
+  uint8_t valid;
+  uint8_t intra;
+  uint8_t skip;                    /* SkipTransform */
+  uint8_t tx_y;                    /* TransformTree.Y (tile.TransformSize: 0 = 4x4 ... 18 = 64x16) */
+  uint8_t tx_uv;                   /* TransformTree.UV */
+  uint8_t has_uv;                  /* TransformTree.HasUV */
+  uint8_t segment_id;
+  uint8_t ref_frame;               /* 0 intra, 1..7 LAST..ALTREF */
+  uint8_t mode;                    /* loopfilter.ModeDeltaClass: 0 GLOBALMV, 1 other inter modes */
+  int8_t delta_lf_from_base;       /* DeltaLFFromBase */
+  int8_t delta_lf[4];              /* DeltaLF (delta_lf_multi: YV, YH, U, V) */
+  uint8_t reserved0;
+  uint16_t tx_split[2];            /* TransformTree.Split: var-tx split bits, depth 0 and 1 */
+  uint32_t reserved1;
+} pf_lf_record;                    /* 32 bytes */
+
+typedef struct pf_lf_levels {      /* loopfilter.PrepareLevelResolver inputs (level.go:86-118) */
+  uint8_t level_y[2];              /* LoopFilterParams.LevelY */
+  uint8_t level_u;
+  uint8_t level_v;
+  uint8_t delta_lf_present;        /* DeltaParams.DeltaLFPresent */
+  uint8_t delta_lf_multi;          /* DeltaParams.DeltaLFMulti */
+  uint8_t segmentation_enabled;    /* SegmentationParams.Enabled */
+  uint8_t mode_ref_delta_enabled;  /* LoopFilterParams.ModeRefDeltaEnabled */
+  int8_t ref_delta[8];             /* Deltas.Ref */
+  int8_t mode_delta[2];            /* Deltas.Mode */
+  uint8_t reserved[2];
+  int16_t segment_delta[8][4];     /* per segment DeltaLFYV, DeltaLFYH, DeltaLFU, DeltaLFV */
+} pf_lf_levels;
+
+/* Builds the masks and level cache on the GPU.  records: mi_cols*mi_rows
+ * records in records_memory (PF_MEM_HOST: copied up in the call); masks and
+ * level_cache: both in out_memory.  ss_x/ss_y/mono: the sequence's chroma
+ * layout (lfmask.Layout; no chroma edges or chroma levels when mono).
+ * Returns when the outputs are written.  Errors, as the reference's walk
+ * meets them in raster order of the level-cache population:
+ *   - PF_ERR_INVALID_BATCH: a visited record's MIColEnd is not past its cell
+ *     or past the grid, or its block size (or transform size, which the
+ *     reference indexes without a check) is out of range;
+ *   - PF_ERR_INVALID_FILTER: ref_frame > 7 or mode > 1, or segment_id > 7
+ *     with segmentation on (ResolveBlockLevels);
+ *   - PF_ERR_INVALID_ARG: null pointers, odd or zero mi_cols/mi_rows (the
+ *     decoder's MI grid is always even), mi_cols or mi_rows above 16384, a
+ *     bad memory kind or layout.
+ * On an error the outputs are unspecified (the reference leaves them
+ * partly written). */
+int pf_lf_build(pf_ctx* ctx, const pf_lf_record* records, int32_t mi_cols, int32_t mi_rows,
+                uint32_t records_memory, const pf_lf_levels* levels, int32_t ss_x, int32_t ss_y, int32_t mono,
+                uint16_t* masks, uint8_t* level_cache, uint32_t out_memory);
 
 /* ---- film grain with no allocation ----
  * No counterpart in the reference; this entry point exists for callers that

@@ -66,6 +66,13 @@ def lib():
         _lib.oracle_superres_row.restype = None
         _lib.oracle_superres_upscale.argtypes = [C.c_void_p, C.c_void_p]
         _lib.oracle_frame_apply_superres.argtypes = [C.c_void_p] * 4
+        _lib.oracle_lf_build.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_void_p]
+        _lib.oracle_lf_build_ordered.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p] + [C.c_int] * 5 + [
+            C.c_void_p]
+        _lib.oracle_lf_mask_block.argtypes = [C.c_int, C.c_void_p] + [C.c_int] * 6 + [C.c_void_p] * 3 + [C.c_int] * 2
+        _lib.oracle_lf_mask_block.restype = None
+        _lib.oracle_lf_block_levels.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     return _lib
 
 

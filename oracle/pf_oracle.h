@@ -102,6 +102,16 @@ int oracle_superres_upscale(const pf_frame* coded, const pf_frame* upscaled);
 int oracle_frame_apply_superres(const pf_frame* coded, const pf_frame_side* side, const pf_frame* upscaled,
                                 const pf_frame* display);
 
+/* Deblocking masks and level cache from the block record map
+ * (oracle/lfmask_oracle.cpp). */
+int oracle_lf_build(const pf_lf_record* rec, int cols, int rows, const pf_lf_levels* lv, int ssx, int ssy, int mono,
+                    uint16_t* masks, uint8_t* level_cache);
+int oracle_lf_build_ordered(const pf_lf_record* rec, int cols, int rows, const int32_t* order, int n, int sb_log2,
+                            int ssx, int ssy, int mono, uint16_t* masks);
+void oracle_lf_mask_block(int kind, uint16_t* region, int by4, int bx4, int w4, int h4, int skip, int tx,
+                          const uint16_t split[2], uint8_t* a, uint8_t* l, int ssx, int ssy);
+int oracle_lf_block_levels(const pf_lf_levels* p, int mono, const pf_lf_record* r, uint8_t out[4]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,11 +33,15 @@ def test_struct_sizes_match_header(L):
     assert C.sizeof(abi.pf_lr_unit) == 10
     assert C.sizeof(abi.pf_plane) == 32
     assert C.sizeof(abi.pf_frame) == 16 + 3 * 32
+    assert C.sizeof(abi.pf_lf_record) == 32 and abi.lf_record_dtype().itemsize == 32
+    assert abi.pf_lf_record.tx_split.offset == 24 and abi.pf_lf_record.delta_lf.offset == 19
+    assert C.sizeof(abi.pf_lf_levels) == 20 + 8 * 4 * 2
 
 
 def test_status_strings(L):
     assert L.pf_status_string(0) == b"ok"
     assert b"cdef" in L.pf_status_string(abi.PF_ERR_INVALID_CDEF)
+    assert b"batch" in L.pf_status_string(abi.PF_ERR_INVALID_BATCH)
 
 
 def _valid(L, fr, si, disp=None):
