@@ -24,8 +24,10 @@
 //
 // The errors the reference returns come from its level-cache walk, which
 // visits cells in a chain per MI row (an invalid cell steps one cell, a
-// valid one jumps to its MIColEnd).  k_lf_check replays that chain for each
-// row over shared memory and keeps the first error in raster order.
+// valid one jumps to its MIColEnd).  k_lf_build's row CTAs find that chain
+// for each row by pointer doubling in shared memory and keep its first
+// error; the host takes the first row's.
+#include <limits.h>
 #include <string.h>
 
 #include "pf_common.cuh"
@@ -44,8 +46,8 @@ struct MapArgs {
   const uint4* rec;  // 32-byte records, two uint4 each
   uint16_t* masks;
   uint32_t* levels;  // one 4-byte level cell per MI cell
-  unsigned long long* err;
-  int cols, rows, sbw, ssx, ssy, mono, ccols, crows;
+  unsigned long long* rowErr;  // per MI row: first error (cell << 8 | kind) or all ones
+  int cols, rows, sbw, regions, ssx, ssy, mono, ccols, crows;
   // ResolveBlockLevels inputs (loopfilter/level.go:86-118)
   uint8_t base[3][2];
   uint8_t lumaZero, deltaPresent, deltaMulti, segEnabled, modeRef;
@@ -134,12 +136,24 @@ __device__ __forceinline__ int safe_tx(int tx) { return tx < 19 ? tx : 0; }
 // build.go:104-111).
 __device__ __forceinline__ bool uniform_tx(const LfRec& r) { return r.intra() || (r.split() & 0xffff) == 0; }
 
+// The head of a record (words 0-3: origin, extent, size and flags,
+// transforms and segment) and, when asked, its split word: what the edge
+// rules read of a neighbouring cell.
+__device__ __forceinline__ LfRec load_head(const MapArgs& a, int x, int y, bool split) {
+  const uint4* p = a.rec + 2 * ((size_t)y * a.cols + x);
+  const uint4 u = __ldg(p);
+  LfRec r;
+  r.w[0] = u.x, r.w[1] = u.y, r.w[2] = u.z, r.w[3] = u.w;
+  r.w[4] = r.w[5] = r.w[7] = 0;
+  r.w[6] = split ? __ldg((const uint32_t*)(p + 1) + 2) : 0;
+  return r;
+}
+
 // The class a neighbouring block carries out of its right column (vertical)
-// or bottom row (horizontal) at the given map cell (fillLeftLumaContext /
-// fillAboveLumaContext, loop_filter_masks.go:553-646): 2 when the cell holds
-// no valid block.
-__device__ int luma_edge_ctx(const MapArgs& a, int x, int y, bool vertical) {
-  const LfRec r = load_rec(a, x, y);
+// or bottom row (horizontal), read at map cell (x, y) whose record is `r`
+// (fillLeftLumaContext / fillAboveLumaContext, loop_filter_masks.go:553-646):
+// 2 when the cell holds no valid block.
+__device__ int luma_edge_ctx(const MapArgs& a, const LfRec& r, int x, int y, bool vertical) {
   if (!r.valid() || r.bs() >= 22) return 2;
   const int nbw = min(a.cols - r.col(), (int)a.t.block[r.bs()][0]);
   const int nbh = min(a.rows - r.row(), (int)a.t.block[r.bs()][1]);
@@ -183,54 +197,66 @@ __device__ uint32_t block_levels(const MapArgs& a, const LfRec& r) {
   return out;
 }
 
-// Luma cell (x, y): the width class of the vertical edge on its left and of
-// the horizontal edge on its top (-1: no edge), and its level cell.
-__device__ void luma_cell(const MapArgs& a, int x, int y, int& sv, int& sh, uint32_t& lv) {
-  const LfRec r = load_rec(a, x, y);
-  if (r.valid() && r.bs() < 22) {
-    const int bx = r.col(), by = r.row();
-    const int bw4 = min(a.cols - bx, (int)a.t.block[r.bs()][0]);
-    const int bh4 = min(a.rows - by, (int)a.t.block[r.bs()][1]);
-    const int lx = x - bx, ly = y - by;
-    if (lx >= 0 && ly >= 0 && lx < bw4 && ly < bh4) {
-      const int tx = safe_tx(r.txy());
-      const bool uni = uniform_tx(r);
-      const bool inner = r.intra() || !r.skip();
-      const Leaf L = tx_leaf(a.t, tx, uni, r.split(), lx, ly);
-      if (lx == 0)
-        sv = min(L.cw, bx > 0 ? luma_edge_ctx(a, x - 1, y, true) : 2);
-      else if (L.left && inner)
-        sv = min(L.cw, tx_leaf(a.t, tx, uni, r.split(), lx - 1, ly).cw);
-      if (ly == 0)
-        sh = min(L.ch, by > 0 ? luma_edge_ctx(a, x, y - 1, false) : 2);
-      else if (L.top && inner)
-        sh = min(L.ch, tx_leaf(a.t, tx, uni, r.split(), lx, ly - 1).ch);
-      lv = block_levels(a, r) & 0xffff;
-    }
-  }
-  // Chroma levels of chroma cell (x, y): the covering block last in raster
-  // order of origin (the reference's walk writes each block's chroma rect).
-  if (!a.mono && x < a.ccols && y < a.crows) {
-    uint32_t bestKey = 0;
-    bool found = false;
-    LfRec best;
-    for (int j = 0; j <= a.ssy; j++)
-      for (int i = 0; i <= a.ssx; i++) {
-        const LfRec c = load_rec(a, (x << a.ssx) + i, (y << a.ssy) + j);
-        if (!c.valid() || c.bs() >= 22) continue;
-        const uint32_t key = (uint32_t)c.row() << 16 | c.col();
-        if (!found || key > bestKey) best = c, bestKey = key, found = true;
-      }
-    if (found) lv |= block_levels(a, best) & 0xffff0000u;
-  }
+// Luma cell (x, y) with its record and those of its left and upper
+// neighbours: the width class of the vertical edge on its left and of the
+// horizontal edge on its top (-1: no edge), and the luma bytes of its level
+// cell.
+__device__ void luma_cell(const MapArgs& a, int x, int y, const LfRec& r, const LfRec& left, const LfRec& above,
+                          int& sv, int& sh, uint32_t& lv) {
+  if (!r.valid() || r.bs() >= 22) return;
+  const int bx = r.col(), by = r.row();
+  const int bw4 = min(a.cols - bx, (int)a.t.block[r.bs()][0]);
+  const int bh4 = min(a.rows - by, (int)a.t.block[r.bs()][1]);
+  const int lx = x - bx, ly = y - by;
+  if (lx < 0 || ly < 0 || lx >= bw4 || ly >= bh4) return;
+  const int tx = safe_tx(r.txy());
+  const bool uni = uniform_tx(r);
+  const bool inner = r.intra() || !r.skip();
+  const Leaf L = tx_leaf(a.t, tx, uni, r.split(), lx, ly);
+  if (lx == 0)
+    sv = min(L.cw, bx > 0 ? luma_edge_ctx(a, left, x - 1, y, true) : 2);
+  else if (L.left && inner)
+    sv = min(L.cw, tx_leaf(a.t, tx, uni, r.split(), lx - 1, ly).cw);
+  if (ly == 0)
+    sh = min(L.ch, by > 0 ? luma_edge_ctx(a, above, x, y - 1, false) : 2);
+  else if (L.top && inner)
+    sh = min(L.ch, tx_leaf(a.t, tx, uni, r.split(), lx, ly - 1).ch);
+  lv = block_levels(a, r) & 0xffff;
 }
 
-// Chroma cell (cx, cy): the block carrying the shared chroma is the one at the
-// bottom-right luma cell of the cell's luma group (the has_chroma gate of
-// dav1d as BuildFromMap applies it, loop_filter_masks.go:508-533).
-__device__ void chroma_cell(const MapArgs& a, int cx, int cy, int& sv, int& sh) {
+// Chroma level bytes of chroma cell (x, y): the covering block last in raster
+// order of origin (the reference's walk writes each block's chroma rect), one
+// of the records at the cell's luma group.
+__device__ uint32_t chroma_levels(const MapArgs& a, int x, int y) {
+  // The group is 1, 2 or 4 cells: k = j * 2 + i with i <= ssx, j <= ssy.
+  uint32_t head0[4], head2[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int i = k & 1, j = k >> 1;
+    head2[k] = 0;
+    if (i <= a.ssx && j <= a.ssy) {
+      const uint4 u = __ldg(a.rec + 2 * ((size_t)((y << a.ssy) + j) * a.cols + (x << a.ssx) + i));
+      head0[k] = u.x, head2[k] = u.z;
+    }
+  }
+  int best = -1;
+  uint32_t bestKey = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const bool valid = (head2[k] >> 8) & 0xff;
+    if (!valid || (head2[k] & 0xff) >= 22) continue;
+    const uint32_t key = head0[k];  // mi_row << 16 | mi_col: raster order of origin
+    if (best < 0 || key > bestKey) best = k, bestKey = key;
+  }
+  if (best < 0) return 0;
+  return block_levels(a, load_rec(a, (x << a.ssx) + (best & 1), (y << a.ssy) + (best >> 1))) & 0xffff0000u;
+}
+
+// Chroma cell (cx, cy) with the record `r` at the bottom-right luma cell of
+// its luma group: the block carrying the shared chroma there (the has_chroma
+// gate of dav1d as BuildFromMap applies it, loop_filter_masks.go:508-533).
+__device__ void chroma_cell(const MapArgs& a, int cx, int cy, const LfRec& r, int& sv, int& sh) {
   const int lx = (cx << a.ssx) + a.ssx, ly = (cy << a.ssy) + a.ssy;
-  const LfRec r = load_rec(a, lx, ly);
   if (!r.valid() || !r.hasUV() || r.bs() >= 22) return;
   const int bx = r.col(), by = r.row();
   const int W4 = a.t.block[r.bs()][0], H4 = a.t.block[r.bs()][1];
@@ -244,41 +270,54 @@ __device__ void chroma_cell(const MapArgs& a, int cx, int cy, int& sv, int& sh) 
   const uint8_t* d = a.t.tx[safe_tx(r.txuv())];
   const int cw = d[2] != 0, ch = d[3] != 0;
   const bool inner = r.intra() || !r.skip();
+  // The two context loads depend only on the block origin: issue both.
+  const bool needL = lcx == 0 && bx > 0, needA = lcy == 0 && by > 0;
+  LfRec nl, na;
+  if (needL) nl = load_head(a, bx - 1, min((cy << a.ssy) + a.ssy, a.rows - 1), false);
+  if (needA) na = load_head(a, min((cx << a.ssx) + a.ssx, a.cols - 1), by - 1, false);
   if (lcx == 0) {
     int ctx = 1;
-    if (bx > 0) {
-      const LfRec n = load_rec(a, bx - 1, min((cy << a.ssy) + a.ssy, a.rows - 1));
-      if (n.valid() && n.hasUV()) ctx = a.t.tx[safe_tx(n.txuv())][2] != 0;
-    }
+    if (needL && nl.valid() && nl.hasUV()) ctx = a.t.tx[safe_tx(nl.txuv())][2] != 0;
     sv = min(cw, ctx);
   } else if (inner && (lcx & (d[0] - 1)) == 0) {
     sv = cw;
   }
   if (lcy == 0) {
     int ctx = 1;
-    if (by > 0) {
-      const LfRec n = load_rec(a, min((cx << a.ssx) + a.ssx, a.cols - 1), by - 1);
-      if (n.valid() && n.hasUV()) ctx = a.t.tx[safe_tx(n.txuv())][3] != 0;
-    }
+    if (needA && na.valid() && na.hasUV()) ctx = a.t.tx[safe_tx(na.txuv())][3] != 0;
     sh = min(ch, ctx);
   } else if (inner && (lcy & (d[1] - 1)) == 0) {
     sh = ch;
   }
 }
 
-// One CTA per 128x128 region (32x32 cells), a thread per cell.
-__global__ void __launch_bounds__(1024) k_lf_masks(MapArgs a) {
-  __shared__ int8_t s_t[32][33];
-  __shared__ uint32_t s_lv[32][33];
-  const int rx = blockIdx.x, ry = blockIdx.y;
+// One 128x128 region (32x32 cells) per CTA, a thread per cell.
+__device__ void region_masks(const MapArgs& a, int region, int8_t (*s_t)[33], uint32_t (*s_lv)[33]) {
+  const int rx = region % a.sbw, ry = region / a.sbw;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* M = (uint32_t*)(a.masks + ((size_t)ry * a.sbw + rx) * PF_LF_MASK_WORDS);
+  uint32_t* M = (uint32_t*)(a.masks + (size_t)region * PF_LF_MASK_WORDS);
+
+  // Every record load that does not depend on another goes out first: the
+  // cell's own record, its left and upper neighbours (read only when the
+  // cell starts its block), and the emitter of this thread's chroma cell.
+  const int x = rx * 32 + w, y = ry * 32 + lane;
+  const bool in = x < a.cols && y < a.rows;
+  const int cwid = 32 >> a.ssx, chgt = 32 >> a.ssy;
+  const int cx = rx * cwid + w, cy = ry * chgt + lane;
+  const bool cin = !a.mono && w < cwid && lane < chgt && cx < a.ccols && cy < a.crows;
+  LfRec own, left, above, em;
+  if (in) own = load_rec(a, x, y);
+  if (in && x > 0) left = load_head(a, x - 1, y, true);
+  if (in && y > 0) above = load_head(a, x, y - 1, true);
+  if (cin) em = load_head(a, (cx << a.ssx) + a.ssx, (cy << a.ssy) + a.ssy, false);
 
   // Luma.  Warp = column w, lane = row: vertical edges of column w.
   int sv = -1, sh = -1;
   uint32_t lv = 0;
-  const int x = rx * 32 + w, y = ry * 32 + lane;
-  if (x < a.cols && y < a.rows) luma_cell(a, x, y, sv, sh, lv);
+  if (in) {
+    luma_cell(a, x, y, own, left, above, sv, sh, lv);
+    if (!a.mono && x < a.ccols && y < a.crows) lv |= chroma_levels(a, x, y);
+  }
   // Y[0][w][s] as one 32-bit word: bit = row within the region.
 #pragma unroll
   for (int s = 0; s < 3; s++) {
@@ -304,10 +343,8 @@ __global__ void __launch_bounds__(1024) k_lf_masks(MapArgs a) {
 
   // Chroma: the region's (32 >> ssx) x (32 >> ssy) chroma cells.  UV[dir][pos][s]
   // is two 16-bit halves split at 16 >> ss of the scanned direction.
-  const int cwid = 32 >> a.ssx, chgt = 32 >> a.ssy;
   int cv = -1, chs = -1;
-  const int cx = rx * cwid + w, cy = ry * chgt + lane;
-  if (!a.mono && w < cwid && lane < chgt && cx < a.ccols && cy < a.crows) chroma_cell(a, cx, cy, cv, chs);
+  if (cin) chroma_cell(a, cx, cy, em, cv, chs);
   const int vsplit = 16 >> a.ssy, hsplit = 16 >> a.ssx;
 #pragma unroll
   for (int s = 0; s < 2; s++) {
@@ -334,7 +371,7 @@ __device__ uint32_t walk_cell(const MapArgs& a, int c, int row) {
   const LfRec r = load_rec(a, c, row);
   if (!r.valid()) return c + 1;
   const int next = r.colEnd();
-  if (next <= c || next > a.cols) return (uint32_t)kLfBatch << 20;
+  if (next <= c || next > a.cols) return (uint32_t)c | (uint32_t)kLfBatch << 20;
   uint32_t code = 0;
   if (r.col() == c && r.row() == row) {
     if (r.ref() >= 8 || r.mode() > 1 || (!a.lumaZero && a.segEnabled && r.seg() >= 8))
@@ -345,31 +382,69 @@ __device__ uint32_t walk_cell(const MapArgs& a, int c, int row) {
   return (uint32_t)next | code << 20;
 }
 
-__global__ void __launch_bounds__(256) k_lf_check(MapArgs a) {
-  __shared__ uint32_t s_info[256];
-  __shared__ int s_pos, s_stop;
-  const int row = blockIdx.x;
-  if (threadIdx.x == 0) s_pos = 0, s_stop = 0;
-  for (int c0 = 0; c0 < a.cols; c0 += 256) {
+struct WalkSmem {
+  int next[1024];
+  int succ[1024];
+  uint8_t mark[1024];
+  int entry, err, exit;
+};
+
+// One MI row's walk, 1024 cells at a time: the chain from the entry cell is
+// found by pointer doubling (after round r every cell within 2^(r+1) - 1
+// steps of the entry is marked), an error cell ending the chain.  Writes the
+// row's first error as (cell index << 8 | kind), or all ones.
+__device__ void row_walk(const MapArgs& a, int row, WalkSmem& S) {
+  const int i = threadIdx.x;
+  if (i == 0) S.entry = 0, S.err = INT_MAX;
+  for (int c0 = 0; c0 < a.cols; c0 += 1024) {
     __syncthreads();
-    if (s_stop) break;
-    const int c = c0 + threadIdx.x;
-    s_info[threadIdx.x] = c < a.cols ? walk_cell(a, c, row) : 0;
+    const int entry = S.entry;
+    if (entry >= a.cols || S.err != INT_MAX) break;
+    if (entry >= c0 + 1024) continue;
+    const int c = c0 + i;
+    const uint32_t v = c < a.cols ? walk_cell(a, c, row) : (uint32_t)(c + 1);
+    const int code = v >> 20, succ = v & 0xfffff;
+    S.succ[i] = v;
+    S.next[i] = code ? c : succ;  // an error cell is a fixed point: the chain ends there
+    S.mark[i] = c == entry;
+    if (i == 0) S.exit = INT_MAX;
     __syncthreads();
-    if (threadIdx.x == 0) {
-      int pos = s_pos;
-      while (pos < c0 + 256 && pos < a.cols) {
-        const uint32_t v = s_info[pos - c0];
-        if (v >> 20) {
-          atomicMin(a.err, (unsigned long long)((size_t)row * a.cols + pos) << 8 | (v >> 20));
-          s_stop = 1;
-          break;
-        }
-        pos = v & 0xfffff;  // strictly past pos: an invalid cell steps one, a valid one jumps to MIColEnd
-      }
-      s_pos = pos;
+#pragma unroll 1
+    for (int r = 0; r < 10; r++) {
+      const int n = S.next[i];
+      const bool m = S.mark[i];
+      const int n2 = n < c0 + 1024 ? S.next[n - c0] : n;
+      __syncthreads();
+      if (m && n < c0 + 1024) S.mark[n - c0] = 1;
+      S.next[i] = n2;
+      __syncthreads();
     }
+    if (S.mark[i]) {
+      if (code) atomicMin(&S.err, c);
+      else if (succ >= c0 + 1024) S.exit = succ;  // the chain's last cell in this chunk
+    }
+    __syncthreads();
+    if (i == 0) S.entry = S.err != INT_MAX ? a.cols : S.exit;
   }
+  __syncthreads();
+  if (i == 0) {
+    unsigned long long out = ~0ull;
+    if (S.err != INT_MAX)  // the error's chunk is the last one loaded
+      out = (unsigned long long)((size_t)row * a.cols + S.err) << 8 | (S.succ[S.err & 1023] >> 20);
+    a.rowErr[row] = out;
+  }
+}
+
+// One launch: CTAs [0, regions) build the masks and level cache of one
+// 128x128 region each, the rest walk one MI row each for the status.
+__global__ void __launch_bounds__(1024) k_lf_build(MapArgs a) {
+  __shared__ int8_t s_t[32][33];
+  __shared__ uint32_t s_lv[32][33];
+  __shared__ WalkSmem s_walk;
+  if ((int)blockIdx.x < a.regions)
+    region_masks(a, blockIdx.x, s_t, s_lv);
+  else
+    row_walk(a, blockIdx.x - a.regions, s_walk);
 }
 
 }  // namespace pf
@@ -417,18 +492,19 @@ extern "C" int pf_lf_build(pf_ctx* ctx, const pf_lf_record* records, int32_t col
                lcB = cells * 4;
   auto up = [](size_t n) { return (n + 255) & ~(size_t)255; };
   const bool hostRec = records_memory == PF_MEM_HOST, hostOut = out_memory == PF_MEM_HOST;
-  const size_t total = 256 + (hostRec ? up(recB) : 0) + (hostOut ? up(maskB) + up(lcB) : 0);
+  const size_t errB = up((size_t)rows * 8);
+  const size_t total = errB + (hostRec ? up(recB) : 0) + (hostOut ? up(maskB) + up(lcB) : 0);
   uint8_t* scratch = (uint8_t*)pf_internal_search_scratch(ctx, total);
-  unsigned long long* hostErr = (unsigned long long*)pf_internal_pinned(ctx, 64);
+  unsigned long long* hostErr = (unsigned long long*)pf_internal_pinned(ctx, (size_t)rows * 8);
   if (!scratch || !hostErr) return PF_ERR_DEVICE;
   const cudaStream_t st = (cudaStream_t)pf_internal_stream(ctx);
-  size_t off = 256;
-  a.err = (unsigned long long*)scratch;
-  cudaError_t e = cudaMemsetAsync(a.err, 0xff, 8, st);
+  size_t off = errB;
+  a.rowErr = (unsigned long long*)scratch;
+  cudaError_t e = cudaSuccess;
   if (hostRec) {
     a.rec = (const uint4*)(scratch + off);
     off += up(recB);
-    if (e == cudaSuccess) e = cudaMemcpyAsync((void*)a.rec, records, recB, cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync((void*)a.rec, records, recB, cudaMemcpyHostToDevice, st);
   } else {
     a.rec = (const uint4*)records;
   }
@@ -441,15 +517,16 @@ extern "C" int pf_lf_build(pf_ctx* ctx, const pf_lf_record* records, int32_t col
     a.levels = (uint32_t*)level_cache;
   }
   if (e != cudaSuccess) return PF_ERR_DEVICE;
-  k_lf_check<<<rows, 256, 0, st>>>(a);
-  k_lf_masks<<<dim3(a.sbw, sbh), 1024, 0, st>>>(a);
+  a.regions = a.sbw * sbh;
+  k_lf_build<<<a.regions + rows, 1024, 0, st>>>(a);
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(hostErr, a.err, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hostErr, a.rowErr, (size_t)rows * 8, cudaMemcpyDeviceToHost, st);
   if (hostOut && e == cudaSuccess) e = cudaMemcpyAsync(masks, a.masks, maskB, cudaMemcpyDeviceToHost, st);
   if (hostOut && e == cudaSuccess) e = cudaMemcpyAsync(level_cache, a.levels, lcB, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return PF_ERR_DEVICE;
-  const unsigned long long err = *hostErr;
+  unsigned long long err = ~0ull;
+  for (int r = 0; r < rows; r++) err = hostErr[r] < err ? hostErr[r] : err;
   if (err == ~0ull) return PF_OK;
   return (err & 0xff) == kLfFilter ? PF_ERR_INVALID_FILTER : PF_ERR_INVALID_BATCH;
 }

@@ -157,3 +157,21 @@ def test_masks_drive_the_deblocking(runner):
     for p, (a, b) in enumerate(zip(want.planes, got.planes)):
         assert np.array_equal(a, b), "plane %d differs in %d samples" % (p, int((a != b).sum()))
     assert not np.array_equal(want.planes[0], frame.planes[0])
+
+
+def test_rows_longer_than_one_walk_chunk(runner):
+    """MI rows of more than 1024 cells (the row walk goes 1024 cells at a time):
+    parity, and errors found in the second and third chunks."""
+    from goav1_b200.postfilter import ErrInvalidBatch, ErrInvalidFilter
+
+    rec, _ = synth.make_lf_map(11, 2200, 40)
+    lv = synth.make_lf_levels(11, "deltas")
+    check(runner, rec, lv)
+    for col, field, value, err in ((1500, "mi_col_end", 0, ErrInvalidBatch), (2100, "ref_frame", 8, ErrInvalidFilter)):
+        r = rec[5, col]
+        blk = (slice(int(r["mi_row"]), int(r["mi_row_end"])), slice(int(r["mi_col"]), int(r["mi_col_end"])))
+        bad = rec.copy()
+        bad[blk][field] = value
+        assert oracle(bad, lv)[0] == err.code
+        with pytest.raises(err):
+            runner.lf_build(bad, lv)
