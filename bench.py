@@ -321,19 +321,9 @@ def run_reference(args):
 
 def _pinned(fr, like=False):
     """A host copy of a HostFrame (or a zeroed one of its geometry) in
-    page-locked memory."""
-    import torch
-
-    out = fr.like() if like else fr.copy()
-    keep = []
-    for k, p in enumerate(out.planes):
-        t = torch.empty(p.shape, dtype=torch.uint8 if p.dtype == np.uint8 else torch.int16, pin_memory=True)
-        a = t.numpy().view(p.dtype)
-        a[:] = p
-        out.planes[k] = a
-        keep.append(t)
-    out._pin = keep
-    return out
+    page-locked memory, its planes back to back in one buffer as goav1's
+    frame.Bind lays a frame out."""
+    return fr.back_to_back(pinned=True, like=like)
 
 
 def call_median(fn, reps):

@@ -999,6 +999,81 @@ static void read_stage_times(pf_ctx* c, pf_stats* stats) {
   }
 }
 
+// Byte offset of each plane from plane 0 when a host frame's planes lie back
+// to back in one buffer, as goav1's frame.Bind lays them out (Y, U, V
+// consecutive, each stride x aligned height: frame/buffer.go:141-236), with
+// 16-byte multiples for the offsets and strides and rows padded by less than
+// 256 bytes; -1 otherwise.
+static int64_t contiguous_span(const pf_frame* f, int64_t off[3]) {
+  const int bps = bps_of(f);
+  const uint8_t* base = (const uint8_t*)f->plane[0].data;
+  int64_t at = 0;
+  for (int p = 0; p < 3; p++) {
+    const pf_plane& pl = f->plane[p];
+    const int64_t row = (int64_t)pl.alloc_width * bps;
+    if ((const uint8_t*)pl.data != base + at || pl.stride < row || pl.stride - row >= 256 || pl.stride % 16 ||
+        at % 16)
+      return -1;
+    off[p] = at;
+    at += pl.stride * pl.alloc_height;
+  }
+  return at;
+}
+
+// Device layout of a host frame's planes at `base`: the host layout itself
+// when its planes are back to back (the frame then moves as one copy), else
+// each plane 256-byte aligned, with the host pitch when rows are packed
+// (pitch = row bytes, a multiple of 16: the plane moves as one contiguous
+// copy) or rows padded to 256 bytes.
+static size_t host_frame_layout(const pf_frame* f, uint8_t* base, void** ptrs, int64_t* strides) {
+  int64_t off[3];
+  const int64_t span = contiguous_span(f, off);
+  if (span > 0) {
+    for (int p = 0; p < 3; p++) {
+      strides[p] = f->plane[p].stride;
+      if (ptrs) ptrs[p] = base + off[p];
+    }
+    return align256((size_t)span);
+  }
+  const int bps = bps_of(f);
+  size_t total = 0;
+  for (int p = 0; p < 3; p++) {
+    const pf_plane& pl = f->plane[p];
+    const int64_t row = (int64_t)pl.alloc_width * bps;
+    strides[p] = pl.stride == row && row % 16 == 0 ? row : (row + 255) & ~(int64_t)255;
+    if (ptrs) ptrs[p] = base + total;
+    total = align256(total + (size_t)strides[p] * pl.alloc_height);
+  }
+  return total;
+}
+
+// Host <-> device copies of a frame laid out by host_frame_layout: one copy
+// for a back-to-back frame, else one per plane (2-D when the pitches differ).
+static cudaError_t copy_planes(const pf_frame* f, void* const* dev, const int64_t* ds, bool up, cudaStream_t st) {
+  int64_t off[3];
+  const int64_t span = contiguous_span(f, off);
+  if (span > 0 && (uint8_t*)dev[1] - (uint8_t*)dev[0] == off[1] && (uint8_t*)dev[2] - (uint8_t*)dev[0] == off[2] &&
+      ds[0] == f->plane[0].stride && ds[1] == f->plane[1].stride && ds[2] == f->plane[2].stride)
+    return up ? cudaMemcpyAsync(dev[0], f->plane[0].data, (size_t)span, cudaMemcpyHostToDevice, st)
+              : cudaMemcpyAsync(f->plane[0].data, dev[0], (size_t)span, cudaMemcpyDeviceToHost, st);
+  const int bps = bps_of(f);
+  for (int p = 0; p < 3; p++) {
+    const pf_plane& pl = f->plane[p];
+    const size_t w = (size_t)pl.alloc_width * bps;
+    cudaError_t e;
+    if (ds[p] == pl.stride && (size_t)pl.stride == w) {
+      const size_t bytes = w * pl.alloc_height;
+      e = up ? cudaMemcpyAsync(dev[p], pl.data, bytes, cudaMemcpyHostToDevice, st)
+             : cudaMemcpyAsync(pl.data, dev[p], bytes, cudaMemcpyDeviceToHost, st);
+    } else {
+      e = up ? cudaMemcpy2DAsync(dev[p], ds[p], pl.data, pl.stride, w, pl.alloc_height, cudaMemcpyHostToDevice, st)
+             : cudaMemcpy2DAsync(pl.data, pl.stride, dev[p], ds[p], w, pl.alloc_height, cudaMemcpyDeviceToHost, st);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side* s, const pf_frame* display,
                               pf_stats* stats) {
   if (!c) return PF_ERR_INVALID_ARG;
@@ -1014,11 +1089,9 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
   const bool wantDisp = (s->stages & PF_STAGE_FILM_GRAIN) && display;
   r.display = wantDisp ? display : nullptr;
   if (f->memory == PF_MEM_HOST) {
-    CK(layout_like(f, c->io, r.io, r.ioStride));
-    for (int p = 0; p < 3; p++)
-      CK(cudaMemcpy2DAsync(r.io[p], r.ioStride[p], f->plane[p].data, f->plane[p].stride,
-                           (size_t)f->plane[p].alloc_width * bps, f->plane[p].alloc_height, cudaMemcpyHostToDevice,
-                           c->stream));
+    CK(c->io.ensure(host_frame_layout(f, nullptr, nullptr, r.ioStride) + 256));
+    host_frame_layout(f, (uint8_t*)c->io.p, r.io, r.ioStride);
+    CK(copy_planes(f, r.io, r.ioStride, true, c->stream));
   } else {
     for (int p = 0; p < 3; p++) {
       r.io[p] = f->plane[p].data;
@@ -1027,7 +1100,8 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
   }
   if (wantDisp) {
     if (display->memory == PF_MEM_HOST) {
-      CK(layout_like(display, c->disp, r.dp, r.dStride));
+      CK(c->disp.ensure(host_frame_layout(display, nullptr, nullptr, r.dStride) + 256));
+      host_frame_layout(display, (uint8_t*)c->disp.p, r.dp, r.dStride);
     } else {
       for (int p = 0; p < 3; p++) {
         r.dp[p] = display->plane[p].data;
@@ -1037,16 +1111,8 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
   }
   st = run_batch(c, &r, 1, stats);
   if (st != PF_OK) return st;
-  if (f->memory == PF_MEM_HOST)
-    for (int p = 0; p < 3; p++)
-      CK(cudaMemcpy2DAsync(f->plane[p].data, f->plane[p].stride, r.io[p], r.ioStride[p],
-                           (size_t)f->plane[p].alloc_width * bps, f->plane[p].alloc_height, cudaMemcpyDeviceToHost,
-                           c->stream));
-  if (wantDisp && display->memory == PF_MEM_HOST)
-    for (int p = 0; p < 3; p++)
-      CK(cudaMemcpy2DAsync(display->plane[p].data, display->plane[p].stride, r.dp[p], r.dStride[p],
-                           (size_t)display->plane[p].alloc_width * bps, display->plane[p].alloc_height,
-                           cudaMemcpyDeviceToHost, c->stream));
+  if (f->memory == PF_MEM_HOST) CK(copy_planes(f, r.io, r.ioStride, false, c->stream));
+  if (wantDisp && display->memory == PF_MEM_HOST) CK(copy_planes(display, r.dp, r.dStride, false, c->stream));
   if (f->memory == PF_MEM_HOST || (wantDisp && display->memory == PF_MEM_HOST) || c->timing) {
     CK(cudaStreamSynchronize(c->stream));
     read_stage_times(c, stats);
@@ -1064,41 +1130,6 @@ static cudaError_t pinned_ensure(void** p, size_t* n, size_t need) {
   const cudaError_t e = cudaMallocHost(p, need);
   if (e == cudaSuccess) *n = need;
   return e;
-}
-
-// Device layout of a host frame's planes at `base`: the host row pitch when
-// rows are packed (pitch = row bytes, a multiple of 16: each plane then moves
-// as one contiguous copy), else rows padded to 256 bytes.
-static size_t host_frame_layout(const pf_frame* f, uint8_t* base, void** ptrs, int64_t* strides) {
-  const int bps = bps_of(f);
-  size_t total = 0;
-  for (int p = 0; p < 3; p++) {
-    const pf_plane& pl = f->plane[p];
-    const int64_t row = (int64_t)pl.alloc_width * bps;
-    strides[p] = pl.stride == row && row % 16 == 0 ? row : (row + 255) & ~(int64_t)255;
-    if (ptrs) ptrs[p] = base + total;
-    total = align256(total + (size_t)strides[p] * pl.alloc_height);
-  }
-  return total;
-}
-
-static cudaError_t copy_planes(const pf_frame* f, void* const* dev, const int64_t* ds, bool up, cudaStream_t st) {
-  const int bps = bps_of(f);
-  for (int p = 0; p < 3; p++) {
-    const pf_plane& pl = f->plane[p];
-    const size_t w = (size_t)pl.alloc_width * bps;
-    cudaError_t e;
-    if (ds[p] == pl.stride && (size_t)pl.stride == w) {
-      const size_t bytes = w * pl.alloc_height;
-      e = up ? cudaMemcpyAsync(dev[p], pl.data, bytes, cudaMemcpyHostToDevice, st)
-             : cudaMemcpyAsync(pl.data, dev[p], bytes, cudaMemcpyDeviceToHost, st);
-    } else {
-      e = up ? cudaMemcpy2DAsync(dev[p], ds[p], pl.data, pl.stride, w, pl.alloc_height, cudaMemcpyHostToDevice, st)
-             : cudaMemcpy2DAsync(pl.data, pl.stride, dev[p], ds[p], w, pl.alloc_height, cudaMemcpyDeviceToHost, st);
-    }
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
 }
 
 // A batch of host frames: chunks of c->host_chunk frames flow through a

@@ -58,6 +58,31 @@ class HostFrame:
         return HostFrame(self.width, self.height, self.bit_depth, self.ss_x, self.ss_y,
                          [np.zeros_like(p) for p in self.planes], list(self.crop), self.mono)
 
+    def back_to_back(self, pinned=False, like=False):
+        """A copy (or, with `like`, a zeroed frame of the same geometry) whose
+        planes lie back to back in one buffer, Y then U then V, as goav1's
+        frame.Bind lays a frame out (frame/buffer.go:141-236); page-locked
+        when `pinned`."""
+        sizes = [p.nbytes for p in self.planes]
+        if pinned:
+            import torch
+
+            buf_t = torch.zeros(sum(sizes), dtype=torch.uint8, pin_memory=True)
+            buf = buf_t.numpy()
+        else:
+            buf_t, buf = None, np.zeros(sum(sizes), np.uint8)
+        planes, at = [], 0
+        for p, n in zip(self.planes, sizes):
+            a = buf[at:at + n].view(p.dtype).reshape(p.shape)
+            if not like:
+                a[:] = p
+            planes.append(a)
+            at += n
+        out = HostFrame(self.width, self.height, self.bit_depth, self.ss_x, self.ss_y, planes, list(self.crop),
+                        self.mono)
+        out._buf = (buf_t, buf)
+        return out
+
     def pf(self, memory=abi.PF_MEM_HOST, ptrs=None):
         f = abi.pf_frame()
         f.width, f.height = self.width, self.height

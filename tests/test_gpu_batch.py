@@ -138,16 +138,21 @@ def _host_copy(fr, pinned, like=False):
     return out
 
 
-@pytest.mark.parametrize("pinned", [True, False])
-def test_host_frame_batches_match_oracle(frames, expected, pinned):
+@pytest.mark.parametrize("pinned,b2b", [(True, False), (False, False), (True, True), (False, True)])
+def test_host_frame_batches_match_oracle(frames, expected, pinned, b2b):
     """Host frames through pf_batch_apply's chunked copy/compute pipeline:
-    13 frames (four chunks, so the three staging slots wrap) in two calls."""
+    13 frames (four chunks, so the three staging slots wrap) in two calls;
+    planes in separate buffers, or back to back in one buffer as goav1
+    allocates a frame (each frame then moves as one copy each way)."""
     from goav1_b200.postfilter import PostFilterRunner
+
+    def host(fr, like=False):
+        return fr.back_to_back(pinned, like=like) if b2b else _host_copy(fr, pinned, like=like)
 
     order = list(range(len(frames))) + list(range(5))
     r = PostFilterRunner()
     for call in range(2):
-        hosts = [(_host_copy(frames[i][0], pinned), _host_copy(frames[i][0], pinned, like=True)) for i in order]
+        hosts = [(host(frames[i][0]), host(frames[i][0], like=True)) for i in order]
         items = [(h.pf(), frames[i][1].side, d.pf()) for (h, d), i in zip(hosts, order)]
         stats = r.apply_batch(items)
         assert stats.completed == abi.PF_STAGES_ALL
@@ -172,3 +177,20 @@ def test_mixed_host_and_device_batch_is_rejected(frames):
         r.apply_batch([(h0.pf(), s0.side, hd0.pf()), (d1.pf(), s1.side, dd1.pf())])
     assert np.array_equal(h0.planes[0], f0.planes[0])
     r.close()
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_single_back_to_back_host_frames(frames, expected, pinned):
+    """pf_frame_apply on host frames whose planes lie back to back."""
+    from goav1_b200.postfilter import PostFilterRunner
+
+    r = PostFilterRunner()
+    for i, (fr, si) in enumerate(frames):
+        h, d = fr.back_to_back(pinned), fr.back_to_back(pinned, like=True)
+        r.apply(h.pf(), si.side, d.pf())
+        ref, disp = expected[i]
+        for name, a, b in (("reference", ref, h), ("display", disp, d)):
+            for p, (pa, pb) in enumerate(zip(a.planes, b.planes)):
+                assert np.array_equal(pa, pb), "frame %d %s plane %d differs" % (i, name, p)
+    r.close()
+
