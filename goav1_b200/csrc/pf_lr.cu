@@ -47,15 +47,16 @@ __device__ __forceinline__ uint32_t rpotu(uint32_t v, int bits) {
 // Wiener filter of the staged window (restoration/wiener.go:132-211): the
 // block's sample (0,0) sits at sm.win[3 * kWin + 3], w x h <= 64 x 64, with
 // the 3-sample halo around it.  hf/vf are the 7 horizontal / vertical taps.
-// out(y, x, v) receives every output sample; threads map to samples as
-// x = tid % PW, y = tid / PW + k * (256 / PW).  Every thread of the CTA calls
-// it; it leaves the window untouched and ends without a barrier.
+// out(y, x, v) receives every output sample; thread tid produces column
+// x = tid % PW over a run of consecutive rows (the h rows split into 256 / PW
+// runs).  Every thread of the CTA calls it; it leaves the window untouched
+// and ends without a barrier.
 template <class Out>
 __device__ __forceinline__ void lr_wiener_window(LrSmem& sm, int w, int h, int bd, const int* hf, const int* vf, int PW,
                                  Out&& out) {
   const uint16_t* s_win = sm.win;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tid = threadIdx.x, tx = tid % PW, ty0 = tid / PW, rowStep = 256 / PW;
+  const int tid = threadIdx.x, tx = tid % PW, ty0 = tid / PW, rpg = (h + 256 / PW - 1) / (256 / PW);
   const int wh = h + 6;
   const int maxv = (1 << bd) - 1;
   // restoration/wiener.go:202-211 (wienerRounds), :132-196.
@@ -79,14 +80,23 @@ __device__ __forceinline__ void lr_wiener_window(LrSmem& sm, int w, int h, int b
   }
   __syncthreads();
   const int32_t offV = 1 << (bd + round1 - 1);
-  if (tx < w)
-    for (int y = ty0; y < h; y += rowStep) {
-      int32_t c3 = temp[(y + 3) * 64 + tx];
-      int32_t sum = (c3 << 7) - offV;
+  // Each thread a run of consecutive output rows of column tx: the seven
+  // vertical taps slide down in registers, one new row read per output.
+  const int ya = ty0 * rpg, yb = imin(h, ya + rpg);
+  if (tx < w && ya < yb) {
+    int32_t t[7];
 #pragma unroll
-      for (int k = 0; k < 7; k++) sum += (int32_t)temp[(y + k) * 64 + tx] * vf[k];
+    for (int k = 0; k < 6; k++) t[k] = temp[(ya + k) * 64 + tx];
+    for (int y = ya; y < yb; y++) {
+      t[6] = temp[(y + 6) * 64 + tx];
+      int32_t sum = (t[3] << 7) - offV;
+#pragma unroll
+      for (int k = 0; k < 7; k++) sum += t[k] * vf[k];
       out(y, tx, imin(imax(rpot(sum, round1), 0), maxv));
+#pragma unroll
+      for (int k = 0; k < 6; k++) t[k] = t[k + 1];
     }
+  }
 }
 
 // Self-guided filter of the staged window (restoration/selfguided.go:111-390)
@@ -99,7 +109,9 @@ __device__ __forceinline__ void lr_sgr_window(LrSmem& sm, int w, int h, int bd, 
   uint16_t* s_A = sm.A;
   int32_t* s_B = sm.B;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tid = threadIdx.x, tx = tid % PW, ty0 = tid / PW, rowStep = 256 / PW;
+  const int tid = threadIdx.x, tx = tid % PW, ty0 = tid / PW, rpg = (h + 256 / PW - 1) / (256 / PW);
+  // Output rows of this thread: a run [ya, yb) of column tx.
+  const int ya = ty0 * rpg, yb = imin(h, ya + rpg);
   const int ww = w + 6;
   const int maxv = (1 << bd) - 1;
   const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][1];
@@ -177,32 +189,58 @@ __device__ __forceinline__ void lr_sgr_window(LrSmem& sm, int w, int h, int bd, 
       }
     }
     __syncthreads();
-    if (tx < w) {
-      for (int y = ty0; y < h; y += rowStep) {
-        const uint16_t* A = &s_A[(y + 1) * 66 + tx + 1];
-        const int32_t* B = &s_B[(y + 1) * 66 + tx + 1];
-        const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
-        if (pass == 0) {
+    // The a/b neighbourhoods slide down the thread's rows: row k of the
+    // tables is s_A/s_B[k * 66 + tx .. tx + 2] (output row y sits at k = y + 1).
+    if (tx < w && ya < yb) {
+      auto rowA = [&](int k, int32_t (&v)[3]) {
+        v[0] = s_A[k * 66 + tx], v[1] = s_A[k * 66 + tx + 1], v[2] = s_A[k * 66 + tx + 2];
+      };
+      auto rowB = [&](int k, int32_t (&v)[3]) {
+        v[0] = s_B[k * 66 + tx], v[1] = s_B[k * 66 + tx + 1], v[2] = s_B[k * 66 + tx + 2];
+      };
+      if (pass == 0) {
+        // Radius 2: a/b exist on even table rows only.  Even y takes rows y
+        // and y + 2 (weights 6 centre / 5 corners, shift 9), odd y row y + 1
+        // (6 / 5, shift 8).
+        const int e = ya & ~1;
+        int32_t uA[3], uB[3], dA[3], dB[3];
+        rowA(e, uA), rowB(e, uB), rowA(e + 2, dA), rowB(e + 2, dB);
+        for (int y = ya; y < yb; y++) {
+          const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
           int32_t av, bv, shift;
           if ((y & 1) == 0) {
-            av = (A[-66] + A[66]) * 6 + (A[-67] + A[-65] + A[65] + A[67]) * 5;
-            bv = (B[-66] + B[66]) * 6 + (B[-67] + B[-65] + B[65] + B[67]) * 5;
+            if (y != e) {
+#pragma unroll
+              for (int k = 0; k < 3; k++) uA[k] = dA[k], uB[k] = dB[k];
+              rowA(y + 2, dA), rowB(y + 2, dB);
+            }
+            av = (uA[1] + dA[1]) * 6 + (uA[0] + uA[2] + dA[0] + dA[2]) * 5;
+            bv = (uB[1] + dB[1]) * 6 + (uB[0] + uB[2] + dB[0] + dB[2]) * 5;
             shift = 9;
           } else {
-            av = A[0] * 6 + (A[-1] + A[1]) * 5;
-            bv = B[0] * 6 + (B[-1] + B[1]) * 5;
+            av = dA[1] * 6 + (dA[0] + dA[2]) * 5;
+            bv = dB[1] * 6 + (dB[0] + dB[2]) * 5;
             shift = 8;
           }
           flt0[y * 64 + tx] = rpot(av * dg + bv, shift);
-        } else {
+        }
+      } else {
+        // Radius 1: rows y, y + 1, y + 2 (weights 4 cross / 3 corners).
+        int32_t uA[3], uB[3], mA[3], mB[3], dA[3], dB[3];
+        rowA(ya, uA), rowB(ya, uB), rowA(ya + 1, mA), rowB(ya + 1, mB);
+        for (int y = ya; y < yb; y++) {
+          rowA(y + 2, dA), rowB(y + 2, dB);
+          const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
           // restoration/selfguided.go:233-247: projection with the int16 wrap.
-          const int32_t av = (A[0] + A[-1] + A[1] + A[-66] + A[66]) * 4 + (A[-67] + A[65] + A[-65] + A[67]) * 3;
-          const int32_t bv = (B[0] + B[-1] + B[1] + B[-66] + B[66]) * 4 + (B[-67] + B[65] + B[-65] + B[67]) * 3;
+          const int32_t av = (mA[0] + mA[1] + mA[2] + uA[1] + dA[1]) * 4 + (uA[0] + uA[2] + dA[0] + dA[2]) * 3;
+          const int32_t bv = (mB[0] + mB[1] + mB[2] + uB[1] + dB[1]) * 4 + (uB[0] + uB[2] + dB[0] + dB[2]) * 3;
           const int32_t f1 = rpot(av * dg + bv, 9);
           const int32_t uu = dg << 4;
           const int32_t v = (uu << 7) + xq0 * (flt0[y * 64 + tx] - uu) + xq1 * (f1 - uu);
           const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
           out(y, tx, imin(imax(wv, 0), maxv));
+#pragma unroll
+          for (int k = 0; k < 3; k++) uA[k] = mA[k], uB[k] = mB[k], mA[k] = dA[k], mB[k] = dB[k];
         }
       }
     }
@@ -210,7 +248,7 @@ __device__ __forceinline__ void lr_sgr_window(LrSmem& sm, int w, int h, int bd, 
   }
   if (r1 == 0 && tx < w) {
     // Only the radius-2 filter: project with xq1 = 0.
-    for (int y = ty0; y < h; y += rowStep) {
+    for (int y = ya; y < yb; y++) {
       const int32_t uu = (int32_t)s_win[(y + 3) * kWin + tx + 3] << 4;
       const int32_t v = (uu << 7) + xq0 * (flt0[y * 64 + tx] - uu);
       const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
@@ -237,7 +275,7 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
   const int x1 = imin(x0 + PW, Wa), y1 = imin((s + 1) * SH - off, Ha);
   const int tid = threadIdx.x;
   const int tx = tid % PW, ty0 = tid / PW, rowStep = 256 / PW;
-  const int bd = src.bd;
+  const int bd = sizeof(T) == 1 ? 8 : src.bd;  // a constant for 8-bit: the rounding shifts fold
 
   // Which restoration unit (if any) covers this tile.
   const pf_lr_unit* u = nullptr;
