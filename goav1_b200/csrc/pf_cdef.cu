@@ -50,7 +50,7 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
   int32_t* s_cost = sm.cost;
   const int tid = threadIdx.x;
   if (tid < 12) sm.ofs[tid] = make_int2(dir_off(tid, 0), dir_off(tid, 1));
-  const int coeffShift = in.bd - 8;
+  const int coeffShift = sizeof(T) == 1 ? 0 : in.bd - 8;
   // The index map is only present when CDEF filters; the copy-only pass (CDEF
   // off, loop restoration on) reads no side information.
   const int mapOff = ur * a.index_stride + uc;

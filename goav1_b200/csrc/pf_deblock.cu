@@ -197,10 +197,11 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
   if (pos0 - reachP < 0 || pos0 + reachQ >= lim || along >= alongLim) return;
   const int sstride = (int)(pl.stride / sizeof(T));
   T* q = row_ptr<T>(pl, r4 * 4) + c4 * 4;
+  const int bd = sizeof(T) == 1 ? 8 : f.bd;  // a constant for 8-bit: the depth shifts fold
   if (dir == 0)
-    lpf_unit<T>(q, sstride, 1, f.bd, E, I, H, wd);
+    lpf_unit<T>(q, sstride, 1, bd, E, I, H, wd);
   else
-    lpf_unit<T>(q, 1, sstride, f.bd, E, I, H, wd);
+    lpf_unit<T>(q, 1, sstride, bd, E, I, H, wd);
 }
 
 // Batched deblocking: each work item is one 32x8 tile of edge units of one

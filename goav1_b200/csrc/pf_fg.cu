@@ -192,7 +192,7 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
     for (int y = y0; y < yend; y++) row_ptr<T>(dp, y)[x] = row_ptr<T>(sp, y)[x];
     return;
   }
-  const int bd = ref.bd;
+  const int bd = sizeof(T) == 1 ? 8 : ref.bd;  // a constant for 8-bit: the depth shifts fold
   const int sx = plane ? ref.ssx : 0, sy = plane ? ref.ssy : 0;
   const int bwl = 5 - sx, bhl = 5 - sy;
   const int bw = 1 << bwl, bh = 1 << bhl;
