@@ -687,6 +687,7 @@ struct Staged {
   uint8_t* idx;
   FinishOut* fo;
   uint8_t* extra;
+  uint8_t* pin;  // page-locked staging: noskip words up, then the results down
   int nfb, maxCfg;
   cudaStream_t st;
 };
@@ -764,6 +765,11 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
   // The noskip words may live in host or device memory: copy them into the
   // scratch either way; host words go through page-locked staging so the
   // copy does not hold the host.
+  // One page-locked block for the call (requested once, so it never moves
+  // while a copy is queued): the noskip words, then the selection results.
+  uint8_t* pin = (uint8_t*)pf_internal_pinned(ctx, al((size_t)nfb * 8) + al(sizeof(FinishOut)) + al(nfb));
+  if (!pin) return PF_ERR_DEVICE;
+  S->pin = pin;
   const uint8_t* ns = nullptr;
   if (noskip && e == cudaSuccess) {
     cudaPointerAttributes at;
@@ -773,8 +779,6 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
     if (dev) {
       e = cudaMemcpyAsync(base + oNs, noskip, (size_t)nfb * 8, cudaMemcpyDeviceToDevice, st);
     } else {
-      void* pin = pf_internal_pinned(ctx, (size_t)nfb * 8);
-      if (!pin) return PF_ERR_DEVICE;
       memcpy(pin, noskip, (size_t)nfb * 8);
       e = cudaMemcpyAsync(base + oNs, pin, (size_t)nfb * 8, cudaMemcpyHostToDevice, st);
     }
@@ -827,14 +831,21 @@ static int search_finish(Staged& S, const pf_cdef_search_params* params, uint64_
   if (launch_search(S.a, st) != cudaSuccess) return PF_ERR_DEVICE;
   if (launch_select(S.s, S.maxCfg, (unsigned long long)params->lambda, S.idx, S.fo, st) != cudaSuccess)
     return PF_ERR_DEVICE;
-  FinishOut fo;
-  if (cudaMemcpyAsync(&fo, S.fo, sizeof(fo), cudaMemcpyDeviceToHost, st) != cudaSuccess) return PF_ERR_DEVICE;
+  // The small results come back through the page-locked block (a pageable
+  // destination would make each copy a staged, synchronous one).
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  uint8_t* pfo = S.pin + al((size_t)S.nfb * 8);
+  uint8_t* pidx = pfo + al(sizeof(FinishOut));
+  if (cudaMemcpyAsync(pfo, S.fo, sizeof(FinishOut), cudaMemcpyDeviceToHost, st) != cudaSuccess) return PF_ERR_DEVICE;
   if (mse_out &&
       cudaMemcpyAsync(mse_out, S.a.mse, (size_t)2 * S.nfb * 64 * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return PF_ERR_DEVICE;
-  if (fb_index_out && cudaMemcpyAsync(fb_index_out, S.idx, S.nfb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+  if (fb_index_out && cudaMemcpyAsync(pidx, S.idx, S.nfb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return PF_ERR_DEVICE;
   if (cudaStreamSynchronize(st) != cudaSuccess) return PF_ERR_DEVICE;
+  FinishOut fo;
+  memcpy(&fo, pfo, sizeof(fo));
+  if (fb_index_out) memcpy(fb_index_out, pidx, S.nfb);
   if (result) {
     memset(result, 0, sizeof(*result));
     result->bits = (uint8_t)fo.bits;
