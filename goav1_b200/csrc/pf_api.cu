@@ -210,6 +210,22 @@ static int plane_dims_ok(const pf_frame* f) {
   return 1;
 }
 
+// Whether any plane of `a` shares bytes with any plane of `b` (each plane
+// spans stride x (alloc_height - 1) + its row).
+static bool frames_overlap(const pf_frame* a, const pf_frame* b) {
+  const int ba = a->bit_depth > 8 ? 2 : 1, bb = b->bit_depth > 8 ? 2 : 1;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      const pf_plane &p = a->plane[i], &q = b->plane[j];
+      if (!p.data || !q.data || p.alloc_height <= 0 || q.alloc_height <= 0) continue;
+      const uintptr_t p0 = (uintptr_t)p.data, q0 = (uintptr_t)q.data;
+      const uintptr_t p1 = p0 + (uintptr_t)(p.stride * (p.alloc_height - 1) + (int64_t)p.alloc_width * ba);
+      const uintptr_t q1 = q0 + (uintptr_t)(q.stride * (q.alloc_height - 1) + (int64_t)q.alloc_width * bb);
+      if (p0 < q1 && q0 < p1) return true;
+    }
+  return false;
+}
+
 static int frames_same_geometry(const pf_frame* a, const pf_frame* b) {
   if (a->width != b->width || a->height != b->height || a->bit_depth != b->bit_depth || a->ss_x != b->ss_x ||
       a->ss_y != b->ss_y || a->mono != b->mono)
@@ -308,6 +324,9 @@ extern "C" int pf_frame_validate(const pf_frame* f, const pf_frame_side* s, cons
     if (!display) return PF_ERR_INVALID_ARG;
     if (display->memory > PF_MEM_DEVICE || !plane_dims_ok(display) || !frames_same_geometry(f, display))
       return PF_ERR_SHORT_BUFFER;
+    // The display picture is a separate output (PostFilterOutput): grain
+    // reads the reference's luma for chroma scaling while it writes display.
+    if (display->memory == f->memory && frames_overlap(f, display)) return PF_ERR_INVALID_ARG;
   }
   return PF_OK;
 }

@@ -253,7 +253,7 @@ void pf_destroy(pf_ctx* ctx);
  * loop restoration, border extension; the result is the publishable
  * reference frame) and, when PF_STAGE_FILM_GRAIN is set and grain applies,
  * writes the grained display picture into `display` (which must have the
- * same geometry).  Host frames are copied to the device and back inside the
+ * same geometry and share no memory with `frame`: PF_ERR_INVALID_ARG).  Host frames are copied to the device and back inside the
  * call; device frames are filtered where they lie.  Returns when the work is
  * complete (host frames) or queued on the context's stream (device frames;
  * pf_sync waits for it). */

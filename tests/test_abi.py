@@ -87,6 +87,11 @@ def test_validate_rejects_bad_restoration_and_grain(L):
     assert _valid(L, fr, si, disp) == abi.PF_ERR_INVALID_FORMAT
     fr, si = synth.make_frame(1, 2, width=256, height=192)
     assert _valid(L, fr, si, None) == abi.PF_ERR_INVALID_ARG
+    # The display picture may not share memory with the frame.
+    assert _valid(L, fr, si, fr) == abi.PF_ERR_INVALID_ARG
+    half = fr.like()
+    half.planes[2] = fr.planes[1]
+    assert _valid(L, fr, si, half) == abi.PF_ERR_INVALID_ARG
 
 
 def test_runner_without_device_raises():
