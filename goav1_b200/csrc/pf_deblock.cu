@@ -152,6 +152,13 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
   const uint16_t* region = a.masks + (size_t)(rRow * a.sb128_w + rCol) * PF_LF_MASK_WORDS;
   const int pos = dir == 0 ? pcol : prow;
   const int bit = dir == 0 ? prow : pcol;
+  // The cell's and its left / upper neighbour's levels (sb.go:122-128,
+  // :142-148) depend only on the cell: their loads go out with the mask
+  // words' instead of after them.
+  const int comp = plane == 0 ? dir : plane + 1;
+  const int li = r4 * a.mi_cols + c4;
+  const int L0 = __ldg(&a.level_cache[4 * li + comp]);
+  const int L1 = __ldg(&a.level_cache[4 * (dir == 0 ? li - 1 : li - a.mi_cols) + comp]);
   int k = -1;
   if (luma) {
     const int half = bit >> 4, b = bit & 15;
@@ -169,13 +176,8 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
   }
   if (k < 0) return;
   const int wd = k == 2 ? 16 : (k == 1 ? (luma ? 8 : 6) : 4);
-  // Level with the left / above fallback (sb.go:122-128, :142-148).
-  const int comp = luma ? dir : plane + 1;
-  const int li = r4 * a.mi_cols + c4;
-  // Both levels are read together; the neighbour's is used when this
-  // cell's is 0 (c4 > 0 for vertical, r4 > 0 for horizontal edges here).
-  const int L0 = __ldg(&a.level_cache[4 * li + comp]);
-  const int L1 = __ldg(&a.level_cache[4 * (dir == 0 ? li - 1 : li - a.mi_cols) + comp]);
+  // Level with the left / above fallback: the neighbour's when this cell's
+  // is 0 (c4 > 0 for vertical, r4 > 0 for horizontal edges here).
   const int L = L0 != 0 ? L0 : L1;
   if (L == 0) return;
   // loopfilter/threshold.go:18-47.
