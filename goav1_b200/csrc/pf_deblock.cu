@@ -13,6 +13,8 @@
 // spacing), so every 4-sample edge unit of one direction is independent: one
 // thread owns one unit (4 lines), warps run along the edge grid so the 32
 // threads of a warp touch one 128-byte span per row.
+#include <type_traits>
+
 #include "pf_common.cuh"
 
 namespace pf {
@@ -20,8 +22,64 @@ namespace pf {
 // loopfilter/sb.go:348-446 (lpfUnit16); reduces to lpfUnit8 at bd == 8.
 // q points at q0 of the first line; sa steps along the edge, sb across it
 // (both in elements).
+// The inner samples of the unit's four lines: P[i][k] = p_k, Q[i][k] = q_k of
+// line i (k < 4).  `q` points at q0 of line 0; dir 0 (vertical edge) steps
+// lines by rows, dir 1 by columns.  With `words`, eight 4-sample words are
+// read (4 bytes, or 8 for 16-bit samples): for a vertical edge the p3..p0
+// and q0..q3 runs of each line, for a horizontal edge the four lines'
+// samples of each of the eight rows; else sample by sample.
 template <typename T>
-__device__ __forceinline__ void lpf_unit(T* q, int sa, int sb, int bd, int E, int I, int H, int wd) {
+__device__ __forceinline__ void lpf_inner(const T* q, int stride, int dir, bool words, int (&P)[4][4],
+                                          int (&Q)[4][4]) {
+  if (!words) {
+    const int sa = dir == 0 ? stride : 1, sb = dir == 0 ? 1 : stride;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        P[i][k] = q[i * sa - (k + 1) * sb];
+        Q[i][k] = q[i * sa + k * sb];
+      }
+    return;
+  }
+  typedef typename std::conditional<sizeof(T) == 1, uint32_t, uint2>::type W;
+  auto lane = [](const W& w, int j) -> int {
+    if constexpr (sizeof(T) == 1) {
+      return (w >> (8 * j)) & 0xff;
+    } else {
+      return ((j < 2 ? w.x : w.y) >> (16 * (j & 1))) & 0xffff;
+    }
+  };
+  W v[8];
+  if (dir == 0) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      v[2 * i] = *reinterpret_cast<const W*>(q + (int64_t)i * stride - 4);
+      v[2 * i + 1] = *reinterpret_cast<const W*>(q + (int64_t)i * stride);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        P[i][k] = lane(v[2 * i], 3 - k);
+        Q[i][k] = lane(v[2 * i + 1], k);
+      }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = *reinterpret_cast<const W*>(q + (int64_t)(j - 4) * stride);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        P[i][k] = lane(v[3 - k], i);
+        Q[i][k] = lane(v[4 + k], i);
+      }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void lpf_unit(T* q, int sa, int sb, int bd, int E, int I, int H, int wd,
+                                         const int (&P)[4][4], const int (&Q)[4][4]) {
   const int bd8 = bd - 8;
   const int F = 1 << bd8;
   E <<= bd8;
@@ -30,18 +88,8 @@ __device__ __forceinline__ void lpf_unit(T* q, int sa, int sb, int bd, int E, in
   const unsigned twoI = 2u * I, twoF = 2u * F, twoH = 2u * H;
   const int maxPix = (1 << bd) - 1;
   const int diffMin = -128 << bd8, diffMax = (128 << bd8) - 1;
-  // The four lines never overlap, so the inner samples of all four (p3..q3
-  // as far as the width reaches) are read before any line is filtered: one
-  // round trip to memory instead of one per line.
-  const int nIn = wd > 6 ? 4 : (wd > 4 ? 3 : 2);
-  int P[4][4], Q[4][4];  // P[i][k] = p_k, Q[i][k] = q_k of line i
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      P[i][k] = k < nIn ? q[i * sa - (k + 1) * sb] : 0;
-      Q[i][k] = k < nIn ? q[i * sa + k * sb] : 0;
-    }
+  // The four lines never overlap, so the inner samples of all four (P, Q:
+  // p3..q3) were read by the caller before any line is filtered.
 #pragma unroll
   for (int i = 0; i < 4; i++, q += sa) {
     const int p1 = P[i][1], p0 = P[i][0], q0 = Q[i][0], q1 = Q[i][1];
@@ -153,12 +201,26 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
   const int pos = dir == 0 ? pcol : prow;
   const int bit = dir == 0 ? prow : pcol;
   // The cell's and its left / upper neighbour's levels (sb.go:122-128,
-  // :142-148) depend only on the cell: their loads go out with the mask
-  // words' instead of after them.
+  // :142-148) and the unit's inner samples depend only on the cell: their
+  // loads go out with the mask words' instead of after them.  The inner
+  // samples p3..q3 of the four lines lie inside the allocated plane for
+  // every unit past the first column / row (edge positions are inside the
+  // 4-aligned crop, which the 8-aligned allocation covers).
   const int comp = plane == 0 ? dir : plane + 1;
   const int li = r4 * a.mi_cols + c4;
   const int L0 = __ldg(&a.level_cache[4 * li + comp]);
   const int L1 = __ldg(&a.level_cache[4 * (dir == 0 ? li - 1 : li - a.mi_cols) + comp]);
+  const DPlane& pl = f.pl[plane];
+  const int pos0 = dir == 0 ? c4 * 4 : r4 * 4;
+  const int lim = dir == 0 ? pl.aw : pl.ah;
+  const int along = dir == 0 ? r4 * 4 + 3 : c4 * 4 + 3;
+  const int alongLim = dir == 0 ? pl.ah : pl.aw;
+  if (pos0 - 4 < 0 || pos0 + 3 >= lim || along >= alongLim) return;
+  const int sstride = (int)(pl.stride / sizeof(T));
+  T* q = row_ptr<T>(pl, r4 * 4) + c4 * 4;
+  const bool words = (((uintptr_t)pl.ptr | (uintptr_t)pl.stride) & (4 * sizeof(T) - 1)) == 0;
+  int P[4][4], Q[4][4];
+  lpf_inner<T>(q, sstride, dir, words, P, Q);
   int k = -1;
   if (luma) {
     const int half = bit >> 4, b = bit & 15;
@@ -186,24 +248,16 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
   if (sh > 0 && limit > 9 - sh) limit = 9 - sh;
   if (limit < 1) limit = 1;
   const int E = 2 * (L + 2) + limit, I = limit, H = L >> 4;
-  const DPlane& pl = f.pl[plane];
-  // The masks are trusted like the reference trusts them, but an edge whose
-  // taps would leave the allocated plane (only a malformed mask can ask for
-  // one; the reference would fault on it) is skipped instead of touched.
-  const int reachP = wd == 16 ? 7 : (wd == 8 ? 4 : (wd == 6 ? 3 : 2));
-  const int reachQ = wd == 16 ? 6 : (wd == 8 ? 3 : (wd == 6 ? 2 : 1));
-  const int pos0 = dir == 0 ? c4 * 4 : r4 * 4;
-  const int lim = dir == 0 ? pl.aw : pl.ah;
-  const int along = dir == 0 ? r4 * 4 + 3 : c4 * 4 + 3;
-  const int alongLim = dir == 0 ? pl.ah : pl.aw;
-  if (pos0 - reachP < 0 || pos0 + reachQ >= lim || along >= alongLim) return;
-  const int sstride = (int)(pl.stride / sizeof(T));
-  T* q = row_ptr<T>(pl, r4 * 4) + c4 * 4;
+  // The masks are trusted like the reference trusts them, but a 14-tap edge
+  // whose outer taps would leave the allocated plane (only a malformed mask
+  // can ask for one; the reference would fault on it) is skipped instead of
+  // touched.
+  if (wd == 16 && (pos0 - 7 < 0 || pos0 + 6 >= lim)) return;
   const int bd = sizeof(T) == 1 ? 8 : f.bd;  // a constant for 8-bit: the depth shifts fold
   if (dir == 0)
-    lpf_unit<T>(q, sstride, 1, bd, E, I, H, wd);
+    lpf_unit<T>(q, sstride, 1, bd, E, I, H, wd, P, Q);
   else
-    lpf_unit<T>(q, 1, sstride, bd, E, I, H, wd);
+    lpf_unit<T>(q, 1, sstride, bd, E, I, H, wd, P, Q);
 }
 
 // Batched deblocking: each work item is one 32x8 tile of edge units of one
