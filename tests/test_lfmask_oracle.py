@@ -245,3 +245,34 @@ def test_errors_in_walk_order(lib):
     assert oracle_build(lib, bad, lv)[0] == abi.PF_ERR_INVALID_FILTER
     lv0 = synth.make_lf_levels(7)  # segmentation off: the segment id is not consulted
     assert oracle_build(lib, bad, lv0)[0] == 0
+
+
+@pytest.mark.parametrize("cols,rows,sb128", [(480, 270, True), (480, 270, False), (38, 24, True), (2, 66, False)])
+def test_synthetic_maps_partition_the_grid(cols, rows, sb128):
+    """The generated record maps are what the decoder writes: every cell
+    holds the record of the one block covering it (its visible rectangle
+    clamped to the grid), blocks are AV1 sizes aligned to their own size
+    inside one superblock, and the decode order lists each origin once."""
+    bdims, txd, _ = synth.av1_tables()
+    rec, order = synth.make_lf_map(5, cols, rows, sb128=sb128)
+    assert rec["valid"].all()
+    seen = np.zeros((rows, cols), np.int32)
+    sb = 32 if sb128 else 16
+    origins = set()
+    for o in order:
+        x, y = int(o) % cols, int(o) // cols
+        r = rec[y, x]
+        assert (r["mi_col"], r["mi_row"]) == (x, y) and o not in origins
+        origins.add(o)
+        w4, h4 = bdims[r["block_size"]]
+        assert x % w4 == 0 and y % h4 == 0  # AV1 blocks sit on their own size
+        assert x // sb == (x + w4 - 1) // sb and y // sb == (y + h4 - 1) // sb
+        x1, y1 = min(x + w4, cols), min(y + h4, rows)
+        assert (r["mi_col_end"], r["mi_row_end"]) == (x1, y1)
+        cells = rec[y:y1, x:x1]
+        assert (cells == r).all()
+        seen[y:y1, x:x1] += 1
+        assert r["tx_y"] < 19 and r["tx_uv"] < 19
+        tw, th = txd[r["tx_y"]][:2]
+        assert tw <= w4 and th <= h4  # a transform never exceeds its block
+    assert (seen == 1).all()
