@@ -33,14 +33,25 @@ __device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
 }
 
 // AR recursion of one template (luma.go:83-158 / chroma.go:92-199 generic
-// form) as a wavefront.  One warp; lanes take rows.  Row y computes column
-// t - 4y at step t, so every causal neighbour (rows above up to x + LAG,
-// LAG <= 3) was written at an earlier step.  The LAG is a template argument:
-// the coefficients sit in registers and the tap loops unroll.
+// form) as a wavefront: every thread of the CTA owns one template row
+// (y = 3 + r) and all take the same steps, a barrier after each.  Row y
+// computes column t - 4y at step t, so every causal neighbour (rows above up
+// to column x + LAG, LAG <= 3) was written at an earlier step.  A row's
+// causal window slides along it in registers: each step reads the LAG new
+// samples of the rows above and takes the row's own previous outputs from
+// registers.  The LAG is a template argument: the coefficients sit in
+// registers and the tap loops unroll.  Threads whose row is outside the
+// template (or whose plane does not run) only take the barriers.
+constexpr int kFgTemplateThreads = 192;
+
 template <int LAG>
-__device__ void ar_wavefront(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h) {
+__device__ void ar_rows(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h, int r,
+                        bool run) {
   constexpr int kTaps = 2 * LAG * (LAG + 1);  // causal neighbours before the centre
-  const int lane = threadIdx.x & 31;
+  constexpr int W = 2 * LAG + 1;
+  constexpr int LU = LAG > 0 ? LAG : 1;
+  const int y = 3 + r;
+  const bool mine = run && y < h;
   const int cs = p.coeff_shift, ro = 1 << (cs - 1);
   const int gmin = -(1 << (p.bd - 1)), gmax = (1 << (p.bd - 1)) - 1;
   int co[kTaps + 1];
@@ -48,18 +59,34 @@ __device__ void ar_wavefront(int16_t* g, const int16_t* luma, const FgTemplateAr
   for (int i = 0; i <= kTaps; i++) co[i] = p.coeffs[plane][i];
   const bool lumaTerm = plane != 0 && p.num_y_points != 0;
   const int sx = plane ? p.ssx : 0, sy = plane ? p.ssy : 0;
+  int up[LU][W];  // rows y - LAG .. y - 1, columns x - LAG .. x + LAG
+  int left[LU];   // row y, columns x - LAG .. x - 1
   const int tmax = (w - 4) + 4 * (h - 1);
   for (int t = 3 + 4 * 3; t <= tmax; t++) {
-    for (int y = 3 + lane; y < h; y += 32) {
-      const int x = t - 4 * y;
-      if (x < 3 || x >= w - 3) continue;
+    const int x = t - 4 * y;
+    if (mine && x >= 3 && x < w - 3) {
+      if (x == 3) {
+#pragma unroll
+        for (int dr = 0; dr < LAG; dr++)
+#pragma unroll
+          for (int dc = 0; dc < W; dc++) up[dr][dc] = g[(y - LAG + dr) * kGW + x - LAG + dc];
+#pragma unroll
+        for (int dc = 0; dc < LAG; dc++) left[dc] = g[y * kGW + x - LAG + dc];
+      } else {
+#pragma unroll
+        for (int dr = 0; dr < LAG; dr++) {
+#pragma unroll
+          for (int dc = 0; dc + 1 < W; dc++) up[dr][dc] = up[dr][dc + 1];
+          up[dr][W - 1] = g[(y - LAG + dr) * kGW + x + LAG];
+        }
+      }
       int sum = 0;
-      const int16_t* c = &g[y * kGW + x];
 #pragma unroll
-      for (int dr = -LAG; dr <= 0; dr++)
+      for (int dr = 0; dr < LAG; dr++)
 #pragma unroll
-        for (int dc = -LAG; dc <= (dr < 0 ? LAG : -1); dc++)
-          sum += co[(dr + LAG) * (2 * LAG + 1) + dc + LAG] * c[dr * kGW + dc];
+        for (int dc = 0; dc < W; dc++) sum += co[dr * W + dc] * up[dr][dc];
+#pragma unroll
+      for (int dc = 0; dc < LAG; dc++) sum += co[LAG * W + dc] * left[dc];
       if (lumaTerm) {
         const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
         int s = 0;
@@ -67,19 +94,23 @@ __device__ void ar_wavefront(int16_t* g, const int16_t* luma, const FgTemplateAr
           for (int dx = 0; dx <= sx; dx++) s += luma[(ly + dy) * kGW + lx + dx];
         sum += rpow2(s, sx + sy) * co[kTaps];
       }
-      g[y * kGW + x] = (int16_t)iclip(c[0] + ((sum + ro) >> cs), gmin, gmax);
+      const int v = iclip(g[y * kGW + x] + ((sum + ro) >> cs), gmin, gmax);
+      g[y * kGW + x] = (int16_t)v;
+#pragma unroll
+      for (int dc = 0; dc + 1 < LAG; dc++) left[dc] = left[dc + 1];
+      if (LAG > 0) left[LU - 1] = v;
     }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
-__device__ void ar_wavefront_lag(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w,
-                                 int h) {
+__device__ void ar_rows_lag(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h, int r,
+                            bool run) {
   switch (p.lag) {
-    case 0: ar_wavefront<0>(g, luma, p, plane, w, h); break;
-    case 1: ar_wavefront<1>(g, luma, p, plane, w, h); break;
-    case 2: ar_wavefront<2>(g, luma, p, plane, w, h); break;
-    default: ar_wavefront<3>(g, luma, p, plane, w, h); break;
+    case 0: ar_rows<0>(g, luma, p, plane, w, h, r, run); break;
+    case 1: ar_rows<1>(g, luma, p, plane, w, h, r, run); break;
+    case 2: ar_rows<2>(g, luma, p, plane, w, h, r, run); break;
+    default: ar_rows<3>(g, luma, p, plane, w, h, r, run); break;
   }
 }
 
@@ -115,7 +146,8 @@ __device__ void gauss_fill(int16_t* g, const int16_t* gauss, uint16_t seed, int 
   }
 }
 
-// One frame's templates: luma (warp 0), then Cb and Cr (warps 1, 2).
+// One frame's templates: Gaussian fills by warps 0-2 (luma, Cb, Cr), then the
+// AR recursions (all threads: luma, then Cb and Cr side by side).
 // s_gauss holds the Gaussian sequence (lanes draw different entries, which
 // constant memory would serialise).
 __device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, int16_t (*s_g)[kGW * kGH],
@@ -139,11 +171,15 @@ __device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, 
     __syncwarp();
   }
   __syncthreads();
-  if (warp == 0 && p.num_y_points != 0 && p.lag != 0) ar_wavefront_lag(s_g[0], nullptr, p, 0, kGW, kGH);
+  // Luma on every thread (row 3 + tid), then Cb (threads 0..95) and Cr
+  // (96..191) side by side; each call's step count is uniform.
+  if (p.num_y_points != 0 && p.lag != 0) ar_rows_lag(s_g[0], nullptr, p, 0, kGW, kGH, threadIdx.x, true);
   __syncthreads();
-  if (warp == 1 || warp == 2) {
-    const bool run = p.active[warp] && !(p.lag == 0 && p.num_y_points == 0);
-    if (run) ar_wavefront_lag(s_g[warp], s_g[0], p, warp, cw, ch);
+  const bool runC[3] = {false, p.active[1] && !(p.lag == 0 && p.num_y_points == 0),
+                        p.active[2] && !(p.lag == 0 && p.num_y_points == 0)};
+  if (runC[1] || runC[2]) {
+    const int pl = threadIdx.x < 96 ? 1 : 2;
+    ar_rows_lag(s_g[pl], s_g[0], p, pl, cw, ch, threadIdx.x % 96, runC[pl]);
   }
   __syncthreads();
   for (int pl = 0; pl < 3; pl++)
@@ -288,7 +324,7 @@ __device__ __forceinline__ void extend_px(const DFrame& f, int plane, int x, int
 
 // ---- batched kernels ----
 
-__global__ void __launch_bounds__(96) k_fg_templates_batch(BatchArgs b) {
+__global__ void __launch_bounds__(kFgTemplateThreads) k_fg_templates_batch(BatchArgs b) {
   __shared__ int16_t s_g[3][kGW * kGH];
   __shared__ int16_t s_gauss[2048];
   for (int i = threadIdx.x; i < 2048; i += blockDim.x) s_gauss[i] = c_gauss[i];
@@ -403,7 +439,7 @@ cudaError_t fg_upload_tables() {
 
 cudaError_t launch_fg_templates_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
-  k_fg_templates_batch<<<grid, 96, 0, st>>>(b);
+  k_fg_templates_batch<<<grid, kFgTemplateThreads, 0, st>>>(b);
   return cudaGetLastError();
 }
 
