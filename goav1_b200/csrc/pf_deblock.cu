@@ -262,7 +262,7 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
 
 // Batched deblocking: each work item is one 32x8 tile of edge units of one
 // plane of one frame; 256 threads, one edge unit each.
-__global__ void __launch_bounds__(256, 3) k_deblock_batch(BatchArgs b, int dir) {
+__global__ void __launch_bounds__(256, 4) k_deblock_batch(BatchArgs b, int dir) {
   const int stage = dir == 0 ? ST_DEBLOCK_V : ST_DEBLOCK_H;
   const int* base = b.base + stage * (b.n + 1);
   for_each_item(base[b.n], b.counters ? b.counters + stage : nullptr, [&](int item) {
