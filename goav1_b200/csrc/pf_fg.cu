@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(64) k_fg_offsets_batch(BatchArgs b) {
 // thread's rows stay inside one grain block: blocks are 32 or 16 rows high,
 // and a thread's per-column set-up is spread over 16 samples).
 // The plane's scaling table is staged in shared memory per tile.
-__global__ void __launch_bounds__(256, 5) k_fg_apply_batch(BatchArgs b) {
+__global__ void __launch_bounds__(256, 6) k_fg_apply_batch(BatchArgs b) {
   __shared__ uint8_t s_lut[256];
   const int* base = b.base + ST_FG_APPLY * (b.n + 1);
   for_each_item(base[b.n], b.counters ? b.counters + ST_FG_APPLY : nullptr, [&](int item) {
