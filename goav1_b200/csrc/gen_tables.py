@@ -167,7 +167,9 @@ def emit(gauss, params, xby, oneby, upf, blocks, tx, maxtx):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GOAV1_REFERENCE")
+    if not ref:
+        sys.exit("usage: %s <path to a goav1 checkout> (or set GOAV1_REFERENCE)" % sys.argv[0])
     tabs = parse(ref)
     check(*tabs)
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pf_tables.h")

@@ -1395,6 +1395,74 @@ extern "C" void oracle_lpf_line(uint16_t* line16, int bit_depth, int level, int 
   for (int i = 0; i < 16; i++) line16[i] = buf[i];
 }
 
+// The same edge unit with explicit thresholds: E (block limit), I (inner
+// limit) and H (high-edge-variance threshold) at 8-bit scale, as goav1's
+// Filter4/6/8/14Edge tests give them (loopfilter/loopfilter_test.go); wd is
+// the dav1d width class 4, 6, 8 or 16 (the 14-tap filter).
+extern "C" void oracle_lpf_line_thr(uint16_t* line16, int bit_depth, int E, int I, int H, int wd) {
+  std::vector<uint16_t> buf(16 * 4);
+  for (int r = 0; r < 4; r++)
+    for (int i = 0; i < 16; i++) buf[r * 16 + i] = line16[i];
+  Plane pl;
+  pl.data = (uint8_t*)buf.data();
+  pl.stride = 32;
+  pl.bps = 2;
+  pl.w = 16;
+  pl.h = 4;
+  lpf_unit(pl, 8, 0, 0, 1, 1, 0, bit_depth, E, I, H, wd);
+  for (int i = 0; i < 16; i++) line16[i] = buf[i];
+}
+
+extern "C" int oracle_sgr_x_by_xplus1(int z) { return pf_sgr_x_by_xplus1[z < 0 ? 0 : (z > 255 ? 255 : z)]; }
+
+extern "C" void oracle_lf_thresholds(int level, int sharpness, int* E, int* I, int* H) {
+  lf_thresholds(level, sharpness, E, I, H);
+}
+
+// convertChromaDirections on one direction (cdef/filter.go:614-633).
+extern "C" int oracle_cdef_chroma_dir(int dir, int xdec, int ydec) {
+  if (xdec == ydec) return dir;
+  CdefGrid g;
+  memset(&g, 0, sizeof(g));
+  g.dir[0][0] = (uint8_t)dir;
+  std::vector<std::pair<int, int>> one(1, std::make_pair(0, 0));
+  convert_chroma_dirs(g, one, xdec);
+  return g.dir[0][0];
+}
+
+// Film grain on one plane with a given template and scaling table
+// (filmgrain/apply.go:72-343 over every 32-row stripe): src/dst hold the
+// plane's samples as uint16 with `stride` samples per row; luma (the luma
+// plane, luma_stride samples per row) gives chroma its scaling index.
+extern "C" int oracle_fg_apply_plane(const uint16_t* src, uint16_t* dst, int stride, const uint16_t* luma,
+                                     int luma_stride, int frame_w, int frame_h, const int16_t* grain, const uint8_t* lut,
+                                     const pf_film_grain* fg, int plane, int bit_depth, int ss_x, int ss_y) {
+  pf_frame fr;
+  memset(&fr, 0, sizeof(fr));
+  fr.width = frame_w;
+  fr.height = frame_h;
+  fr.bit_depth = (uint8_t)bit_depth;
+  fr.ss_x = (uint8_t)ss_x;
+  fr.ss_y = (uint8_t)ss_y;
+  const int sx = plane ? ss_x : 0, sy = plane ? ss_y : 0;
+  Plane s, d, l;
+  s.data = (uint8_t*)src;
+  d.data = (uint8_t*)dst;
+  s.stride = d.stride = (int64_t)stride * 2;
+  s.bps = d.bps = 2;
+  s.w = d.w = (frame_w + sx) >> sx;
+  s.h = d.h = (frame_h + sy) >> sy;
+  l.data = (uint8_t*)(luma ? luma : src);
+  l.stride = (int64_t)(luma ? luma_stride : stride) * 2;
+  l.bps = 2;
+  l.w = frame_w;
+  l.h = frame_h;
+  FGPlaneCtx pc{s, d, grain, lut};
+  const int bh = 32 >> sy;
+  for (int r = 0; r < (s.h + bh - 1) / bh; r++) fg_stripe(&fr, *fg, plane, r, pc, l);
+  return PF_OK;
+}
+
 extern "C" uint16_t oracle_lfsr_next(uint16_t* reg, int bits) { return lfsr_number(*reg, bits); }
 extern "C" uint16_t oracle_stripe_seed(uint16_t seed, int luma_line) { return stripe_seed(seed, luma_line); }
 extern "C" int oracle_scaling_lut(uint8_t* dst256, const uint8_t* points, int n) {

@@ -43,6 +43,19 @@ void oracle_cdef_filter_block(uint16_t* dst, const uint16_t* in, int in_origin,
 int oracle_cdef_adjust_strength(int strength, int32_t variance);
 /* loopfilter/sb.go:348-446 on a line of 16 samples (q0 at index 8). */
 void oracle_lpf_line(uint16_t* line16, int bit_depth, int level, int sharpness, int wd);
+/* restoration/selfguided.go's x/(x+1) table entry (z clamped to 0..255). */
+int oracle_sgr_x_by_xplus1(int z);
+/* loopfilter/threshold.go:18-47: E (block limit), I (limit), H (hev). */
+void oracle_lf_thresholds(int level, int sharpness, int* E, int* I, int* H);
+/* The same with explicit 8-bit-scale thresholds E, I, H; wd 4, 6, 8 or 16. */
+void oracle_lpf_line_thr(uint16_t* line16, int bit_depth, int E, int I, int H, int wd);
+/* cdef/filter.go:614-633 on one direction. */
+int oracle_cdef_chroma_dir(int dir, int xdec, int ydec);
+/* filmgrain/apply.go:72-343 on one plane (uint16 samples) with a given
+ * template (73x82, stride 82) and scaling table. */
+int oracle_fg_apply_plane(const uint16_t* src, uint16_t* dst, int stride, const uint16_t* luma, int luma_stride,
+                          int frame_w, int frame_h, const int16_t* grain, const uint8_t* lut,
+                          const pf_film_grain* fg, int plane, int bit_depth, int ss_x, int ss_y);
 /* filmgrain/random.go */
 uint16_t oracle_lfsr_next(uint16_t* reg, int bits);
 uint16_t oracle_stripe_seed(uint16_t seed, int luma_line);
@@ -111,6 +124,31 @@ int oracle_lf_build_ordered(const pf_lf_record* rec, int cols, int rows, const i
 void oracle_lf_mask_block(int kind, uint16_t* region, int by4, int bx4, int w4, int h4, int skip, int tx,
                           const uint16_t split[2], uint8_t* a, uint8_t* l, int ssx, int ssy);
 int oracle_lf_block_levels(const pf_lf_levels* p, int mono, const pf_lf_record* r, uint8_t out[4]);
+
+/* ---- the second oracle (oracle/second_oracle.c) ----
+ * Independent restatements of the filter arithmetic: goav1's in-test libaom
+ * restatements and the AV1 specification's formulation. */
+int so_lf_filter(int width, int* samples, int bit_depth, int limit, int blimit, int hev);
+void so_cdef_filter_block(uint16_t* dst, int dst_stride, int dst_origin, const uint16_t* input, int input_origin,
+                          int pri, int sec, int dir, int pri_damping, int sec_damping, int coeff_shift, int width,
+                          int height);
+int so_cdef_find_dir(const uint16_t* img, int stride, int coeff_shift, int32_t* variance);
+int so_cdef_adjust_strength(int strength, int32_t variance);
+int so_cdef_chroma_dir(int dir, int xdec, int ydec);
+void so_wiener(const uint16_t* src, int stride, int origin, uint16_t* dst, int dst_stride, int w, int h,
+               const int16_t* vf7, const int16_t* hf7, int bit_depth);
+void so_sgr_params(int set, int* r0, int* s0, int* r1, int* s1);
+void so_sgr_decode_xq(const int8_t* xqd, int set, int* xq0, int* xq1);
+int so_sgr_x_by_xplus1(int z);
+int so_sgr_one_by_n(int n);
+void so_sgr(const uint16_t* src, int stride, int origin, uint16_t* dst, int dst_stride, int w, int h, int set,
+            const int8_t* xqd, int bit_depth);
+void so_grain_templates(int16_t* luma, int16_t* cb, int16_t* cr, const pf_film_grain* fg, int bit_depth, int ss_x,
+                        int ss_y);
+void so_scaling_lut(uint8_t* lut, const uint8_t (*points)[2], int n);
+void so_grain_apply_plane(const uint16_t* src, uint16_t* dst, int stride, const uint16_t* luma, int luma_stride,
+                          int frame_w, int frame_h, const int16_t* grain, const uint8_t* lut, const pf_film_grain* fg,
+                          int plane, int bit_depth, int ss_x, int ss_y);
 
 #ifdef __cplusplus
 }
