@@ -71,6 +71,7 @@ def lib():
                               C.c_void_p, C.c_uint32]
     L.pf_lr_search.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame),
                                C.POINTER(abi.pf_frame), C.c_void_p, C.c_int32]
+    L.pf_diag_issue_rate.argtypes = [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     if L.pf_abi_version() != 1:
         raise RuntimeError("goav1_b200: ABI version mismatch")
     _lib = L

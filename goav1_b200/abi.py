@@ -3,7 +3,7 @@
 These Structure classes are the Python view of the boundary structs; field
 order and types follow the header exactly.  They carry plain pointers and
 sizes only, so the same layout is what a cgo binding passes from goav1's
-FrameWorkPostFilterContext (see INTEGRATION.md).
+FrameWorkPostFilterContext.
 """
 
 import ctypes as C
@@ -387,4 +387,5 @@ EXPORTED_SYMBOLS = (
     "pf_superres_upscale",
     "pf_frame_apply_superres",
     "pf_lf_build",
+    "pf_diag_issue_rate",
 )

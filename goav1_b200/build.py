@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgoav1pf.so")
 SOURCES = ["pf_api.cu", "pf_deblock.cu", "pf_cdef.cu", "pf_lr.cu", "pf_fg.cu", "pf_grain_static.cu", "pf_search.cu", "pf_mlp.cu", "pf_superres.cu",
-           "pf_lfmask.cu"]
+           "pf_lfmask.cu", "pf_diag.cu"]
 HEADERS = ["pf_common.cuh", "pf_cdef_dev.cuh", "pf_search.cuh", "pf_tables.h", os.path.join("..", "..", "include", "goav1pf.h")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

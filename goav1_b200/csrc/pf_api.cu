@@ -370,8 +370,11 @@ static cudaError_t layout_like(const pf_frame* f, DevBuf& buf, void** ptrs, int6
   return cudaSuccess;
 }
 
-static void build_scaling_lut(uint8_t* dst, const uint8_t (*pts)[2], int n) {
-  // filmgrain/scaling.go:18-48 (BuildScalingLUT).
+namespace pf {
+// The 256-entry scaling table of a piecewise-linear point list
+// (filmgrain/scaling.go:18-48, BuildScalingLUT); also used by
+// pf_film_grain_static.
+void build_scaling_lut(uint8_t* dst, const uint8_t (*pts)[2], int n) {
   memset(dst, 0, 256);
   if (n == 0) return;
   for (int x = 0; x < pts[0][0]; x++) dst[x] = pts[0][1];
@@ -382,6 +385,7 @@ static void build_scaling_lut(uint8_t* dst, const uint8_t (*pts)[2], int n) {
   }
   for (int x = pts[n - 1][0]; x < 256; x++) dst[x] = pts[n - 1][1];
 }
+}  // namespace pf
 
 // The last failing CUDA call of this thread, for pf_status_detail().
 static thread_local char g_detail[256];

@@ -418,7 +418,7 @@ static uint16_t lfsr_step_host(uint16_t reg) {
 cudaError_t fg_upload_tables() {
   cudaError_t e = cudaMemcpyToSymbol(c_gauss, pf_gaussian_sequence, sizeof(pf_gaussian_sequence));
   if (e != cudaSuccess) return e;
-  static uint16_t jump[3][32][16];
+  uint16_t jump[3][32][16];
   int lens[3];
   const int samples[3] = {82 * 73, 44 * 73, 44 * 38};
   for (int t = 0; t < 3; t++) {

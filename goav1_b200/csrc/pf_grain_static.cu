@@ -15,8 +15,11 @@
 // The array is shared by every call on a device and keeps whatever the last
 // call left in it.  Nothing in it has to start at zero: each call rewrites the
 // job record, the stage table, all three templates and every offset it reads.
-// Calls whose work overlaps on the GPU (two streams, or two threads) race on
-// the array; callers must order them, e.g. by issuing them on one stream.
+// The job record and stage table reach the array through a one-CTA kernel
+// that takes them as its by-value argument, so no host buffer is read after
+// the call returns.  Calls whose work overlaps on the GPU (two streams, or two
+// threads) race on the array; callers must order them, e.g. by issuing them
+// on one stream.
 #include <mutex>
 
 #include <string.h>
@@ -25,6 +28,7 @@
 
 namespace pf {
 cudaError_t fg_upload_tables();
+void build_scaling_lut(uint8_t* dst, const uint8_t (*pts)[2], int n);
 cudaError_t launch_fg_templates_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
 cudaError_t launch_fg_offsets_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
 cudaError_t launch_fg_apply_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
@@ -51,21 +55,42 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-uint8_t* g_scratch_addr[kMaxDevices];  // device address of g_grain_scratch, per device
+bool g_tables_loaded[kMaxDevices];  // grain tables in this device's constant memory
 
-// Once per device, with that device current: the device address of the
-// scratch array (host code cannot use the symbol itself as an address) and
-// the grain tables in constant memory.
+// Per call, with the call's device current: the device address of the
+// scratch array (host code cannot use the symbol itself as an address).  The
+// first call on a device also loads the grain tables into constant memory and
+// waits for that upload to land, so a first call made on a non-blocking
+// stream cannot read the tables before they are written.  Tables live in the
+// library's module: after cudaDeviceReset the process must not call this
+// entry point again on that device.
 int setup_device(int dev, uint8_t** out) {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_grain_scratch) != cudaSuccess || !p) return PF_ERR_DEVICE;
   std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_grain_scratch) != cudaSuccess || !p) return PF_ERR_DEVICE;
-    if (fg_upload_tables() != cudaSuccess) return PF_ERR_DEVICE;
-    g_scratch_addr[dev] = (uint8_t*)p;
+  if (!g_tables_loaded[dev]) {
+    if (fg_upload_tables() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return PF_ERR_DEVICE;
+    g_tables_loaded[dev] = true;
   }
-  *out = g_scratch_addr[dev];
+  *out = (uint8_t*)p;
   return PF_OK;
+}
+
+// The job record and the stage prefix table, written into the scratch array
+// by one CTA from its kernel argument.
+struct StaticRecord {
+  FrameJob job;
+  int base[ST_COUNT * 2];
+};
+static_assert(sizeof(FrameJob) % 4 == 0, "record is copied as 32-bit words");
+static_assert(sizeof(StaticRecord) <= 4096, "record must fit the kernel parameter space");
+
+__global__ void k_grain_static_record(StaticRecord r, uint8_t* scratch) {
+  const uint32_t* job = (const uint32_t*)&r.job;
+  uint32_t* dj = (uint32_t*)scratch;
+  for (int i = threadIdx.x; i < (int)(sizeof(FrameJob) / 4); i += blockDim.x) dj[i] = job[i];
+  int* db = (int*)(scratch + kBaseOff);
+  for (int i = threadIdx.x; i < ST_COUNT * 2; i += blockDim.x) db[i] = r.base[i];
 }
 
 DFrame device_frame(const pf_frame* f) {
@@ -86,20 +111,6 @@ DFrame device_frame(const pf_frame* f) {
     d.pl[p].ah = f->plane[p].alloc_height;
   }
   return d;
-}
-
-// The 256-entry scaling table of a piecewise-linear point list (the AV1
-// film-grain scaling function; filmgrain/scaling.go:18-48 in goav1).
-void scaling_table(uint8_t* dst, const uint8_t (*pts)[2], int n) {
-  memset(dst, 0, 256);
-  if (n == 0) return;
-  for (int x = 0; x < pts[0][0]; x++) dst[x] = pts[0][1];
-  for (int i = 0; i + 1 < n; i++) {
-    const int dx = pts[i + 1][0] - pts[i][0], dy = pts[i + 1][1] - pts[i][1];
-    const int64_t slope = (int64_t)dy * ((65536 + (dx >> 1)) / dx);
-    for (int x = 0; x < dx; x++) dst[pts[i][0] + x] = (uint8_t)(pts[i][1] + (int)(((int64_t)x * slope + 32768) >> 16));
-  }
-  for (int x = pts[n - 1][0]; x < 256; x++) dst[x] = pts[n - 1][1];
 }
 
 }  // namespace
@@ -124,8 +135,9 @@ extern "C" int pf_film_grain_static(const pf_frame* ref, const pf_film_grain* fg
   if (st != PF_OK) return st;
 
   // The one-frame job: film grain only.
-  FrameJob J;
-  memset(&J, 0, sizeof(J));
+  StaticRecord R;
+  memset(&R, 0, sizeof(R));
+  FrameJob& J = R.job;
   J.io = device_frame(ref);
   J.disp = device_frame(display);
   FgArgs& a = J.fg;
@@ -143,13 +155,13 @@ extern "C" int pf_film_grain_static(const pf_frame* ref, const pf_film_grain* fg
     a.offsets = scratch + kOffsetsOff;
     a.off_rows = rows;
     a.off_cols = cols;
-    scaling_table(a.lut[0], fg->y_points, fg->num_y_points);
+    build_scaling_lut(a.lut[0], fg->y_points, fg->num_y_points);
     if (fg->chroma_scaling_from_luma) {
       memcpy(a.lut[1], a.lut[0], 256);
       memcpy(a.lut[2], a.lut[0], 256);
     } else {
-      scaling_table(a.lut[1], fg->cb_points, fg->num_cb_points);
-      scaling_table(a.lut[2], fg->cr_points, fg->num_cr_points);
+      build_scaling_lut(a.lut[1], fg->cb_points, fg->num_cb_points);
+      build_scaling_lut(a.lut[2], fg->cr_points, fg->num_cr_points);
     }
     a.scaling_shift = fg->scaling_shift;
     a.overlap = fg->overlap;
@@ -186,17 +198,13 @@ extern "C" int pf_film_grain_static(const pf_frame* ref, const pf_film_grain* fg
     tiles += J.fg_tx[p] * J.fg_ty[p];
   }
   counts[ST_FG_APPLY] = tiles;
-  int base[ST_COUNT * 2];
   for (int k = 0; k < ST_COUNT; k++) {
-    base[2 * k] = 0;
-    base[2 * k + 1] = counts[k];
+    R.base[2 * k] = 0;
+    R.base[2 * k + 1] = counts[k];
   }
-  // Pageable host sources: each copy returns once its bytes are staged, so
-  // the stack records above may go out of scope afterwards.
   const cudaStream_t s = (cudaStream_t)stream;
-  if (cudaMemcpyAsync(scratch, &J, sizeof(J), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(scratch + kBaseOff, base, sizeof(base), cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return PF_ERR_DEVICE;
+  k_grain_static_record<<<1, 128, 0, s>>>(R, scratch);
+  if (cudaGetLastError() != cudaSuccess) return PF_ERR_DEVICE;
   BatchArgs b;
   b.jobs = (const FrameJob*)scratch;
   b.base = (const int*)(scratch + kBaseOff);

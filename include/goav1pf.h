@@ -496,9 +496,15 @@ int pf_lf_build(pf_ctx* ctx, const pf_lf_record* records, int32_t mi_cols, int32
  *   - Frames with more than PF_GRAIN_STATIC_MAX_BLOCKS 32x32 luma blocks
  *     (ceil(width/32) * ceil(height/32), e.g. 8192x8192) are rejected with
  *     PF_ERR_SHORT_BUFFER before anything is queued.
- *   - The first call on a device sets up that device (looks up the array's
- *     device address and loads the grain tables into constant memory, a
- *     synchronous copy); make that first call before any stream capture.
+ *   - The first call on a device sets up that device: it loads the grain
+ *     tables into constant memory and waits for the device to finish
+ *     (cudaDeviceSynchronize), so make that first call before any stream
+ *     capture.  Every call looks up the array's device address (host code
+ *     cannot use the symbol as an address).  The tables live in the library's
+ *     module, so after cudaDeviceReset this entry point must not be called
+ *     again on that device.
+ *   - The job record reaches the array as a kernel argument: nothing the
+ *     call reads from host memory is needed after it returns.
  *   - Work is queued on `stream` (a cudaStream_t, or NULL for the legacy
  *     default stream); the call returns without waiting for it.
  *   - Every call shares the one array and it keeps the last call's contents;
@@ -662,6 +668,18 @@ typedef struct pf_lr_search_unit {
 } pf_lr_search_unit;
 int pf_lr_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const pf_frame* restored,
                  pf_lr_search_unit* units, int32_t max_units);
+
+/* ---- measurement ----
+ * No counterpart in the reference.  The warp-instruction issue rate of the
+ * current device, measured by a fixed inline-PTX instruction stream over every
+ * SM (kind 0: integer logic ops only, the ALU pipe; kind 1: 32-bit integer
+ * multiply-adds only; kind 2: the two interleaved; kind 3: FP32 fused
+ * multiply-adds, a pipe that takes an instruction every cycle, so its rate
+ * is the issue ceiling).  The post-filter kernels are bound by instruction
+ * issue, not by DRAM bytes, so their roofline is reported against this
+ * ceiling as well as against copy bandwidth.  Synchronous; allocates and
+ * frees a small buffer.  *ms receives the fastest launch's time. */
+int pf_diag_issue_rate(int32_t kind, double* warp_inst_per_s, double* ms);
 
 #ifdef __cplusplus
 }
