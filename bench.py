@@ -700,6 +700,10 @@ def main():
         from goav1_b200 import learned as _l
 
         model = _l.load_model()
+        from goav1_b200.postfilter import cdef_plan_picture
+
+        plan5 = cdef_plan_picture(5, True)
+        plan8 = cdef_plan_picture(8, False, is_base=True)
         rows = []
         for seed, src, rec, sside, sigma in _l.search_frames(range(2000, 2000 + args.search_frames), 1920, 1080,
                                                              workers=min(8, args.search_frames)):
@@ -719,8 +723,14 @@ def main():
             te = timed(lambda: runner.cdef_search(sp, rp, ns, q, _l.LAMBDA, want_mse=False))
             tl = timed(lambda: runner.cdef_search_learned(sp, rp, ns, q, _l.LAMBDA, model, want_mse=False,
                                                          want_stats=False))
+            # The levels goav1's real-time encoder runs: 5 on intra pictures,
+            # 8 on camera-content inter pictures (base layer: the level's four
+            # trials, luma rows every 4th, chroma presets copying luma's; on
+            # other layers level 8 takes the reference's strengths unsearched).
+            t5 = timed(lambda: runner.cdef_search_ex(sp, rp, ns, q, _l.LAMBDA, plan5.ctrls, want_mse=False))
+            t8 = timed(lambda: runner.cdef_search_ex(sp, rp, ns, q, _l.LAMBDA, plan8.ctrls, want_mse=False))
             base = _l.luma_sse(r0, i0, m0)
-            rows.append(dict(nfb=m0.shape[1], te=te, tl=tl, inc=_l.luma_sse(r1, i1, m0) / base - 1,
+            rows.append(dict(nfb=m0.shape[1], te=te, tl=tl, t5=t5, t8=t8, inc=_l.luma_sse(r1, i1, m0) / base - 1,
                              blocks=st.blocks, fbl=st.fallback_luma, fbc=st.fallback_chroma,
                              trials=(st.trials_luma * 4096 + st.trials_chroma * 2048) / (st.blocks * 64 * 6144)))
         nfb = sum(r["nfb"] for r in rows)
@@ -731,7 +741,15 @@ def main():
                "{2,4,8}, device-resident, lambda %g" % (len(rows), 1999 + len(rows), _l.LAMBDA))
         search = {"metric": "CDEF search blocks/s", "value": nfb / te, "unit": "blocks/s",
                   "ms_per_frame": te / len(rows) * 1e3,
-                  "config": "level-1 exhaustive (64 luma x 64 chroma strengths) + greedy preset selection; " + cfg}
+                  "config": "level-1 exhaustive (64 luma x 64 chroma strengths) + greedy preset selection; " + cfg,
+                  "rtc_levels": {
+                      "level5_intra": {"value": nfb / sum(r["t5"] for r in rows), "unit": "blocks/s",
+                                       "ms_per_frame": sum(r["t5"] for r in rows) / len(rows) * 1e3,
+                                       "trials": plan5.ctrls.count},
+                      "level8_inter": {"value": nfb / sum(r["t8"] for r in rows), "unit": "blocks/s",
+                                       "ms_per_frame": sum(r["t8"] for r in rows) / len(rows) * 1e3,
+                                       "trials": plan8.ctrls.count, "luma_row_subsampling": 4,
+                                       "note": "base-layer inter picture"}}}
         learned_leg = {"metric": "learned CDEF search blocks/s", "value": nfb / tl, "unit": "blocks/s",
                        "ms_per_frame": tl / len(rows) * 1e3, "speedup_vs_exhaustive": te / tl,
                        "luma_sse_increase_mean": float(np.mean([r["inc"] for r in rows])),

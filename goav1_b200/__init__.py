@@ -72,7 +72,13 @@ def lib():
     L.pf_lr_search.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame),
                                C.POINTER(abi.pf_frame), C.c_void_p, C.c_int32]
     L.pf_diag_issue_rate.argtypes = [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
-    if L.pf_abi_version() != 1:
+    L.pf_cdef_search_level_rtc.argtypes = [C.c_int32, C.c_int32]
+    L.pf_cdef_plan_picture.argtypes = [C.c_int32] * 4 + [C.POINTER(abi.pf_cdef_ref_strengths), C.c_int32,
+                                                         C.POINTER(abi.pf_cdef_plan)]
+    L.pf_cdef_search_ex.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame), C.c_void_p,
+                                    C.POINTER(abi.pf_cdef_search_params), C.POINTER(abi.pf_cdef_search_ctrls),
+                                    C.c_void_p, C.c_void_p, C.POINTER(abi.pf_cdef_search_result)]
+    if L.pf_abi_version() != 2:
         raise RuntimeError("goav1_b200: ABI version mismatch")
     _lib = L
     return L

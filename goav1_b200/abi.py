@@ -175,6 +175,7 @@ class pf_config(C.Structure):
         ("timing", C.c_int32),
         ("max_width", C.c_int64),
         ("max_height", C.c_int64),
+        ("wait_timeout_us", C.c_int64),
     ]
 
 
@@ -203,6 +204,39 @@ class pf_cdef_search_result(C.Structure):
         ("uv_strength", C.c_uint8 * 8),
         ("reserved", C.c_uint8 * 2),
         ("cost", C.c_double),
+    ]
+
+
+PF_CDEF_MAX_TRIALS = 64
+PF_CDEF_NOT_A_TRIAL = 0x7FFFFFFF
+
+
+class pf_cdef_search_ctrls(C.Structure):
+    _fields_ = [
+        ("count", C.c_int32),
+        ("y", C.c_int8 * PF_CDEF_MAX_TRIALS),
+        ("uv", C.c_int8 * PF_CDEF_MAX_TRIALS),
+        ("subsampling", C.c_int32),
+        ("uv_from_y", C.c_int32),
+    ]
+
+
+class pf_cdef_ref_strengths(C.Structure):
+    _fields_ = [
+        ("count", C.c_uint8),
+        ("y", C.c_uint8 * 8),
+        ("uv", C.c_uint8 * 8),
+    ]
+
+
+class pf_cdef_plan(C.Structure):
+    _fields_ = [
+        ("on", C.c_int32),
+        ("search", C.c_int32),
+        ("y_strength", C.c_uint8),
+        ("uv_strength", C.c_uint8),
+        ("reserved", C.c_uint8 * 2),
+        ("ctrls", pf_cdef_search_ctrls),
     ]
 
 
@@ -388,4 +422,7 @@ EXPORTED_SYMBOLS = (
     "pf_frame_apply_superres",
     "pf_lf_build",
     "pf_diag_issue_rate",
+    "pf_cdef_search_level_rtc",
+    "pf_cdef_plan_picture",
+    "pf_cdef_search_ex",
 )

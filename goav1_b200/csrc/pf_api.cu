@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "pf_common.cuh"
+#include "pf_wait.h"
 
 namespace pf {
 cudaError_t launch_deblock_batch(const BatchArgs& b, int total, int grid, int dir, cudaStream_t st);
@@ -98,6 +99,7 @@ using PinnedBytes = std::vector<uint8_t, PinnedAlloc<uint8_t>>;
 struct pf_ctx {
   int device = 0;
   int sm_count = 148;
+  int64_t wait_timeout_us = 0;    // 0: synchronous calls block; else PF_ERR_TIMEOUT at the deadline
   cudaStream_t stream = nullptr;  // main stream (returned by pf_stream)
   cudaStream_t side = nullptr;    // film-grain templates/offsets overlap the chain here
   int timing = 0;
@@ -407,6 +409,63 @@ static void last_error(cudaError_t e, const char* expr, int line) {
 
 extern "C" const char* pf_status_detail(void) { return g_detail; }
 
+// A synchronous call's wait on its own device work: blocking, or polled with
+// the context's deadline (pf_config.wait_timeout_us).  PF_OK, PF_ERR_TIMEOUT
+// (the work stays queued) or PF_ERR_DEVICE.
+template <class Q, class B>
+static int ctx_wait(pf_ctx* c, Q query, B block, const char* what, int line) {
+  if (c->wait_timeout_us <= 0) {
+    const cudaError_t e = block();
+    if (e != cudaSuccess) {
+      last_error(e, what, line);
+      return PF_ERR_DEVICE;
+    }
+    return PF_OK;
+  }
+  cudaError_t failed = cudaSuccess;
+  const int r = wait_until(
+      [&]() {
+        const cudaError_t e = query();
+        if (e == cudaSuccess) return (int)kWaitReady;
+        if (e == cudaErrorNotReady) {
+          cudaGetLastError();  // not an error: keep it out of later launch checks
+          return (int)kWaitPending;
+        }
+        failed = e;
+        return (int)kWaitFailed;
+      },
+      c->wait_timeout_us);
+  if (r == kWaitTimedOut) {
+    snprintf(g_detail, sizeof(g_detail), "%s at pf_api.cu:%d: still running after %lld us", what, line,
+             (long long)c->wait_timeout_us);
+    return PF_ERR_TIMEOUT;
+  }
+  if (r == kWaitError) {
+    last_error(failed, what, line);
+    return PF_ERR_DEVICE;
+  }
+  return PF_OK;
+}
+
+static int wait_stream(pf_ctx* c, cudaStream_t st, int line) {
+  return ctx_wait(
+      c, [&]() { return cudaStreamQuery(st); }, [&]() { return cudaStreamSynchronize(st); }, "stream wait", line);
+}
+
+static int wait_event(pf_ctx* c, cudaEvent_t ev, int line) {
+  return ctx_wait(
+      c, [&]() { return cudaEventQuery(ev); }, [&]() { return cudaEventSynchronize(ev); }, "event wait", line);
+}
+
+#define CKW(expr)                  \
+  do {                             \
+    const int _w = (expr);         \
+    if (_w != PF_OK) return _w;    \
+  } while (0)
+
+// The other entry points' waits (pf_search.cu, pf_lr.cu, ...).
+int pf_internal_wait(pf_ctx* c, void* stream) { return wait_stream(c, (cudaStream_t)stream, __LINE__); }
+
 extern "C" int pf_abi_version(void) { return PF_ABI_VERSION; }
 
 extern "C" const char* pf_status_string(int s) {
@@ -443,9 +502,14 @@ extern "C" pf_ctx* pf_create(const pf_config* cfg, int* status) {
     if (status) *status = PF_ERR_DEVICE;
     return nullptr;
   }
+  if (cfg && cfg->wait_timeout_us < 0) {
+    if (status) *status = PF_ERR_INVALID_ARG;
+    return nullptr;
+  }
   pf_ctx* c = new pf_ctx();
   c->device = dev;
   c->timing = cfg ? cfg->timing : 0;
+  c->wait_timeout_us = cfg ? cfg->wait_timeout_us : 0;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess || lr_upload_tables() != cudaSuccess ||
       fg_upload_tables() != cudaSuccess) {
     delete c;
@@ -502,7 +566,7 @@ extern "C" void pf_destroy(pf_ctx* c) {
 
 extern "C" int pf_sync(pf_ctx* c) {
   if (!c) return PF_ERR_INVALID_ARG;
-  return cudaStreamSynchronize(c->stream) == cudaSuccess ? PF_OK : PF_ERR_DEVICE;
+  return wait_stream(c, c->stream, __LINE__);
 }
 
 extern "C" void* pf_stream(pf_ctx* c) { return c ? (void*)c->stream : nullptr; }
@@ -919,7 +983,7 @@ static int replay_or_capture(pf_ctx* c, int n, bool fg) {
       return PF_ERR_DEVICE;
     CK(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
   } else {
-    CK(cudaEventSynchronize(g.done));  // the slot's previous run has read its tables
+    CKW(wait_event(c, g.done, __LINE__));  // the slot's previous run has read its tables
   }
   memcpy(g.pjobs, c->hjobs.data(), nj);
   memcpy(g.pbase, c->hbase.data(), nb);
@@ -1137,7 +1201,7 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
   if (f->memory == PF_MEM_HOST) CK(copy_planes(f, r.io, r.ioStride, false, c->stream));
   if (wantDisp && display->memory == PF_MEM_HOST) CK(copy_planes(display, r.dp, r.dStride, false, c->stream));
   if (f->memory == PF_MEM_HOST || (wantDisp && display->memory == PF_MEM_HOST) || c->timing) {
-    CK(cudaStreamSynchronize(c->stream));
+    CKW(wait_stream(c, c->stream, __LINE__));
     read_stage_times(c, stats);
   }
   CK(cudaGetLastError());
@@ -1189,7 +1253,7 @@ static int run_host_pipeline(pf_ctx* c, const pf_batch_item* items, int n, pf_st
   CK(c->arena.ensure(maxArena + 256));
   for (pf_ctx::HostSlot& h : c->hslot)
     if (h.dside.n < maxSide + 256) {
-      if (h.used) CK(cudaEventSynchronize(h.comp));
+      if (h.used) CKW(wait_event(c, h.comp, __LINE__));
       CK(h.dside.ensure(maxSide + 256));
     }
   if (stats) memset(stats, 0, sizeof(*stats));
@@ -1198,7 +1262,7 @@ static int run_host_pipeline(pf_ctx* c, const pf_batch_item* items, int n, pf_st
     pf_ctx::HostSlot& h = c->hslot[k % 3];
     const int i0 = k * chunk, m = std::min(chunk, n - i0);
     // The slot's tables were read by its previous chunk's launch.
-    if (h.used) CK(cudaEventSynchronize(h.comp));
+    if (h.used) CKW(wait_event(c, h.comp, __LINE__));
     size_t ioBytes = 0, dBytes = 0;
     for (int i = 0; i < m; i++) {
       const pf_batch_item& it = items[i0 + i];
@@ -1207,7 +1271,7 @@ static int run_host_pipeline(pf_ctx* c, const pf_batch_item* items, int n, pf_st
       if ((it.side->stages & PF_STAGE_FILM_GRAIN) && it.display)
         dBytes += host_frame_layout(it.display, nullptr, nullptr, st);
     }
-    if (h.used && (ioBytes > h.io.n || dBytes > h.disp.n)) CK(cudaEventSynchronize(h.down));
+    if (h.used && (ioBytes > h.io.n || dBytes > h.disp.n)) CKW(wait_event(c, h.down, __LINE__));
     CK(h.io.ensure(ioBytes + 256));
     CK(h.disp.ensure(dBytes + 256));
     if (h.used) CK(cudaStreamWaitEvent(c->h2d, h.down, 0));
@@ -1261,8 +1325,8 @@ static int run_host_pipeline(pf_ctx* c, const pf_batch_item* items, int n, pf_st
     CK(cudaEventRecord(h.down, c->d2h));
     h.used = true;
   }
-  CK(cudaStreamSynchronize(c->d2h));
-  CK(cudaStreamSynchronize(c->stream));
+  CKW(wait_stream(c, c->d2h, __LINE__));
+  CKW(wait_stream(c, c->stream, __LINE__));
   read_stage_times(c, stats);
   CK(cudaGetLastError());
   return PF_OK;
@@ -1396,7 +1460,7 @@ extern "C" int pf_frame_apply_superres(pf_ctx* c, const pf_frame* coded, const p
     CK(down(up, uio, ust));
     if (wantDisp) CK(down(display, dio, dst3));
   }
-  CK(cudaStreamSynchronize(cs));
+  CKW(wait_stream(c, cs, __LINE__));
   if (stats) {
     stats->completed |= done;
     read_stage_times(c, stats);
@@ -1469,7 +1533,7 @@ extern "C" int pf_batch_apply(pf_ctx* c, const pf_batch_item* items, int32_t n, 
   bool hostSide = false;
   for (int i = 0; i < n; i++) hostSide |= items[i].side->side_memory == PF_MEM_HOST;
   if (hostSide || c->timing) {
-    CK(cudaStreamSynchronize(c->stream));
+    CKW(wait_stream(c, c->stream, __LINE__));
     read_stage_times(c, stats);
   }
   CK(cudaGetLastError());

@@ -8,11 +8,12 @@
 // apply.go:72-343, :414-546 and blend.go:16-25 (per-32x32 block offsets drawn
 // in order from each stripe's LFSR, overlap blends, noise and clipping).
 //
-// GPU shape: the 82x73 templates are generated by one CTA per frame.  The
-// Gaussian fill is split over 32 lanes: the LFSR is linear over GF(2)^16, so
-// lane k starts from M^(kL) * seed (jump matrices precomputed on the host) and
-// walks its L draws; the AR filter runs as a wavefront over t = x + 4y (every
-// AR input of sample (y, x) has a smaller t), one warp per template.  Offsets
+// GPU shape: the 82x73 templates are generated by one 3-warp CTA per frame.
+// The Gaussian fill is split over 32 lanes: the LFSR is linear over
+// GF(2)^16, so lane k starts from M^(kL) * seed (jump matrices precomputed on
+// the host) and walks its L draws; the AR filter runs as a wavefront over
+// t = x + 4y (every AR input of sample (y, x) has a smaller t), one warp per
+// template, rows in lanes, neighbours by warp shuffles.  Offsets
 // come from one thread per 32-row stripe.  The apply is one thread per output
 // sample, 64x16-sample tiles per CTA.
 #include "pf_common.cuh"
@@ -33,25 +34,27 @@ __device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
 }
 
 // AR recursion of one template (luma.go:83-158 / chroma.go:92-199 generic
-// form) as a wavefront: every thread of the CTA owns one template row
-// (y = 3 + r) and all take the same steps, a barrier after each.  Row y
-// computes column t - 4y at step t, so every causal neighbour (rows above up
-// to column x + LAG, LAG <= 3) was written at an earlier step.  A row's
-// causal window slides along it in registers: each step reads the LAG new
-// samples of the rows above and takes the row's own previous outputs from
-// registers.  The LAG is a template argument: the coefficients sit in
-// registers and the tap loops unroll.  Threads whose row is outside the
-// template (or whose plane does not run) only take the barriers.
-constexpr int kFgTemplateThreads = 192;
+// form), run by one warp as a wavefront with no CTA barrier.  The template's
+// AR rows are taken in bands of 32 rows, one row per lane; at step t lane r
+// (row y) handles column x = t - 4r, so the neighbour it needs from row y-d
+// at column x + LAG was produced by lane r-d at step t - 4d + LAG.  Every
+// lane keeps a short history H of its own outputs and the neighbours come
+// across by __shfl_up_sync (lanes r < d read the rows above the band, which
+// are final, from shared memory); each row's 2*LAG+1-wide window of the rows
+// above and its own LAG previous outputs slide in registers.  Only the
+// shuffle from the lane directly above is on the loop-carried path.  A lane
+// outside the AR columns passes the template's value through unchanged, so
+// the windows always hold the template as it stands.  Bands run one after
+// the other; the LAG is a template argument (coefficients in registers,
+// unrolled taps).
+constexpr int kFgTemplateThreads = 96;
 
 template <int LAG>
-__device__ void ar_rows(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h, int r,
-                        bool run) {
+__device__ void ar_warp(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h) {
   constexpr int kTaps = 2 * LAG * (LAG + 1);  // causal neighbours before the centre
   constexpr int W = 2 * LAG + 1;
-  constexpr int LU = LAG > 0 ? LAG : 1;
-  const int y = 3 + r;
-  const bool mine = run && y < h;
+  constexpr int HL = 3 * LAG > 0 ? 3 * LAG : 1;  // history: the outputs of steps t-1 .. t-3*LAG
+  const int lane = threadIdx.x & 31;
   const int cs = p.coeff_shift, ro = 1 << (cs - 1);
   const int gmin = -(1 << (p.bd - 1)), gmax = (1 << (p.bd - 1)) - 1;
   int co[kTaps + 1];
@@ -59,58 +62,72 @@ __device__ void ar_rows(int16_t* g, const int16_t* luma, const FgTemplateArgs& p
   for (int i = 0; i <= kTaps; i++) co[i] = p.coeffs[plane][i];
   const bool lumaTerm = plane != 0 && p.num_y_points != 0;
   const int sx = plane ? p.ssx : 0, sy = plane ? p.ssy : 0;
-  int up[LU][W];  // rows y - LAG .. y - 1, columns x - LAG .. x + LAG
-  int left[LU];   // row y, columns x - LAG .. x - 1
-  const int tmax = (w - 4) + 4 * (h - 1);
-  for (int t = 3 + 4 * 3; t <= tmax; t++) {
-    const int x = t - 4 * y;
-    if (mine && x >= 3 && x < w - 3) {
-      if (x == 3) {
+  for (int y0 = 3; y0 < h; y0 += 32) {
+    const int y = y0 + lane;
+    const bool row = y < h;
+    int win[LAG > 0 ? LAG : 1][W];  // win[d-1][c]: row y-d, column x-LAG+c
+    int H[HL];
 #pragma unroll
-        for (int dr = 0; dr < LAG; dr++)
+    for (int d = 0; d < (LAG > 0 ? LAG : 1); d++)
 #pragma unroll
-          for (int dc = 0; dc < W; dc++) up[dr][dc] = g[(y - LAG + dr) * kGW + x - LAG + dc];
+      for (int c = 0; c < W; c++) win[d][c] = 0;
 #pragma unroll
-        for (int dc = 0; dc < LAG; dc++) left[dc] = g[y * kGW + x - LAG + dc];
-      } else {
+    for (int k = 0; k < HL; k++) H[k] = 0;
+    const int tend = 4 * 31 + w;
+    for (int t = -LAG; t < tend; t++) {
+      const int x = t - 4 * lane;
+      const int xn = x + LAG;  // the column entering the windows
 #pragma unroll
-        for (int dr = 0; dr < LAG; dr++) {
+      for (int d = 1; d <= LAG; d++) {
+        int v = __shfl_up_sync(0xffffffffu, H[4 * d - LAG - 1], d);
+        if (lane < d) v = (xn >= 0 && xn < w) ? g[(y - d) * kGW + xn] : 0;
 #pragma unroll
-          for (int dc = 0; dc + 1 < W; dc++) up[dr][dc] = up[dr][dc + 1];
-          up[dr][W - 1] = g[(y - LAG + dr) * kGW + x + LAG];
+        for (int c = 0; c + 1 < W; c++) win[d - 1][c] = win[d - 1][c + 1];
+        win[d - 1][W - 1] = v;
+      }
+      int out = 0;
+      if (row && x >= 0 && x < w) {
+        const int g0 = g[y * kGW + x];
+        out = g0;
+        if (x >= 3 && x < w - 3) {
+          int sum = 0;
+#pragma unroll
+          for (int d = 1; d <= LAG; d++) {
+            int part = 0;
+#pragma unroll
+            for (int c = 0; c < W; c++) part += co[(LAG - d) * W + c] * win[d - 1][c];
+            sum += part;
+          }
+#pragma unroll
+          for (int c = 0; c < LAG; c++) sum += co[LAG * W + c] * H[LAG - 1 - c];
+          if (lumaTerm) {
+            const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
+            int s = luma[ly * kGW + lx];
+            if (sx) s += luma[ly * kGW + lx + 1];
+            if (sy) {
+              s += luma[(ly + 1) * kGW + lx];
+              if (sx) s += luma[(ly + 1) * kGW + lx + 1];
+            }
+            sum += rpow2(s, sx + sy) * co[kTaps];
+          }
+          out = iclip(g0 + ((sum + ro) >> cs), gmin, gmax);
+          g[y * kGW + x] = (int16_t)out;
         }
       }
-      int sum = 0;
 #pragma unroll
-      for (int dr = 0; dr < LAG; dr++)
-#pragma unroll
-        for (int dc = 0; dc < W; dc++) sum += co[dr * W + dc] * up[dr][dc];
-#pragma unroll
-      for (int dc = 0; dc < LAG; dc++) sum += co[LAG * W + dc] * left[dc];
-      if (lumaTerm) {
-        const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
-        int s = 0;
-        for (int dy = 0; dy <= sy; dy++)
-          for (int dx = 0; dx <= sx; dx++) s += luma[(ly + dy) * kGW + lx + dx];
-        sum += rpow2(s, sx + sy) * co[kTaps];
-      }
-      const int v = iclip(g[y * kGW + x] + ((sum + ro) >> cs), gmin, gmax);
-      g[y * kGW + x] = (int16_t)v;
-#pragma unroll
-      for (int dc = 0; dc + 1 < LAG; dc++) left[dc] = left[dc + 1];
-      if (LAG > 0) left[LU - 1] = v;
+      for (int k = HL - 1; k > 0; k--) H[k] = H[k - 1];
+      H[0] = out;
     }
-    __syncthreads();
+    __syncwarp();  // this band's rows are final for the next band's first lanes
   }
 }
 
-__device__ void ar_rows_lag(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h, int r,
-                            bool run) {
+__device__ void ar_warp_lag(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h) {
   switch (p.lag) {
-    case 0: ar_rows<0>(g, luma, p, plane, w, h, r, run); break;
-    case 1: ar_rows<1>(g, luma, p, plane, w, h, r, run); break;
-    case 2: ar_rows<2>(g, luma, p, plane, w, h, r, run); break;
-    default: ar_rows<3>(g, luma, p, plane, w, h, r, run); break;
+    case 0: ar_warp<0>(g, luma, p, plane, w, h); break;
+    case 1: ar_warp<1>(g, luma, p, plane, w, h); break;
+    case 2: ar_warp<2>(g, luma, p, plane, w, h); break;
+    default: ar_warp<3>(g, luma, p, plane, w, h); break;
   }
 }
 
@@ -171,16 +188,12 @@ __device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, 
     __syncwarp();
   }
   __syncthreads();
-  // Luma on every thread (row 3 + tid), then Cb (threads 0..95) and Cr
-  // (96..191) side by side; each call's step count is uniform.
-  if (p.num_y_points != 0 && p.lag != 0) ar_rows_lag(s_g[0], nullptr, p, 0, kGW, kGH, threadIdx.x, true);
+  // Luma on warp 0; then Cb and Cr side by side on warps 1 and 2 (their
+  // luma term reads the finished luma template).
+  if (warp == 0 && p.num_y_points != 0 && p.lag != 0) ar_warp_lag(s_g[0], nullptr, p, 0, kGW, kGH);
   __syncthreads();
-  const bool runC[3] = {false, p.active[1] && !(p.lag == 0 && p.num_y_points == 0),
-                        p.active[2] && !(p.lag == 0 && p.num_y_points == 0)};
-  if (runC[1] || runC[2]) {
-    const int pl = threadIdx.x < 96 ? 1 : 2;
-    ar_rows_lag(s_g[pl], s_g[0], p, pl, cw, ch, threadIdx.x % 96, runC[pl]);
-  }
+  const bool runC = warp >= 1 && warp <= 2 && p.active[warp] && !(p.lag == 0 && p.num_y_points == 0);
+  if (runC) ar_warp_lag(s_g[warp], s_g[0], p, warp, cw, ch);
   __syncthreads();
   for (int pl = 0; pl < 3; pl++)
     if (outs[pl])

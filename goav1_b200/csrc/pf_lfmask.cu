@@ -450,6 +450,7 @@ __global__ void __launch_bounds__(1024) k_lf_build(MapArgs a) {
 }  // namespace pf
 
 void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
+int pf_internal_wait(pf_ctx* c, void* stream);  // pf_api.cu: blocking or bounded by the context's deadline
 void* pf_internal_stream(pf_ctx* c);
 void* pf_internal_pinned(pf_ctx* c, size_t bytes);
 
@@ -523,8 +524,9 @@ extern "C" int pf_lf_build(pf_ctx* ctx, const pf_lf_record* records, int32_t col
   if (e == cudaSuccess) e = cudaMemcpyAsync(hostErr, a.rowErr, (size_t)rows * 8, cudaMemcpyDeviceToHost, st);
   if (hostOut && e == cudaSuccess) e = cudaMemcpyAsync(masks, a.masks, maskB, cudaMemcpyDeviceToHost, st);
   if (hostOut && e == cudaSuccess) e = cudaMemcpyAsync(level_cache, a.levels, lcB, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return PF_ERR_DEVICE;
+  const int w = pf_internal_wait(ctx, st);
+  if (w != PF_OK) return w;
   unsigned long long err = ~0ull;
   for (int r = 0; r < rows; r++) err = hostErr[r] < err ? hostErr[r] : err;
   if (err == ~0ull) return PF_OK;

@@ -723,6 +723,7 @@ static int lrs_check(const pf_frame* f, const pf_frame* ref) {
 }  // namespace pf
 
 void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
+int pf_internal_wait(pf_ctx* c, void* stream);  // pf_api.cu: blocking or bounded by the context's deadline
 void* pf_internal_stream(pf_ctx* c);
 void* pf_internal_pinned(pf_ctx* c, size_t bytes);
 
@@ -808,7 +809,7 @@ extern "C" int pf_lr_search(pf_ctx* ctx, const pf_frame* source, const pf_frame*
                           cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && units)
     e = cudaMemcpyAsync(units, a.out, sizeof(pf_lr_search_unit) * n, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  return e == cudaSuccess ? PF_OK : PF_ERR_DEVICE;
+  if (e != cudaSuccess) return PF_ERR_DEVICE;
+  return pf_internal_wait(ctx, st);
 }
 

@@ -1,8 +1,13 @@
 // pf_search.cu - the encoder's CDEF strength search on the GPU.
 //
-// Follows goav1's cdefSearcher (internal/av1/encoder/cdef_search.go) at
-// level-1 controls (:98-110: all 64 packed strengths in the svtPfGI order,
-// chroma the same list, row subsampling 1):
+// Follows goav1's cdefSearcher (internal/av1/encoder/cdef_search.go) over a
+// trial list: level 1's (:98-110: all 64 packed strengths in the svtPfGI
+// order, chroma the same list, row subsampling 1) for pf_cdef_search and the
+// learned search, any level's for pf_cdef_search_ex (chroma trials the level
+// does not measure, luma rows every subsamplingFactor-th with the SSE scaled
+// back).  Trial indices past the list hold kNotATrial, which no selection
+// step picks, so the selection over all 64 indices equals finish's over the
+// list (:892-899: endGI = len(filterMap)):
 //   k_cdef_search   one CTA per 64x64 filter block: the noskip 8x8 list
 //                   (computeCDEFList, :410-447), the VeryLarge-padded input
 //                   (loadCDEFInput, :479-506), luma directions from the
@@ -60,16 +65,19 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   uint64_t* m0 = a.mse + (size_t)fb * 64;
   uint64_t* m1 = a.mse + (size_t)nfb * 64 + (size_t)fb * 64;
   const uint64_t listed = fb_listed(a, fb, lr, lc);
+  const int count = a.trials.count;
   if (listed == 0) {
     if (tid < 64) {
-      m0[tid] = 0;
-      m1[tid] = 0;
+      m0[tid] = tid < count ? 0 : (uint64_t)kNotATrial;
+      m1[tid] = tid < count ? 0 : (uint64_t)kNotATrial;
     }
     if (tid == 0) a.skip[fb] = 1;
     return;
   }
-  const uint64_t mask0 = a.tmask ? a.tmask[2 * fb] : ~0ull;
-  const uint64_t mask1 = a.tmask ? a.tmask[2 * fb + 1] : ~0ull;
+  const uint64_t listMask = count >= 64 ? ~0ull : (1ull << count) - 1;
+  const uint64_t mask0 = a.tmask ? a.tmask[2 * fb] : listMask;
+  const uint64_t mask1 = a.tmask ? a.tmask[2 * fb + 1] : a.trials.uvMask;
+  const int ssY = a.trials.ss;
   if (tid == 0) {
     a.skip[fb] = 0;
     int c0 = 0, c1 = 0;
@@ -178,10 +186,12 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
     __syncthreads();
     const int ngrp = (h + 7) >> 3;
     const int ntask = s_cnt[P] * ngrp;
+    // Luma rows every ssY-th (the subsampled search), chroma every row.
+    const int step = P ? 1 : ssY;
     for (int task = warp; task < ntask; task += 8) {
       const int g = s_list[P][task / ngrp];
       const int grp = task - (task / ngrp) * ngrp;
-      const int packed = trial_strength(g);
+      const int packed = P ? a.trials.uv[g] : a.trials.y[g];
       const int pri = packed >> 2;
       int sec = packed & 3;
       if (sec == 3) sec = 4;
@@ -200,7 +210,7 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
           const int dir = pri != 0 ? s_dir[b] : 0;
           const int16_t* tp = &s_tab[strength][256];
           const int2 po = s_ofs[dir + 2], q0 = s_ofs[dir + 4], q1 = s_ofs[dir];
-          for (int yy = yb; yy < yb + (1 << bl); yy++) {
+          for (int yy = yb; yy < yb + (1 << bl); yy += step) {
             // An unfiltered block keeps the reconstruction (cdefDist8 against
             // recon / the copyFB trial buffer), which below the crop is not
             // the VeryLarge-padded input.
@@ -221,8 +231,13 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   }
   __syncthreads();
   if (tid < 64) {
-    m0[tid] = ((mask0 >> tid) & 1) ? (uint64_t)s_sse[0][tid] : (uint64_t)kUntestedMSE;
-    m1[tid] = ((mask1 >> tid) & 1) ? (uint64_t)s_sse[1][tid] : (uint64_t)kUntestedMSE;
+    if (tid >= count) {
+      m0[tid] = m1[tid] = kNotATrial;
+    } else {
+      // A subsampled luma SSE is scaled back by the row step (searchRow, :722-734).
+      m0[tid] = ((mask0 >> tid) & 1) ? (uint64_t)s_sse[0][tid] * (uint64_t)ssY : (uint64_t)kUntestedMSE;
+      m1[tid] = ((mask1 >> tid) & 1) ? (uint64_t)s_sse[1][tid] : (uint64_t)kUntestedMSE;
+    }
   }
 }
 
@@ -524,7 +539,7 @@ __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsig
       fo->cost = bestTot;
       for (int j = 0; j < (1 << best); j++) {
         fo->ys[j] = st->lev0[best][j];
-        fo->uvs[j] = st->lev1[best][j];
+        fo->uvs[j] = a.uvFromY ? st->lev0[best][j] : st->lev1[best][j];
       }
     }
   }
@@ -540,7 +555,8 @@ __global__ void __launch_bounds__(256) k_sel_finish(SelArgs a, int maxCfg, unsig
     int bg = 0;
     unsigned long long bm = 1ull << 63;
     for (int g = 0; g < nb; g++) {
-      const unsigned long long v = M0[(size_t)fb * 64 + st->lev0[c][g]] + M1[(size_t)fb * 64 + st->lev1[c][g]];
+      const int uvg = a.uvFromY ? st->lev0[c][g] : st->lev1[c][g];
+      const unsigned long long v = M0[(size_t)fb * 64 + st->lev0[c][g]] + M1[(size_t)fb * 64 + uvg];
       if (v < bm) {
         bg = g;
         bm = v;
@@ -643,6 +659,7 @@ void* pf_internal_stream(pf_ctx* c);
 void* pf_internal_pinned(pf_ctx* c, size_t bytes);
 void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, size_t extra, cudaStream_t st,
                                 int* changed);
+int pf_internal_wait(pf_ctx* c, void* stream);  // pf_api.cu: blocking or bounded by the context's deadline
 
 static void* stage_frame(const pf_frame* f, void* dst, int64_t* strides, cudaStream_t st, cudaError_t* e) {
   size_t off = 0;
@@ -690,6 +707,7 @@ struct Staged {
   uint8_t* pin;  // page-locked staging: noskip words up, then the results down
   int nfb, maxCfg;
   cudaStream_t st;
+  pf_ctx* ctx;
 };
 
 static int check_search_frame(const pf_frame* f, const pf_frame* recon) {
@@ -708,6 +726,8 @@ static int check_search_frame(const pf_frame* f, const pf_frame* recon) {
   }
   return PF_OK;
 }
+
+static void level1_trials(TrialList* t);
 
 // source may be null (features only: the source is never read).
 static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
@@ -799,12 +819,14 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
   a.skip = base + oSkip;
   a.dirs = nullptr;
   a.ais = nullptr;
+  level1_trials(&a.trials);
   SelArgs& s = S->s;
   s.mse = a.mse;
   s.skip = a.skip;
   s.nfb = nfb;
   s.cap = 0;
   s.refine = 1;
+  s.uvFromY = 0;
   s.out = (SelOut*)(base + oSel);
   S->idx = base + oIdx;
   S->fo = (FinishOut*)(base + oFin);
@@ -812,7 +834,17 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
   S->nfb = nfb;
   S->maxCfg = maxCfg;
   S->st = st;
+  S->ctx = ctx;
   return PF_OK;
+}
+
+// The level-1 list (cdef_search.go:98-110).
+static void level1_trials(TrialList* t) {
+  memset(t, 0, sizeof(*t));
+  for (int g = 0; g < 64; g++) t->y[g] = t->uv[g] = (int8_t)trial_strength(g);
+  t->uvMask = ~0ull;
+  t->count = 64;
+  t->ss = 1;
 }
 
 static int search_damping(const pf_cdef_search_params* params) {
@@ -842,7 +874,8 @@ static int search_finish(Staged& S, const pf_cdef_search_params* params, uint64_
     return PF_ERR_DEVICE;
   if (fb_index_out && cudaMemcpyAsync(pidx, S.idx, S.nfb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return PF_ERR_DEVICE;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return PF_ERR_DEVICE;
+  const int w = pf_internal_wait(S.ctx, st);
+  if (w != PF_OK) return w;
   FinishOut fo;
   memcpy(&fo, pfo, sizeof(fo));
   if (fb_index_out) memcpy(fb_index_out, pidx, S.nfb);
@@ -850,9 +883,11 @@ static int search_finish(Staged& S, const pf_cdef_search_params* params, uint64_
     memset(result, 0, sizeof(*result));
     result->bits = (uint8_t)fo.bits;
     result->strength_count = (uint8_t)(1 << fo.bits);
+    // Presets map back through the luma list, chroma's too (finish,
+    // cdef_search.go:937-940).
     for (int j = 0; j < (1 << fo.bits); j++) {
-      result->y_strength[j] = (uint8_t)trial_strength(fo.ys[j]);
-      result->uv_strength[j] = (uint8_t)trial_strength(fo.uvs[j]);
+      result->y_strength[j] = (uint8_t)S.a.trials.y[fo.ys[j]];
+      result->uv_strength[j] = (uint8_t)S.a.trials.y[fo.uvs[j]];
     }
     result->cost = (double)fo.cost;
   }
@@ -867,6 +902,166 @@ extern "C" int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_fram
   const int stt = stage_search(ctx, source, recon, noskip, search_damping(params), search_max_cfg(params), 0, &S);
   if (stt != PF_OK) return stt;
   return search_finish(S, params, mse_out, fb_index_out, result);
+}
+
+extern "C" int pf_cdef_search_ex(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
+                                 const pf_cdef_search_params* params, const pf_cdef_search_ctrls* ctrls,
+                                 uint64_t* mse_out, uint8_t* fb_index_out, pf_cdef_search_result* result) {
+  if (!ctx || !source || !recon || !params || !ctrls) return PF_ERR_INVALID_ARG;
+  if (ctrls->count < 1 || ctrls->count > PF_CDEF_MAX_TRIALS || ctrls->subsampling < 1) return PF_ERR_INVALID_ARG;
+  TrialList t;
+  memset(&t, 0, sizeof(t));
+  for (int g = 0; g < ctrls->count; g++) {
+    if (ctrls->y[g] < 0 || ctrls->y[g] > 63 || ctrls->uv[g] < -1 || ctrls->uv[g] > 63) return PF_ERR_INVALID_CDEF;
+    t.y[g] = ctrls->y[g];
+    t.uv[g] = ctrls->uv[g];
+    if (ctrls->uv[g] >= 0) t.uvMask |= 1ull << g;
+  }
+  t.count = ctrls->count;
+  t.ss = ctrls->subsampling < 4 ? ctrls->subsampling : 4;  // BLOCK_8X8 caps the luma step (searchRow, :694-699)
+  Staged S;
+  const int stt = stage_search(ctx, source, recon, noskip, search_damping(params), search_max_cfg(params), 0, &S);
+  if (stt != PF_OK) return stt;
+  S.a.trials = t;
+  S.s.uvFromY = ctrls->uv_from_y ? 1 : 0;
+  return search_finish(S, params, mse_out, fb_index_out, result);
+}
+
+// ---------------------------------------------------------------------------
+// Search controls per level and the picture plan (host logic).
+
+extern "C" int pf_cdef_search_level_rtc(int32_t islice, int32_t screen) {
+  // svtRTCCDEFSearchLevel (cdef_search.go:208-221).
+  if (islice) return 5;
+  return screen ? 7 : 8;
+}
+
+namespace {
+// One level's controls: first- and second-pass luma and chroma lists and the
+// flags updateOnRefInfo and the plan read (svtCDEFSearchCtrls,
+// cdef_search.go:55-70, filled as setSVTCDEFSearchControls does, :72-202).
+struct LevelCtrls {
+  bool enabled = false, useRef = false, bestRef = false, skipDetector = false, uvFromY = false;
+  int first = 0, second = 0, ss = 1;
+  int8_t fs1[64] = {}, fs2[64] = {}, uv1[64] = {}, uv2[64] = {};
+  int predY = 0;
+};
+
+// The first-pass primaries of levels 1-8 (indices into svtPfGI, p * 4).
+const int8_t* level_primaries(int level, int* n) {
+  static const int8_t l1[16] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15};
+  static const int8_t l2[12] = {0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14};
+  static const int8_t l3[5] = {0, 4, 8, 12, 15};
+  static const int8_t l45[3] = {0, 7, 15};
+  static const int8_t l678[2] = {0, 15};
+  switch (level) {
+    case 1: *n = 16; return l1;
+    case 2: *n = 12; return l2;
+    case 3: *n = 5; return l3;
+    case 4:
+    case 5: *n = 3; return l45;
+    default: *n = 2; return l678;
+  }
+}
+
+LevelCtrls level_ctrls(int level, bool isBase, bool notHighest) {
+  LevelCtrls c;
+  c.enabled = true;
+  int n;
+  const int8_t* pri = level_primaries(level, &n);
+  c.first = n;
+  for (int i = 0; i < n; i++) c.fs1[i] = c.uv1[i] = (int8_t)(4 * pri[i]);
+  if (level <= 4) {
+    // Second pass: each first-pass strength's three secondaries.
+    c.second = 3 * n;
+    for (int i = 0; i < n; i++)
+      for (int j = 1; j < 4; j++) c.fs2[3 * i + j - 1] = (int8_t)(c.fs1[i] + j);
+    for (int i = 0; i < c.second; i++) c.uv2[i] = level == 1 ? c.fs2[i] : (int8_t)-1;
+    return c;
+  }
+  // Levels 5-8: secondary 2 of each first-pass strength, chroma untested there.
+  c.second = n;
+  for (int i = 0; i < n; i++) {
+    c.fs2[i] = (int8_t)(c.fs1[i] + 2);
+    c.uv2[i] = -1;
+  }
+  if (level == 5) {
+    c.bestRef = !notHighest;
+    return c;
+  }
+  if (level == 8) c.uv1[0] = c.uv1[1] = -1;
+  c.uv1[2] = -1;
+  c.ss = 4;
+  if (level == 6) c.bestRef = !notHighest;
+  if (level == 7) {
+    c.useRef = !notHighest;
+    c.bestRef = !isBase;
+    c.skipDetector = !isBase;
+  }
+  if (level == 8) {
+    c.useRef = !isBase;
+    c.bestRef = !isBase;
+    c.uvFromY = true;
+    for (int i = 0; i < c.first; i++) c.uv1[i] = -1;
+    for (int i = 0; i < c.second; i++) c.uv2[i] = -1;
+  }
+  return c;
+}
+
+// updateOnRefInfo (cdef_search.go:237-272): false when CDEF turns off.
+bool on_ref_info(LevelCtrls& c, const pf_cdef_ref_strengths& ref) {
+  if (c.useRef) {
+    int lo = 63, hi = 0;
+    for (int i = 0; i < ref.count; i++) {
+      lo = ref.y[i] < lo ? ref.y[i] : lo;
+      hi = ref.y[i] > hi ? ref.y[i] : hi;
+    }
+    c.predY = (lo + hi) / 2 < 63 ? (lo + hi) / 2 : 63;
+    c.first = c.second = 0;
+    return c.predY != 0;
+  }
+  if (c.bestRef) {
+    c.first = 1;
+    c.second = 0;
+    if ((int8_t)ref.y[0] != c.fs1[0]) c.fs1[c.first++] = (int8_t)ref.y[0];
+    if ((int8_t)ref.uv[0] == c.uv1[0]) c.uv1[0] = c.uv1[1] = -1;
+    return c.first != 1;
+  }
+  return true;
+}
+}  // namespace
+
+extern "C" int pf_cdef_plan_picture(int32_t level, int32_t islice, int32_t is_base, int32_t not_highest_layer,
+                                    const pf_cdef_ref_strengths* ref, int32_t ref_skip_percent, pf_cdef_plan* plan) {
+  if (!plan) return PF_ERR_INVALID_ARG;
+  if (level == 9) return PF_ERR_UNSUPPORTED;
+  if (level < 0 || level > 9) return PF_ERR_INVALID_ARG;
+  memset(plan, 0, sizeof(*plan));
+  if (level == 0) return PF_OK;
+  LevelCtrls c = level_ctrls(level, is_base != 0, not_highest_layer != 0);
+  bool on = c.enabled;
+  // planSVTCDEF (cdef_frame.go:34-54): on inter pictures, the skip detector,
+  // else the reference's strengths.
+  if (!islice) {
+    if (ref_skip_percent > 75 && c.skipDetector) {
+      on = false;
+    } else if (c.useRef || c.bestRef) {
+      if (!ref || ref->count < 1 || ref->count > 8) return PF_ERR_INVALID_ARG;
+      on = on_ref_info(c, *ref);
+    }
+  }
+  plan->on = on;
+  plan->search = on && !c.useRef;
+  if (on && c.useRef) plan->y_strength = (uint8_t)c.predY;  // predUVF is 0
+  pf_cdef_search_ctrls& t = plan->ctrls;
+  t.count = c.first + c.second;
+  for (int g = 0; g < t.count; g++) {
+    t.y[g] = g < c.first ? c.fs1[g] : c.fs2[g - c.first];
+    t.uv[g] = g < c.first ? c.uv1[g] : c.uv2[g - c.first];
+  }
+  t.subsampling = c.ss;
+  t.uv_from_y = c.uvFromY;
+  return PF_OK;
 }
 
 // Host or device bytes into a host vector.
@@ -949,10 +1144,8 @@ extern "C" int pf_cdef_features(pf_ctx* ctx, const pf_frame* recon, const uint8_
   if (stt != PF_OK) return stt;
   float* X = (float*)S.extra;
   if (launch_features(S.a, qindex, X, true, S.st) != cudaSuccess) return PF_ERR_DEVICE;
-  if (cudaMemcpyAsync(features, X, xBytes, cudaMemcpyDeviceToHost, S.st) != cudaSuccess ||
-      cudaStreamSynchronize(S.st) != cudaSuccess)
-    return PF_ERR_DEVICE;
-  return PF_OK;
+  if (cudaMemcpyAsync(features, X, xBytes, cudaMemcpyDeviceToHost, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  return pf_internal_wait(ctx, S.st);
 }
 
 extern "C" int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,

@@ -23,6 +23,21 @@ __host__ __device__ __forceinline__ int trial_strength(int g) {
   return (k / 3) * 4 + (k % 3) + 1;
 }
 
+// The trials a search measures (a level's controls, cdefSearchJob in
+// encoder/cdef_search.go:581-596): trial g tests luma packed strength y[g]
+// and chroma uv[g] (uvMask bit clear: not measured); luma rows every ss-th.
+struct TrialList {
+  int8_t y[64];
+  int8_t uv[64];
+  uint64_t uvMask;
+  int count;
+  int ss;
+};
+
+// SSE-table entry of a trial index past the list (PF_CDEF_NOT_A_TRIAL): no
+// selection step can pick it (see k_sel_greedy).
+constexpr uint32_t kNotATrial = 0x7fffffffu;
+
 struct SearchArgs {
   DFrame src, rec;          // 8-bit 4:2:0
   const uint8_t* noskip;    // 8 bytes per filter block, or null (all blocks)
@@ -37,6 +52,7 @@ struct SearchArgs {
   // pass when non-null.
   uint8_t* dirs;            // [nfb][64]
   int8_t* ais;              // [nfb][64]
+  TrialList trials;         // tmask searches use the level-1 list
 };
 
 struct SelOut {
@@ -55,6 +71,7 @@ struct SelArgs {
   const uint8_t* skip;   // [nfb]; the kernels list the non-skip blocks themselves
   int nfb, cap;
   int refine;            // 1: the reference's 4*nb refinement passes after the nb greedy picks
+  int uvFromY;           // the presets' chroma trials are their luma trials (finish, :920-925)
   SelOut* out;
 };
 

@@ -220,6 +220,7 @@ cudaError_t launch_superres_frame(const uint8_t* const* src, const int64_t* sstr
 }  // namespace pf
 
 void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
+int pf_internal_wait(pf_ctx* c, void* stream);  // pf_api.cu: blocking or bounded by the context's deadline
 void* pf_internal_stream(pf_ctx* c);
 
 // Step and initial phase of one plane (superres.go:45-51).
@@ -310,6 +311,6 @@ extern "C" int pf_superres_upscale(pf_ctx* ctx, const pf_frame* coded, const pf_
     for (int p = 0; p < nplanes && e == cudaSuccess; p++)
       e = cudaMemcpy2DAsync(upscaled->plane[p].data, upscaled->plane[p].stride, a.pl[p].dst, a.pl[p].dstride,
                             (size_t)dw[p] * bps, rows[p], cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  return e == cudaSuccess ? PF_OK : PF_ERR_DEVICE;
+  if (e != cudaSuccess) return PF_ERR_DEVICE;
+  return pf_internal_wait(ctx, st);
 }

@@ -96,9 +96,9 @@ def validate(frame, side, display=None):
 class PostFilterRunner:
     """One post-filter runner per decoder; calls are serialised by the caller."""
 
-    def __init__(self, device=0, timing=False):
+    def __init__(self, device=0, timing=False, wait_timeout_us=0):
         L = lib()
-        cfg = abi.pf_config(device=device, timing=1 if timing else 0)
+        cfg = abi.pf_config(device=device, timing=1 if timing else 0, wait_timeout_us=wait_timeout_us)
         st = C.c_int(0)
         h = L.pf_create(C.byref(cfg), C.byref(st))
         if not h:
@@ -160,6 +160,20 @@ class PostFilterRunner:
         ns = noskip.ctypes.data if noskip is not None else None
         check(lib().pf_cdef_search(self._h, C.byref(source), C.byref(recon), ns, C.byref(prm),
                                    mse.ctypes.data if want_mse else None, idx.ctypes.data, C.byref(res)))
+        return res, mse, idx
+
+    def cdef_search_ex(self, source, recon, noskip, qindex, lam, ctrls, max_presets=8, damping=0, want_mse=True):
+        """cdef_search over an explicit trial list (abi.pf_cdef_search_ctrls,
+        e.g. a picture plan's from cdef_plan_picture): any search level.
+        Returns (pf_cdef_search_result, mse uint64[2, nfb, 64], fb_index)."""
+        nfb = _nfb(recon.width, recon.height)
+        mse = np.empty((2, nfb, 64), np.uint64) if want_mse else None
+        idx = np.empty(nfb, np.uint8)
+        res = abi.pf_cdef_search_result()
+        prm = abi.pf_cdef_search_params(qindex=qindex, damping=damping, max_presets=max_presets, lam=lam)
+        ns = noskip.ctypes.data if noskip is not None else None
+        check(lib().pf_cdef_search_ex(self._h, C.byref(source), C.byref(recon), ns, C.byref(prm), C.byref(ctrls),
+                                      mse.ctypes.data if want_mse else None, idx.ctypes.data, C.byref(res)))
         return res, mse, idx
 
     def cdef_apply(self, recon, noskip, qindex, result, fb_index, damping=0):
@@ -399,3 +413,20 @@ def device_side(si, frame, device="cuda"):
     from .synth import SideInfo
 
     return SideInfo(side=s, keep=keep + [si], blocks=si.blocks)
+
+
+def cdef_plan_picture(level, islice, is_base=True, not_highest_layer=False, ref=None, ref_skip_percent=0):
+    """A picture's CDEF plan at search level 1-8 (planSVTCDEF with the
+    level's controls and updateOnRefInfo, internal/av1/encoder/cdef_frame.go:34-54):
+    abi.pf_cdef_plan.  ref: the LAST reference's strengths
+    (abi.pf_cdef_ref_strengths), needed by inter pictures at levels 5-8.
+    Host logic only."""
+    plan = abi.pf_cdef_plan()
+    check(lib().pf_cdef_plan_picture(level, int(islice), int(is_base), int(not_highest_layer),
+                                     C.byref(ref) if ref is not None else None, ref_skip_percent, C.byref(plan)))
+    return plan
+
+
+def cdef_search_level_rtc(islice, screen=False):
+    """The search level goav1's real-time encoder uses (svtRTCCDEFSearchLevel)."""
+    return lib().pf_cdef_search_level_rtc(int(islice), int(screen))

@@ -56,7 +56,7 @@
 extern "C" {
 #endif
 
-#define PF_ABI_VERSION 1
+#define PF_ABI_VERSION 2
 
 /* ---- status codes (negative = error; the frame is untouched on every error
  *      reported before any kernel was queued, mirroring the reference's
@@ -232,6 +232,16 @@ typedef struct pf_config {
   int32_t timing;        /* 1 = record per-stage CUDA events */
   int64_t max_width;     /* largest luma frame the context will see (0 = grow) */
   int64_t max_height;
+  int64_t wait_timeout_us; /* 0: a call that waits for its device work (pf_sync,
+                              host-frame pf_frame_apply / pf_batch_apply, the
+                              searches, pf_superres_upscale, pf_lf_build)
+                              blocks until it is done; > 0: each such wait
+                              polls and the call returns PF_ERR_TIMEOUT once
+                              this many microseconds have passed in it.  The
+                              queued work, copies into the caller's host
+                              buffers included, still runs: call pf_sync
+                              before reusing those buffers or reading the
+                              call's outputs. */
 } pf_config;
 
 typedef struct pf_ctx pf_ctx;
@@ -356,6 +366,70 @@ int pf_cdef_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon,
                    const uint8_t* noskip, const pf_cdef_search_params* params,
                    uint64_t* mse_out, uint8_t* fb_index_out,
                    pf_cdef_search_result* result);
+
+/* The search controls of one picture (goav1's svtCDEFSearchCtrls after
+ * updateOnRefInfo, as cdefSearcher.search reads them,
+ * internal/av1/encoder/cdef_search.go:581-596): trial i measures luma packed
+ * strength y[i] and chroma packed strength uv[i] (-1: chroma not measured,
+ * its SSE is the untested figure 1040400 * 64); luma rows are measured every
+ * `subsampling`-th row (capped at 4) with the SSE scaled back by that factor;
+ * uv_from_y makes each preset's chroma strength its luma strength. */
+#define PF_CDEF_MAX_TRIALS 64
+typedef struct pf_cdef_search_ctrls {
+  int32_t count;                    /* trials, first pass then second: 1..64 */
+  int8_t y[PF_CDEF_MAX_TRIALS];
+  int8_t uv[PF_CDEF_MAX_TRIALS];
+  int32_t subsampling;              /* subsamplingFactor: 1 or 4 */
+  int32_t uv_from_y;
+} pf_cdef_search_ctrls;
+
+/* SSE-table entries at and beyond ctrls->count (not trials of the list). */
+#define PF_CDEF_NOT_A_TRIAL 0x7fffffffu
+
+/* The LAST reference's signalled strengths (svtCDEFRefStrengths,
+ * cdef_search.go:224-235): count = 1 << cdef_bits. */
+typedef struct pf_cdef_ref_strengths {
+  uint8_t count;
+  uint8_t y[8];
+  uint8_t uv[8];
+} pf_cdef_ref_strengths;
+
+/* A picture's CDEF plan (svtCDEFFramePlan, encoder/cdef_frame.go:13-54). */
+typedef struct pf_cdef_plan {
+  int32_t on;              /* CDEF is on for the picture (cdef_level != 0) */
+  int32_t search;          /* the strengths come from pf_cdef_search_ex(ctrls) */
+  uint8_t y_strength;      /* on && !search (use_reference_cdef_fs): the one */
+  uint8_t uv_strength;     /*   strength pair the picture signals (bits 0)    */
+  uint8_t reserved[2];
+  pf_cdef_search_ctrls ctrls;
+} pf_cdef_plan;
+
+/* The search level goav1's real-time encoder picks
+ * (svtRTCCDEFSearchLevel, cdef_search.go:208-221): 5 on intra pictures,
+ * otherwise 7 for screen content and 8 for camera content. */
+int pf_cdef_search_level_rtc(int32_t islice, int32_t screen);
+
+/* planSVTCDEF (encoder/cdef_frame.go:34-54) at search level 1-8: the level's
+ * controls (setSVTCDEFSearchControls, cdef_search.go:72-202), then, on
+ * inter pictures, the skip detector (CDEF off when more than 75 % of the
+ * LAST reference was coded skip and the level uses it) or updateOnRefInfo
+ * (cdef_search.go:237-272) with `ref`, which inter pictures at levels 5-8
+ * need.  Level 0 gives a plan with CDEF off; level 9 (the QP-derived
+ * strengths) is PF_ERR_UNSUPPORTED.  Host logic only: no device call. */
+int pf_cdef_plan_picture(int32_t level, int32_t islice, int32_t is_base, int32_t not_highest_layer,
+                         const pf_cdef_ref_strengths* ref, int32_t ref_skip_percent, pf_cdef_plan* plan);
+
+/* pf_cdef_search over an explicit trial list (cdefSearcher.search with any
+ * level's controls, cdef_search.go:581-634): mse_out entries
+ * [plane][fb][i] for i < ctrls->count as pf_cdef_search describes (untested
+ * chroma trials at 1040400 * 64; luma at the subsampled, rescaled SSE),
+ * entries from ctrls->count on hold PF_CDEF_NOT_A_TRIAL; the greedy
+ * selection runs over the list and result's strengths are ctrls->y of the
+ * chosen trials (chroma too, as finish maps them, :937-940; luma's with
+ * uv_from_y). */
+int pf_cdef_search_ex(pf_ctx* ctx, const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
+                      const pf_cdef_search_params* params, const pf_cdef_search_ctrls* ctrls, uint64_t* mse_out,
+                      uint8_t* fb_index_out, pf_cdef_search_result* result);
 
 /* The encoder's CDEF application (cdefApplier.apply,
  * internal/av1/encoder/cdef_apply.go:258-371): filters `recon` in place with

@@ -1,13 +1,19 @@
 // cdef_search_oracle.cpp - CPU oracle for goav1's encoder CDEF strength
 // search (internal/av1/encoder/cdef_search.go), test infrastructure only.
 //
-// Level-1 search controls (setSVTCDEFSearchControls level 1,
-// cdef_search.go:98-110): all 64 packed strengths, first pass the 16
-// primaries with secondary 0 (svtPfGI), second pass pf+1..pf+3, chroma the
-// same list, row subsampling 1.  Per 64x64 filter block and trial gi the SSE
-// of the CDEF-filtered reconstruction against the source over the block's
-// non-skip 8x8 blocks (cdef_search.go:649-745) goes to mse[0] (luma) or
-// mse[1] (U+V); finish (:886-945) picks the frame presets greedily.
+// The search runs over a trial list (cdefSearchJob, cdef_search.go:581-596):
+// trial gi tests luma packed strength fsY[gi] and chroma fsUV[gi] (-1: not
+// tested, the chroma SSE is cdefDefaultMSEUV * 64), luma rows measured every
+// subsamplingFactor-th row with the SSE scaled back (:694-701, :722-734).
+// Per 64x64 filter block and trial the SSE of the CDEF-filtered
+// reconstruction against the source over the block's non-skip 8x8 blocks
+// (cdef_search.go:649-745) goes to mse[0] (luma) or mse[1] (U+V); finish
+// (:886-945) picks the frame presets greedily over the list and maps them
+// back through fsY (chroma too, or luma's with uvFromY).  The controls of
+// each search level and the picture plan (setSVTCDEFSearchControls :72-202,
+// updateOnRefInfo :237-272, planSVTCDEF in cdef_frame.go:34-54) are
+// restated in oracle_cdef_plan_picture.  Level 1 (all 64 strengths, chroma
+// the same list, subsampling 1) is oracle_cdef_search.
 #include <stdint.h>
 #include <string.h>
 
@@ -136,11 +142,15 @@ P8 plane8(const pf_frame* f, int p) {
 }
 
 // The level-1 trial list (gi -> packed strength), cdef_search.go:98-110.
-void trial_list(int8_t fs[64]) {
-  for (int i = 0; i < 16; i++) fs[i] = (int8_t)(i * 4);
+void level1_ctrls(pf_cdef_search_ctrls* c) {
+  memset(c, 0, sizeof(*c));
+  for (int i = 0; i < 16; i++) c->y[i] = (int8_t)(i * 4);
   int k = 16;
   for (int i = 0; i < 16; i++)
-    for (int j = 1; j < 4; j++) fs[k++] = (int8_t)(i * 4 + j);
+    for (int j = 1; j < 4; j++) c->y[k++] = (int8_t)(i * 4 + j);
+  for (int g = 0; g < 64; g++) c->uv[g] = c->y[g];
+  c->count = 64;
+  c->subsampling = 1;
 }
 
 uint64_t rdcost(uint64_t lambda, int64_t rate, uint64_t dist) {  // cdef_search.go:302-304
@@ -215,17 +225,19 @@ uint64_t search_one_dual(const std::vector<const uint64_t*>& m0, const std::vect
 // direction search on the reconstruction, FilterBlocksU8SubsampledTrusted
 // with row step 1 (cdef/filter_search.go:20-74: in place, skip when the
 // adjusted strength and the secondary are both zero) and computeCDEFDist8.
-extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, const uint8_t* noskip,
-                                  const pf_cdef_search_params* prm, uint64_t* mse_out, uint8_t* fb_index_out,
-                                  pf_cdef_search_result* result) {
-  if (!src || !rec || !prm || !mse_out || rec->bit_depth != 8 || rec->ss_x != 1 || rec->ss_y != 1)
+extern "C" int oracle_cdef_search_ex(const pf_frame* src, const pf_frame* rec, const uint8_t* noskip,
+                                     const pf_cdef_search_params* prm, const pf_cdef_search_ctrls* ctrls,
+                                     uint64_t* mse_out, uint8_t* fb_index_out, pf_cdef_search_result* result) {
+  if (!src || !rec || !prm || !ctrls || !mse_out || rec->bit_depth != 8 || rec->ss_x != 1 || rec->ss_y != 1)
     return PF_ERR_INVALID_ARG;
+  const int total = ctrls->count;
+  if (total < 1 || total > 64 || ctrls->subsampling < 1) return PF_ERR_INVALID_ARG;
   const int W = rec->width, H = rec->height;
   const int miCols = ((W + 7) >> 3) << 1, miRows = ((H + 7) >> 3) << 1;
   const int nhfb = (miCols + 15) / 16, nvfb = (miRows + 15) / 16, nfb = nhfb * nvfb;
   const int damping = prm->damping ? prm->damping : 3 + (prm->qindex >> 6);
-  int8_t fs[64];
-  trial_list(fs);
+  // Luma rows every ss-th (BLOCK_8X8 caps it at 4); chroma every row.
+  const int ssY = imin(ctrls->subsampling, 4);
   std::vector<uint16_t> in(kBS * (128 + 4));
   std::vector<uint8_t> tmp(64 * 64);
   std::vector<uint8_t> skipFB(nfb, 0);
@@ -246,14 +258,15 @@ extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, cons
           if ((word >> ((r >> 1) * 8 + (c >> 1))) & 1) dlist.emplace_back(r >> 1, c >> 1);
       uint64_t* m0 = mse_out + (size_t)fb * 64;
       uint64_t* m1 = mse_out + (size_t)nfb * 64 + (size_t)fb * 64;
+      for (int g = total; g < 64; g++) m0[g] = m1[g] = PF_CDEF_NOT_A_TRIAL;
       if (dlist.empty()) {
         skipFB[fb] = 1;
-        for (int g = 0; g < 64; g++) m0[g] = m1[g] = 0;
+        for (int g = 0; g < total; g++) m0[g] = m1[g] = 0;
         continue;
       }
       uint8_t dir[8][8] = {};
       int32_t var[8][8] = {};
-      for (int g = 0; g < 64; g++) m1[g] = 0;
+      for (int g = 0; g < total; g++) m1[g] = 0;
       for (int pli = 0; pli < 3; pli++) {
         const int dec = pli ? 1 : 0;
         const int x0 = (lc * 4) >> dec, y0 = (lr * 4) >> dec;
@@ -274,8 +287,13 @@ extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, cons
                 (uint8_t)find_dir(rp.d + (int64_t)(y0 + 8 * b.first) * rp.s + x0 + 8 * b.second, (int)rp.s,
                                   &var[b.first][b.second]);
         const int bl = 3 - dec, bsz = 1 << bl;
-        for (int g = 0; g < 64; g++) {
-          const int packed = fs[g];
+        const int ss = pli ? 1 : ssY;
+        for (int g = 0; g < total; g++) {
+          if (pli && ctrls->uv[g] < 0) {
+            m1[g] = (uint64_t)1040400 * 64;  // cdefDefaultMSEUV * 64 (:669-672)
+            continue;
+          }
+          const int packed = pli ? ctrls->uv[g] : ctrls->y[g];
           const int pri = packed >> 2;
           int sec = packed & 3;
           if (sec == 3) sec = 4;
@@ -284,7 +302,7 @@ extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, cons
             const int strength = (pli == 0 && pri != 0) ? adjust(pri, var[b.first][b.second]) : pri;
             const int d = pri != 0 ? dir[b.first][b.second] : 0;
             const int dmp = pli ? damping - 1 : damping;
-            for (int i = 0; i < bsz; i++)
+            for (int i = 0; i < bsz; i += ss)
               for (int j = 0; j < bsz; j++) {
                 const int yy = (b.first << bl) + i, xx = (b.second << bl) + j;
                 int v;
@@ -297,21 +315,27 @@ extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, cons
               }
           }
           if (pli == 0)
-            m0[g] = sse;
+            m0[g] = sse * ss;
           else
-            m1[g] += sse;
+            m1[g] += sse * ss;
         }
       }
     }
   }
-  return oracle_cdef_select(mse_out, skipFB.data(), nfb, prm, fb_index_out, result);
+  return oracle_cdef_select_ctrls(mse_out, skipFB.data(), nfb, prm, ctrls, 1, fb_index_out, result);
 }
 
-extern "C" int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, int nfb,
-                                     const pf_cdef_search_params* prm, int refine, uint8_t* fb_index_out,
-                                     pf_cdef_search_result* result);
+// Level 1 (cdef_search.go:98-110): all 64 strengths in the svtPfGI order,
+// chroma the same list, every row measured.
+extern "C" int oracle_cdef_search(const pf_frame* src, const pf_frame* rec, const uint8_t* noskip,
+                                  const pf_cdef_search_params* prm, uint64_t* mse_out, uint8_t* fb_index_out,
+                                  pf_cdef_search_result* result) {
+  pf_cdef_search_ctrls c;
+  level1_ctrls(&c);
+  return oracle_cdef_search_ex(src, rec, noskip, prm, &c, mse_out, fb_index_out, result);
+}
 
-// finish (cdef_search.go:886-945) over a given SSE table.
+// finish (cdef_search.go:886-945) over a given SSE table, at level 1.
 extern "C" int oracle_cdef_select(const uint64_t* mse, const uint8_t* skip, int nfb, const pf_cdef_search_params* prm,
                                   uint8_t* fb_index_out, pf_cdef_search_result* result) {
   return oracle_cdef_select_ex(mse, skip, nfb, prm, 1, fb_index_out, result);
@@ -322,8 +346,18 @@ extern "C" int oracle_cdef_select(const uint64_t* mse, const uint8_t* skip, int 
 extern "C" int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, int nfb,
                                      const pf_cdef_search_params* prm, int refine, uint8_t* fb_index_out,
                                      pf_cdef_search_result* result) {
-  int8_t fs[64];
-  trial_list(fs);
+  pf_cdef_search_ctrls c;
+  level1_ctrls(&c);
+  return oracle_cdef_select_ctrls(mse, skip, nfb, prm, &c, refine, fb_index_out, result);
+}
+
+// finish over the first ctrls->count trials (endGI = len(filterMap)); the
+// presets map back through the luma list fsY, chroma's too (:937-940), or
+// copy luma's with uvFromY (:920-925).
+extern "C" int oracle_cdef_select_ctrls(const uint64_t* mse, const uint8_t* skip, int nfb,
+                                        const pf_cdef_search_params* prm, const pf_cdef_search_ctrls* ctrls,
+                                        int refine, uint8_t* fb_index_out, pf_cdef_search_result* result) {
+  const int end = ctrls->count;
   std::vector<const uint64_t*> s0, s1;
   std::vector<int> sbIndex;
   for (int fb = 0; fb < nfb; fb++) {
@@ -342,13 +376,13 @@ extern "C" int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, i
     int lev0[8] = {}, lev1[8] = {};
     const int nb = 1 << i;
     uint64_t tot = (uint64_t)1 << 63;
-    for (int k = 0; k < nb; k++) tot = search_one_dual(s0, s1, lev0, lev1, k, 64);
+    for (int k = 0; k < nb; k++) tot = search_one_dual(s0, s1, lev0, lev1, k, end);
     for (int k = 0; refine && k < 4 * nb; k++) {
       for (int j = 0; j < nb - 1; j++) {
         lev0[j] = lev0[j + 1];
         lev1[j] = lev1[j + 1];
       }
-      tot = search_one_dual(s0, s1, lev0, lev1, nb - 1, 64);
+      tot = search_one_dual(s0, s1, lev0, lev1, nb - 1, end);
     }
     const int totalBits = sbCount * i + nb * 6 * 2;
     const uint64_t cost = rdcost(lambda, (int64_t)totalBits << 9, tot * 16);
@@ -357,7 +391,7 @@ extern "C" int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, i
       bestBits = i;
       for (int j = 0; j < nb; j++) {
         ys[j] = lev0[j];
-        uvs[j] = lev1[j];
+        uvs[j] = ctrls->uv_from_y ? lev0[j] : lev1[j];
       }
     }
   }
@@ -379,11 +413,182 @@ extern "C" int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, i
     result->bits = (uint8_t)bestBits;
     result->strength_count = (uint8_t)nb;
     for (int j = 0; j < nb; j++) {
-      result->y_strength[j] = (uint8_t)fs[ys[j]];
-      result->uv_strength[j] = (uint8_t)fs[uvs[j]];
+      result->y_strength[j] = (uint8_t)ctrls->y[ys[j]];
+      result->uv_strength[j] = (uint8_t)ctrls->y[uvs[j]];
     }
     result->cost = (double)bestTot;
   }
   return PF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Search controls per level and the picture plan.
+namespace {
+const int8_t kPfGI[16] = {0, 4, 8, 12, 16, 20, 24, 28, 32, 36, 40, 44, 48, 52, 56, 60};  // svtPfGI
+
+struct Ctrls {  // svtCDEFSearchCtrls (cdef_search.go:55-70)
+  bool enabled = false;
+  int first = 0, second = 0;
+  int8_t fs[64] = {}, fs2[64] = {}, fsuv[64] = {}, fs2uv[64] = {};
+  bool useRef = false, bestRef = false, skipDet = false, uvFromY = false, qp = false;
+  int ss = 0;
+  int predY = 0, predUV = 0;
+};
+
+// setSVTCDEFSearchControls (cdef_search.go:72-202).
+Ctrls controls(int level, bool isBase, bool notHighest) {
+  Ctrls c;
+  auto secondPass = [&]() {
+    int sf = 0;
+    for (int i = 0; i < c.first; i++)
+      for (int j = 1; j < 4; j++) c.fs2[sf++] = (int8_t)(c.fs[i] + j);
+  };
+  auto uvFirst = [&]() {
+    for (int i = 0; i < c.first; i++) c.fsuv[i] = c.fs[i];
+  };
+  auto uvSecondOff = [&]() {
+    for (int i = 0; i < c.second; i++) c.fs2uv[i] = -1;
+  };
+  auto firstFrom = [&](std::initializer_list<int> gs) {
+    int i = 0;
+    for (int g : gs) c.fs[i++] = kPfGI[g];
+    c.first = i;
+  };
+  switch (level) {
+    case 1:
+      c.enabled = true;
+      firstFrom({0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15});
+      c.second = c.first * 3;
+      secondPass();
+      uvFirst();
+      for (int i = 0; i < c.second; i++) c.fs2uv[i] = c.fs2[i];
+      c.ss = 1;
+      break;
+    case 2:
+    case 3:
+    case 4:
+      c.enabled = true;
+      if (level == 2) firstFrom({0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14});
+      if (level == 3) firstFrom({0, 4, 8, 12, 15});
+      if (level == 4) firstFrom({0, 7, 15});
+      c.second = c.first * 3;
+      secondPass();
+      uvFirst();
+      uvSecondOff();
+      c.ss = 1;
+      break;
+    case 5:
+      c.enabled = true;
+      firstFrom({0, 7, 15});
+      c.second = c.first;
+      for (int i = 0; i < 3; i++) c.fs2[i] = (int8_t)(c.fs[i] + 2);
+      uvFirst();
+      uvSecondOff();
+      c.bestRef = !notHighest;
+      c.ss = 1;
+      break;
+    case 6:
+    case 7:
+    case 8:
+      c.enabled = true;
+      c.first = 2;
+      c.second = 2;
+      c.fs[0] = kPfGI[0];
+      c.fs[1] = kPfGI[15];
+      c.fs2[0] = (int8_t)(kPfGI[0] + 2);
+      c.fs2[1] = (int8_t)(kPfGI[15] + 2);
+      if (level == 8) {
+        c.fsuv[0] = c.fsuv[1] = -1;
+      } else {
+        c.fsuv[0] = c.fs[0];
+        c.fsuv[1] = c.fs[1];
+      }
+      c.fsuv[2] = -1;
+      c.fs2uv[0] = c.fs2uv[1] = -1;
+      c.ss = 4;
+      if (level == 6) c.bestRef = !notHighest;
+      if (level == 7) {
+        c.useRef = !notHighest;
+        c.bestRef = !isBase;
+        c.skipDet = !isBase;
+      }
+      if (level == 8) {
+        c.useRef = !isBase;
+        c.bestRef = !isBase;
+        c.uvFromY = true;
+      }
+      break;
+    default:
+      break;
+  }
+  if (c.uvFromY && !c.qp) {
+    for (int i = 0; i < c.first; i++) c.fsuv[i] = -1;
+    for (int i = 0; i < c.second; i++) c.fs2uv[i] = -1;
+  }
+  return c;
+}
+
+// updateOnRefInfo (cdef_search.go:237-272).
+bool update_on_ref(Ctrls& c, const pf_cdef_ref_strengths& ref) {
+  if (c.useRef) {
+    int lo = 63, hi = 0;
+    for (int i = 0; i < ref.count; i++) {
+      lo = imin(lo, ref.y[i]);
+      hi = imax(hi, ref.y[i]);
+    }
+    c.predY = imin(63, (lo + hi) / 2);
+    c.predUV = 0;
+    c.first = 0;
+    c.second = 0;
+    return c.predY != 0 || c.predUV != 0;
+  }
+  if (c.bestRef) {
+    c.first = 1;
+    c.second = 0;
+    if ((int8_t)ref.y[0] != c.fs[0]) {
+      c.fs[1] = (int8_t)ref.y[0];
+      c.first++;
+    }
+    if ((int8_t)ref.uv[0] == c.fsuv[0]) {
+      c.fsuv[0] = -1;
+      c.fsuv[1] = -1;
+    }
+    return c.first != 1;
+  }
+  return true;
+}
+}  // namespace
+
+// planSVTCDEF (cdef_frame.go:34-54) at an explicit search level, and the
+// job's trial list (cdef_search.go:585-596).
+extern "C" int oracle_cdef_plan_picture(int level, int islice, int is_base, int not_highest_layer,
+                                        const pf_cdef_ref_strengths* ref, int ref_skip_percent, pf_cdef_plan* plan) {
+  if (!plan || level < 0 || level > 8) return PF_ERR_INVALID_ARG;
+  memset(plan, 0, sizeof(*plan));
+  if (level == 0) return PF_OK;
+  Ctrls c = controls(level, is_base != 0, not_highest_layer != 0);
+  bool on = c.enabled;
+  if (!islice && on) {
+    if (ref_skip_percent > 75 && c.skipDet) {
+      on = false;
+    } else if (c.useRef || c.bestRef) {
+      if (!ref) return PF_ERR_INVALID_ARG;
+      on = update_on_ref(c, *ref);
+    }
+  }
+  plan->on = on;
+  plan->search = on && !c.useRef;
+  if (on && c.useRef) {
+    plan->y_strength = (uint8_t)c.predY;
+    plan->uv_strength = (uint8_t)c.predUV;
+  }
+  pf_cdef_search_ctrls& t = plan->ctrls;
+  t.count = c.first + c.second;
+  for (int g = 0; g < t.count; g++) {
+    t.y[g] = g < c.first ? c.fs[g] : c.fs2[g - c.first];
+    t.uv[g] = g < c.first ? c.fsuv[g] : c.fs2uv[g - c.first];
+  }
+  t.subsampling = c.ss;
+  t.uv_from_y = c.uvFromY;
+  return PF_OK;
+}

@@ -92,6 +92,17 @@ int oracle_cdef_select(const uint64_t* mse, const uint8_t* skip, int nfb, const 
 int oracle_cdef_select_ex(const uint64_t* mse, const uint8_t* skip, int nfb, const pf_cdef_search_params* params,
                           int refine, uint8_t* fb_index_out, pf_cdef_search_result* result);
 
+/* The same over an explicit trial list (pf_cdef_search_ex), its selection,
+ * and the picture plan (pf_cdef_plan_picture). */
+int oracle_cdef_search_ex(const pf_frame* source, const pf_frame* recon, const uint8_t* noskip,
+                          const pf_cdef_search_params* params, const pf_cdef_search_ctrls* ctrls, uint64_t* mse_out,
+                          uint8_t* fb_index_out, pf_cdef_search_result* result);
+int oracle_cdef_select_ctrls(const uint64_t* mse, const uint8_t* skip, int nfb, const pf_cdef_search_params* params,
+                             const pf_cdef_search_ctrls* ctrls, int refine, uint8_t* fb_index_out,
+                             pf_cdef_search_result* result);
+int oracle_cdef_plan_picture(int level, int islice, int is_base, int not_highest_layer,
+                             const pf_cdef_ref_strengths* ref, int ref_skip_percent, pf_cdef_plan* plan);
+
 /* Learned CDEF selection (oracle/learned_oracle.cpp); see pf_cdef_features
  * and the pf_cdef_mlp_* entry points.  grads: PF_MLP_PARAMS floats. */
 int oracle_cdef_features(const pf_frame* recon, const uint8_t* noskip, int qindex, int damping, float* X);
