@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--search-frames", type=int, default=8)
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-config2", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="time the default schedule instead of the autotuned one")
     return ap.parse_args()
 
 
@@ -192,12 +193,12 @@ def mixed_leg(local, steps, warmup):
             "batched_over_single_stream": ms_s / ms_b,
             "homogeneous_batches_ms_sum": ms_kinds, "mixed_rate_over_homogeneous": ms_kinds / ms_b,
             "algorithmic_gbs": algo_bytes / (ms_b / 1e3) / 1e9,
-            "autotune": {n: {"ctas": int(tune.ctas[i]), "ms": round(float(tune.ms[i]), 4),
-                             "ms_one_cta_per_item": round(float(tune.ms_default[i]), 4)}
+            "autotune": {n: dict(tune.chosen[i].as_dict(), ms=round(float(tune.ms[i]), 4),
+                                 ms_default_schedule=round(float(tune.ms_default[i]), 4))
                          for i, n in enumerate(names)},
             "config": "48 frames, seeds 100-147: 16x640x360 8-bit 4:2:0, 16x1280x720 8-bit 4:2:0, "
                       "8x1920x1080 10-bit 4:2:0, 8x1280x720 8-bit 4:4:4, full chain; batched = one pf_batch_apply "
-                      "(autotuned persistent CTAs, CUDA graph replay), single stream = one call per frame, "
+                      "(autotuned schedules, CUDA graph replay), single stream = one call per frame, "
                       "homogeneous = each of the four kinds batched alone; "
                       "256 MB L2 flush between steps; %.1f Mpix per step" % (px / 1e6)}
 
@@ -416,13 +417,16 @@ def cpu_baseline_lr_search(pair, seconds=5.0):
             "kind": "port", "sample": "%d calls on one 1920x1080 frame (seed 2000) in %.1f s, one thread" % (calls, dt)}
 
 
-def stage_times(local, reset, items, reps=3):
+def stage_times(local, reset, items, reps=3, schedule=None):
     """Per-stage device times of the batched launches (CUDA events the library
     records on its stream), summed over the batch, averaged over `reps`
-    batches after one untimed batch."""
+    batches after one untimed batch, under the timed run's stage schedules."""
     from goav1_b200.postfilter import PostFilterRunner
 
     trunner = PostFilterRunner(device=local, timing=True)
+    for g, nm in enumerate(["deblock", "cdef", "restoration", "film_grain"]):
+        if schedule:
+            trunner.set_schedule(g, **{k: schedule[nm][k] for k in ("ctas", "units_per_cta", "staging", "tile")})
     stage = np.zeros(5)
     for k in range(reps + 1):
         reset()
@@ -593,6 +597,18 @@ def main():
     def step():
         runner.apply_batch(pf_frames)
 
+    # The stage schedules (tile shape, work items per CTA, staging depth,
+    # persistent CTAs) searched on this batch before anything is timed; the
+    # tuner filters the frames in place, and reset() restores them before
+    # every step.
+    schedule = None
+    if not args.no_tune:
+        reset()
+        tune = runner.autotune(pf_frames, reps=2)
+        schedule = {nm: dict(tune.chosen[i].as_dict(), ms=round(float(tune.ms[i]), 4),
+                             ms_default_schedule=round(float(tune.ms_default[i]), 4))
+                    for i, nm in enumerate(["deblock", "cdef", "restoration", "film_grain"])}
+
     clocks = ClockSampler(local)
     clocks.start()
     # Warm-up.
@@ -622,7 +638,7 @@ def main():
     # Per-stage device times of the batched launches (CUDA events the library
     # records on its stream), averaged over a few batches.
     stage_names = ["deblock", "cdef", "restoration", "extend", "film_grain"]
-    per_frame = stage_times(local, reset, pf_frames) / n
+    per_frame = stage_times(local, reset, pf_frames, schedule=schedule) / n
 
     # Every frame of the timed batch against the oracle: the device frames
     # now hold one chain application (the stage-timing batches start from the
@@ -934,7 +950,7 @@ def main():
                            "l2": "inputs (%.0f MB per rank) larger than L2, and a 256 MB L2 flush between steps"
                                  % (sum(fr.nbytes() for fr, _ in frames) / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "parity_checked": parity,
-                "config2": c2, "cdef_search": search,
+                "schedule": schedule, "config2": c2, "cdef_search": search,
                 "cdef_search_learned": learned_leg, "lr_search": lr_leg, "superres": sr_leg, "lf_build": lf_leg, "mixed_batch": mixed,
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))

@@ -59,6 +59,8 @@ def lib():
                                          C.POINTER(abi.pf_cdef_learned_stats)]
     L.pf_batch_graphs.argtypes = [C.c_void_p, C.c_int32]
     L.pf_set_persistent.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+    L.pf_set_schedule.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.pf_schedule)]
+    L.pf_get_schedule.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.pf_schedule)]
     L.pf_autotune.argtypes = [C.c_void_p, C.POINTER(abi.pf_batch_item), C.c_int32, C.c_int32,
                               C.POINTER(abi.pf_tune_result)]
     L.pf_cdef_apply.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.c_void_p, C.POINTER(abi.pf_cdef_search_params),
@@ -78,7 +80,7 @@ def lib():
     L.pf_cdef_search_ex.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame), C.c_void_p,
                                     C.POINTER(abi.pf_cdef_search_params), C.POINTER(abi.pf_cdef_search_ctrls),
                                     C.c_void_p, C.c_void_p, C.POINTER(abi.pf_cdef_search_result)]
-    if L.pf_abi_version() != 2:
+    if L.pf_abi_version() != 3:
         raise RuntimeError("goav1_b200: ABI version mismatch")
     _lib = L
     return L

@@ -244,9 +244,22 @@ PF_LEARNED_REFINE = 1
 PF_TUNE_DEBLOCK, PF_TUNE_CDEF, PF_TUNE_RESTORATION, PF_TUNE_FILM_GRAIN, PF_TUNE_GROUPS = 0, 1, 2, 3, 4
 
 
+class pf_schedule(C.Structure):
+    _fields_ = [
+        ("ctas", C.c_int32),
+        ("units_per_cta", C.c_int32),
+        ("staging", C.c_int32),
+        ("tile", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {"ctas": self.ctas, "units_per_cta": self.units_per_cta, "staging": self.staging,
+                "tile": self.tile}
+
+
 class pf_tune_result(C.Structure):
     _fields_ = [
-        ("ctas", C.c_int32 * PF_TUNE_GROUPS),
+        ("chosen", pf_schedule * PF_TUNE_GROUPS),
         ("ms", C.c_float * PF_TUNE_GROUPS),
         ("ms_default", C.c_float * PF_TUNE_GROUPS),
     ]
@@ -415,6 +428,8 @@ EXPORTED_SYMBOLS = (
     "pf_cdef_search_learned",
     "pf_batch_graphs",
     "pf_set_persistent",
+    "pf_set_schedule",
+    "pf_get_schedule",
     "pf_autotune",
     "pf_lr_search",
     "pf_cdef_apply",

@@ -119,8 +119,13 @@ struct pf_ctx {
   std::vector<FrameJob> hjobs;
   std::vector<int> hbase;
   std::vector<uint8_t> hside;
-  // Persistent-CTA count per stage (0 = one CTA per work item).
+  // The schedule of each stage's launch (pf_schedule): persistent-CTA count
+  // (0 = one CTA per chunk), work items per chunk, items prefetched ahead,
+  // and the deblocking tile shape.
   int persistent[ST_COUNT] = {};
+  int chunk[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1};
+  int ahead[ST_COUNT] = {};
+  int db_tile = 0;
   // CUDA graphs of pf_batch_apply, one per batch signature (see run_batch).
   int graphs = 0;
   std::vector<struct GraphEntry*> gcache;
@@ -129,6 +134,10 @@ struct pf_ctx {
   // staging slots, each a chunk of frames on the device with the page-locked
   // tables of its launch.
   cudaStream_t h2d = nullptr, d2h = nullptr;
+  // Recorded after the border extension when mark_chain is set: the reference
+  // frame is final there, so its download can overlap the grain stage.
+  cudaEvent_t chain_done = nullptr;
+  bool mark_chain = false;
   struct HostSlot {
     DevBuf io, disp;
     void* pjobs = nullptr;
@@ -559,6 +568,7 @@ extern "C" void pf_destroy(pf_ctx* c) {
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   cudaEventDestroy(c->fork);
   cudaEventDestroy(c->join);
+  if (c->chain_done) cudaEventDestroy(c->chain_done);
   cudaStreamDestroy(c->side);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -672,7 +682,8 @@ static const void* put_side(Bytes& hs, Cursor& dev, const void* src, size_t n) {
 }
 
 template <class Bytes>
-static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, Bytes& hs, FrameJob& J, int counts[ST_COUNT]) {
+static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, Bytes& hs, FrameJob& J, int counts[ST_COUNT],
+                     int dbTile) {
   const pf_frame* f = r.f;
   const pf_frame_side* s = r.s;
   const int bps = bps_of(f);
@@ -704,12 +715,13 @@ static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, Bytes& hs, 
     a.gate_chroma[1] = f->mono || lumaZero || lf.level_u == 0;
     a.gate_chroma[2] = f->mono || lumaZero || lf.level_v == 0;
     int tiles = 0;
+    J.db_tile = dbTile;
     for (int p = 0; p < 3; p++) {
       if (a.gate_chroma[p]) continue;
       const int sx = p ? f->ss_x : 0, sy = p ? f->ss_y : 0;
       const int w4 = (((f->width + sx) >> sx) + 3) >> 2, h4 = (((f->height + sy) >> sy) + 3) >> 2;
-      J.db_tx[p] = (w4 + 31) / 32;
-      J.db_ty[p] = (h4 + 7) / 8;
+      J.db_tx[p] = (w4 + db_tile_w(dbTile) - 1) / db_tile_w(dbTile);
+      J.db_ty[p] = (h4 + db_tile_h(dbTile) - 1) / db_tile_h(dbTile);
       tiles += J.db_tx[p] * J.db_ty[p];
     }
     counts[ST_DEBLOCK_V] = counts[ST_DEBLOCK_H] = tiles;
@@ -894,11 +906,14 @@ static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, con
   auto args = [&](int k, int* grid) {
     BatchArgs a = b;
     const int t = total(k);
-    if (c->persistent[k] > 0 && t > c->persistent[k]) {
+    a.chunk = c->chunk[k];
+    a.ahead = c->ahead[k];
+    const int chunks = (t + a.chunk - 1) / a.chunk;
+    if (c->persistent[k] > 0 && chunks > c->persistent[k]) {
       *grid = c->persistent[k];
       a.counters = (int*)c->counters.p;
     } else {
-      *grid = t;
+      *grid = chunks;
       a.counters = nullptr;
     }
     return a;
@@ -929,6 +944,7 @@ static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, con
   a = args(ST_EXTEND, &g);
   CK(launch_extend_batch(a, total(ST_EXTEND), g, st));
   if (c->timing) CK(cudaEventRecord(c->ev[4], st));
+  if (c->mark_chain) CK(cudaEventRecord(c->chain_done, st));
   if (fg) CK(cudaStreamWaitEvent(st, c->join, 0));
   a = args(ST_FG_APPLY, &g);
   CK(launch_fg_apply_batch(a, total(ST_FG_APPLY), g, st));
@@ -945,7 +961,12 @@ static std::vector<int64_t> batch_key(const pf_ctx* c, int n, bool fg) {
   k.push_back(n);
   k.push_back((int64_t)c->hside.size());
   k.push_back(fg);
-  for (int i = 0; i < ST_COUNT; i++) k.push_back(c->persistent[i]);
+  for (int i = 0; i < ST_COUNT; i++) {
+    k.push_back(c->persistent[i]);
+    k.push_back(c->chunk[i]);
+    k.push_back(c->ahead[i]);
+  }
+  k.push_back(c->db_tile);
   for (int v : c->hbase) k.push_back(v);
   return k;
 }
@@ -1030,7 +1051,7 @@ static int prepare_batch(pf_ctx* c, const FrameRef* refs, int n, Bytes& hs, DevB
   uint32_t done = 0;
   for (int i = 0; i < n; i++) {
     int counts[ST_COUNT];
-    fill_job(refs[i], arena, side, hs, c->hjobs[i], counts);
+    fill_job(refs[i], arena, side, hs, c->hjobs[i], counts, c->db_tile);
     for (int k = 0; k < ST_COUNT; k++) c->hbase[(size_t)k * (n + 1) + i + 1] = c->hbase[(size_t)k * (n + 1) + i] + counts[k];
     const pf_frame_side* s = refs[i].s;
     if (counts[ST_DEBLOCK_V]) done |= PF_STAGE_LOOP_FILTER;
@@ -1196,12 +1217,29 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
       }
     }
   }
+  // Host reference and display frames: the reference frame goes down on the
+  // copy stream as soon as the border extension has run, beside the grain
+  // stage and ahead of the display frame's download.
+  const bool split = f->memory == PF_MEM_HOST && wantDisp && display->memory == PF_MEM_HOST;
+  if (split && !c->d2h) {
+    CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+  }
+  if (split && !c->chain_done) CK(cudaEventCreateWithFlags(&c->chain_done, cudaEventDisableTiming));
+  c->mark_chain = split;
   st = run_batch(c, &r, 1, stats);
+  c->mark_chain = false;
   if (st != PF_OK) return st;
-  if (f->memory == PF_MEM_HOST) CK(copy_planes(f, r.io, r.ioStride, false, c->stream));
+  if (split) {
+    CK(cudaStreamWaitEvent(c->d2h, c->chain_done, 0));
+    CK(copy_planes(f, r.io, r.ioStride, false, c->d2h));
+  } else if (f->memory == PF_MEM_HOST) {
+    CK(copy_planes(f, r.io, r.ioStride, false, c->stream));
+  }
   if (wantDisp && display->memory == PF_MEM_HOST) CK(copy_planes(display, r.dp, r.dStride, false, c->stream));
   if (f->memory == PF_MEM_HOST || (wantDisp && display->memory == PF_MEM_HOST) || c->timing) {
     CKW(wait_stream(c, c->stream, __LINE__));
+    if (split) CKW(wait_stream(c, c->d2h, __LINE__));
     read_stage_times(c, stats);
   }
   CK(cudaGetLastError());
@@ -1607,6 +1645,34 @@ static const int kTuneStages[PF_TUNE_GROUPS][2] = {
     {ST_DEBLOCK_V, ST_DEBLOCK_H}, {ST_CDEF, -1}, {ST_LR, -1}, {ST_FG_APPLY, -1}};
 static const int kTuneStatIndex[PF_TUNE_GROUPS] = {0, 1, 2, 4};  // pf_stats.stage_ms
 
+static bool schedule_ok(int group, const pf_schedule& s) {
+  return s.ctas >= 0 && s.ctas <= (1 << 20) && s.units_per_cta >= 1 && s.units_per_cta <= 16 && s.staging >= 0 &&
+         s.staging <= 3 && (s.staging == 0 || s.staging < s.units_per_cta) && s.tile >= 0 &&
+         s.tile <= (group == PF_TUNE_DEBLOCK ? 3 : 0);
+}
+
+extern "C" int pf_set_schedule(pf_ctx* c, int32_t group, const pf_schedule* s) {
+  if (!c || !s || group < 0 || group >= PF_TUNE_GROUPS || !schedule_ok(group, *s)) return PF_ERR_INVALID_ARG;
+  for (int k : kTuneStages[group])
+    if (k >= 0) {
+      c->persistent[k] = s->ctas;
+      c->chunk[k] = s->units_per_cta;
+      c->ahead[k] = s->staging;
+    }
+  if (group == PF_TUNE_DEBLOCK) c->db_tile = s->tile;
+  return PF_OK;
+}
+
+extern "C" int pf_get_schedule(const pf_ctx* c, int32_t group, pf_schedule* s) {
+  if (!c || !s || group < 0 || group >= PF_TUNE_GROUPS) return PF_ERR_INVALID_ARG;
+  const int k = kTuneStages[group][0];
+  s->ctas = c->persistent[k];
+  s->units_per_cta = c->chunk[k];
+  s->staging = c->ahead[k];
+  s->tile = group == PF_TUNE_DEBLOCK ? c->db_tile : 0;
+  return PF_OK;
+}
+
 extern "C" int pf_set_persistent(pf_ctx* c, int32_t group, int32_t ctas) {
   if (!c || group < 0 || group >= PF_TUNE_GROUPS || ctas < 0 || ctas > (1 << 20)) return PF_ERR_INVALID_ARG;
   for (int k : kTuneStages[group])
@@ -1619,32 +1685,61 @@ extern "C" int pf_autotune(pf_ctx* c, const pf_batch_item* items, int32_t n, int
   const int savedTiming = c->timing;
   c->timing = 1;  // per-stage CUDA events; no graphs while timing
   memset(out, 0, sizeof(*out));
-  static const int kMult[] = {0, 1, 2, 4, 8, 16};  // x SM count; 0 = one CTA per work item
   int status = PF_OK;
-  for (int gi = 0; gi < PF_TUNE_GROUPS && status == PF_OK; gi++) {
-    float best = 3.4e38f;
-    int bestCtas = 0;
-    for (int m : kMult) {
-      const int ctas = m * c->sm_count;
-      pf_set_persistent(c, gi, ctas);
-      std::vector<float> t;
-      for (int r = 0; r <= reps && status == PF_OK; r++) {  // run 0 warms up
-        pf_stats st;
-        status = pf_batch_apply(c, items, n, &st);
-        if (r > 0 && status == PF_OK) t.push_back(st.stage_ms[kTuneStatIndex[gi]]);
-      }
-      if (status != PF_OK) break;
-      std::sort(t.begin(), t.end());
-      const float med = t[t.size() / 2];
-      if (m == 0) out->ms_default[gi] = med;
-      if (med < best) {
-        best = med;
-        bestCtas = ctas;
-      }
+  // Median stage time of group gi under schedule s.
+  auto measure = [&](int gi, const pf_schedule& s, float* med) {
+    pf_set_schedule(c, gi, &s);
+    std::vector<float> t;
+    for (int r = 0; r <= reps && status == PF_OK; r++) {  // run 0 warms up
+      pf_stats st;
+      status = pf_batch_apply(c, items, n, &st);
+      if (r > 0 && status == PF_OK) t.push_back(st.stage_ms[kTuneStatIndex[gi]]);
     }
-    pf_set_persistent(c, gi, bestCtas);
-    out->ctas[gi] = bestCtas;
-    out->ms[gi] = best;
+    if (status != PF_OK) return false;
+    std::sort(t.begin(), t.end());
+    *med = t[t.size() / 2];
+    return true;
+  };
+  for (int gi = 0; gi < PF_TUNE_GROUPS && status == PF_OK; gi++) {
+    pf_schedule best{0, 1, 0, 0};
+    float bestMs = 0;
+    if (!measure(gi, best, &bestMs)) break;
+    out->ms_default[gi] = bestMs;
+    // One dimension at a time, each from the best schedule so far.
+    auto tryOne = [&](pf_schedule cand) {
+      if (!schedule_ok(gi, cand) || status != PF_OK) return;
+      float ms;
+      if (measure(gi, cand, &ms) && ms < bestMs) {
+        bestMs = ms;
+        best = cand;
+      }
+    };
+    if (gi == PF_TUNE_DEBLOCK)
+      for (int t = 1; t <= 3; t++) {
+        pf_schedule s = best;
+        s.tile = t;
+        tryOne(s);
+      }
+    for (int u : {2, 4, 8}) {
+      pf_schedule s = best;
+      s.units_per_cta = u;
+      s.staging = 0;
+      tryOne(s);
+    }
+    for (int d = 1; d <= 2; d++) {
+      pf_schedule s = best;
+      s.staging = d;
+      tryOne(s);
+    }
+    for (int m : {1, 2, 4, 8, 16}) {
+      pf_schedule s = best;
+      s.ctas = m * c->sm_count;
+      tryOne(s);
+    }
+    if (status != PF_OK) break;
+    pf_set_schedule(c, gi, &best);
+    out->chosen[gi] = best;
+    out->ms[gi] = bestMs;
   }
   c->timing = savedTiming;
   return status;

@@ -97,7 +97,7 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
     const int tx = tid % uwMax, ty0 = tid / uwMax;
     if (!active) {
       // Copy-through (inactive unit / plane or the CDEF stage is off).
-      if (tx < unitW) copy_column<T>(ip, op, unitX + tx, unitY + ty0, unitY + unitH, rowStep);
+      copy_block<T>(ip, op, unitX, unitX + unitW, unitY, unitY + unitH);
     } else {
       // ---- stage the unit + halo (frameWorkFillCDEFInputSentinels /
       //      frameWorkCopyCDEFInput with the replicate quirk) ----
@@ -311,16 +311,33 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
 __global__ void __launch_bounds__(256, 4) k_cdef_batch(BatchArgs b) {
   __shared__ CdefSmem sm;
   const int* base = b.base + ST_CDEF * (b.n + 1);
-  for_each_item(base[b.n], b.counters ? b.counters + ST_CDEF : nullptr, [&](int item) {
-    const int fi = find_frame(base, b.n, item);
-    const FrameJob& J = b.jobs[fi];
-    const int local = item - base[fi];
-    const int uc = local % J.cdef.ucols, ur = local / J.cdef.ucols;
-    if (J.io.bd == 8)
-      cdef_unit<uint8_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, sm);
-    else
-      cdef_unit<uint16_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, sm);
-  });
+  for_each_item(
+      b, ST_CDEF, base[b.n],
+      [&](int item) {
+        const int fi = find_frame(base, b.n, item);
+        const FrameJob& J = b.jobs[fi];
+        const int local = item - base[fi];
+        const int uc = local % J.cdef.ucols, ur = local / J.cdef.ucols;
+        if (J.io.bd == 8)
+          cdef_unit<uint8_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, sm);
+        else
+          cdef_unit<uint16_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, sm);
+      },
+      [&](int item) {
+        // Every plane's unit with its 8-column / 2-row halo.
+        const int fi = find_frame(base, b.n, item);
+        const FrameJob& J = b.jobs[fi];
+        const int local = item - base[fi];
+        const int uc = local % J.cdef.ucols, ur = local / J.cdef.ucols;
+        for (int plane = 0; plane < (J.io.mono ? 1 : 3); plane++) {
+          const int xdec = plane ? J.io.ssx : 0, ydec = plane ? J.io.ssy : 0;
+          const int x = (uc * 64) >> xdec, y = (ur * 64) >> ydec;
+          if (J.io.bd == 8)
+            prefetch_block<uint8_t>(J.io.pl[plane], x - 8, x + (64 >> xdec) + 8, y - 2, y + (64 >> ydec) + 2);
+          else
+            prefetch_block<uint16_t>(J.io.pl[plane], x - 8, x + (64 >> xdec) + 8, y - 2, y + (64 >> ydec) + 2);
+        }
+      });
 }
 
 cudaError_t launch_cdef_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {

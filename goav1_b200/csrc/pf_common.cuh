@@ -42,6 +42,47 @@ __device__ __forceinline__ void copy_column(const DPlane& from, const DPlane& to
   }
 }
 
+// Copies the block [x0, x1) x [y0, y1) of one plane to another (the planes
+// may not alias) with the whole CTA: 16-byte words, up to four per thread in
+// flight, when both rows' starts and strides are 16-byte aligned and a row is
+// a whole number of words; otherwise column by column.
+template <typename T>
+__device__ __forceinline__ void copy_block(const DPlane& from, const DPlane& to, int x0, int x1, int y0, int y1) {
+  if (x1 <= x0 || y1 <= y0) return;
+  const int rowBytes = (x1 - x0) * (int)sizeof(T);
+  const uint8_t* s0 = from.ptr + (int64_t)y0 * from.stride + (int64_t)x0 * sizeof(T);
+  uint8_t* d0 = to.ptr + (int64_t)y0 * to.stride + (int64_t)x0 * sizeof(T);
+  if (((reinterpret_cast<uintptr_t>(s0) | reinterpret_cast<uintptr_t>(d0) | (uintptr_t)from.stride |
+        (uintptr_t)to.stride | (uintptr_t)rowBytes) & 15) == 0) {
+    const int wpr = rowBytes >> 4, total = (y1 - y0) * wpr;
+    for (int i0 = threadIdx.x; i0 < total; i0 += 4 * blockDim.x) {
+      uint4 v[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int i = i0 + k * blockDim.x;
+        if (i < total) {
+          const int r = i / wpr, c = i - r * wpr;
+          v[k] = *reinterpret_cast<const uint4*>(s0 + (int64_t)r * from.stride + c * 16);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int i = i0 + k * blockDim.x;
+        if (i < total) {
+          const int r = i / wpr, c = i - r * wpr;
+          *reinterpret_cast<uint4*>(d0 + (int64_t)r * to.stride + c * 16) = v[k];
+        }
+      }
+    }
+    return;
+  }
+  const int w = x1 - x0;
+  for (int i = threadIdx.x; i < w * (y1 - y0); i += blockDim.x) {
+    const int r = i / w, c = i - r * w;
+    row_ptr<T>(to, y0 + r)[x0 + c] = row_ptr<T>(from, y0 + r)[x0 + c];
+  }
+}
+
 __host__ __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 __host__ __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ __forceinline__ int iclip(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -134,7 +175,8 @@ struct FrameJob {
   FgArgs fg;
   FgTemplateArgs fgt;
   int aw[3], ah[3];          // MI-aligned plane extents
-  int db_tx[3], db_ty[3];    // deblock tiles (32x8 edge units) per plane (0 = gated)
+  int db_tile;               // deblocking tile shape (db_tile_w / db_tile_h)
+  int db_tx[3], db_ty[3];    // deblock tiles per plane (0 = gated)
   int lr_cols[3], lr_rows[3];  // restoration tiles (processing column x stripe)
   int fg_tx[3], fg_ty[3];    // 64x64-sample tiles of the display planes
   int ext_r[3][2], ext_b[3][2];  // extension tiles: right strip, bottom strip
@@ -146,7 +188,38 @@ struct BatchArgs {
   const int* base;  // ST_COUNT arrays of n+1 ints, stage-major
   int n;
   int* counters;    // ST_COUNT work counters (persistent mode), or null
+  // The launch's schedule (pf_schedule): consecutive work items a CTA takes
+  // at a time (one launch grid slot, or one counter grab when persistent),
+  // and how many items ahead of the current one the CTA prefetches into L2.
+  int chunk;
+  int ahead;
 };
+
+// Deblocking tile shapes (pf_schedule.tile): width x height in 4x4 edge
+// units, 256 units (one per thread) a tile.
+__host__ __device__ __forceinline__ int db_tile_w(int tile) { return tile == 1 ? 64 : tile == 2 ? 16 : tile == 3 ? 8 : 32; }
+__host__ __device__ __forceinline__ int db_tile_h(int tile) { return 256 / db_tile_w(tile); }
+
+// Prefetches the samples [x0, x1) x [y0, y1) of a plane (clamped to its
+// allocation) into L2, one 128-byte line per thread at a time.  A hint only:
+// nothing is read into registers and nothing is ordered.
+template <typename T>
+__device__ __forceinline__ void prefetch_block(const DPlane& p, int x0, int x1, int y0, int y1) {
+  x0 = x0 < 0 ? 0 : x0;
+  y0 = y0 < 0 ? 0 : y0;
+  x1 = x1 > p.aw ? p.aw : x1;
+  y1 = y1 > p.ah ? p.ah : y1;
+  if (x1 <= x0 || y1 <= y0) return;
+  const uintptr_t row0 = reinterpret_cast<uintptr_t>(p.ptr) + (uintptr_t)x0 * sizeof(T);
+  const uintptr_t l0 = row0 & ~(uintptr_t)127;
+  const int lines = (int)(((row0 + (uintptr_t)(x1 - x0) * sizeof(T) - 1) >> 7) - (l0 >> 7)) + 1;
+  const int n = lines * (y1 - y0);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int r = i / lines, l = i - r * lines;
+    const uintptr_t a = ((row0 + (uintptr_t)(y0 + r) * (uintptr_t)p.stride) & ~(uintptr_t)127) + (uintptr_t)l * 128;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+  }
+}
 
 __device__ __forceinline__ int find_frame(const int* base, int n, int item) {
   int lo = 0, hi = n;  // base[lo] <= item < base[hi]
@@ -157,23 +230,53 @@ __device__ __forceinline__ int find_frame(const int* base, int n, int item) {
   return lo;
 }
 
-// Runs f(item) for the CTA's work items: one item per CTA (grid = total), or
-// a persistent CTA draining the stage's queue through an atomic counter.
-template <typename F>
-__device__ __forceinline__ void for_each_item(int total, int* counter, F f) {
+// Runs f(item) over the items [first, last) of one chunk, prefetch(item)
+// for the items `ahead` places further on inside the chunk, a barrier
+// between items.
+template <typename F, typename P>
+__device__ __forceinline__ void run_chunk(int first, int last, int ahead, F& f, P& prefetch) {
+  for (int it = first; it < last; it++) {
+    if (it != first) __syncthreads();
+    if (ahead > 0) {
+      if (it == first)
+        for (int k = 1; k <= ahead && first + k < last; k++) prefetch(first + k);
+      else if (it + ahead < last)
+        prefetch(it + ahead);
+    }
+    f(it);
+  }
+}
+
+// Runs f(item) for the CTA's work items: a chunk of b.chunk consecutive
+// items per CTA (grid = ceil(total / chunk)), or a persistent CTA draining
+// the stage's queue a chunk at a time through an atomic counter.  Inside a
+// chunk, prefetch(item) warms L2 with the input of the item b.ahead places
+// on.  Every item is independent of the others, so no schedule changes a
+// result.
+template <typename F, typename P>
+__device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, int total, F f, P prefetch) {
+  const int chunk = b.chunk > 1 ? b.chunk : 1;
+  int* counter = b.counters ? b.counters + stage : nullptr;
   if (counter == nullptr) {
-    if ((int)blockIdx.x < total) f((int)blockIdx.x);
+    const int first = (int)blockIdx.x * chunk;
+    run_chunk(first, first + chunk < total ? first + chunk : total, b.ahead, f, prefetch);
     return;
   }
   __shared__ int s_item;
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, chunk);
     __syncthreads();
-    const int it = s_item;
-    if (it >= total) break;
-    f(it);
+    const int first = s_item;
+    if (first >= total) break;
+    run_chunk(first, first + chunk < total ? first + chunk : total, b.ahead, f, prefetch);
   }
+}
+
+template <typename F>
+__device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, int total, F f) {
+  auto none = [](int) {};
+  for_each_item(b, stage, total, f, none);
 }
 
 }  // namespace pf

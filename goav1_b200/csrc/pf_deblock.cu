@@ -260,27 +260,51 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
     lpf_unit<T>(q, 1, sstride, bd, E, I, H, wd, P, Q);
 }
 
-// Batched deblocking: each work item is one 32x8 tile of edge units of one
-// plane of one frame; 256 threads, one edge unit each.
+// Batched deblocking: each work item is one tile of edge units of one plane
+// of one frame (db_tile_w x db_tile_h units, 32x8 by default); 256 threads,
+// one edge unit each.
+struct DbTile {
+  const FrameJob* J;
+  int plane, tx, ty;
+};
+
+__device__ __forceinline__ DbTile db_locate(const BatchArgs& b, const int* base, int item) {
+  const int fi = find_frame(base, b.n, item);
+  const FrameJob& J = b.jobs[fi];
+  int local = item - base[fi];
+  int plane = 0;
+  while (plane < 2 && local >= J.db_tx[plane] * J.db_ty[plane]) {
+    local -= J.db_tx[plane] * J.db_ty[plane];
+    plane++;
+  }
+  return DbTile{&J, plane, local % J.db_tx[plane], local / J.db_tx[plane]};
+}
+
 __global__ void __launch_bounds__(256, 4) k_deblock_batch(BatchArgs b, int dir) {
   const int stage = dir == 0 ? ST_DEBLOCK_V : ST_DEBLOCK_H;
   const int* base = b.base + stage * (b.n + 1);
-  for_each_item(base[b.n], b.counters ? b.counters + stage : nullptr, [&](int item) {
-    const int fi = find_frame(base, b.n, item);
-    const FrameJob& J = b.jobs[fi];
-    int local = item - base[fi];
-    int plane = 0;
-    while (plane < 2 && local >= J.db_tx[plane] * J.db_ty[plane]) {
-      local -= J.db_tx[plane] * J.db_ty[plane];
-      plane++;
-    }
-    const int tx = local % J.db_tx[plane], ty = local / J.db_tx[plane];
-    const int c4 = tx * 32 + (threadIdx.x & 31), r4 = ty * 8 + (threadIdx.x >> 5);
-    if (J.io.bd == 8)
-      deblock_unit<uint8_t>(J.io, J.lf, dir, plane, c4, r4);
-    else
-      deblock_unit<uint16_t>(J.io, J.lf, dir, plane, c4, r4);
-  });
+  for_each_item(
+      b, stage, base[b.n],
+      [&](int item) {
+        const DbTile t = db_locate(b, base, item);
+        const FrameJob& J = *t.J;
+        const int tw = db_tile_w(J.db_tile), lg = 31 - __clz(tw);
+        const int c4 = t.tx * tw + (threadIdx.x & (tw - 1)), r4 = t.ty * (256 >> lg) + (threadIdx.x >> lg);
+        if (J.io.bd == 8)
+          deblock_unit<uint8_t>(J.io, J.lf, dir, t.plane, c4, r4);
+        else
+          deblock_unit<uint16_t>(J.io, J.lf, dir, t.plane, c4, r4);
+      },
+      [&](int item) {
+        // The tile's samples and the 8 on each side its edges can reach.
+        const DbTile t = db_locate(b, base, item);
+        const int tw = db_tile_w(t.J->db_tile), th = 256 / tw;
+        const int x0 = t.tx * tw * 4, y0 = t.ty * th * 4;
+        if (t.J->io.bd == 8)
+          prefetch_block<uint8_t>(t.J->io.pl[t.plane], x0 - 8, x0 + tw * 4 + 8, y0 - 8, y0 + th * 4 + 8);
+        else
+          prefetch_block<uint16_t>(t.J->io.pl[t.plane], x0 - 8, x0 + tw * 4 + 8, y0 - 8, y0 + th * 4 + 8);
+      });
 }
 
 cudaError_t launch_deblock_batch(const BatchArgs& b, int total, int grid, int dir, cudaStream_t st) {

@@ -13,7 +13,7 @@
 // GF(2)^16, so lane k starts from M^(kL) * seed (jump matrices precomputed on
 // the host) and walks its L draws; the AR filter runs as a wavefront over
 // t = x + 4y (every AR input of sample (y, x) has a smaller t), one warp per
-// template, rows in lanes, neighbours by warp shuffles.  Offsets
+// template, rows in lanes, neighbours read from the shared template.  Offsets
 // come from one thread per 32-row stripe.  The apply is one thread per output
 // sample, 64x16-sample tiles per CTA.
 #include "pf_common.cuh"
@@ -35,25 +35,28 @@ __device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
 
 // AR recursion of one template (luma.go:83-158 / chroma.go:92-199 generic
 // form), run by one warp as a wavefront with no CTA barrier.  The template's
-// AR rows are taken in bands of 32 rows, one row per lane; at step t lane r
-// (row y) handles column x = t - 4r, so the neighbour it needs from row y-d
-// at column x + LAG was produced by lane r-d at step t - 4d + LAG.  Every
-// lane keeps a short history H of its own outputs and the neighbours come
-// across by __shfl_up_sync (lanes r < d read the rows above the band, which
-// are final, from shared memory); each row's 2*LAG+1-wide window of the rows
-// above and its own LAG previous outputs slide in registers.  Only the
-// shuffle from the lane directly above is on the loop-carried path.  A lane
-// outside the AR columns passes the template's value through unchanged, so
-// the windows always hold the template as it stands.  Bands run one after
-// the other; the LAG is a template argument (coefficients in registers,
-// unrolled taps).
+// AR rows are taken in bands of up to 32 rows, one row per lane; at step t
+// lane r (row y) handles column x = t - 4r, so every sample of the rows
+// above that its output needs (columns up to x + LAG <= x + 3) was written
+// to the shared template by lanes r-1.. at an earlier step, and the warp
+// barrier that ends each step makes it visible.  The filter runs in
+// transposed form: when the value of row y-d at column x + LAG arrives, its
+// products go straight into the partial sums acc[j] of the outputs x .. x +
+// 2*LAG it reaches, and the lane's own output adds its in-row products to
+// acc[1..LAG]; the output then needs only acc[0] (and the luma term), so a
+// step is one new load per row above, 3*(2*LAG+1) + LAG multiply-adds and a
+// shift of the partial sums, and its loop-carried path is load -> one
+// multiply-add -> round -> clip -> store.  A lane outside the AR columns
+// passes the template's value through unchanged, so the rows above always
+// hold the template as it stands.  Bands run one after the other, each only
+// as long as its own rows need.  LAG is a template argument (coefficients
+// in registers, unrolled taps).
 constexpr int kFgTemplateThreads = 96;
 
 template <int LAG>
 __device__ void ar_warp(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h) {
   constexpr int kTaps = 2 * LAG * (LAG + 1);  // causal neighbours before the centre
   constexpr int W = 2 * LAG + 1;
-  constexpr int HL = 3 * LAG > 0 ? 3 * LAG : 1;  // history: the outputs of steps t-1 .. t-3*LAG
   const int lane = threadIdx.x & 31;
   const int cs = p.coeff_shift, ro = 1 << (cs - 1);
   const int gmin = -(1 << (p.bd - 1)), gmax = (1 << (p.bd - 1)) - 1;
@@ -63,62 +66,55 @@ __device__ void ar_warp(int16_t* g, const int16_t* luma, const FgTemplateArgs& p
   const bool lumaTerm = plane != 0 && p.num_y_points != 0;
   const int sx = plane ? p.ssx : 0, sy = plane ? p.ssy : 0;
   for (int y0 = 3; y0 < h; y0 += 32) {
+    const int rows = imin(32, h - y0);
     const int y = y0 + lane;
-    const bool row = y < h;
-    int win[LAG > 0 ? LAG : 1][W];  // win[d-1][c]: row y-d, column x-LAG+c
-    int H[HL];
+    const bool row = lane < rows;
+    int acc[W];  // acc[j]: partial sum of output column x + j
 #pragma unroll
-    for (int d = 0; d < (LAG > 0 ? LAG : 1); d++)
-#pragma unroll
-      for (int c = 0; c < W; c++) win[d][c] = 0;
-#pragma unroll
-    for (int k = 0; k < HL; k++) H[k] = 0;
-    const int tend = 4 * 31 + w;
+    for (int j = 0; j < W; j++) acc[j] = 0;
+    // The first step brings column 0 of the rows above into the windows;
+    // the last one finishes column w - 4 of the band's last row.
+    const int tend = 4 * (rows - 1) + w - 3;
     for (int t = -LAG; t < tend; t++) {
       const int x = t - 4 * lane;
       const int xn = x + LAG;  // the column entering the windows
+      const bool inCol = row && x >= 0 && x < w;
+      const int g0 = inCol ? g[y * kGW + x] : 0;
+      if (row && xn >= 0 && xn < w) {
+        // Farthest row first: the row directly above (written one step ago
+        // when LAG = 3) enters the sum of this step's output last.
 #pragma unroll
-      for (int d = 1; d <= LAG; d++) {
-        int v = __shfl_up_sync(0xffffffffu, H[4 * d - LAG - 1], d);
-        if (lane < d) v = (xn >= 0 && xn < w) ? g[(y - d) * kGW + xn] : 0;
+        for (int d = LAG; d >= 1; d--) {
+          const int v = g[(y - d) * kGW + xn];
 #pragma unroll
-        for (int c = 0; c + 1 < W; c++) win[d - 1][c] = win[d - 1][c + 1];
-        win[d - 1][W - 1] = v;
-      }
-      int out = 0;
-      if (row && x >= 0 && x < w) {
-        const int g0 = g[y * kGW + x];
-        out = g0;
-        if (x >= 3 && x < w - 3) {
-          int sum = 0;
-#pragma unroll
-          for (int d = 1; d <= LAG; d++) {
-            int part = 0;
-#pragma unroll
-            for (int c = 0; c < W; c++) part += co[(LAG - d) * W + c] * win[d - 1][c];
-            sum += part;
-          }
-#pragma unroll
-          for (int c = 0; c < LAG; c++) sum += co[LAG * W + c] * H[LAG - 1 - c];
-          if (lumaTerm) {
-            const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
-            int s = luma[ly * kGW + lx];
-            if (sx) s += luma[ly * kGW + lx + 1];
-            if (sy) {
-              s += luma[(ly + 1) * kGW + lx];
-              if (sx) s += luma[(ly + 1) * kGW + lx + 1];
-            }
-            sum += rpow2(s, sx + sy) * co[kTaps];
-          }
-          out = iclip(g0 + ((sum + ro) >> cs), gmin, gmax);
-          g[y * kGW + x] = (int16_t)out;
+          for (int j = W - 1; j >= 0; j--) acc[j] += co[(LAG - d) * W + 2 * LAG - j] * v;
         }
       }
+      int out = g0;
+      if (inCol && x >= 3 && x < w - 3) {
+        int sum = acc[0];
+        if (lumaTerm) {
+          const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
+          int s = luma[ly * kGW + lx];
+          if (sx) s += luma[ly * kGW + lx + 1];
+          if (sy) {
+            s += luma[(ly + 1) * kGW + lx];
+            if (sx) s += luma[(ly + 1) * kGW + lx + 1];
+          }
+          sum += rpow2(s, sx + sy) * co[kTaps];
+        }
+        out = iclip(g0 + ((sum + ro) >> cs), gmin, gmax);
+        g[y * kGW + x] = (int16_t)out;
+      }
+      // This output's in-row products for columns x + 1 .. x + LAG, then
+      // the partial sums move one column on.
 #pragma unroll
-      for (int k = HL - 1; k > 0; k--) H[k] = H[k - 1];
-      H[0] = out;
+      for (int m = 1; m <= LAG; m++) acc[m] += co[LAG * W + LAG - m] * out;
+#pragma unroll
+      for (int j = 0; j + 1 < W; j++) acc[j] = acc[j + 1];
+      acc[W - 1] = 0;
+      __syncwarp();
     }
-    __syncwarp();  // this band's rows are final for the next band's first lanes
   }
 }
 
@@ -343,7 +339,7 @@ __global__ void __launch_bounds__(kFgTemplateThreads) k_fg_templates_batch(Batch
   for (int i = threadIdx.x; i < 2048; i += blockDim.x) s_gauss[i] = c_gauss[i];
   __syncthreads();
   const int* base = b.base + ST_FG_TEMPLATES * (b.n + 1);
-  for_each_item(base[b.n], b.counters ? b.counters + ST_FG_TEMPLATES : nullptr, [&](int item) {
+  for_each_item(b, ST_FG_TEMPLATES, base[b.n], [&](int item) {
     const FrameJob& J = b.jobs[find_frame(base, b.n, item)];
     fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], s_g, s_gauss);
   });
@@ -351,7 +347,7 @@ __global__ void __launch_bounds__(kFgTemplateThreads) k_fg_templates_batch(Batch
 
 __global__ void __launch_bounds__(64) k_fg_offsets_batch(BatchArgs b) {
   const int* base = b.base + ST_FG_OFFSETS * (b.n + 1);
-  for_each_item(base[b.n], b.counters ? b.counters + ST_FG_OFFSETS : nullptr, [&](int item) {
+  for_each_item(b, ST_FG_OFFSETS, base[b.n], [&](int item) {
     const int fi = find_frame(base, b.n, item);
     const FrameJob& J = b.jobs[fi];
     const int r = (item - base[fi]) * 64 + threadIdx.x;
@@ -363,36 +359,58 @@ __global__ void __launch_bounds__(64) k_fg_offsets_batch(BatchArgs b) {
 // thread's rows stay inside one grain block: blocks are 32 or 16 rows high,
 // and a thread's per-column set-up is spread over 16 samples).
 // The plane's scaling table is staged in shared memory per tile.
+struct FgTile {
+  const FrameJob* J;
+  int plane, tx, ty;
+};
+
+__device__ __forceinline__ FgTile fg_locate(const BatchArgs& b, const int* base, int item) {
+  const int fi = find_frame(base, b.n, item);
+  const FrameJob& J = b.jobs[fi];
+  int local = item - base[fi];
+  int plane = 0;
+  while (plane < 2 && local >= J.fg_tx[plane] * J.fg_ty[plane]) {
+    local -= J.fg_tx[plane] * J.fg_ty[plane];
+    plane++;
+  }
+  return FgTile{&J, plane, local % J.fg_tx[plane], local / J.fg_tx[plane]};
+}
+
 __global__ void __launch_bounds__(256, 6) k_fg_apply_batch(BatchArgs b) {
   __shared__ uint8_t s_lut[256];
   const int* base = b.base + ST_FG_APPLY * (b.n + 1);
-  for_each_item(base[b.n], b.counters ? b.counters + ST_FG_APPLY : nullptr, [&](int item) {
-    const int fi = find_frame(base, b.n, item);
-    const FrameJob& J = b.jobs[fi];
-    int local = item - base[fi];
-    int plane = 0;
-    while (plane < 2 && local >= J.fg_tx[plane] * J.fg_ty[plane]) {
-      local -= J.fg_tx[plane] * J.fg_ty[plane];
-      plane++;
-    }
-    s_lut[threadIdx.x] = J.fg.lut[plane][threadIdx.x];
-    __syncthreads();
-    const int tx = local % J.fg_tx[plane], ty = local / J.fg_tx[plane];
-    const int x = tx * 64 + (threadIdx.x & 63);
-    const int y0 = ty * 64 + (threadIdx.x >> 6) * 16;
-    if (J.io.bd == 8)
-      fg_apply_col<uint8_t>(J.io, J.disp, J.fg, s_lut, plane, x, y0, 16);
-    else
-      fg_apply_col<uint16_t>(J.io, J.disp, J.fg, s_lut, plane, x, y0, 16);
-    __syncthreads();  // the table is rewritten by the next tile (persistent CTAs)
-  });
+  for_each_item(
+      b, ST_FG_APPLY, base[b.n],
+      [&](int item) {
+        const FgTile t = fg_locate(b, base, item);
+        const FrameJob& J = *t.J;
+        s_lut[threadIdx.x] = J.fg.lut[t.plane][threadIdx.x];
+        __syncthreads();
+        const int x = t.tx * 64 + (threadIdx.x & 63);
+        const int y0 = t.ty * 64 + (threadIdx.x >> 6) * 16;
+        if (J.io.bd == 8)
+          fg_apply_col<uint8_t>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
+        else
+          fg_apply_col<uint16_t>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
+        __syncthreads();  // the table is rewritten by the next tile
+      },
+      [&](int item) {
+        // The tile of the filtered frame (the grain's input).
+        const FgTile t = fg_locate(b, base, item);
+        const FrameJob& J = *t.J;
+        const int x0 = t.tx * 64, y0 = t.ty * 64;
+        if (J.io.bd == 8)
+          prefetch_block<uint8_t>(J.io.pl[t.plane], x0, x0 + 64, y0, y0 + 64);
+        else
+          prefetch_block<uint16_t>(J.io.pl[t.plane], x0, x0 + 64, y0, y0 + 64);
+      });
 }
 
 // Border extension: 64x4-sample tiles of the right strip [w, aw) x [0, h)
 // then of the bottom strip [0, aw) x [h, ah), per plane.
 __global__ void __launch_bounds__(256) k_extend_batch(BatchArgs b) {
   const int* base = b.base + ST_EXTEND * (b.n + 1);
-  for_each_item(base[b.n], b.counters ? b.counters + ST_EXTEND : nullptr, [&](int item) {
+  for_each_item(b, ST_EXTEND, base[b.n], [&](int item) {
     const int fi = find_frame(base, b.n, item);
     const FrameJob& J = b.jobs[fi];
     int local = item - base[fi];

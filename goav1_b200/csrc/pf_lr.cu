@@ -72,9 +72,10 @@ __device__ __forceinline__ void lr_wiener_window(LrSmem& sm, int w, int h, int b
   for (int r = warp; r < wh; r += 8) {
     for (int c = lane; c < w; c += 32) {
       const uint16_t* sw = &s_win[r * kWin + c];
-      int32_t sum = ((int32_t)sw[3] << 7) + offH;
+      // Symmetric taps (hf[k] == hf[6 - k]): pair sums first.
+      int32_t sum = ((int32_t)sw[3] << 7) + offH + (int32_t)sw[3] * hf[3];
 #pragma unroll
-      for (int k = 0; k < 7; k++) sum += (int32_t)sw[k] * hf[k];
+      for (int k = 0; k < 3; k++) sum += ((int32_t)sw[k] + (int32_t)sw[6 - k]) * hf[k];
       temp[r * 64 + c] = (uint16_t)imin(imax(rpot(sum, round0), 0), limit - 1);
     }
   }
@@ -89,9 +90,9 @@ __device__ __forceinline__ void lr_wiener_window(LrSmem& sm, int w, int h, int b
     for (int k = 0; k < 6; k++) t[k] = temp[(ya + k) * 64 + tx];
     for (int y = ya; y < yb; y++) {
       t[6] = temp[(y + 6) * 64 + tx];
-      int32_t sum = (t[3] << 7) - offV;
+      int32_t sum = (t[3] << 7) - offV + t[3] * vf[3];
 #pragma unroll
-      for (int k = 0; k < 7; k++) sum += t[k] * vf[k];
+      for (int k = 0; k < 3; k++) sum += (t[k] + t[6 - k]) * vf[k];
       out(y, tx, imin(imax(rpot(sum, round1), 0), maxv));
 #pragma unroll
       for (int k = 0; k < 6; k++) t[k] = t[k + 1];
@@ -160,10 +161,12 @@ __device__ __forceinline__ void lr_sgr_window(LrSmem& sm, int w, int h, int bd, 
           vq += v * v;
         }
       for (; rr < re; rr += step) {
-        uint32_t bs = 0, bq = 0;
-        for (int dx = -r; dx <= r; dx++) {
-          bs += __shfl_sync(0xffffffffu, vs, imin(imax(lane + dx, 0), 31));
-          bq += __shfl_sync(0xffffffffu, vq, imin(imax(lane + dx, 0), 31));
+        // Row sums of the column sums: lanes r .. 31 - r (the ones stored)
+        // read exactly lanes lane - r .. lane + r.
+        uint32_t bs = vs, bq = vq;
+        for (int dx = 1; dx <= r; dx++) {
+          bs += __shfl_up_sync(0xffffffffu, vs, dx) + __shfl_down_sync(0xffffffffu, vs, dx);
+          bq += __shfl_up_sync(0xffffffffu, vq, dx) + __shfl_down_sync(0xffffffffu, vq, dx);
         }
         if (lane >= r && lane < 32 - r && cc < ncols) {
           const int32_t sum = (int32_t)bs, sq = (int32_t)bq;
@@ -288,7 +291,7 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
     if (cand->type == PF_LR_WIENER || cand->type == PF_LR_SGRPROJ) u = cand;
   }
   if (!u) {
-    if (tx < x1 - x0) copy_column<T>(sp, dp, x0 + tx, y0 + ty0, y1, rowStep);
+    copy_block<T>(sp, dp, x0, x1, y0, y1);
     return;
   }
   const int h = yf1 - y0, w = xf1 - x0;
@@ -358,25 +361,49 @@ cudaError_t lr_upload_tables() {
 // Batched restoration: each work item is one (processing column, stripe)
 // tile of one plane of one frame.  Frames without restoration get the copy
 // of the CDEF output back into the frame.
+struct LrTile {
+  const FrameJob* J;
+  int plane, j, s;
+};
+
+__device__ __forceinline__ LrTile lr_locate(const BatchArgs& b, const int* base, int item) {
+  const int fi = find_frame(base, b.n, item);
+  const FrameJob& J = b.jobs[fi];
+  int local = item - base[fi];
+  int plane = 0;
+  while (plane < 2 && local >= J.lr_cols[plane] * J.lr_rows[plane]) {
+    local -= J.lr_cols[plane] * J.lr_rows[plane];
+    plane++;
+  }
+  return LrTile{&J, plane, local % J.lr_cols[plane], local / J.lr_cols[plane]};
+}
+
 __global__ void __launch_bounds__(256, 4) k_lr_batch(BatchArgs b) {
   extern __shared__ __align__(16) uint8_t lr_smem_raw[];
   LrSmem& sm = *reinterpret_cast<LrSmem*>(lr_smem_raw);
   const int* base = b.base + ST_LR * (b.n + 1);
-  for_each_item(base[b.n], b.counters ? b.counters + ST_LR : nullptr, [&](int item) {
-    const int fi = find_frame(base, b.n, item);
-    const FrameJob& J = b.jobs[fi];
-    int local = item - base[fi];
-    int plane = 0;
-    while (plane < 2 && local >= J.lr_cols[plane] * J.lr_rows[plane]) {
-      local -= J.lr_cols[plane] * J.lr_rows[plane];
-      plane++;
-    }
-    const int j = local % J.lr_cols[plane], s = local / J.lr_cols[plane];
-    if (J.io.bd == 8)
-      lr_tile<uint8_t>(J.scr, J.io, J.lr, J.aw, J.ah, J.do_lr, plane, j, s, sm);
-    else
-      lr_tile<uint16_t>(J.scr, J.io, J.lr, J.aw, J.ah, J.do_lr, plane, j, s, sm);
-  });
+  for_each_item(
+      b, ST_LR, base[b.n],
+      [&](int item) {
+        const LrTile t = lr_locate(b, base, item);
+        const FrameJob& J = *t.J;
+        if (J.io.bd == 8)
+          lr_tile<uint8_t>(J.scr, J.io, J.lr, J.aw, J.ah, J.do_lr, t.plane, t.j, t.s, sm);
+        else
+          lr_tile<uint16_t>(J.scr, J.io, J.lr, J.aw, J.ah, J.do_lr, t.plane, t.j, t.s, sm);
+      },
+      [&](int item) {
+        // The tile's stripe of the CDEF output with its 3-sample halo.
+        const LrTile t = lr_locate(b, base, item);
+        const FrameJob& J = *t.J;
+        const int ssx = t.plane ? J.io.ssx : 0, ssy = t.plane ? J.io.ssy : 0;
+        const int PW = 64 >> ssx, SH = 64 >> ssy, off = 8 >> ssy;
+        const int x0 = t.j * PW, y0 = t.s * SH - off;
+        if (J.io.bd == 8)
+          prefetch_block<uint8_t>(J.scr.pl[t.plane], x0 - 3, x0 + PW + 3, y0 - 3, y0 + SH + 3);
+        else
+          prefetch_block<uint16_t>(J.scr.pl[t.plane], x0 - 3, x0 + PW + 3, y0 - 3, y0 + SH + 3);
+      });
 }
 
 cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {

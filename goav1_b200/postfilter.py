@@ -140,9 +140,20 @@ class PostFilterRunner:
         """Persistent CTA count of a stage group (abi.PF_TUNE_*); 0 = one CTA per item."""
         check(lib().pf_set_persistent(self._h, group, ctas))
 
+    def set_schedule(self, group, ctas=0, units_per_cta=1, staging=0, tile=0):
+        """Schedule of a stage group (abi.PF_TUNE_*): persistent CTAs, work
+        items per CTA, items prefetched ahead, deblocking tile shape."""
+        s = abi.pf_schedule(ctas, units_per_cta, staging, tile)
+        check(lib().pf_set_schedule(self._h, group, C.byref(s)))
+
+    def get_schedule(self, group):
+        s = abi.pf_schedule()
+        check(lib().pf_get_schedule(self._h, group, C.byref(s)))
+        return s
+
     def autotune(self, items, reps=3):
-        """Picks each stage group's persistent setting on this batch (run in
-        place: pass copies).  Returns pf_tune_result."""
+        """Searches each stage group's schedule on this batch (run in place:
+        pass copies).  Returns pf_tune_result."""
         arr = items if isinstance(items, C.Array) else self.batch_items(items)
         out = abi.pf_tune_result()
         check(lib().pf_autotune(self._h, arr, len(arr), reps, C.byref(out)))

@@ -56,7 +56,7 @@
 extern "C" {
 #endif
 
-#define PF_ABI_VERSION 2
+#define PF_ABI_VERSION 3
 
 /* ---- status codes (negative = error; the frame is untouched on every error
  *      reported before any kernel was queued, mirroring the reference's
@@ -307,28 +307,51 @@ int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats*
  * prefix counts.  Two knobs shape those launches:
  *   - CUDA graphs (pf_batch_graphs): the first batch of a given signature
  *     (frame count, each frame's work per stage, side-information bytes and
- *     the persistent settings) is captured as a graph and later batches of
+ *     the schedules) is captured as a graph and later batches of
  *     that signature replay it, with only their job tables refreshed.  Up to
  *     8 signatures are kept; a change of the context's scratch buffers
  *     recaptures.  Graphs are not used while the context times stages.
- *   - Persistent CTAs (pf_set_persistent): per stage group, a fixed number
- *     of CTAs draining the stage's items through an atomic counter instead
- *     of one CTA per item (0).
- * pf_autotune picks the persistent setting of each group on a given batch:
- * for each group it runs the batch reps + 1 times per candidate (one CTA per
- * item, then 1, 2, 4, 8 and 16 CTAs per SM), keeps the candidate with the
- * lowest median stage time, and leaves the winners set on the context.  It
- * runs the batch in place, so pass frames whose contents may be overwritten
- * (copies).  out->ms_default is the one-CTA-per-item time of each group. */
+ *   - The schedule of each stage group (pf_schedule, pf_set_schedule):
+ *       ctas           persistent CTAs draining the stage's items through an
+ *                      atomic counter (0 = one CTA per chunk);
+ *       units_per_cta  consecutive work items (tiles / 64x64 units, in the
+ *                      stage's numbering: along a row first) a CTA takes at
+ *                      a time, 1..16, amortising per-item set-up;
+ *       staging        how many items ahead of the current one, inside the
+ *                      chunk, the CTA prefetches its input rows into L2
+ *                      (0..3, below units_per_cta);
+ *       tile           the tile shape, deblocking only: 0 = 32x8, 1 = 64x4,
+ *                      2 = 16x16, 3 = 8x32 edge units a tile (one thread
+ *                      each); 0 for the other groups.
+ *     Work items are independent, so every schedule gives the same samples.
+ * pf_autotune searches the schedule of each group on a given batch, one
+ * dimension at a time (tile shape, units per CTA, staging depth, persistent
+ * CTAs at 0, 1, 2, 4, 8 and 16 per SM), keeping after each the candidate
+ * with the lowest median stage time over reps timed runs (one untimed run
+ * first), and leaves the winners set on the context.  It runs the batch in
+ * place, so pass frames whose contents may be overwritten (copies).
+ * out->ms_default is each group's time with the default schedule
+ * {0, 1, 0, 0}. */
 enum { PF_TUNE_DEBLOCK = 0, PF_TUNE_CDEF = 1, PF_TUNE_RESTORATION = 2, PF_TUNE_FILM_GRAIN = 3, PF_TUNE_GROUPS = 4 };
 
+typedef struct pf_schedule {
+  int32_t ctas;           /* persistent CTAs (0 = one CTA per chunk) */
+  int32_t units_per_cta;  /* work items per chunk, 1..16 */
+  int32_t staging;        /* items prefetched ahead, 0..3 and < units_per_cta */
+  int32_t tile;           /* deblocking tile shape 0..3; 0 for other groups */
+} pf_schedule;
+
 typedef struct pf_tune_result {
-  int32_t ctas[PF_TUNE_GROUPS];      /* chosen persistent CTA count (0 = one per item) */
-  float ms[PF_TUNE_GROUPS];          /* its median stage time */
-  float ms_default[PF_TUNE_GROUPS];  /* one CTA per item */
+  pf_schedule chosen[PF_TUNE_GROUPS];  /* the schedule left set per group */
+  float ms[PF_TUNE_GROUPS];            /* its median stage time */
+  float ms_default[PF_TUNE_GROUPS];    /* the default schedule's */
 } pf_tune_result;
 
 int pf_batch_graphs(pf_ctx* ctx, int32_t enable);
+/* Sets / reads one group's schedule (PF_ERR_INVALID_ARG outside the ranges
+ * above).  pf_set_persistent(ctx, g, n) sets only the ctas field. */
+int pf_set_schedule(pf_ctx* ctx, int32_t group, const pf_schedule* schedule);
+int pf_get_schedule(const pf_ctx* ctx, int32_t group, pf_schedule* schedule);
 int pf_set_persistent(pf_ctx* ctx, int32_t group, int32_t ctas);
 int pf_autotune(pf_ctx* ctx, const pf_batch_item* items, int32_t n, int32_t reps,
                 pf_tune_result* out);

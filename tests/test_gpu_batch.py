@@ -1,5 +1,6 @@
-"""Batch scheduling on the GPU: CUDA-graph capture and replay, persistent
-CTAs and the autotuner must not change a single sample.
+"""Batch scheduling on the GPU: CUDA-graph capture and replay, the stage
+schedules (persistent CTAs, work items per CTA, staging depth, deblocking
+tile shape) and the autotuner must not change a single sample.
 
 The batch is a reduced form of the mixed workload (640x360 and 1280x720
 8-bit 4:2:0, 1920x1080 10-bit 4:2:0, 1280x720 8-bit 4:4:4, each with its own
@@ -89,13 +90,45 @@ def test_persistent_ctas_match_oracle(frames, expected):
     r.close()
 
 
+# Every value of every schedule dimension (tile shape, work items per CTA,
+# staging depth), alone and with persistent CTAs, on every stage group.
+SCHEDULES = [dict(tile=t) for t in range(1, 4)] + \
+    [dict(units_per_cta=u) for u in (2, 3, 4, 8, 16)] + \
+    [dict(units_per_cta=u, staging=d) for u, d in ((2, 1), (4, 2), (4, 3), (16, 3))] + \
+    [dict(units_per_cta=4, staging=2, ctas=148), dict(units_per_cta=2, staging=1, ctas=7, tile=2)]
+
+
+@pytest.mark.parametrize("sched", SCHEDULES, ids=lambda d: "-".join("%s%d" % kv for kv in sorted(d.items())))
+def test_schedules_match_oracle(frames, expected, sched):
+    from goav1_b200.postfilter import PostFilterRunner
+
+    r = PostFilterRunner()
+    for g in range(abi.PF_TUNE_GROUPS):
+        kw = dict(sched)
+        if g != abi.PF_TUNE_DEBLOCK:
+            kw.pop("tile", None)
+        r.set_schedule(g, **kw)
+        got = r.get_schedule(g).as_dict()
+        assert all(got[k] == v for k, v in kw.items())
+    b = Batch(frames)
+    r.apply_batch(b.items)
+    r.sync()
+    assert_batch(b, expected, "schedule %r" % sched)
+    r.close()
+
+
 def test_autotune_then_graphs_match_oracle(frames, expected):
     from goav1_b200.postfilter import PostFilterRunner
 
     r = PostFilterRunner()
     scratch = Batch(frames)  # the tuner filters these in place
     res = r.autotune(scratch.items, reps=1)
-    assert all(c >= 0 for c in res.ctas) and all(m > 0 for m in res.ms)
+    for g in range(abi.PF_TUNE_GROUPS):
+        c = res.chosen[g]
+        assert c.ctas >= 0 and 1 <= c.units_per_cta <= 16 and 0 <= c.staging <= 3
+        assert c.tile == 0 or g == abi.PF_TUNE_DEBLOCK
+        assert r.get_schedule(g).as_dict() == c.as_dict()
+    assert all(m > 0 for m in res.ms)
     assert all(m <= d for m, d in zip(res.ms, res.ms_default))
     r.batch_graphs(True)
     b = Batch(frames)
@@ -117,6 +150,11 @@ def test_scheduling_arguments_are_checked():
         r.set_persistent(0, -1)
     with pytest.raises(ErrInvalidArgument):
         r.batch_graphs(2)
+    for g, kw in ((abi.PF_TUNE_CDEF, dict(tile=1)), (0, dict(tile=4)), (0, dict(units_per_cta=0)),
+                  (0, dict(units_per_cta=17)), (0, dict(staging=1)), (0, dict(units_per_cta=2, staging=2)),
+                  (0, dict(units_per_cta=8, staging=4)), (0, dict(ctas=-1)), (abi.PF_TUNE_GROUPS, {})):
+        with pytest.raises(ErrInvalidArgument):
+            r.set_schedule(g, **kw)
     r.close()
 
 
