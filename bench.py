@@ -839,6 +839,44 @@ def main():
                            "config": "one 1280x1080 -> 1920x1080 8-bit 4:2:0 frame, full chain (deblock, CDEF, "
                                      "boundary rows and frame upscaled, restoration, border extension, grain), "
                                      "device-resident, one call with its synchronisation, upscaled Mpix/s"}
+        # The same chain on 8 super-resolved frames through one
+        # pf_batch_apply_superres (stages batched over the frames), CUDA
+        # events on the library stream around the call, inputs reset outside.
+        nb_sr = 8
+        bf = []
+        for i in range(nb_sr):
+            cfi, csii = synth.make_frame(1, 40 + i, width=1280, height=1080)
+            ufi, usii = synth.make_frame(1, 80 + i, width=1920, height=1080)
+            si = abi.pf_frame_side()
+            _C.memmove(_C.byref(si), _C.byref(csii.side), _C.sizeof(si))
+            si.lr = usii.side.lr
+            dci = DeviceFrame(cfi)
+            bf.append((dci, [t.clone() for t in dci.tensors], DeviceFrame(ufi.like()), DeviceFrame(ufi.like()), si,
+                       (csii, usii)))
+        sr_items = [(dci.pf(), si, dui.pf(), ddi.pf()) for dci, _, dui, ddi, si, _ in bf]
+        sstream = torch.cuda.ExternalStream(runner.stream)
+
+        def sr_batch():
+            with torch.cuda.stream(sstream):
+                for dci, p0, _, _, _, _ in bf:
+                    for t, t0 in zip(dci.tensors, p0):
+                        t.copy_(t0)
+                flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(sstream)
+            runner.apply_batch_superres(sr_items)
+            e1.record(sstream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / 1e3
+
+        sr_batch()
+        t_b = statistics.median(sr_batch() for _ in range(max(5, args.steps // 2)))
+        sr_leg["chain_batched"] = {"metric": "super-resolved chain Mpix/s", "value": nb_sr * 1920 * 1080 / t_b / 1e6,
+                                   "unit": "Mpix/s", "ms_per_step": t_b * 1e3,
+                                   "config": "8 frames 1280x1080 -> 1920x1080 8-bit 4:2:0 (seeds 40-47 coded, "
+                                             "80-87 restoration grid), full chain, one pf_batch_apply_superres per "
+                                             "step, device-resident, CUDA events on the library stream, L2 flushed "
+                                             "between steps, upscaled Mpix/s"}
 
     # Deblocking masks and level cache from the block record map
     # (pf_lf_build): 8 random 1080p maps (480x270 MI cells, 128x128

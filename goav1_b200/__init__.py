@@ -68,6 +68,8 @@ def lib():
     L.pf_frame_apply_superres.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame_side),
                                           C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame), C.POINTER(abi.pf_stats)]
     L.pf_superres_upscale.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.POINTER(abi.pf_frame)]
+    L.pf_batch_apply_superres.argtypes = [C.c_void_p, C.POINTER(abi.pf_superres_item), C.c_int32,
+                                          C.POINTER(abi.pf_stats)]
     L.pf_lf_build.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_uint32,
                               C.POINTER(abi.pf_lf_levels), C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                               C.c_void_p, C.c_uint32]

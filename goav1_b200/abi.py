@@ -187,6 +187,15 @@ class pf_batch_item(C.Structure):
     ]
 
 
+class pf_superres_item(C.Structure):
+    _fields_ = [
+        ("coded", C.POINTER(pf_frame)),
+        ("side", C.POINTER(pf_frame_side)),
+        ("up", C.POINTER(pf_frame)),
+        ("display", C.POINTER(pf_frame)),
+    ]
+
+
 class pf_cdef_search_params(C.Structure):
     _fields_ = [
         ("qindex", C.c_int32),
@@ -435,6 +444,7 @@ EXPORTED_SYMBOLS = (
     "pf_cdef_apply",
     "pf_superres_upscale",
     "pf_frame_apply_superres",
+    "pf_batch_apply_superres",
     "pf_lf_build",
     "pf_diag_issue_rate",
     "pf_cdef_search_level_rtc",

@@ -1377,22 +1377,52 @@ static int run_host_pipeline(pf_ctx* c, const pf_batch_item* items, int n, pf_st
 // (tile/restoration_boundary.go:257-406), the CDEF output upscaled
 // (superres.UpscalePlaneCoded), then restoration, border extension and grain
 // on the upscaled frame.
-extern "C" int pf_frame_apply_superres(pf_ctx* c, const pf_frame* coded, const pf_frame_side* s,
-                                       const pf_frame* up, const pf_frame* display, pf_stats* stats) {
-  if (!c || !coded || !s || !up) return PF_ERR_INVALID_ARG;
+// A super-resolved frame's arguments checked, and its side information split
+// into the coded-grid stages (sa: deblocking, CDEF) and the upscaled-grid
+// ones (sb: restoration, extension, grain).
+static int superres_validate(const pf_frame* coded, const pf_frame_side* s, const pf_frame* up,
+                             const pf_frame* display, pf_frame_side* sa, pf_frame_side* sb) {
+  if (!coded || !s || !up) return PF_ERR_INVALID_ARG;
   if (s->stages & ~0x1Fu) return PF_ERR_UNSUPPORTED;
   if (coded->memory > PF_MEM_DEVICE || up->memory != coded->memory) return PF_ERR_INVALID_ARG;
   if (up->bit_depth != coded->bit_depth || up->ss_x != coded->ss_x || up->ss_y != coded->ss_y ||
       up->mono != coded->mono || up->height != coded->height || up->width <= coded->width || up->width > 16384)
     return PF_ERR_INVALID_FORMAT;
-  pf_frame_side sa = *s, sb = *s;
-  sa.stages = s->stages & (PF_STAGE_LOOP_FILTER | PF_STAGE_CDEF);
-  sb.stages = s->stages & (PF_STAGE_LOOP_RESTORATION | PF_STAGE_EXTEND_BORDERS | PF_STAGE_FILM_GRAIN);
-  const bool wantDisp = (sb.stages & PF_STAGE_FILM_GRAIN) && display;
+  *sa = *s;
+  *sb = *s;
+  sa->stages = s->stages & (PF_STAGE_LOOP_FILTER | PF_STAGE_CDEF);
+  sb->stages = s->stages & (PF_STAGE_LOOP_RESTORATION | PF_STAGE_EXTEND_BORDERS | PF_STAGE_FILM_GRAIN);
+  const bool wantDisp = (sb->stages & PF_STAGE_FILM_GRAIN) && display;
   if (wantDisp && display->memory != up->memory) return PF_ERR_INVALID_ARG;
-  int st = pf_frame_validate(coded, &sa, nullptr);
-  if (st == PF_OK) st = pf_frame_validate(up, &sb, display);
+  int st = pf_frame_validate(coded, sa, nullptr);
+  if (st == PF_OK) st = pf_frame_validate(up, sb, display);
+  return st;
+}
+
+// Rows of upscaled restoration boundary lines a super-resolved frame needs
+// per plane (0: none), and their pitch.
+static size_t superres_line_bytes(const pf_frame* up, const pf_frame_side* sb, int nb[3], int64_t lstride[3]) {
+  size_t total = 0;
+  const int bps = bps_of(up);
+  for (int p = 0; p < 3; p++) {
+    nb[p] = 0;
+    lstride[p] = 0;
+    if (!lr_any(sb) || p >= (up->mono ? 1 : 3) || sb->lr.type[p] == PF_LR_NONE) continue;
+    const int sy = p ? up->ss_y : 0;
+    nb[p] = (up->plane[p].height + (8 >> sy)) / (64 >> sy) + 2;
+    lstride[p] = (int64_t)align256((size_t)up->plane[p].width * bps);
+    total += align256((size_t)nb[p] * 4 * lstride[p]);
+  }
+  return total;
+}
+
+extern "C" int pf_frame_apply_superres(pf_ctx* c, const pf_frame* coded, const pf_frame_side* s,
+                                       const pf_frame* up, const pf_frame* display, pf_stats* stats) {
+  if (!c) return PF_ERR_INVALID_ARG;
+  pf_frame_side sa, sb;
+  int st = superres_validate(coded, s, up, display, &sa, &sb);
   if (st != PF_OK) return st;
+  const bool wantDisp = (sb.stages & PF_STAGE_FILM_GRAIN) && display;
   CK(cudaSetDevice(c->device));
   if (stats) memset(stats, 0, sizeof(*stats));
   const int bps = bps_of(coded);
@@ -1450,19 +1480,15 @@ extern "C" int pf_frame_apply_superres(pf_ctx* c, const pf_frame* coded, const p
   uint8_t* lines[3] = {};
   int64_t lstride[3] = {};
   if (lr_any(&sb)) {
-    int nb[3] = {};
-    size_t total = 0, off[3] = {};
-    for (int p = 0; p < nplanes; p++) {
-      if (sb.lr.type[p] == PF_LR_NONE) continue;
-      const int sy = p ? up->ss_y : 0;
-      nb[p] = (up->plane[p].height + (8 >> sy)) / (64 >> sy) + 2;
-      lstride[p] = (int64_t)align256((size_t)up->plane[p].width * bps);
-      off[p] = total;
-      total += align256((size_t)nb[p] * 4 * lstride[p]);
-    }
+    int nb[3];
+    const size_t total = superres_line_bytes(up, &sb, nb, lstride);
     CK(c->sr_lines.ensure(total + 256));
+    size_t off = 0;
     for (int p = 0; p < nplanes; p++)
-      if (nb[p]) lines[p] = (uint8_t*)c->sr_lines.p + off[p];
+      if (nb[p]) {
+        lines[p] = (uint8_t*)c->sr_lines.p + off;
+        off += align256((size_t)nb[p] * 4 * lstride[p]);
+      }
     CK(launch_superres_lines((const uint8_t* const*)cio, cst, lines, lstride, nb, coded, up->width, cs));
   }
   if ((sa.stages & PF_STAGE_CDEF) && cdef_any(coded, &sa)) {
@@ -1503,6 +1529,138 @@ extern "C" int pf_frame_apply_superres(pf_ctx* c, const pf_frame* coded, const p
     stats->completed |= done;
     read_stage_times(c, stats);
   }
+  CK(cudaGetLastError());
+  return PF_OK;
+}
+
+// A batch of super-resolved frames: each stage of the chain runs as one
+// launch over every frame that has it (deblocking over the coded frames,
+// then CDEF, then restoration / extension / grain over the upscaled ones);
+// the boundary-line upscale and the frame upscale are launched per frame
+// between them, in the decoder's order.  Device frames: returns once the
+// work is queued; host frames: one pf_frame_apply_superres per item.
+extern "C" int pf_batch_apply_superres(pf_ctx* c, const pf_superres_item* items, int32_t n, pf_stats* stats) {
+  if (!c || !items || n <= 0) return PF_ERR_INVALID_ARG;
+  std::vector<pf_frame_side> sa((size_t)n), sb((size_t)n);
+  for (int i = 0; i < n; i++) {
+    if (!items[i].coded || items[i].coded->memory != items[0].coded->memory) return PF_ERR_INVALID_ARG;
+    const int st = superres_validate(items[i].coded, items[i].side, items[i].up, items[i].display, &sa[i], &sb[i]);
+    if (st != PF_OK) return st;
+  }
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (items[0].coded->memory == PF_MEM_HOST) {
+    for (int i = 0; i < n; i++) {
+      pf_stats one;
+      const int st = pf_frame_apply_superres(c, items[i].coded, items[i].side, items[i].up, items[i].display,
+                                             stats ? &one : nullptr);
+      if (st != PF_OK) return st;
+      if (stats) {
+        stats->completed |= one.completed;
+        stats->cdef_units += one.cdef_units;
+        stats->lr_units += one.lr_units;
+        stats->fg_rows += one.fg_rows;
+      }
+    }
+    return PF_OK;
+  }
+  CK(cudaSetDevice(c->device));
+  const cudaStream_t cs = c->stream;
+  auto ref_of = [](const pf_frame* f, const pf_frame_side* side) {
+    FrameRef x;
+    memset(&x, 0, sizeof(x));
+    x.f = f;
+    x.s = side;
+    for (int p = 0; p < 3; p++) {
+      x.io[p] = f->plane[p].data;
+      x.ioStride[p] = f->plane[p].stride;
+    }
+    return x;
+  };
+  pf_stats acc;
+  memset(&acc, 0, sizeof(acc));
+  auto run = [&](std::vector<FrameRef>& refs) {
+    if (refs.empty()) return (int)PF_OK;
+    pf_stats one;
+    const int st = run_batch(c, refs.data(), (int)refs.size(), &one);
+    acc.completed |= one.completed;
+    acc.cdef_units += one.cdef_units;
+    acc.lr_units += one.lr_units;
+    acc.fg_rows += one.fg_rows;
+    return st;
+  };
+  std::vector<pf_frame_side> s1((size_t)n), s2((size_t)n);
+  std::vector<FrameRef> refs;
+  refs.reserve((size_t)n);
+  // Deblocking, every coded frame in one launch per pass.
+  for (int i = 0; i < n; i++)
+    if (sa[i].stages & PF_STAGE_LOOP_FILTER) {
+      s1[i] = sa[i];
+      s1[i].stages = PF_STAGE_LOOP_FILTER;
+      refs.push_back(ref_of(items[i].coded, &s1[i]));
+    }
+  int st = run(refs);
+  if (st != PF_OK) return st;
+  // The deblocked rows around each frame's stripe boundaries, upscaled, into
+  // one buffer for the whole batch.
+  std::vector<int> nb((size_t)n * 3);
+  std::vector<int64_t> lstride((size_t)n * 3);
+  std::vector<size_t> loff((size_t)n);
+  size_t ltotal = 0;
+  for (int i = 0; i < n; i++) {
+    loff[i] = ltotal;
+    ltotal += superres_line_bytes(items[i].up, &sb[i], &nb[3 * i], &lstride[3 * i]);
+  }
+  if (ltotal) CK(c->sr_lines.ensure(ltotal + 256));
+  std::vector<uint8_t*> lines((size_t)n * 3, nullptr);
+  for (int i = 0; i < n; i++) {
+    if (!lr_any(&sb[i])) continue;
+    size_t off = loff[i];
+    for (int p = 0; p < 3; p++)
+      if (nb[3 * i + p]) {
+        lines[3 * i + p] = (uint8_t*)c->sr_lines.p + off;
+        off += align256((size_t)nb[3 * i + p] * 4 * lstride[3 * i + p]);
+      }
+    const pf_frame* cf = items[i].coded;
+    void* cio[3] = {cf->plane[0].data, cf->plane[1].data, cf->plane[2].data};
+    const int64_t cst[3] = {cf->plane[0].stride, cf->plane[1].stride, cf->plane[2].stride};
+    CK(launch_superres_lines((const uint8_t* const*)cio, cst, &lines[3 * i], &lstride[3 * i], &nb[3 * i], cf,
+                             items[i].up->width, cs));
+  }
+  // CDEF over the coded frames.
+  refs.clear();
+  for (int i = 0; i < n; i++)
+    if ((sa[i].stages & PF_STAGE_CDEF) && cdef_any(items[i].coded, &sa[i])) {
+      s2[i] = sa[i];
+      s2[i].stages = PF_STAGE_CDEF;
+      refs.push_back(ref_of(items[i].coded, &s2[i]));
+    }
+  if ((st = run(refs)) != PF_OK) return st;
+  // Upscale, then the upscaled-grid stages over every frame.
+  refs.clear();
+  for (int i = 0; i < n; i++) {
+    const pf_frame* cf = items[i].coded;
+    const pf_frame* uf = items[i].up;
+    void* cio[3] = {cf->plane[0].data, cf->plane[1].data, cf->plane[2].data};
+    const int64_t cst[3] = {cf->plane[0].stride, cf->plane[1].stride, cf->plane[2].stride};
+    void* uio[3] = {uf->plane[0].data, uf->plane[1].data, uf->plane[2].data};
+    const int64_t ust[3] = {uf->plane[0].stride, uf->plane[1].stride, uf->plane[2].stride};
+    CK(launch_superres_frame((const uint8_t* const*)cio, cst, (uint8_t* const*)uio, ust, cf, uf->width, cs));
+    if (!sb[i].stages) continue;
+    FrameRef x = ref_of(uf, &sb[i]);
+    const bool wantDisp = (sb[i].stages & PF_STAGE_FILM_GRAIN) && items[i].display;
+    x.display = wantDisp ? items[i].display : nullptr;
+    for (int p = 0; p < 3; p++) {
+      if (wantDisp) {
+        x.dp[p] = items[i].display->plane[p].data;
+        x.dStride[p] = items[i].display->plane[p].stride;
+      }
+      x.ext_lines[p] = lines[3 * i + p];
+      x.ext_line_stride[p] = lstride[3 * i + p];
+    }
+    refs.push_back(x);
+  }
+  if ((st = run(refs)) != PF_OK) return st;
+  if (stats) *stats = acc;
   CK(cudaGetLastError());
   return PF_OK;
 }

@@ -308,10 +308,11 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
 }
 
 // Batched CDEF: each work item is one 64x64 unit of one frame.
+template <bool kLoop>
 __global__ void __launch_bounds__(256, 4) k_cdef_batch(BatchArgs b) {
   __shared__ CdefSmem sm;
   const int* base = b.base + ST_CDEF * (b.n + 1);
-  for_each_item(
+  for_each_item<kLoop>(
       b, ST_CDEF, base[b.n],
       [&](int item) {
         const int fi = find_frame(base, b.n, item);
@@ -342,7 +343,10 @@ __global__ void __launch_bounds__(256, 4) k_cdef_batch(BatchArgs b) {
 
 cudaError_t launch_cdef_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
-  k_cdef_batch<<<grid, 256, 0, st>>>(b);
+  if (batch_loops(b))
+    k_cdef_batch<true><<<grid, 256, 0, st>>>(b);
+  else
+    k_cdef_batch<false><<<grid, 256, 0, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -230,53 +230,71 @@ __device__ __forceinline__ int find_frame(const int* base, int n, int item) {
   return lo;
 }
 
-// Runs f(item) over the items [first, last) of one chunk, prefetch(item)
-// for the items `ahead` places further on inside the chunk, a barrier
-// between items.
-template <typename F, typename P>
-__device__ __forceinline__ void run_chunk(int first, int last, int ahead, F& f, P& prefetch) {
-  for (int it = first; it < last; it++) {
-    if (it != first) __syncthreads();
-    if (ahead > 0) {
-      if (it == first)
-        for (int k = 1; k <= ahead && first + k < last; k++) prefetch(first + k);
-      else if (it + ahead < last)
-        prefetch(it + ahead);
-    }
-    f(it);
-  }
-}
-
 // Runs f(item) for the CTA's work items: a chunk of b.chunk consecutive
 // items per CTA (grid = ceil(total / chunk)), or a persistent CTA draining
 // the stage's queue a chunk at a time through an atomic counter.  Inside a
 // chunk, prefetch(item) warms L2 with the input of the item b.ahead places
 // on.  Every item is independent of the others, so no schedule changes a
-// result.
-template <typename F, typename P>
+// result.  The loop's position lives in shared memory, so that nothing but
+// f's own state is held in registers across f.
+// kLoop = false compiles only the one-item-per-CTA schedule (the launcher's
+// choice when the stage has no chunks and no persistent CTAs), which keeps
+// the loop's bookkeeping out of the kernel's register allocation.
+template <bool kLoop = true, typename F, typename P>
 __device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, int total, F f, P prefetch) {
   const int chunk = b.chunk > 1 ? b.chunk : 1;
   int* counter = b.counters ? b.counters + stage : nullptr;
-  if (counter == nullptr) {
-    const int first = (int)blockIdx.x * chunk;
-    run_chunk(first, first + chunk < total ? first + chunk : total, b.ahead, f, prefetch);
+  if (!kLoop || (counter == nullptr && chunk == 1)) {
+    if ((int)blockIdx.x < total) f((int)blockIdx.x);
     return;
   }
-  __shared__ int s_item;
+  // Next item, end of the chunk, first item of the chunk, total, chunk.
+  __shared__ int s_pos[5];
+  if (threadIdx.x == 0) {
+    const int first = counter ? atomicAdd(counter, chunk) : (int)blockIdx.x * chunk;
+    s_pos[0] = s_pos[2] = first;
+    s_pos[1] = first + chunk < total ? first + chunk : total;
+    s_pos[3] = total;
+    s_pos[4] = chunk;
+  }
+  __syncthreads();
   for (;;) {
+    int it = s_pos[0];
+    if (it >= s_pos[1]) {
+      // Chunk done: the next one (persistent CTAs) or the end.
+      if (b.counters == nullptr) break;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const int n = s_pos[3], c = s_pos[4];
+        const int first = atomicAdd(b.counters + stage, c);
+        s_pos[0] = s_pos[2] = first;
+        s_pos[1] = first + c < n ? first + c : n;
+      }
+      __syncthreads();
+      it = s_pos[0];
+      if (it >= s_pos[3]) break;
+    }
+    if (b.ahead > 0) {
+      const int last = s_pos[1];
+      if (it == s_pos[2])
+        for (int k = 1; k <= b.ahead && it + k < last; k++) prefetch(it + k);
+      else if (it + b.ahead < last)
+        prefetch(it + b.ahead);
+    }
+    f(it);
     __syncthreads();
-    if (threadIdx.x == 0) s_item = atomicAdd(counter, chunk);
+    if (threadIdx.x == 0) s_pos[0] = s_pos[0] + 1;
     __syncthreads();
-    const int first = s_item;
-    if (first >= total) break;
-    run_chunk(first, first + chunk < total ? first + chunk : total, b.ahead, f, prefetch);
   }
 }
 
-template <typename F>
+template <bool kLoop = true, typename F>
 __device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, int total, F f) {
   auto none = [](int) {};
-  for_each_item(b, stage, total, f, none);
+  for_each_item<kLoop>(b, stage, total, f, none);
 }
+
+// Whether a launch needs the looping form of for_each_item.
+inline bool batch_loops(const BatchArgs& b) { return b.counters != nullptr || b.chunk > 1; }
 
 }  // namespace pf

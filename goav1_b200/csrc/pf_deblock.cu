@@ -280,10 +280,11 @@ __device__ __forceinline__ DbTile db_locate(const BatchArgs& b, const int* base,
   return DbTile{&J, plane, local % J.db_tx[plane], local / J.db_tx[plane]};
 }
 
+template <bool kLoop>
 __global__ void __launch_bounds__(256, 4) k_deblock_batch(BatchArgs b, int dir) {
   const int stage = dir == 0 ? ST_DEBLOCK_V : ST_DEBLOCK_H;
   const int* base = b.base + stage * (b.n + 1);
-  for_each_item(
+  for_each_item<kLoop>(
       b, stage, base[b.n],
       [&](int item) {
         const DbTile t = db_locate(b, base, item);
@@ -309,7 +310,10 @@ __global__ void __launch_bounds__(256, 4) k_deblock_batch(BatchArgs b, int dir) 
 
 cudaError_t launch_deblock_batch(const BatchArgs& b, int total, int grid, int dir, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
-  k_deblock_batch<<<grid, 256, 0, st>>>(b, dir);
+  if (batch_loops(b))
+    k_deblock_batch<true><<<grid, 256, 0, st>>>(b, dir);
+  else
+    k_deblock_batch<false><<<grid, 256, 0, st>>>(b, dir);
   return cudaGetLastError();
 }
 

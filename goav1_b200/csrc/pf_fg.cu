@@ -376,10 +376,11 @@ __device__ __forceinline__ FgTile fg_locate(const BatchArgs& b, const int* base,
   return FgTile{&J, plane, local % J.fg_tx[plane], local / J.fg_tx[plane]};
 }
 
+template <bool kLoop>
 __global__ void __launch_bounds__(256, 6) k_fg_apply_batch(BatchArgs b) {
   __shared__ uint8_t s_lut[256];
   const int* base = b.base + ST_FG_APPLY * (b.n + 1);
-  for_each_item(
+  for_each_item<kLoop>(
       b, ST_FG_APPLY, base[b.n],
       [&](int item) {
         const FgTile t = fg_locate(b, base, item);
@@ -482,7 +483,10 @@ cudaError_t launch_fg_offsets_batch(const BatchArgs& b, int total, int grid, cud
 
 cudaError_t launch_fg_apply_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
-  k_fg_apply_batch<<<grid, 256, 0, st>>>(b);
+  if (batch_loops(b))
+    k_fg_apply_batch<true><<<grid, 256, 0, st>>>(b);
+  else
+    k_fg_apply_batch<false><<<grid, 256, 0, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -28,12 +28,21 @@ __constant__ uint16_t c_x_by_xplus1[256];
 __constant__ uint16_t c_one_by_x[25];
 
 constexpr int kWin = 70;  // 64 + 2*3
+constexpr int kLrMaxRun = 16;  // rows of one thread's output run (see lr_wiener_window)
 
 struct LrSmem {
   uint16_t win[kWin * kWin];
-  int32_t flt0[64 * 64];     // SGR radius-2 filter output between the passes (Wiener: row-pass temp)
-  uint16_t A[66 * 66];       // SGR a (<= 256)
-  int32_t B[66 * 66];
+  union {
+    // SGR a (<= 256) / b tables: radius 1 for rows -1..h, radius 2 for the
+    // rows -1, 1, 3, ... it is computed on; columns -1..w.
+    struct {
+      uint16_t A1[66 * 66];
+      int32_t B1[66 * 66];
+      uint16_t A2[33 * 66];
+      int32_t B2[33 * 66];
+    } sgr;
+    uint16_t wtemp[kWin * 64];  // Wiener row-pass output, (h+6) x 64
+  };
   uint16_t x_by_xplus1[256];  // data-dependent lookup: smem, not constant memory
 };
 
@@ -68,27 +77,42 @@ __device__ __forceinline__ void lr_wiener_window(LrSmem& sm, int w, int h, int b
   }
   const int32_t limit = 1 << (bd + 1 + 7 - round0);
   const int32_t offH = 1 << (bd + 7 - 1);
-  uint16_t* temp = reinterpret_cast<uint16_t*>(sm.flt0);  // (h+6) x 64
+  uint16_t* temp = sm.wtemp;  // (h+6) x 64
+  // Row pass: a lane takes the column pair (2 lane, 2 lane + 1) of a row,
+  // its eight window samples read as four aligned 32-bit words (kWin and
+  // the column are even); the taps are symmetric (hf[k] == hf[6 - k]), so
+  // the mirrored samples are summed first.
+  const int hc = hf[3] + 128;
   for (int r = warp; r < wh; r += 8) {
-    for (int c = lane; c < w; c += 32) {
-      const uint16_t* sw = &s_win[r * kWin + c];
-      // Symmetric taps (hf[k] == hf[6 - k]): pair sums first.
-      int32_t sum = ((int32_t)sw[3] << 7) + offH + (int32_t)sw[3] * hf[3];
-#pragma unroll
-      for (int k = 0; k < 3; k++) sum += ((int32_t)sw[k] + (int32_t)sw[6 - k]) * hf[k];
-      temp[r * 64 + c] = (uint16_t)imin(imax(rpot(sum, round0), 0), limit - 1);
+    const int c = 2 * lane;
+    if (c < w) {
+      const uint32_t* sw = reinterpret_cast<const uint32_t*>(&s_win[r * kWin + c]);
+      const uint32_t p01 = sw[0], p23 = sw[1], p45 = sw[2], p67 = sw[3];
+      const int32_t v0 = p01 & 0xffff, v1 = p01 >> 16, v2 = p23 & 0xffff, v3 = p23 >> 16;
+      const int32_t v4 = p45 & 0xffff, v5 = p45 >> 16, v6 = p67 & 0xffff, v7 = p67 >> 16;
+      const int32_t s0 = offH + v3 * hc + (v0 + v6) * hf[0] + (v1 + v5) * hf[1] + (v2 + v4) * hf[2];
+      const int32_t s1 = offH + v4 * hc + (v1 + v7) * hf[0] + (v2 + v6) * hf[1] + (v3 + v5) * hf[2];
+      const uint32_t o0 = (uint32_t)imin(imax(rpot(s0, round0), 0), limit - 1);
+      const uint32_t o1 = (uint32_t)imin(imax(rpot(s1, round0), 0), limit - 1);
+      *reinterpret_cast<uint32_t*>(&temp[r * 64 + c]) = o0 | (o1 << 16);
     }
   }
   __syncthreads();
   const int32_t offV = 1 << (bd + round1 - 1);
   // Each thread a run of consecutive output rows of column tx: the seven
-  // vertical taps slide down in registers, one new row read per output.
+  // vertical taps slide down in registers, one new row read per output.  A
+  // run is at most kLrMaxRun rows (h <= 64 over 4 runs per column at PW 64,
+  // over 8 at PW 32), and the loop is unrolled to that bound so that the
+  // slide is register renaming.
   const int ya = ty0 * rpg, yb = imin(h, ya + rpg);
   if (tx < w && ya < yb) {
     int32_t t[7];
 #pragma unroll
     for (int k = 0; k < 6; k++) t[k] = temp[(ya + k) * 64 + tx];
-    for (int y = ya; y < yb; y++) {
+#pragma unroll
+    for (int i = 0; i < kLrMaxRun; i++) {
+      const int y = ya + i;
+      if (y >= yb) break;
       t[6] = temp[(y + 6) * 64 + tx];
       int32_t sum = (t[3] << 7) - offV + t[3] * vf[3];
 #pragma unroll
@@ -100,164 +124,192 @@ __device__ __forceinline__ void lr_wiener_window(LrSmem& sm, int w, int h, int b
   }
 }
 
+// a and b of one SGR box (restoration/selfguided.go:132-231): the box's sum
+// and sum of squares, area N (9 or 25), strength sv.
+template <int N>
+__device__ __forceinline__ void sgr_ab(uint32_t bs, uint32_t bq, int bd, int sv, const uint16_t* xbx, uint16_t* A,
+                                       int32_t* B) {
+  const int32_t sum = (int32_t)bs, sq = (int32_t)bq;
+  const uint32_t av = (uint32_t)rpot(sq, 2 * (bd - 8));
+  const uint32_t bv = (uint32_t)rpot(sum, bd - 8);
+  uint32_t p = 0;
+  if (av * N >= bv * bv) p = av * N - bv * bv;
+  uint32_t z = rpotu(p * (uint32_t)sv, 20);
+  if (z > 255) z = 255;
+  const int32_t a = xbx[z];
+  *A = (uint16_t)a;
+  *B = (int32_t)rpotu((uint32_t)(256 - a) * (uint32_t)sum * (uint32_t)c_one_by_x[N - 1], 12);
+}
+
 // Self-guided filter of the staged window (restoration/selfguided.go:111-390)
-// with parameter set `set` and the coded xqd pair; same window, thread
-// mapping and out() contract as lr_wiener_window.  sm.x_by_xplus1 must hold
-// the table.  Ends with a barrier.
-template <class Out>
-__device__ __forceinline__ void lr_sgr_window(LrSmem& sm, int w, int h, int bd, int set, int xqd0, int xqd1, int PW, Out&& out) {
+// for a parameter set whose radius-2 (R2) and radius-1 (R1) filters are on
+// or off, with the decoded projection weights xq0 / xq1; same window,
+// thread mapping and out() contract as lr_wiener_window.  sm.x_by_xplus1
+// must hold the table.  Ends with a barrier.
+//
+// Box sums: one sweep down the window for both radii.  A warp takes a chunk
+// of 32 - 2*halo box columns and a segment of box rows; each lane slides the
+// 3-row and 5-row column sums of its window column down the segment (two
+// window loads a row: the rows entering the 5-row sum and leaving the 3-row
+// one; the other two moves reuse the previous row's), and the row sums come
+// from the neighbouring lanes by shuffles.  Radius 1 has a box on every row,
+// radius 2 on the rows -1, 1, 3, ....  Filters: one pass, each thread a run
+// of rows of one column, the a/b neighbourhoods of both radii sliding down
+// in registers, projected straight to out().
+template <bool R2, bool R1, class Out>
+__device__ __forceinline__ void lr_sgr_window_t(LrSmem& sm, int w, int h, int bd, int s2, int s1, int xq0, int xq1,
+                                                int PW, Out&& out) {
   const uint16_t* s_win = sm.win;
-  uint16_t* s_A = sm.A;
-  int32_t* s_B = sm.B;
+  uint16_t* A1 = sm.sgr.A1;
+  int32_t* B1 = sm.sgr.B1;
+  uint16_t* A2 = sm.sgr.A2;
+  int32_t* B2 = sm.sgr.B2;
+  const uint16_t* xbx = sm.x_by_xplus1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tid = threadIdx.x, tx = tid % PW, ty0 = tid / PW, rpg = (h + 256 / PW - 1) / (256 / PW);
-  // Output rows of this thread: a run [ya, yb) of column tx.
   const int ya = ty0 * rpg, yb = imin(h, ya + rpg);
   const int ww = w + 6;
   const int maxv = (1 << bd) - 1;
-  const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][1];
-  // restoration/selfguided.go:111-127 (DecodeSGRXQ).
-  int xq0, xq1;
-  if (r0 == 0) {
-    xq0 = 0;
-    xq1 = 128 - xqd1;
-  } else if (r1 == 0) {
-    xq0 = xqd0;
-    xq1 = 0;
-  } else {
-    xq0 = xqd0;
-    xq1 = 128 - xq0 - xqd1;
-  }
-  int32_t* flt0 = sm.flt0;  // [y * 64 + x]
-  if (r0 == 0)
-    for (int y = warp; y < h; y += 8)
-      for (int x = lane; x < w; x += 32) flt0[y * 64 + x] = 0;
+  constexpr int kHalo = R2 ? 2 : 1;
+  constexpr int kOutPer = 32 - 2 * kHalo;
+  constexpr unsigned kAll = 0xffffffffu;
   const int nrows = h + 2, ncols = w + 2;
-  for (int pass = 0; pass < 2; pass++) {
-    const int r = pass == 0 ? r0 : r1;
-    if (r == 0) continue;
-    const int sv = c_sgr_params[set][2 + pass];
-    const uint32_t n = (uint32_t)((2 * r + 1) * (2 * r + 1));
-    const int step = pass == 0 ? 2 : 1;  // the r = 2 pass computes rows -1, 1, 3, ...
-    // a/b for rows -1..h and cols -1..w at [(row+1)*66 + col+1].  Box sums:
-    // each lane slides a (2r+1)-row column sum down its window column; the
-    // (2r+1)-wide row sum comes from the neighbouring lanes by shuffles, so
-    // a warp yields 32-2r output columns per row.
-    const int outPer = 32 - 2 * r;
-    const int nch = (ncols + outPer - 1) / outPer;
-    const int nseg = (nrows + 15) / 16;
-    for (int item = warp; item < nch * nseg; item += 8) {
-      const int q = item % nch, seg = item / nch;
-      const int cc = q * outPer + lane - r;   // output column of this lane
-      const int wc = cc + 2;                  // its window column (centre)
-      const bool colIn = wc >= 0 && wc < ww;
-      const int rs = seg * 16, re = imin(rs + 16, nrows);
-      int rr = rs + (step == 2 ? (rs & 1) : 0);
-      uint32_t vs = 0, vq = 0;
-      if (colIn && rr < re)
-        for (int dy = -r; dy <= r; dy++) {
-          const uint32_t v = s_win[(rr + 2 + dy) * kWin + wc];
-          vs += v;
-          vq += v * v;
+  const int nch = (ncols + kOutPer - 1) / kOutPer;
+  const int segLen = (nrows + 7) >> 3;  // 8 row segments per column chunk
+  for (int item = warp; item < nch * 8; item += 8) {
+    const int seg = item / nch, q = item - seg * nch;
+    const int cc = q * kOutPer + lane - kHalo;  // box column + 1 of this lane
+    const int wc = cc + 2;                      // its window column
+    const bool colIn = wc >= 0 && wc < ww;
+    const bool store = lane >= kHalo && lane < 32 - kHalo && cc < ncols;
+    const int rs = seg * segLen, re = imin(rs + segLen, nrows);
+    if (rs >= re) continue;
+    auto ld = [&](int r) -> uint32_t { return colIn ? (uint32_t)s_win[r * kWin + wc] : 0u; };
+    // Box row rr (= row + 1) covers window rows rr+1 .. rr+3 (radius 1) and
+    // rr .. rr+4 (radius 2).
+    const uint32_t v0 = ld(rs), v1 = ld(rs + 1), v2 = ld(rs + 2), v3 = ld(rs + 3), v4 = ld(rs + 4);
+    uint32_t c3s = v1 + v2 + v3, c3q = v1 * v1 + v2 * v2 + v3 * v3;
+    uint32_t c5s = c3s + v0 + v4, c5q = c3q + v0 * v0 + v4 * v4;
+    uint32_t enter3 = v4, leave5 = v0;  // window rows rr+4 (enters the 3-row sum) and rr (leaves the 5-row one)
+    for (int rr = rs; rr < re; rr++) {
+      if (R1) {
+        const uint32_t bs = c3s + __shfl_up_sync(kAll, c3s, 1) + __shfl_down_sync(kAll, c3s, 1);
+        const uint32_t bq = c3q + __shfl_up_sync(kAll, c3q, 1) + __shfl_down_sync(kAll, c3q, 1);
+        if (store) sgr_ab<9>(bs, bq, bd, s1, xbx, &A1[rr * 66 + cc], &B1[rr * 66 + cc]);
+      }
+      if (R2 && (rr & 1) == 0) {
+        const uint32_t bs = c5s + __shfl_up_sync(kAll, c5s, 1) + __shfl_down_sync(kAll, c5s, 1) +
+                            __shfl_up_sync(kAll, c5s, 2) + __shfl_down_sync(kAll, c5s, 2);
+        const uint32_t bq = c5q + __shfl_up_sync(kAll, c5q, 1) + __shfl_down_sync(kAll, c5q, 1) +
+                            __shfl_up_sync(kAll, c5q, 2) + __shfl_down_sync(kAll, c5q, 2);
+        if (store) sgr_ab<25>(bs, bq, bd, s2, xbx, &A2[(rr >> 1) * 66 + cc], &B2[(rr >> 1) * 66 + cc]);
+      }
+      if (rr + 1 < re) {
+        const uint32_t l3 = ld(rr + 1);
+        if (R1) {
+          c3s += enter3 - l3;
+          c3q += enter3 * enter3 - l3 * l3;
         }
-      for (; rr < re; rr += step) {
-        // Row sums of the column sums: lanes r .. 31 - r (the ones stored)
-        // read exactly lanes lane - r .. lane + r.
-        uint32_t bs = vs, bq = vq;
-        for (int dx = 1; dx <= r; dx++) {
-          bs += __shfl_up_sync(0xffffffffu, vs, dx) + __shfl_down_sync(0xffffffffu, vs, dx);
-          bq += __shfl_up_sync(0xffffffffu, vq, dx) + __shfl_down_sync(0xffffffffu, vq, dx);
+        if (R2) {
+          const uint32_t e5 = ld(rr + 5);
+          c5s += e5 - leave5;
+          c5q += e5 * e5 - leave5 * leave5;
+          enter3 = e5;
+        } else {
+          enter3 = ld(rr + 4 + 1);
         }
-        if (lane >= r && lane < 32 - r && cc < ncols) {
-          const int32_t sum = (int32_t)bs, sq = (int32_t)bq;
-          const uint32_t av = (uint32_t)rpot(sq, 2 * (bd - 8));
-          const uint32_t bv = (uint32_t)rpot(sum, bd - 8);
-          uint32_t p = 0;
-          if (av * n >= bv * bv) p = av * n - bv * bv;
-          uint32_t z = rpotu(p * (uint32_t)sv, 20);
-          if (z > 255) z = 255;
-          const int32_t A = sm.x_by_xplus1[z];
-          s_A[rr * 66 + cc] = (uint16_t)A;
-          s_B[rr * 66 + cc] = (int32_t)rpotu((uint32_t)(256 - A) * (uint32_t)sum * (uint32_t)c_one_by_x[n - 1], 12);
-        }
-        // Slide the column sums down to the next computed row.
-        if (colIn && rr + step < re) {
-          for (int k = 0; k < step; k++) {
-            const uint32_t vin = s_win[(rr + 2 + r + 1 + k) * kWin + wc];
-            const uint32_t vout = s_win[(rr + 2 - r + k) * kWin + wc];
-            vs += vin - vout;
-            vq += vin * vin - vout * vout;
-          }
-        }
+        leave5 = l3;
       }
     }
-    __syncthreads();
-    // The a/b neighbourhoods slide down the thread's rows: row k of the
-    // tables is s_A/s_B[k * 66 + tx .. tx + 2] (output row y sits at k = y + 1).
-    if (tx < w && ya < yb) {
-      auto rowA = [&](int k, int32_t (&v)[3]) {
-        v[0] = s_A[k * 66 + tx], v[1] = s_A[k * 66 + tx + 1], v[2] = s_A[k * 66 + tx + 2];
-      };
-      auto rowB = [&](int k, int32_t (&v)[3]) {
-        v[0] = s_B[k * 66 + tx], v[1] = s_B[k * 66 + tx + 1], v[2] = s_B[k * 66 + tx + 2];
-      };
-      if (pass == 0) {
-        // Radius 2: a/b exist on even table rows only.  Even y takes rows y
-        // and y + 2 (weights 6 centre / 5 corners, shift 9), odd y row y + 1
-        // (6 / 5, shift 8).
-        const int e = ya & ~1;
-        int32_t uA[3], uB[3], dA[3], dB[3];
-        rowA(e, uA), rowB(e, uB), rowA(e + 2, dA), rowB(e + 2, dB);
-        for (int y = ya; y < yb; y++) {
-          const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
-          int32_t av, bv, shift;
-          if ((y & 1) == 0) {
-            if (y != e) {
-#pragma unroll
-              for (int k = 0; k < 3; k++) uA[k] = dA[k], uB[k] = dB[k];
-              rowA(y + 2, dA), rowB(y + 2, dB);
-            }
-            av = (uA[1] + dA[1]) * 6 + (uA[0] + uA[2] + dA[0] + dA[2]) * 5;
-            bv = (uB[1] + dB[1]) * 6 + (uB[0] + uB[2] + dB[0] + dB[2]) * 5;
-            shift = 9;
-          } else {
-            av = dA[1] * 6 + (dA[0] + dA[2]) * 5;
-            bv = dB[1] * 6 + (dB[0] + dB[2]) * 5;
-            shift = 8;
-          }
-          flt0[y * 64 + tx] = rpot(av * dg + bv, shift);
-        }
-      } else {
-        // Radius 1: rows y, y + 1, y + 2 (weights 4 cross / 3 corners).
-        int32_t uA[3], uB[3], mA[3], mB[3], dA[3], dB[3];
-        rowA(ya, uA), rowB(ya, uB), rowA(ya + 1, mA), rowB(ya + 1, mB);
-        for (int y = ya; y < yb; y++) {
-          rowA(y + 2, dA), rowB(y + 2, dB);
-          const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
-          // restoration/selfguided.go:233-247: projection with the int16 wrap.
-          const int32_t av = (mA[0] + mA[1] + mA[2] + uA[1] + dA[1]) * 4 + (uA[0] + uA[2] + dA[0] + dA[2]) * 3;
-          const int32_t bv = (mB[0] + mB[1] + mB[2] + uB[1] + dB[1]) * 4 + (uB[0] + uB[2] + dB[0] + dB[2]) * 3;
-          const int32_t f1 = rpot(av * dg + bv, 9);
-          const int32_t uu = dg << 4;
-          const int32_t v = (uu << 7) + xq0 * (flt0[y * 64 + tx] - uu) + xq1 * (f1 - uu);
-          const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
-          out(y, tx, imin(imax(wv, 0), maxv));
-#pragma unroll
-          for (int k = 0; k < 3; k++) uA[k] = mA[k], uB[k] = mB[k], mA[k] = dA[k], mB[k] = dB[k];
-        }
-      }
-    }
-    __syncthreads();
   }
-  if (r1 == 0 && tx < w) {
-    // Only the radius-2 filter: project with xq1 = 0.
-    for (int y = ya; y < yb; y++) {
-      const int32_t uu = (int32_t)s_win[(y + 3) * kWin + tx + 3] << 4;
-      const int32_t v = (uu << 7) + xq0 * (flt0[y * 64 + tx] - uu);
+  __syncthreads();
+  if (tx < w && ya < yb) {
+    // Radius 2: even y weighs table rows y and y + 2 (6 centre / 5 corners,
+    // shift 9), odd y row y + 1 (6 / 5, shift 8); the tables hold the even
+    // rows k at k / 2.  Radius 1: rows y, y + 1, y + 2 (4 cross / 3
+    // corners).  A table row enters as its 3-sum S and centre C over columns
+    // tx .. tx + 2: 6 C + 5 (S - C) = 5 S + C, and the radius-1 weights sum
+    // to 4 S(y+1) + 3 (S(y) + S(y+2)) + C(y) + C(y+2).
+    struct SC {
+      int32_t sa, ca, sb, cb;
+    };
+    auto row2 = [&](int i) {
+      const int o = i * 66 + tx;
+      const int32_t a0 = A2[o], a1 = A2[o + 1], a2 = A2[o + 2];
+      const int32_t b0 = B2[o], b1 = B2[o + 1], b2 = B2[o + 2];
+      return SC{a0 + a1 + a2, a1, b0 + b1 + b2, b1};
+    };
+    auto row1 = [&](int k) {
+      const int o = k * 66 + tx;
+      const int32_t a0 = A1[o], a1 = A1[o + 1], a2 = A1[o + 2];
+      const int32_t b0 = B1[o], b1 = B1[o + 1], b2 = B1[o + 2];
+      return SC{a0 + a1 + a2, a1, b0 + b1 + b2, b1};
+    };
+    // For y = ya: the pair (ya / 2, ya / 2 + 1) when ya is even, the one
+    // row (ya + 1) / 2 in d2 when it is odd.
+    SC u2{}, d2{}, u1{}, m1{};
+    if (R2) {
+      u2 = row2(ya >> 1);
+      d2 = row2((ya >> 1) + 1);
+    }
+    if (R1) {
+      u1 = row1(ya);
+      m1 = row1(ya + 1);
+    }
+#pragma unroll
+    for (int i = 0; i < kLrMaxRun; i++) {
+      const int y = ya + i;
+      if (y >= yb) break;
+      const int32_t dg = s_win[(y + 3) * kWin + tx + 3];
+      const int32_t uu = dg << 4;
+      int32_t v = uu << 7;
+      if (R2) {
+        int32_t av, bv, shift;
+        if ((y & 1) == 0) {
+          if (i != 0) {
+            u2 = d2;
+            d2 = row2((y >> 1) + 1);
+          }
+          av = 5 * (u2.sa + d2.sa) + u2.ca + d2.ca;
+          bv = 5 * (u2.sb + d2.sb) + u2.cb + d2.cb;
+          shift = 9;
+        } else {
+          av = 5 * d2.sa + d2.ca;
+          bv = 5 * d2.sb + d2.cb;
+          shift = 8;
+        }
+        v += xq0 * (rpot(av * dg + bv, shift) - uu);
+      }
+      if (R1) {
+        const SC d1 = row1(y + 2);
+        const int32_t av = 4 * m1.sa + 3 * (u1.sa + d1.sa) + u1.ca + d1.ca;
+        const int32_t bv = 4 * m1.sb + 3 * (u1.sb + d1.sb) + u1.cb + d1.cb;
+        v += xq1 * (rpot(av * dg + bv, 9) - uu);
+        u1 = m1;
+        m1 = d1;
+      }
+      // restoration/selfguided.go:233-247: projection with the int16 wrap.
       const int32_t wv = (int32_t)(int16_t)rpot(v, 11);
       out(y, tx, imin(imax(wv, 0), maxv));
     }
   }
+  __syncthreads();
+}
+
+// The self-guided filter with parameter set `set` and the coded xqd pair
+// (restoration/selfguided.go:111-127, DecodeSGRXQ), dispatched on which of
+// its two radii are on (r0 is 0 or 2, r1 is 0 or 1).
+template <class Out>
+__device__ __forceinline__ void lr_sgr_window(LrSmem& sm, int w, int h, int bd, int set, int xqd0, int xqd1, int PW,
+                                              Out&& out) {
+  const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][1];
+  const int s0 = c_sgr_params[set][2], s1 = c_sgr_params[set][3];
+  if (r0 == 0)
+    lr_sgr_window_t<false, true>(sm, w, h, bd, s0, s1, 0, 128 - xqd1, PW, out);
+  else if (r1 == 0)
+    lr_sgr_window_t<true, false>(sm, w, h, bd, s0, s1, xqd0, 0, PW, out);
+  else
+    lr_sgr_window_t<true, true>(sm, w, h, bd, s0, s1, xqd0, 128 - xqd0 - xqd1, PW, out);
 }
 
 // One restoration tile: processing column j of stripe s of `plane`.
@@ -334,7 +386,7 @@ __device__ void lr_tile(const DFrame& src, const DFrame& dst, const LrArgs& a, c
   __syncthreads();
 
   // Pixels of the tile outside the cropped plane are copied through.
-  if (tx < x1 - x0)
+  if ((x1 > Wc || y1 > Hc) && tx < x1 - x0)
     for (int y = y0 + ty0; y < y1; y += rowStep)
       if (x0 + tx >= Wc || y >= Hc) row_ptr<T>(dp, y)[x0 + tx] = row_ptr<T>(sp, y)[x0 + tx];
 
@@ -378,11 +430,12 @@ __device__ __forceinline__ LrTile lr_locate(const BatchArgs& b, const int* base,
   return LrTile{&J, plane, local % J.lr_cols[plane], local / J.lr_cols[plane]};
 }
 
+template <bool kLoop>
 __global__ void __launch_bounds__(256, 4) k_lr_batch(BatchArgs b) {
   extern __shared__ __align__(16) uint8_t lr_smem_raw[];
   LrSmem& sm = *reinterpret_cast<LrSmem*>(lr_smem_raw);
   const int* base = b.base + ST_LR * (b.n + 1);
-  for_each_item(
+  for_each_item<kLoop>(
       b, ST_LR, base[b.n],
       [&](int item) {
         const LrTile t = lr_locate(b, base, item);
@@ -410,11 +463,16 @@ cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_
   if (total <= 0) return cudaSuccess;
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_lr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LrSmem));
+    cudaError_t e = cudaFuncSetAttribute(k_lr_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LrSmem));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_lr_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LrSmem));
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  k_lr_batch<<<grid, 256, sizeof(LrSmem), st>>>(b);
+  if (batch_loops(b))
+    k_lr_batch<true><<<grid, 256, sizeof(LrSmem), st>>>(b);
+  else
+    k_lr_batch<false><<<grid, 256, sizeof(LrSmem), st>>>(b);
   return cudaGetLastError();
 }
 

@@ -208,6 +208,19 @@ class PostFilterRunner:
         self._display = display if (side.stages & abi.PF_STAGE_FILM_GRAIN) else None
         return self.stats
 
+    def apply_batch_superres(self, items):
+        """pf_batch_apply_superres: items are (coded, side, upscaled, display)
+        tuples (display may be None), all device or all host frames; the
+        chain's stages run as batched launches over the frames."""
+        arr = (abi.pf_superres_item * len(items))()
+        for i, (c, s, u, d) in enumerate(items):
+            arr[i].coded = C.pointer(c)
+            arr[i].side = C.pointer(s)
+            arr[i].up = C.pointer(u)
+            arr[i].display = C.pointer(d) if d is not None else None
+        check(lib().pf_batch_apply_superres(self._h, arr, len(arr), C.byref(self.stats)))
+        return self.stats
+
     def superres_upscale(self, coded, upscaled):
         """The normative super-resolution upscale (superres.UpscalePlaneCoded,
         internal/av1/superres/superres.go:40-107) of every plane of `coded`

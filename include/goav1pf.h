@@ -501,6 +501,26 @@ int pf_superres_upscale(pf_ctx* ctx, const pf_frame* coded, const pf_frame* upsc
 int pf_frame_apply_superres(pf_ctx* ctx, const pf_frame* coded, const pf_frame_side* side,
                             const pf_frame* upscaled, const pf_frame* display, pf_stats* stats);
 
+/* A batch of super-resolved frames (pf_batch_apply for frames with
+ * FrameSize.SuperResEnabled): the same result as pf_frame_apply_superres on
+ * each item in turn.  Device frames: deblocking runs as one launch per pass
+ * over every coded frame, then the boundary rows and CDEF, then the upscale
+ * of each frame, then restoration, border extension and grain as one launch
+ * per stage over every upscaled frame; the call returns once the work is
+ * queued (host side information: once it is copied).  Host frames: one
+ * pf_frame_apply_superres per item.  Every frame of the batch in host memory
+ * or every one in device memory (else PF_ERR_INVALID_ARG); an item's
+ * arguments are checked as pf_frame_apply_superres checks them, and the
+ * first failing item's status is returned before anything is queued. */
+typedef struct pf_superres_item {
+  const pf_frame* coded;      /* coded-width frame, deblocked and CDEF-filtered in place */
+  const pf_frame_side* side;  /* lf / cdef on the coded grid, lr on the upscaled grid */
+  const pf_frame* up;         /* upscaled frame: restoration, extension, grain */
+  const pf_frame* display;    /* grain output (upscaled geometry), or null */
+} pf_superres_item;
+
+int pf_batch_apply_superres(pf_ctx* ctx, const pf_superres_item* items, int32_t n, pf_stats* stats);
+
 /* ---- deblocking masks and level cache from the block record map ----
  * The record map is threading.FrameWorkLoopFilterMap
  * (threading/loop_filter_map.go:46-72): one record per 4x4 MI cell, row-major

@@ -114,3 +114,66 @@ def test_arguments_are_checked(runner):
     with pytest.raises(ErrInvalidFormat):
         runner.apply_superres(case.coded.pf(), case.side, narrow.pf())
     assert_same(before, case.coded, "coded after a rejected call")
+
+
+# A batch of super-resolved frames of mixed size, depth, layout, denominator
+# and stage set through one pf_batch_apply_superres: every frame must equal
+# the oracle's per-frame chain.
+BATCH = [
+    dict(w=1920, h=1080, denom=12, seed=700),
+    dict(w=640, h=360, denom=13, seed=701, bd=10),
+    dict(w=416, h=240, denom=10, seed=702, bd=12),
+    dict(w=320, h=200, denom=11, seed=703, ss=(0, 0)),
+    dict(w=352, h=144, denom=15, seed=704, bd=10, ss=(1, 0)),
+    dict(w=480, h=272, denom=9, seed=705, stages=abi.PF_STAGE_LOOP_FILTER | abi.PF_STAGE_CDEF),
+    dict(w=480, h=272, denom=16, seed=706, stages=abi.PF_STAGE_LOOP_RESTORATION | abi.PF_STAGE_FILM_GRAIN),
+    dict(w=1280, h=720, denom=12, seed=707),
+]
+
+
+def _cases():
+    out = []
+    for kw in BATCH:
+        kw = dict(kw)
+        out.append(SuperResCase(kw.pop("w"), kw.pop("h"), kw.pop("denom"), kw.pop("seed"), **kw))
+    return out
+
+
+def test_batch_device_frames_match_oracle(runner):
+    from goav1_b200.postfilter import DeviceFrame
+
+    cases = _cases()
+    wants = [run_oracle(c) for c in cases]
+    dev = [(DeviceFrame(c.coded.copy()), DeviceFrame(c.up.copy()), DeviceFrame(c.up.like())) for c in cases]
+    st = runner.apply_batch_superres([(dc.pf(), c.side, du.pf(), dd.pf()) for c, (dc, du, dd) in zip(cases, dev)])
+    runner.sync()
+    assert st.completed & abi.PF_STAGE_LOOP_RESTORATION
+    for i, (want, (dc, du, dd)) in enumerate(zip(wants, dev)):
+        for name, a, b in zip(("coded", "upscaled", "display"), want, (dc.download(), du.download(), dd.download())):
+            assert_same(a, b, "frame %d %s" % (i, name))
+
+
+def test_batch_host_frames_match_oracle(runner):
+    cases = _cases()[1:4]
+    wants = [run_oracle(c) for c in cases]
+    got = [(c.coded.copy(), c.up.copy(), c.up.like()) for c in cases]
+    runner.apply_batch_superres([(gc.pf(), c.side, gu.pf(), gd.pf()) for c, (gc, gu, gd) in zip(cases, got)])
+    for i, (want, g) in enumerate(zip(wants, got)):
+        for name, a, b in zip(("coded", "upscaled", "display"), want, g):
+            assert_same(a, b, "frame %d %s" % (i, name))
+
+
+def test_batch_rejects_mixed_memory_and_bad_items(runner):
+    from goav1_b200.postfilter import DeviceFrame, ErrInvalidArgument, ErrInvalidFormat
+
+    cases = _cases()[2:4]
+    dc = DeviceFrame(cases[0].coded.copy())
+    du = DeviceFrame(cases[0].up.copy())
+    with pytest.raises(ErrInvalidArgument):
+        runner.apply_batch_superres([(dc.pf(), cases[0].side, du.pf(), None),
+                                     (cases[1].coded.pf(), cases[1].side, cases[1].up.pf(), None)])
+    before = cases[0].coded.copy()
+    with pytest.raises(ErrInvalidFormat):
+        runner.apply_batch_superres([(cases[0].coded.pf(), cases[0].side, cases[0].up.pf(), None),
+                                     (cases[1].coded.pf(), cases[1].side, cases[1].coded.pf(), None)])
+    assert_same(before, cases[0].coded, "coded after a rejected batch")
