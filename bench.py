@@ -549,10 +549,10 @@ def config2_leg(local, steps, warmup, issue):
         b.record(stream)
     torch.cuda.synchronize()
     ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
-    runner.close()
     stage_names = ["deblock", "cdef", "restoration", "extend", "film_grain"]
-    per_frame = stage_times(local, reset, items) / n
+    per_frame = stage_times(local, reset, items) / n  # reset() runs on this runner's stream
     torch.cuda.synchronize()
+    runner.close()
     bad = oracle_parity([(fr, si, d.download(), dd.download()) for (fr, si), (d, dd, _) in zip(frames, dev)])
     roof = chain_roofline(stage_names, per_frame, n, 3840 * 2160, 1.5, 2, px, ms, load_peaks(), issue)
     return {"metric": METRIC, "value": px / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms, "dtype": "u16",
@@ -719,6 +719,7 @@ def main():
         from goav1_b200.postfilter import cdef_plan_picture
 
         plan5 = cdef_plan_picture(5, True)
+        trunner = PostFilterRunner(device=local, timing=True)
         plan8 = cdef_plan_picture(8, False, is_base=True)
         rows = []
         for seed, src, rec, sside, sigma in _l.search_frames(range(2000, 2000 + args.search_frames), 1920, 1080,
@@ -743,10 +744,15 @@ def main():
             # 8 on camera-content inter pictures (base layer: the level's four
             # trials, luma rows every 4th, chroma presets copying luma's; on
             # other layers level 8 takes the reference's strengths unsearched).
+            # Device time of each kernel group of the learned search (CUDA
+            # events the library records when its context times stages).
+            _, _, _, sts = trunner.cdef_search_learned(sp, rp, ns, q, _l.LAMBDA, model, want_mse=False)
+            _, _, _, sts = trunner.cdef_search_learned(sp, rp, ns, q, _l.LAMBDA, model, want_mse=False)
             t5 = timed(lambda: runner.cdef_search_ex(sp, rp, ns, q, _l.LAMBDA, plan5.ctrls, want_mse=False))
             t8 = timed(lambda: runner.cdef_search_ex(sp, rp, ns, q, _l.LAMBDA, plan8.ctrls, want_mse=False))
             base = _l.luma_sse(r0, i0, m0)
             rows.append(dict(nfb=m0.shape[1], te=te, tl=tl, t5=t5, t8=t8, inc=_l.luma_sse(r1, i1, m0) / base - 1,
+                             kms=list(sts.stage_ms),
                              blocks=st.blocks, fbl=st.fallback_luma, fbc=st.fallback_chroma,
                              trials=(st.trials_luma * 4096 + st.trials_chroma * 2048) / (st.blocks * 64 * 6144)))
         nfb = sum(r["nfb"] for r in rows)
@@ -773,8 +779,12 @@ def main():
                        "fallback_luma_frac": sum(r["fbl"] for r in rows) / blocks,
                        "fallback_chroma_frac": sum(r["fbc"] for r in rows) / blocks,
                        "trial_work_frac": float(np.mean([r["trials"] for r in rows])),
+                       "kernel_ms_per_frame": {k: float(np.mean([r["kms"][i] for r in rows]))
+                                               for i, k in enumerate(["features", "network", "trial_search",
+                                                                      "selection"])},
                        "config": "network goav1_b200/data/cdef_mlp_1080p.bin, threshold 0.5, 3 candidates per "
                                  "head; " + cfg}
+        trunner.close()
 
     # Encoder loop-restoration search (pf_lr_search: every 64x64 luma unit
     # searched with the six Wiener tap sets and the four SGR presets, the

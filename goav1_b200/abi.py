@@ -325,6 +325,7 @@ class pf_cdef_learned_stats(C.Structure):
         ("fallback_chroma", C.c_int32),
         ("trials_luma", C.c_int32),
         ("trials_chroma", C.c_int32),
+        ("stage_ms", C.c_float * 4),
     ]
 
 

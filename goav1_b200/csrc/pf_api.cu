@@ -27,6 +27,8 @@
 namespace pf {
 cudaError_t launch_deblock_batch(const BatchArgs& b, int total, int grid, int dir, cudaStream_t st);
 cudaError_t launch_cdef_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
+size_t cdef_tables_bytes();
+cudaError_t launch_cdef_tables(int16_t* dst, cudaStream_t st);
 cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
 cudaError_t launch_fg_templates_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
 cudaError_t launch_fg_offsets_batch(const BatchArgs& b, int total, int grid, cudaStream_t st);
@@ -111,6 +113,7 @@ struct pf_ctx {
   DevBuf sidebuf;            // host side information copied up
   DevBuf jobs, bases, counters;
   DevBuf search;             // encoder CDEF search scratch
+  DevBuf ctab;               // CDEF constrain() tables (CdefArgs.ctab)
   DevBuf model;              // the learned search's network, uploaded when it changes
   std::vector<uint8_t> model_shadow;  // host copy of what `model` holds
   void* pinned = nullptr;    // page-locked staging for small host inputs
@@ -530,6 +533,14 @@ extern "C" pf_ctx* pf_create(const pf_config* cfg, int* status) {
   cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
   cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
   c->sm_count = prop.multiProcessorCount;
+  // The CDEF kernel's constrain() tables, built once on the context's stream
+  // (every later launch is ordered after it).
+  if (c->ctab.ensure(cdef_tables_bytes()) != cudaSuccess ||
+      launch_cdef_tables((int16_t*)c->ctab.p, c->stream) != cudaSuccess) {
+    pf_destroy(c);
+    if (status) *status = PF_ERR_DEVICE;
+    return nullptr;
+  }
   if (status) *status = PF_OK;
   return c;
 }
@@ -541,8 +552,8 @@ extern "C" void pf_destroy(pf_ctx* c) {
   cudaStreamSynchronize(c->side);
   if (c->h2d) cudaStreamSynchronize(c->h2d);
   if (c->d2h) cudaStreamSynchronize(c->d2h);
-  DevBuf* bufs[] = {&c->io,   &c->disp,  &c->arena,    &c->sidebuf, &c->jobs,
-                    &c->bases, &c->counters, &c->search, &c->sr_up,   &c->sr_lines};
+  DevBuf* bufs[] = {&c->io,     &c->disp,     &c->arena,  &c->sidebuf, &c->jobs,    &c->bases,
+                    &c->counters, &c->search, &c->sr_up,   &c->sr_lines, &c->ctab};
   for (DevBuf* b : bufs) b->release();
   for (pf_ctx::HostSlot& h : c->hslot) {
     h.io.release();
@@ -1052,6 +1063,7 @@ static int prepare_batch(pf_ctx* c, const FrameRef* refs, int n, Bytes& hs, DevB
   for (int i = 0; i < n; i++) {
     int counts[ST_COUNT];
     fill_job(refs[i], arena, side, hs, c->hjobs[i], counts, c->db_tile);
+    c->hjobs[i].cdef.ctab = (const int16_t*)c->ctab.p;
     for (int k = 0; k < ST_COUNT; k++) c->hbase[(size_t)k * (n + 1) + i + 1] = c->hbase[(size_t)k * (n + 1) + i] + counts[k];
     const pf_frame_side* s = refs[i].s;
     if (counts[ST_DEBLOCK_V]) done |= PF_STAGE_LOOP_FILTER;
@@ -1742,6 +1754,8 @@ void* pf_internal_search_scratch(pf_ctx* c, size_t bytes) {
   return c->search.p;
 }
 void* pf_internal_stream(pf_ctx* c) { return (void*)c->stream; }
+// The context's stage events when it times stages (pf_config.timing), else null.
+cudaEvent_t* pf_internal_events(pf_ctx* c) { return c->timing ? c->ev : nullptr; }
 
 // Page-locked host staging of at least `bytes` (grown, never shrunk), so
 // small host inputs go up with an asynchronous copy.  Valid until the next

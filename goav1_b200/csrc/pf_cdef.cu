@@ -33,7 +33,7 @@ struct CdefSmem {
   int32_t blk[64];   // per block: filter flag << 16 | priShift << 12 | strength << 4 | dir
   int2 ofs[12];      // direction tap offsets in smem units (cdef/filter.go:53-66)
   uint8_t dir[64];
-  int16_t tab[kSecTab + 1][kTabLen];
+  alignas(16) int16_t tab[kSecTab + 1][kTabLen];
   uint32_t strengths;    // bit k: a block of the plane filters with primary strength k
   int8_t slot[16];       // table of each primary strength
   int8_t slot_str[16];   // strength of each table
@@ -242,14 +242,15 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
           if (on) sm.slot_str[k] = (int8_t)tid;
         }
         __syncthreads();
-        for (int i = tid; i < (ntab + 1) * 511; i += 256) {
-          const int t = i / 511, d = i - t * 511 - 255;
-          if (t < ntab) {
-            const int st = sm.slot_str[t];
-            sm.tab[t][d + 255] = (int16_t)constrain(d, st, constrain_shift(st, damping));
-          } else {
-            sm.tab[kSecTab][d + 255] = (int16_t)(sec ? constrain(d, sec, secShift) : 0);
-          }
+        // Each table is a copy of the context's precomputed one for its
+        // strength and shift (64 16-byte words; zeros for no secondary).
+        for (int i = tid; i < (ntab + 1) * (kTabLen / 8); i += 256) {
+          const int t = i / (kTabLen / 8), wd = i - t * (kTabLen / 8);
+          const int st = t < ntab ? sm.slot_str[t] : sec;
+          const int sh = t < ntab ? constrain_shift(st, damping) : secShift;
+          uint4 v = make_uint4(0, 0, 0, 0);
+          if (st) v = reinterpret_cast<const uint4*>(a.ctab + (size_t)(st * 8 + sh) * kTabLen)[wd];
+          reinterpret_cast<uint4*>(&sm.tab[t < ntab ? t : kSecTab][0])[wd] = v;
         }
         __syncthreads();
       }
@@ -339,6 +340,20 @@ __global__ void __launch_bounds__(256, 4) k_cdef_batch(BatchArgs b) {
             prefetch_block<uint16_t>(J.io.pl[plane], x - 8, x + (64 >> xdec) + 8, y - 2, y + (64 >> ydec) + 2);
         }
       });
+}
+
+// The constrain() tables of CdefArgs.ctab, from constrain() itself: one
+// CTA per (strength, shift).
+__global__ void __launch_bounds__(kTabLen) k_cdef_tables(int16_t* t) {
+  const int st = blockIdx.x >> 3, sh = blockIdx.x & 7, i = threadIdx.x;
+  t[(size_t)blockIdx.x * kTabLen + i] = (int16_t)(i < 511 ? constrain(i - 255, st, sh) : 0);
+}
+
+size_t cdef_tables_bytes() { return (size_t)16 * 8 * kTabLen * sizeof(int16_t); }
+
+cudaError_t launch_cdef_tables(int16_t* dst, cudaStream_t st) {
+  k_cdef_tables<<<16 * 8, kTabLen, 0, st>>>(dst);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_cdef_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {

@@ -112,6 +112,10 @@ struct CdefArgs {
   uint8_t* lines[3];    // [boundary k][4 rows][stride] samples of T
   int64_t line_stride[3];  // bytes per line row
   int save_lines[3];
+  // constrain() of every 8-bit strength (0..15) and shift (0..7): table
+  // [strength][shift] of 512 entries, entry 255 + d for a difference d in
+  // -255..255 (entry 511 is 0).
+  const int16_t* ctab;
 };
 
 struct LrArgs {

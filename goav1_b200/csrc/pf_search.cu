@@ -656,6 +656,7 @@ using namespace pf;
 
 void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
 void* pf_internal_stream(pf_ctx* c);
+cudaEvent_t* pf_internal_events(pf_ctx* c);  // pf_api.cu: null unless the context times stages
 void* pf_internal_pinned(pf_ctx* c, size_t bytes);
 void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, size_t extra, cudaStream_t st,
                                 int* changed);
@@ -858,11 +859,13 @@ static int search_max_cfg(const pf_cdef_search_params* params) {
 // Search (with S.a.tmask already set by the caller, or null), selection,
 // results to the host.
 static int search_finish(Staged& S, const pf_cdef_search_params* params, uint64_t* mse_out, uint8_t* fb_index_out,
-                         pf_cdef_search_result* result) {
+                         pf_cdef_search_result* result, cudaEvent_t* ev = nullptr) {
   const cudaStream_t st = S.st;
   if (launch_search(S.a, st) != cudaSuccess) return PF_ERR_DEVICE;
+  if (ev && cudaEventRecord(ev[3], st) != cudaSuccess) return PF_ERR_DEVICE;
   if (launch_select(S.s, S.maxCfg, (unsigned long long)params->lambda, S.idx, S.fo, st) != cudaSuccess)
     return PF_ERR_DEVICE;
+  if (ev && cudaEventRecord(ev[4], st) != cudaSuccess) return PF_ERR_DEVICE;
   // The small results come back through the page-locked block (a pageable
   // destination would make each copy a staged, synchronous one).
   auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
@@ -1177,12 +1180,18 @@ extern "C" int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const
   float* W = (float*)(mbase + ((sizeof(pf_cdef_mlp) + 255) & ~(size_t)255));
   S.a.dirs = S.extra + xBytes + mBytes;
   S.a.ais = (int8_t*)(S.extra + xBytes + mBytes + (size_t)nfb * 64);
+  // With stage timing on: events around features, network, trial search
+  // and selection (read into stats->stage_ms).
+  cudaEvent_t* ev = stats ? pf_internal_events(ctx) : nullptr;
+  if (ev && cudaEventRecord(ev[0], S.st) != cudaSuccess) return PF_ERR_DEVICE;
   if (launch_features(S.a, params->qindex, X, false, S.st) != cudaSuccess) return PF_ERR_DEVICE;
+  if (ev && cudaEventRecord(ev[1], S.st) != cudaSuccess) return PF_ERR_DEVICE;
   if (launch_mlp_masks(dmodel, W, changed != 0, X, nfb, threshold, candidates, masks, S.st) != cudaSuccess)
     return PF_ERR_DEVICE;
+  if (ev && cudaEventRecord(ev[2], S.st) != cudaSuccess) return PF_ERR_DEVICE;
   S.a.tmask = masks;
   S.s.refine = (flags & PF_LEARNED_REFINE) ? 1 : 0;
-  const int r = search_finish(S, params, mse_out, fb_index_out, result);
+  const int r = search_finish(S, params, mse_out, fb_index_out, result, ev);
   if (r != PF_OK) return r;
   // The statistics are read back after the search (no host wait between the
   // network and the search it steers).
@@ -1193,6 +1202,14 @@ extern "C" int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const
         cudaMemcpy(skip.data(), S.a.skip, nfb, cudaMemcpyDeviceToHost) != cudaSuccess)
       return PF_ERR_DEVICE;
     memset(stats, 0, sizeof(*stats));
+    for (int i = 0; i < 4; i++) {
+      float ms = -1.f;
+      if (ev && cudaEventElapsedTime(&ms, ev[i], ev[i + 1]) != cudaSuccess) {
+        ms = -1.f;
+        (void)cudaGetLastError();
+      }
+      stats->stage_ms[i] = ev ? ms : -1.f;
+    }
     for (int fb = 0; fb < nfb; fb++) {
       if (skip[fb]) continue;
       stats->blocks++;

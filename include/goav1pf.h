@@ -691,6 +691,8 @@ typedef struct pf_cdef_learned_stats {
   int32_t fallback_chroma;  /* blocks whose chroma head measured all 64 trials */
   int32_t trials_luma;      /* luma trials measured, all blocks */
   int32_t trials_chroma;    /* chroma trials measured, all blocks */
+  float stage_ms[4];        /* device time of features, network, trial search,
+                               selection when the context times stages, else -1 */
 } pf_cdef_learned_stats;
 
 /* Per-filter-block features of an 8-bit 4:2:0 deblocked reconstruction
