@@ -21,30 +21,49 @@ static __constant__ int8_t c_cdef_dir[12][2][2] = {
 
 __device__ __forceinline__ int dir_off(int e, int k) { return c_cdef_dir[e][k][0] * kSW + c_cdef_dir[e][k][1]; }
 
-// Direction cost of direction D over one 8x8 block (cdef/direction.go:37-79
-// partial sums, :469-501 cost).  blk points at the block's top-left in smem
-// (16-byte aligned: each row is read as one 16-byte word).
+// Direction cost over one 8x8 block (cdef/direction.go:37-79 partial sums,
+// :469-501 cost): for direction D the samples (i, j), shifted to 8 bits
+// and less 128, are summed into partials p[dir_k(D, i, j)], and the cost is
+// the weighted sum of their squares.  dir_k is that index; dir_count is how
+// many samples each partial sums.
+__host__ __device__ constexpr int dir_k(int D, int i, int j) {
+  return D == 0 ? i + j : D == 1 ? i + (j >> 1) : D == 2 ? i : D == 3 ? 3 + i - (j >> 1) :
+         D == 4 ? 7 + i - j : D == 5 ? 3 - (i >> 1) + j : D == 6 ? j : (i >> 1) + j;
+}
+__host__ __device__ constexpr int dir_count(int D, int k) {
+  int n = 0;
+  for (int i = 0; i < 8; i++)
+    for (int j = 0; j < 8; j++) n += dir_k(D, i, j) == k;
+  return n;
+}
+
+// The direction cost on packed sample pairs: w[i][m] holds samples (i, 2m) and
+// (i, 2m + 1) of the block in its low and high halves, raw.  Each pair is
+// added as one 32-bit word into the accumulator of its even sample's index
+// (the odd sample's index differs from it by the same -1, 0 or +1 for every
+// pair of a direction), with the samples shifted to 8 bits and left biased
+// by +128: a half never sums more than eight values below 256, so it never
+// carries into the other.  The halves are then split into the partial sums,
+// the bias taken off by each sum's sample count, and the cost formed from
+// them (direction.go:469-501), so the result is the same integer as summing
+// the shifted, unbiased samples one by one.
 template <int D>
-__device__ __forceinline__ int32_t dir_cost(const uint16_t* blk, int shift) {
+__host__ __device__ __forceinline__ int32_t dir_cost_pairs(const uint32_t (&w)[8][4], int shift) {
+  constexpr int kDelta = dir_k(D, 0, 1) - dir_k(D, 0, 0);
+  const uint32_t mask = (0xffffu >> shift) * 0x10001u;
+  uint32_t acc[15];
+#pragma unroll
+  for (int k = 0; k < 15; k++) acc[k] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int m = 0; m < 4; m++) acc[dir_k(D, i, 2 * m)] += (w[i][m] >> shift) & mask;
   int32_t p[15];
 #pragma unroll
-  for (int k = 0; k < 15; k++) p[k] = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const uint4 row = *reinterpret_cast<const uint4*>(blk + i * kSW);
-    const uint32_t rw[4] = {row.x, row.y, row.z, row.w};
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int32_t x = (int32_t)(((rw[j >> 1] >> (16 * (j & 1))) & 0xffffu) >> shift) - 128;
-      if (D == 0) p[i + j] += x;
-      if (D == 1) p[i + (j >> 1)] += x;
-      if (D == 2) p[i] += x;
-      if (D == 3) p[3 + i - (j >> 1)] += x;
-      if (D == 4) p[7 + i - j] += x;
-      if (D == 5) p[3 - (i >> 1) + j] += x;
-      if (D == 6) p[j] += x;
-      if (D == 7) p[(i >> 1) + j] += x;
-    }
+  for (int k = 0; k < 15; k++) {
+    int32_t v = (int32_t)(acc[k] & 0xffffu);
+    if (k - kDelta >= 0 && k - kDelta < 15) v += (int32_t)(acc[k - kDelta] >> 16);
+    p[k] = v - 128 * dir_count(D, k);
   }
   if (D == 2 || D == 6) {
     int32_t s = 0;
@@ -64,16 +83,27 @@ __device__ __forceinline__ int32_t dir_cost(const uint16_t* blk, int shift) {
          (p[2] * p[2] + p[8] * p[8]) * 140;
 }
 
+template <int D>
+__device__ __forceinline__ int32_t dir_cost_packed(const uint16_t* blk, int shift) {
+  uint32_t w[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint4 row = *reinterpret_cast<const uint4*>(blk + i * kSW);
+    w[i][0] = row.x, w[i][1] = row.y, w[i][2] = row.z, w[i][3] = row.w;
+  }
+  return dir_cost_pairs<D>(w, shift);
+}
+
 __device__ __forceinline__ int32_t dir_cost_any(int d, const uint16_t* blk, int shift) {
   switch (d) {
-    case 0: return dir_cost<0>(blk, shift);
-    case 1: return dir_cost<1>(blk, shift);
-    case 2: return dir_cost<2>(blk, shift);
-    case 3: return dir_cost<3>(blk, shift);
-    case 4: return dir_cost<4>(blk, shift);
-    case 5: return dir_cost<5>(blk, shift);
-    case 6: return dir_cost<6>(blk, shift);
-    default: return dir_cost<7>(blk, shift);
+    case 0: return dir_cost_packed<0>(blk, shift);
+    case 1: return dir_cost_packed<1>(blk, shift);
+    case 2: return dir_cost_packed<2>(blk, shift);
+    case 3: return dir_cost_packed<3>(blk, shift);
+    case 4: return dir_cost_packed<4>(blk, shift);
+    case 5: return dir_cost_packed<5>(blk, shift);
+    case 6: return dir_cost_packed<6>(blk, shift);
+    default: return dir_cost_packed<7>(blk, shift);
   }
 }
 

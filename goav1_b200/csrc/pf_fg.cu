@@ -41,20 +41,24 @@ __device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
 // to the shared template by lanes r-1.. at an earlier step, and the warp
 // barrier that ends each step makes it visible.  The filter runs in
 // transposed form: when the value of row y-d at column x + LAG arrives, its
-// products go straight into the partial sums acc[j] of the outputs x .. x +
-// 2*LAG it reaches, and the lane's own output adds its in-row products to
-// acc[1..LAG]; the output then needs only acc[0] (and the luma term), so a
-// step is one new load per row above, 3*(2*LAG+1) + LAG multiply-adds and a
-// shift of the partial sums, and its loop-carried path is load -> one
-// multiply-add -> round -> clip -> store.  A lane outside the AR columns
-// passes the template's value through unchanged, so the rows above always
-// hold the template as it stands.  Bands run one after the other, each only
-// as long as its own rows need.  LAG is a template argument (coefficients
-// in registers, unrolled taps).
+// products go straight into the partial sums of the outputs x .. x + 2*LAG
+// it reaches, and the lane's own output adds its in-row products to the
+// next LAG outputs' sums; the output then needs only its own sum, so the
+// loop-carried path is load -> one multiply-add -> round -> clip -> store.
+// The 2*LAG+1 partial sums rotate through acc[] with the step (the steps
+// run in groups of 2*LAG+1, slot (j + k) mod (2*LAG+1) holding output x + j
+// at step k of a group), so moving to the next column renames registers
+// instead of copying them.  A chroma template's luma term comes from lt[]
+// (the averaged luma grain at each chroma position, filled before the
+// recursion).  A lane outside the AR columns passes the template's value
+// through unchanged, so the rows above always hold the template as it
+// stands.  Bands run one after the other, each only as long as its own rows
+// need.  LAG is a template argument (coefficients in registers, unrolled
+// taps).
 constexpr int kFgTemplateThreads = 96;
 
 template <int LAG>
-__device__ void ar_warp(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h) {
+__device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
   constexpr int kTaps = 2 * LAG * (LAG + 1);  // causal neighbours before the centre
   constexpr int W = 2 * LAG + 1;
   const int lane = threadIdx.x & 31;
@@ -63,67 +67,79 @@ __device__ void ar_warp(int16_t* g, const int16_t* luma, const FgTemplateArgs& p
   int co[kTaps + 1];
 #pragma unroll
   for (int i = 0; i <= kTaps; i++) co[i] = p.coeffs[plane][i];
-  const bool lumaTerm = plane != 0 && p.num_y_points != 0;
-  const int sx = plane ? p.ssx : 0, sy = plane ? p.ssy : 0;
+  const int coL = lt ? co[kTaps] : 0;
   for (int y0 = 3; y0 < h; y0 += 32) {
     const int rows = imin(32, h - y0);
     const int y = y0 + lane;
     const bool row = lane < rows;
-    int acc[W];  // acc[j]: partial sum of output column x + j
+    int acc[W];
 #pragma unroll
     for (int j = 0; j < W; j++) acc[j] = 0;
-    // The first step brings column 0 of the rows above into the windows;
-    // the last one finishes column w - 4 of the band's last row.
+    // The first step brings column 0 of the rows above into the sums; the
+    // last one finishes column w - 4 of the band's last row.
     const int tend = 4 * (rows - 1) + w - 3;
-    for (int t = -LAG; t < tend; t++) {
-      const int x = t - 4 * lane;
-      const int xn = x + LAG;  // the column entering the windows
-      const bool inCol = row && x >= 0 && x < w;
-      const int g0 = inCol ? g[y * kGW + x] : 0;
-      if (row && xn >= 0 && xn < w) {
-        // Farthest row first: the row directly above (written one step ago
-        // when LAG = 3) enters the sum of this step's output last.
+    for (int t0 = -LAG; t0 < tend; t0 += W) {
 #pragma unroll
-        for (int d = LAG; d >= 1; d--) {
-          const int v = g[(y - d) * kGW + xn];
+      for (int k = 0; k < W; k++) {
+        const int t = t0 + k;
+        if (t < tend) {
+          const int x = t - 4 * lane;
+          const int xn = x + LAG;  // the column entering the sums
+          const bool inCol = row && x >= 0 && x < w;
+          const int g0 = inCol ? g[y * kGW + x] : 0;
+          if (row && xn >= 0 && xn < w) {
+            // Farthest row first: the row directly above (written one step
+            // ago when LAG = 3) enters this step's output last.
 #pragma unroll
-          for (int j = W - 1; j >= 0; j--) acc[j] += co[(LAG - d) * W + 2 * LAG - j] * v;
-        }
-      }
-      int out = g0;
-      if (inCol && x >= 3 && x < w - 3) {
-        int sum = acc[0];
-        if (lumaTerm) {
-          const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
-          int s = luma[ly * kGW + lx];
-          if (sx) s += luma[ly * kGW + lx + 1];
-          if (sy) {
-            s += luma[(ly + 1) * kGW + lx];
-            if (sx) s += luma[(ly + 1) * kGW + lx + 1];
+            for (int d = LAG; d >= 1; d--) {
+              const int v = g[(y - d) * kGW + xn];
+#pragma unroll
+              for (int j = W - 1; j >= 0; j--) acc[(j + k) % W] += co[(LAG - d) * W + 2 * LAG - j] * v;
+            }
           }
-          sum += rpow2(s, sx + sy) * co[kTaps];
+          int out = g0;
+          if (inCol && x >= 3 && x < w - 3) {
+            int sum = acc[k % W];
+            if (lt) sum += lt[y * kGW + x] * coL;
+            out = iclip(g0 + ((sum + ro) >> cs), gmin, gmax);
+            g[y * kGW + x] = (int16_t)out;
+          }
+          // Output x's in-row products for columns x + 1 .. x + LAG; its
+          // slot then serves column x + W.
+#pragma unroll
+          for (int m = 1; m <= LAG; m++) acc[(m + k) % W] += co[LAG * W + LAG - m] * out;
+          acc[k % W] = 0;
         }
-        out = iclip(g0 + ((sum + ro) >> cs), gmin, gmax);
-        g[y * kGW + x] = (int16_t)out;
+        __syncwarp();
       }
-      // This output's in-row products for columns x + 1 .. x + LAG, then
-      // the partial sums move one column on.
-#pragma unroll
-      for (int m = 1; m <= LAG; m++) acc[m] += co[LAG * W + LAG - m] * out;
-#pragma unroll
-      for (int j = 0; j + 1 < W; j++) acc[j] = acc[j + 1];
-      acc[W - 1] = 0;
-      __syncwarp();
     }
   }
 }
 
-__device__ void ar_warp_lag(int16_t* g, const int16_t* luma, const FgTemplateArgs& p, int plane, int w, int h) {
+// Luma term of the chroma AR (chroma.go:92-199): at each chroma AR position
+// the luma grain averaged over the co-located 1, 2 or 4 samples, into lt
+// (same layout as the templates).  All threads of the CTA.
+__device__ void luma_term(int16_t* lt, const int16_t* luma, int sx, int sy, int w, int h) {
+  const int aw = w - 6;
+  for (int i = threadIdx.x; i < aw * (h - 3); i += blockDim.x) {
+    const int y = 3 + i / aw, x = 3 + i % aw;
+    const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
+    int s = luma[ly * kGW + lx];
+    if (sx) s += luma[ly * kGW + lx + 1];
+    if (sy) {
+      s += luma[(ly + 1) * kGW + lx];
+      if (sx) s += luma[(ly + 1) * kGW + lx + 1];
+    }
+    lt[y * kGW + x] = (int16_t)rpow2(s, sx + sy);
+  }
+}
+
+__device__ void ar_warp_lag(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
   switch (p.lag) {
-    case 0: ar_warp<0>(g, luma, p, plane, w, h); break;
-    case 1: ar_warp<1>(g, luma, p, plane, w, h); break;
-    case 2: ar_warp<2>(g, luma, p, plane, w, h); break;
-    default: ar_warp<3>(g, luma, p, plane, w, h); break;
+    case 0: ar_warp<0>(g, lt, p, plane, w, h); break;
+    case 1: ar_warp<1>(g, lt, p, plane, w, h); break;
+    case 2: ar_warp<2>(g, lt, p, plane, w, h); break;
+    default: ar_warp<3>(g, lt, p, plane, w, h); break;
   }
 }
 
@@ -160,15 +176,19 @@ __device__ void gauss_fill(int16_t* g, const int16_t* gauss, uint16_t seed, int 
 }
 
 // One frame's templates: Gaussian fills by warps 0-2 (luma, Cb, Cr), then the
-// AR recursions (all threads: luma, then Cb and Cr side by side).
-// s_gauss holds the Gaussian sequence (lanes draw different entries, which
-// constant memory would serialise).
+// AR recursions (luma on warp 0, then Cb and Cr side by side).  s_gl holds
+// the Gaussian sequence while the templates are filled (lanes draw
+// different entries, which constant memory would serialise), then the
+// chroma AR's luma term.
 __device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, int16_t (*s_g)[kGW * kGH],
-                             const int16_t* s_gauss) {
+                             int16_t* s_gl) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int16_t* outs[3] = {gy, gu, gv};
   const int cw = p.ssx ? 44 : kGW, ch = p.ssy ? 38 : kGH;
   const int cshape = p.ssx ? (p.ssy ? 2 : 1) : 0;
+  const int16_t* s_gauss = s_gl;
+  for (int i = threadIdx.x; i < 2048; i += blockDim.x) s_gl[i] = c_gauss[i];
+  __syncthreads();
   if (warp < 3) {
     int16_t* g = s_g[warp];
     for (int i = lane; i < kGW * kGH; i += 32) g[i] = 0;
@@ -188,8 +208,13 @@ __device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, 
   // luma term reads the finished luma template).
   if (warp == 0 && p.num_y_points != 0 && p.lag != 0) ar_warp_lag(s_g[0], nullptr, p, 0, kGW, kGH);
   __syncthreads();
+  const bool lumaTerm = p.num_y_points != 0;
+  if (lumaTerm) {
+    luma_term(s_gl, s_g[0], p.ssx, p.ssy, cw, ch);
+    __syncthreads();
+  }
   const bool runC = warp >= 1 && warp <= 2 && p.active[warp] && !(p.lag == 0 && p.num_y_points == 0);
-  if (runC) ar_warp_lag(s_g[warp], s_g[0], p, warp, cw, ch);
+  if (runC) ar_warp_lag(s_g[warp], lumaTerm ? s_gl : nullptr, p, warp, cw, ch);
   __syncthreads();
   for (int pl = 0; pl < 3; pl++)
     if (outs[pl])
@@ -335,13 +360,11 @@ __device__ __forceinline__ void extend_px(const DFrame& f, int plane, int x, int
 
 __global__ void __launch_bounds__(kFgTemplateThreads) k_fg_templates_batch(BatchArgs b) {
   __shared__ int16_t s_g[3][kGW * kGH];
-  __shared__ int16_t s_gauss[2048];
-  for (int i = threadIdx.x; i < 2048; i += blockDim.x) s_gauss[i] = c_gauss[i];
-  __syncthreads();
+  __shared__ int16_t s_gl[kGW * kGH];  // Gaussian sequence, then the luma term
   const int* base = b.base + ST_FG_TEMPLATES * (b.n + 1);
   for_each_item(b, ST_FG_TEMPLATES, base[b.n], [&](int item) {
     const FrameJob& J = b.jobs[find_frame(base, b.n, item)];
-    fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], s_g, s_gauss);
+    fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], s_g, s_gl);
   });
 }
 

@@ -173,7 +173,8 @@ def test_batch_rejects_mixed_memory_and_bad_items(runner):
         runner.apply_batch_superres([(dc.pf(), cases[0].side, du.pf(), None),
                                      (cases[1].coded.pf(), cases[1].side, cases[1].up.pf(), None)])
     before = cases[0].coded.copy()
+    disp = cases[0].up.like()
     with pytest.raises(ErrInvalidFormat):
-        runner.apply_batch_superres([(cases[0].coded.pf(), cases[0].side, cases[0].up.pf(), None),
+        runner.apply_batch_superres([(cases[0].coded.pf(), cases[0].side, cases[0].up.pf(), disp.pf()),
                                      (cases[1].coded.pf(), cases[1].side, cases[1].coded.pf(), None)])
     assert_same(before, cases[0].coded, "coded after a rejected batch")
