@@ -121,14 +121,20 @@ struct pf_ctx {
   void* model_pin = nullptr; // page-locked staging of the network upload
   std::vector<FrameJob> hjobs;
   std::vector<int> hbase;
-  std::vector<uint8_t> hside;
+  // Side information of the current batch, page-locked so its upload is an
+  // asynchronous DMA; side_done marks the upload's end, and the buffer is
+  // not rewritten before it (side_pending).
+  PinnedBytes hside;
+  cudaEvent_t side_done = nullptr;
+  bool side_pending = false;
   // The schedule of each stage's launch (pf_schedule): persistent-CTA count
   // (0 = one CTA per chunk), work items per chunk, items prefetched ahead,
   // and the deblocking tile shape.
   int persistent[ST_COUNT] = {};
   int chunk[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1};
   int ahead[ST_COUNT] = {};
-  int db_tile = 0;
+  int tile[ST_COUNT] = {};  // launch-level tile setting (grain apply: rows per load group)
+  int db_tile = 0;          // deblocking tile shape (per job: it sets the tile counts)
   // CUDA graphs of pf_batch_apply, one per batch signature (see run_batch).
   int graphs = 0;
   std::vector<struct GraphEntry*> gcache;
@@ -580,6 +586,7 @@ extern "C" void pf_destroy(pf_ctx* c) {
   cudaEventDestroy(c->fork);
   cudaEventDestroy(c->join);
   if (c->chain_done) cudaEventDestroy(c->chain_done);
+  if (c->side_done) cudaEventDestroy(c->side_done);
   cudaStreamDestroy(c->side);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -900,7 +907,14 @@ static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, con
                          int n, bool fg, const void* djobs = nullptr, const void* dbases = nullptr) {
   const cudaStream_t st = c->stream;
   if (!djobs) {
-    if (nside) CK(cudaMemcpyAsync(c->sidebuf.p, hside, nside, cudaMemcpyHostToDevice, st));
+    if (nside) {
+      CK(cudaMemcpyAsync(c->sidebuf.p, hside, nside, cudaMemcpyHostToDevice, st));
+      if (hside == c->hside.data()) {
+        if (!c->side_done) CK(cudaEventCreateWithFlags(&c->side_done, cudaEventDisableTiming));
+        CK(cudaEventRecord(c->side_done, st));
+        c->side_pending = true;
+      }
+    }
     CK(cudaMemcpyAsync(c->jobs.p, hjobs, sizeof(FrameJob) * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->bases.p, hbase, sizeof(int) * c->hbase.size(), cudaMemcpyHostToDevice, st));
     djobs = c->jobs.p;
@@ -919,6 +933,7 @@ static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, con
     const int t = total(k);
     a.chunk = c->chunk[k];
     a.ahead = c->ahead[k];
+    a.tile = c->tile[k];
     const int chunks = (t + a.chunk - 1) / a.chunk;
     if (c->persistent[k] > 0 && chunks > c->persistent[k]) {
       *grid = c->persistent[k];
@@ -976,6 +991,7 @@ static std::vector<int64_t> batch_key(const pf_ctx* c, int n, bool fg) {
     k.push_back(c->persistent[i]);
     k.push_back(c->chunk[i]);
     k.push_back(c->ahead[i]);
+    k.push_back(c->tile[i]);
   }
   k.push_back(c->db_tile);
   for (int v : c->hbase) k.push_back(v);
@@ -1093,6 +1109,11 @@ static void add_stats(const pf_ctx* c, int n, uint32_t done, pf_stats* stats) {
 static int run_batch(pf_ctx* c, const FrameRef* refs, int n, pf_stats* stats, bool useGraph = false) {
   uint32_t done = 0;
   bool fg = false;
+  // The previous batch's side information may still be on its way up.
+  if (c->side_pending) {
+    CKW(wait_event(c, c->side_done, __LINE__));
+    c->side_pending = false;
+  }
   int st = prepare_batch(c, refs, n, c->hside, c->sidebuf, &done, &fg);
   if (st != PF_OK) return st;
   const int est = (useGraph && !c->timing)
@@ -1197,21 +1218,31 @@ static cudaError_t copy_planes(const pf_frame* f, void* const* dev, const int64_
 extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side* s, const pf_frame* display,
                               pf_stats* stats) {
   if (!c) return PF_ERR_INVALID_ARG;
+  FrameRef r;
+  memset(&r, 0, sizeof(r));
+  // A host frame's upload goes out first, once the frame's own planes are
+  // known to be what it describes (the copy reads exactly those); the
+  // side information's validation (a scan of its level cache on the host)
+  // then runs while the frame is on its way.  A rejected call has only
+  // written the context's staging.
+  const bool early = f && s && f->memory == PF_MEM_HOST && plane_dims_ok(f);
+  if (early) {
+    CK(cudaSetDevice(c->device));
+    CK(c->io.ensure(host_frame_layout(f, nullptr, nullptr, r.ioStride) + 256));
+    host_frame_layout(f, (uint8_t*)c->io.p, r.io, r.ioStride);
+    CK(copy_planes(f, r.io, r.ioStride, true, c->stream));
+  }
   int st = pf_frame_validate(f, s, display);
   if (st != PF_OK) return st;
   CK(cudaSetDevice(c->device));
   if (stats) memset(stats, 0, sizeof(*stats));
   const int bps = bps_of(f);
-  FrameRef r;
-  memset(&r, 0, sizeof(r));
   r.f = f;
   r.s = s;
   const bool wantDisp = (s->stages & PF_STAGE_FILM_GRAIN) && display;
   r.display = wantDisp ? display : nullptr;
   if (f->memory == PF_MEM_HOST) {
-    CK(c->io.ensure(host_frame_layout(f, nullptr, nullptr, r.ioStride) + 256));
-    host_frame_layout(f, (uint8_t*)c->io.p, r.io, r.ioStride);
-    CK(copy_planes(f, r.io, r.ioStride, true, c->stream));
+    if (!early) return PF_ERR_SHORT_BUFFER;  // unreachable: validation checks the planes too
   } else {
     for (int p = 0; p < 3; p++) {
       r.io[p] = f->plane[p].data;
@@ -1756,6 +1787,8 @@ void* pf_internal_search_scratch(pf_ctx* c, size_t bytes) {
 void* pf_internal_stream(pf_ctx* c) { return (void*)c->stream; }
 // The context's stage events when it times stages (pf_config.timing), else null.
 cudaEvent_t* pf_internal_events(pf_ctx* c) { return c->timing ? c->ev : nullptr; }
+// The context's CDEF constrain() tables (CdefArgs.ctab).
+const int16_t* pf_internal_ctab(pf_ctx* c) { return (const int16_t*)c->ctab.p; }
 
 // Page-locked host staging of at least `bytes` (grown, never shrunk), so
 // small host inputs go up with an asynchronous copy.  Valid until the next
@@ -1820,7 +1853,7 @@ static const int kTuneStatIndex[PF_TUNE_GROUPS] = {0, 1, 2, 4};  // pf_stats.sta
 static bool schedule_ok(int group, const pf_schedule& s) {
   return s.ctas >= 0 && s.ctas <= (1 << 20) && s.units_per_cta >= 1 && s.units_per_cta <= 16 && s.staging >= 0 &&
          s.staging <= 3 && (s.staging == 0 || s.staging < s.units_per_cta) && s.tile >= 0 &&
-         s.tile <= (group == PF_TUNE_DEBLOCK ? 3 : 0);
+         s.tile <= (group == PF_TUNE_DEBLOCK ? 3 : group == PF_TUNE_FILM_GRAIN ? 2 : 0);
 }
 
 extern "C" int pf_set_schedule(pf_ctx* c, int32_t group, const pf_schedule* s) {
@@ -1830,6 +1863,7 @@ extern "C" int pf_set_schedule(pf_ctx* c, int32_t group, const pf_schedule* s) {
       c->persistent[k] = s->ctas;
       c->chunk[k] = s->units_per_cta;
       c->ahead[k] = s->staging;
+      c->tile[k] = group == PF_TUNE_DEBLOCK ? 0 : s->tile;
     }
   if (group == PF_TUNE_DEBLOCK) c->db_tile = s->tile;
   return PF_OK;
@@ -1841,7 +1875,7 @@ extern "C" int pf_get_schedule(const pf_ctx* c, int32_t group, pf_schedule* s) {
   s->ctas = c->persistent[k];
   s->units_per_cta = c->chunk[k];
   s->staging = c->ahead[k];
-  s->tile = group == PF_TUNE_DEBLOCK ? c->db_tile : 0;
+  s->tile = group == PF_TUNE_DEBLOCK ? c->db_tile : c->tile[k];
   return PF_OK;
 }
 
@@ -1886,12 +1920,11 @@ extern "C" int pf_autotune(pf_ctx* c, const pf_batch_item* items, int32_t n, int
         best = cand;
       }
     };
-    if (gi == PF_TUNE_DEBLOCK)
-      for (int t = 1; t <= 3; t++) {
-        pf_schedule s = best;
-        s.tile = t;
-        tryOne(s);
-      }
+    for (int t = 1; t <= 3; t++) {  // tile settings the group has (schedule_ok)
+      pf_schedule s = best;
+      s.tile = t;
+      tryOne(s);
+    }
     for (int u : {2, 4, 8}) {
       pf_schedule s = best;
       s.units_per_cta = u;

@@ -197,6 +197,7 @@ struct BatchArgs {
   // and how many items ahead of the current one the CTA prefetches into L2.
   int chunk;
   int ahead;
+  int tile;  // the stage's tile setting (pf_schedule.tile; deblocking reads it from the job)
 };
 
 // Deblocking tile shapes (pf_schedule.tile): width x height in 4x4 edge

@@ -249,7 +249,9 @@ __device__ __forceinline__ int blend_w(int prev, int cur, int pw, int cw, int bd
 // every allocated sample of the display frame is written.
 // One column x of up to 4 rows y0.. of one display plane (all inside one
 // 32-row grain block row): per-block values once, then per sample.
-template <typename T>
+// kFgRowGroup: rows of the column whose loads go out together (1, 2 or 4,
+// the grain group's tile setting).
+template <typename T, int kFgRowGroup>
 __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& disp, const FgArgs& a, const uint8_t* lut,
                                              int plane, int x, int y0, int nrows) {
   // Plane descriptors and parameters by value: they live in the job table in
@@ -259,7 +261,17 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
   if (x >= sp.aw) return;
   const int yend = imin(y0 + nrows, sp.ah);
   if (!a.active[plane] || x >= sp.w) {
-    for (int y = y0; y < yend; y++) row_ptr<T>(dp, y)[x] = row_ptr<T>(sp, y)[x];
+    // Loads of a group of rows before its stores (the compiler may not move
+    // a load of the frame above a store to the display frame).
+    for (int yg = y0; yg < yend; yg += kFgRowGroup) {
+      T v[kFgRowGroup];
+#pragma unroll
+      for (int k = 0; k < kFgRowGroup; k++)
+        if (yg + k < yend) v[k] = row_ptr<T>(sp, yg + k)[x];
+#pragma unroll
+      for (int k = 0; k < kFgRowGroup; k++)
+        if (yg + k < yend) row_ptr<T>(dp, yg + k)[x] = v[k];
+    }
     return;
   }
   const int bd = sizeof(T) == 1 ? 8 : ref.bd;  // a constant for 8-bit: the depth shifts fold
@@ -308,40 +320,56 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
   const bool cfl = a.cfl, oddLuma = a.odd_luma;
   const int lumaMult = a.luma_mult[plane] - 128, mult = a.mult[plane] - 128;
   const int offs0 = (a.offset[plane] << (bd - 8)) - (1 << bd);
-  for (int y = y0; y < yend; y++) {
-    const int s = row_ptr<T>(sp, y)[x];
-    if (y >= yclip) {
-      row_ptr<T>(dp, y)[x] = (T)s;
-      continue;
-    }
-    const int yi = y - (row << bhl);
-    int g = gr[(r00 + yi) * kGW + c00];
-    if (left) g = blend_w(gr[(r10 + yi) * kGW + c10], g, hpw, hcw, bd);
-    if (yi < yStart) {
-      int top = gr[(r01 + yi) * kGW + c01];
-      if (left) top = blend_w(gr[(r11 + yi) * kGW + c11], top, hpw, hcw, bd);
-      const int vpw = sy ? 23 : (yi == 1 ? 17 : 27), vcw = sy ? 22 : (yi == 1 ? 27 : 17);
-      g = blend_w(top, g, vpw, vcw, bd);
-    }
-    int idx;
-    if (plane == 0) {
-      idx = s;
-    } else {
-      // chromaScalingIndex (apply.go:501-520) on the un-grained luma.
-      const T* lrow = row_ptr<T>(lp, y << sy);
-      const int lx = x << sx;
-      int avg = lrow[lx];
-      if (sx && !(oddLuma && x == sp.w - 1)) avg = (avg + lrow[lx + 1] + 1) >> 1;
-      if (cfl) {
-        idx = avg;
-      } else {
-        const int combined = avg * lumaMult + s * mult;
-        idx = iclip((combined >> 6) + offs0, 0, (1 << bd) - 1);
+  // Groups of rows: every load of a group (frame sample, grain, co-located
+  // luma) is issued before the group's first store to the display frame.
+  for (int yg = y0; yg < yend; yg += kFgRowGroup) {
+    int sv[kFgRowGroup], gv[kFgRowGroup], lv[kFgRowGroup];
+#pragma unroll
+    for (int k = 0; k < kFgRowGroup; k++) {
+      const int y = yg + k;
+      sv[k] = gv[k] = lv[k] = 0;
+      if (y >= yend) continue;
+      sv[k] = row_ptr<T>(sp, y)[x];
+      if (y >= yclip) continue;
+      const int yi = y - (row << bhl);
+      int g = gr[(r00 + yi) * kGW + c00];
+      if (left) g = blend_w(gr[(r10 + yi) * kGW + c10], g, hpw, hcw, bd);
+      if (yi < yStart) {
+        int top = gr[(r01 + yi) * kGW + c01];
+        if (left) top = blend_w(gr[(r11 + yi) * kGW + c11], top, hpw, hcw, bd);
+        const int vpw = sy ? 23 : (yi == 1 ? 17 : 27), vcw = sy ? 22 : (yi == 1 ? 27 : 17);
+        g = blend_w(top, g, vpw, vcw, bd);
+      }
+      gv[k] = g;
+      if (plane != 0) {
+        // chromaScalingIndex (apply.go:501-520) on the un-grained luma.
+        const T* lrow = row_ptr<T>(lp, y << sy);
+        const int lx = x << sx;
+        int avg = lrow[lx];
+        if (sx && !(oddLuma && x == sp.w - 1)) avg = (avg + lrow[lx + 1] + 1) >> 1;
+        lv[k] = avg;
       }
     }
-    const int scale = scale_lut(lut, idx, bd);
-    const int noise = rpow2(scale * g, shift);
-    row_ptr<T>(dp, y)[x] = (T)iclip(s + noise, minV, maxV);
+#pragma unroll
+    for (int k = 0; k < kFgRowGroup; k++) {
+      const int y = yg + k;
+      if (y >= yend) break;
+      const int s = sv[k];
+      if (y >= yclip) {
+        row_ptr<T>(dp, y)[x] = (T)s;
+        continue;
+      }
+      int idx;
+      if (plane == 0 || cfl) {
+        idx = plane == 0 ? s : lv[k];
+      } else {
+        const int combined = lv[k] * lumaMult + s * mult;
+        idx = iclip((combined >> 6) + offs0, 0, (1 << bd) - 1);
+      }
+      const int scale = scale_lut(lut, idx, bd);
+      const int noise = rpow2(scale * gv[k], shift);
+      row_ptr<T>(dp, y)[x] = (T)iclip(s + noise, minV, maxV);
+    }
   }
 }
 
@@ -399,8 +427,10 @@ __device__ __forceinline__ FgTile fg_locate(const BatchArgs& b, const int* base,
   return FgTile{&J, plane, local % J.fg_tx[plane], local / J.fg_tx[plane]};
 }
 
-template <bool kLoop>
-__global__ void __launch_bounds__(256, 6) k_fg_apply_batch(BatchArgs b) {
+// kGroup rows per load group (fg_apply_col); one row at a time keeps 40
+// registers (6 CTAs per SM), groups of 2 or 4 need 64 (4 CTAs per SM).
+template <bool kLoop, int kGroup>
+__global__ void __launch_bounds__(256, kGroup == 1 ? 6 : 4) k_fg_apply_batch(BatchArgs b) {
   __shared__ uint8_t s_lut[256];
   const int* base = b.base + ST_FG_APPLY * (b.n + 1);
   for_each_item<kLoop>(
@@ -413,9 +443,9 @@ __global__ void __launch_bounds__(256, 6) k_fg_apply_batch(BatchArgs b) {
         const int x = t.tx * 64 + (threadIdx.x & 63);
         const int y0 = t.ty * 64 + (threadIdx.x >> 6) * 16;
         if (J.io.bd == 8)
-          fg_apply_col<uint8_t>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
+          fg_apply_col<uint8_t, kGroup>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
         else
-          fg_apply_col<uint16_t>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
+          fg_apply_col<uint16_t, kGroup>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
         __syncthreads();  // the table is rewritten by the next tile
       },
       [&](int item) {
@@ -506,10 +536,17 @@ cudaError_t launch_fg_offsets_batch(const BatchArgs& b, int total, int grid, cud
 
 cudaError_t launch_fg_apply_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
-  if (batch_loops(b))
-    k_fg_apply_batch<true><<<grid, 256, 0, st>>>(b);
-  else
-    k_fg_apply_batch<false><<<grid, 256, 0, st>>>(b);
+  const bool loop = batch_loops(b);
+  switch (b.tile) {
+    case 1:
+      loop ? k_fg_apply_batch<true, 2><<<grid, 256, 0, st>>>(b) : k_fg_apply_batch<false, 2><<<grid, 256, 0, st>>>(b);
+      break;
+    case 2:
+      loop ? k_fg_apply_batch<true, 4><<<grid, 256, 0, st>>>(b) : k_fg_apply_batch<false, 4><<<grid, 256, 0, st>>>(b);
+      break;
+    default:
+      loop ? k_fg_apply_batch<true, 1><<<grid, 256, 0, st>>>(b) : k_fg_apply_batch<false, 1><<<grid, 256, 0, st>>>(b);
+  }
   return cudaGetLastError();
 }
 

@@ -41,6 +41,8 @@ namespace cg = cooperative_groups;
 
 namespace pf {
 
+constexpr int kLearnedSlices = 4;
+
 __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   __shared__ uint16_t s_in[kSH * kSW];
   __shared__ __align__(16) uint8_t s_src[64 * 64];
@@ -53,11 +55,15 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   __shared__ uint8_t s_list[2][64];  // tested trials, ascending
   __shared__ int s_cnt[2];
   // constrain() of the plane's damping: primary strength k at row k (0..15),
-  // secondary strengths 1, 2, 4 at rows 16..18; entry 256 is a difference of
-  // 0, entries 0 and 512 stand for every difference beyond +/-255.
-  __shared__ int16_t s_tab[19][513];
+  // secondary strengths 1, 2, 4 at rows 16..18; entry kTab0 is a difference
+  // of 0, entries kTab0 -/+ 256 stand for every difference beyond +/-255
+  // (both 0).  A row is a copy of the context's table for its strength and
+  // shift, two entries in, so its 32-bit words stay aligned.
+  constexpr int kTabStride = 520, kTab0 = 257;
+  __shared__ __align__(16) int16_t s_tab[19][kTabStride];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int fb = blockIdx.x;
+  const int slices = a.slices > 1 ? a.slices : 1;
+  const int fb = blockIdx.x / slices, slice = blockIdx.x - fb * slices;
   const int fbr = fb / a.nhfb, fbc = fb - fbr * a.nhfb;
   const int lr = 16 * fbr, lc = 16 * fbc;
   const int nhb = imin(16, a.miCols - lc), nvb = imin(16, a.miRows - lr);
@@ -67,11 +73,11 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   const uint64_t listed = fb_listed(a, fb, lr, lc);
   const int count = a.trials.count;
   if (listed == 0) {
-    if (tid < 64) {
+    if (tid < 64 && slice == 0) {
       m0[tid] = tid < count ? 0 : (uint64_t)kNotATrial;
       m1[tid] = tid < count ? 0 : (uint64_t)kNotATrial;
     }
-    if (tid == 0) a.skip[fb] = 1;
+    if (tid == 0 && slice == 0) a.skip[fb] = 1;
     return;
   }
   const uint64_t listMask = count >= 64 ? ~0ull : (1ull << count) - 1;
@@ -79,11 +85,19 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   const uint64_t mask1 = a.tmask ? a.tmask[2 * fb + 1] : a.trials.uvMask;
   const int ssY = a.trials.ss;
   if (tid == 0) {
-    a.skip[fb] = 0;
-    int c0 = 0, c1 = 0;
+    if (slice == 0) a.skip[fb] = 0;
+    // This slice's share of the tested trials: list positions slice,
+    // slice + slices, ...
+    int c0 = 0, c1 = 0, n0 = 0, n1 = 0;
     for (int g = 0; g < 64; g++) {
-      if ((mask0 >> g) & 1) s_list[0][c0++] = (uint8_t)g;
-      if ((mask1 >> g) & 1) s_list[1][c1++] = (uint8_t)g;
+      if ((mask0 >> g) & 1) {
+        if (n0 % slices == slice) s_list[0][c0++] = (uint8_t)g;
+        n0++;
+      }
+      if ((mask1 >> g) & 1) {
+        if (n1 % slices == slice) s_list[1][c1++] = (uint8_t)g;
+        n1++;
+      }
     }
     s_cnt[0] = c0;
     s_cnt[1] = c1;
@@ -177,12 +191,17 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
     }
     const int bl = 3 - dec;
     const int dmp = pli ? damping - 1 : damping;
-    if (pli < 2)  // chroma planes share one damping
-      for (int i = tid; i < 19 * 513; i += 256) {
-        const int t = i / 513, d = i - t * 513 - 256;
+    if (pli < 2) {  // chroma planes share one damping
+      // Rows of 256 32-bit words (entries -255 .. 256 at kTab0 - 255 ..),
+      // then entry kTab0 - 256 (a difference below -255) set to 0.
+      for (int i = tid; i < 19 * 256; i += 256) {
+        const int t = i >> 8, wd = i & 255;
         const int k = t < 16 ? t : (t == 16 ? 1 : (t == 17 ? 2 : 4));
-        s_tab[t][i - t * 513] = (int16_t)(d < -255 || d > 255 ? 0 : constrain(d, k, constrain_shift(k, dmp)));
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.ctab + (size_t)(k * 8 + constrain_shift(k, dmp)) * 512);
+        reinterpret_cast<uint32_t*>(&s_tab[t][kTab0 - 255])[wd] = src[wd];
       }
+      if (tid < 19) s_tab[tid][kTab0 - 256] = 0;
+    }
     __syncthreads();
     const int ngrp = (h + 7) >> 3;
     const int ntask = s_cnt[P] * ngrp;
@@ -195,7 +214,7 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
       const int pri = packed >> 2;
       int sec = packed & 3;
       if (sec == 3) sec = 4;
-      const int16_t* ts = &s_tab[sec == 1 ? 16 : (sec == 2 ? 17 : 18)][256];
+      const int16_t* ts = &s_tab[sec == 1 ? 16 : (sec == 2 ? 17 : 18)][kTab0];
       uint32_t sse = 0;
       for (int xx = lane; xx < w; xx += 32) {
         for (int yb = grp * 8; yb < imin(grp * 8 + 8, h); yb += 1 << bl) {
@@ -208,7 +227,7 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
           }
           const bool filt = (strength | sec) != 0;
           const int dir = pri != 0 ? s_dir[b] : 0;
-          const int16_t* tp = &s_tab[strength][256];
+          const int16_t* tp = &s_tab[strength][kTab0];
           const int2 po = s_ofs[dir + 2], q0 = s_ofs[dir + 4], q1 = s_ofs[dir];
           for (int yy = yb; yy < yb + (1 << bl); yy += step) {
             // An unfiltered block keeps the reconstruction (cdefDist8 against
@@ -231,12 +250,20 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   }
   __syncthreads();
   if (tid < 64) {
+    // Each entry written once: a tested trial by the slice that measured
+    // it, the rest by slice 0.
+    const uint64_t below = (1ull << tid) - 1;
+    const bool t0 = (mask0 >> tid) & 1, t1 = (mask1 >> tid) & 1;
+    const bool own0 = t0 && __popcll(mask0 & below) % slices == slice;
+    const bool own1 = t1 && __popcll(mask1 & below) % slices == slice;
     if (tid >= count) {
-      m0[tid] = m1[tid] = kNotATrial;
+      if (slice == 0) m0[tid] = m1[tid] = kNotATrial;
     } else {
       // A subsampled luma SSE is scaled back by the row step (searchRow, :722-734).
-      m0[tid] = ((mask0 >> tid) & 1) ? (uint64_t)s_sse[0][tid] * (uint64_t)ssY : (uint64_t)kUntestedMSE;
-      m1[tid] = ((mask1 >> tid) & 1) ? (uint64_t)s_sse[1][tid] : (uint64_t)kUntestedMSE;
+      if (own0) m0[tid] = (uint64_t)s_sse[0][tid] * (uint64_t)ssY;
+      else if (!t0 && slice == 0) m0[tid] = (uint64_t)kUntestedMSE;
+      if (own1) m1[tid] = (uint64_t)s_sse[1][tid];
+      else if (!t1 && slice == 0) m1[tid] = (uint64_t)kUntestedMSE;
     }
   }
 }
@@ -572,7 +599,7 @@ size_t sel_smem_bytes(int nfb, bool rows) {
 }
 
 cudaError_t launch_search(const SearchArgs& a, cudaStream_t st) {
-  k_cdef_search<<<a.nhfb * a.nvfb, 256, 0, st>>>(a);
+  k_cdef_search<<<a.nhfb * a.nvfb * (a.slices > 1 ? a.slices : 1), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -657,6 +684,7 @@ using namespace pf;
 void* pf_internal_search_scratch(pf_ctx* c, size_t bytes);  // pf_api.cu
 void* pf_internal_stream(pf_ctx* c);
 cudaEvent_t* pf_internal_events(pf_ctx* c);  // pf_api.cu: null unless the context times stages
+const int16_t* pf_internal_ctab(pf_ctx* c);  // pf_api.cu
 void* pf_internal_pinned(pf_ctx* c, size_t bytes);
 void* pf_internal_cached_upload(pf_ctx* c, const void* host, size_t bytes, size_t extra, cudaStream_t st,
                                 int* changed);
@@ -820,6 +848,8 @@ static int stage_search(pf_ctx* ctx, const pf_frame* source, const pf_frame* rec
   a.skip = base + oSkip;
   a.dirs = nullptr;
   a.ais = nullptr;
+  a.ctab = pf_internal_ctab(ctx);
+  a.slices = 1;
   level1_trials(&a.trials);
   SelArgs& s = S->s;
   s.mse = a.mse;
@@ -1190,6 +1220,10 @@ extern "C" int pf_cdef_search_learned(pf_ctx* ctx, const pf_frame* source, const
     return PF_ERR_DEVICE;
   if (ev && cudaEventRecord(ev[2], S.st) != cudaSuccess) return PF_ERR_DEVICE;
   S.a.tmask = masks;
+  // A block's tested trials vary from a few to all 64 (a fallback head):
+  // four CTAs share each block's list, so the fallback blocks do not set
+  // the launch's length alone.
+  S.a.slices = kLearnedSlices;
   S.s.refine = (flags & PF_LEARNED_REFINE) ? 1 : 0;
   const int r = search_finish(S, params, mse_out, fb_index_out, result, ev);
   if (r != PF_OK) return r;

@@ -2,6 +2,7 @@
 // (pf_search.cu) and the learned strength selection built on it (pf_mlp.cu).
 #pragma once
 
+#include "pf_cdef_dev.cuh"
 #include "pf_common.cuh"
 
 namespace pf {
@@ -53,6 +54,12 @@ struct SearchArgs {
   uint8_t* dirs;            // [nfb][64]
   int8_t* ais;              // [nfb][64]
   TrialList trials;         // tmask searches use the level-1 list
+  // constrain() tables of the context ([strength 16][shift 8][512], entry
+  // 255 + d for a difference d, entry 511 = 0: CdefArgs.ctab).
+  const int16_t* ctab;
+  // CTAs per filter block: slice s of a block measures the tested trials at
+  // positions s, s + slices, ... of its list (1: one CTA measures them all).
+  int slices;
 };
 
 struct SelOut {
@@ -95,42 +102,27 @@ __device__ __forceinline__ uint64_t fb_listed(const SearchArgs& a, int fb, int l
 }
 
 // cdef/direction.go:37-79 (partial sums) and :469-501 (cost), 8-bit samples
-// read straight from the frame; shared by the search and the features.
+// read straight from the frame or a staged copy; shared by the search and
+// the features.  The samples go in as packed pairs (dir_cost_pairs): two
+// 32-bit loads a row when the rows are 4-byte aligned, bytes otherwise.
 template <int D>
 __device__ __forceinline__ int32_t dir_cost8(const uint8_t* blk, int64_t stride) {
-  int32_t p[15];
+  uint32_t w[8][4];
+  if (((reinterpret_cast<uintptr_t>(blk) | (uintptr_t)stride) & 3) == 0) {
 #pragma unroll
-  for (int k = 0; k < 15; k++) p[k] = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int32_t x = (int32_t)blk[i * stride + j] - 128;
-      if (D == 0) p[i + j] += x;
-      if (D == 1) p[i + (j >> 1)] += x;
-      if (D == 2) p[i] += x;
-      if (D == 3) p[3 + i - (j >> 1)] += x;
-      if (D == 4) p[7 + i - j] += x;
-      if (D == 5) p[3 - (i >> 1) + j] += x;
-      if (D == 6) p[j] += x;
-      if (D == 7) p[(i >> 1) + j] += x;
+    for (int i = 0; i < 8; i++) {
+      const uint32_t* r = reinterpret_cast<const uint32_t*>(blk + i * stride);
+      const uint32_t lo = r[0], hi = r[1];
+      w[i][0] = __byte_perm(lo, 0, 0x4140), w[i][1] = __byte_perm(lo, 0, 0x4342);
+      w[i][2] = __byte_perm(hi, 0, 0x4140), w[i][3] = __byte_perm(hi, 0, 0x4342);
     }
-  }
-  if (D == 2 || D == 6) {
-    int32_t s = 0;
+  } else {
 #pragma unroll
-    for (int i = 0; i < 8; i++) s += p[i] * p[i];
-    return s * 105;
-  }
-  if (D == 0 || D == 4) {
-    const int32_t div[8] = {840, 420, 280, 210, 168, 140, 120, 105};
-    int32_t s = 0;
+    for (int i = 0; i < 8; i++)
 #pragma unroll
-    for (int i = 0; i < 7; i++) s += (p[i] * p[i] + p[14 - i] * p[14 - i]) * div[i];
-    return s + p[7] * p[7] * 105;
+      for (int m = 0; m < 4; m++) w[i][m] = blk[i * stride + 2 * m] | ((uint32_t)blk[i * stride + 2 * m + 1] << 16);
   }
-  return (p[3] * p[3] + p[4] * p[4] + p[5] * p[5] + p[6] * p[6] + p[7] * p[7]) * 105 +
-         (p[0] * p[0] + p[10] * p[10]) * 420 + (p[1] * p[1] + p[9] * p[9]) * 210 + (p[2] * p[2] + p[8] * p[8]) * 140;
+  return dir_cost_pairs<D>(w, 0);
 }
 
 __device__ __forceinline__ int32_t dir_cost8_dev(int d, const uint8_t* blk, int64_t stride) {

@@ -320,12 +320,15 @@ int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats*
  *       staging        how many items ahead of the current one, inside the
  *                      chunk, the CTA prefetches its input rows into L2
  *                      (0..3, below units_per_cta);
- *       tile           the tile shape, deblocking only: 0 = 32x8, 1 = 64x4,
+ *       tile           deblocking: the tile shape, 0 = 32x8, 1 = 64x4,
  *                      2 = 16x16, 3 = 8x32 edge units a tile (one thread
- *                      each); 0 for the other groups.
+ *                      each); grain apply: rows of a column whose loads are
+ *                      issued together, 0 = 1 (40 registers, 6 CTAs per SM),
+ *                      1 = 2, 2 = 4 (64 registers, 4 CTAs per SM); 0 for
+ *                      the other groups.
  *     Work items are independent, so every schedule gives the same samples.
  * pf_autotune searches the schedule of each group on a given batch, one
- * dimension at a time (tile shape, units per CTA, staging depth, persistent
+ * dimension at a time (tile setting, units per CTA, staging depth, persistent
  * CTAs at 0, 1, 2, 4, 8 and 16 per SM), keeping after each the candidate
  * with the lowest median stage time over reps timed runs (one untimed run
  * first), and leaves the winners set on the context.  It runs the batch in
@@ -338,7 +341,7 @@ typedef struct pf_schedule {
   int32_t ctas;           /* persistent CTAs (0 = one CTA per chunk) */
   int32_t units_per_cta;  /* work items per chunk, 1..16 */
   int32_t staging;        /* items prefetched ahead, 0..3 and < units_per_cta */
-  int32_t tile;           /* deblocking tile shape 0..3; 0 for other groups */
+  int32_t tile;           /* deblocking 0..3, grain apply 0..2, else 0 */
 } pf_schedule;
 
 typedef struct pf_tune_result {
