@@ -261,6 +261,10 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
   if (x >= sp.aw) return;
   const int yend = imin(y0 + nrows, sp.ah);
   if (!a.active[plane] || x >= sp.w) {
+    if (kFgRowGroup == 1) {
+      for (int y = y0; y < yend; y++) row_ptr<T>(dp, y)[x] = row_ptr<T>(sp, y)[x];
+      return;
+    }
     // Loads of a group of rows before its stores (the compiler may not move
     // a load of the frame above a store to the display frame).
     for (int yg = y0; yg < yend; yg += kFgRowGroup) {
@@ -320,6 +324,45 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
   const bool cfl = a.cfl, oddLuma = a.odd_luma;
   const int lumaMult = a.luma_mult[plane] - 128, mult = a.mult[plane] - 128;
   const int offs0 = (a.offset[plane] << (bd - 8)) - (1 << bd);
+  if (kFgRowGroup == 1) {
+    // One row at a time (40 registers, 6 CTAs per SM).
+    for (int y = y0; y < yend; y++) {
+      const int s = row_ptr<T>(sp, y)[x];
+      if (y >= yclip) {
+        row_ptr<T>(dp, y)[x] = (T)s;
+        continue;
+      }
+      const int yi = y - (row << bhl);
+      int g = gr[(r00 + yi) * kGW + c00];
+      if (left) g = blend_w(gr[(r10 + yi) * kGW + c10], g, hpw, hcw, bd);
+      if (yi < yStart) {
+        int top = gr[(r01 + yi) * kGW + c01];
+        if (left) top = blend_w(gr[(r11 + yi) * kGW + c11], top, hpw, hcw, bd);
+        const int vpw = sy ? 23 : (yi == 1 ? 17 : 27), vcw = sy ? 22 : (yi == 1 ? 27 : 17);
+        g = blend_w(top, g, vpw, vcw, bd);
+      }
+      int idx;
+      if (plane == 0) {
+        idx = s;
+      } else {
+        // chromaScalingIndex (apply.go:501-520) on the un-grained luma.
+        const T* lrow = row_ptr<T>(lp, y << sy);
+        const int lx = x << sx;
+        int avg = lrow[lx];
+        if (sx && !(oddLuma && x == sp.w - 1)) avg = (avg + lrow[lx + 1] + 1) >> 1;
+        if (cfl) {
+          idx = avg;
+        } else {
+          const int combined = avg * lumaMult + s * mult;
+          idx = iclip((combined >> 6) + offs0, 0, (1 << bd) - 1);
+        }
+      }
+      const int scale = scale_lut(lut, idx, bd);
+      const int noise = rpow2(scale * g, shift);
+      row_ptr<T>(dp, y)[x] = (T)iclip(s + noise, minV, maxV);
+    }
+    return;
+  }
   // Groups of rows: every load of a group (frame sample, grain, co-located
   // luma) is issued before the group's first store to the display frame.
   for (int yg = y0; yg < yend; yg += kFgRowGroup) {
