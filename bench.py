@@ -460,14 +460,13 @@ def measure_issue_peaks():
 # Per-frame counters of the batched chain kernels at the 1080p 8-bit 4:2:0
 # workload, from one ncu capture of a 60-frame launch of each kernel of the
 # current code (profiles/postfilter_chain_counters_1080p8_60frames.md has the
-# command and the raw figures): DRAM bytes read + written, warp instructions
-# executed, and the ALU-pipe share of peak (deblocking: both passes).
+# command and the raw figures): DRAM bytes read + written and warp
+# instructions executed (deblocking: both passes).
 KERNEL_COUNTERS_1080P8 = {
-    "deblock": {"dram_bytes": (222.0e6 + 123.1e6 + 221.9e6 + 52.7e6) / 60, "warp_inst": (303.9e6 + 277.7e6) / 60,
-                "alu_pct": 68.3},
-    "cdef": {"dram_bytes": (187.2e6 + 163.8e6) / 60, "warp_inst": 1244.8e6 / 60, "alu_pct": 65.3},
-    "restoration": {"dram_bytes": (206.7e6 + 152.0e6) / 60, "warp_inst": 1422.0e6 / 60, "alu_pct": 54.2},
-    "film_grain": {"dram_bytes": (190.1e6 + 157.6e6) / 60, "warp_inst": 615.6e6 / 60, "alu_pct": 45.0},
+    "deblock": {"dram_bytes": (443.97e6 + 175.47e6) / 60, "warp_inst": 593.75e6 / 60},
+    "cdef": {"dram_bytes": (187.91e6 + 163.16e6) / 60, "warp_inst": 1122.57e6 / 60},
+    "restoration": {"dram_bytes": (205.90e6 + 152.75e6) / 60, "warp_inst": 928.93e6 / 60},
+    "film_grain": {"dram_bytes": (189.52e6 + 157.82e6) / 60, "warp_inst": 622.57e6 / 60},
 }
 
 
