@@ -193,9 +193,11 @@ def mixed_leg(local, steps, warmup):
             "batched_over_single_stream": ms_s / ms_b,
             "homogeneous_batches_ms_sum": ms_kinds, "mixed_rate_over_homogeneous": ms_kinds / ms_b,
             "algorithmic_gbs": algo_bytes / (ms_b / 1e3) / 1e9,
-            "autotune": {n: dict(tune.chosen[i].as_dict(), ms=round(float(tune.ms[i]), 4),
-                                 ms_default_schedule=round(float(tune.ms_default[i]), 4))
-                         for i, n in enumerate(names)},
+            "autotune": dict({n: dict(tune.chosen[i].as_dict(), ms=round(float(tune.ms[i]), 4),
+                                      ms_default_schedule=round(float(tune.ms_default[i]), 4))
+                              for i, n in enumerate(names)},
+                             frame_groups={"chosen": int(tune.frame_groups),
+                                           "batch_ms": [round(float(v), 4) for v in tune.ms_groups]}),
             "config": "48 frames, seeds 100-147: 16x640x360 8-bit 4:2:0, 16x1280x720 8-bit 4:2:0, "
                       "8x1920x1080 10-bit 4:2:0, 8x1280x720 8-bit 4:4:4, full chain; batched = one pf_batch_apply "
                       "(autotuned schedules, CUDA graph replay), single stream = one call per frame, "
@@ -427,6 +429,7 @@ def stage_times(local, reset, items, reps=3, schedule=None):
     for g, nm in enumerate(["deblock", "cdef", "restoration", "film_grain"]):
         if schedule:
             trunner.set_schedule(g, **{k: schedule[nm][k] for k in ("ctas", "units_per_cta", "staging", "tile")})
+    # (one frame group: per-stage times need the stages in sequence)
     stage = np.zeros(5)
     for k in range(reps + 1):
         reset()
@@ -607,6 +610,8 @@ def main():
         schedule = {nm: dict(tune.chosen[i].as_dict(), ms=round(float(tune.ms[i]), 4),
                              ms_default_schedule=round(float(tune.ms_default[i]), 4))
                     for i, nm in enumerate(["deblock", "cdef", "restoration", "film_grain"])}
+        schedule["frame_groups"] = {"chosen": int(tune.frame_groups),
+                                    "batch_ms": [round(float(v), 4) for v in tune.ms_groups]}
 
     clocks = ClockSampler(local)
     clocks.start()

@@ -61,6 +61,7 @@ def lib():
     L.pf_set_persistent.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
     L.pf_set_schedule.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.pf_schedule)]
     L.pf_get_schedule.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.pf_schedule)]
+    L.pf_set_frame_groups.argtypes = [C.c_void_p, C.c_int32]
     L.pf_autotune.argtypes = [C.c_void_p, C.POINTER(abi.pf_batch_item), C.c_int32, C.c_int32,
                               C.POINTER(abi.pf_tune_result)]
     L.pf_cdef_apply.argtypes = [C.c_void_p, C.POINTER(abi.pf_frame), C.c_void_p, C.POINTER(abi.pf_cdef_search_params),

@@ -271,6 +271,8 @@ class pf_tune_result(C.Structure):
         ("chosen", pf_schedule * PF_TUNE_GROUPS),
         ("ms", C.c_float * PF_TUNE_GROUPS),
         ("ms_default", C.c_float * PF_TUNE_GROUPS),
+        ("frame_groups", C.c_int32),
+        ("ms_groups", C.c_float * 2),
     ]
 
 PF_MLP_FEATURES = 40
@@ -440,6 +442,7 @@ EXPORTED_SYMBOLS = (
     "pf_set_persistent",
     "pf_set_schedule",
     "pf_get_schedule",
+    "pf_set_frame_groups",
     "pf_autotune",
     "pf_lr_search",
     "pf_cdef_apply",

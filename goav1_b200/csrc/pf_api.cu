@@ -135,6 +135,11 @@ struct pf_ctx {
   int ahead[ST_COUNT] = {};
   int tile[ST_COUNT] = {};  // launch-level tile setting (grain apply: rows per load group)
   int db_tile = 0;          // deblocking tile shape (per job: it sets the tile counts)
+  // Frame groups (pf_set_frame_groups): 2 runs the batch's two halves on the
+  // main stream and stream2.
+  int frame_groups = 1;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t gfork = nullptr, gjoin = nullptr;
   // CUDA graphs of pf_batch_apply, one per batch signature (see run_batch).
   int graphs = 0;
   std::vector<struct GraphEntry*> gcache;
@@ -538,6 +543,9 @@ extern "C" pf_ctx* pf_create(const pf_config* cfg, int* status) {
   cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
   cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+  cudaEventCreateWithFlags(&c->gfork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&c->gjoin, cudaEventDisableTiming);
   c->sm_count = prop.multiProcessorCount;
   // The CDEF kernel's constrain() tables, built once on the context's stream
   // (every later launch is ordered after it).
@@ -556,6 +564,7 @@ extern "C" void pf_destroy(pf_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   cudaStreamSynchronize(c->side);
+  if (c->stream2) cudaStreamSynchronize(c->stream2);
   if (c->h2d) cudaStreamSynchronize(c->h2d);
   if (c->d2h) cudaStreamSynchronize(c->d2h);
   DevBuf* bufs[] = {&c->io,     &c->disp,     &c->arena,  &c->sidebuf, &c->jobs,    &c->bases,
@@ -587,6 +596,9 @@ extern "C" void pf_destroy(pf_ctx* c) {
   cudaEventDestroy(c->join);
   if (c->chain_done) cudaEventDestroy(c->chain_done);
   if (c->side_done) cudaEventDestroy(c->side_done);
+  if (c->gfork) cudaEventDestroy(c->gfork);
+  if (c->gjoin) cudaEventDestroy(c->gjoin);
+  if (c->stream2) cudaStreamDestroy(c->stream2);
   cudaStreamDestroy(c->side);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -920,24 +932,40 @@ static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, con
     djobs = c->jobs.p;
     dbases = c->bases.p;
   }
+  // Frame groups: with two, the batch's frames are split where half of its
+  // restoration tiles lie, and each half runs the chain on its own stream,
+  // so one half's stage overlaps the other's (the tail of each launch is
+  // filled by the other stream's CTAs).
+  const int groups = c->frame_groups > 1 && n >= 2 ? 2 : 1;
+  int fmid = n;
+  if (groups == 2) {
+    const int* lrBase = hbase + (size_t)ST_LR * (n + 1);
+    const int half = lrBase[n] / 2;
+    fmid = 1;
+    while (fmid < n - 1 && lrBase[fmid] < half) fmid++;
+  }
   bool persistent = false;
   for (int k = 0; k < ST_COUNT; k++) persistent |= c->persistent[k] > 0;
-  if (persistent) CK(cudaMemsetAsync(c->counters.p, 0, sizeof(int) * ST_COUNT, st));
+  if (persistent) CK(cudaMemsetAsync(c->counters.p, 0, sizeof(int) * ST_COUNT * groups, st));
   BatchArgs b;
   b.jobs = (const FrameJob*)djobs;
   b.base = (const int*)dbases;
   b.n = n;
-  auto total = [&](int k) { return hbase[(size_t)k * (n + 1) + n]; };
-  auto args = [&](int k, int* grid) {
+  auto count = [&](int k, int f0, int f1) {
+    return hbase[(size_t)k * (n + 1) + f1] - hbase[(size_t)k * (n + 1) + f0];
+  };
+  auto args = [&](int k, int f0, int f1, int grp, int* grid) {
     BatchArgs a = b;
-    const int t = total(k);
+    a.f0 = f0;
+    a.f1 = f1;
+    const int t = count(k, f0, f1);
     a.chunk = c->chunk[k];
     a.ahead = c->ahead[k];
     a.tile = c->tile[k];
     const int chunks = (t + a.chunk - 1) / a.chunk;
     if (c->persistent[k] > 0 && chunks > c->persistent[k]) {
       *grid = c->persistent[k];
-      a.counters = (int*)c->counters.p;
+      a.counters = (int*)c->counters.p + grp * ST_COUNT;
     } else {
       *grid = chunks;
       a.counters = nullptr;
@@ -949,31 +977,48 @@ static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, con
   if (fg) {
     CK(cudaEventRecord(c->fork, st));
     CK(cudaStreamWaitEvent(c->side, c->fork, 0));
-    BatchArgs a = args(ST_FG_TEMPLATES, &g);
-    CK(launch_fg_templates_batch(a, total(ST_FG_TEMPLATES), g, c->side));
-    a = args(ST_FG_OFFSETS, &g);
-    CK(launch_fg_offsets_batch(a, total(ST_FG_OFFSETS), g, c->side));
+    BatchArgs a = args(ST_FG_TEMPLATES, 0, n, 0, &g);
+    CK(launch_fg_templates_batch(a, count(ST_FG_TEMPLATES, 0, n), g, c->side));
+    a = args(ST_FG_OFFSETS, 0, n, 0, &g);
+    CK(launch_fg_offsets_batch(a, count(ST_FG_OFFSETS, 0, n), g, c->side));
     CK(cudaEventRecord(c->join, c->side));
   }
+  // Stage events: per stage with one group; with two only the whole batch
+  // is timed (it reads as the deblocking stage's time, the others as zero).
+  const bool stageEv = c->timing && groups == 1;
   if (c->timing) CK(cudaEventRecord(c->ev[0], st));
-  BatchArgs a = args(ST_DEBLOCK_V, &g);
-  CK(launch_deblock_batch(a, total(ST_DEBLOCK_V), g, 0, st));
-  a = args(ST_DEBLOCK_H, &g);
-  CK(launch_deblock_batch(a, total(ST_DEBLOCK_H), g, 1, st));
-  if (c->timing) CK(cudaEventRecord(c->ev[1], st));
-  a = args(ST_CDEF, &g);
-  CK(launch_cdef_batch(a, total(ST_CDEF), g, st));
-  if (c->timing) CK(cudaEventRecord(c->ev[2], st));
-  a = args(ST_LR, &g);
-  CK(launch_lr_batch(a, total(ST_LR), g, st));
-  if (c->timing) CK(cudaEventRecord(c->ev[3], st));
-  a = args(ST_EXTEND, &g);
-  CK(launch_extend_batch(a, total(ST_EXTEND), g, st));
-  if (c->timing) CK(cudaEventRecord(c->ev[4], st));
-  if (c->mark_chain) CK(cudaEventRecord(c->chain_done, st));
-  if (fg) CK(cudaStreamWaitEvent(st, c->join, 0));
-  a = args(ST_FG_APPLY, &g);
-  CK(launch_fg_apply_batch(a, total(ST_FG_APPLY), g, st));
+  if (groups == 2) {
+    CK(cudaEventRecord(c->gfork, st));
+    CK(cudaStreamWaitEvent(c->stream2, c->gfork, 0));
+  }
+  for (int gi = 0; gi < groups; gi++) {
+    const cudaStream_t gs = gi ? c->stream2 : st;
+    const int f0 = gi ? fmid : 0, f1 = groups == 2 && gi == 0 ? fmid : n;
+    BatchArgs a = args(ST_DEBLOCK_V, f0, f1, gi, &g);
+    CK(launch_deblock_batch(a, count(ST_DEBLOCK_V, f0, f1), g, 0, gs));
+    a = args(ST_DEBLOCK_H, f0, f1, gi, &g);
+    CK(launch_deblock_batch(a, count(ST_DEBLOCK_H, f0, f1), g, 1, gs));
+    if (stageEv) CK(cudaEventRecord(c->ev[1], gs));
+    a = args(ST_CDEF, f0, f1, gi, &g);
+    CK(launch_cdef_batch(a, count(ST_CDEF, f0, f1), g, gs));
+    if (stageEv) CK(cudaEventRecord(c->ev[2], gs));
+    a = args(ST_LR, f0, f1, gi, &g);
+    CK(launch_lr_batch(a, count(ST_LR, f0, f1), g, gs));
+    if (stageEv) CK(cudaEventRecord(c->ev[3], gs));
+    a = args(ST_EXTEND, f0, f1, gi, &g);
+    CK(launch_extend_batch(a, count(ST_EXTEND, f0, f1), g, gs));
+    if (stageEv) CK(cudaEventRecord(c->ev[4], gs));
+    if (c->mark_chain && gi == 0) CK(cudaEventRecord(c->chain_done, gs));
+    if (fg) CK(cudaStreamWaitEvent(gs, c->join, 0));
+    a = args(ST_FG_APPLY, f0, f1, gi, &g);
+    CK(launch_fg_apply_batch(a, count(ST_FG_APPLY, f0, f1), g, gs));
+  }
+  if (groups == 2) {
+    CK(cudaEventRecord(c->gjoin, c->stream2));
+    CK(cudaStreamWaitEvent(st, c->gjoin, 0));
+    if (c->timing)
+      for (int i = 1; i < 5; i++) CK(cudaEventRecord(c->ev[i], st));  // after ev[0]: zero-length stages
+  }
   if (c->timing) CK(cudaEventRecord(c->ev[5], st));
   return PF_OK;
 }
@@ -994,6 +1039,7 @@ static std::vector<int64_t> batch_key(const pf_ctx* c, int n, bool fg) {
     k.push_back(c->tile[i]);
   }
   k.push_back(c->db_tile);
+  k.push_back(c->frame_groups);
   for (int v : c->hbase) k.push_back(v);
   return k;
 }
@@ -1090,7 +1136,7 @@ static int prepare_batch(pf_ctx* c, const FrameRef* refs, int n, Bytes& hs, DevB
   }
   CK(c->jobs.ensure(sizeof(FrameJob) * n));
   CK(c->bases.ensure(sizeof(int) * c->hbase.size()));
-  CK(c->counters.ensure(sizeof(int) * ST_COUNT));
+  CK(c->counters.ensure(sizeof(int) * ST_COUNT * 2));  // one set per frame group
   *fg = c->hbase[(size_t)ST_FG_TEMPLATES * (n + 1) + n] > 0;
   *completed = done;
   return PF_OK;
@@ -1879,6 +1925,12 @@ extern "C" int pf_get_schedule(const pf_ctx* c, int32_t group, pf_schedule* s) {
   return PF_OK;
 }
 
+extern "C" int pf_set_frame_groups(pf_ctx* c, int32_t groups) {
+  if (!c || (groups != 1 && groups != 2)) return PF_ERR_INVALID_ARG;
+  c->frame_groups = groups;
+  return PF_OK;
+}
+
 extern "C" int pf_set_persistent(pf_ctx* c, int32_t group, int32_t ctas) {
   if (!c || group < 0 || group >= PF_TUNE_GROUPS || ctas < 0 || ctas > (1 << 20)) return PF_ERR_INVALID_ARG;
   for (int k : kTuneStages[group])
@@ -1890,6 +1942,7 @@ extern "C" int pf_autotune(pf_ctx* c, const pf_batch_item* items, int32_t n, int
   if (!c || !items || n <= 0 || reps <= 0 || reps > 1000 || !out) return PF_ERR_INVALID_ARG;
   const int savedTiming = c->timing;
   c->timing = 1;  // per-stage CUDA events; no graphs while timing
+  c->frame_groups = 1;  // per-stage times need one group
   memset(out, 0, sizeof(*out));
   int status = PF_OK;
   // Median stage time of group gi under schedule s.
@@ -1946,6 +1999,23 @@ extern "C" int pf_autotune(pf_ctx* c, const pf_batch_item* items, int32_t n, int
     out->chosen[gi] = best;
     out->ms[gi] = bestMs;
   }
+  // Frame groups last, on the whole batch's time.
+  for (int groups = 1; groups <= 2 && status == PF_OK; groups++) {
+    c->frame_groups = groups;
+    std::vector<float> t;
+    for (int r = 0; r <= reps && status == PF_OK; r++) {
+      pf_stats st;
+      status = pf_batch_apply(c, items, n, &st);
+      float sum = 0.f;
+      for (int i = 0; i < 5; i++) sum += st.stage_ms[i];
+      if (r > 0 && status == PF_OK) t.push_back(sum);
+    }
+    if (status != PF_OK) break;
+    std::sort(t.begin(), t.end());
+    out->ms_groups[groups - 1] = t[t.size() / 2];
+  }
+  c->frame_groups = out->ms_groups[1] < out->ms_groups[0] ? 2 : 1;
+  out->frame_groups = c->frame_groups;
   c->timing = savedTiming;
   return status;
 }

@@ -293,17 +293,21 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
           const int b = k * SHs - off;
           if (b >= Hc) break;
           const int ya = imax(unitY, b - 2), yb = imin(yEnd - 1, b + 1);
-          for (int i = tid; i < (yb - ya + 1) * unitW; i += 256) {
-            const int y = ya + i / unitW, x = unitX + i % unitW;
-            if (x >= Wc) continue;
+          // At most 4 rows of at most 64 samples: one sample per thread,
+          // from the staged unit when this plane was staged (the rows lie
+          // inside the unit, so they are frame samples there too).
+          const int r = tid >> (6 - xdec), c = tid & (uwMax - 1);
+          const int y = ya + r, x = unitX + c;
+          if (y <= yb && c < unitW && x < Wc) {
             const int j = y - (b - 2);
-            const T v = row_ptr<T>(ip, y)[x];
+            const T v = active ? (T)s_in[(y - unitY + 2) * kSW + 8 + c] : row_ptr<T>(ip, y)[x];
             reinterpret_cast<T*>(a.lines[plane] + (int64_t)(k * 4 + j) * a.line_stride[plane])[x] = v;
             if (j == 2 && b + 1 >= Hc)
               reinterpret_cast<T*>(a.lines[plane] + (int64_t)(k * 4 + 3) * a.line_stride[plane])[x] = v;
           }
         }
       }
+      if (active) __syncthreads();  // the next plane restages s_in
     }
   }
 }
@@ -314,7 +318,7 @@ __global__ void __launch_bounds__(256, 4) k_cdef_batch(BatchArgs b) {
   __shared__ CdefSmem sm;
   const int* base = b.base + ST_CDEF * (b.n + 1);
   for_each_item<kLoop>(
-      b, ST_CDEF, base[b.n],
+      b, ST_CDEF,
       [&](int item) {
         const int fi = find_frame(base, b.n, item);
         const FrameJob& J = b.jobs[fi];

@@ -198,6 +198,9 @@ struct BatchArgs {
   int chunk;
   int ahead;
   int tile;  // the stage's tile setting (pf_schedule.tile; deblocking reads it from the job)
+  // The frames [f0, f1) this launch covers (a frame group of the batch;
+  // items base[f0] .. base[f1] - 1 of each stage).
+  int f0, f1;
 };
 
 // Deblocking tile shapes (pf_schedule.tile): width x height in 4x4 edge
@@ -246,21 +249,25 @@ __device__ __forceinline__ int find_frame(const int* base, int n, int item) {
 // choice when the stage has no chunks and no persistent CTAs), which keeps
 // the loop's bookkeeping out of the kernel's register allocation.
 template <bool kLoop = true, typename F, typename P>
-__device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, int total, F f, P prefetch) {
+__device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, F f, P prefetch) {
+  const int* base = b.base + stage * (b.n + 1);
+  const int lo = __ldg(&base[b.f0]), total = __ldg(&base[b.f1]);
   const int chunk = b.chunk > 1 ? b.chunk : 1;
   int* counter = b.counters ? b.counters + stage : nullptr;
   if (!kLoop || (counter == nullptr && chunk == 1)) {
-    if ((int)blockIdx.x < total) f((int)blockIdx.x);
+    if (lo + (int)blockIdx.x < total) f(lo + (int)blockIdx.x);
     return;
   }
-  // Next item, end of the chunk, first item of the chunk, total, chunk.
-  __shared__ int s_pos[5];
+  // Next item, end of the chunk, first item of the chunk, end of the
+  // range, chunk, start of the range.
+  __shared__ int s_pos[6];
   if (threadIdx.x == 0) {
-    const int first = counter ? atomicAdd(counter, chunk) : (int)blockIdx.x * chunk;
+    const int first = lo + (counter ? atomicAdd(counter, chunk) : (int)blockIdx.x * chunk);
     s_pos[0] = s_pos[2] = first;
     s_pos[1] = first + chunk < total ? first + chunk : total;
     s_pos[3] = total;
     s_pos[4] = chunk;
+    s_pos[5] = lo;
   }
   __syncthreads();
   for (;;) {
@@ -271,7 +278,7 @@ __device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, int
       __syncthreads();
       if (threadIdx.x == 0) {
         const int n = s_pos[3], c = s_pos[4];
-        const int first = atomicAdd(b.counters + stage, c);
+        const int first = s_pos[5] + atomicAdd(b.counters + stage, c);
         s_pos[0] = s_pos[2] = first;
         s_pos[1] = first + c < n ? first + c : n;
       }
@@ -294,9 +301,9 @@ __device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, int
 }
 
 template <bool kLoop = true, typename F>
-__device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, int total, F f) {
+__device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, F f) {
   auto none = [](int) {};
-  for_each_item<kLoop>(b, stage, total, f, none);
+  for_each_item<kLoop>(b, stage, f, none);
 }
 
 // Whether a launch needs the looping form of for_each_item.

@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(256, 4) k_deblock_batch(BatchArgs b, int dir) 
   const int stage = dir == 0 ? ST_DEBLOCK_V : ST_DEBLOCK_H;
   const int* base = b.base + stage * (b.n + 1);
   for_each_item<kLoop>(
-      b, stage, base[b.n],
+      b, stage,
       [&](int item) {
         const DbTile t = db_locate(b, base, item);
         const FrameJob& J = *t.J;

@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(kFgTemplateThreads) k_fg_templates_batch(Batch
   __shared__ int16_t s_g[3][kGW * kGH];
   __shared__ int16_t s_gl[kGW * kGH];  // Gaussian sequence, then the luma term
   const int* base = b.base + ST_FG_TEMPLATES * (b.n + 1);
-  for_each_item(b, ST_FG_TEMPLATES, base[b.n], [&](int item) {
+  for_each_item(b, ST_FG_TEMPLATES, [&](int item) {
     const FrameJob& J = b.jobs[find_frame(base, b.n, item)];
     fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], s_g, s_gl);
   });
@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(kFgTemplateThreads) k_fg_templates_batch(Batch
 
 __global__ void __launch_bounds__(64) k_fg_offsets_batch(BatchArgs b) {
   const int* base = b.base + ST_FG_OFFSETS * (b.n + 1);
-  for_each_item(b, ST_FG_OFFSETS, base[b.n], [&](int item) {
+  for_each_item(b, ST_FG_OFFSETS, [&](int item) {
     const int fi = find_frame(base, b.n, item);
     const FrameJob& J = b.jobs[fi];
     const int r = (item - base[fi]) * 64 + threadIdx.x;
@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(256, kGroup == 1 ? 6 : 4) k_fg_apply_batch(Bat
   __shared__ uint8_t s_lut[256];
   const int* base = b.base + ST_FG_APPLY * (b.n + 1);
   for_each_item<kLoop>(
-      b, ST_FG_APPLY, base[b.n],
+      b, ST_FG_APPLY,
       [&](int item) {
         const FgTile t = fg_locate(b, base, item);
         const FrameJob& J = *t.J;
@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(256, kGroup == 1 ? 6 : 4) k_fg_apply_batch(Bat
 // then of the bottom strip [0, aw) x [h, ah), per plane.
 __global__ void __launch_bounds__(256) k_extend_batch(BatchArgs b) {
   const int* base = b.base + ST_EXTEND * (b.n + 1);
-  for_each_item(b, ST_EXTEND, base[b.n], [&](int item) {
+  for_each_item(b, ST_EXTEND, [&](int item) {
     const int fi = find_frame(base, b.n, item);
     const FrameJob& J = b.jobs[fi];
     int local = item - base[fi];

@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(256, 4) k_lr_batch(BatchArgs b) {
   LrSmem& sm = *reinterpret_cast<LrSmem*>(lr_smem_raw);
   const int* base = b.base + ST_LR * (b.n + 1);
   for_each_item<kLoop>(
-      b, ST_LR, base[b.n],
+      b, ST_LR,
       [&](int item) {
         const LrTile t = lr_locate(b, base, item);
         const FrameJob& J = *t.J;

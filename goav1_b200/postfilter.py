@@ -146,6 +146,10 @@ class PostFilterRunner:
         s = abi.pf_schedule(ctas, units_per_cta, staging, tile)
         check(lib().pf_set_schedule(self._h, group, C.byref(s)))
 
+    def set_frame_groups(self, groups):
+        """1 or 2 frame groups per batch (two halves on two streams)."""
+        check(lib().pf_set_frame_groups(self._h, groups))
+
     def get_schedule(self, group):
         s = abi.pf_schedule()
         check(lib().pf_get_schedule(self._h, group, C.byref(s)))

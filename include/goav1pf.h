@@ -331,7 +331,8 @@ int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats*
  * dimension at a time (tile setting, units per CTA, staging depth, persistent
  * CTAs at 0, 1, 2, 4, 8 and 16 per SM), keeping after each the candidate
  * with the lowest median stage time over reps timed runs (one untimed run
- * first), and leaves the winners set on the context.  It runs the batch in
+ * first), then the frame-group count (1 or 2) by the whole batch's median
+ * time, and leaves the winners set on the context.  It runs the batch in
  * place, so pass frames whose contents may be overwritten (copies).
  * out->ms_default is each group's time with the default schedule
  * {0, 1, 0, 0}. */
@@ -348,6 +349,8 @@ typedef struct pf_tune_result {
   pf_schedule chosen[PF_TUNE_GROUPS];  /* the schedule left set per group */
   float ms[PF_TUNE_GROUPS];            /* its median stage time */
   float ms_default[PF_TUNE_GROUPS];    /* the default schedule's */
+  int32_t frame_groups;                /* the frame-group count left set (1 or 2) */
+  float ms_groups[2];                  /* median batch time with 1 and 2 groups */
 } pf_tune_result;
 
 int pf_batch_graphs(pf_ctx* ctx, int32_t enable);
@@ -356,6 +359,12 @@ int pf_batch_graphs(pf_ctx* ctx, int32_t enable);
 int pf_set_schedule(pf_ctx* ctx, int32_t group, const pf_schedule* schedule);
 int pf_get_schedule(const pf_ctx* ctx, int32_t group, pf_schedule* schedule);
 int pf_set_persistent(pf_ctx* ctx, int32_t group, int32_t ctas);
+/* Frame groups: 2 splits each batch where half of its restoration tiles lie
+ * and runs the two halves' chains on two streams, so each half's launches
+ * overlap the other's tails; 1 (the default) runs the batch as one group.
+ * The output is the same either way.  With 2, a context that times stages
+ * reports the whole batch as stage_ms[0] (the other stages 0). */
+int pf_set_frame_groups(pf_ctx* ctx, int32_t groups);
 int pf_autotune(pf_ctx* ctx, const pf_batch_item* items, int32_t n, int32_t reps,
                 pf_tune_result* out);
 

@@ -119,6 +119,26 @@ def test_schedules_match_oracle(frames, expected, sched):
     r.close()
 
 
+@pytest.mark.parametrize("graphs", [False, True])
+def test_frame_groups_match_oracle(frames, expected, graphs):
+    """Two frame groups on two streams, with persistent CTAs and chunks on
+    some stages, plain and captured as a graph (two runs: capture, replay)."""
+    from goav1_b200.postfilter import PostFilterRunner
+
+    r = PostFilterRunner()
+    r.set_frame_groups(2)
+    r.set_schedule(abi.PF_TUNE_CDEF, ctas=148, units_per_cta=2)
+    r.set_schedule(abi.PF_TUNE_RESTORATION, units_per_cta=4, staging=1)
+    r.batch_graphs(graphs)
+    b = Batch(frames)
+    for run in range(2 if graphs else 1):
+        b.reset()
+        r.apply_batch(b.items)
+        r.sync()
+        assert_batch(b, expected, "frame groups run %d" % run)
+    r.close()
+
+
 def test_autotune_then_graphs_match_oracle(frames, expected):
     from goav1_b200.postfilter import PostFilterRunner
 
@@ -132,6 +152,7 @@ def test_autotune_then_graphs_match_oracle(frames, expected):
         assert r.get_schedule(g).as_dict() == c.as_dict()
     assert all(m > 0 for m in res.ms)
     assert all(m <= d for m, d in zip(res.ms, res.ms_default))
+    assert res.frame_groups in (1, 2) and all(m > 0 for m in res.ms_groups)
     r.batch_graphs(True)
     b = Batch(frames)
     for run in range(2):
@@ -152,6 +173,9 @@ def test_scheduling_arguments_are_checked():
         r.set_persistent(0, -1)
     with pytest.raises(ErrInvalidArgument):
         r.batch_graphs(2)
+    for bad in (0, 3, -1):
+        with pytest.raises(ErrInvalidArgument):
+            r.set_frame_groups(bad)
     for g, kw in ((abi.PF_TUNE_CDEF, dict(tile=1)), (abi.PF_TUNE_FILM_GRAIN, dict(tile=3)), (0, dict(tile=4)),
                   (0, dict(units_per_cta=0)),
                   (0, dict(units_per_cta=17)), (0, dict(staging=1)), (0, dict(units_per_cta=2, staging=2)),
