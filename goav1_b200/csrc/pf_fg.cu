@@ -52,15 +52,24 @@ __device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
 // (the averaged luma grain at each chroma position, filled before the
 // recursion).  A lane outside the AR columns passes the template's value
 // through unchanged, so the rows above always hold the template as it
-// stands.  Bands run one after the other, each only as long as its own rows
-// need.  LAG is a template argument (coefficients in registers, unrolled
-// taps).
+// stands.  The (up to three) bands run in the same loop, band b + 1 a fixed
+// number of steps behind band b, far enough that every row it reads from
+// band b was written at an earlier step: one warp then carries two or three
+// independent wavefronts at once, which fills the issue slots a single
+// wavefront's dependent chain leaves empty.  LAG is a template argument
+// (coefficients in registers, unrolled taps).
 constexpr int kFgTemplateThreads = 96;
 
 template <int LAG>
 __device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
   constexpr int kTaps = 2 * LAG * (LAG + 1);  // causal neighbours before the centre
   constexpr int W = 2 * LAG + 1;
+  // Band b + 1 runs kOff steps behind band b: its lane 0 needs band b's
+  // lane 31 (4 * 31 steps behind band b's lane 0) at column x + LAG, so
+  // kOff > LAG + 124; a multiple of W, so that every band's partial sums
+  // rotate in step.
+  constexpr int kOff = W * ((LAG + 125 + W - 1) / W);
+  constexpr int kBands = 3;  // up to 70 AR rows (3 .. 72) in bands of 32
   const int lane = threadIdx.x & 31;
   const int cs = p.coeff_shift, ro = 1 << (cs - 1);
   const int gmin = -(1 << (p.bd - 1)), gmax = (1 << (p.bd - 1)) - 1;
@@ -68,21 +77,29 @@ __device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, 
 #pragma unroll
   for (int i = 0; i <= kTaps; i++) co[i] = p.coeffs[plane][i];
   const int coL = lt ? co[kTaps] : 0;
-  for (int y0 = 3; y0 < h; y0 += 32) {
-    const int rows = imin(32, h - y0);
-    const int y = y0 + lane;
-    const bool row = lane < rows;
-    int acc[W];
+  const int nb = (h - 3 + 31) >> 5;
+  int acc[kBands][W];
+  int tendB[kBands];
+  int tEnd = 0;
 #pragma unroll
-    for (int j = 0; j < W; j++) acc[j] = 0;
+  for (int s = 0; s < kBands; s++) {
+#pragma unroll
+    for (int j = 0; j < W; j++) acc[s][j] = 0;
     // The first step brings column 0 of the rows above into the sums; the
     // last one finishes column w - 4 of the band's last row.
-    const int tend = 4 * (rows - 1) + w - 3;
-    for (int t0 = -LAG; t0 < tend; t0 += W) {
+    const int rows = imin(32, h - 3 - 32 * s);
+    tendB[s] = s < nb ? 4 * (rows - 1) + w - 3 : -LAG;
+    if (s < nb) tEnd = imax(tEnd, kOff * s + tendB[s]);
+  }
+  for (int t0 = -LAG; t0 < tEnd; t0 += W) {
 #pragma unroll
-      for (int k = 0; k < W; k++) {
-        const int t = t0 + k;
-        if (t < tend) {
+    for (int k = 0; k < W; k++) {
+#pragma unroll
+      for (int s = 0; s < kBands; s++) {
+        const int t = t0 + k - kOff * s;
+        if (t >= -LAG && t < tendB[s]) {
+          const int y = 3 + 32 * s + lane;
+          const bool row = y < h;
           const int x = t - 4 * lane;
           const int xn = x + LAG;  // the column entering the sums
           const bool inCol = row && x >= 0 && x < w;
@@ -94,12 +111,12 @@ __device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, 
             for (int d = LAG; d >= 1; d--) {
               const int v = g[(y - d) * kGW + xn];
 #pragma unroll
-              for (int j = W - 1; j >= 0; j--) acc[(j + k) % W] += co[(LAG - d) * W + 2 * LAG - j] * v;
+              for (int j = W - 1; j >= 0; j--) acc[s][(j + k) % W] += co[(LAG - d) * W + 2 * LAG - j] * v;
             }
           }
           int out = g0;
           if (inCol && x >= 3 && x < w - 3) {
-            int sum = acc[k % W];
+            int sum = acc[s][k % W];
             if (lt) sum += lt[y * kGW + x] * coL;
             out = iclip(g0 + ((sum + ro) >> cs), gmin, gmax);
             g[y * kGW + x] = (int16_t)out;
@@ -107,11 +124,11 @@ __device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, 
           // Output x's in-row products for columns x + 1 .. x + LAG; its
           // slot then serves column x + W.
 #pragma unroll
-          for (int m = 1; m <= LAG; m++) acc[(m + k) % W] += co[LAG * W + LAG - m] * out;
-          acc[k % W] = 0;
+          for (int m = 1; m <= LAG; m++) acc[s][(m + k) % W] += co[LAG * W + LAG - m] * out;
+          acc[s][k % W] = 0;
         }
-        __syncwarp();
       }
+      __syncwarp();
     }
   }
 }
