@@ -951,6 +951,7 @@ static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, con
   b.jobs = (const FrameJob*)djobs;
   b.base = (const int*)dbases;
   b.n = n;
+  b.wave = 0;
   auto count = [&](int k, int f0, int f1) {
     return hbase[(size_t)k * (n + 1) + f1] - hbase[(size_t)k * (n + 1) + f0];
   };
@@ -1898,7 +1899,7 @@ static const int kTuneStatIndex[PF_TUNE_GROUPS] = {0, 1, 2, 4};  // pf_stats.sta
 
 static bool schedule_ok(int group, const pf_schedule& s) {
   return s.ctas >= 0 && s.ctas <= (1 << 20) && s.units_per_cta >= 1 && s.units_per_cta <= 16 && s.staging >= 0 &&
-         s.staging <= 3 && (s.staging == 0 || s.staging < s.units_per_cta) && s.tile >= 0 &&
+         s.staging <= 3 && (s.units_per_cta == 1 || s.staging < s.units_per_cta) && s.tile >= 0 &&
          s.tile <= (group == PF_TUNE_DEBLOCK ? 3 : group == PF_TUNE_FILM_GRAIN ? 2 : 0);
 }
 
@@ -1984,7 +1985,7 @@ extern "C" int pf_autotune(pf_ctx* c, const pf_batch_item* items, int32_t n, int
       s.staging = 0;
       tryOne(s);
     }
-    for (int d = 1; d <= 2; d++) {
+    for (int d = 1; d <= 2; d++) {  // items (one per CTA: waves) prefetched ahead
       pf_schedule s = best;
       s.staging = d;
       tryOne(s);

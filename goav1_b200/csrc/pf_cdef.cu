@@ -362,10 +362,11 @@ cudaError_t launch_cdef_tables(int16_t* dst, cudaStream_t st) {
 
 cudaError_t launch_cdef_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
+  static int wave = 0;
   if (batch_loops(b))
     k_cdef_batch<true><<<grid, 256, 0, st>>>(b);
   else
-    k_cdef_batch<false><<<grid, 256, 0, st>>>(b);
+    k_cdef_batch<false><<<grid, 256, 0, st>>>(with_wave(b, k_cdef_batch<false>, 256, 0, wave));
   return cudaGetLastError();
 }
 

@@ -201,6 +201,9 @@ struct BatchArgs {
   // The frames [f0, f1) this launch covers (a frame group of the batch;
   // items base[f0] .. base[f1] - 1 of each stage).
   int f0, f1;
+  // CTAs of this launch resident at once (SMs x CTAs per SM): with one item
+  // per CTA, `ahead` counts in these waves.
+  int wave;
 };
 
 // Deblocking tile shapes (pf_schedule.tile): width x height in 4x4 edge
@@ -255,7 +258,14 @@ __device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, F f
   const int chunk = b.chunk > 1 ? b.chunk : 1;
   int* counter = b.counters ? b.counters + stage : nullptr;
   if (!kLoop || (counter == nullptr && chunk == 1)) {
-    if (lo + (int)blockIdx.x < total) f(lo + (int)blockIdx.x);
+    // One item per CTA: the item `ahead` waves on, which a CTA starting
+    // about when this one ends will take, is prefetched first.
+    const int it = lo + (int)blockIdx.x;
+    if (b.ahead > 0) {
+      const int next = it + b.ahead * b.wave;
+      if (next < total) prefetch(next);
+    }
+    if (it < total) f(it);
     return;
   }
   // Next item, end of the chunk, first item of the chunk, end of the
@@ -308,5 +318,31 @@ __device__ __forceinline__ void for_each_item(const BatchArgs& b, int stage, F f
 
 // Whether a launch needs the looping form of for_each_item.
 inline bool batch_loops(const BatchArgs& b) { return b.counters != nullptr || b.chunk > 1; }
+
+// CTAs of `kernel` the current device holds at once (SMs x CTAs per SM at
+// `threads` threads and `smem` dynamic shared bytes): a launch's wave.
+template <class K>
+inline int resident_ctas(K kernel, int threads, size_t smem) {
+  int occ = 0, dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1) {
+    (void)cudaGetLastError();
+    occ = 1;
+  }
+  return occ * (sms > 0 ? sms : 1);
+}
+
+// The launch arguments with `wave` filled in when the one-item-per-CTA form
+// prefetches waves ahead (the count is settled once per kernel).
+template <class K>
+inline BatchArgs with_wave(const BatchArgs& b, K kernel, int threads, size_t smem, int& cached) {
+  BatchArgs a = b;
+  if (a.ahead > 0 && !batch_loops(a)) {
+    if (!cached) cached = resident_ctas(kernel, threads, smem);
+    a.wave = cached;
+  }
+  return a;
+}
 
 }  // namespace pf

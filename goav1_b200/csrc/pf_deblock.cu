@@ -310,10 +310,11 @@ __global__ void __launch_bounds__(256, 4) k_deblock_batch(BatchArgs b, int dir) 
 
 cudaError_t launch_deblock_batch(const BatchArgs& b, int total, int grid, int dir, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
+  static int wave = 0;
   if (batch_loops(b))
     k_deblock_batch<true><<<grid, 256, 0, st>>>(b, dir);
   else
-    k_deblock_batch<false><<<grid, 256, 0, st>>>(b, dir);
+    k_deblock_batch<false><<<grid, 256, 0, st>>>(with_wave(b, k_deblock_batch<false>, 256, 0, wave), dir);
   return cudaGetLastError();
 }
 

@@ -52,24 +52,15 @@ __device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
 // (the averaged luma grain at each chroma position, filled before the
 // recursion).  A lane outside the AR columns passes the template's value
 // through unchanged, so the rows above always hold the template as it
-// stands.  The (up to three) bands run in the same loop, band b + 1 a fixed
-// number of steps behind band b, far enough that every row it reads from
-// band b was written at an earlier step: one warp then carries two or three
-// independent wavefronts at once, which fills the issue slots a single
-// wavefront's dependent chain leaves empty.  LAG is a template argument
-// (coefficients in registers, unrolled taps).
+// stands.  Bands run one after the other, each only as long as its own rows
+// need.  LAG is a template argument (coefficients in registers, unrolled
+// taps).
 constexpr int kFgTemplateThreads = 96;
 
 template <int LAG>
-__device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
+__device__ __forceinline__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
   constexpr int kTaps = 2 * LAG * (LAG + 1);  // causal neighbours before the centre
   constexpr int W = 2 * LAG + 1;
-  // Band b + 1 runs kOff steps behind band b: its lane 0 needs band b's
-  // lane 31 (4 * 31 steps behind band b's lane 0) at column x + LAG, so
-  // kOff > LAG + 124; a multiple of W, so that every band's partial sums
-  // rotate in step.
-  constexpr int kOff = W * ((LAG + 125 + W - 1) / W);
-  constexpr int kBands = 3;  // up to 70 AR rows (3 .. 72) in bands of 32
   const int lane = threadIdx.x & 31;
   const int cs = p.coeff_shift, ro = 1 << (cs - 1);
   const int gmin = -(1 << (p.bd - 1)), gmax = (1 << (p.bd - 1)) - 1;
@@ -77,29 +68,21 @@ __device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, 
 #pragma unroll
   for (int i = 0; i <= kTaps; i++) co[i] = p.coeffs[plane][i];
   const int coL = lt ? co[kTaps] : 0;
-  const int nb = (h - 3 + 31) >> 5;
-  int acc[kBands][W];
-  int tendB[kBands];
-  int tEnd = 0;
+  for (int y0 = 3; y0 < h; y0 += 32) {
+    const int rows = imin(32, h - y0);
+    const int y = y0 + lane;
+    const bool row = lane < rows;
+    int acc[W];
 #pragma unroll
-  for (int s = 0; s < kBands; s++) {
-#pragma unroll
-    for (int j = 0; j < W; j++) acc[s][j] = 0;
+    for (int j = 0; j < W; j++) acc[j] = 0;
     // The first step brings column 0 of the rows above into the sums; the
     // last one finishes column w - 4 of the band's last row.
-    const int rows = imin(32, h - 3 - 32 * s);
-    tendB[s] = s < nb ? 4 * (rows - 1) + w - 3 : -LAG;
-    if (s < nb) tEnd = imax(tEnd, kOff * s + tendB[s]);
-  }
-  for (int t0 = -LAG; t0 < tEnd; t0 += W) {
+    const int tend = 4 * (rows - 1) + w - 3;
+    for (int t0 = -LAG; t0 < tend; t0 += W) {
 #pragma unroll
-    for (int k = 0; k < W; k++) {
-#pragma unroll
-      for (int s = 0; s < kBands; s++) {
-        const int t = t0 + k - kOff * s;
-        if (t >= -LAG && t < tendB[s]) {
-          const int y = 3 + 32 * s + lane;
-          const bool row = y < h;
+      for (int k = 0; k < W; k++) {
+        const int t = t0 + k;
+        if (t < tend) {
           const int x = t - 4 * lane;
           const int xn = x + LAG;  // the column entering the sums
           const bool inCol = row && x >= 0 && x < w;
@@ -111,12 +94,12 @@ __device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, 
             for (int d = LAG; d >= 1; d--) {
               const int v = g[(y - d) * kGW + xn];
 #pragma unroll
-              for (int j = W - 1; j >= 0; j--) acc[s][(j + k) % W] += co[(LAG - d) * W + 2 * LAG - j] * v;
+              for (int j = W - 1; j >= 0; j--) acc[(j + k) % W] += co[(LAG - d) * W + 2 * LAG - j] * v;
             }
           }
           int out = g0;
           if (inCol && x >= 3 && x < w - 3) {
-            int sum = acc[s][k % W];
+            int sum = acc[k % W];
             if (lt) sum += lt[y * kGW + x] * coL;
             out = iclip(g0 + ((sum + ro) >> cs), gmin, gmax);
             g[y * kGW + x] = (int16_t)out;
@@ -124,11 +107,11 @@ __device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, 
           // Output x's in-row products for columns x + 1 .. x + LAG; its
           // slot then serves column x + W.
 #pragma unroll
-          for (int m = 1; m <= LAG; m++) acc[s][(m + k) % W] += co[LAG * W + LAG - m] * out;
-          acc[s][k % W] = 0;
+          for (int m = 1; m <= LAG; m++) acc[(m + k) % W] += co[LAG * W + LAG - m] * out;
+          acc[k % W] = 0;
         }
+        __syncwarp();
       }
-      __syncwarp();
     }
   }
 }
@@ -136,7 +119,7 @@ __device__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, 
 // Luma term of the chroma AR (chroma.go:92-199): at each chroma AR position
 // the luma grain averaged over the co-located 1, 2 or 4 samples, into lt
 // (same layout as the templates).  All threads of the CTA.
-__device__ void luma_term(int16_t* lt, const int16_t* luma, int sx, int sy, int w, int h) {
+__device__ __forceinline__ void luma_term(int16_t* lt, const int16_t* luma, int sx, int sy, int w, int h) {
   const int aw = w - 6;
   for (int i = threadIdx.x; i < aw * (h - 3); i += blockDim.x) {
     const int y = 3 + i / aw, x = 3 + i % aw;
@@ -151,7 +134,7 @@ __device__ void luma_term(int16_t* lt, const int16_t* luma, int sx, int sy, int 
   }
 }
 
-__device__ void ar_warp_lag(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
+__device__ __forceinline__ void ar_warp_lag(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
   switch (p.lag) {
     case 0: ar_warp<0>(g, lt, p, plane, w, h); break;
     case 1: ar_warp<1>(g, lt, p, plane, w, h); break;
@@ -175,7 +158,7 @@ __device__ __forceinline__ uint16_t gf2_apply(const uint16_t* cols, uint16_t v) 
 
 // Gaussian fill of one template (luma.go:32-38 / chroma.go:38-44): draw i of
 // the plane's LFSR goes to sample (i / w, i % w).  One warp.
-__device__ void gauss_fill(int16_t* g, const int16_t* gauss, uint16_t seed, int w, int h, int shape, int shift) {
+__device__ __forceinline__ void gauss_fill(int16_t* g, const int16_t* gauss, uint16_t seed, int w, int h, int shape, int shift) {
   const int lane = threadIdx.x & 31;
   const int L = c_jump_len[shape];
   uint16_t reg = gf2_apply(c_jump[shape][lane], seed);
@@ -197,7 +180,7 @@ __device__ void gauss_fill(int16_t* g, const int16_t* gauss, uint16_t seed, int 
 // the Gaussian sequence while the templates are filled (lanes draw
 // different entries, which constant memory would serialise), then the
 // chroma AR's luma term.
-__device__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, int16_t (*s_g)[kGW * kGH],
+__device__ __forceinline__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, int16_t (*s_g)[kGW * kGH],
                              int16_t* s_gl) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int16_t* outs[3] = {gy, gu, gv};
@@ -597,15 +580,19 @@ cudaError_t launch_fg_offsets_batch(const BatchArgs& b, int total, int grid, cud
 cudaError_t launch_fg_apply_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
   const bool loop = batch_loops(b);
+  static int w1 = 0, w2 = 0, w4 = 0;
   switch (b.tile) {
     case 1:
-      loop ? k_fg_apply_batch<true, 2><<<grid, 256, 0, st>>>(b) : k_fg_apply_batch<false, 2><<<grid, 256, 0, st>>>(b);
+      loop ? k_fg_apply_batch<true, 2><<<grid, 256, 0, st>>>(b)
+           : k_fg_apply_batch<false, 2><<<grid, 256, 0, st>>>(with_wave(b, k_fg_apply_batch<false, 2>, 256, 0, w2));
       break;
     case 2:
-      loop ? k_fg_apply_batch<true, 4><<<grid, 256, 0, st>>>(b) : k_fg_apply_batch<false, 4><<<grid, 256, 0, st>>>(b);
+      loop ? k_fg_apply_batch<true, 4><<<grid, 256, 0, st>>>(b)
+           : k_fg_apply_batch<false, 4><<<grid, 256, 0, st>>>(with_wave(b, k_fg_apply_batch<false, 4>, 256, 0, w4));
       break;
     default:
-      loop ? k_fg_apply_batch<true, 1><<<grid, 256, 0, st>>>(b) : k_fg_apply_batch<false, 1><<<grid, 256, 0, st>>>(b);
+      loop ? k_fg_apply_batch<true, 1><<<grid, 256, 0, st>>>(b)
+           : k_fg_apply_batch<false, 1><<<grid, 256, 0, st>>>(with_wave(b, k_fg_apply_batch<false, 1>, 256, 0, w1));
   }
   return cudaGetLastError();
 }

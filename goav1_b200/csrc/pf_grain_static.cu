@@ -215,6 +215,7 @@ extern "C" int pf_film_grain_static(const pf_frame* ref, const pf_film_grain* fg
   b.tile = 0;
   b.f0 = 0;
   b.f1 = 1;
+  b.wave = 0;
   if (launch_fg_templates_batch(b, counts[ST_FG_TEMPLATES], counts[ST_FG_TEMPLATES], s) != cudaSuccess ||
       launch_fg_offsets_batch(b, counts[ST_FG_OFFSETS], counts[ST_FG_OFFSETS], s) != cudaSuccess ||
       launch_fg_apply_batch(b, counts[ST_FG_APPLY], counts[ST_FG_APPLY], s) != cudaSuccess)

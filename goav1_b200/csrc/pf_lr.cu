@@ -469,10 +469,11 @@ cudaError_t launch_lr_batch(const BatchArgs& b, int total, int grid, cudaStream_
     if (e != cudaSuccess) return e;
     configured = true;
   }
+  static int wave = 0;
   if (batch_loops(b))
     k_lr_batch<true><<<grid, 256, sizeof(LrSmem), st>>>(b);
   else
-    k_lr_batch<false><<<grid, 256, sizeof(LrSmem), st>>>(b);
+    k_lr_batch<false><<<grid, 256, sizeof(LrSmem), st>>>(with_wave(b, k_lr_batch<false>, 256, sizeof(LrSmem), wave));
   return cudaGetLastError();
 }
 

@@ -317,9 +317,12 @@ int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats*
  *       units_per_cta  consecutive work items (tiles / 64x64 units, in the
  *                      stage's numbering: along a row first) a CTA takes at
  *                      a time, 1..16, amortising per-item set-up;
- *       staging        how many items ahead of the current one, inside the
- *                      chunk, the CTA prefetches its input rows into L2
- *                      (0..3, below units_per_cta);
+ *       staging        0..3: with one item per CTA, the CTA first prefetches
+ *                      into L2 the input rows of the item that many waves
+ *                      on (a wave: the CTAs the device holds at once), which
+ *                      a CTA starting about when this one ends will take;
+ *                      with larger chunks, the item that many places on
+ *                      inside the chunk (then below units_per_cta);
  *       tile           deblocking: the tile shape, 0 = 32x8, 1 = 64x4,
  *                      2 = 16x16, 3 = 8x32 edge units a tile (one thread
  *                      each); grain apply: rows of a column whose loads are
@@ -341,7 +344,7 @@ enum { PF_TUNE_DEBLOCK = 0, PF_TUNE_CDEF = 1, PF_TUNE_RESTORATION = 2, PF_TUNE_F
 typedef struct pf_schedule {
   int32_t ctas;           /* persistent CTAs (0 = one CTA per chunk) */
   int32_t units_per_cta;  /* work items per chunk, 1..16 */
-  int32_t staging;        /* items prefetched ahead, 0..3 and < units_per_cta */
+  int32_t staging;        /* prefetch distance 0..3 (< units_per_cta when > 1) */
   int32_t tile;           /* deblocking 0..3, grain apply 0..2, else 0 */
 } pf_schedule;
 

@@ -94,7 +94,7 @@ def test_persistent_ctas_match_oracle(frames, expected):
 # staging depth), alone and with persistent CTAs, on every stage group.
 SCHEDULES = [dict(tile=t) for t in range(1, 4)] + \
     [dict(units_per_cta=u) for u in (2, 3, 4, 8, 16)] + \
-    [dict(units_per_cta=u, staging=d) for u, d in ((2, 1), (4, 2), (4, 3), (16, 3))] + \
+    [dict(units_per_cta=u, staging=d) for u, d in ((1, 1), (1, 3), (2, 1), (4, 2), (4, 3), (16, 3))] + \
     [dict(units_per_cta=4, staging=2, ctas=148), dict(units_per_cta=2, staging=1, ctas=7, tile=2)]
 
 
@@ -178,7 +178,7 @@ def test_scheduling_arguments_are_checked():
             r.set_frame_groups(bad)
     for g, kw in ((abi.PF_TUNE_CDEF, dict(tile=1)), (abi.PF_TUNE_FILM_GRAIN, dict(tile=3)), (0, dict(tile=4)),
                   (0, dict(units_per_cta=0)),
-                  (0, dict(units_per_cta=17)), (0, dict(staging=1)), (0, dict(units_per_cta=2, staging=2)),
+                  (0, dict(units_per_cta=17)), (0, dict(staging=4)), (0, dict(units_per_cta=2, staging=2)),
                   (0, dict(units_per_cta=8, staging=4)), (0, dict(ctas=-1)), (abi.PF_TUNE_GROUPS, {})):
         with pytest.raises(ErrInvalidArgument):
             r.set_schedule(g, **kw)
