@@ -1900,7 +1900,7 @@ static const int kTuneStatIndex[PF_TUNE_GROUPS] = {0, 1, 2, 4};  // pf_stats.sta
 static bool schedule_ok(int group, const pf_schedule& s) {
   return s.ctas >= 0 && s.ctas <= (1 << 20) && s.units_per_cta >= 1 && s.units_per_cta <= 16 && s.staging >= 0 &&
          s.staging <= 3 && (s.units_per_cta == 1 || s.staging < s.units_per_cta) && s.tile >= 0 &&
-         s.tile <= (group == PF_TUNE_DEBLOCK ? 3 : group == PF_TUNE_FILM_GRAIN ? 2 : 0);
+         s.tile <= (group == PF_TUNE_DEBLOCK || group == PF_TUNE_FILM_GRAIN ? 3 : 0);
 }
 
 extern "C" int pf_set_schedule(pf_ctx* c, int32_t group, const pf_schedule* s) {

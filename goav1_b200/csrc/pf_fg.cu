@@ -416,6 +416,128 @@ __device__ __forceinline__ void fg_apply_col(const DFrame& ref, const DFrame& di
   }
 }
 
+// fg_apply_col for four adjacent columns x .. x + 3 (x a multiple of 4,
+// 8-bit planes): the four samples of a row are read and written as one
+// 32-bit word, and the block set-up (offsets, template positions, blend
+// weights) is shared by the four columns, which always lie in one grain
+// block.  Planes whose rows are not 4-byte aligned, or a quad reaching past
+// the allocated width, go column by column.
+__device__ __forceinline__ void fg_apply_quad(const DFrame& ref, const DFrame& disp, const FgArgs& a,
+                                              const uint8_t* lut, int plane, int x, int y0, int nrows) {
+  const DPlane sp = ref.pl[plane];
+  const DPlane dp = disp.pl[plane];
+  if (x >= sp.aw) return;
+  const DPlane lp = ref.pl[0];
+  const uintptr_t al = reinterpret_cast<uintptr_t>(sp.ptr) | (uintptr_t)sp.stride |
+                       reinterpret_cast<uintptr_t>(dp.ptr) | (uintptr_t)dp.stride |
+                       reinterpret_cast<uintptr_t>(lp.ptr) | (uintptr_t)lp.stride;
+  if (x + 4 > sp.aw || (al & 3)) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) fg_apply_col<uint8_t, 1>(ref, disp, a, lut, plane, x + k, y0, nrows);
+    return;
+  }
+  const int yend = imin(y0 + nrows, sp.ah);
+  auto word = [](const DPlane& p, int y, int xx) { return reinterpret_cast<uint32_t*>(row_ptr<uint8_t>(p, y) + xx); };
+  if (!a.active[plane] || x >= sp.w) {
+    for (int y = y0; y < yend; y++) *word(dp, y, x) = *word(sp, y, x);
+    return;
+  }
+  const int sx = plane ? ref.ssx : 0, sy = plane ? ref.ssy : 0;
+  const int bwl = 5 - sx, bhl = 5 - sy;
+  const int bw = 1 << bwl, bh = 1 << bhl;
+  const int row = y0 >> bhl, bcol = x >> bwl;
+  const int xi = x - (bcol << bwl);
+  const int ovl = 2;
+  const int xStart = (a.overlap && bcol > 0) ? imin(sp.w - (bcol << bwl), ovl >> sx) : 0;
+  const int yStart = (a.overlap && row > 0) ? imin(sp.h - (row << bhl), ovl >> sy) : 0;
+  const uint8_t* offs = a.offsets + row * a.off_cols + bcol;
+  const int16_t* gr = a.grain[plane];
+  auto gcol = [&](int offset, int bc) { return 3 + (ovl >> sx) * (3 + (offset >> 4)) + xi + bw * bc; };
+  auto grow = [&](int offset, int br) { return 3 + (ovl >> sy) * (3 + (offset & 15)) + bh * br; };
+  const int o00 = offs[0];
+  const int c00 = gcol(o00, 0), r00 = grow(o00, 0);
+  const bool left = xi < xStart;  // only column xi (and xi + 1 for luma) of the first quad of a block
+  int c10 = 0, r10 = 0, c01 = 0, r01 = 0, c11 = 0, r11 = 0;
+  if (left) {
+    const int o10 = offs[-1];
+    c10 = gcol(o10, 1);
+    r10 = grow(o10, 0);
+  }
+  if (yStart > 0) {
+    const int o01 = offs[-a.off_cols];
+    c01 = gcol(o01, 0);
+    r01 = grow(o01, 1);
+    if (left) {
+      const int o11 = offs[-a.off_cols - 1];
+      c11 = gcol(o11, 1);
+      r11 = grow(o11, 1);
+    }
+  }
+  const int shift = a.scaling_shift;
+  int minV = 0, maxV = 255;
+  if (a.clip_restricted) {
+    minV = 16;
+    maxV = plane == 0 ? 235 : (a.matrix_identity ? 235 : 240);
+  }
+  const int yclip = imin(yend, sp.h);
+  const bool cfl = a.cfl, oddLuma = a.odd_luma;
+  const int lumaMult = a.luma_mult[plane] - 128, mult = a.mult[plane] - 128;
+  const int offs0 = a.offset[plane] - 256;
+  for (int y = y0; y < yend; y++) {
+    const uint32_t s4 = *word(sp, y, x);
+    if (y >= yclip) {
+      *word(dp, y, x) = s4;
+      continue;
+    }
+    const int yi = y - (row << bhl);
+    // The co-located luma of the four chroma samples: 8 bytes (4:2:x) or 4,
+    // the second word only when a column it serves is inside the crop.
+    uint32_t l0 = 0, l1 = 0;
+    if (plane != 0) {
+      l0 = *word(lp, y << sy, x << sx);
+      if (sx && x + 2 < sp.w) l1 = *word(lp, y << sy, (x << sx) + 4);
+    }
+    const int16_t* g00 = gr + (r00 + yi) * kGW + c00;
+    uint32_t out = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int s = (s4 >> (8 * k)) & 0xff;
+      int o = s;
+      if (x + k < sp.w) {
+        const bool lk = xi + k < xStart;
+        const int hpw = sx ? 23 : (xi + k == 1 ? 17 : 27), hcw = sx ? 22 : (xi + k == 1 ? 27 : 17);
+        int g = g00[k];
+        if (lk) g = blend_w(gr[(r10 + yi) * kGW + c10 + k], g, hpw, hcw, 8);
+        if (yi < yStart) {
+          int top = gr[(r01 + yi) * kGW + c01 + k];
+          if (lk) top = blend_w(gr[(r11 + yi) * kGW + c11 + k], top, hpw, hcw, 8);
+          const int vpw = sy ? 23 : (yi == 1 ? 17 : 27), vcw = sy ? 22 : (yi == 1 ? 27 : 17);
+          g = blend_w(top, g, vpw, vcw, 8);
+        }
+        int idx;
+        if (plane == 0) {
+          idx = s;
+        } else {
+          // chromaScalingIndex (apply.go:501-520) on the un-grained luma.
+          int avg;
+          if (sx) {
+            const uint32_t lw = k < 2 ? l0 : l1;
+            const int b0 = (lw >> (16 * (k & 1))) & 0xff, b1 = (lw >> (16 * (k & 1) + 8)) & 0xff;
+            avg = (oddLuma && x + k == sp.w - 1) ? b0 : (b0 + b1 + 1) >> 1;
+          } else {
+            avg = (l0 >> (8 * k)) & 0xff;
+          }
+          idx = cfl ? avg : iclip(((avg * lumaMult + s * mult) >> 6) + offs0, 0, 255);
+        }
+        const int noise = rpow2(lut[idx] * g, shift);
+        o = iclip(s + noise, minV, maxV);
+      }
+      out |= (uint32_t)o << (8 * k);
+    }
+    *word(dp, y, x) = out;
+  }
+}
+
 // frame/buffer.go:339-400: replicate the last visible column into the padding
 // columns of every visible row, then the last visible row into padding rows.
 template <typename T>
@@ -472,6 +594,7 @@ __device__ __forceinline__ FgTile fg_locate(const BatchArgs& b, const int* base,
 
 // kGroup rows per load group (fg_apply_col); one row at a time keeps 40
 // registers (6 CTAs per SM), groups of 2 or 4 need 64 (4 CTAs per SM).
+// kGroup 0: four columns by four rows a thread (fg_apply_quad, 8-bit).
 template <bool kLoop, int kGroup>
 __global__ void __launch_bounds__(256, kGroup == 1 ? 6 : 4) k_fg_apply_batch(BatchArgs b) {
   __shared__ uint8_t s_lut[256];
@@ -483,12 +606,24 @@ __global__ void __launch_bounds__(256, kGroup == 1 ? 6 : 4) k_fg_apply_batch(Bat
         const FrameJob& J = *t.J;
         s_lut[threadIdx.x] = J.fg.lut[t.plane][threadIdx.x];
         __syncthreads();
-        const int x = t.tx * 64 + (threadIdx.x & 63);
-        const int y0 = t.ty * 64 + (threadIdx.x >> 6) * 16;
-        if (J.io.bd == 8)
-          fg_apply_col<uint8_t, kGroup>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
-        else
-          fg_apply_col<uint16_t, kGroup>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
+        if constexpr (kGroup == 0) {
+          // Four columns by four rows a thread.
+          const int x = t.tx * 64 + (threadIdx.x & 15) * 4;
+          const int y0 = t.ty * 64 + (threadIdx.x >> 4) * 4;
+          if (J.io.bd == 8) {
+            fg_apply_quad(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 4);
+          } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) fg_apply_col<uint16_t, 1>(J.io, J.disp, J.fg, s_lut, t.plane, x + k, y0, 4);
+          }
+        } else {
+          const int x = t.tx * 64 + (threadIdx.x & 63);
+          const int y0 = t.ty * 64 + (threadIdx.x >> 6) * 16;
+          if (J.io.bd == 8)
+            fg_apply_col<uint8_t, kGroup>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
+          else
+            fg_apply_col<uint16_t, kGroup>(J.io, J.disp, J.fg, s_lut, t.plane, x, y0, 16);
+        }
         __syncthreads();  // the table is rewritten by the next tile
       },
       [&](int item) {
@@ -580,8 +715,12 @@ cudaError_t launch_fg_offsets_batch(const BatchArgs& b, int total, int grid, cud
 cudaError_t launch_fg_apply_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
   const bool loop = batch_loops(b);
-  static int w1 = 0, w2 = 0, w4 = 0;
+  static int w0 = 0, w1 = 0, w2 = 0, w4 = 0;
   switch (b.tile) {
+    case 3:
+      loop ? k_fg_apply_batch<true, 0><<<grid, 256, 0, st>>>(b)
+           : k_fg_apply_batch<false, 0><<<grid, 256, 0, st>>>(with_wave(b, k_fg_apply_batch<false, 0>, 256, 0, w0));
+      break;
     case 1:
       loop ? k_fg_apply_batch<true, 2><<<grid, 256, 0, st>>>(b)
            : k_fg_apply_batch<false, 2><<<grid, 256, 0, st>>>(with_wave(b, k_fg_apply_batch<false, 2>, 256, 0, w2));

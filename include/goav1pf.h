@@ -327,8 +327,9 @@ int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats*
  *                      2 = 16x16, 3 = 8x32 edge units a tile (one thread
  *                      each); grain apply: rows of a column whose loads are
  *                      issued together, 0 = 1 (40 registers, 6 CTAs per SM),
- *                      1 = 2, 2 = 4 (64 registers, 4 CTAs per SM); 0 for
- *                      the other groups.
+ *                      1 = 2, 2 = 4 (64 registers, 4 CTAs per SM), 3 = four
+ *                      columns by four rows a thread, 8-bit samples moved as
+ *                      32-bit words (64 registers); 0 for the other groups.
  *     Work items are independent, so every schedule gives the same samples.
  * pf_autotune searches the schedule of each group on a given batch, one
  * dimension at a time (tile setting, units per CTA, staging depth, persistent
@@ -345,7 +346,7 @@ typedef struct pf_schedule {
   int32_t ctas;           /* persistent CTAs (0 = one CTA per chunk) */
   int32_t units_per_cta;  /* work items per chunk, 1..16 */
   int32_t staging;        /* prefetch distance 0..3 (< units_per_cta when > 1) */
-  int32_t tile;           /* deblocking 0..3, grain apply 0..2, else 0 */
+  int32_t tile;           /* deblocking 0..3, grain apply 0..3, else 0 */
 } pf_schedule;
 
 typedef struct pf_tune_result {

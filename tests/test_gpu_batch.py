@@ -105,9 +105,7 @@ def test_schedules_match_oracle(frames, expected, sched):
     r = PostFilterRunner()
     for g in range(abi.PF_TUNE_GROUPS):
         kw = dict(sched)
-        if g == abi.PF_TUNE_FILM_GRAIN and "tile" in kw:
-            kw["tile"] = min(kw["tile"], 2)  # rows per load group: 1, 2, 4
-        elif g != abi.PF_TUNE_DEBLOCK:
+        if g not in (abi.PF_TUNE_DEBLOCK, abi.PF_TUNE_FILM_GRAIN):
             kw.pop("tile", None)
         r.set_schedule(g, **kw)
         got = r.get_schedule(g).as_dict()
@@ -176,7 +174,7 @@ def test_scheduling_arguments_are_checked():
     for bad in (0, 3, -1):
         with pytest.raises(ErrInvalidArgument):
             r.set_frame_groups(bad)
-    for g, kw in ((abi.PF_TUNE_CDEF, dict(tile=1)), (abi.PF_TUNE_FILM_GRAIN, dict(tile=3)), (0, dict(tile=4)),
+    for g, kw in ((abi.PF_TUNE_CDEF, dict(tile=1)), (abi.PF_TUNE_FILM_GRAIN, dict(tile=4)), (0, dict(tile=4)),
                   (0, dict(units_per_cta=0)),
                   (0, dict(units_per_cta=17)), (0, dict(staging=4)), (0, dict(units_per_cta=2, staging=2)),
                   (0, dict(units_per_cta=8, staging=4)), (0, dict(ctas=-1)), (abi.PF_TUNE_GROUPS, {})):
