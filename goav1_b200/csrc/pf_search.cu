@@ -114,6 +114,16 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
     const DPlane& sp = a.src.pl[pli];
     const int planeW = rp.w, planeH = rp.h;
     __syncthreads();  // the previous plane's tasks are done with the buffers
+    // A slice with none of the block's tested trials in this plane skips it
+    // (the chroma planes share one count); the chroma trials still need the
+    // luma directions, which the features kernel left in a.dirs.
+    if (s_cnt[P] == 0 && !(pli == 0 && s_cnt[1] > 0 && !a.dirs)) {
+      if (pli == 0 && s_cnt[1] > 0 && tid < 64 && ((listed >> tid) & 1)) {
+        s_dir[tid] = a.dirs[(size_t)fb * 64 + tid];
+        s_ai[tid] = a.ais[(size_t)fb * 64 + tid];
+      }
+      continue;
+    }
     // loadCDEFInput: frame samples where they exist, VeryLarge elsewhere.
     // A row wholly inside the plane whose start is 4-byte aligned is read
     // four samples at a time (w + 16 is a multiple of 4).
