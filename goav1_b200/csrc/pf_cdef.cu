@@ -255,27 +255,37 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
         __syncthreads();
       }
       if (tx < unitW) {
-        for (int y = ty0; y < unitH; y += rowStep) {
-          const int b = ((y >> bhLog2) << 3) + (tx >> bwLog2);
-          const uint16_t* c = &s_in[(2 + y) * kSW + 8 + tx];
+        // A thread takes one column over a run of whole block rows (16 or
+        // 8 luma rows, 4 or 8 chroma rows), so each block's parameters
+        // (strength, direction taps, table) are read once per block, not
+        // once per sample; a warp still covers 32 adjacent columns of one
+        // row at a time.
+        const int rpt = (64 >> ydec) / rowStep;
+        const int ya = ty0 * rpt, yb = imin(unitH, ya + rpt);
+        const int bh = 1 << bhLog2;
+        for (int yblk = ya; yblk < yb; yblk += bh) {
+          const int b = ((yblk >> bhLog2) << 3) + (tx >> bwLog2);
           const int pk = sm.blk[b];
-          int v = c[0];
-          if (pk >> 16) {
-            const int strength = (pk >> 4) & 255, dir = pk & 7;
-            if (useTab) {
-              if (strength | sec)
-                v = cdef_filter_px_tab(c, strength, strength ? &sm.tab[sm.slot[strength]][255] : nullptr, sec,
-                                       &sm.tab[kSecTab][255], sm.ofs[dir + 2], sm.ofs[dir + 4], sm.ofs[dir]);
-            } else if (strength | sec) {
-              if (interior)  // no VeryLarge sentinel anywhere in the halo
-                v = cdef_filter_px<false>(c, strength, (pk >> 12) & 15, sec, secShift, sm.ofs[dir + 2],
-                                          sm.ofs[dir + 4], sm.ofs[dir], coeffShift);
+          const int yend = imin(yblk + bh, yb);
+          const int strength = (pk >> 4) & 255, dir = pk & 7;
+          const bool filt = (pk >> 16) && (strength | sec);
+          const int2 po = sm.ofs[dir + 2], s0 = sm.ofs[dir + 4], s1 = sm.ofs[dir];
+          const int16_t* tp = (useTab && strength) ? &sm.tab[sm.slot[strength]][255] : nullptr;
+          const int16_t* ts = &sm.tab[kSecTab][255];
+          const int priShift = (pk >> 12) & 15;
+          for (int y = yblk; y < yend; y++) {
+            const uint16_t* c = &s_in[(2 + y) * kSW + 8 + tx];
+            int v = c[0];
+            if (filt) {
+              if (useTab)
+                v = cdef_filter_px_tab(c, strength, tp, sec, ts, po, s0, s1);
+              else if (interior)  // no VeryLarge sentinel anywhere in the halo
+                v = cdef_filter_px<false>(c, strength, priShift, sec, secShift, po, s0, s1, coeffShift);
               else
-                v = cdef_filter_px<true>(c, strength, (pk >> 12) & 15, sec, secShift, sm.ofs[dir + 2],
-                                         sm.ofs[dir + 4], sm.ofs[dir], coeffShift);
+                v = cdef_filter_px<true>(c, strength, priShift, sec, secShift, po, s0, s1, coeffShift);
             }
+            reinterpret_cast<T*>(obase + (int64_t)(unitY + y) * ostride)[unitX + tx] = (T)v;
           }
-          reinterpret_cast<T*>(obase + (int64_t)(unitY + y) * ostride)[unitX + tx] = (T)v;
         }
       }
       __syncthreads();

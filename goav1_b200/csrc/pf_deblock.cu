@@ -221,20 +221,20 @@ __device__ __forceinline__ void deblock_unit(const DFrame& f, const LfArgs& a, i
   const bool words = (((uintptr_t)pl.ptr | (uintptr_t)pl.stride) & (4 * sizeof(T) - 1)) == 0;
   int P[4][4], Q[4][4];
   lpf_inner<T>(q, sstride, dir, words, P, Q);
+  // The width class: the widest mask lane with this unit's bit set; every
+  // lane's word is read up front so the loads go out together.
   int k = -1;
   if (luma) {
     const int half = bit >> 4, b = bit & 15;
-#pragma unroll
-    for (int kk = 2; kk >= 0; kk--) {
-      if (k < 0 && ((__ldg(&region[((dir * 32 + pos) * 3 + kk) * 2 + half]) >> b) & 1)) k = kk;
-    }
+    const uint16_t* m = &region[((dir * 32 + pos) * 3) * 2 + half];
+    const int w0 = __ldg(&m[0]), w1 = __ldg(&m[2]), w2 = __ldg(&m[4]);
+    k = ((w2 >> b) & 1) ? 2 : ((w1 >> b) & 1) ? 1 : ((w0 >> b) & 1) ? 0 : -1;
   } else {
     const int lane = dir == 0 ? (16 >> ssy) : (16 >> ssx);
     const int half = bit / lane, b = bit - half * lane;
-#pragma unroll
-    for (int kk = 1; kk >= 0; kk--) {
-      if (k < 0 && ((__ldg(&region[384 + ((dir * 32 + pos) * 2 + kk) * 2 + half]) >> b) & 1)) k = kk;
-    }
+    const uint16_t* m = &region[384 + ((dir * 32 + pos) * 2) * 2 + half];
+    const int w0 = __ldg(&m[0]), w1 = __ldg(&m[2]);
+    k = ((w1 >> b) & 1) ? 1 : ((w0 >> b) & 1) ? 0 : -1;
   }
   if (k < 0) return;
   const int wd = k == 2 ? 16 : (k == 1 ? (luma ? 8 : 6) : 4);
