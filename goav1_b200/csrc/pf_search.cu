@@ -42,6 +42,7 @@ namespace cg = cooperative_groups;
 namespace pf {
 
 constexpr int kLearnedSlices = 4;
+constexpr int kTrialsPerSlice = 16;
 
 __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   __shared__ uint16_t s_in[kSH * kSW];
@@ -84,18 +85,23 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
   const uint64_t mask0 = a.tmask ? a.tmask[2 * fb] : listMask;
   const uint64_t mask1 = a.tmask ? a.tmask[2 * fb + 1] : a.trials.uvMask;
   const int ssY = a.trials.ss;
+  // The slices this block uses: one per kTrialsPerSlice tested trials (a
+  // block with a handful of trials is measured by one CTA, a fallback block
+  // by all of its CTAs); the others have nothing to do.
+  const int used = imin(slices, 1 + (__popcll(mask0) + __popcll(mask1)) / kTrialsPerSlice);
+  if (slice >= used) return;
   if (tid == 0) {
     if (slice == 0) a.skip[fb] = 0;
     // This slice's share of the tested trials: list positions slice,
-    // slice + slices, ...
+    // slice + used, ...
     int c0 = 0, c1 = 0, n0 = 0, n1 = 0;
     for (int g = 0; g < 64; g++) {
       if ((mask0 >> g) & 1) {
-        if (n0 % slices == slice) s_list[0][c0++] = (uint8_t)g;
+        if (n0 % used == slice) s_list[0][c0++] = (uint8_t)g;
         n0++;
       }
       if ((mask1 >> g) & 1) {
-        if (n1 % slices == slice) s_list[1][c1++] = (uint8_t)g;
+        if (n1 % used == slice) s_list[1][c1++] = (uint8_t)g;
         n1++;
       }
     }
@@ -264,8 +270,8 @@ __global__ void __launch_bounds__(256) k_cdef_search(SearchArgs a) {
     // it, the rest by slice 0.
     const uint64_t below = (1ull << tid) - 1;
     const bool t0 = (mask0 >> tid) & 1, t1 = (mask1 >> tid) & 1;
-    const bool own0 = t0 && __popcll(mask0 & below) % slices == slice;
-    const bool own1 = t1 && __popcll(mask1 & below) % slices == slice;
+    const bool own0 = t0 && __popcll(mask0 & below) % used == slice;
+    const bool own1 = t1 && __popcll(mask1 & below) % used == slice;
     if (tid >= count) {
       if (slice == 0) m0[tid] = m1[tid] = kNotATrial;
     } else {
