@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-config2", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="time the default schedule instead of the autotuned one")
+    ap.add_argument("--schedule", action="append", default=[], metavar="GROUP:CTAS:UNITS:STAGING:TILE",
+                    help="with --no-tune: set a stage group's schedule (pf_schedule) by hand; repeatable")
+    ap.add_argument("--frame-groups", type=int, default=1, help="with --no-tune: frame groups (1 or 2)")
     return ap.parse_args()
 
 
@@ -604,7 +607,17 @@ def main():
     # tuner filters the frames in place, and reset() restores them before
     # every step.
     schedule = None
-    if not args.no_tune:
+    if args.no_tune:
+        # Hand-set schedules (for captures of the kernels the tuned run uses).
+        for spec in args.schedule:
+            g, ctas, units, staging, tile = (int(v) for v in spec.split(":"))
+            runner.set_schedule(g, ctas=ctas, units_per_cta=units, staging=staging, tile=tile)
+        runner.set_frame_groups(args.frame_groups)
+        if args.schedule:
+            schedule = {nm: runner.get_schedule(i).as_dict()
+                        for i, nm in enumerate(["deblock", "cdef", "restoration", "film_grain"])}
+            schedule["frame_groups"] = {"chosen": args.frame_groups, "set_by_hand": True}
+    else:
         reset()
         tune = runner.autotune(pf_frames, reps=2)
         schedule = {nm: dict(tune.chosen[i].as_dict(), ms=round(float(tune.ms[i]), 4),
