@@ -713,7 +713,7 @@ static const void* put_side(Bytes& hs, Cursor& dev, const void* src, size_t n) {
 
 template <class Bytes>
 static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, Bytes& hs, FrameJob& J, int counts[ST_COUNT],
-                     int dbTile, int cdefParts) {
+                     int dbTile) {
   const pf_frame* f = r.f;
   const pf_frame_side* s = r.s;
   const int bps = bps_of(f);
@@ -822,8 +822,7 @@ static void fill_job(const FrameRef& r, Cursor& arena, Cursor& side, Bytes& hs, 
         l.line_stride[p] = a.line_stride[p];
       }
     }
-    J.cdef_parts = cdefParts;
-    counts[ST_CDEF] = ucols * urows * cdefParts;
+    counts[ST_CDEF] = ucols * urows;
     int tiles = 0;
     for (int p = 0; p < (f->mono ? 1 : 3); p++) {
       const int sx = p ? f->ss_x : 0, sy = p ? f->ss_y : 0;
@@ -1112,17 +1111,11 @@ static int replay_or_capture(pf_ctx* c, int n, bool fg) {
 template <class Bytes>
 static int prepare_batch(pf_ctx* c, const FrameRef* refs, int n, Bytes& hs, DevBuf& sideDev, uint32_t* completed,
                          bool* fg) {
-  size_t arenaBytes = 0, sideBytes = 0, units = 0;
+  size_t arenaBytes = 0, sideBytes = 0;
   for (int i = 0; i < n; i++) {
     arenaBytes += frame_scratch(refs[i].f, refs[i].s);
     sideBytes += frame_side_bytes(refs[i].f, refs[i].s);
-    units += (size_t)((refs[i].f->width + 63) / 64) * ((refs[i].f->height + 63) / 64);
   }
-  // CDEF work items: whole 64x64 units, or their halves (tile setting 2;
-  // setting 0 picks halves when the batch has fewer units than two waves of
-  // the CDEF kernel, as a single frame has, so its units' latency halves).
-  const int cdefTile = c->tile[ST_CDEF];
-  const int cdefParts = cdefTile == 2 || (cdefTile == 0 && units < (size_t)c->sm_count * 8) ? 2 : 1;
   CK(c->arena.ensure(arenaBytes + 256));
   CK(sideDev.ensure(sideBytes + 256));
   Cursor arena{(uint8_t*)c->arena.p, 0}, side{(uint8_t*)sideDev.p, 0};
@@ -1132,7 +1125,7 @@ static int prepare_batch(pf_ctx* c, const FrameRef* refs, int n, Bytes& hs, DevB
   uint32_t done = 0;
   for (int i = 0; i < n; i++) {
     int counts[ST_COUNT];
-    fill_job(refs[i], arena, side, hs, c->hjobs[i], counts, c->db_tile, cdefParts);
+    fill_job(refs[i], arena, side, hs, c->hjobs[i], counts, c->db_tile);
     c->hjobs[i].cdef.ctab = (const int16_t*)c->ctab.p;
     for (int k = 0; k < ST_COUNT; k++) c->hbase[(size_t)k * (n + 1) + i + 1] = c->hbase[(size_t)k * (n + 1) + i] + counts[k];
     const pf_frame_side* s = refs[i].s;
@@ -1907,7 +1900,7 @@ static const int kTuneStatIndex[PF_TUNE_GROUPS] = {0, 1, 2, 4};  // pf_stats.sta
 static bool schedule_ok(int group, const pf_schedule& s) {
   return s.ctas >= 0 && s.ctas <= (1 << 20) && s.units_per_cta >= 1 && s.units_per_cta <= 16 && s.staging >= 0 &&
          s.staging <= 3 && (s.units_per_cta == 1 || s.staging < s.units_per_cta) && s.tile >= 0 &&
-         s.tile <= (group == PF_TUNE_DEBLOCK || group == PF_TUNE_FILM_GRAIN ? 3 : group == PF_TUNE_CDEF ? 2 : 0);
+         s.tile <= (group == PF_TUNE_DEBLOCK || group == PF_TUNE_FILM_GRAIN ? 3 : 0);
 }
 
 extern "C" int pf_set_schedule(pf_ctx* c, int32_t group, const pf_schedule* s) {

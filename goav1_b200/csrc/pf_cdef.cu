@@ -39,14 +39,11 @@ struct CdefSmem {
   int8_t slot_str[16];   // strength of each table
 };
 
-// One 64x64 filter unit (uc, ur), all planes, or one of its `parts` row
-// bands (whole 8x8-block rows: the top and bottom halves for parts = 2).
-// A band filters exactly what the unit would there: its halo rows inside
-// the unit are the frame's rows, as the unit's own are.  aw/ah: MI-aligned
-// extents (frameWorkCDEFAlignedPlane).
+// One 64x64 filter unit (uc, ur), all planes.  aw/ah: MI-aligned extents
+// (frameWorkCDEFAlignedPlane).
 template <typename T>
 __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a, const int* aw, const int* ah,
-                          int uc, int ur, int part, int parts, CdefSmem& sm) {
+                          int uc, int ur, CdefSmem& sm) {
   uint16_t* s_in = sm.in;
   uint8_t* s_dir = sm.dir;
   int32_t* s_var = sm.var;
@@ -66,15 +63,12 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
 #pragma unroll
     for (int i = 0; i < 8; i++) word |= (uint64_t)w[i] << (8 * i);
   }
-  // A band's 8x8-block rows become rows 0.. of the word.
-  if (parts > 1) word >>= part * (64 / parts);
   const int nplanes = in.mono ? 1 : 3;
   for (int plane = 0; plane < nplanes; plane++) {
     const int xdec = plane ? in.ssx : 0, ydec = plane ? in.ssy : 0;
     const int Wa = aw[plane], Ha = ah[plane];
-    const int bandH = (64 >> ydec) / parts;
-    const int unitX = (uc * 64) >> xdec, unitY = ((ur * 64) >> ydec) + part * bandH;
-    const int unitW = imin(64 >> xdec, Wa - unitX), unitH = imin(bandH, Ha - unitY);
+    const int unitX = (uc * 64) >> xdec, unitY = (ur * 64) >> ydec;
+    const int unitW = imin(64 >> xdec, Wa - unitX), unitH = imin(64 >> ydec, Ha - unitY);
     if (unitW <= 0 || unitH <= 0) continue;
     const DPlane& ip = in.pl[plane];
     const DPlane& op = out.pl[plane];
@@ -266,13 +260,13 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
         // (strength, direction taps, table) are read once per block, not
         // once per sample; a warp still covers 32 adjacent columns of one
         // row at a time.
-        const int rpt = imax(((64 >> ydec) / parts) / rowStep, 1);
+        const int rpt = (64 >> ydec) / rowStep;
         const int ya = ty0 * rpt, yb = imin(unitH, ya + rpt);
         const int bh = 1 << bhLog2;
-        for (int yblk = ya; yblk < yb;) {
+        for (int yblk = ya; yblk < yb; yblk += bh) {
           const int b = ((yblk >> bhLog2) << 3) + (tx >> bwLog2);
           const int pk = sm.blk[b];
-          const int yend = imin((yblk | (bh - 1)) + 1, yb);
+          const int yend = imin(yblk + bh, yb);
           const int strength = (pk >> 4) & 255, dir = pk & 7;
           const bool filt = (pk >> 16) && (strength | sec);
           const int2 po = sm.ofs[dir + 2], s0 = sm.ofs[dir + 4], s1 = sm.ofs[dir];
@@ -292,7 +286,6 @@ __device__ void cdef_unit(const DFrame& in, const DFrame& out, const CdefArgs& a
             }
             reinterpret_cast<T*>(obase + (int64_t)(unitY + y) * ostride)[unitX + tx] = (T)v;
           }
-          yblk = yend;
         }
       }
       __syncthreads();
@@ -340,28 +333,25 @@ __global__ void __launch_bounds__(256, 4) k_cdef_batch(BatchArgs b) {
         const int fi = find_frame(base, b.n, item);
         const FrameJob& J = b.jobs[fi];
         const int local = item - base[fi];
-        const int parts = J.cdef_parts, band = local / J.cdef.ucols;
-        const int uc = local % J.cdef.ucols, ur = band / parts, part = band - ur * parts;
+        const int uc = local % J.cdef.ucols, ur = local / J.cdef.ucols;
         if (J.io.bd == 8)
-          cdef_unit<uint8_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, part, parts, sm);
+          cdef_unit<uint8_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, sm);
         else
-          cdef_unit<uint16_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, part, parts, sm);
+          cdef_unit<uint16_t>(J.io, J.scr, J.cdef, J.aw, J.ah, uc, ur, sm);
       },
       [&](int item) {
         // Every plane's unit with its 8-column / 2-row halo.
         const int fi = find_frame(base, b.n, item);
         const FrameJob& J = b.jobs[fi];
         const int local = item - base[fi];
-        const int parts = J.cdef_parts, band = local / J.cdef.ucols;
-        const int uc = local % J.cdef.ucols, ur = band / parts, part = band - ur * parts;
+        const int uc = local % J.cdef.ucols, ur = local / J.cdef.ucols;
         for (int plane = 0; plane < (J.io.mono ? 1 : 3); plane++) {
           const int xdec = plane ? J.io.ssx : 0, ydec = plane ? J.io.ssy : 0;
-          const int bandH = (64 >> ydec) / parts;
-          const int x = (uc * 64) >> xdec, y = ((ur * 64) >> ydec) + part * bandH;
+          const int x = (uc * 64) >> xdec, y = (ur * 64) >> ydec;
           if (J.io.bd == 8)
-            prefetch_block<uint8_t>(J.io.pl[plane], x - 8, x + (64 >> xdec) + 8, y - 2, y + bandH + 2);
+            prefetch_block<uint8_t>(J.io.pl[plane], x - 8, x + (64 >> xdec) + 8, y - 2, y + (64 >> ydec) + 2);
           else
-            prefetch_block<uint16_t>(J.io.pl[plane], x - 8, x + (64 >> xdec) + 8, y - 2, y + bandH + 2);
+            prefetch_block<uint16_t>(J.io.pl[plane], x - 8, x + (64 >> xdec) + 8, y - 2, y + (64 >> ydec) + 2);
         }
       });
 }

@@ -180,7 +180,6 @@ struct FrameJob {
   FgTemplateArgs fgt;
   int aw[3], ah[3];          // MI-aligned plane extents
   int db_tile;               // deblocking tile shape (db_tile_w / db_tile_h)
-  int cdef_parts;            // CDEF work items per 64x64 unit: 1, or 2 (top and bottom halves)
   int db_tx[3], db_ty[3];    // deblock tiles per plane (0 = gated)
   int lr_cols[3], lr_rows[3];  // restoration tiles (processing column x stripe)
   int fg_tx[3], fg_ty[3];    // 64x64-sample tiles of the display planes

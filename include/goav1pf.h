@@ -329,11 +329,7 @@ int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats*
  *                      issued together, 0 = 1 (40 registers, 6 CTAs per SM),
  *                      1 = 2, 2 = 4 (64 registers, 4 CTAs per SM), 3 = four
  *                      columns by four rows a thread, 8-bit samples moved as
- *                      32-bit words (64 registers); CDEF: 0 = whole 64x64
- *                      units, or their top and bottom halves when the batch
- *                      has fewer units than two waves of the kernel (a
- *                      single frame), 1 = whole units, 2 = halves; 0 for the
- *                      other groups.
+ *                      32-bit words (64 registers); 0 for the other groups.
  *     Work items are independent, so every schedule gives the same samples.
  * pf_autotune searches the schedule of each group on a given batch, one
  * dimension at a time (tile setting, units per CTA, staging depth, persistent
@@ -350,7 +346,7 @@ typedef struct pf_schedule {
   int32_t ctas;           /* persistent CTAs (0 = one CTA per chunk) */
   int32_t units_per_cta;  /* work items per chunk, 1..16 */
   int32_t staging;        /* prefetch distance 0..3 (< units_per_cta when > 1) */
-  int32_t tile;           /* deblocking 0..3, grain apply 0..3, CDEF 0..2, else 0 */
+  int32_t tile;           /* deblocking 0..3, grain apply 0..3, else 0 */
 } pf_schedule;
 
 typedef struct pf_tune_result {

@@ -105,9 +105,7 @@ def test_schedules_match_oracle(frames, expected, sched):
     r = PostFilterRunner()
     for g in range(abi.PF_TUNE_GROUPS):
         kw = dict(sched)
-        if g == abi.PF_TUNE_CDEF and "tile" in kw:
-            kw["tile"] = min(kw["tile"], 2)  # 1: whole units, 2: halves
-        elif g not in (abi.PF_TUNE_DEBLOCK, abi.PF_TUNE_FILM_GRAIN):
+        if g not in (abi.PF_TUNE_DEBLOCK, abi.PF_TUNE_FILM_GRAIN):
             kw.pop("tile", None)
         r.set_schedule(g, **kw)
         got = r.get_schedule(g).as_dict()
@@ -148,7 +146,7 @@ def test_autotune_then_graphs_match_oracle(frames, expected):
     for g in range(abi.PF_TUNE_GROUPS):
         c = res.chosen[g]
         assert c.ctas >= 0 and 1 <= c.units_per_cta <= 16 and 0 <= c.staging <= 3
-        assert c.tile == 0 or g in (abi.PF_TUNE_DEBLOCK, abi.PF_TUNE_FILM_GRAIN, abi.PF_TUNE_CDEF)
+        assert c.tile == 0 or g in (abi.PF_TUNE_DEBLOCK, abi.PF_TUNE_FILM_GRAIN)
         assert r.get_schedule(g).as_dict() == c.as_dict()
     assert all(m > 0 for m in res.ms)
     assert all(m <= d for m, d in zip(res.ms, res.ms_default))
@@ -176,7 +174,7 @@ def test_scheduling_arguments_are_checked():
     for bad in (0, 3, -1):
         with pytest.raises(ErrInvalidArgument):
             r.set_frame_groups(bad)
-    for g, kw in ((abi.PF_TUNE_CDEF, dict(tile=3)), (abi.PF_TUNE_RESTORATION, dict(tile=1)), (abi.PF_TUNE_FILM_GRAIN, dict(tile=4)), (0, dict(tile=4)),
+    for g, kw in ((abi.PF_TUNE_CDEF, dict(tile=1)), (abi.PF_TUNE_FILM_GRAIN, dict(tile=4)), (0, dict(tile=4)),
                   (0, dict(units_per_cta=0)),
                   (0, dict(units_per_cta=17)), (0, dict(staging=4)), (0, dict(units_per_cta=2, staging=2)),
                   (0, dict(units_per_cta=8, staging=4)), (0, dict(ctas=-1)), (abi.PF_TUNE_GROUPS, {})):
