@@ -464,15 +464,16 @@ def measure_issue_peaks():
 
 
 # Per-frame counters of the batched chain kernels at the 1080p 8-bit 4:2:0
-# workload, from one ncu capture of a 60-frame launch of each kernel of the
-# current code (profiles/postfilter_chain_counters_1080p8_60frames.md has the
-# command and the raw figures): DRAM bytes read + written and warp
+# workload, from one ncu capture of a 60-frame launch of each kernel as the
+# autotuner sets them on this batch (deblocking 16x16 tiles, grain apply four
+# columns a thread; profiles/postfilter_chain_counters_1080p8_60frames.md has
+# the command and the raw figures): DRAM bytes read + written and warp
 # instructions executed (deblocking: both passes).
 KERNEL_COUNTERS_1080P8 = {
-    "deblock": {"dram_bytes": (443.97e6 + 175.47e6) / 60, "warp_inst": 593.75e6 / 60},
-    "cdef": {"dram_bytes": (187.91e6 + 163.16e6) / 60, "warp_inst": 1122.57e6 / 60},
-    "restoration": {"dram_bytes": (205.90e6 + 152.75e6) / 60, "warp_inst": 928.93e6 / 60},
-    "film_grain": {"dram_bytes": (189.52e6 + 157.82e6) / 60, "warp_inst": 622.57e6 / 60},
+    "deblock": {"dram_bytes": (443.94e6 + 176.06e6) / 60, "warp_inst": 571.48e6 / 60},
+    "cdef": {"dram_bytes": (187.19e6 + 164.21e6) / 60, "warp_inst": 1097.56e6 / 60},
+    "restoration": {"dram_bytes": (205.87e6 + 152.76e6) / 60, "warp_inst": 943.62e6 / 60},
+    "film_grain": {"dram_bytes": (189.65e6 + 151.37e6) / 60, "warp_inst": 500.34e6 / 60},
 }
 
 
