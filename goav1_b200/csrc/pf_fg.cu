@@ -9,19 +9,19 @@
 // in order from each stripe's LFSR, overlap blends, noise and clipping).
 //
 // GPU shape: the 82x73 templates are generated by one 3-warp CTA per frame.
-// The Gaussian fill is split over 32 lanes: the LFSR is linear over
-// GF(2)^16, so lane k starts from M^(kL) * seed (jump matrices precomputed on
-// the host) and walks its L draws; the AR filter runs as a wavefront over
-// t = x + 4y (every AR input of sample (y, x) has a smaller t), one warp per
-// template, rows in lanes, neighbours read from the shared template.  Offsets
-// come from one thread per 32-row stripe.  The apply is one thread per output
-// sample, 64x16-sample tiles per CTA.
+// The Gaussian fill is split over the CTA's 96 threads: the LFSR is linear
+// over GF(2)^16, so thread k starts from M^(kL) * seed (jump matrices
+// precomputed on the host) and walks its L draws; the AR filter runs as a
+// wavefront over t = x + 4y (every AR input of sample (y, x) has a smaller
+// t), one warp per template, rows in lanes, neighbours passed between lanes
+// by shuffles.  Offsets come from one thread per 32-row stripe.  The apply
+// is one thread per output sample, 64x16-sample tiles per CTA.
+#include <atomic>
+
 #include "pf_common.cuh"
 #include "pf_tables.h"
 
 namespace pf {
-
-__constant__ int16_t c_gauss[2048];
 
 constexpr int kGW = 82, kGH = 73;
 
@@ -33,120 +33,182 @@ __device__ __forceinline__ uint16_t lfsr(uint16_t& reg, int bits) {
   return (uint16_t)((reg >> (16 - bits)) & ((1 << bits) - 1));
 }
 
-// AR recursion of one template (luma.go:83-158 / chroma.go:92-199 generic
-// form), run by one warp as a wavefront with no CTA barrier.  The template's
-// AR rows are taken in bands of up to 32 rows, one row per lane; at step t
-// lane r (row y) handles column x = t - 4r, so every sample of the rows
-// above that its output needs (columns up to x + LAG <= x + 3) was written
-// to the shared template by lanes r-1.. at an earlier step, and the warp
-// barrier that ends each step makes it visible.  The filter runs in
-// transposed form: when the value of row y-d at column x + LAG arrives, its
-// products go straight into the partial sums of the outputs x .. x + 2*LAG
-// it reaches, and the lane's own output adds its in-row products to the
-// next LAG outputs' sums; the output then needs only its own sum, so the
-// loop-carried path is load -> one multiply-add -> round -> clip -> store.
-// The 2*LAG+1 partial sums rotate through acc[] with the step (the steps
-// run in groups of 2*LAG+1, slot (j + k) mod (2*LAG+1) holding output x + j
-// at step k of a group), so moving to the next column renames registers
-// instead of copying them.  A chroma template's luma term comes from lt[]
-// (the averaged luma grain at each chroma position, filled before the
-// recursion).  A lane outside the AR columns passes the template's value
-// through unchanged, so the rows above always hold the template as it
-// stands.  Bands run one after the other, each only as long as its own rows
-// need.  LAG is a template argument (coefficients in registers, unrolled
-// taps).
+// ---- grain templates ----
+//
+// Shared layout of a template while it is generated: 32 lanes x 4 padded
+// rows of 128 samples.  Template row y is AR row v = y - 3 (v = -3..h-4);
+// it lives in padded row 4 * (v mod 32) + floor(v / 32) + 1, column x at
+// x + 4.  Lane r of the AR warp owns AR rows r, r + 32, r + 64 (rows -3..-1
+// ride on lanes 29..31), so the rows a lane visits are consecutive in
+// memory and its position at wavefront step t is one running address,
+// 508 r + t + 132.  Samples that the recursion must pass through unchanged
+// (rows 0-2, the three border columns on each side, the padding) are
+// stored with kNonAr added; an AR output is a plain sample.  The stored
+// value then tells each step what to do, and no step needs a bounds test.
+constexpr int kTplRow = 128;
+constexpr int kTplPlane = 32 * 4 * kTplRow;
+constexpr int kTplCol0 = 4;
+constexpr int kNonAr = 16384;  // above any grain sample (|g| <= 2048)
 constexpr int kFgTemplateThreads = 96;
 
-template <int LAG>
+struct TplSmem {
+  int16_t g[3][kTplPlane];  // luma, Cb, Cr
+  int16_t lt[kTplPlane];    // the chroma AR's luma term, chroma layout
+  int16_t gauss[2048];      // the Gaussian sequence
+};
+
+__device__ __forceinline__ int tpl_at(int y, int x) {
+  const int v = y - 3;
+  return (4 * (v & 31) + (v >> 5) + 1) * kTplRow + x + kTplCol0;
+}
+
+__device__ __forceinline__ int tpl_decode(int s) { return s >= kNonAr / 2 ? s - kNonAr : s; }
+
+// AR recursion of one template (luma.go:83-158 / chroma.go:92-199 generic
+// form), run by one warp as a single wavefront with no barrier: AR row v
+// is at column x = t - 4v at step t, so every AR input of (v, x) from the
+// rows above was finished at an earlier step.  Rows v - d at column
+// x + LAG reach the lane from lane r - 1 by warp shuffles out of small
+// register rings: the row directly above as that lane's output of 4 - LAG
+// steps back, and the rows further up as the values that lane itself
+// received 4 steps back (for LAG 3 those two are passed on as one packed
+// pair of int16; for LAG 2 and 3 a pair of taps costs one __dp2a_lo).
+// The filter runs in transposed form: a value arriving from the rows above
+// goes straight into the partial sums of the outputs x .. x + 2*LAG it
+// reaches, and the lane's own output adds its in-row products to the next
+// LAG outputs' sums, so the loop-carried path is shuffle -> multiply-add ->
+// shift -> clip.  The partial sums rotate through acc[] with the step and
+// start from the rounding offset; the rings are whole rotations long, so
+// the unrolled steps rename registers.
+// The wavefront starts 4*LAG steps early so that the pass-through rows
+// above the first AR row are in the rings when row 0 needs them, and may
+// run a few steps past the last AR output (those steps only rewrite
+// pass-through samples with their own values).  LAG is a template argument
+// (coefficients in registers, unrolled taps); with LAG 0 only the luma
+// term remains, one sample a lane.
+template <int LAG, bool kLt>
 __device__ __forceinline__ void ar_warp(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
   constexpr int kTaps = 2 * LAG * (LAG + 1);  // causal neighbours before the centre
-  constexpr int W = 2 * LAG + 1;
   const int lane = threadIdx.x & 31;
   const int cs = p.coeff_shift, ro = 1 << (cs - 1);
   const int gmin = -(1 << (p.bd - 1)), gmax = (1 << (p.bd - 1)) - 1;
-  int co[kTaps + 1];
+  const int8_t* cf = p.coeffs[plane];
+  if constexpr (LAG == 0) {
+    if constexpr (!kLt) return;
+    const int coL = cf[0], aw = w - 6;
+    for (int i = lane; i < aw * (h - 3); i += 32) {
+      const int o = tpl_at(3 + i / aw, 3 + i % aw);
+      g[o] = (int16_t)iclip(g[o] + ((lt[o] * coL + ro) >> cs), gmin, gmax);
+    }
+  } else {
+    constexpr int W = 2 * LAG + 1;
+    constexpr int U = 2 * W;  // ring length (at least 5) and unroll
+    // Per output slot j (the output j columns right of the arriving value):
+    // the two farthest rows' taps as a byte pair (LAG 2 and 3) and the
+    // nearest row's tap (LAG 1 and 3).
+    int cp[W], c1[W], cin[LAG + 1];
 #pragma unroll
-  for (int i = 0; i <= kTaps; i++) co[i] = p.coeffs[plane][i];
-  const int coL = lt ? co[kTaps] : 0;
-  for (int y0 = 3; y0 < h; y0 += 32) {
-    const int rows = imin(32, h - y0);
-    const int y = y0 + lane;
-    const bool row = lane < rows;
-    int acc[W];
+    for (int j = 0; j < W; j++) {
+      cp[j] = 0;
+      c1[j] = 0;
+      if constexpr (LAG >= 2)
+        cp[j] = (int)(uint8_t)cf[2 * LAG - j] | ((int)(uint8_t)cf[W + 2 * LAG - j] << 8);
+      if constexpr (LAG == 3) c1[j] = cf[2 * W + 2 * LAG - j];
+      if constexpr (LAG == 1) c1[j] = cf[2 * LAG - j];
+    }
 #pragma unroll
-    for (int j = 0; j < W; j++) acc[j] = 0;
-    // The first step brings column 0 of the rows above into the sums; the
-    // last one finishes column w - 4 of the band's last row.
-    const int tend = 4 * (rows - 1) + w - 3;
-    for (int t0 = -LAG; t0 < tend; t0 += W) {
+    for (int m = 1; m <= LAG; m++) cin[m] = cf[LAG * W + LAG - m];
+    const int coL = kLt ? cf[kTaps] : 0;
+    int acc[W], ring[U], ring2[U];
 #pragma unroll
-      for (int k = 0; k < W; k++) {
-        const int t = t0 + k;
-        if (t < tend) {
-          const int x = t - 4 * lane;
-          const int xn = x + LAG;  // the column entering the sums
-          const bool inCol = row && x >= 0 && x < w;
-          const int g0 = inCol ? g[y * kGW + x] : 0;
-          if (row && xn >= 0 && xn < w) {
-            // Farthest row first: the row directly above (written one step
-            // ago when LAG = 3) enters this step's output last.
+    for (int j = 0; j < W; j++) acc[j] = ro;
 #pragma unroll
-            for (int d = LAG; d >= 1; d--) {
-              const int v = g[(y - d) * kGW + xn];
+    for (int j = 0; j < U; j++) ring[j] = ring2[j] = 0;
+    const int src = (lane + 31) & 31;
+    const int pos0 = 508 * lane + 132;
+    // The last step finishes column w - 4 of the last AR row.
+    const int tend = 4 * (h - 4) + w - 3;
+    for (int t0 = -4 * LAG; t0 < tend; t0 += U) {
+      int16_t* gp = g + pos0 + t0;
+      const int16_t* lp = kLt ? lt + pos0 + t0 : nullptr;
 #pragma unroll
-              for (int j = W - 1; j >= 0; j--) acc[(j + k) % W] += co[(LAG - d) * W + 2 * LAG - j] * v;
-            }
-          }
-          int out = g0;
-          if (inCol && x >= 3 && x < w - 3) {
-            int sum = acc[k % W];
-            if (lt) sum += lt[y * kGW + x] * coL;
-            out = iclip(g0 + ((sum + ro) >> cs), gmin, gmax);
-            g[y * kGW + x] = (int16_t)out;
-          }
-          // Output x's in-row products for columns x + 1 .. x + LAG; its
-          // slot then serves column x + W.
+      for (int k = 0; k < U; k++) {
+        if constexpr (LAG == 3) {
+          // (row y-3, row y-2) as a pair, then row y-1.
+          const int q = __shfl_sync(0xffffffffu, ring2[(k + U - 4) % U], src);
+          const int v1 = __shfl_sync(0xffffffffu, ring[(k + U - 1) % U], src);
 #pragma unroll
-          for (int m = 1; m <= LAG; m++) acc[(m + k) % W] += co[LAG * W + LAG - m] * out;
-          acc[k % W] = 0;
+          for (int j = W - 1; j >= 0; j--) acc[(j + k) % W] = __dp2a_lo(q, cp[j], acc[(j + k) % W]);
+#pragma unroll
+          for (int j = W - 1; j >= 0; j--) acc[(j + k) % W] += c1[j] * v1;
+          ring2[k] = (int)__byte_perm((unsigned)q, (unsigned)v1, 0x5432);
+        } else if constexpr (LAG == 2) {
+          const int v1 = __shfl_sync(0xffffffffu, ring[(k + U - 2) % U], src);
+          const int v2 = __shfl_sync(0xffffffffu, ring2[(k + U - 4) % U], src);
+          const int pr = (int)__byte_perm((unsigned)v2, (unsigned)v1, 0x5410);
+          ring2[k] = v1;
+#pragma unroll
+          for (int j = W - 1; j >= 0; j--) acc[(j + k) % W] = __dp2a_lo(pr, cp[j], acc[(j + k) % W]);
+        } else {
+          const int v1 = __shfl_sync(0xffffffffu, ring[(k + U - 3) % U], src);
+#pragma unroll
+          for (int j = W - 1; j >= 0; j--) acc[(j + k) % W] += c1[j] * v1;
         }
-        __syncwarp();
+        const int g0 = gp[k];
+        int s = acc[k % W];
+        if constexpr (kLt) s += lp[k] * coL;
+        const int o = iclip(g0 + (s >> cs), gmin, gmax);
+        const int out = g0 >= kNonAr / 2 ? g0 - kNonAr : o;
+        gp[k] = (int16_t)out;
+        ring[k] = out;
+        // Output x's in-row products for columns x + 1 .. x + LAG; its slot
+        // then serves column x + W.
+        acc[k % W] = ro;
+#pragma unroll
+        for (int m = 1; m <= LAG; m++) acc[(m + k) % W] += cin[m] * out;
       }
     }
   }
 }
 
+template <bool kLt>
+__device__ __forceinline__ void ar_warp_lag(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
+  switch (p.lag) {
+    case 0: ar_warp<0, kLt>(g, lt, p, plane, w, h); break;
+    case 1: ar_warp<1, kLt>(g, lt, p, plane, w, h); break;
+    case 2: ar_warp<2, kLt>(g, lt, p, plane, w, h); break;
+    default: ar_warp<3, kLt>(g, lt, p, plane, w, h); break;
+  }
+}
+
 // Luma term of the chroma AR (chroma.go:92-199): at each chroma AR position
 // the luma grain averaged over the co-located 1, 2 or 4 samples, into lt
-// (same layout as the templates).  All threads of the CTA.
+// (chroma layout).  The luma samples read are all AR positions, which hold
+// plain values.  All threads of the CTA.
 __device__ __forceinline__ void luma_term(int16_t* lt, const int16_t* luma, int sx, int sy, int w, int h) {
   const int aw = w - 6;
   for (int i = threadIdx.x; i < aw * (h - 3); i += blockDim.x) {
     const int y = 3 + i / aw, x = 3 + i % aw;
     const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
-    int s = luma[ly * kGW + lx];
-    if (sx) s += luma[ly * kGW + lx + 1];
+    const int a = tpl_at(ly, lx);
+    int s = luma[a];
+    if (sx) s += luma[a + 1];
     if (sy) {
-      s += luma[(ly + 1) * kGW + lx];
-      if (sx) s += luma[(ly + 1) * kGW + lx + 1];
+      const int b = tpl_at(ly + 1, lx);
+      s += luma[b];
+      if (sx) s += luma[b + 1];
     }
-    lt[y * kGW + x] = (int16_t)rpow2(s, sx + sy);
+    lt[tpl_at(y, x)] = (int16_t)rpow2(s, sx + sy);
   }
 }
 
-__device__ __forceinline__ void ar_warp_lag(int16_t* g, const int16_t* lt, const FgTemplateArgs& p, int plane, int w, int h) {
-  switch (p.lag) {
-    case 0: ar_warp<0>(g, lt, p, plane, w, h); break;
-    case 1: ar_warp<1>(g, lt, p, plane, w, h); break;
-    case 2: ar_warp<2>(g, lt, p, plane, w, h); break;
-    default: ar_warp<3>(g, lt, p, plane, w, h); break;
-  }
-}
-
-// Jump matrices: c_jump[t][k][c] = M^(k*L_t) e_c for the three template
-// shapes (t = 0: 82x73, 1: 44x73, 2: 44x38), L_t = ceil(samples / 32).
-__constant__ uint16_t c_jump[3][32][16];
-__constant__ int c_jump_len[3];
+// Jump matrices: g_jump[t][k][c] = M^(k*L_t) e_c for the three template
+// shapes (t = 0: 82x73, 1: 44x73, 2: 44x38), L_t = ceil(samples / 96), so
+// that thread k of the CTA starts its share of the draws at draw k * L_t.
+// Global memory rather than constant: every thread reads its own row.
+__device__ int16_t g_gauss[2048];
+__device__ uint16_t g_jump[3][kFgTemplateThreads][16];
+__device__ int g_jump_len[3];
 
 __device__ __forceinline__ uint16_t gf2_apply(const uint16_t* cols, uint16_t v) {
   uint16_t r = 0;
@@ -157,68 +219,77 @@ __device__ __forceinline__ uint16_t gf2_apply(const uint16_t* cols, uint16_t v) 
 }
 
 // Gaussian fill of one template (luma.go:32-38 / chroma.go:38-44): draw i of
-// the plane's LFSR goes to sample (i / w, i % w).  One warp.
+// the plane's LFSR goes to sample (i / w, i % w).  All threads of the CTA,
+// each walking L consecutive draws from its jumped LFSR state.
 __device__ __forceinline__ void gauss_fill(int16_t* g, const int16_t* gauss, uint16_t seed, int w, int h, int shape, int shift) {
-  const int lane = threadIdx.x & 31;
-  const int L = c_jump_len[shape];
-  uint16_t reg = gf2_apply(c_jump[shape][lane], seed);
-  const int n = w * h;
-  int i = lane * L;
-  const int iend = imin(i + L, n);
+  const int L = g_jump_len[shape];
+  uint16_t reg = gf2_apply(g_jump[shape][threadIdx.x], seed);
+  int i = threadIdx.x * L;
+  const int iend = imin(i + L, w * h);
+  if (i >= iend) return;
   int y = i / w, x = i - y * w;
+  int row = tpl_at(y, 0);
   for (; i < iend; i++) {
-    g[y * kGW + x] = (int16_t)rpow2(gauss[lfsr(reg, 11)], shift);
+    const int v = rpow2(gauss[lfsr(reg, 11)], shift);
+    const bool ar = y >= 3 && x >= 3 && x < w - 3;
+    g[row + x] = (int16_t)(ar ? v : v + kNonAr);
     if (++x == w) {
       x = 0;
-      y++;
+      row = tpl_at(++y, 0);
     }
   }
 }
 
-// One frame's templates: Gaussian fills by warps 0-2 (luma, Cb, Cr), then the
-// AR recursions (luma on warp 0, then Cb and Cr side by side).  s_gl holds
-// the Gaussian sequence while the templates are filled (lanes draw
-// different entries, which constant memory would serialise), then the
-// chroma AR's luma term.
-__device__ __forceinline__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, int16_t (*s_g)[kGW * kGH],
-                             int16_t* s_gl) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// One frame's templates: Gaussian fills of the three planes by the whole
+// CTA, the luma AR on warp 0, the luma term, then the Cb and Cr AR side by
+// side on warps 1 and 2, and the templates written out (stride 82) with
+// the pass-through marks taken off.
+__device__ __forceinline__ void fg_templates(const FgTemplateArgs& p, int16_t* gy, int16_t* gu, int16_t* gv, TplSmem& S) {
+  const int warp = threadIdx.x >> 5;
   int16_t* outs[3] = {gy, gu, gv};
   const int cw = p.ssx ? 44 : kGW, ch = p.ssy ? 38 : kGH;
   const int cshape = p.ssx ? (p.ssy ? 2 : 1) : 0;
-  const int16_t* s_gauss = s_gl;
-  for (int i = threadIdx.x; i < 2048; i += blockDim.x) s_gl[i] = c_gauss[i];
-  __syncthreads();
-  if (warp < 3) {
-    int16_t* g = s_g[warp];
-    for (int i = lane; i < kGW * kGH; i += 32) g[i] = 0;
-    __syncwarp();
-    const bool active = warp == 0 ? p.num_y_points != 0 : p.active[warp];
-    const int shift = 12 - p.bd + p.grain_scale_shift;
-    if (active) {
-      if (warp == 0)
-        gauss_fill(g, s_gauss, p.seed, kGW, kGH, 0, shift);
-      else
-        gauss_fill(g, s_gauss, (uint16_t)(p.seed ^ (warp == 1 ? 0xb524 : 0x49d8)), cw, ch, cshape, shift);
-    }
-    __syncwarp();
+  {
+    const int4 fill = make_int4(0x40004000, 0x40004000, 0x40004000, 0x40004000);
+    static_assert(kNonAr == 0x4000, "fill pattern");
+    int4* g4 = reinterpret_cast<int4*>(S.g[0]);
+    for (int i = threadIdx.x; i < 3 * kTplPlane / 8; i += blockDim.x) g4[i] = fill;
+    const int4* src = reinterpret_cast<const int4*>(g_gauss);
+    int4* dst = reinterpret_cast<int4*>(S.gauss);
+    for (int i = threadIdx.x; i < 2048 / 8; i += blockDim.x) dst[i] = src[i];
   }
   __syncthreads();
-  // Luma on warp 0; then Cb and Cr side by side on warps 1 and 2 (their
-  // luma term reads the finished luma template).
-  if (warp == 0 && p.num_y_points != 0 && p.lag != 0) ar_warp_lag(s_g[0], nullptr, p, 0, kGW, kGH);
+  const int shift = 12 - p.bd + p.grain_scale_shift;
+  if (p.num_y_points != 0) gauss_fill(S.g[0], S.gauss, p.seed, kGW, kGH, 0, shift);
+  if (p.active[1]) gauss_fill(S.g[1], S.gauss, (uint16_t)(p.seed ^ 0xb524), cw, ch, cshape, shift);
+  if (p.active[2]) gauss_fill(S.g[2], S.gauss, (uint16_t)(p.seed ^ 0x49d8), cw, ch, cshape, shift);
+  __syncthreads();
+  if (warp == 0 && p.num_y_points != 0 && p.lag != 0) ar_warp_lag<false>(S.g[0], nullptr, p, 0, kGW, kGH);
   __syncthreads();
   const bool lumaTerm = p.num_y_points != 0;
   if (lumaTerm) {
-    luma_term(s_gl, s_g[0], p.ssx, p.ssy, cw, ch);
+    luma_term(S.lt, S.g[0], p.ssx, p.ssy, cw, ch);
     __syncthreads();
   }
   const bool runC = warp >= 1 && warp <= 2 && p.active[warp] && !(p.lag == 0 && p.num_y_points == 0);
-  if (runC) ar_warp_lag(s_g[warp], lumaTerm ? s_gl : nullptr, p, warp, cw, ch);
+  if (runC) {
+    if (lumaTerm)
+      ar_warp_lag<true>(S.g[warp], S.lt, p, warp, cw, ch);
+    else
+      ar_warp_lag<false>(S.g[warp], nullptr, p, warp, cw, ch);
+  }
   __syncthreads();
-  for (int pl = 0; pl < 3; pl++)
-    if (outs[pl])
-      for (int i = threadIdx.x; i < kGW * kGH; i += blockDim.x) outs[pl][i] = s_g[pl][i];
+  // Two samples per 32-bit store (rows of 82 samples keep pairs aligned).
+  for (int pl = 0; pl < 3; pl++) {
+    if (!outs[pl]) continue;
+    uint32_t* o = reinterpret_cast<uint32_t*>(outs[pl]);
+    for (int i = threadIdx.x; i < kGH * kGW / 2; i += blockDim.x) {
+      const int y = i / (kGW / 2), x = 2 * (i - y * (kGW / 2));
+      const uint32_t s = *reinterpret_cast<const uint32_t*>(&S.g[pl][tpl_at(y, x)]);
+      const int lo = tpl_decode((int16_t)(s & 0xffff)), hi = tpl_decode((int16_t)(s >> 16));
+      o[i] = (uint32_t)(uint16_t)lo | ((uint32_t)(uint16_t)hi << 16);
+    }
+  }
 }
 
 // Offsets of every 32x32 block: row r uses the LFSR seeded by stripe r
@@ -552,12 +623,12 @@ __device__ __forceinline__ void extend_px(const DFrame& f, int plane, int x, int
 // ---- batched kernels ----
 
 __global__ void __launch_bounds__(kFgTemplateThreads) k_fg_templates_batch(BatchArgs b) {
-  __shared__ int16_t s_g[3][kGW * kGH];
-  __shared__ int16_t s_gl[kGW * kGH];  // Gaussian sequence, then the luma term
+  extern __shared__ __align__(16) unsigned char s_tpl[];
+  TplSmem& S = *reinterpret_cast<TplSmem*>(s_tpl);
   const int* base = b.base + ST_FG_TEMPLATES * (b.n + 1);
   for_each_item(b, ST_FG_TEMPLATES, [&](int item) {
     const FrameJob& J = b.jobs[find_frame(base, b.n, item)];
-    fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], s_g, s_gl);
+    fg_templates(J.fgt, J.fg.grain[0], J.fg.grain[1], J.fg.grain[2], S);
   });
 }
 
@@ -679,30 +750,43 @@ static uint16_t lfsr_step_host(uint16_t reg) {
 }
 
 cudaError_t fg_upload_tables() {
-  cudaError_t e = cudaMemcpyToSymbol(c_gauss, pf_gaussian_sequence, sizeof(pf_gaussian_sequence));
+  static_assert(sizeof(pf_gaussian_sequence) == sizeof(g_gauss), "Gaussian sequence length");
+  cudaError_t e = cudaMemcpyToSymbol(g_gauss, pf_gaussian_sequence, sizeof(pf_gaussian_sequence));
   if (e != cudaSuccess) return e;
-  uint16_t jump[3][32][16];
+  uint16_t jump[3][kFgTemplateThreads][16];
   int lens[3];
   const int samples[3] = {82 * 73, 44 * 73, 44 * 38};
   for (int t = 0; t < 3; t++) {
-    const int L = (samples[t] + 31) / 32;
+    const int L = (samples[t] + kFgTemplateThreads - 1) / kFgTemplateThreads;
     lens[t] = L;
     uint16_t cols[16];
     for (int c = 0; c < 16; c++) cols[c] = (uint16_t)(1u << c);
-    for (int k = 0; k < 32; k++) {
+    for (int k = 0; k < kFgTemplateThreads; k++) {
       for (int c = 0; c < 16; c++) jump[t][k][c] = cols[c];
       for (int c = 0; c < 16; c++)
         for (int s = 0; s < L; s++) cols[c] = lfsr_step_host(cols[c]);
     }
   }
-  e = cudaMemcpyToSymbol(c_jump, jump, sizeof(jump));
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_jump_len, lens, sizeof(lens));
+  e = cudaMemcpyToSymbol(g_jump, jump, sizeof(jump));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_jump_len, lens, sizeof(lens));
   return e;
 }
 
 cudaError_t launch_fg_templates_batch(const BatchArgs& b, int total, int grid, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
-  k_fg_templates_batch<<<grid, kFgTemplateThreads, 0, st>>>(b);
+  // The shared layout is above the default 48 KB: opt in once per device.
+  constexpr int kMaxDevices = 64;
+  static std::atomic<bool> configured[kMaxDevices];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!configured[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(k_fg_templates_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TplSmem));
+    if (e != cudaSuccess) return e;
+    configured[dev].store(true, std::memory_order_release);
+  }
+  k_fg_templates_batch<<<grid, kFgTemplateThreads, sizeof(TplSmem), st>>>(b);
   return cudaGetLastError();
 }
 
