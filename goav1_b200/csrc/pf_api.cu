@@ -1009,7 +1009,14 @@ static int enqueue_batch(pf_ctx* c, const FrameJob* hjobs, const int* hbase, con
     a = args(ST_EXTEND, f0, f1, gi, &g);
     CK(launch_extend_batch(a, count(ST_EXTEND, f0, f1), g, gs));
     if (stageEv) CK(cudaEventRecord(c->ev[4], gs));
-    if (c->mark_chain && gi == 0) CK(cudaEventRecord(c->chain_done, gs));
+    if (c->mark_chain && gi == 0) {
+      // While capturing, an external event node: each replay records it
+      // for the copy stream that waits on it outside the graph.
+      cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+      CK(cudaStreamIsCapturing(gs, &cap));
+      CK(cap == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(c->chain_done, gs, cudaEventRecordExternal)
+                                               : cudaEventRecord(c->chain_done, gs));
+    }
     if (fg) CK(cudaStreamWaitEvent(gs, c->join, 0));
     a = args(ST_FG_APPLY, f0, f1, gi, &g);
     CK(launch_fg_apply_batch(a, count(ST_FG_APPLY, f0, f1), g, gs));
@@ -1041,6 +1048,7 @@ static std::vector<int64_t> batch_key(const pf_ctx* c, int n, bool fg) {
   }
   k.push_back(c->db_tile);
   k.push_back(c->frame_groups);
+  k.push_back(c->mark_chain);
   for (int v : c->hbase) k.push_back(v);
   return k;
 }
@@ -1317,7 +1325,7 @@ extern "C" int pf_frame_apply(pf_ctx* c, const pf_frame* f, const pf_frame_side*
   }
   if (split && !c->chain_done) CK(cudaEventCreateWithFlags(&c->chain_done, cudaEventDisableTiming));
   c->mark_chain = split;
-  st = run_batch(c, &r, 1, stats);
+  st = run_batch(c, &r, 1, stats, c->graphs != 0);
   c->mark_chain = false;
   if (st != PF_OK) return st;
   if (split) {

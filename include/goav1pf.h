@@ -311,6 +311,9 @@ int pf_batch_apply(pf_ctx* ctx, const pf_batch_item* items, int32_t n, pf_stats*
  *     that signature replay it, with only their job tables refreshed.  Up to
  *     8 signatures are kept; a change of the context's scratch buffers
  *     recaptures.  Graphs are not used while the context times stages.
+ *     The switch covers batches of device frames and single-frame calls
+ *     (pf_frame_apply, a batch of one); host-frame batches pipeline their
+ *     chunks without graphs.
  *   - The schedule of each stage group (pf_schedule, pf_set_schedule):
  *       ctas           persistent CTAs draining the stage's items through an
  *                      atomic counter (0 = one CTA per chunk);

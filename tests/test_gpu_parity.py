@@ -175,3 +175,34 @@ def test_film_grain_ar_lags(runner, lag, variant):
     if variant == "cfl":
         fg.chroma_scaling_from_luma = 1
     _check(runner, fr, si)
+
+
+def test_frame_apply_graphs_match_oracle():
+    """Single-frame calls with the context's graphs on (pf_batch_graphs): a
+    call of a new signature captures the chain, with the event the
+    reference frame's download waits on as an external node, and the next
+    call of that signature replays it with new frames.  Pageable host frames,
+    page-locked host frames and device frames, each call against the oracle."""
+    from goav1_b200.postfilter import DeviceFrame, PostFilterRunner, device_side
+
+    r = PostFilterRunner()
+    try:
+        r.batch_graphs(True)
+        frames = [synth.make_frame(1, 7 + i, width=320, height=240) for i in range(2)]
+        for fr, si in frames:
+            ref, rdisp = _oracle(fr, si)
+            for call in range(2):  # capture, then replay
+                out, gdisp = _gpu(r, fr, si)
+                _assert_same(ref, out, "pageable reference frame, call %d" % call)
+                _assert_same(rdisp, gdisp, "pageable display frame, call %d" % call)
+                out, gdisp = fr.back_to_back(pinned=True), fr.back_to_back(pinned=True, like=True)
+                r.apply(out.pf(), si.side, gdisp.pf())
+                _assert_same(ref, out, "page-locked reference frame, call %d" % call)
+                _assert_same(rdisp, gdisp, "page-locked display frame, call %d" % call)
+                d, dd, ds = DeviceFrame(fr), DeviceFrame(fr.like()), device_side(si, fr)
+                r.apply(d.pf(), ds.side, dd.pf())
+                r.sync()
+                _assert_same(ref, d.download(), "device reference frame, call %d" % call)
+                _assert_same(rdisp, dd.download(), "device display frame, call %d" % call)
+    finally:
+        r.close()
