@@ -714,16 +714,12 @@ def main():
             for out, disp, si in hb:
                 runner.apply(out.pf(), si.side, disp.pf())
 
-        # One call per frame, as a decoder makes them, with the context's
-        # graphs on (each call replays the chain captured for its signature).
-        runner.batch_graphs(True)
         per_frame()
         ps = dist.max_over_ranks(timed_host(per_frame, 2), world, device="cuda")
-        runner.batch_graphs(False)
         e2e = {"value": world * px / es / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": es * 1e3, "per_frame_calls_value": world * px / ps / 1e6,
                "note": "page-locked host frames; one pf_batch_apply per step (median of steps), per_frame_calls = "
-                       "one pf_frame_apply per frame (graphs on)"}
+                       "one pf_frame_apply per frame"}
 
     # Encoder CDEF strength search, exhaustive and learned, on the held-out
     # learned-selection frames (1080p 8-bit 4:2:0, seeds 2000..): source
