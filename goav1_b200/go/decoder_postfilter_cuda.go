@@ -87,8 +87,8 @@ func statusError(st C.int) error {
 	}
 }
 
-// cbool and cbool32 convert flags for the C structs (the record map binding
-// in INTEGRATION.md uses them too).
+// cbool and cbool32 convert flags for the C structs (a binding of
+// pf_lf_build's block record map would use them too).
 func cbool(v bool) C.uint8_t {
 	if v {
 		return 1
