@@ -316,7 +316,7 @@ __device__ int compact_blocks(const uint8_t* skip, int nfb, int* list, int* wsum
     const int fb = b0 + t;
     const bool keep = fb < nfb && !skip[fb];
     const unsigned m = __ballot_sync(0xffffffffu, keep);
-    __syncthreads();  // the previous round is done with wsum
+    __syncthreads();  // the previous chunk of blocks is done with wsum
     if ((t & 31) == 0) wsum[t >> 5] = __popc(m);
     __syncthreads();
     int off = base;
